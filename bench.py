@@ -1,0 +1,342 @@
+"""Benchmark of the candidate-verification path on B200.
+
+Workload (default): every unpruned length-2 target over the reference's
+8-bit instruction list (9,818,041 targets), candidates of length 1, the
+first-found semantics of pkg/search (QuickCheck -> ExhaustiveCheck per
+target, shortest/first candidate wins).  One step = one pass of the whole
+pipeline over the whole target set.
+
+Metric: candidate checks/s = (target, candidate) pairs of the workload that
+pass the byte-size and prune filters (the QuickCheck unit of work), per
+second of the step.  `value` runs on targets already resident in HBM
+(z80b_stage_job / z80b_run_staged, device time from CUDA events on the
+library's stream); `e2e` calls z80b_search with pinned host buffers, so
+every step includes the H2D copy of the targets and the D2H copy of the
+rules.  Between steps L2 is flushed by writing a 512 MiB buffer.
+
+`--impl reference` times the CPU oracle (the C++ restatement of the
+reference's Go search; the Go toolchain is not available) on a bounded
+sample of the same workload with all host threads.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "z80-optimizer_b200")
+sys.path.insert(0, PKG)
+
+import numpy as np  # noqa: E402
+
+METRIC = "Z80 candidate checks/s on 1 B200, batched vs plain GPU; p50/p99 query latency"
+UNIT = "candidate checks/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--targets", type=int, default=0, help="limit the target count (0 = all)")
+    ap.add_argument("--dead-flags", default="none")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample", type=int, default=0, help="targets in the CPU sample (0 = auto)")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while running (median SM clock, reasons)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.stop = threading.Event()
+        self.t = None
+
+    def _run(self):
+        while not self.stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"],
+                                     capture_output=True, text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self.stop.wait(0.2)
+
+    def __enter__(self):
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop.set()
+        self.t.join()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if len(r) > 5 + i and r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def eligible_checks(targets):
+    """QuickCheck units of a target set: candidates of the 4,531-instruction
+    list shorter than the target and not pruned (162 one-byte ones for a
+    two-byte target, 4,523 otherwise)."""
+    import z80b
+    sizes = np.array([z80b.op_info(op)["size"] for op in range(455)], dtype=np.int32)
+    pool = np.array(z80b.pool8(), dtype=np.uint32)
+    psize = sizes[pool & 0xFFFF]
+    prune = np.array([z80b.should_prune([int(w)]) for w in pool])
+    tb = sizes[(targets & 0xFFFF)].sum(axis=1)
+    counts = np.array([np.count_nonzero((psize < b) & ~prune) for b in range(0, 9)], dtype=np.int64)
+    return int(counts[tb].sum())
+
+
+def make_job(z80b, arr, dead):
+    n, L = arr.shape
+    job = z80b.Job()
+    job.targets = ctypes.cast(arr.ctypes.data, ctypes.POINTER(ctypes.c_uint32))
+    job.n_targets = n
+    job.target_len = L
+    job.target_stride = L
+    job.max_cand_len = 1
+    job.global_dead_flags = dead
+    job.mode = z80b.MODE_FIRST
+    job.path = z80b.PATH_BATCHED
+    return job
+
+
+def cpu_run(sample, dead, workers):
+    """Oracle (CPU restatement of the reference search) over a target sample;
+    returns (seconds, rules)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib
+    t0 = time.perf_counter()
+    rules, _ = oracle_lib.search([list(map(int, r)) for r in sample], 1, dead=dead, workers=workers)
+    return time.perf_counter() - t0, len(rules)
+
+
+def cpu_baseline(all_targets, dead, n_sample, seed=0):
+    workers = os.cpu_count() or 1
+    rng = np.random.default_rng(seed)
+    idx = np.sort(rng.choice(len(all_targets), size=min(n_sample, len(all_targets)), replace=False))
+    sample = all_targets[idx]
+    secs, _ = cpu_run(sample, dead, workers)
+    checks = eligible_checks(sample)
+    return {"value": checks / secs, "unit": UNIT, "cores": workers, "kind": "port",
+            "sample": f"{len(sample)} targets drawn by index (seed {seed}) from the workload; "
+                      f"{checks} candidate checks in {secs:.2f} s with {workers} threads"}
+
+
+def auto_cpu_sample():
+    # about 20 core-seconds of oracle work (~0.8 ms per target per core)
+    return max(2000, min(60000, 25000 * (os.cpu_count() or 1) // 8))
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    import z80b
+    import workloads
+    dead = z80b.parse_dead_flags(args.dead_flags)
+    allt = workloads.c2_targets()
+    if args.targets:
+        allt = allt[:args.targets]
+    workload = {"workload": "full length-2 (C2)", "targets": int(len(allt)), "target_len": 2,
+                "max_cand_len": 1, "candidates": 4531, "semantics": "pkg/search first-found",
+                "dead_flags": dead, "vectors": "reference QuickCheck 8 (verifier.go:19-28)",
+                "l2": "flushed between steps (512 MiB write)"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        n_sample = args.cpu_sample or max(1000, auto_cpu_sample() // 4)
+        workers = os.cpu_count() or 1
+        times, checks = [], 0
+        rng = np.random.default_rng(1)
+        for i in range(args.warmup + args.steps):
+            idx = np.sort(rng.choice(len(allt), size=n_sample, replace=False))
+            sample = allt[idx]
+            secs, _ = cpu_run(sample, dead, workers)
+            if i >= args.warmup:
+                times.append(secs)
+                checks += eligible_checks(sample)
+        total = sum(times)
+        value = checks / total
+        line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u8",
+                "data": "synthetic", "config": dict(workload, sample_targets_per_step=n_sample),
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port",
+                                 "sample": f"{n_sample} targets per step, seeded draws by index"},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    # strong scaling: the fixed target set is split into contiguous shards
+    lo = len(allt) * rank // world
+    hi = len(allt) * (rank + 1) // world
+    mine = np.ascontiguousarray(allt[lo:hi])
+    ctx = z80b.Context(local if world > 1 else 0)
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+
+    # ---- value: targets resident in HBM
+    job = make_job(z80b, mine, dead)
+    ctx.stage(job)
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        ctx.run_staged()
+    dev_ms, exh_ms, qc_ms, launches, checks, states, rules = 0.0, 0.0, 0.0, 0, 0, 0, 0
+    stats_last = None
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            n, st = ctx.run_staged()
+            dev_ms += st.device_ms
+            exh_ms += st.exh_ms
+            qc_ms += st.qc_ms
+            launches += st.launches
+            checks += st.checks
+            states += st.exhaustive_states
+            rules = n
+            stats_last = st
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    t_step = dev_ms / args.steps
+    if dist:
+        t = torch.tensor([t_step], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_step = float(t.item())
+        c = torch.tensor([checks], device="cuda", dtype=torch.float64)
+        dist.all_reduce(c)
+        checks_all = float(c.item())
+    else:
+        checks_all = float(checks)
+    value = checks_all / args.steps / (t_step / 1e3)
+
+    # ---- e2e: public API with pinned host buffers
+    pinned = torch.from_numpy(mine).pin_memory()
+    pj = make_job(z80b, mine, dead)
+    pj.targets = ctypes.cast(pinned.data_ptr(), ctypes.POINTER(ctypes.c_uint32))
+    cap = max(1024, 2 * rules + 1024)
+    out = (z80b.Rule * cap)()
+    nr = ctypes.c_uint64()
+    st2 = z80b.Stats()
+    L = z80b.lib()
+    for _ in range(max(1, args.warmup)):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        ctx._check(L.z80b_search(ctx._h, ctypes.byref(pj), out, cap, ctypes.byref(nr), ctypes.byref(st2)))
+    e2e_t = 0.0
+    e2e_checks = 0
+    for _ in range(args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t1 = time.perf_counter()
+        ctx._check(L.z80b_search(ctx._h, ctypes.byref(pj), out, cap, ctypes.byref(nr), ctypes.byref(st2)))
+        e2e_t += time.perf_counter() - t1
+        e2e_checks += st2.checks
+    e2e_step = e2e_t / args.steps
+    if dist:
+        t = torch.tensor([e2e_step], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_step = float(t.item())
+        c = torch.tensor([e2e_checks], device="cuda", dtype=torch.float64)
+        dist.all_reduce(c)
+        e2e_checks = float(c.item())
+    e2e_value = e2e_checks / args.steps / e2e_step
+    h2d = int(mine.nbytes)
+    d2h = int(nr.value) * 12 + 64
+
+    # ---- roofline of the dominant kernel (ExhaustiveCheck sweep)
+    rl = json.load(open(os.path.join(PKG, "roofline.json")))
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    sm_mhz = peaks.get("sm_max_mhz", 1965.0)
+    per_state = 3 * rl["ops_per_emulated_insn"] + rl["ops_per_state"]  # 2-insn target + 1-insn candidate
+    achieved = states / args.steps * per_state / (exh_ms / args.steps / 1e3) / 1e12 if exh_ms else 0.0
+    peak = rl["sms"] * rl["int32_lanes_per_sm"] * sm_mhz * 1e6 / 1e12
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "exhaustive_c2_traffic.txt")
+    if os.path.exists(tf):
+        for line in open(tf):
+            if line.startswith("dram_bytes_per_launch:"):
+                traffic = float(line.split(":")[1])
+    roofline = {"bound": "issue", "kernel": "k_exhaustive", "achieved": achieved, "peak": peak,
+                "unit": "Tops/s (INT32 lane-ops)", "frac": achieved / peak if peak else None,
+                "traffic": traffic,
+                "peak_source": f"{rl['sms']} SMs x {rl['int32_lanes_per_sm']} INT32 lanes x "
+                               f"sm_max_mhz {sm_mhz} of MEASURED_PEAKS.json",
+                "algorithmic_ops_per_state": per_state,
+                "exhaustive_ms_per_step": exh_ms / args.steps, "qc_ms_per_step": qc_ms / args.steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(allt, dead, args.cpu_sample or auto_cpu_sample())
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_step, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": dict(workload, path="batched", parallelism=f"targets sharded over {world} GPU(s)"),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": 1e3 * e2e_step},
+            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
+            "gpu_launches": launches,
+            "detail": {"rules": rules, "checked_ref": stats_last.checked_ref if stats_last else None,
+                       "qc_survivors": stats_last.qc_survivors if stats_last else None,
+                       "exhaustive_pairs": stats_last.exhaustive_pairs if stats_last else None,
+                       "exhaustive_states_per_step": states / args.steps, "rounds": stats_last.rounds if stats_last else None,
+                       "wall_s_timed": wall}}
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

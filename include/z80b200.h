@@ -1,0 +1,198 @@
+/* z80b200.h -- C ABI of libz80b200.so, the B200 (sm_100a) implementation of
+ * the Z80 superoptimizer's candidate-verification path.
+ *
+ * Drop-in boundary: these entry points replace the child process
+ * `cuda/z80qc --server` and its stdin/stdout protocol (pkg/gpu/cuda.go:32-113,
+ * cuda/z80_quickcheck.cu:823-923) with in-process calls, and expose the whole
+ * verification pipeline of pkg/search (QuickCheck -> [MidCheck] ->
+ * ExhaustiveCheck, first-found or all-hits) for a batch of targets.
+ *
+ * Conventions
+ *  - Instructions are packed as uint32 op | imm << 16, the packing of
+ *    pkg/gpu/cuda.go:310 (op = the reference's OpCode enum, 0..454).
+ *  - The caller owns every host buffer; the library copies in and out.  The
+ *    library owns all device memory.
+ *  - Every call returns a status (Z80B_OK = 0).  z80b_last_error() gives the
+ *    message of the last failure on a context.
+ *  - A context is bound to one device and is not thread-safe: use one
+ *    context per host thread (queries of one context are serialized, as
+ *    pkg/gpu/cuda.go:80 serializes queries with a mutex).
+ */
+#ifndef Z80B200_H_
+#define Z80B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define Z80B_OK 0
+#define Z80B_EINVAL 1     /* bad argument (null pointer, opcode > 454, length) */
+#define Z80B_ENOMEM 2     /* device allocation failed */
+#define Z80B_ECUDA 3      /* CUDA runtime error */
+#define Z80B_ETIMEOUT 4   /* a bounded device wait ran out */
+#define Z80B_ECAPACITY 5  /* caller's output buffer too small (count reported) */
+#define Z80B_ENODEV 6     /* no CUDA device / wrong architecture */
+#define Z80B_ESTATE 7     /* call order (e.g. quickcheck before load) */
+
+#define Z80B_NUM_OPS 455
+#define Z80B_FP_LEN 80    /* search.FingerprintLen (pkg/search/verifier.go:130) */
+
+typedef struct z80b_ctx z80b_ctx;
+
+/* cpu.State (pkg/cpu/state.go:11-15) in C layout (12 bytes). */
+typedef struct z80b_state {
+  uint8_t a, f, b, c, d, e, h, l;
+  uint16_t sp;
+  uint8_t m, pad;
+} z80b_state;
+
+/* result.Rule (pkg/result/table.go:11-17) plus the index of its target in
+ * the job.  dead_regs is the register extension (bit 0..5 = B,C,D,E,H,L):
+ * 0 for every rule of the reference semantics. */
+typedef struct z80b_rule {
+  uint32_t src[4];
+  uint32_t rep[4];
+  int32_t src_len, rep_len;
+  int32_t bytes_saved, cycles_saved;
+  int32_t dead_flags;
+  int32_t target_index;
+  int32_t dead_regs;
+  int32_t reserved;
+} z80b_rule;
+
+typedef struct z80b_stats {
+  uint64_t targets;
+  uint64_t checks;          /* (target, candidate) QuickCheck evaluations after the
+                               byte-size and prune filters */
+  uint64_t checked_ref;     /* the reference's 'checked' counter (worker.go:134) */
+  uint64_t qc_survivors;
+  uint64_t mid_survivors;   /* Z80B_MODE_ALL only */
+  uint64_t exhaustive_pairs;
+  uint64_t exhaustive_states;
+  uint64_t rules;
+  uint32_t rounds;          /* ExhaustiveCheck rounds of the first-found pass */
+  uint32_t launches;        /* kernels launched by this call */
+  double device_ms;         /* whole pipeline, first to last event on the context's stream */
+  double qc_ms, exh_ms;     /* summed durations of the QuickCheck scan kernels and of the
+                               ExhaustiveCheck kernels (CUDA events around each launch) */
+} z80b_stats;
+
+/* Semantics of a search job. */
+#define Z80B_MODE_FIRST 0 /* pkg/search worker.go:124-265: per target the first
+                             candidate (enumeration order, shortest length first)
+                             passing QuickCheck + ExhaustiveCheck; then, if dead
+                             flags are set, the masked pass */
+#define Z80B_MODE_ALL 1   /* pkg/gpu/search.go:80-199: fingerprint QuickCheck,
+                             byte filter, prune, MidCheck, ExhaustiveCheck; every
+                             passing length-1 candidate kept */
+/* Execution path. */
+#define Z80B_PATH_BATCHED 0 /* every target of the job in one pipeline */
+#define Z80B_PATH_PLAIN 1   /* one target per launch, synchronizing per target */
+
+typedef struct z80b_job {
+  const uint32_t* targets;      /* n_targets * target_stride packed instructions */
+  const uint8_t* target_lens;   /* per-target length 1..4, or NULL: target_len */
+  const uint8_t* dead_flags;    /* per-target dead-flag mask or NULL: global_dead_flags */
+  const uint8_t* dead_regs;     /* per-target dead-register mask (extension) or NULL */
+  uint32_t n_targets;
+  uint32_t target_len;
+  uint32_t target_stride;       /* words per target, >= the longest target */
+  uint32_t max_cand_len;        /* 1 (candidates are the 4,531 8-bit instructions) */
+  uint32_t global_dead_flags;   /* search.FlagMask applied to every target */
+  uint32_t mode;                /* Z80B_MODE_* */
+  uint32_t path;                /* Z80B_PATH_* */
+  uint32_t reserved;
+} z80b_job;
+
+/* ---- context ---------------------------------------------------------- */
+int z80b_init(int device, z80b_ctx** out);
+void z80b_destroy(z80b_ctx* ctx);
+const char* z80b_last_error(const z80b_ctx* ctx);
+const char* z80b_status_string(int status);
+int z80b_version(void);
+
+/* ---- primitives --------------------------------------------------------- */
+/* search.Fingerprint (pkg/search/verifier.go:134-151) of n sequences of
+ * `len` instructions each: 80 bytes per sequence into out. */
+int z80b_fingerprints(z80b_ctx* ctx, const uint32_t* seqs, uint32_t n, uint32_t len, uint8_t* out);
+
+/* Runs n sequences (stride words, lengths lens[] or len) from initial states
+ * in[] and writes the final states (execSeq, pkg/search/verifier.go:75-81). */
+int z80b_exec(z80b_ctx* ctx, const z80b_state* in, const uint32_t* seqs, const uint8_t* lens,
+              uint32_t len, uint32_t stride, uint32_t n, z80b_state* out);
+
+/* gpu.NewCUDAProcess (pkg/gpu/cuda.go:32-75): uploads the candidate list
+ * once; count * seq_len packed instructions. */
+int z80b_load_candidates(z80b_ctx* ctx, const uint32_t* cands, uint32_t count, uint32_t seq_len);
+
+/* CUDAProcess.QuickCheckGPU (pkg/gpu/cuda.go:79-107): indices (ascending) of
+ * the loaded candidates whose 80-byte fingerprint equals fp with the flag
+ * bits of dead_flags ignored in every F byte.  Writes up to cap indices and
+ * the full count to *n_hits (Z80B_ECAPACITY if count > cap). */
+int z80b_quickcheck(z80b_ctx* ctx, const uint8_t* fp80, uint32_t dead_flags, uint32_t* hits,
+                    uint32_t cap, uint32_t* n_hits);
+
+/* Batched verifier tiers over n (target, candidate) pairs: for pair i,
+ * tgt[i*stride..] (tlens[i]) vs cand[i*stride..] (clens[i]).
+ * tiers: bit0 QuickCheck[Masked], bit1 MidCheck[Masked], bit2
+ * ExhaustiveCheck[Masked] (verifier.go:85-123,159-171,626-654); out[i] has
+ * bit k set when tier k passed (tiers not requested are left 0).
+ * dead: per-pair dead-flag masks or NULL (0).  flagdiff: optional out,
+ * FlagDiff (verifier.go:658-673) per pair. */
+int z80b_verify_pairs(z80b_ctx* ctx, const uint32_t* tgt, const uint8_t* tlens,
+                      const uint32_t* cand, const uint8_t* clens, uint32_t stride, uint32_t n,
+                      const uint8_t* dead, uint32_t tiers, uint8_t* out, uint8_t* flagdiff);
+
+/* ---- whole pipeline ------------------------------------------------------ */
+/* Runs the job and writes its rules (grouped by target index; within a
+ * target the full-equivalence rule precedes the masked one, and all-hits
+ * rules follow candidate order).  Writes up to cap rules and the total to
+ * *n_rules (Z80B_ECAPACITY if it did not fit).  stats may be NULL. */
+int z80b_search(z80b_ctx* ctx, const z80b_job* job, z80b_rule* out, uint64_t cap,
+                uint64_t* n_rules, z80b_stats* stats);
+
+/* Device-resident variant for timing the pipeline without host copies:
+ * z80b_stage_job uploads the job's targets once; z80b_run_staged runs the
+ * pipeline on them and keeps the rules on the device (count in *n_rules);
+ * z80b_fetch_rules copies them out. */
+int z80b_stage_job(z80b_ctx* ctx, const z80b_job* job);
+int z80b_run_staged(z80b_ctx* ctx, uint64_t* n_rules, z80b_stats* stats);
+int z80b_fetch_rules(z80b_ctx* ctx, z80b_rule* out, uint64_t cap, uint64_t* n_rules);
+
+/* ---- host helpers (no device work) ---------------------------------------- */
+/* inst.Catalog entry (pkg/inst/catalog.go:4-145): mnemonic with n/nn
+ * placeholders, encoded size incl. immediate, T-states, immediate kind
+ * (0 none, 1 imm8, 2 imm16) and the opReads/opWrites register masks
+ * (pkg/search/verifier.go:199-408, pruner.go:66-236). */
+int z80b_op_info(uint32_t op, char* mnemonic, uint32_t cap, int* size, int* tstates, int* imm_kind,
+                 int* reads, int* writes);
+/* inst.Disassemble of a sequence joined by " : " (pkg/search/worker.go:273-282);
+ * returns the text length, -1 on a bad opcode. */
+int z80b_disasm_seq(const uint32_t* seq, uint32_t n, char* buf, uint32_t cap);
+/* parseAssembly (cmd/z80opt/main.go:325-397): returns the instruction count
+ * (writing up to cap) or -1 when the text does not parse. */
+int z80b_parse_assembly(const char* text, uint32_t* out, uint32_t cap);
+/* parseDeadFlags (cmd/z80opt/main.go:305-322). */
+int z80b_parse_dead_flags(const char* text, uint32_t* out);
+/* result.DeadFlagDesc (pkg/result/output.go:93-129). */
+int z80b_dead_flag_desc(uint32_t mask, char* buf, uint32_t cap);
+/* search.ShouldPrune (pkg/search/pruner.go:7-35): 1, 0, or -1 on a bad opcode. */
+int z80b_should_prune(const uint32_t* seq, uint32_t n);
+/* The 8-bit instruction list in EnumerateSequences8 order
+ * (pkg/search/enumerator.go:319-345); returns its length (4531). */
+uint32_t z80b_pool8(uint32_t* out, uint32_t cap);
+/* EnumerateSequences + ShouldPrune over a caller's instruction pool
+ * (pkg/search/enumerator.go:280-345, search.go:341-361): the unpruned
+ * sequences of length len (1..4) in odometer order, len words each; writes up
+ * to cap sequences and returns the total. */
+uint64_t z80b_enumerate(const uint32_t* pool, uint32_t npool, uint32_t len, uint32_t* out, uint64_t cap);
+/* result.WriteJSON (pkg/result/output.go:70-90). */
+long long z80b_rules_json(const z80b_rule* rules, uint64_t n, char* buf, uint64_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* Z80B200_H_ */

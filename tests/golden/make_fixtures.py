@@ -1,0 +1,24 @@
+"""Regenerates the golden fixtures derived from the reference's data files.
+
+Run in a checkout where the reference is mounted (its path is the only
+argument, default /root/reference).  Writes:
+  peephole_top500_pairs.json -- (source, replacement, bytes_saved,
+      cycles_saved) of the reference's data/peephole_top500.json, the 500
+      rules its CUDA pipeline reported for length-2 targets.  Every pair is
+      an equivalence the ExhaustiveCheck of pkg/search must accept.
+reference_known_answers.json is transcribed by hand from the reference's
+Go tests (each case cites its file:line) and is not regenerated here.
+"""
+import json
+import os
+import sys
+
+ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+here = os.path.dirname(os.path.abspath(__file__))
+src = json.load(open(os.path.join(ref, "data", "peephole_top500.json")))
+pairs = [{"source": r["source"], "replacement": r["replacement"],
+          "bytes_saved": r["bytes_saved"], "cycles_saved": r["cycles_saved"]} for r in src]
+with open(os.path.join(here, "peephole_top500_pairs.json"), "w") as f:
+    json.dump({"_about": "derived from data/peephole_top500.json of the reference by make_fixtures.py",
+               "pairs": pairs}, f, indent=1)
+print(len(pairs), "pairs")

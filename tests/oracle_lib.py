@@ -1,0 +1,250 @@
+"""ctypes binding of the CPU oracle (test infrastructure only).
+
+The oracle (oracle/*.cpp) restates the reference's pkg/inst, pkg/cpu and
+pkg/search behaviour; tests use it as the checker for the CUDA path.
+"""
+import ctypes
+import os
+import subprocess
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE_DIR = os.path.join(ROOT, "oracle")
+ORACLE_SO = os.path.join(ORACLE_DIR, "_build", "liboracle.so")
+
+
+class OrcState(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint8) for n in "AFBCDEHL"] + [
+        ("SP", ctypes.c_uint16), ("M", ctypes.c_uint8), ("pad", ctypes.c_uint8)]
+
+    def tup(self):
+        return (self.A, self.F, self.B, self.C, self.D, self.E, self.H, self.L, self.SP, self.M)
+
+
+class OrcRule(ctypes.Structure):
+    _fields_ = [("src", ctypes.c_uint32 * 4), ("rep", ctypes.c_uint32 * 4),
+                ("src_len", ctypes.c_int32), ("rep_len", ctypes.c_int32),
+                ("bytes_saved", ctypes.c_int32), ("cycles_saved", ctypes.c_int32),
+                ("dead_flags", ctypes.c_int32), ("target_index", ctypes.c_int32)]
+
+    def key(self):
+        return (self.target_index, tuple(self.src[:self.src_len]), tuple(self.rep[:self.rep_len]),
+                self.bytes_saved, self.cycles_saved, self.dead_flags)
+
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            build()
+        L = ctypes.CDLL(ORACLE_SO)
+        u32p = ctypes.POINTER(ctypes.c_uint32)
+        L.orc_exhaustive_states.restype = ctypes.c_ulonglong
+        L.orc_search.restype = ctypes.c_longlong
+        L.orc_search.argtypes = [u32p, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
+                                 ctypes.c_int, ctypes.c_int, ctypes.POINTER(OrcRule),
+                                 ctypes.c_longlong, ctypes.POINTER(ctypes.c_ulonglong)]
+        L.orc_search_gpu.restype = ctypes.c_longlong
+        L.orc_search_gpu.argtypes = [u32p, ctypes.POINTER(ctypes.c_int), ctypes.c_int, u32p,
+                                     ctypes.c_int, ctypes.c_int, ctypes.POINTER(OrcRule),
+                                     ctypes.c_longlong]
+        L.orc_init()
+        _lib = L
+    return _lib
+
+
+def pack(op, imm=0):
+    return (op & 0xFFFF) | ((imm & 0xFFFF) << 16)
+
+
+def arr(seq):
+    return (ctypes.c_uint32 * max(1, len(seq)))(*seq)
+
+
+def op_count():
+    return lib().orc_op_count()
+
+
+def op_name(op):
+    b = ctypes.create_string_buffer(32)
+    lib().orc_op_name(op, b, 32)
+    return b.value.decode()
+
+
+OPS = None
+
+
+def ops():
+    """name -> opcode"""
+    global OPS
+    if OPS is None:
+        OPS = {op_name(i): i for i in range(op_count())}
+    return OPS
+
+
+def catalog(op):
+    m = ctypes.create_string_buffer(64)
+    enc = (ctypes.c_uint8 * 4)()
+    n, t, b = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    lib().orc_catalog(op, m, 64, enc, ctypes.byref(n), ctypes.byref(t), ctypes.byref(b))
+    return m.value.decode(), bytes(enc[:n.value]), t.value, b.value
+
+
+def state(**kw):
+    s = OrcState()
+    for k, v in kw.items():
+        setattr(s, k, v)
+    return s
+
+
+def exec1(st, op, imm=0):
+    t = lib().orc_exec(ctypes.byref(st), op, imm)
+    return t
+
+
+def exec_seq(st, seq):
+    out = OrcState()
+    lib().orc_exec_seq(ctypes.byref(st), arr(seq), len(seq), ctypes.byref(out))
+    return out
+
+
+def disasm(seq):
+    b = ctypes.create_string_buffer(256)
+    lib().orc_disasm_seq(arr(seq), len(seq), b, 256)
+    return b.value.decode()
+
+
+def quickcheck(t, c, dead=0):
+    return bool(lib().orc_quickcheck(arr(t), len(t), arr(c), len(c), dead))
+
+
+def midcheck(t, c, dead=0):
+    return bool(lib().orc_midcheck(arr(t), len(t), arr(c), len(c), dead))
+
+
+def exhaustive(t, c, dead=0):
+    return bool(lib().orc_exhaustive(arr(t), len(t), arr(c), len(c), dead))
+
+
+def exhaustive_states(t, c):
+    return int(lib().orc_exhaustive_states(arr(t), len(t), arr(c), len(c)))
+
+
+def flagdiff(t, c):
+    return lib().orc_flagdiff(arr(t), len(t), arr(c), len(c))
+
+
+def fingerprint(seq):
+    out = (ctypes.c_uint8 * 80)()
+    lib().orc_fingerprint(arr(seq), len(seq), out)
+    return bytes(out)
+
+
+def should_prune(seq):
+    return bool(lib().orc_should_prune(arr(seq), len(seq)))
+
+
+def op_reads(op):
+    return lib().orc_op_reads(op)
+
+
+def op_writes(op):
+    return lib().orc_op_writes(op)
+
+
+def instructions8():
+    buf = (ctypes.c_uint32 * 8192)()
+    n = lib().orc_instructions8(buf, 8192)
+    return list(buf[:n])
+
+
+def test_vectors():
+    qc = (OrcState * 8)()
+    mid = (OrcState * 32)()
+    lib().orc_test_vectors(qc, mid)
+    return [s.tup() for s in qc], [s.tup() for s in mid]
+
+
+def _targets(targets):
+    n = len(targets)
+    flat = (ctypes.c_uint32 * max(1, 4 * n))()
+    lens = (ctypes.c_int * max(1, n))()
+    for i, t in enumerate(targets):
+        lens[i] = len(t)
+        for j, w in enumerate(t):
+            flat[4 * i + j] = w
+    return flat, lens
+
+
+def search(targets, max_cand_len, dead=0, workers=0, cap=None):
+    """worker.go semantics over a target list; returns (rules, checked)."""
+    flat, lens = _targets(targets)
+    cap = cap or (2 * len(targets) + 16)
+    out = (OrcRule * cap)()
+    checked = ctypes.c_ulonglong()
+    w = workers or os.cpu_count() or 1
+    n = lib().orc_search(flat, lens, len(targets), max_cand_len, dead, w, out, cap,
+                         ctypes.byref(checked))
+    assert n >= 0, "rule buffer too small"
+    return [out[i] for i in range(n)], checked.value
+
+
+def search_gpu_semantics(targets, candidates, dead=0, cap=None):
+    flat, lens = _targets(targets)
+    cap = cap or (64 * len(targets) + 16)
+    out = (OrcRule * cap)()
+    cands = arr(candidates)
+    n = lib().orc_search_gpu(flat, lens, len(targets), cands, len(candidates), dead, out, cap)
+    assert n >= 0, "rule buffer too small"
+    return [out[i] for i in range(n)]
+
+
+def write_json(rules):
+    n = len(rules)
+    a = (OrcRule * max(1, n))(*rules)
+    need = lib().orc_write_json(a, n, None, 0)
+    b = ctypes.create_string_buffer(need + 1)
+    lib().orc_write_json(a, n, b, need + 1)
+    return b.value.decode()
+
+
+def dead_flag_desc(mask):
+    b = ctypes.create_string_buffer(64)
+    lib().orc_dead_flag_desc(mask, b, 64)
+    return b.value.decode()
+
+
+def parse_dead_flags(s):
+    v = ctypes.c_int()
+    ok = lib().orc_parse_dead_flags(s.encode(), ctypes.byref(v))
+    return v.value if ok else None
+
+
+def parse_assembly(text):
+    buf = (ctypes.c_uint32 * 64)()
+    n = lib().orc_parse_assembly(text.encode(), buf, 64)
+    return None if n < 0 else list(buf[:n])
+
+
+def mul_find(k, min_len, max_len, b, c, f):
+    ln, t = ctypes.c_int(), ctypes.c_int()
+    ops_ = (ctypes.c_int * 16)()
+    ok = lib().orc_mul_find(k, min_len, max_len, b, c, f, ctypes.byref(ln), ctypes.byref(t), ops_)
+    if not ok:
+        return None
+    return ln.value, t.value, list(ops_[:ln.value])
+
+
+def mul_run(seq, x, b, c, f):
+    a = (ctypes.c_int * max(1, len(seq)))(*seq)
+    return lib().orc_mul_run(a, len(seq), x, b, c, f)
+
+
+def mul_tstates(i):
+    return lib().orc_mul_tstates(i)

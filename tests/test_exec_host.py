@@ -1,0 +1,17 @@
+"""The device step function (z80_exec.cuh) compiled for the host agrees
+with the CPU oracle on every opcode (all A x F pairs, random other state)."""
+import os
+import subprocess
+
+from conftest import ROOT
+
+
+def test_exec_header_matches_oracle(tmp_path):
+    exe = tmp_path / "exec_check"
+    srcs = [os.path.join(ROOT, "tests", "native", "exec_check.cpp"),
+            os.path.join(ROOT, "oracle", "z80_oracle_isa_cpu.cpp"),
+            os.path.join(ROOT, "oracle", "z80_oracle_search.cpp")]
+    subprocess.run(["g++", "-O2", "-std=c++17", "-o", str(exe)] + srcs + ["-lpthread"], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.startswith("OK")

@@ -1,0 +1,242 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Every comparison is bit-exact: states, fingerprints, verifier verdicts,
+FlagDiff masks, rule lists and the reference's 'checked' counter.
+"""
+import os
+import random
+
+import numpy as np
+import pytest
+
+import workloads
+import z80b
+
+pytestmark = pytest.mark.gpu
+
+FULL = os.environ.get("Z80B_FULL_PARITY") == "1"
+
+
+def rule_keys(rules):
+    return [(r.target_index, tuple(r.src[:r.src_len]), tuple(r.rep[:r.rep_len]),
+             r.bytes_saved, r.cycles_saved, r.dead_flags) for r in rules]
+
+
+def test_exec_all_opcodes(ctx, O):
+    rng = random.Random(11)
+    states, seqs, exp = [], [], []
+    for op in range(455):
+        for _ in range(64):
+            vals = {k: rng.randrange(256) for k in "AFBCDEHL"}
+            vals["SP"] = rng.randrange(65536)
+            vals["M"] = rng.randrange(256)
+            imm = rng.randrange(65536)
+            st = O.state(**vals)
+            seq = [O.pack(op, imm)]
+            exp.append(O.exec_seq(st, seq).tup())
+            s = z80b.State(vals["A"], vals["F"], vals["B"], vals["C"], vals["D"], vals["E"],
+                           vals["H"], vals["L"], vals["SP"], vals["M"], 0)
+            states.append(s)
+            seqs.append(seq)
+    got = ctx.exec(states, seqs)
+    for i, (g, e) in enumerate(zip(got, exp)):
+        assert g.tup() == e, (i // 64, O.op_name(i // 64))
+
+
+def test_fingerprints(ctx, O):
+    pool = z80b.pool8()
+    fps = ctx.fingerprints([[w] for w in pool], 1)
+    for w, fp in zip(pool, fps):
+        assert fp == O.fingerprint([w]), O.disasm([w])
+    rng = random.Random(5)
+    seqs = [[rng.choice(pool), rng.choice(pool)] for _ in range(3000)]
+    fps = ctx.fingerprints(seqs, 2)
+    for s, fp in zip(seqs, fps):
+        assert fp == O.fingerprint(s)
+
+
+def test_quickcheck_gpu_reference_cases(ctx, O):
+    # pkg/gpu/cuda_test.go:18-157
+    o = O.ops()
+    cands = [O.pack(o[n], v) for n, v in [("XOR_A", 0), ("LD_A_N", 0), ("AND_A", 0), ("OR_A", 0),
+                                            ("ADD_A_B", 0), ("SUB_B", 0), ("NOP", 0), ("LD_A_N", 0x42)]]
+    ctx.load_candidates(cands, 1)
+    for i, c in enumerate(cands):
+        hits = ctx.quickcheck_gpu(O.fingerprint([c]), 0)
+        assert i in hits
+    # every loaded candidate against the oracle's fingerprint matching
+    for dead in (0, 0x28, 0xFF):
+        for c in cands:
+            fp = O.fingerprint([c])
+            exp = []
+            for j, d in enumerate(cands):
+                a, b = bytearray(O.fingerprint([d])), bytearray(fp)
+                for k in range(1, 80, 10):
+                    a[k] &= ~dead & 0xFF
+                    b[k] &= ~dead & 0xFF
+                if a == b:
+                    exp.append(j)
+            assert ctx.quickcheck_gpu(fp, dead) == exp
+
+
+def test_quickcheck_gpu_full_first_op(ctx, O):
+    # the 266,675 candidates SearchGPU uploads (enumerator.go:358-374)
+    pool = z80b.pool8()
+    first = pool + [z80b.pack(op, v) for op in (382, 383, 384, 385) for v in range(65536)]
+    ctx.load_candidates(first, 1)
+    rng = random.Random(9)
+    fps_all = None
+    for trial in range(6):
+        t = [rng.choice(pool), rng.choice(pool)]
+        fp = O.fingerprint(t)
+        hits = ctx.quickcheck_gpu(fp, 0)
+        for h in hits:
+            assert O.fingerprint([first[h]]) == fp
+    # a target equal to a 16-bit load: its own instruction must be among the hits
+    t = [z80b.pack(384, 0x1234)]
+    hits = ctx.quickcheck_gpu(O.fingerprint(t), 0)
+    assert first.index(t[0]) in hits
+
+
+def test_verify_pairs(ctx, O):
+    rng = random.Random(21)
+    pool = z80b.pool8()
+    o = O.ops()
+    pairs = []
+    # equivalences and near misses (reference tests + peephole data)
+    pairs.append(([O.pack(o["AND_N"], 0xFF)], [O.pack(o["AND_A"])]))
+    pairs.append(([O.pack(o["LD_A_N"], 0)], [O.pack(o["XOR_A"])]))
+    pairs.append(([O.pack(o["ADD_A_N"], 1)], [O.pack(o["INC_A"])]))
+    pairs.append(([O.pack(o["SUB_A"]), O.pack(o["LD_A_N"], 0)], [O.pack(o["SUB_A"])]))
+    # pairs that pass QuickCheck, found by scanning, so the sweeps run long
+    targets = workloads.to_lists(workloads.c2_subset(3000, seed=4))
+    for t in targets:
+        for c in pool:
+            if O.quickcheck(t, [c]):
+                pairs.append((t, [c]))
+                break
+        if len(pairs) > 60:
+            break
+    for _ in range(400):
+        pairs.append(([rng.choice(pool), rng.choice(pool)], [rng.choice(pool)]))
+    for dead in (0, 0x28, 0xFF):
+        deads = [dead] * len(pairs)
+        got = ctx.verify_pairs(pairs, dead=deads)
+        for (t, c), (bits, fd) in zip(pairs, got):
+            exp = (int(O.quickcheck(t, c, dead)) | (int(O.midcheck(t, c, dead)) << 1) |
+                   (int(O.exhaustive(t, c, dead)) << 2))
+            assert bits == exp, (O.disasm(t), O.disasm(c), dead, bits, exp)
+            assert fd == O.flagdiff(t, c)
+
+
+def _search_both(ctx, O, targets, dead=0, path=z80b.PATH_BATCHED, per_target_dead=None):
+    rules, st = ctx.search(targets, dead_flags=dead, path=path, per_target_dead=per_target_dead)
+    if per_target_dead is None:
+        exp, checked = O.search(targets, 1, dead=dead)
+        return rules, st, exp, checked
+    exp, checked = [], 0
+    groups = {}
+    for i, d in enumerate(per_target_dead):
+        groups.setdefault(d, []).append(i)
+    for d, idx in groups.items():
+        r, ch = O.search([targets[i] for i in idx], 1, dead=d)
+        for x in r:
+            x.target_index = idx[x.target_index]
+        exp += r
+        checked += ch
+    exp.sort(key=lambda r: (r.target_index, r.dead_flags != 0))
+    return rules, st, exp, checked
+
+
+@pytest.mark.parametrize("dead", [0x00, 0xFF, 0x28])
+def test_search_first_c2_subset(ctx, O, dead):
+    n = 100000 if FULL else 6000
+    targets = workloads.to_lists(workloads.c2_subset(n, seed=0))
+    rules, st, exp, checked = _search_both(ctx, O, targets, dead)
+    assert rule_keys(rules) == rule_keys(exp)
+    assert st.checked_ref == checked
+    assert st.targets == n
+
+
+def test_search_first_c1(ctx, O):
+    t = workloads.c1_targets()
+    if not FULL:
+        t = t[np.random.default_rng(0).choice(len(t), 8000, replace=False)]
+        t = t[np.argsort(t[:, 0] * 2**32 + t[:, 1], kind="stable")]
+    targets = workloads.to_lists(t)
+    rules, st, exp, checked = _search_both(ctx, O, targets, 0)
+    assert rule_keys(rules) == rule_keys(exp)
+    assert st.checked_ref == checked
+
+
+def test_search_per_target_dead(ctx, O):
+    targets = workloads.to_lists(workloads.c2_subset(3000, seed=8))
+    g = workloads.splitmix64(1)
+    dead = [next(g) & 0xFF for _ in targets]
+    rules, st, exp, checked = _search_both(ctx, O, targets, per_target_dead=dead)
+    assert rule_keys(rules) == rule_keys(exp)
+    assert st.checked_ref == checked
+
+
+def test_plain_path_equals_batched(ctx, O):
+    targets = workloads.to_lists(workloads.c2_subset(300, seed=3))
+    a, sa = ctx.search(targets, dead_flags=0xFF, path=z80b.PATH_BATCHED)
+    b, sb = ctx.search(targets, dead_flags=0xFF, path=z80b.PATH_PLAIN)
+    assert rule_keys(a) == rule_keys(b)
+    assert sa.checked_ref == sb.checked_ref and sa.checks == sb.checks
+    exp, _ = O.search(targets, 1, dead=0xFF)
+    assert rule_keys(a) == rule_keys(exp)
+
+
+def test_search_all_hits(ctx, O):
+    # gpu.SearchGPU semantics: every candidate of EnumerateFirstOp that passes
+    pool = z80b.pool8()
+    first = pool + [z80b.pack(op, v) for op in (382, 383, 384, 385) for v in range(65536)]
+    ctx.load_candidates(first, 1)
+    targets = workloads.to_lists(workloads.c2_subset(150, seed=5))
+    o = O.ops()
+    targets += [[O.pack(o["SUB_A"]), O.pack(o["LD_A_N"], 0)], [O.pack(o["LD_A_N"], 0), O.pack(o["NEG"])],
+                [O.pack(o["LD_H_N"], 0x12), O.pack(o["LD_L_N"], 0x34)]]
+    for dead in (0, 0xFF):
+        rules, st = ctx.search(targets, dead_flags=dead, mode=z80b.MODE_ALL)
+        exp = O.search_gpu_semantics(targets, first, dead)
+        assert rule_keys(rules) == rule_keys(exp), dead
+    assert any(r.rep[0] & 0xFFFF >= 382 for r in rules)  # a 16-bit load replacement was found
+
+
+def test_target_lengths_and_edges(ctx, O):
+    pool = z80b.pool8()
+    rng = random.Random(13)
+    targets = [[rng.choice(pool)] for _ in range(300)]
+    targets += [[rng.choice(pool) for _ in range(3)] for _ in range(150)]
+    targets += [[rng.choice(pool) for _ in range(4)] for _ in range(60)]
+    o = O.ops()
+    targets += [[O.pack(o["AND_N"], 0xFF)], [O.pack(o["OR_N"], 0)], [O.pack(o["LD_A_N"], 0)]]
+    rules, st = ctx.search(targets, dead_flags=0xFF)
+    exp, checked = O.search(targets, 1, dead=0xFF)
+    assert rule_keys(rules) == rule_keys(exp)
+    assert st.checked_ref == checked
+    # empty job
+    rules, st = ctx.search([])
+    assert rules == [] and st.targets == 0
+
+
+def test_invalid_inputs(ctx):
+    with pytest.raises(z80b.Z80BError) as e:
+        ctx.search([[455]])
+    assert e.value.status == z80b.EINVAL
+    with pytest.raises(z80b.Z80BError) as e:
+        ctx.search([[1, 2, 3, 4, 5]])
+    assert e.value.status == z80b.EINVAL
+    with pytest.raises(z80b.Z80BError):
+        ctx.search([[1]], max_cand_len=0)
+
+
+def test_staged_equals_search(ctx):
+    targets = workloads.to_lists(workloads.c2_subset(2000, seed=6))
+    job, keep = ctx.make_job(targets, dead_flags=0xFF)
+    ctx.stage(job)
+    n, st = ctx.run_staged()
+    staged = ctx.fetch_rules(n)
+    rules, _ = ctx.search(targets, dead_flags=0xFF)
+    assert rule_keys(staged) == rule_keys(rules)

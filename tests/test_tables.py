@@ -1,0 +1,83 @@
+"""Host-side tables of the product library (catalog, masks, pruning,
+enumeration order, disassembly, parsing, JSON) against the CPU oracle."""
+import json
+import random
+
+import z80b
+import workloads
+
+
+def test_op_info_matches_oracle(O):
+    for op in range(455):
+        info = z80b.op_info(op)
+        m, enc, t, size = O.catalog(op)
+        assert info["mnemonic"] == m
+        assert info["size"] == size and info["tstates"] == t
+        assert info["reads"] == O.op_reads(op), (op, O.op_name(op))
+        assert info["writes"] == O.op_writes(op), (op, O.op_name(op))
+
+
+def test_pool8_order_matches_enumerator(O):
+    assert z80b.pool8() == O.instructions8()
+
+
+def test_opcode_names(O):
+    ops = workloads.ops()
+    for name, op in ops.items():
+        assert O.op_name(op) == name
+
+
+def test_disasm_and_prune_random(O):
+    rng = random.Random(7)
+    pool = z80b.pool8()
+    pool16 = pool + [z80b.pack(op, rng.randrange(65536)) for op in (382, 383, 384, 385) for _ in range(4)]
+    for _ in range(20000):
+        n = rng.randint(1, 3)
+        seq = [rng.choice(pool16) for _ in range(n)]
+        assert z80b.disasm(seq) == O.disasm(seq)
+        assert z80b.should_prune(seq) == O.should_prune(seq), O.disasm(seq)
+
+
+def test_prune_all_pairs_sample(O):
+    pool = z80b.pool8()
+    rng = random.Random(3)
+    for _ in range(30000):
+        seq = [rng.choice(pool), rng.choice(pool)]
+        assert z80b.should_prune(seq) == O.should_prune(seq), O.disasm(seq)
+
+
+def test_enumerate_counts():
+    c2 = workloads.c2_targets()
+    assert len(c2) == 9818041
+    c1 = workloads.c1_targets()
+    assert len(c1) > 0 and c1.shape[1] == 2
+
+
+def test_parse_and_flags(O):
+    for text in ["SUB A : LD A, 0", "AND 0FFh", "ld a, 0x00 : neg", "LD (HL), 12h", "BIT 7, (HL)",
+                 "EX DE, HL", "ADC HL, SP", "SLL (HL)"]:
+        assert z80b.parse_assembly(text) == O.parse_assembly(text), text
+    for s in ["none", "undoc", "all", "0x13", "FF", "0x00"]:
+        assert z80b.parse_dead_flags(s) == O.parse_dead_flags(s)
+    for m in range(256):
+        assert z80b.dead_flag_desc(m) == O.dead_flag_desc(m)
+
+
+def test_rules_json_matches_oracle(O):
+    o = O.ops()
+    targets = [[O.pack(o["AND_N"], 0xFF)], [O.pack(o["SUB_A"]), O.pack(o["LD_A_N"], 0)],
+               [O.pack(o["LD_A_N"], 0)]]
+    rules, _ = O.search(targets, 1, dead=0xFF)
+    mine = []
+    for r in rules:
+        x = z80b.Rule()
+        x.src_len, x.rep_len = r.src_len, r.rep_len
+        for i in range(r.src_len):
+            x.src[i] = r.src[i]
+        for i in range(r.rep_len):
+            x.rep[i] = r.rep[i]
+        x.bytes_saved, x.cycles_saved, x.dead_flags = r.bytes_saved, r.cycles_saved, r.dead_flags
+        mine.append(x)
+    assert z80b.write_json(mine) == O.write_json(rules)
+    assert any(r.dead_flags for r in rules)
+    json.loads(z80b.write_json(mine))

@@ -1,0 +1,463 @@
+// z80_tables.cpp -- host-side catalog, masks, pruning and enumeration order.
+// See z80_tables.h for the reference files each part follows.
+#include "z80_tables.h"
+
+#include <cctype>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+
+namespace z80b {
+
+namespace {
+
+struct Entry {
+  std::string mnem;
+  uint8_t enc[2];
+  int nenc;
+};
+
+// Register naming for the enum families (A,B,C,D,E,H,L) and their 3-bit
+// Z80 operand field.
+const char* const kName7[7] = {"A", "B", "C", "D", "E", "H", "L"};
+const uint8_t kField7[7] = {7, 0, 1, 2, 3, 4, 5};
+// ALU and LD-A source order B,C,D,E,H,L,A expressed as family indices.
+const int kSrcOrder[7] = {1, 2, 3, 4, 5, 6, 0};
+const uint16_t kMask7[7] = {kRegA, kRegB, kRegC, kRegD, kRegE, kRegH, kRegL};
+const uint16_t kPair[4] = {kRegB | kRegC, kRegD | kRegE, kRegH | kRegL, kRegSP};
+const char* const kPairName[4] = {"BC", "DE", "HL", "SP"};
+
+struct Tables {
+  OpInfo info[kNumOps];
+  Entry cat[kNumOps];
+  std::vector<uint32_t> pool;
+};
+
+void set(Tables& T, int op, std::string m, std::initializer_list<uint8_t> enc, int t, int imm,
+         uint16_t rd, uint16_t wr) {
+  Entry& e = T.cat[op];
+  e.mnem = std::move(m);
+  e.nenc = 0;
+  for (uint8_t b : enc) e.enc[e.nenc++] = b;
+  OpInfo& o = T.info[op];
+  o.size = uint8_t(e.nenc + imm);
+  o.tstates = uint8_t(t);
+  o.imm = uint8_t(imm);
+  o.nopish = 0;
+  o.reads = rd;
+  o.writes = wr;
+}
+
+void build(Tables& T) {
+  int op = 0;
+  // LD r,r' (catalog.go:151-187): reads the source, writes the destination.
+  for (int d = 0; d < 7; d++)
+    for (int k = 0; k < 7; k++, op++) {
+      int s = d == 0 ? kSrcOrder[k] : k;
+      set(T, op, std::string("LD ") + kName7[d] + ", " + kName7[s],
+          {uint8_t(0x40 | kField7[d] << 3 | kField7[s])}, 4, 0, kMask7[s], kMask7[d]);
+      if (s == d) T.info[op].nopish = 1;
+    }
+  for (int d = 0; d < 7; d++, op++)
+    set(T, op, std::string("LD ") + kName7[d] + ", n", {uint8_t(0x06 | kField7[d] << 3)}, 7, 1, 0, kMask7[d]);
+  // ALU A,src / A,n.  Reads: the source register only (the accumulator is
+  // not listed), plus F for ADC/SBC; the immediate forms read nothing except
+  // ADC/SBC (A|F).  Writes A|F, CP only F.
+  const char* const alu[8] = {"ADD A, ", "ADC A, ", "SUB ", "SBC A, ", "AND ", "XOR ", "OR ", "CP "};
+  for (int a = 0; a < 8; a++) {
+    bool cin = a == 1 || a == 3;
+    uint16_t wr = a == 7 ? uint16_t(kRegF) : uint16_t(kRegA | kRegF);
+    for (int k = 0; k < 7; k++, op++) {
+      int s = kSrcOrder[k];
+      set(T, op, std::string(alu[a]) + kName7[s], {uint8_t(0x80 | a << 3 | kField7[s])}, 4, 0,
+          uint16_t(kMask7[s] | (cin ? kRegF : 0)), wr);
+    }
+    set(T, op, std::string(alu[a]) + "n", {uint8_t(0xC6 | a << 3)}, 7, 1,
+        cin ? uint16_t(kRegA | kRegF) : uint16_t(0), wr);
+    op++;
+  }
+  for (int r = 0; r < 7; r++, op++)
+    set(T, op, std::string("INC ") + kName7[r], {uint8_t(0x04 | kField7[r] << 3)}, 4, 0, kMask7[r],
+        uint16_t(kMask7[r] | kRegF));
+  for (int r = 0; r < 7; r++, op++)
+    set(T, op, std::string("DEC ") + kName7[r], {uint8_t(0x05 | kField7[r] << 3)}, 4, 0, kMask7[r],
+        uint16_t(kMask7[r] | kRegF));
+  const uint16_t AF = kRegA | kRegF;
+  set(T, RLCA, "RLCA", {0x07}, 4, 0, kRegA, AF);
+  set(T, RRCA, "RRCA", {0x0F}, 4, 0, kRegA, AF);
+  set(T, RLA, "RLA", {0x17}, 4, 0, AF, AF);
+  set(T, RRA, "RRA", {0x1F}, 4, 0, AF, AF);
+  set(T, DAA, "DAA", {0x27}, 4, 0, kRegA, AF);
+  set(T, CPL, "CPL", {0x2F}, 4, 0, kRegA, AF);
+  set(T, SCF, "SCF", {0x37}, 4, 0, kRegF, kRegF);
+  set(T, CCF, "CCF", {0x3F}, 4, 0, kRegF, kRegF);
+  set(T, NEG, "NEG", {0xED, 0x44}, 8, 0, kRegA, AF);
+  set(T, NOP, "NOP", {0x00}, 4, 0, 0, 0);
+  T.info[NOP].nopish = 1;
+  op = RLC_A;
+  // CB shifts: enum kinds RLC,RRC,RL,RR,SLA,SRA,SRL; CB field values.
+  const char* const sh[7] = {"RLC", "RRC", "RL", "RR", "SLA", "SRA", "SRL"};
+  const uint8_t shf[7] = {0, 1, 2, 3, 4, 5, 7};
+  for (int k = 0; k < 7; k++)
+    for (int r = 0; r < 7; r++, op++)
+      set(T, op, std::string(sh[k]) + " " + kName7[r], {0xCB, uint8_t(shf[k] << 3 | kField7[r])}, 8, 0,
+          uint16_t(kMask7[r] | ((k == 2 || k == 3) ? kRegF : 0)), uint16_t(kMask7[r] | kRegF));
+  for (int r = 0; r < 7; r++, op++)
+    set(T, op, std::string("SLL ") + kName7[r], {0xCB, uint8_t(0x30 | kField7[r])}, 8, 0, kMask7[r],
+        uint16_t(kMask7[r] | kRegF));
+  const char* const bn[3] = {"BIT ", "RES ", "SET "};
+  for (int f = 0; f < 3; f++)
+    for (int n = 0; n < 8; n++)
+      for (int r = 0; r < 7; r++, op++)
+        set(T, op, std::string(bn[f]) + char('0' + n) + ", " + kName7[r],
+            {0xCB, uint8_t((f + 1) << 6 | n << 3 | kField7[r])}, 8, 0, kMask7[r],
+            f == 0 ? uint16_t(kRegF) : kMask7[r]);
+  for (int p = 0; p < 4; p++) {
+    set(T, INC_BC + p, std::string("INC ") + kPairName[p], {uint8_t(0x03 | p << 4)}, 6, 0, kPair[p], kPair[p]);
+    set(T, DEC_BC + p, std::string("DEC ") + kPairName[p], {uint8_t(0x0B | p << 4)}, 6, 0, kPair[p], kPair[p]);
+    set(T, ADD_HL_BC + p, std::string("ADD HL, ") + kPairName[p], {uint8_t(0x09 | p << 4)}, 11, 0,
+        uint16_t(kRegH | kRegL | kPair[p]), uint16_t(kRegH | kRegL | kRegF));
+    set(T, LD_BC_NN + p, std::string("LD ") + kPairName[p] + ", nn", {uint8_t(0x01 | p << 4)}, 10, 2, 0, kPair[p]);
+    set(T, ADC_HL_BC + p, std::string("ADC HL, ") + kPairName[p], {0xED, uint8_t(0x4A | p << 4)}, 15, 0,
+        uint16_t(kRegH | kRegL | kPair[p] | kRegF), uint16_t(kRegH | kRegL | kRegF));
+    set(T, SBC_HL_BC + p, std::string("SBC HL, ") + kPairName[p], {0xED, uint8_t(0x42 | p << 4)}, 15, 0,
+        uint16_t(kRegH | kRegL | kPair[p] | kRegF), uint16_t(kRegH | kRegL | kRegF));
+  }
+  set(T, EX_DE_HL, "EX DE, HL", {0xEB}, 4, 0, kRegD | kRegE | kRegH | kRegL, kRegD | kRegE | kRegH | kRegL);
+  set(T, LD_SP_HL, "LD SP, HL", {0xF9}, 6, 0, kRegH | kRegL, kRegSP);
+  // Memory ops: reads as opReads lists them; writes always 0 (the
+  // reference's opWrites has no memory cases).
+  for (int r = 0; r < 7; r++) {
+    set(T, LD_A_HLI + r, std::string("LD ") + kName7[r] + ", (HL)", {uint8_t(0x46 | kField7[r] << 3)}, 7, 0, kRegM, 0);
+    set(T, LD_HLI_A + r, std::string("LD (HL), ") + kName7[r], {uint8_t(0x70 | kField7[r])}, 7, 0, kMask7[r], 0);
+  }
+  set(T, LD_HLI_N, "LD (HL), n", {0x36}, 10, 1, 0, 0);
+  set(T, LD_A_BCI, "LD A, (BC)", {0x0A}, 7, 0, kRegM, 0);
+  set(T, LD_A_DEI, "LD A, (DE)", {0x1A}, 7, 0, kRegM, 0);
+  set(T, LD_BCI_A, "LD (BC), A", {0x02}, 7, 0, kRegA, 0);
+  set(T, LD_DEI_A, "LD (DE), A", {0x12}, 7, 0, kRegA, 0);
+  const char* const am[8] = {"ADD A, (HL)", "ADC A, (HL)", "SUB (HL)", "SBC A, (HL)",
+                             "AND (HL)", "XOR (HL)", "OR (HL)", "CP (HL)"};
+  for (int a = 0; a < 8; a++)
+    set(T, ADD_A_HLI + a, am[a], {uint8_t(0x86 | a << 3)}, 7, 0,
+        uint16_t(kRegA | kRegM | ((a == 1 || a == 3) ? kRegF : 0)), 0);
+  set(T, INC_HLI, "INC (HL)", {0x34}, 11, 0, kRegM, 0);
+  set(T, DEC_HLI, "DEC (HL)", {0x35}, 11, 0, kRegM, 0);
+  const char* const mh[8] = {"RLC", "RRC", "RL", "RR", "SLA", "SRA", "SRL", "SLL"};
+  const uint8_t mhf[8] = {0, 1, 2, 3, 4, 5, 7, 6};
+  for (int k = 0; k < 8; k++)
+    set(T, RLC_HLI + k, std::string(mh[k]) + " (HL)", {0xCB, uint8_t(mhf[k] << 3 | 6)}, 15, 0,
+        uint16_t(kRegM | ((k == 2 || k == 3) ? kRegF : 0)), 0);
+  for (int n = 0; n < 8; n++) {
+    set(T, BIT_0_HLI + n, std::string("BIT ") + char('0' + n) + ", (HL)", {0xCB, uint8_t(0x46 | n << 3)}, 12, 0, kRegM, 0);
+    set(T, RES_0_HLI + n, std::string("RES ") + char('0' + n) + ", (HL)", {0xCB, uint8_t(0x86 | n << 3)}, 15, 0, kRegM, 0);
+    set(T, SET_0_HLI + n, std::string("SET ") + char('0' + n) + ", (HL)", {0xCB, uint8_t(0xC6 | n << 3)}, 15, 0, kRegM, 0);
+  }
+  // Enumeration order (enumerator.go:319-345).
+  for (int o = 0; o < kNumOps; o++)
+    if (T.info[o].imm == 0) T.pool.push_back(insn(uint16_t(o)));
+  for (int o = 0; o < kNumOps; o++)
+    if (T.info[o].imm == 1)
+      for (int v = 0; v < 256; v++) T.pool.push_back(insn(uint16_t(o), uint16_t(v)));
+}
+
+Tables& tables() {
+  static Tables* T = [] {
+    auto* t = new Tables();
+    build(*t);
+    return t;
+  }();
+  return *T;
+}
+
+void hex2(std::string& o, unsigned v, int digits) {
+  static const char* hx = "0123456789ABCDEF";
+  if ((v >> (4 * (digits - 1))) >= 0xA) o += '0';
+  for (int i = digits - 1; i >= 0; i--) o += hx[(v >> (4 * i)) & 15];
+  o += 'h';
+}
+
+}  // namespace
+
+const OpInfo* op_table() { return tables().info; }
+const char* op_mnemonic(uint16_t op) { return tables().cat[op].mnem.c_str(); }
+const uint8_t* op_encoding(uint16_t op, int* n) {
+  *n = tables().cat[op].nenc;
+  return tables().cat[op].enc;
+}
+const std::vector<uint32_t>& pool8() { return tables().pool; }
+
+std::vector<uint32_t> first_op_pool() {
+  std::vector<uint32_t> v = pool8();
+  for (int o = 0; o < kNumOps; o++)
+    if (op_table()[o].imm == 2)
+      for (int x = 0; x < 65536; x++) v.push_back(insn(uint16_t(o), uint16_t(x)));
+  return v;
+}
+
+std::string disassemble(uint32_t w) {
+  uint16_t op = insn_op(w), imm = insn_imm(w);
+  const std::string& m = tables().cat[op].mnem;
+  const int kind = op_table()[op].imm;
+  if (kind == 0) return m;
+  std::string out;
+  for (size_t i = 0; i < m.size(); i++) {
+    if (kind == 2 && i + 1 < m.size() && m[i] == 'n' && m[i + 1] == 'n') {
+      hex2(out, imm, 4);
+      i++;
+    } else if (kind == 1 && m[i] == 'n' && (i + 1 == m.size() || m[i + 1] == ' ' || m[i + 1] == ',')) {
+      hex2(out, imm & 0xFFu, 2);
+    } else {
+      out += m[i];
+    }
+  }
+  return out;
+}
+
+std::string disasm_seq(const uint32_t* seq, int n) {
+  std::string s;
+  for (int i = 0; i < n; i++) {
+    if (i) s += " : ";
+    s += disassemble(seq[i]);
+  }
+  return s;
+}
+
+bool should_prune(const uint32_t* seq, int n) {
+  const OpInfo* T = op_table();
+  for (int i = 0; i < n; i++) {
+    if (T[insn_op(seq[i])].nopish) return true;  // NOP and LD r,r
+    if (i + 1 < n) {
+      const OpInfo& x = T[insn_op(seq[i])];
+      const OpInfo& y = T[insn_op(seq[i + 1])];
+      // dead write: written by both, not read by the second, flags excluded
+      if (x.writes && (x.writes & y.writes & ~kRegF & ~y.reads)) return true;
+    }
+  }
+  for (int i = 0; i + 1 < n; i++) {
+    const OpInfo& x = T[insn_op(seq[i])];
+    const OpInfo& y = T[insn_op(seq[i + 1])];
+    bool indep = !((x.writes & y.reads) || (x.reads & y.writes) || (x.writes & y.writes));
+    // canonical order key op<<16|imm (pruner.go:254-256) -- the packed word
+    // with its halves swapped
+    uint32_t kx = (uint32_t(insn_op(seq[i])) << 16) | insn_imm(seq[i]);
+    uint32_t ky = (uint32_t(insn_op(seq[i + 1])) << 16) | insn_imm(seq[i + 1]);
+    if (indep && kx > ky) return true;
+  }
+  return false;
+}
+
+uint16_t seq_reads(const uint32_t* s, int n) {
+  uint16_t m = 0;
+  for (int i = 0; i < n; i++) m |= op_table()[insn_op(s[i])].reads;
+  return m;
+}
+
+Sweep sweep_for(uint16_t reads) {
+  Sweep w{};
+  const uint16_t order[7] = {kRegB, kRegC, kRegD, kRegE, kRegH, kRegL, kRegM};
+  for (int i = 0; i < 7; i++)
+    if (reads & order[i]) w.regs[w.nextra++] = uint8_t(i);
+  w.sp = (reads & kRegSP) != 0;
+  if (w.nextra == 0 && !w.sp) {
+    w.kind = 0;
+    w.states = 512;
+  } else if (w.nextra <= 2 && !w.sp) {
+    w.kind = 1;
+    w.states = 512ull << (8 * w.nextra);
+  } else {
+    w.kind = 2;
+    w.states = (512ull << (5 * w.nextra)) * (w.sp ? 16 : 1);
+  }
+  if (w.kind != 2) w.sp = false;
+  return w;
+}
+
+std::string dead_flag_desc(uint8_t mask) {
+  if (mask == 0) return "";
+  if (mask == 0xFF) return "all";
+  if (mask == 0x28) return "undoc";
+  static const char* const nm[8] = {"C", "N", "P/V", "X3", "H", "X5", "Z", "S"};
+  std::string s;
+  for (int b = 0; b < 8; b++)
+    if (mask >> b & 1) {
+      if (!s.empty()) s += ',';
+      s += nm[b];
+    }
+  return s;
+}
+
+namespace {
+std::string up(std::string s) {
+  for (auto& c : s) c = char(std::toupper((unsigned char)c));
+  return s;
+}
+std::string trim(const std::string& s) {
+  size_t a = s.find_first_not_of(" \t\r\n");
+  if (a == std::string::npos) return "";
+  size_t b = s.find_last_not_of(" \t\r\n");
+  return s.substr(a, b - a + 1);
+}
+// fmt.Sscanf-style integer: optional sign, longest digit run, >= 1 digit.
+bool scan(const std::string& s, int base, long* v) {
+  size_t i = 0;
+  bool neg = false;
+  if (i < s.size() && (s[i] == '-' || s[i] == '+')) neg = s[i++] == '-';
+  size_t st = i;
+  long x = 0;
+  for (; i < s.size(); i++) {
+    int d = std::isdigit((unsigned char)s[i]) ? s[i] - '0'
+            : (base == 16 && std::isxdigit((unsigned char)s[i])) ? (std::toupper((unsigned char)s[i]) - 'A' + 10)
+            : -1;
+    if (d < 0) break;
+    x = x * base + d;
+  }
+  if (i == st) return false;
+  *v = neg ? -x : x;
+  return true;
+}
+bool parse_imm(std::string s, long* v) {
+  s = trim(s);
+  if (s.empty()) return false;
+  if (s.size() >= 2 && s[0] == '0' && (s[1] == 'x' || s[1] == 'X')) return scan(s.substr(2), 16, v);
+  if (std::toupper((unsigned char)s.back()) == 'H') return scan(s.substr(0, s.size() - 1), 16, v);
+  return scan(s, 10, v);
+}
+bool parse_one(const std::string& text0, uint32_t* out) {
+  std::string text = trim(text0), U = up(text);
+  for (int op = 0; op < kNumOps; op++) {
+    const std::string& m = tables().cat[op].mnem;
+    if (op_table()[op].imm == 0) {
+      if (up(m) == U) {
+        *out = insn(uint16_t(op));
+        return true;
+      }
+      continue;
+    }
+    std::string pat = up(m);
+    size_t n = pat.rfind('N');
+    std::string pre = pat.substr(0, n), suf = pat.substr(n + 1);
+    if (U.size() < pre.size() || U.compare(0, pre.size(), pre) != 0) continue;
+    if (!suf.empty() && (U.size() < suf.size() || U.compare(U.size() - suf.size(), suf.size(), suf) != 0)) continue;
+    std::string val = U.substr(pre.size());
+    if (!suf.empty()) {
+      if (val.size() < suf.size()) continue;
+      val.resize(val.size() - suf.size());
+    }
+    long v;
+    if (!parse_imm(val, &v)) continue;
+    *out = insn(uint16_t(op), uint16_t(v));
+    return true;
+  }
+  return false;
+}
+}  // namespace
+
+bool parse_dead_flags(const std::string& in, uint8_t* out) {
+  std::string s;
+  for (char c : in) s += char(std::tolower((unsigned char)c));
+  if (s.empty() || s == "none") { *out = 0x00; return true; }
+  if (s == "undoc") { *out = 0x28; return true; }
+  if (s == "all") { *out = 0xFF; return true; }
+  if (s.compare(0, 2, "0x") == 0) s = s.substr(2);
+  if (s.empty()) return false;
+  unsigned v = 0;
+  for (char c : s) {
+    if (!std::isxdigit((unsigned char)c)) return false;
+    v = v * 16 + unsigned(std::isdigit((unsigned char)c) ? c - '0' : c - 'a' + 10);
+    if (v > 0xFF) return false;
+  }
+  *out = uint8_t(v);
+  return true;
+}
+
+bool parse_assembly(const std::string& text, std::vector<uint32_t>* out) {
+  out->clear();
+  size_t st = 0;
+  for (;;) {
+    size_t p = text.find(':', st);
+    std::string part = trim(text.substr(st, p == std::string::npos ? std::string::npos : p - st));
+    if (!part.empty()) {
+      uint32_t w;
+      if (!parse_one(part, &w)) return false;
+      out->push_back(w);
+    }
+    if (p == std::string::npos) break;
+    st = p + 1;
+  }
+  return !out->empty();
+}
+
+}  // namespace z80b
+
+namespace z80b {
+namespace {
+struct V {
+  uint8_t a, f, b, c, d, e, h, l;
+  uint16_t sp;
+  uint8_t m;
+};
+// verifier.go:35-72; the first 8 rows are the QuickCheck vectors (19-28).
+const V kVec[32] = {
+    {0x00, 0x00, 0x00, 0x00, 0x00, 0x00, 0x00, 0x00, 0x0000, 0x42},
+    {0xFF, 0xFF, 0xFF, 0xFF, 0xFF, 0xFF, 0xFF, 0xFF, 0xFFFF, 0xBD},
+    {0x01, 0x00, 0x02, 0x03, 0x04, 0x05, 0x06, 0x07, 0x1234, 0x13},
+    {0x80, 0x01, 0x40, 0x20, 0x10, 0x08, 0x04, 0x02, 0x8000, 0x7E},
+    {0x55, 0x00, 0xAA, 0x55, 0xAA, 0x55, 0xAA, 0x55, 0x5555, 0xA5},
+    {0xAA, 0x01, 0x55, 0xAA, 0x55, 0xAA, 0x55, 0xAA, 0xAAAA, 0x5A},
+    {0x0F, 0x00, 0xF0, 0x0F, 0xF0, 0x0F, 0xF0, 0x0F, 0xFFFE, 0xE1},
+    {0x7F, 0x01, 0x80, 0x7F, 0x80, 0x7F, 0x80, 0x7F, 0x7FFF, 0x33},
+    {0x02, 0x00, 0x01, 0x02, 0x04, 0x08, 0x10, 0x20, 0x0102, 0x91},
+    {0x04, 0x01, 0x08, 0x10, 0x20, 0x40, 0x80, 0x01, 0x0408, 0x48},
+    {0x08, 0x00, 0x10, 0x20, 0x40, 0x80, 0x01, 0x02, 0x1020, 0x24},
+    {0x10, 0x01, 0x20, 0x40, 0x80, 0x01, 0x02, 0x04, 0x4080, 0xD7},
+    {0x20, 0x00, 0x40, 0x80, 0x01, 0x02, 0x04, 0x08, 0x0201, 0x6B},
+    {0x40, 0x01, 0x80, 0x01, 0x02, 0x04, 0x08, 0x10, 0x8040, 0xB2},
+    {0x03, 0x00, 0x05, 0x09, 0x11, 0x21, 0x41, 0x81, 0x0309, 0x0F},
+    {0x05, 0x01, 0x0A, 0x14, 0x28, 0x50, 0xA0, 0x41, 0x0A14, 0xF0},
+    {0x11, 0x00, 0x01, 0x02, 0x04, 0x08, 0x10, 0x20, 0x0100, 0xC3},
+    {0x22, 0x01, 0x04, 0x08, 0x10, 0x20, 0x40, 0x80, 0x0200, 0x3C},
+    {0x44, 0x00, 0x10, 0x20, 0x40, 0x80, 0x01, 0x02, 0x0400, 0x87},
+    {0x88, 0x01, 0x40, 0x80, 0x01, 0x02, 0x04, 0x08, 0x0800, 0x69},
+    {0x33, 0x00, 0x03, 0x0C, 0x30, 0xC0, 0x05, 0x0A, 0x3300, 0xAE},
+    {0xCC, 0x01, 0x30, 0xC0, 0x03, 0x0C, 0x50, 0xA0, 0xCC00, 0x51},
+    {0x66, 0x00, 0x06, 0x60, 0x09, 0x90, 0x0C, 0xC0, 0x6600, 0xDA},
+    {0x99, 0x01, 0x09, 0x90, 0x06, 0x60, 0xA0, 0x0A, 0x9900, 0x25},
+    {0xFE, 0x00, 0x7F, 0x80, 0x01, 0xFE, 0x55, 0xAA, 0x0001, 0x01},
+    {0x81, 0x01, 0xFE, 0x01, 0x80, 0x7F, 0xAA, 0x55, 0x8001, 0xFE},
+    {0x7E, 0x00, 0x81, 0x42, 0x24, 0x18, 0xE7, 0xDB, 0x7FFE, 0x80},
+    {0xBF, 0x01, 0x40, 0xBF, 0x40, 0xBF, 0x40, 0xBF, 0xBF00, 0x40},
+    {0xC0, 0x00, 0x3F, 0xC0, 0x3F, 0xC0, 0x3F, 0xC0, 0xC000, 0x1F},
+    {0xE0, 0x01, 0x1F, 0xE0, 0x1F, 0xE0, 0x1F, 0xE0, 0xE000, 0xEF},
+    {0xF0, 0x00, 0x0F, 0xF0, 0x0F, 0xF0, 0x0F, 0xF0, 0xF000, 0x55},
+    {0x0E, 0x01, 0xE0, 0x0E, 0xE0, 0x0E, 0xE0, 0x0E, 0x0E0E, 0xAA},
+};
+uint32_t g_vec[32][3];
+const uint8_t kRep[32] = {0x00, 0x01, 0x02, 0x0F, 0x10, 0x1F, 0x20, 0x3F, 0x40, 0x55, 0x7E,
+                          0x7F, 0x80, 0x81, 0xAA, 0xBF, 0xC0, 0xD5, 0xE0, 0xEF, 0xF0, 0xF7,
+                          0xFE, 0xFF, 0x03, 0x07, 0x11, 0x33, 0x77, 0xBB, 0xDD, 0xEE};
+const uint16_t kRepSP[16] = {0x0000, 0x0001, 0x00FF, 0x0100, 0x7FFE, 0x7FFF, 0x8000, 0x8001,
+                             0xFFFE, 0xFFFF, 0x1234, 0x5678, 0xABCD, 0xDEAD, 0xBEEF, 0xCAFE};
+std::once_flag g_vec_once;
+void pack_vectors() {
+  for (int i = 0; i < 32; i++) {
+    const V& v = kVec[i];
+    g_vec[i][0] = uint32_t(v.a) | uint32_t(v.f) << 8 | uint32_t(v.b) << 16 | uint32_t(v.c) << 24;
+    g_vec[i][1] = uint32_t(v.d) | uint32_t(v.e) << 8 | uint32_t(v.h) << 16 | uint32_t(v.l) << 24;
+    g_vec[i][2] = uint32_t(v.sp) | uint32_t(v.m) << 16;
+  }
+}
+}  // namespace
+
+const uint32_t (*qc_vectors())[3] {
+  std::call_once(g_vec_once, pack_vectors);
+  return g_vec;
+}
+const uint32_t (*mid_vectors())[3] {
+  std::call_once(g_vec_once, pack_vectors);
+  return g_vec;
+}
+const uint8_t* rep_values() { return kRep; }
+const uint16_t* rep_sp() { return kRepSP; }
+
+}  // namespace z80b

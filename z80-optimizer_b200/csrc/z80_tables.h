@@ -1,0 +1,73 @@
+// z80_tables.h -- host-side instruction catalog and static analysis.
+//
+// The catalog (mnemonics, encodings, T-states) is the reference's
+// pkg/inst/catalog.go data; the read/write masks are the reference's
+// opReads/opWrites (pkg/search/verifier.go:199-408, pruner.go:66-236),
+// including their omissions, because pruning and sweep selection depend on
+// them bit for bit.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "z80_isa.h"
+
+namespace z80b {
+
+const OpInfo* op_table();                 // kNumOps entries
+const char* op_mnemonic(uint16_t op);     // "ADD A, n" style with placeholders
+const uint8_t* op_encoding(uint16_t op, int* n);
+std::string disassemble(uint32_t insn);   // catalog.go:73-127
+std::string disasm_seq(const uint32_t* seq, int n);  // " : " joined
+
+inline int seq_bytes(const uint32_t* s, int n) {
+  int b = 0;
+  for (int i = 0; i < n; i++) b += op_table()[insn_op(s[i])].size;
+  return b;
+}
+inline int seq_tstates(const uint32_t* s, int n) {
+  int t = 0;
+  for (int i = 0; i < n; i++) t += op_table()[insn_op(s[i])].tstates;
+  return t;
+}
+
+// pkg/search/pruner.go:7-35
+bool should_prune(const uint32_t* seq, int n);
+
+// The 8-bit instruction list in the enumeration order of
+// pkg/search/enumerator.go:319-345: non-immediate opcodes ascending, then
+// the imm8 opcodes ascending with imm 0..255.  4531 entries.
+const std::vector<uint32_t>& pool8();
+// EnumerateFirstOp order (enumerator.go:358-374): pool8 then the imm16 ops
+// with imm 0..65535.  266,675 entries.
+std::vector<uint32_t> first_op_pool();
+
+// Sweep shape of ExhaustiveCheck for a pair (verifier.go:159-171,428-476):
+// kind 0 = A x carry (512 states), 1 = full sweep of n extra 8-bit
+// registers (512 * 256^n states), 2 = reduced sweep (512 * 32^n [* 16]).
+struct Sweep {
+  int kind;
+  int nextra;         // extra 8-bit registers swept
+  uint8_t regs[7];    // 0..6 = B,C,D,E,H,L,M in that order
+  bool sp;            // reduced sweep includes 16 SP values
+  uint64_t states;
+};
+Sweep sweep_for(uint16_t reads);
+uint16_t seq_reads(const uint32_t* s, int n);
+
+// Fixed test vectors, packed as {A|F<<8|B<<16|C<<24, D|E<<8|H<<16|L<<24,
+// SP|M<<16}: the 8 QuickCheck vectors (pkg/search/verifier.go:19-28) and the
+// 32 MidCheck vectors (verifier.go:35-72).  Reduced-sweep representative
+// values (verifier.go:537-542) and SP values (verifier.go:564-567).
+const uint32_t (*qc_vectors())[3];
+const uint32_t (*mid_vectors())[3];
+const uint8_t* rep_values();    // 32
+const uint16_t* rep_sp();       // 16
+
+// cmd/z80opt/main.go:305-322 and 325-397,478-504
+bool parse_dead_flags(const std::string& s, uint8_t* out);
+bool parse_assembly(const std::string& text, std::vector<uint32_t>* out);
+// pkg/result/output.go:93-129
+std::string dead_flag_desc(uint8_t mask);
+
+}  // namespace z80b

@@ -1,0 +1,956 @@
+// z80b_engine.cu -- context, pipeline orchestration and the C ABI of
+// libz80b200.so (declared in include/z80b200.h).
+//
+// The batched pipeline of one job (first-found semantics, pkg/search
+// worker.go:124-265):
+//   1. QuickCheck count pass   (k_qc_scan<false>)  survivors per target
+//   2. exclusive scan          -> contiguous per-target survivor ranges
+//   3. QuickCheck collect pass (k_qc_scan<true>)   survivors in enumeration order
+//   4. rounds: each unresolved (target, pass) lane offers its next survivor;
+//      ExhaustiveCheck of all offered pairs at once; a passing pair resolves
+//      its lane (first passing survivor in enumeration order = the
+//      reference's first found), a failing one advances it.
+//   5. rule compaction in target order.
+// The all-hits pipeline (pkg/gpu/search.go:80-199) replaces 4 by MidCheck on
+// every survivor and one ExhaustiveCheck pass over the MidCheck survivors.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <cub/device/device_scan.cuh>
+#include <string>
+#include <vector>
+
+#include "../../include/z80b200.h"
+#include "z80_tables.h"
+#include "z80b_kernels.cuh"
+
+using namespace z80b;
+
+namespace {
+
+struct DBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~DBuf() {
+    if (p) cudaFree(p);
+  }
+  cudaError_t ensure(size_t b) {
+    if (b <= bytes && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+    size_t want = std::max<size_t>(b, 256);
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaSuccess) bytes = want;
+    return e;
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+struct PoolBufs {
+  DBuf insn, qc, mid, size, prune, reads, lens;
+  DevPool dev{};
+  std::vector<uint32_t> host_insn;
+  std::vector<uint8_t> host_lens;
+  uint32_t n = 0, len = 0;
+  bool loaded = false;
+};
+
+struct Staged {
+  std::vector<uint32_t> targets;
+  std::vector<uint8_t> lens, dead, dregs;
+  z80b_job job{};
+  bool valid = false;
+  DBuf d_targets, d_lens, d_dead, d_dregs;
+};
+
+}  // namespace
+
+struct z80b_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[4] = {};
+  std::vector<cudaEvent_t> kev;  // per-kernel timing events (pairs)
+  std::vector<int> kev_cat;      // category of each pair: 0 qc, 1 exhaustive
+  size_t kev_used = 0;
+  std::string err;
+  PoolBufs pool8;    // the 4,531 8-bit instructions (first-found candidates)
+  PoolBufs loaded;   // z80b_load_candidates
+  PoolBufs firstop;  // EnumerateFirstOp pool for all-hits jobs
+  Staged staged;
+  // pipeline scratch
+  DBuf cnt_f, cnt_m, cnt_all, base, meta, surv, sdiff, checks;
+  DBuf next, win, windiff;
+  DBuf pairs, pair_src, nchunks, cbase, rejected, npairs, counter, states;
+  DBuf rcnt, rbase, rules, checked, surv_target, midpass, flag;
+  DBuf cub_tmp;
+  DBuf hits, nhits, fpq;
+  DBuf v_tgt, v_cand, v_tl, v_cl, v_dead, v_out, v_fd, v_in, v_outs;
+  uint64_t n_rules_dev = 0;
+  uint32_t launches = 0;
+};
+
+namespace {
+
+int fail(z80b_ctx* c, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+#define CK(call)                                                                       \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return fail(ctx, e_ == cudaErrorMemoryAllocation ? Z80B_ENOMEM : Z80B_ECUDA,     \
+                  "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+#define CKR(expr)              \
+  do {                         \
+    int r_ = (expr);           \
+    if (r_ != Z80B_OK) return r_; \
+  } while (0)
+
+int check_launch(z80b_ctx* ctx, const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(ctx, Z80B_ECUDA, "%s launch: %s", what, cudaGetErrorString(e));
+  ctx->launches++;
+  return Z80B_OK;
+}
+
+// Exclusive prefix sum (CUB) of n items.
+template <class T>
+int scan(z80b_ctx* ctx, const T* in, T* out, uint32_t n) {
+  if (!n) return Z80B_OK;
+  size_t tmp = 0;
+  CK(cub::DeviceScan::ExclusiveSum(nullptr, tmp, in, out, n, ctx->stream));
+  CK(ctx->cub_tmp.ensure(tmp));
+  CK(cub::DeviceScan::ExclusiveSum(ctx->cub_tmp.p, tmp, in, out, n, ctx->stream));
+  ctx->launches++;
+  return Z80B_OK;
+}
+
+template <class T>
+int fetch(z80b_ctx* ctx, T* host, const T* dev, size_t n = 1) {
+  CK(cudaMemcpyAsync(host, dev, sizeof(T) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return Z80B_OK;
+}
+
+// Uploads a candidate list and computes its QuickCheck (and optionally
+// MidCheck) outputs on the device.
+int build_pool(z80b_ctx* ctx, PoolBufs& P, const uint32_t* insn, uint32_t n, uint32_t len,
+               const uint8_t* lens, bool with_mid) {
+  P.loaded = false;
+  P.n = n;
+  P.len = len;
+  P.host_insn.assign(insn, insn + (size_t)n * len);
+  P.host_lens.clear();
+  if (lens) P.host_lens.assign(lens, lens + n);
+  std::vector<uint8_t> size(n), prune(n);
+  std::vector<uint16_t> reads(n);
+  for (uint32_t i = 0; i < n; i++) {
+    const uint32_t* s = insn + (size_t)i * len;
+    int l = lens ? lens[i] : int(len);
+    size[i] = uint8_t(seq_bytes(s, l));
+    prune[i] = should_prune(s, l) ? 1 : 0;
+    reads[i] = seq_reads(s, l);
+  }
+  CK(P.insn.ensure(sizeof(uint32_t) * n * len));
+  CK(P.qc.ensure(sizeof(uint4) * 8 * n));
+  if (with_mid) CK(P.mid.ensure(sizeof(uint4) * 32 * n));
+  CK(P.size.ensure(n));
+  CK(P.prune.ensure(n));
+  CK(P.reads.ensure(sizeof(uint16_t) * n));
+  if (lens) CK(P.lens.ensure(n));
+  CK(cudaMemcpyAsync(P.insn.p, insn, sizeof(uint32_t) * n * len, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(P.size.p, size.data(), n, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(P.prune.p, prune.data(), n, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(P.reads.p, reads.data(), sizeof(uint16_t) * n, cudaMemcpyHostToDevice, ctx->stream));
+  if (lens) CK(cudaMemcpyAsync(P.lens.p, lens, n, cudaMemcpyHostToDevice, ctx->stream));
+  if (lens) {
+    // variable-length pools run through k_exec-style outputs: lengths are
+    // honoured by padding with NOP-free zero words is not possible, so the
+    // pool kernel requires a fixed length
+    return fail(ctx, Z80B_EINVAL, "candidate pools need a fixed sequence length");
+  }
+  launch_pool_outputs(P.insn.as<uint32_t>(), n, len, P.qc.as<uint4>(), with_mid ? P.mid.as<uint4>() : nullptr,
+                      ctx->stream);
+  CKR(check_launch(ctx, "pool_outputs"));
+  CK(cudaStreamSynchronize(ctx->stream));
+  P.dev = DevPool{};
+  P.dev.insn = P.insn.as<uint32_t>();
+  P.dev.qc = P.qc.as<uint4>();
+  P.dev.mid = with_mid ? P.mid.as<uint4>() : nullptr;
+  P.dev.size = P.size.as<uint8_t>();
+  P.dev.prune = P.prune.as<uint8_t>();
+  P.dev.reads = P.reads.as<uint16_t>();
+  P.dev.lens = nullptr;
+  P.dev.n = n;
+  P.dev.len = len;
+  P.dev.stride = len;
+  P.loaded = true;
+  return Z80B_OK;
+}
+
+int ensure_firstop(z80b_ctx* ctx) {
+  if (ctx->firstop.loaded) return Z80B_OK;
+  std::vector<uint32_t> v = first_op_pool();
+  return build_pool(ctx, ctx->firstop, v.data(), uint32_t(v.size()), 1, nullptr, false);
+}
+
+bool valid_seq(const uint32_t* s, int n) {
+  for (int i = 0; i < n; i++)
+    if (insn_op(s[i]) >= kNumOps) return false;
+  return true;
+}
+
+int validate_job(z80b_ctx* ctx, const z80b_job* job) {
+  if (!job) return fail(ctx, Z80B_EINVAL, "job is null");
+  if (job->n_targets && !job->targets) return fail(ctx, Z80B_EINVAL, "targets is null");
+  if (job->target_stride < 1 || job->target_stride > 64) return fail(ctx, Z80B_EINVAL, "bad target_stride");
+  if (job->mode != Z80B_MODE_FIRST && job->mode != Z80B_MODE_ALL) return fail(ctx, Z80B_EINVAL, "bad mode");
+  if (job->path != Z80B_PATH_BATCHED && job->path != Z80B_PATH_PLAIN) return fail(ctx, Z80B_EINVAL, "bad path");
+  if (job->max_cand_len != 1) return fail(ctx, Z80B_EINVAL, "max_cand_len must be 1");
+  if (job->global_dead_flags > 0xFF) return fail(ctx, Z80B_EINVAL, "dead flags > 0xFF");
+  for (uint32_t i = 0; i < job->n_targets; i++) {
+    uint32_t l = job->target_lens ? job->target_lens[i] : job->target_len;
+    if (l < 1 || l > uint32_t(kMaxSeq) || l > job->target_stride)
+      return fail(ctx, Z80B_EINVAL, "target %u: length %u outside 1..%d", i, l, kMaxSeq);
+    if (!valid_seq(job->targets + (size_t)i * job->target_stride, int(l)))
+      return fail(ctx, Z80B_EINVAL, "target %u: opcode > 454", i);
+    if (job->dead_regs && (job->dead_regs[i] & ~0x3Fu))
+      return fail(ctx, Z80B_EINVAL, "target %u: dead_regs uses bits above B..L", i);
+  }
+  return Z80B_OK;
+}
+
+// Brackets one kernel launch with a pair of events on the context stream.
+int kbegin(z80b_ctx* ctx, int cat) {
+  if (ctx->kev_used + 2 > ctx->kev.size()) {
+    for (int i = 0; i < 64; i++) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) return -1;
+      ctx->kev.push_back(e);
+    }
+  }
+  int i = int(ctx->kev_used);
+  ctx->kev_used += 2;
+  ctx->kev_cat.resize(ctx->kev_used / 2);
+  ctx->kev_cat[size_t(i / 2)] = cat;
+  cudaEventRecord(ctx->kev[size_t(i)], ctx->stream);
+  return i;
+}
+void kend(z80b_ctx* ctx, int i) {
+  if (i >= 0) cudaEventRecord(ctx->kev[size_t(i) + 1], ctx->stream);
+}
+void ksum(z80b_ctx* ctx, double* qc, double* exh) {
+  for (size_t p = 0; p < ctx->kev_used / 2; p++) {
+    float f = 0;
+    cudaEventSynchronize(ctx->kev[2 * p + 1]);
+    cudaEventElapsedTime(&f, ctx->kev[2 * p], ctx->kev[2 * p + 1]);
+    if (ctx->kev_cat[p] == 0) *qc += f;
+    else *exh += f;
+  }
+  ctx->kev_used = 0;
+}
+
+struct Timer {
+  z80b_ctx* ctx;
+  int a, b;
+  void start() { cudaEventRecord(ctx->ev[a], ctx->stream); }
+  void stop() { cudaEventRecord(ctx->ev[b], ctx->stream); }
+  double ms() {
+    float f = 0;
+    cudaEventSynchronize(ctx->ev[b]);
+    cudaEventElapsedTime(&f, ctx->ev[a], ctx->ev[b]);
+    return f;
+  }
+};
+
+// Runs the pipeline on device-resident targets.  Rules stay in ctx->rules
+// (DevRule), count in *nr.
+int run_pipeline(z80b_ctx* ctx, const DevTargets& T, uint32_t mode, z80b_stats* st, uint64_t* nr) {
+  const uint32_t n = T.n;
+  cudaStream_t s = ctx->stream;
+  PoolBufs* pool = &ctx->pool8;
+  QCConfig cfg{0xFFFFFFFFu, 0, 1};
+  if (mode == Z80B_MODE_ALL) {
+    if (ctx->loaded.loaded) pool = &ctx->loaded;
+    else {
+      CKR(ensure_firstop(ctx));
+      pool = &ctx->firstop;
+    }
+    cfg.w2mask = 0x0000FFFFu;  // 80-byte fingerprint: SP but not M
+    cfg.all_hits = 1;
+  }
+  cfg.use_smem = pool->dev.n <= 6144 ? 1 : 0;
+  const DevPool& P = pool->dev;
+  *nr = 0;
+  if (n == 0) return Z80B_OK;
+
+  CK(ctx->cnt_f.ensure(4ull * n));
+  CK(ctx->cnt_m.ensure(4ull * n));
+  CK(ctx->cnt_all.ensure(4ull * n));
+  CK(ctx->base.ensure(4ull * n));
+  CK(ctx->meta.ensure(sizeof(TargetMeta) * n));
+  CK(ctx->checks.ensure(8));
+  CK(ctx->checked.ensure(8));
+  CK(ctx->states.ensure(8));
+  CK(ctx->npairs.ensure(4));
+  CK(ctx->counter.ensure(8));
+  CK(cudaMemsetAsync(ctx->checks.p, 0, 8, s));
+  CK(cudaMemsetAsync(ctx->checked.p, 0, 8, s));
+  CK(cudaMemsetAsync(ctx->states.p, 0, 8, s));
+
+  Timer tall{ctx, 0, 1};
+  ctx->kev_used = 0;
+  tall.start();
+  int kq = kbegin(ctx, 0);
+  QCOut q{};
+  q.cnt_f = ctx->cnt_f.as<uint32_t>();
+  q.cnt_m = ctx->cnt_m.as<uint32_t>();
+  q.cnt_all = ctx->cnt_all.as<uint32_t>();
+  q.meta = ctx->meta.as<TargetMeta>();
+  q.checks = ctx->checks.as<unsigned long long>();
+  launch_qc_scan(T, P, cfg, q, false, s);
+  kend(ctx, kq);
+  CKR(check_launch(ctx, "qc_count"));
+  CKR(scan(ctx, ctx->cnt_all.as<uint32_t>(), ctx->base.as<uint32_t>(), n));
+  uint32_t last[4] = {0, 0, 0, 0};
+  CK(cudaMemcpyAsync(&last[0], ctx->base.as<uint32_t>() + (n - 1), 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&last[1], ctx->cnt_f.as<uint32_t>() + (n - 1), 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&last[2], ctx->cnt_m.as<uint32_t>() + (n - 1), 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  const uint64_t nsurv = uint64_t(last[0]) + last[1] + last[2];
+  if (nsurv > 0xFFFFFFF0ull) return fail(ctx, Z80B_ECAPACITY, "too many QuickCheck survivors (%llu)", (unsigned long long)nsurv);
+  CK(ctx->surv.ensure(4ull * std::max<uint64_t>(nsurv, 1)));
+  CK(ctx->sdiff.ensure(2ull * std::max<uint64_t>(nsurv, 1)));
+  q.base = ctx->base.as<uint32_t>();
+  q.surv = ctx->surv.as<uint32_t>();
+  q.sdiff = ctx->sdiff.as<uint16_t>();
+  if (nsurv) {
+    int kc = kbegin(ctx, 0);
+    launch_qc_scan(T, P, cfg, q, true, s);
+    kend(ctx, kc);
+    CKR(check_launch(ctx, "qc_collect"));
+  }
+
+  RoundBuf R{};
+  uint32_t rounds = 0;
+  uint64_t exh_pairs = 0, mid_surv = 0;
+  if (mode == Z80B_MODE_FIRST) {
+    CK(ctx->next.ensure(8ull * n));
+    CK(ctx->win.ensure(8ull * n));
+    CK(ctx->windiff.ensure(4ull * n));
+    CK(ctx->pairs.ensure(sizeof(PairRec) * 2ull * n));
+    CK(ctx->pair_src.ensure(8ull * n));
+    CK(ctx->nchunks.ensure(16ull * n));
+    CK(ctx->cbase.ensure(16ull * n));
+    CK(ctx->rejected.ensure(8ull * n));
+    CK(cudaMemsetAsync(ctx->next.p, 0, 8ull * n, s));
+    CK(cudaMemsetAsync(ctx->win.p, 0xFF, 8ull * n, s));
+    Lanes L{ctx->next.as<uint32_t>(), ctx->win.as<uint32_t>(), ctx->windiff.as<uint16_t>()};
+    R.pairs = ctx->pairs.as<PairRec>();
+    R.pair_src = ctx->pair_src.as<uint32_t>();
+    R.nchunks = ctx->nchunks.as<unsigned long long>();
+    R.cbase = ctx->cbase.as<unsigned long long>();
+    R.rejected = ctx->rejected.as<uint32_t>();
+    R.npairs = ctx->npairs.as<uint32_t>();
+    R.counter = ctx->counter.as<unsigned long long>();
+    R.states = ctx->states.as<unsigned long long>();
+    if (nsurv) {
+      for (;;) {
+        CK(cudaMemsetAsync(R.npairs, 0, 4, s));
+        launch_round_build(T, P, q, L, R, s);
+        CKR(check_launch(ctx, "round_build"));
+        uint32_t np = 0;
+        CKR(fetch(ctx, &np, R.npairs));
+        if (np == 0) break;
+        rounds++;
+        exh_pairs += np;
+        CKR(scan(ctx, R.nchunks, R.cbase, np));
+        unsigned long long lastb = 0, lastn = 0;
+        CK(cudaMemcpyAsync(&lastb, R.cbase + (np - 1), 8, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(&lastn, R.nchunks + (np - 1), 8, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        CK(cudaMemsetAsync(R.counter, 0, 8, s));
+        int ke = kbegin(ctx, 1);
+        launch_exhaustive(T, P, R, np, lastb + lastn, s);
+        kend(ctx, ke);
+        CKR(check_launch(ctx, "exhaustive"));
+        launch_round_resolve(R, np, q, L, s);
+        CKR(check_launch(ctx, "round_resolve"));
+      }
+    }
+    CK(ctx->rcnt.ensure(4ull * n));
+    CK(ctx->rbase.ensure(4ull * n));
+    launch_rule_count_first(L, n, ctx->rcnt.as<uint32_t>(), T, ctx->checked.as<unsigned long long>(),
+                            uint32_t(pool8().size()), s);
+    CKR(check_launch(ctx, "rule_count"));
+    CKR(scan(ctx, ctx->rcnt.as<uint32_t>(), ctx->rbase.as<uint32_t>(), n));
+    uint32_t lb = 0, lc = 0;
+    CK(cudaMemcpyAsync(&lb, ctx->rbase.as<uint32_t>() + (n - 1), 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&lc, ctx->rcnt.as<uint32_t>() + (n - 1), 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    *nr = uint64_t(lb) + lc;
+    CK(ctx->rules.ensure(sizeof(DevRule) * std::max<uint64_t>(*nr, 1)));
+    launch_rule_write_first(L, n, ctx->rbase.as<uint32_t>(), ctx->rules.as<DevRule>(), s);
+    CKR(check_launch(ctx, "rule_write"));
+  } else {
+    // all-hits: MidCheck on every survivor, one ExhaustiveCheck pass
+    const uint32_t S = uint32_t(nsurv);
+    CK(ctx->surv_target.ensure(4ull * std::max<uint32_t>(S, 1)));
+    CK(ctx->midpass.ensure(std::max<uint32_t>(S, 1)));
+    CK(ctx->flag.ensure(4ull * std::max<uint32_t>(S, 1)));
+    CK(ctx->rbase.ensure(4ull * std::max<uint32_t>(S, 1)));
+    CK(ctx->pairs.ensure(sizeof(PairRec) * std::max<uint32_t>(S, 1)));
+    CK(ctx->pair_src.ensure(4ull * std::max<uint32_t>(S, 1)));
+    CK(ctx->nchunks.ensure(8ull * std::max<uint32_t>(S, 1)));
+    CK(ctx->cbase.ensure(8ull * std::max<uint32_t>(S, 1)));
+    CK(ctx->rejected.ensure(4ull * std::max<uint32_t>(S, 1)));
+    R.pairs = ctx->pairs.as<PairRec>();
+    R.pair_src = ctx->pair_src.as<uint32_t>();
+    R.nchunks = ctx->nchunks.as<unsigned long long>();
+    R.cbase = ctx->cbase.as<unsigned long long>();
+    R.rejected = ctx->rejected.as<uint32_t>();
+    R.npairs = ctx->npairs.as<uint32_t>();
+    R.counter = ctx->counter.as<unsigned long long>();
+    R.states = ctx->states.as<unsigned long long>();
+    if (S) {
+      launch_surv_targets(q, n, ctx->surv_target.as<uint32_t>(), s);
+      CKR(check_launch(ctx, "surv_targets"));
+      launch_midcheck(T, P, q.surv, ctx->surv_target.as<uint32_t>(), S, ctx->midpass.as<uint8_t>(), s);
+      CKR(check_launch(ctx, "midcheck"));
+      CK(cudaMemsetAsync(R.npairs, 0, 4, s));
+      launch_pairs_from_survivors(T, P, q, ctx->midpass.as<uint8_t>(), S, ctx->surv_target.as<uint32_t>(), R, s);
+      CKR(check_launch(ctx, "pairs"));
+      uint32_t np = 0;
+      CKR(fetch(ctx, &np, R.npairs));
+      mid_surv = np;
+      exh_pairs = np;
+      CK(cudaMemsetAsync(ctx->flag.p, 0, 4ull * S, s));
+      if (np) {
+        rounds = 1;
+        CKR(scan(ctx, R.nchunks, R.cbase, np));
+        unsigned long long lastb = 0, lastn = 0;
+        CK(cudaMemcpyAsync(&lastb, R.cbase + (np - 1), 8, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(&lastn, R.nchunks + (np - 1), 8, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        CK(cudaMemsetAsync(R.counter, 0, 8, s));
+        int ke = kbegin(ctx, 1);
+        launch_exhaustive(T, P, R, np, lastb + lastn, s);
+        kend(ctx, ke);
+        CKR(check_launch(ctx, "exhaustive"));
+        launch_rule_count_all(R, np, ctx->flag.as<uint32_t>(), s);
+        CKR(check_launch(ctx, "rule_count_all"));
+      }
+      CKR(scan(ctx, ctx->flag.as<uint32_t>(), ctx->rbase.as<uint32_t>(), S));
+      uint32_t lb = 0, lc = 0;
+      CK(cudaMemcpyAsync(&lb, ctx->rbase.as<uint32_t>() + (S - 1), 4, cudaMemcpyDeviceToHost, s));
+      CK(cudaMemcpyAsync(&lc, ctx->flag.as<uint32_t>() + (S - 1), 4, cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      *nr = uint64_t(lb) + lc;
+      CK(ctx->rules.ensure(sizeof(DevRule) * std::max<uint64_t>(*nr, 1)));
+      launch_rule_write_all(ctx->flag.as<uint32_t>(), ctx->rbase.as<uint32_t>(), S, q.surv, q.sdiff,
+                            ctx->surv_target.as<uint32_t>(), ctx->rules.as<DevRule>(), s);
+      CKR(check_launch(ctx, "rule_write_all"));
+    }
+  }
+  tall.stop();
+  CK(cudaStreamSynchronize(s));
+  if (st) {
+    unsigned long long checks = 0, checked = 0, states = 0;
+    CKR(fetch(ctx, &checks, ctx->checks.as<unsigned long long>()));
+    CKR(fetch(ctx, &checked, ctx->checked.as<unsigned long long>()));
+    CKR(fetch(ctx, &states, ctx->states.as<unsigned long long>()));
+    st->targets += n;
+    st->checks += checks;
+    st->checked_ref += (mode == Z80B_MODE_FIRST) ? checked : 0;
+    st->qc_survivors += nsurv;
+    st->mid_survivors += mid_surv;
+    st->exhaustive_pairs += exh_pairs;
+    st->exhaustive_states += states;
+    st->rules += *nr;
+    st->rounds += rounds;
+    double a = 0, b = 0;
+    ksum(ctx, &a, &b);
+    st->qc_ms += a;
+    st->exh_ms += b;
+    st->device_ms += tall.ms();
+  }
+  ctx->n_rules_dev = *nr;
+  return Z80B_OK;
+}
+
+// Converts device rules to z80b_rule records.
+void to_rules(z80b_ctx* ctx, const std::vector<DevRule>& dr, const uint32_t* targets, const uint8_t* tlens,
+              uint32_t tlen, uint32_t stride, uint32_t mode, uint32_t tindex_offset, z80b_rule* out) {
+  const PoolBufs& P = (mode == Z80B_MODE_ALL) ? (ctx->loaded.loaded ? ctx->loaded : ctx->firstop) : ctx->pool8;
+  for (size_t i = 0; i < dr.size(); i++) {
+    const DevRule& r = dr[i];
+    z80b_rule& o = out[i];
+    std::memset(&o, 0, sizeof o);
+    const uint32_t* t = targets + (size_t)r.target * stride;
+    int tl = tlens ? tlens[r.target] : int(tlen);
+    const uint32_t* c = P.host_insn.data() + (size_t)r.cand * P.len;
+    int cl = int(P.len);
+    o.src_len = tl;
+    o.rep_len = cl;
+    for (int k = 0; k < tl; k++) o.src[k] = t[k];
+    for (int k = 0; k < cl; k++) o.rep[k] = c[k];
+    o.bytes_saved = seq_bytes(t, tl) - seq_bytes(c, cl);
+    o.cycles_saved = seq_tstates(t, tl) - seq_tstates(c, cl);
+    o.dead_flags = (r.kind == 0) ? 0 : int(r.diff & 0xFFu);
+    o.dead_regs = (r.kind == 0) ? 0 : int(r.diff >> 8);
+    o.target_index = int(r.target + tindex_offset);
+  }
+}
+
+// Uploads the job's arrays straight from the caller's buffers (pinned
+// buffers make this a DMA).  keep_host copies the targets for a later
+// z80b_fetch_rules; z80b_search converts rules while the caller's buffers
+// are still valid and skips the copy.
+int upload_targets(z80b_ctx* ctx, Staged& S, const z80b_job* job, DevTargets* T, bool keep_host) {
+  const uint32_t n = job->n_targets;
+  const size_t words = (size_t)n * job->target_stride;
+  S.targets.clear();
+  if (keep_host) S.targets.assign(job->targets, job->targets + words);
+  S.lens.clear();
+  S.dead.clear();
+  S.dregs.clear();
+  if (job->target_lens) S.lens.assign(job->target_lens, job->target_lens + n);
+  if (job->dead_flags) S.dead.assign(job->dead_flags, job->dead_flags + n);
+  if (job->dead_regs) S.dregs.assign(job->dead_regs, job->dead_regs + n);
+  S.job = *job;
+  cudaStream_t s = ctx->stream;
+  CK(S.d_targets.ensure(4ull * std::max<size_t>(words, 1)));
+  if (n) CK(cudaMemcpyAsync(S.d_targets.p, job->targets, 4ull * words, cudaMemcpyHostToDevice, s));
+  *T = DevTargets{};
+  T->insn = S.d_targets.as<uint32_t>();
+  T->n = n;
+  T->stride = job->target_stride;
+  T->fixed_len = job->target_len;
+  T->global_dead = job->global_dead_flags;
+  if (!S.lens.empty()) {
+    CK(S.d_lens.ensure(n));
+    CK(cudaMemcpyAsync(S.d_lens.p, S.lens.data(), n, cudaMemcpyHostToDevice, s));
+    T->len = S.d_lens.as<uint8_t>();
+  }
+  if (!S.dead.empty()) {
+    CK(S.d_dead.ensure(n));
+    CK(cudaMemcpyAsync(S.d_dead.p, S.dead.data(), n, cudaMemcpyHostToDevice, s));
+    T->dead = S.d_dead.as<uint8_t>();
+  }
+  if (!S.dregs.empty()) {
+    CK(S.d_dregs.ensure(n));
+    CK(cudaMemcpyAsync(S.d_dregs.p, S.dregs.data(), n, cudaMemcpyHostToDevice, s));
+    T->dead_regs = S.d_dregs.as<uint8_t>();
+  }
+  S.valid = true;
+  return Z80B_OK;
+}
+
+DevTargets staged_targets(Staged& S) {
+  DevTargets T{};
+  T.insn = S.d_targets.as<uint32_t>();
+  T.n = S.job.n_targets;
+  T.stride = S.job.target_stride;
+  T.fixed_len = S.job.target_len;
+  T.global_dead = S.job.global_dead_flags;
+  if (!S.lens.empty()) T.len = S.d_lens.as<uint8_t>();
+  if (!S.dead.empty()) T.dead = S.d_dead.as<uint8_t>();
+  if (!S.dregs.empty()) T.dead_regs = S.d_dregs.as<uint8_t>();
+  return T;
+}
+
+// Runs the staged job (batched or plain path) and leaves rules on the device
+// (batched) or appends them to host_rules (plain).
+int run_staged(z80b_ctx* ctx, z80b_stats* st, uint64_t* nr, std::vector<z80b_rule>* host_rules,
+               const uint32_t* host_targets) {
+  Staged& S = ctx->staged;
+  DevTargets T = staged_targets(S);
+  const z80b_job& job = S.job;
+  if (job.path == Z80B_PATH_BATCHED) return run_pipeline(ctx, T, job.mode, st, nr);
+  // plain: one target per pipeline launch, synchronizing in between
+  uint64_t total = 0;
+  std::vector<DevRule> dr;
+  for (uint32_t i = 0; i < T.n; i++) {
+    DevTargets one = T;
+    one.insn = T.insn + (size_t)i * T.stride;
+    one.n = 1;
+    if (T.len) one.len = T.len + i;
+    if (T.dead) one.dead = T.dead + i;
+    if (T.dead_regs) one.dead_regs = T.dead_regs + i;
+    uint64_t k = 0;
+    CKR(run_pipeline(ctx, one, job.mode, st, &k));
+    if (k) {
+      dr.resize(k);
+      CK(cudaMemcpyAsync(dr.data(), ctx->rules.p, sizeof(DevRule) * k, cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+      if (host_rules) {
+        size_t off = host_rules->size();
+        host_rules->resize(off + k);
+        to_rules(ctx, dr, host_targets + (size_t)i * T.stride, S.lens.empty() ? nullptr : &S.lens[i],
+                 job.target_len, T.stride, job.mode, i, host_rules->data() + off);
+      }
+    }
+    total += k;
+  }
+  *nr = total;
+  return Z80B_OK;
+}
+
+}  // namespace
+
+// ============================================================== C ABI
+
+extern "C" {
+
+int z80b_version(void) { return 1; }
+
+const char* z80b_status_string(int s) {
+  switch (s) {
+    case Z80B_OK: return "ok";
+    case Z80B_EINVAL: return "invalid argument";
+    case Z80B_ENOMEM: return "out of device memory";
+    case Z80B_ECUDA: return "CUDA error";
+    case Z80B_ETIMEOUT: return "device wait timed out";
+    case Z80B_ECAPACITY: return "output buffer too small";
+    case Z80B_ENODEV: return "no usable CUDA device";
+    case Z80B_ESTATE: return "call out of order";
+  }
+  return "unknown status";
+}
+
+const char* z80b_last_error(const z80b_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int z80b_init(int device, z80b_ctx** out) {
+  if (!out) return Z80B_EINVAL;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return Z80B_ENODEV;
+  if (device < 0 || device >= ndev) return Z80B_EINVAL;
+  cudaDeviceProp prop{};
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return Z80B_ENODEV;
+  if (prop.major < 10) return Z80B_ENODEV;  // built for sm_100a only
+  z80b_ctx* ctx = new z80b_ctx();
+  ctx->device = device;
+  if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return Z80B_ECUDA;
+  }
+  for (auto& e : ctx->ev) cudaEventCreate(&e);
+  dev_upload_tables(ctx->stream);
+  const auto& p8 = pool8();
+  int r = build_pool(ctx, ctx->pool8, p8.data(), uint32_t(p8.size()), 1, nullptr, false);
+  if (r != Z80B_OK) {
+    z80b_destroy(ctx);
+    return r;
+  }
+  *out = ctx;
+  return Z80B_OK;
+}
+
+void z80b_destroy(z80b_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto& e : ctx->ev)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : ctx->kev) cudaEventDestroy(e);
+  cudaStream_t s = ctx->stream;
+  delete ctx;
+  if (s) cudaStreamDestroy(s);
+}
+
+int z80b_fingerprints(z80b_ctx* ctx, const uint32_t* seqs, uint32_t n, uint32_t len, uint8_t* out) {
+  if (!ctx) return Z80B_EINVAL;
+  if ((n && (!seqs || !out)) || len < 1 || len > uint32_t(kMaxSeq)) return fail(ctx, Z80B_EINVAL, "bad arguments");
+  if (!n) return Z80B_OK;
+  for (uint32_t i = 0; i < n; i++)
+    if (!valid_seq(seqs + (size_t)i * len, int(len))) return fail(ctx, Z80B_EINVAL, "sequence %u: opcode > 454", i);
+  cudaSetDevice(ctx->device);
+  CK(ctx->v_tgt.ensure(4ull * n * len));
+  CK(ctx->v_out.ensure(80ull * n));
+  CK(cudaMemcpyAsync(ctx->v_tgt.p, seqs, 4ull * n * len, cudaMemcpyHostToDevice, ctx->stream));
+  launch_fingerprints(ctx->v_tgt.as<uint32_t>(), n, len, ctx->v_out.as<uint8_t>(), ctx->stream);
+  CKR(check_launch(ctx, "fingerprints"));
+  CK(cudaMemcpyAsync(out, ctx->v_out.p, 80ull * n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return Z80B_OK;
+}
+
+int z80b_exec(z80b_ctx* ctx, const z80b_state* in, const uint32_t* seqs, const uint8_t* lens, uint32_t len,
+              uint32_t stride, uint32_t n, z80b_state* out) {
+  if (!ctx) return Z80B_EINVAL;
+  if (n && (!in || !seqs || !out)) return fail(ctx, Z80B_EINVAL, "null pointer");
+  if (stride < 1 || stride > 64) return fail(ctx, Z80B_EINVAL, "bad stride");
+  if (!n) return Z80B_OK;
+  for (uint32_t i = 0; i < n; i++) {
+    uint32_t l = lens ? lens[i] : len;
+    if (l > uint32_t(kMaxSeq) || l > stride) return fail(ctx, Z80B_EINVAL, "sequence %u: bad length", i);
+    if (!valid_seq(seqs + (size_t)i * stride, int(l))) return fail(ctx, Z80B_EINVAL, "sequence %u: opcode > 454", i);
+  }
+  cudaSetDevice(ctx->device);
+  std::vector<uint32_t> packed(3ull * n);
+  for (uint32_t i = 0; i < n; i++) {
+    const z80b_state& s = in[i];
+    packed[3 * i] = uint32_t(s.a) | uint32_t(s.f) << 8 | uint32_t(s.b) << 16 | uint32_t(s.c) << 24;
+    packed[3 * i + 1] = uint32_t(s.d) | uint32_t(s.e) << 8 | uint32_t(s.h) << 16 | uint32_t(s.l) << 24;
+    packed[3 * i + 2] = uint32_t(s.sp) | uint32_t(s.m) << 16;
+  }
+  CK(ctx->v_in.ensure(12ull * n));
+  CK(ctx->v_outs.ensure(12ull * n));
+  CK(ctx->v_tgt.ensure(4ull * n * stride));
+  CK(ctx->v_tl.ensure(n));
+  CK(cudaMemcpyAsync(ctx->v_in.p, packed.data(), 12ull * n, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->v_tgt.p, seqs, 4ull * n * stride, cudaMemcpyHostToDevice, ctx->stream));
+  if (lens) CK(cudaMemcpyAsync(ctx->v_tl.p, lens, n, cudaMemcpyHostToDevice, ctx->stream));
+  launch_exec(ctx->v_in.as<uint32_t>(), ctx->v_tgt.as<uint32_t>(), lens ? ctx->v_tl.as<uint8_t>() : nullptr, len,
+              stride, n, ctx->v_outs.as<uint32_t>(), ctx->stream);
+  CKR(check_launch(ctx, "exec"));
+  CK(cudaMemcpyAsync(packed.data(), ctx->v_outs.p, 12ull * n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (uint32_t i = 0; i < n; i++) {
+    z80b_state& s = out[i];
+    uint32_t w0 = packed[3 * i], w1 = packed[3 * i + 1], w2 = packed[3 * i + 2];
+    s.a = uint8_t(w0); s.f = uint8_t(w0 >> 8); s.b = uint8_t(w0 >> 16); s.c = uint8_t(w0 >> 24);
+    s.d = uint8_t(w1); s.e = uint8_t(w1 >> 8); s.h = uint8_t(w1 >> 16); s.l = uint8_t(w1 >> 24);
+    s.sp = uint16_t(w2); s.m = uint8_t(w2 >> 16); s.pad = 0;
+  }
+  return Z80B_OK;
+}
+
+int z80b_load_candidates(z80b_ctx* ctx, const uint32_t* cands, uint32_t count, uint32_t seq_len) {
+  if (!ctx) return Z80B_EINVAL;
+  if ((count && !cands) || seq_len < 1 || seq_len > 3) return fail(ctx, Z80B_EINVAL, "bad arguments");
+  for (uint32_t i = 0; i < count; i++)
+    if (!valid_seq(cands + (size_t)i * seq_len, int(seq_len)))
+      return fail(ctx, Z80B_EINVAL, "candidate %u: opcode > 454", i);
+  cudaSetDevice(ctx->device);
+  return build_pool(ctx, ctx->loaded, cands, count, seq_len, nullptr, false);
+}
+
+int z80b_quickcheck(z80b_ctx* ctx, const uint8_t* fp80, uint32_t dead_flags, uint32_t* hits, uint32_t cap,
+                    uint32_t* n_hits) {
+  if (!ctx) return Z80B_EINVAL;
+  if (!fp80 || !n_hits || (cap && !hits)) return fail(ctx, Z80B_EINVAL, "null pointer");
+  if (!ctx->loaded.loaded) return fail(ctx, Z80B_ESTATE, "z80b_load_candidates has not been called");
+  cudaSetDevice(ctx->device);
+  // fingerprint bytes -> packed words (F byte masked on the device)
+  uint32_t w[24];
+  for (int v = 0; v < 8; v++) {
+    const uint8_t* p = fp80 + v * 10;
+    w[3 * v] = uint32_t(p[0]) | uint32_t(p[1]) << 8 | uint32_t(p[2]) << 16 | uint32_t(p[3]) << 24;
+    w[3 * v + 1] = uint32_t(p[4]) | uint32_t(p[5]) << 8 | uint32_t(p[6]) << 16 | uint32_t(p[7]) << 24;
+    w[3 * v + 2] = uint32_t(p[8]) << 8 | uint32_t(p[9]);
+  }
+  const uint32_t dev_cap = ctx->loaded.n;
+  CK(ctx->fpq.ensure(sizeof w));
+  CK(ctx->hits.ensure(4ull * std::max<uint32_t>(dev_cap, 1)));
+  CK(ctx->nhits.ensure(4));
+  CK(cudaMemcpyAsync(ctx->fpq.p, w, sizeof w, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaMemsetAsync(ctx->nhits.p, 0, 4, ctx->stream));
+  launch_fp_query(ctx->loaded.dev, ctx->fpq.as<uint32_t>(), dead_flags & 0xFFu, ctx->hits.as<uint32_t>(),
+                  ctx->nhits.as<uint32_t>(), dev_cap, ctx->stream);
+  CKR(check_launch(ctx, "fp_query"));
+  uint32_t nh = 0;
+  CKR(fetch(ctx, &nh, ctx->nhits.as<uint32_t>()));
+  std::vector<uint32_t> h(nh);
+  if (nh) CKR(fetch(ctx, h.data(), ctx->hits.as<uint32_t>(), nh));
+  std::sort(h.begin(), h.end());
+  *n_hits = nh;
+  for (uint32_t i = 0; i < nh && i < cap; i++) hits[i] = h[i];
+  return nh > cap ? fail(ctx, Z80B_ECAPACITY, "%u hits, capacity %u", nh, cap) : Z80B_OK;
+}
+
+int z80b_verify_pairs(z80b_ctx* ctx, const uint32_t* tgt, const uint8_t* tlens, const uint32_t* cand,
+                      const uint8_t* clens, uint32_t stride, uint32_t n, const uint8_t* dead, uint32_t tiers,
+                      uint8_t* out, uint8_t* flagdiff) {
+  if (!ctx) return Z80B_EINVAL;
+  if (n && (!tgt || !tlens || !cand || !clens || !out)) return fail(ctx, Z80B_EINVAL, "null pointer");
+  if (stride < 1 || stride > 64) return fail(ctx, Z80B_EINVAL, "bad stride");
+  if (!n) return Z80B_OK;
+  for (uint32_t i = 0; i < n; i++) {
+    if (tlens[i] < 1 || tlens[i] > kMaxSeq || tlens[i] > stride || clens[i] < 1 || clens[i] > kMaxSeq - 1 ||
+        clens[i] > stride)
+      return fail(ctx, Z80B_EINVAL, "pair %u: bad length", i);
+    if (!valid_seq(tgt + (size_t)i * stride, tlens[i]) || !valid_seq(cand + (size_t)i * stride, clens[i]))
+      return fail(ctx, Z80B_EINVAL, "pair %u: opcode > 454", i);
+  }
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  CK(ctx->v_tgt.ensure(4ull * n * stride));
+  CK(ctx->v_cand.ensure(4ull * n * stride));
+  CK(ctx->v_tl.ensure(n));
+  CK(ctx->v_cl.ensure(n));
+  CK(ctx->v_dead.ensure(n));
+  CK(ctx->v_out.ensure(n));
+  CK(ctx->v_fd.ensure(n));
+  CK(cudaMemcpyAsync(ctx->v_tgt.p, tgt, 4ull * n * stride, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(ctx->v_cand.p, cand, 4ull * n * stride, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(ctx->v_tl.p, tlens, n, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(ctx->v_cl.p, clens, n, cudaMemcpyHostToDevice, s));
+  if (dead) CK(cudaMemcpyAsync(ctx->v_dead.p, dead, n, cudaMemcpyHostToDevice, s));
+  else CK(cudaMemsetAsync(ctx->v_dead.p, 0, n, s));
+  launch_verify_small(ctx->v_tgt.as<uint32_t>(), ctx->v_tl.as<uint8_t>(), ctx->v_cand.as<uint32_t>(),
+                      ctx->v_cl.as<uint8_t>(), stride, n, ctx->v_dead.as<uint8_t>(), tiers, ctx->v_out.as<uint8_t>(),
+                      ctx->v_fd.as<uint8_t>(), s);
+  CKR(check_launch(ctx, "verify_small"));
+  std::vector<uint8_t> res(n), fd(n);
+  CK(cudaMemcpyAsync(res.data(), ctx->v_out.p, n, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(fd.data(), ctx->v_fd.p, n, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (tiers & 4u) {
+    // ExhaustiveCheck of every pair: pairs are (i, i) of a target batch and
+    // a candidate pool with per-candidate lengths
+    DevTargets T{};
+    T.insn = ctx->v_tgt.as<uint32_t>();
+    T.len = ctx->v_tl.as<uint8_t>();
+    T.dead = ctx->v_dead.as<uint8_t>();
+    T.n = n;
+    T.stride = stride;
+    DevPool P{};
+    P.insn = ctx->v_cand.as<uint32_t>();
+    P.lens = ctx->v_cl.as<uint8_t>();
+    P.n = n;
+    P.stride = stride;
+    std::vector<PairRec> pr(n);
+    std::vector<unsigned long long> nch(n), cb(n);
+    unsigned long long tot = 0;
+    for (uint32_t i = 0; i < n; i++) {
+      uint16_t rd = uint16_t(seq_reads(tgt + (size_t)i * stride, tlens[i]) | seq_reads(cand + (size_t)i * stride, clens[i]));
+      Sweep w = sweep_for(rd);
+      pr[i] = PairRec{};
+      pr[i].target = i;
+      pr[i].cand = i;
+      pr[i].reads = rd;
+      pr[i].nblocks = w.states / 256;
+      pr[i].keepF = uint8_t(~(dead ? dead[i] : 0u));
+      pr[i].keepR = 0x3F;
+      unsigned long long c = (pr[i].nblocks + 31) / 32;
+      nch[i] = c > 65536 ? 65536 : c;
+      cb[i] = tot;
+      tot += nch[i];
+    }
+    CK(ctx->pairs.ensure(sizeof(PairRec) * n));
+    CK(ctx->cbase.ensure(8ull * n));
+    CK(ctx->rejected.ensure(4ull * n));
+    CK(ctx->counter.ensure(8));
+    CK(ctx->states.ensure(8));
+    CK(cudaMemcpyAsync(ctx->pairs.p, pr.data(), sizeof(PairRec) * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(ctx->cbase.p, cb.data(), 8ull * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(ctx->rejected.p, 0, 4ull * n, s));
+    CK(cudaMemsetAsync(ctx->counter.p, 0, 8, s));
+    RoundBuf R{};
+    R.pairs = ctx->pairs.as<PairRec>();
+    R.cbase = ctx->cbase.as<unsigned long long>();
+    R.rejected = ctx->rejected.as<uint32_t>();
+    R.counter = ctx->counter.as<unsigned long long>();
+    R.states = ctx->states.as<unsigned long long>();
+    launch_exhaustive(T, P, R, n, tot, s);
+    CKR(check_launch(ctx, "exhaustive"));
+    std::vector<uint32_t> rej(n);
+    CK(cudaMemcpyAsync(rej.data(), ctx->rejected.p, 4ull * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    for (uint32_t i = 0; i < n; i++)
+      if (!rej[i]) res[i] |= 4;
+  }
+  std::memcpy(out, res.data(), n);
+  if (flagdiff) std::memcpy(flagdiff, fd.data(), n);
+  return Z80B_OK;
+}
+
+int z80b_stage_job(z80b_ctx* ctx, const z80b_job* job) {
+  if (!ctx) return Z80B_EINVAL;
+  CKR(validate_job(ctx, job));
+  cudaSetDevice(ctx->device);
+  DevTargets T;
+  CKR(upload_targets(ctx, ctx->staged, job, &T, true));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return Z80B_OK;
+}
+
+int z80b_run_staged(z80b_ctx* ctx, uint64_t* n_rules, z80b_stats* stats) {
+  if (!ctx) return Z80B_EINVAL;
+  if (!ctx->staged.valid) return fail(ctx, Z80B_ESTATE, "no staged job");
+  if (ctx->staged.job.path != Z80B_PATH_BATCHED) return fail(ctx, Z80B_EINVAL, "staged runs use the batched path");
+  cudaSetDevice(ctx->device);
+  if (stats) std::memset(stats, 0, sizeof *stats);
+  ctx->launches = 0;
+  uint64_t nr = 0;
+  CKR(run_staged(ctx, stats, &nr, nullptr, ctx->staged.targets.data()));
+  if (stats) stats->launches = ctx->launches;
+  if (n_rules) *n_rules = nr;
+  return Z80B_OK;
+}
+
+int z80b_fetch_rules(z80b_ctx* ctx, z80b_rule* out, uint64_t cap, uint64_t* n_rules) {
+  if (!ctx) return Z80B_EINVAL;
+  if (!ctx->staged.valid) return fail(ctx, Z80B_ESTATE, "no staged job");
+  uint64_t nr = ctx->n_rules_dev;
+  if (n_rules) *n_rules = nr;
+  if (nr > cap) return fail(ctx, Z80B_ECAPACITY, "%llu rules, capacity %llu", (unsigned long long)nr,
+                            (unsigned long long)cap);
+  if (nr && !out) return fail(ctx, Z80B_EINVAL, "null output");
+  std::vector<DevRule> dr(nr);
+  if (nr) {
+    CK(cudaMemcpyAsync(dr.data(), ctx->rules.p, sizeof(DevRule) * nr, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  const Staged& S = ctx->staged;
+  to_rules(ctx, dr, S.targets.data(), S.lens.empty() ? nullptr : S.lens.data(), S.job.target_len,
+           S.job.target_stride, S.job.mode, 0, out);
+  return Z80B_OK;
+}
+
+int z80b_search(z80b_ctx* ctx, const z80b_job* job, z80b_rule* out, uint64_t cap, uint64_t* n_rules,
+                z80b_stats* stats) {
+  if (!ctx) return Z80B_EINVAL;
+  if (!n_rules) return fail(ctx, Z80B_EINVAL, "n_rules is null");
+  CKR(validate_job(ctx, job));
+  cudaSetDevice(ctx->device);
+  if (stats) std::memset(stats, 0, sizeof *stats);
+  ctx->launches = 0;
+  DevTargets T;
+  CKR(upload_targets(ctx, ctx->staged, job, &T, false));
+  ctx->staged.valid = false;  // this job's targets are not kept for z80b_fetch_rules
+  uint64_t nr = 0;
+  if (job->path == Z80B_PATH_PLAIN) {
+    std::vector<z80b_rule> hr;
+    CKR(run_staged(ctx, stats, &nr, &hr, job->targets));
+    *n_rules = nr;
+    if (stats) stats->launches = ctx->launches;
+    for (uint64_t i = 0; i < nr && i < cap; i++) out[i] = hr[i];
+    return nr > cap ? fail(ctx, Z80B_ECAPACITY, "%llu rules, capacity %llu", (unsigned long long)nr,
+                           (unsigned long long)cap)
+                    : Z80B_OK;
+  }
+  CKR(run_pipeline(ctx, T, job->mode, stats, &nr));
+  if (stats) stats->launches = ctx->launches;
+  *n_rules = nr;
+  if (nr > cap)
+    return fail(ctx, Z80B_ECAPACITY, "%llu rules, capacity %llu", (unsigned long long)nr, (unsigned long long)cap);
+  if (nr && !out) return fail(ctx, Z80B_EINVAL, "null output");
+  std::vector<DevRule> dr(nr);
+  if (nr) {
+    CK(cudaMemcpyAsync(dr.data(), ctx->rules.p, sizeof(DevRule) * nr, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  to_rules(ctx, dr, job->targets, job->target_lens, job->target_len, job->target_stride, job->mode, 0, out);
+  return Z80B_OK;
+}
+
+}  // extern "C"

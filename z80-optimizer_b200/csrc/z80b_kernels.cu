@@ -1,0 +1,767 @@
+// z80b_kernels.cu -- the CUDA kernels of the verification pipeline (sm_100a).
+//
+// Tier 1, QuickCheck (pkg/search/verifier.go:85-94,626-638): one warp per
+// target.  Lanes 0..7 run the target on the eight test vectors (same opcode
+// in every lane), the outputs are broadcast with shuffles, then the warp
+// scans the candidate table 32 candidates at a time.  Candidate outputs are
+// precomputed once (k_pool_outputs), so a check is a compare of vector 0
+// (one 16-byte shared-memory load) and, on the rare match, of vectors 1..7.
+// __ballot_sync turns the per-lane verdicts into ordered survivor slots.
+//
+// Tier 2, MidCheck (verifier.go:98-123): one warp per pair, lane v runs both
+// sequences on MidCheck vector v, __all_sync decides.
+//
+// Tier 3, ExhaustiveCheck (verifier.go:159-612,642-853): the sweep of a pair
+// is cut into chunks of "A-blocks" (the 256 values of A for one carry and
+// one assignment of the swept registers).  A persistent grid pulls chunks
+// from an atomic dispenser; within a chunk the 32 lanes take 32 consecutive
+// A values, so every lane executes the same opcode and the swept registers
+// are warp-uniform.  A mismatch sets the pair's rejected flag, which the
+// other chunks of the pair poll to stop early.  The reference's sweep order
+// only matters for its early exit; the verdict (all states equal) does not
+// depend on it.
+#include <cuda_runtime.h>
+
+#include "z80b_kernels.cuh"
+
+namespace z80b {
+
+namespace {
+constexpr unsigned kFull = 0xFFFFFFFFu;
+constexpr uint32_t kResolved = 0x80000000u;
+constexpr int kBlock = 256;
+
+__constant__ OpInfo c_ops[kNumOps];
+__constant__ uint32_t c_vec[32][3];  // MidCheck vectors; the first 8 are the QuickCheck vectors
+__constant__ uint8_t c_rep[32];
+__constant__ uint16_t c_repsp[16];
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Runs n instructions held one per lane (lane first+i holds instruction i).
+// Every lane of the warp must call this with the same n.
+__device__ __forceinline__ void run_lanes(Z80S& s, uint32_t lane_word, int first, int n) {
+#pragma unroll 1
+  for (int i = 0; i < n; i++) {
+    uint32_t w = __shfl_sync(kFull, lane_word, first + i);
+    z_step(s, w & 0xFFFFu, w >> 16);
+  }
+}
+
+__device__ __forceinline__ Z80S vec_state(int v) {
+  return z_unpack(c_vec[v][0], c_vec[v][1], c_vec[v][2]);
+}
+
+// Byte masks of compared registers from keepR bits (B,C,D,E,H,L).
+struct Keep {
+  uint32_t f, b, c, d, e, h, l, sp, m;
+};
+__device__ __forceinline__ Keep make_keep(uint32_t keepF, uint32_t keepR, bool cmpM) {
+  Keep k;
+  k.f = keepF & 0xFFu;
+  k.b = (keepR & 1u) ? 0xFFu : 0u;
+  k.c = (keepR & 2u) ? 0xFFu : 0u;
+  k.d = (keepR & 4u) ? 0xFFu : 0u;
+  k.e = (keepR & 8u) ? 0xFFu : 0u;
+  k.h = (keepR & 16u) ? 0xFFu : 0u;
+  k.l = (keepR & 32u) ? 0xFFu : 0u;
+  k.sp = 0xFFFFu;
+  k.m = cmpM ? 0xFFu : 0u;
+  return k;
+}
+__device__ __forceinline__ bool eq_keep(const Z80S& x, const Z80S& y, const Keep& k) {
+  uint32_t d = (x.a ^ y.a) | ((x.f ^ y.f) & k.f) | ((x.b ^ y.b) & k.b) | ((x.c ^ y.c) & k.c) |
+               ((x.d ^ y.d) & k.d) | ((x.e ^ y.e) & k.e) | ((x.h ^ y.h) & k.h) | ((x.l ^ y.l) & k.l) |
+               ((x.sp ^ y.sp) & k.sp) | ((x.m ^ y.m) & k.m);
+  return d == 0;
+}
+// Registers (B,C,D,E,H,L -> bit 0..5) differing between packed words.
+__device__ __forceinline__ uint32_t reg_diff(uint32_t d0, uint32_t d1) {
+  return ((d0 >> 16) & 0xFFu ? 1u : 0u) | ((d0 >> 24) ? 2u : 0u) | ((d1 & 0xFFu) ? 4u : 0u) |
+         ((d1 >> 8) & 0xFFu ? 8u : 0u) | ((d1 >> 16) & 0xFFu ? 16u : 0u) | ((d1 >> 24) ? 32u : 0u);
+}
+
+// Number of A-blocks of the ExhaustiveCheck sweep for a read mask
+// (verifier.go:159-171,428-476).
+__device__ __forceinline__ unsigned long long sweep_blocks(uint32_t reads) {
+  uint32_t ext = reads & (kRegB | kRegC | kRegD | kRegE | kRegH | kRegL | kRegM);
+  int n = __popc(ext);
+  bool sp = (reads & kRegSP) != 0;
+  if (n == 0 && !sp) return 2ull;
+  if (n <= 2 && !sp) return 2ull << (8 * n);
+  return (2ull << (5 * n)) * (sp ? 16ull : 1ull);
+}
+constexpr unsigned long long kChunkBlocks = 32;  // 8192 states
+constexpr unsigned long long kMaxChunks = 65536;
+__device__ __forceinline__ unsigned long long chunks_for(unsigned long long nb) {
+  unsigned long long c = (nb + kChunkBlocks - 1) / kChunkBlocks;
+  return c > kMaxChunks ? kMaxChunks : c;
+}
+
+// ------------------------------------------------------------------ kernels
+
+__global__ void k_pool_outputs(const uint32_t* __restrict__ insn, uint32_t n, uint32_t len,
+                               uint4* __restrict__ qc, uint4* __restrict__ mid) {
+  uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  uint32_t prog[kMaxSeq];
+  for (uint32_t i = 0; i < kMaxSeq; i++) prog[i] = i < len ? insn[(size_t)c * len + i] : 0u;
+  const int nv = mid ? 32 : 8;
+  for (int v = 0; v < nv; v++) {
+    Z80S s = vec_state(v);
+    for (uint32_t i = 0; i < len; i++) z_step(s, prog[i] & 0xFFFFu, prog[i] >> 16);
+    uint32_t w[3];
+    z_pack(s, w);
+    uint4 q = make_uint4(w[0], w[1], w[2], 0u);
+    if (v < 8) qc[(size_t)v * n + c] = q;
+    if (mid) mid[(size_t)v * n + c] = q;
+  }
+}
+
+__global__ void k_exec(const uint32_t* __restrict__ in, const uint32_t* __restrict__ seqs,
+                       const uint8_t* __restrict__ lens, uint32_t len, uint32_t stride, uint32_t n,
+                       uint32_t* __restrict__ out) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Z80S s = z_unpack(in[3 * i], in[3 * i + 1], in[3 * i + 2]);
+  uint32_t l = lens ? lens[i] : len;
+  for (uint32_t k = 0; k < l && k < kMaxSeq; k++) {
+    uint32_t w = seqs[(size_t)i * stride + k];
+    z_step(s, w & 0xFFFFu, w >> 16);
+  }
+  uint32_t w[3];
+  z_pack(s, w);
+  out[3 * i] = w[0];
+  out[3 * i + 1] = w[1];
+  out[3 * i + 2] = w[2];
+}
+
+// search.Fingerprint: 8 x {A,F,B,C,D,E,H,L,SP_hi,SP_lo}.
+__global__ void k_fingerprints(const uint32_t* __restrict__ seqs, uint32_t n, uint32_t len,
+                               uint8_t* __restrict__ out) {
+  uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t i = gid >> 3, v = gid & 7u;
+  if (i >= n) return;
+  Z80S s = vec_state(int(v));
+  for (uint32_t k = 0; k < len; k++) {
+    uint32_t w = seqs[(size_t)i * len + k];
+    z_step(s, w & 0xFFFFu, w >> 16);
+  }
+  uint8_t* p = out + (size_t)i * 80 + v * 10;
+  p[0] = uint8_t(s.a); p[1] = uint8_t(s.f); p[2] = uint8_t(s.b); p[3] = uint8_t(s.c);
+  p[4] = uint8_t(s.d); p[5] = uint8_t(s.e); p[6] = uint8_t(s.h); p[7] = uint8_t(s.l);
+  p[8] = uint8_t(s.sp >> 8); p[9] = uint8_t(s.sp);
+}
+
+// z80qc query semantics (cuda/z80_quickcheck.cu:666-681 over pkg/cpu
+// outputs): candidate c matches when its fingerprint equals the query with
+// the dead flag bits cleared in every F byte.
+__global__ void k_fp_query(DevPool P, const uint32_t* __restrict__ fp, uint32_t dead,
+                           uint32_t* __restrict__ hits, uint32_t* __restrict__ nhits, uint32_t cap) {
+  uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  bool hit = false;
+  if (c < P.n) {
+    uint32_t keep0 = ~(dead << 8);
+    hit = true;
+#pragma unroll
+    for (int v = 0; v < 8; v++) {
+      uint4 q = P.qc[(size_t)v * P.n + c];
+      uint32_t d0 = (q.x ^ fp[3 * v]) & keep0, d1 = q.y ^ fp[3 * v + 1], d2 = (q.z ^ fp[3 * v + 2]) & 0xFFFFu;
+      hit = hit && ((d0 | d1 | d2) == 0);
+    }
+  }
+  unsigned b = __ballot_sync(kFull, hit);
+  if (b) {
+    uint32_t base = 0;
+    if (lane_id() == 0) base = atomicAdd(nhits, (uint32_t)__popc(b));
+    base = __shfl_sync(kFull, base, 0);
+    uint32_t idx = base + __popc(b & lanemask_lt());
+    if (hit && idx < cap) hits[idx] = c;
+  }
+}
+
+template <bool COLLECT>
+__global__ void __launch_bounds__(kBlock) k_qc_scan(DevTargets T, DevPool P, QCConfig cfg, QCOut o) {
+  extern __shared__ uint4 smem[];
+  uint4* s_q0 = smem;
+  uint8_t* s_el = reinterpret_cast<uint8_t*>(smem + (cfg.use_smem ? P.n : 0));
+  if (cfg.use_smem) {
+    for (uint32_t i = threadIdx.x; i < P.n; i += blockDim.x) {
+      s_q0[i] = P.qc[i];
+      s_el[i] = uint8_t(P.size[i] | (P.prune[i] ? 0x80u : 0u));
+    }
+    __syncthreads();
+  }
+  const unsigned lane = lane_id();
+  const uint32_t warps_per_block = blockDim.x >> 5;
+  const uint32_t gw = blockIdx.x * warps_per_block + (threadIdx.x >> 5);
+  const uint32_t nw = gridDim.x * warps_per_block;
+  unsigned long long my_checks = 0;
+
+  for (uint32_t t = gw; t < T.n; t += nw) {
+    uint32_t nf_total = 0, obase = 0;
+    if (COLLECT) {
+      nf_total = o.cnt_f[t];
+      if (nf_total + o.cnt_m[t] == 0) continue;
+      obase = o.base[t];
+    }
+    const uint32_t tl = target_len(T, t);
+    const uint32_t pw = lane < tl ? T.insn[(size_t)t * T.stride + lane] : 0u;
+    uint32_t sz = 0, ts = 0, rd = 0;
+    if (lane < tl) {
+      const OpInfo& oi = c_ops[pw & 0xFFFFu];
+      sz = oi.size;
+      ts = oi.tstates;
+      rd = oi.reads;
+    }
+#pragma unroll
+    for (int off = 2; off >= 1; off >>= 1) {
+      sz += __shfl_down_sync(kFull, sz, off);
+      ts += __shfl_down_sync(kFull, ts, off);
+      rd |= __shfl_down_sync(kFull, rd, off);
+    }
+    const uint32_t tb = __shfl_sync(kFull, sz, 0);
+    const uint32_t tts = __shfl_sync(kFull, ts, 0);
+    const uint32_t trd = __shfl_sync(kFull, rd, 0);
+
+    Z80S s = vec_state(int(lane & 7u));
+    run_lanes(s, pw, 0, int(tl));
+    uint32_t w[3];
+    z_pack(s, w);
+    uint32_t tw[8][3];
+#pragma unroll
+    for (int v = 0; v < 8; v++) {
+      tw[v][0] = __shfl_sync(kFull, w[0], v);
+      tw[v][1] = __shfl_sync(kFull, w[1], v);
+      tw[v][2] = __shfl_sync(kFull, w[2], v);
+    }
+    const uint32_t dead = target_dead(T, t) & 0xFFu;
+    const uint32_t dregs = target_dead_regs(T, t) & 0x3Fu;
+    const uint32_t keep0 = 0xFFu | ((~dead & 0xFFu) << 8) | ((dregs & 1u) ? 0u : 0xFF0000u) |
+                           ((dregs & 2u) ? 0u : 0xFF000000u);
+    const uint32_t keep1 = ((dregs & 4u) ? 0u : 0xFFu) | ((dregs & 8u) ? 0u : 0xFF00u) |
+                           ((dregs & 16u) ? 0u : 0xFF0000u) | ((dregs & 32u) ? 0u : 0xFF000000u);
+    const uint32_t keep2 = cfg.w2mask;
+
+    uint32_t nf = 0, nm = 0;
+    for (uint32_t base = 0; base < P.n; base += 32) {
+      const uint32_t c = base + lane;
+      bool el = false;
+      if (c < P.n) {
+        uint32_t e = cfg.use_smem ? s_el[c] : (P.size[c] | (P.prune[c] ? 0x80u : 0u));
+        el = (e & 0x7Fu) < tb && !(e & 0x80u);
+      }
+      bool fp = false, mp = false;
+      uint32_t diff = 0;
+      if (el) {
+        uint4 q = cfg.use_smem ? s_q0[c] : P.qc[c];
+        uint32_t d0 = q.x ^ tw[0][0], d1 = q.y ^ tw[0][1], d2 = q.z ^ tw[0][2];
+        if (((d0 & keep0) | (d1 & keep1) | (d2 & keep2)) == 0) {
+          bool full = (d0 | d1 | (d2 & keep2)) == 0;
+          uint32_t fd = (d0 >> 8) & 0xFFu, rdf = reg_diff(d0, d1);
+          bool ok = true;
+#pragma unroll
+          for (int v = 1; v < 8; v++) {
+            uint4 qv = P.qc[(size_t)v * P.n + c];
+            uint32_t e0 = qv.x ^ tw[v][0], e1 = qv.y ^ tw[v][1], e2 = qv.z ^ tw[v][2];
+            ok = ok && (((e0 & keep0) | (e1 & keep1) | (e2 & keep2)) == 0);
+            full = full && ((e0 | e1 | (e2 & keep2)) == 0);
+            fd |= (e0 >> 8) & 0xFFu;
+            rdf |= reg_diff(e0, e1);
+          }
+          if (ok) {
+            if (cfg.all_hits) {
+              fp = true;
+            } else {
+              fp = full;
+              mp = !full;
+            }
+            diff = fd | (rdf << 8);
+          }
+        }
+      }
+      if (!COLLECT) {
+        const unsigned be = __ballot_sync(kFull, el);
+        if (lane == 0) my_checks += __popc(be);
+      }
+      const unsigned bf = __ballot_sync(kFull, fp);
+      const unsigned bm = __ballot_sync(kFull, mp);
+      if (COLLECT) {
+        if (fp) {
+          uint32_t idx = obase + nf + __popc(bf & lanemask_lt());
+          o.surv[idx] = c;
+          o.sdiff[idx] = uint16_t(diff);
+        }
+        if (mp) {
+          uint32_t idx = obase + nf_total + nm + __popc(bm & lanemask_lt());
+          o.surv[idx] = c;
+          o.sdiff[idx] = uint16_t(diff);
+        }
+      }
+      nf += __popc(bf);
+      nm += __popc(bm);
+    }
+    if (!COLLECT && lane == 0) {
+      o.cnt_f[t] = nf;
+      o.cnt_m[t] = nm;
+      o.cnt_all[t] = nf + nm;
+      TargetMeta m;
+      m.tstates = uint16_t(tts);
+      m.bytes = uint8_t(tb);
+      m.len = uint8_t(tl);
+      m.reads = uint16_t(trd);
+      m.pad = 0;
+      o.meta[t] = m;
+    }
+  }
+  if (!COLLECT && lane == 0 && my_checks) atomicAdd(o.checks, my_checks);
+}
+
+// Appends one pair per unresolved (target, kind) lane with an untried survivor.
+__global__ void k_round_build(DevTargets T, DevPool P, QCOut q, Lanes L, RoundBuf R) {
+  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  bool have[2] = {false, false};
+  PairRec pr[2];
+  uint32_t src[2] = {0, 0};
+  if (t < T.n) {
+    const uint32_t cf = q.cnt_f[t], cm = q.cnt_m[t];
+#pragma unroll
+    for (int kind = 0; kind < 2; kind++) {
+      const uint32_t idx = 2 * t + kind;
+      uint32_t nx = L.next[idx];
+      if (nx & kResolved) continue;
+      const uint32_t cnt = kind ? cm : cf;
+      if (nx >= cnt) {
+        L.next[idx] = nx | kResolved;
+        continue;
+      }
+      const uint32_t sidx = q.base[t] + (kind ? cf : 0u) + nx;
+      const uint32_t c = q.surv[sidx];
+      const uint32_t reads = q.meta[t].reads | P.reads[c];
+      pr[kind].target = t;
+      pr[kind].cand = c;
+      pr[kind].reads = uint16_t(reads);
+      pr[kind].nblocks = sweep_blocks(reads);
+      pr[kind].keepF = kind ? uint8_t(~target_dead(T, t)) : uint8_t(0xFFu);
+      pr[kind].keepR = kind ? uint8_t((~target_dead_regs(T, t) & 0x3Fu) | 0x80u) : uint8_t(0x3Fu);
+      src[kind] = sidx;
+      have[kind] = true;
+    }
+  }
+#pragma unroll
+  for (int kind = 0; kind < 2; kind++) {
+    unsigned b = __ballot_sync(kFull, have[kind]);
+    if (!b) continue;
+    uint32_t base = 0;
+    if (lane_id() == 0) base = atomicAdd(R.npairs, (uint32_t)__popc(b));
+    base = __shfl_sync(kFull, base, 0);
+    if (have[kind]) {
+      uint32_t p = base + __popc(b & lanemask_lt());
+      R.pairs[p] = pr[kind];
+      R.pair_src[p] = src[kind];
+      R.nchunks[p] = chunks_for(pr[kind].nblocks);
+      R.rejected[p] = 0;
+    }
+  }
+}
+
+// pkg/gpu semantics: one pair per MidCheck survivor (all survivors when
+// midpass is null).
+__global__ void k_pairs_from_survivors(DevTargets T, DevPool P, QCOut q, const uint8_t* __restrict__ midpass,
+                                       uint32_t nsurv, const uint32_t* __restrict__ surv_target,
+                                       RoundBuf R) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool have = false;
+  PairRec pr;
+  if (i < nsurv && (!midpass || midpass[i])) {
+    const uint32_t t = surv_target[i], c = q.surv[i];
+    const uint32_t reads = q.meta[t].reads | P.reads[c];
+    pr.target = t;
+    pr.cand = c;
+    pr.reads = uint16_t(reads);
+    pr.nblocks = sweep_blocks(reads);
+    pr.keepF = uint8_t(~target_dead(T, t));
+    pr.keepR = uint8_t(~target_dead_regs(T, t) & 0x3Fu);
+    have = true;
+  }
+  unsigned b = __ballot_sync(kFull, have);
+  if (!b) return;
+  uint32_t base = 0;
+  if (lane_id() == 0) base = atomicAdd(R.npairs, (uint32_t)__popc(b));
+  base = __shfl_sync(kFull, base, 0);
+  if (have) {
+    uint32_t p = base + __popc(b & lanemask_lt());
+    R.pairs[p] = pr;
+    R.pair_src[p] = i;
+    R.nchunks[p] = chunks_for(pr.nblocks);
+    R.rejected[p] = 0;
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_exhaustive(DevTargets T, DevPool P, RoundBuf R, uint32_t npairs,
+                                                       unsigned long long total) {
+  const unsigned lane = lane_id();
+  unsigned long long my_states = 0;
+  for (;;) {
+    unsigned long long k = 0;
+    if (lane == 0) k = atomicAdd(R.counter, 1ull);
+    k = __shfl_sync(kFull, k, 0);
+    if (k >= total) break;
+    // pair p: cbase[p] <= k < cbase[p + 1]
+    uint32_t lo = 0, hi = npairs - 1;
+    while (lo < hi) {
+      uint32_t mid = (lo + hi + 1) >> 1;
+      if (R.cbase[mid] <= k) lo = mid;
+      else hi = mid - 1;
+    }
+    const uint32_t p = lo;
+    if (*reinterpret_cast<volatile uint32_t*>(&R.rejected[p])) continue;
+    const PairRec pr = R.pairs[p];
+    const unsigned long long nch = (p + 1 < npairs ? R.cbase[p + 1] : total) - R.cbase[p];
+    const unsigned long long bpc = (pr.nblocks + nch - 1) / nch;
+    const unsigned long long j = k - R.cbase[p];
+    const unsigned long long b0 = j * bpc;
+    unsigned long long b1 = b0 + bpc;
+    if (b1 > pr.nblocks) b1 = pr.nblocks;
+
+    // programs: lanes 0..tl-1 target, tl..tl+cl-1 candidate
+    const uint32_t tl = target_len(T, pr.target), cl = pool_len(P, pr.cand);
+    uint32_t pw = 0;
+    if (lane < tl) pw = T.insn[(size_t)pr.target * T.stride + lane];
+    else if (lane < tl + cl) pw = P.insn[(size_t)pr.cand * P.stride + (lane - tl)];
+
+    // sweep shape (verifier.go:428-476): extra registers in B,C,D,E,H,L,M order
+    const uint32_t ext = pr.reads & (kRegB | kRegC | kRegD | kRegE | kRegH | kRegL | kRegM);
+    const int nx = __popc(ext);
+    const bool spw = (pr.reads & kRegSP) != 0;
+    const bool reduced = spw || nx > 2;
+    const int fw = reduced ? 5 : 8;  // bits per swept register in the block index
+    // slot of each register (-1 = not swept)
+    int slot[7];
+    {
+      int k2 = 0;
+      const uint32_t bits[7] = {kRegB, kRegC, kRegD, kRegE, kRegH, kRegL, kRegM};
+#pragma unroll
+      for (int r = 0; r < 7; r++) slot[r] = (ext & bits[r]) ? k2++ : -1;
+    }
+    const Keep keep = make_keep(pr.keepF, pr.keepR, true);
+
+    bool bad = false;
+    for (unsigned long long ab = b0; ab < b1; ab++) {
+      const uint32_t carry = uint32_t(ab & 1ull);
+      const unsigned long long rest = ab >> 1;
+      uint32_t rv[7];
+#pragma unroll
+      for (int r = 0; r < 7; r++) {
+        if (slot[r] < 0) {
+          rv[r] = 0;
+        } else {
+          uint32_t f = uint32_t(rest >> (fw * slot[r]));
+          rv[r] = reduced ? c_rep[f & 31u] : (f & 0xFFu);
+        }
+      }
+      const uint32_t sp = spw ? c_repsp[uint32_t(rest >> (5 * nx)) & 15u] : 0u;
+#pragma unroll 1
+      for (uint32_t i = 0; i < 8; i++) {
+        Z80S x;
+        x.a = i * 32u + lane;
+        x.f = carry;
+        x.b = rv[0]; x.c = rv[1]; x.d = rv[2]; x.e = rv[3]; x.h = rv[4]; x.l = rv[5]; x.m = rv[6];
+        x.sp = sp;
+        Z80S y = x;
+        run_lanes(x, pw, 0, int(tl));
+        run_lanes(y, pw, int(tl), int(cl));
+        bad = bad || !eq_keep(x, y, keep);
+      }
+      my_states += 256;
+      if (__any_sync(kFull, bad)) break;
+      if ((ab & 15ull) == 15ull && *reinterpret_cast<volatile uint32_t*>(&R.rejected[p])) break;
+    }
+    if (__any_sync(kFull, bad) && lane == 0) atomicExch(&R.rejected[p], 1u);
+  }
+  if (lane == 0 && my_states) atomicAdd(R.states, my_states);
+}
+
+__global__ void k_round_resolve(RoundBuf R, uint32_t npairs, QCOut q, Lanes L) {
+  uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npairs) return;
+  const PairRec pr = R.pairs[p];
+  const uint32_t idx = 2 * pr.target + ((pr.keepR & 0x80u) ? 1u : 0u);
+  if (R.rejected[p] == 0) {
+    L.win[idx] = pr.cand;
+    L.windiff[idx] = q.sdiff[R.pair_src[p]];
+    L.next[idx] |= kResolved;
+  } else {
+    L.next[idx] += 1;
+  }
+}
+
+__global__ void k_midcheck(DevTargets T, DevPool P, const uint32_t* __restrict__ surv,
+                           const uint32_t* __restrict__ surv_target, uint32_t nsurv, uint8_t* __restrict__ pass) {
+  const unsigned lane = lane_id();
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t i = gw; i < nsurv; i += nw) {
+    const uint32_t t = surv_target[i], c = surv[i];
+    const uint32_t tl = target_len(T, t), cl = pool_len(P, c);
+    uint32_t pw = 0;
+    if (lane < tl) pw = T.insn[(size_t)t * T.stride + lane];
+    else if (lane < tl + cl) pw = P.insn[(size_t)c * P.stride + (lane - tl)];
+    Z80S x = vec_state(int(lane)), y = x;
+    run_lanes(x, pw, 0, int(tl));
+    run_lanes(y, pw, int(tl), int(cl));
+    const Keep keep = make_keep(~target_dead(T, t), ~target_dead_regs(T, t) & 0x3Fu, true);
+    bool ok = __all_sync(kFull, eq_keep(x, y, keep));
+    if (lane == 0) pass[i] = ok ? 1 : 0;
+  }
+}
+
+__global__ void k_surv_targets(QCOut q, uint32_t n, uint32_t* __restrict__ st) {
+  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  uint32_t b = q.base[t], c = q.cnt_f[t] + q.cnt_m[t];
+  for (uint32_t j = 0; j < c; j++) st[b + j] = t;
+}
+
+__global__ void k_rule_count_first(Lanes L, uint32_t n, uint32_t* __restrict__ cnt, DevTargets T,
+                                   unsigned long long* checked, uint32_t pool_enum) {
+  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long ch = 0;
+  if (t < n) {
+    uint32_t wf = L.win[2 * t], wm = L.win[2 * t + 1];
+    cnt[t] = (wf != kNone ? 1u : 0u) + (wm != kNone ? 1u : 0u);
+    // worker.go:134 counts every enumerated candidate up to and including
+    // the winner (the pool index is the enumeration ordinal)
+    ch = (wf != kNone) ? (unsigned long long)wf + 1ull : pool_enum;
+    if (target_dead(T, t) != 0 || target_dead_regs(T, t) != 0)
+      ch += (wm != kNone) ? (unsigned long long)wm + 1ull : pool_enum;
+  }
+  for (int off = 16; off; off >>= 1) ch += __shfl_down_sync(kFull, ch, off);
+  if (lane_id() == 0 && ch) atomicAdd(checked, ch);
+}
+
+__global__ void k_rule_write_first(Lanes L, uint32_t n, const uint32_t* __restrict__ base,
+                                   DevRule* __restrict__ out) {
+  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  uint32_t b = base[t];
+  for (int kind = 0; kind < 2; kind++) {
+    uint32_t w = L.win[2 * t + kind];
+    if (w == kNone) continue;
+    DevRule r;
+    r.target = t;
+    r.cand = w;
+    r.diff = kind ? L.windiff[2 * t + kind] : uint16_t(0);
+    r.kind = uint8_t(kind);
+    r.pad = 0;
+    out[b++] = r;
+  }
+}
+
+// All-hits: flag[i] = 1 when survivor i passed MidCheck and ExhaustiveCheck.
+__global__ void k_rule_count_all(RoundBuf R, uint32_t npairs, uint32_t* __restrict__ flag) {
+  uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npairs) return;
+  if (R.rejected[p] == 0) flag[R.pair_src[p]] = 1u;
+}
+
+__global__ void k_rule_write_all(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ base,
+                                 uint32_t nsurv, const uint32_t* __restrict__ surv,
+                                 const uint16_t* __restrict__ sdiff, const uint32_t* __restrict__ surv_target,
+                                 DevRule* __restrict__ out) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nsurv || !flag[i]) return;
+  DevRule r;
+  r.target = surv_target[i];
+  r.cand = surv[i];
+  r.diff = sdiff[i];
+  r.kind = 2;
+  r.pad = 0;
+  out[base[i]] = r;
+}
+
+// Verifier tiers for explicit pairs (QuickCheck, MidCheck, FlagDiff); warp
+// per pair, lane v = vector v.
+__global__ void k_verify_small(const uint32_t* __restrict__ tgt, const uint8_t* __restrict__ tlens,
+                               const uint32_t* __restrict__ cand, const uint8_t* __restrict__ clens,
+                               uint32_t stride, uint32_t n, const uint8_t* __restrict__ dead,
+                               uint32_t tiers, uint8_t* __restrict__ out, uint8_t* __restrict__ flagdiff) {
+  const unsigned lane = lane_id();
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t i = gw; i < n; i += nw) {
+    const uint32_t tl = tlens[i], cl = clens[i];
+    uint32_t pw = 0;
+    if (lane < tl) pw = tgt[(size_t)i * stride + lane];
+    else if (lane < tl + cl) pw = cand[(size_t)i * stride + (lane - tl)];
+    Z80S x = vec_state(int(lane)), y = x;
+    run_lanes(x, pw, 0, int(tl));
+    run_lanes(y, pw, int(tl), int(cl));
+    const uint32_t dm = dead ? dead[i] : 0u;
+    const Keep keep = make_keep(~dm, 0x3Fu, true);
+    const bool eq = eq_keep(x, y, keep);
+    // FlagDiff (verifier.go:658-673) over the 8 QuickCheck vectors
+    const bool regs_eq = (x.a == y.a) && (x.b == y.b) && (x.c == y.c) && (x.d == y.d) &&
+                         (x.e == y.e) && (x.h == y.h) && (x.l == y.l) && (x.sp == y.sp) && (x.m == y.m);
+    const unsigned q8 = __ballot_sync(kFull, eq) & 0xFFu;
+    const unsigned all32 = __ballot_sync(kFull, eq);
+    const unsigned r8 = __ballot_sync(kFull, regs_eq) & 0xFFu;
+    uint32_t fx = lane < 8 ? (x.f ^ y.f) : 0u;
+    for (int off = 16; off; off >>= 1) fx |= __shfl_down_sync(kFull, fx, off);
+    if (lane == 0) {
+      uint8_t r = 0;
+      if ((tiers & 1u) && q8 == 0xFFu) r |= 1;
+      if ((tiers & 2u) && all32 == kFull) r |= 2;
+      out[i] = r;
+      if (flagdiff) flagdiff[i] = (r8 == 0xFFu) ? uint8_t(fx) : uint8_t(0);
+    }
+  }
+}
+
+unsigned grid_for(uint32_t n, unsigned block) { return (n + block - 1) / block; }
+
+int g_num_sms = 0;
+
+}  // namespace
+
+int dev_num_sms() {
+  if (!g_num_sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_num_sms <= 0) g_num_sms = 1;
+  }
+  return g_num_sms;
+}
+
+}  // namespace z80b
+
+// Host helpers that need the tables (kept out of the anonymous namespace).
+#include "z80_tables.h"
+
+namespace z80b {
+
+void dev_upload_tables(cudaStream_t s) {
+  cudaMemcpyToSymbolAsync(c_ops, op_table(), sizeof(OpInfo) * kNumOps, 0, cudaMemcpyHostToDevice, s);
+  cudaMemcpyToSymbolAsync(c_vec, mid_vectors(), sizeof(uint32_t) * 32 * 3, 0, cudaMemcpyHostToDevice, s);
+  cudaMemcpyToSymbolAsync(c_rep, rep_values(), 32, 0, cudaMemcpyHostToDevice, s);
+  cudaMemcpyToSymbolAsync(c_repsp, rep_sp(), 32, 0, cudaMemcpyHostToDevice, s);
+}
+
+void launch_pool_outputs(const uint32_t* insn, uint32_t n, uint32_t len, uint4* qc, uint4* mid,
+                         cudaStream_t s) {
+  if (!n) return;
+  k_pool_outputs<<<grid_for(n, 128), 128, 0, s>>>(insn, n, len, qc, mid);
+}
+void launch_exec(const uint32_t* in, const uint32_t* seqs, const uint8_t* lens, uint32_t len,
+                 uint32_t stride, uint32_t n, uint32_t* out, cudaStream_t s) {
+  if (!n) return;
+  k_exec<<<grid_for(n, 128), 128, 0, s>>>(in, seqs, lens, len, stride, n, out);
+}
+void launch_fingerprints(const uint32_t* seqs, uint32_t n, uint32_t len, uint8_t* out, cudaStream_t s) {
+  if (!n) return;
+  k_fingerprints<<<grid_for(n * 8, 256), 256, 0, s>>>(seqs, n, len, out);
+}
+void launch_fp_query(const DevPool& P, const uint32_t* fp, uint32_t dead, uint32_t* hits,
+                     uint32_t* nhits, uint32_t cap, cudaStream_t s) {
+  if (!P.n) return;
+  k_fp_query<<<grid_for(P.n, 256), 256, 0, s>>>(P, fp, dead, hits, nhits, cap);
+}
+void launch_qc_scan(const DevTargets& T, const DevPool& P, const QCConfig& cfg, const QCOut& o,
+                    bool collect, cudaStream_t s) {
+  if (!T.n) return;
+  size_t smem = cfg.use_smem ? (size_t)P.n * 17 + 16 : 0;
+  static bool attr_done = false;
+  if (!attr_done) {
+    cudaFuncSetAttribute(k_qc_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(k_qc_scan<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_done = true;
+  }
+  int per_sm = 0;
+  if (collect)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_qc_scan<true>, kBlock, smem);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_qc_scan<false>, kBlock, smem);
+  if (per_sm < 1) per_sm = 1;
+  unsigned need = grid_for(T.n, kBlock / 32);
+  unsigned grid = unsigned(dev_num_sms() * per_sm);
+  if (grid > need) grid = need;
+  if (collect) k_qc_scan<true><<<grid, kBlock, smem, s>>>(T, P, cfg, o);
+  else k_qc_scan<false><<<grid, kBlock, smem, s>>>(T, P, cfg, o);
+}
+void launch_round_build(const DevTargets& T, const DevPool& P, const QCOut& q, const Lanes& L,
+                        const RoundBuf& R, cudaStream_t s) {
+  if (!T.n) return;
+  k_round_build<<<grid_for(T.n, 256), 256, 0, s>>>(T, P, q, L, R);
+}
+void launch_pairs_from_survivors(const DevTargets& T, const DevPool& P, const QCOut& q,
+                                 const uint8_t* midpass, uint32_t nsurv, const uint32_t* surv_target,
+                                 const RoundBuf& R, cudaStream_t s) {
+  if (!nsurv) return;
+  k_pairs_from_survivors<<<grid_for(nsurv, 256), 256, 0, s>>>(T, P, q, midpass, nsurv, surv_target, R);
+}
+void launch_exhaustive(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
+                       unsigned long long total, cudaStream_t s) {
+  if (!npairs || !total) return;
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_exhaustive, kBlock, 0);
+  if (per_sm < 1) per_sm = 1;
+  unsigned long long need = (total + (kBlock / 32) - 1) / (kBlock / 32);
+  unsigned long long grid = (unsigned long long)dev_num_sms() * per_sm;
+  if (grid > need) grid = need;
+  k_exhaustive<<<unsigned(grid), kBlock, 0, s>>>(T, P, R, npairs, total);
+}
+void launch_round_resolve(const RoundBuf& R, uint32_t npairs, const QCOut& q, const Lanes& L,
+                          cudaStream_t s) {
+  if (!npairs) return;
+  k_round_resolve<<<grid_for(npairs, 256), 256, 0, s>>>(R, npairs, q, L);
+}
+void launch_midcheck(const DevTargets& T, const DevPool& P, const uint32_t* surv,
+                     const uint32_t* surv_target, uint32_t nsurv, uint8_t* pass, cudaStream_t s) {
+  if (!nsurv) return;
+  unsigned long long need = (unsigned long long)nsurv * 32;
+  unsigned grid = unsigned(need / 256 + 1);
+  unsigned cap = unsigned(dev_num_sms() * 8);
+  if (grid > cap) grid = cap;
+  k_midcheck<<<grid, 256, 0, s>>>(T, P, surv, surv_target, nsurv, pass);
+}
+void launch_surv_targets(const QCOut& q, uint32_t n, uint32_t* st, cudaStream_t s) {
+  if (!n) return;
+  k_surv_targets<<<grid_for(n, 256), 256, 0, s>>>(q, n, st);
+}
+void launch_rule_count_first(const Lanes& L, uint32_t n, uint32_t* cnt, const DevTargets& T,
+                             unsigned long long* checked, uint32_t pool_enum, cudaStream_t s) {
+  if (!n) return;
+  k_rule_count_first<<<grid_for(n, 256), 256, 0, s>>>(L, n, cnt, T, checked, pool_enum);
+}
+void launch_rule_write_first(const Lanes& L, uint32_t n, const uint32_t* base, DevRule* out,
+                             cudaStream_t s) {
+  if (!n) return;
+  k_rule_write_first<<<grid_for(n, 256), 256, 0, s>>>(L, n, base, out);
+}
+void launch_rule_count_all(const RoundBuf& R, uint32_t npairs, uint32_t* flag, cudaStream_t s) {
+  if (!npairs) return;
+  k_rule_count_all<<<grid_for(npairs, 256), 256, 0, s>>>(R, npairs, flag);
+}
+void launch_rule_write_all(const uint32_t* flag, const uint32_t* base, uint32_t nsurv,
+                           const uint32_t* surv, const uint16_t* sdiff, const uint32_t* surv_target,
+                           DevRule* out, cudaStream_t s) {
+  if (!nsurv) return;
+  k_rule_write_all<<<grid_for(nsurv, 256), 256, 0, s>>>(flag, base, nsurv, surv, sdiff, surv_target, out);
+}
+void launch_verify_small(const uint32_t* tgt, const uint8_t* tlens, const uint32_t* cand,
+                         const uint8_t* clens, uint32_t stride, uint32_t n, const uint8_t* dead,
+                         uint32_t tiers, uint8_t* out, uint8_t* flagdiff, cudaStream_t s) {
+  if (!n) return;
+  unsigned grid = unsigned(((unsigned long long)n * 32 + 255) / 256);
+  unsigned cap = unsigned(dev_num_sms() * 8);
+  if (grid > cap) grid = cap;
+  k_verify_small<<<grid, 256, 0, s>>>(tgt, tlens, cand, clens, stride, n, dead, tiers, out, flagdiff);
+}
+
+}  // namespace z80b

@@ -1,0 +1,91 @@
+// z80b_kernels.cuh -- kernel declarations and launch parameters.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "z80b_device.cuh"
+
+namespace z80b {
+
+// Surviving (target, candidate) pairs of the QuickCheck scan.
+struct QCOut {
+  uint32_t* cnt_f;   // [n] full-equivalence survivors per target
+  uint32_t* cnt_m;   // [n] masked-only survivors per target
+  uint32_t* cnt_all; // [n] cnt_f + cnt_m (scan input)
+  const uint32_t* base;  // [n] exclusive prefix of cnt_f + cnt_m (collect pass)
+  uint32_t* surv;    // survivor pool indices
+  uint16_t* sdiff;   // FlagDiff (low byte) | differing registers << 8
+  TargetMeta* meta;  // [n]
+  unsigned long long* checks;  // eligible pairs evaluated (count pass)
+};
+
+struct QCConfig {
+  uint32_t w2mask;   // 0xFFFFFFFF: compare SP and M; 0x0000FFFF: fingerprint (SP only)
+  int all_hits;      // 1: pkg/gpu semantics (one list: masked-QC passes)
+  int use_smem;      // pool QC0 staged in shared memory
+};
+
+// Per-(target, kind) progress of the first-found rounds.
+struct Lanes {
+  uint32_t* next;    // [2n] survivor index to try next; bit31 = resolved
+  uint32_t* win;     // [2n] winning pool index or kNone
+  uint16_t* windiff; // [2n] sdiff of the winner
+};
+
+struct RoundBuf {
+  PairRec* pairs;
+  uint32_t* pair_src;              // index of the (target, kind) lane or survivor
+  unsigned long long* nchunks;     // per pair (scan input)
+  unsigned long long* cbase;       // exclusive prefix of nchunks
+  uint32_t* rejected;              // per pair
+  uint32_t* npairs;                // device counter
+  unsigned long long* counter;     // chunk dispenser
+  unsigned long long* states;      // states verified (stat)
+};
+
+struct DevRule {
+  uint32_t target;
+  uint32_t cand;
+  uint16_t diff;   // flag diff | reg diff << 8
+  uint8_t kind;    // 0 full, 1 masked, 2 all-hits
+  uint8_t pad;
+};
+
+void dev_upload_tables(cudaStream_t s);
+int dev_num_sms();
+
+void launch_pool_outputs(const uint32_t* insn, uint32_t n, uint32_t len, uint4* qc, uint4* mid,
+                         cudaStream_t s);
+void launch_exec(const uint32_t* in_states, const uint32_t* seqs, const uint8_t* lens, uint32_t len,
+                 uint32_t stride, uint32_t n, uint32_t* out_states, cudaStream_t s);
+void launch_fingerprints(const uint32_t* seqs, uint32_t n, uint32_t len, uint8_t* out, cudaStream_t s);
+void launch_qc_scan(const DevTargets& T, const DevPool& P, const QCConfig& cfg, const QCOut& o,
+                    bool collect, cudaStream_t s);
+void launch_fp_query(const DevPool& P, const uint32_t* fp3x8, uint32_t dead, uint32_t* hits,
+                     uint32_t* nhits, uint32_t cap, cudaStream_t s);
+void launch_round_build(const DevTargets& T, const DevPool& P, const QCOut& q, const Lanes& L,
+                        const RoundBuf& R, cudaStream_t s);
+void launch_pairs_from_survivors(const DevTargets& T, const DevPool& P, const QCOut& q,
+                                 const uint8_t* midpass, uint32_t nsurv, const uint32_t* surv_target,
+                                 const RoundBuf& R, cudaStream_t s);
+void launch_exhaustive(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
+                       unsigned long long total_chunks, cudaStream_t s);
+void launch_round_resolve(const RoundBuf& R, uint32_t npairs, const QCOut& q, const Lanes& L,
+                          cudaStream_t s);
+void launch_midcheck(const DevTargets& T, const DevPool& P, const uint32_t* surv,
+                     const uint32_t* surv_target, uint32_t nsurv, uint8_t* pass, cudaStream_t s);
+void launch_surv_targets(const QCOut& q, uint32_t n, uint32_t* surv_target, cudaStream_t s);
+void launch_rule_count_first(const Lanes& L, uint32_t n, uint32_t* cnt, const DevTargets& T,
+                             unsigned long long* checked, uint32_t pool_enum, cudaStream_t s);
+void launch_rule_write_first(const Lanes& L, uint32_t n, const uint32_t* base, DevRule* out,
+                             cudaStream_t s);
+void launch_rule_write_all(const uint32_t* flag, const uint32_t* base, uint32_t nsurv,
+                           const uint32_t* surv, const uint16_t* sdiff, const uint32_t* surv_target,
+                           DevRule* out, cudaStream_t s);
+void launch_rule_count_all(const RoundBuf& R, uint32_t npairs, uint32_t* flag, cudaStream_t s);
+void launch_verify_small(const uint32_t* tgt, const uint8_t* tlens, const uint32_t* cand,
+                         const uint8_t* clens, uint32_t stride, uint32_t n, const uint8_t* dead,
+                         uint32_t tiers, uint8_t* out, uint8_t* flagdiff, cudaStream_t s);
+
+}  // namespace z80b

@@ -1,0 +1,393 @@
+"""Python binding of libz80b200.so (the sm_100a candidate-verification path).
+
+Mirrors the reference's host interface for this path:
+  * ``Context.load_candidates`` / ``Context.quickcheck_gpu`` --
+    gpu.NewCUDAProcess / CUDAProcess.QuickCheckGPU (pkg/gpu/cuda.go:32-107)
+  * ``Context.fingerprints`` -- search.Fingerprint (pkg/search/verifier.go:134)
+  * ``Context.verify_pairs`` -- QuickCheck / MidCheck / ExhaustiveCheck
+    [Masked] and FlagDiff over pairs (pkg/search/verifier.go)
+  * ``Context.search`` -- search.Run worker semantics (mode "first",
+    pkg/search/worker.go:124-265) or gpu.SearchGPU semantics (mode "all",
+    pkg/gpu/search.go:80-199) over a batch of targets
+  * ``search_single`` / ``search_single_masked`` -- search.SearchSingle[Masked]
+    (pkg/search/search.go:82-110)
+  * ``write_json`` -- result.WriteJSON (pkg/result/output.go:70-90)
+
+Errors raise ``Z80BError`` with the library's status and message; the module
+never falls back to a CPU implementation.  Instructions are packed as
+``op | imm << 16`` (pkg/gpu/cuda.go:310).
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_build", "libz80b200.so")
+
+OK, EINVAL, ENOMEM, ECUDA, ETIMEOUT, ECAPACITY, ENODEV, ESTATE = range(8)
+MODE_FIRST, MODE_ALL = 0, 1
+PATH_BATCHED, PATH_PLAIN = 0, 1
+TIER_QC, TIER_MID, TIER_EXH = 1, 2, 4
+DEAD_NONE, DEAD_UNDOC, DEAD_ALL = 0x00, 0x28, 0xFF
+
+
+class Z80BError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"z80b status {status}: {msg}")
+        self.status = status
+
+
+class State(ctypes.Structure):
+    """cpu.State (pkg/cpu/state.go:11-15)."""
+    _fields_ = [(n, ctypes.c_uint8) for n in "afbcdehl"] + [
+        ("sp", ctypes.c_uint16), ("m", ctypes.c_uint8), ("pad", ctypes.c_uint8)]
+
+    def tup(self):
+        return (self.a, self.f, self.b, self.c, self.d, self.e, self.h, self.l, self.sp, self.m)
+
+
+class Rule(ctypes.Structure):
+    """result.Rule (pkg/result/table.go:11-17) + target index."""
+    _fields_ = [("src", ctypes.c_uint32 * 4), ("rep", ctypes.c_uint32 * 4),
+                ("src_len", ctypes.c_int32), ("rep_len", ctypes.c_int32),
+                ("bytes_saved", ctypes.c_int32), ("cycles_saved", ctypes.c_int32),
+                ("dead_flags", ctypes.c_int32), ("target_index", ctypes.c_int32),
+                ("dead_regs", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+    @property
+    def source(self):
+        return list(self.src[:self.src_len])
+
+    @property
+    def replacement(self):
+        return list(self.rep[:self.rep_len])
+
+    def key(self):
+        return (self.target_index, tuple(self.source), tuple(self.replacement),
+                self.bytes_saved, self.cycles_saved, self.dead_flags, self.dead_regs)
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("targets", ctypes.c_uint64), ("checks", ctypes.c_uint64),
+                ("checked_ref", ctypes.c_uint64), ("qc_survivors", ctypes.c_uint64),
+                ("mid_survivors", ctypes.c_uint64), ("exhaustive_pairs", ctypes.c_uint64),
+                ("exhaustive_states", ctypes.c_uint64), ("rules", ctypes.c_uint64),
+                ("rounds", ctypes.c_uint32), ("launches", ctypes.c_uint32),
+                ("device_ms", ctypes.c_double), ("qc_ms", ctypes.c_double),
+                ("exh_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Job(ctypes.Structure):
+    _fields_ = [("targets", ctypes.POINTER(ctypes.c_uint32)),
+                ("target_lens", ctypes.POINTER(ctypes.c_uint8)),
+                ("dead_flags", ctypes.POINTER(ctypes.c_uint8)),
+                ("dead_regs", ctypes.POINTER(ctypes.c_uint8)),
+                ("n_targets", ctypes.c_uint32), ("target_len", ctypes.c_uint32),
+                ("target_stride", ctypes.c_uint32), ("max_cand_len", ctypes.c_uint32),
+                ("global_dead_flags", ctypes.c_uint32), ("mode", ctypes.c_uint32),
+                ("path", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+_lib = None
+EXPORTS = [
+    "z80b_init", "z80b_destroy", "z80b_last_error", "z80b_status_string", "z80b_version",
+    "z80b_fingerprints", "z80b_exec", "z80b_load_candidates", "z80b_quickcheck",
+    "z80b_verify_pairs", "z80b_search", "z80b_stage_job", "z80b_run_staged", "z80b_fetch_rules",
+    "z80b_op_info", "z80b_disasm_seq", "z80b_parse_assembly", "z80b_parse_dead_flags",
+    "z80b_dead_flag_desc", "z80b_should_prune", "z80b_pool8", "z80b_rules_json",
+]
+
+
+def lib():
+    """Loads libz80b200.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise Z80BError(ENODEV, f"{LIB_PATH} not built (run make in {_HERE})")
+        L = ctypes.CDLL(LIB_PATH)
+        vp = ctypes.c_void_p
+        u32p = ctypes.POINTER(ctypes.c_uint32)
+        u8p = ctypes.POINTER(ctypes.c_uint8)
+        L.z80b_init.argtypes = [ctypes.c_int, ctypes.POINTER(vp)]
+        L.z80b_destroy.argtypes = [vp]
+        L.z80b_destroy.restype = None
+        L.z80b_last_error.argtypes = [vp]
+        L.z80b_last_error.restype = ctypes.c_char_p
+        L.z80b_status_string.restype = ctypes.c_char_p
+        L.z80b_fingerprints.argtypes = [vp, u32p, ctypes.c_uint32, ctypes.c_uint32, u8p]
+        L.z80b_exec.argtypes = [vp, ctypes.POINTER(State), u32p, u8p, ctypes.c_uint32,
+                                ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(State)]
+        L.z80b_load_candidates.argtypes = [vp, u32p, ctypes.c_uint32, ctypes.c_uint32]
+        L.z80b_quickcheck.argtypes = [vp, u8p, ctypes.c_uint32, u32p, ctypes.c_uint32, u32p]
+        L.z80b_verify_pairs.argtypes = [vp, u32p, u8p, u32p, u8p, ctypes.c_uint32, ctypes.c_uint32,
+                                        u8p, ctypes.c_uint32, u8p, u8p]
+        L.z80b_search.argtypes = [vp, ctypes.POINTER(Job), ctypes.POINTER(Rule), ctypes.c_uint64,
+                                  ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(Stats)]
+        L.z80b_stage_job.argtypes = [vp, ctypes.POINTER(Job)]
+        L.z80b_run_staged.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(Stats)]
+        L.z80b_fetch_rules.argtypes = [vp, ctypes.POINTER(Rule), ctypes.c_uint64,
+                                       ctypes.POINTER(ctypes.c_uint64)]
+        L.z80b_op_info.argtypes = [ctypes.c_uint32, ctypes.c_char_p, ctypes.c_uint32] + \
+            [ctypes.POINTER(ctypes.c_int)] * 5
+        L.z80b_disasm_seq.argtypes = [u32p, ctypes.c_uint32, ctypes.c_char_p, ctypes.c_uint32]
+        L.z80b_parse_assembly.argtypes = [ctypes.c_char_p, u32p, ctypes.c_uint32]
+        L.z80b_parse_dead_flags.argtypes = [ctypes.c_char_p, u32p]
+        L.z80b_dead_flag_desc.argtypes = [ctypes.c_uint32, ctypes.c_char_p, ctypes.c_uint32]
+        L.z80b_should_prune.argtypes = [u32p, ctypes.c_uint32]
+        L.z80b_pool8.argtypes = [u32p, ctypes.c_uint32]
+        L.z80b_pool8.restype = ctypes.c_uint32
+        L.z80b_rules_json.argtypes = [ctypes.POINTER(Rule), ctypes.c_uint64, ctypes.c_char_p,
+                                      ctypes.c_uint64]
+        L.z80b_rules_json.restype = ctypes.c_longlong
+        _lib = L
+    return _lib
+
+
+def pack(op, imm=0):
+    return (op & 0xFFFF) | ((imm & 0xFFFF) << 16)
+
+
+def _u32(seq):
+    return (ctypes.c_uint32 * max(1, len(seq)))(*seq)
+
+
+def _u8(seq):
+    return (ctypes.c_uint8 * max(1, len(seq)))(*seq)
+
+
+# ------------------------------------------------------------ host helpers
+
+def op_info(op):
+    m = ctypes.create_string_buffer(32)
+    vals = [ctypes.c_int() for _ in range(5)]
+    st = lib().z80b_op_info(op, m, 32, *[ctypes.byref(v) for v in vals])
+    if st != OK:
+        raise Z80BError(st, f"opcode {op}")
+    size, t, imm, rd, wr = (v.value for v in vals)
+    return {"mnemonic": m.value.decode(), "size": size, "tstates": t, "imm": imm,
+            "reads": rd, "writes": wr}
+
+
+def disasm(seq):
+    n = lib().z80b_disasm_seq(_u32(seq), len(seq), None, 0)
+    if n < 0:
+        raise Z80BError(EINVAL, "bad opcode")
+    b = ctypes.create_string_buffer(n + 1)
+    lib().z80b_disasm_seq(_u32(seq), len(seq), b, n + 1)
+    return b.value.decode()
+
+
+def parse_assembly(text):
+    buf = (ctypes.c_uint32 * 256)()
+    n = lib().z80b_parse_assembly(text.encode(), buf, 256)
+    if n < 0:
+        raise Z80BError(EINVAL, f"cannot parse {text!r}")
+    return list(buf[:n])
+
+
+def parse_dead_flags(text):
+    v = ctypes.c_uint32()
+    st = lib().z80b_parse_dead_flags(text.encode(), ctypes.byref(v))
+    if st != OK:
+        raise Z80BError(st, f"invalid --dead-flags value {text!r}")
+    return v.value
+
+
+def dead_flag_desc(mask):
+    b = ctypes.create_string_buffer(64)
+    lib().z80b_dead_flag_desc(mask, b, 64)
+    return b.value.decode()
+
+
+def should_prune(seq):
+    r = lib().z80b_should_prune(_u32(seq), len(seq))
+    if r < 0:
+        raise Z80BError(EINVAL, "bad opcode")
+    return bool(r)
+
+
+def pool8():
+    buf = (ctypes.c_uint32 * 8192)()
+    n = lib().z80b_pool8(buf, 8192)
+    return list(buf[:n])
+
+
+def write_json(rules):
+    arr = (Rule * max(1, len(rules)))(*rules)
+    n = lib().z80b_rules_json(arr, len(rules), None, 0)
+    if n < 0:
+        raise Z80BError(EINVAL, "bad rule")
+    b = ctypes.create_string_buffer(n + 1)
+    lib().z80b_rules_json(arr, len(rules), b, n + 1)
+    return b.value.decode()
+
+
+# ----------------------------------------------------------------- context
+
+class Context:
+    """One device context (z80b_init).  Not thread-safe; one per thread."""
+
+    def __init__(self, device=0):
+        self._h = ctypes.c_void_p()
+        st = lib().z80b_init(device, ctypes.byref(self._h))
+        if st != OK:
+            raise Z80BError(st, lib().z80b_status_string(st).decode())
+
+    def close(self):
+        if self._h:
+            lib().z80b_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st != OK:
+            raise Z80BError(st, lib().z80b_last_error(self._h).decode())
+
+    # search.Fingerprint
+    def fingerprints(self, seqs, length):
+        flat = [w for s in seqs for w in s]
+        out = (ctypes.c_uint8 * (80 * max(1, len(seqs))))()
+        self._check(lib().z80b_fingerprints(self._h, _u32(flat), len(seqs), length, out))
+        return [bytes(out[80 * i:80 * i + 80]) for i in range(len(seqs))]
+
+    def exec(self, states, seqs, stride=4):
+        n = len(seqs)
+        flat = []
+        lens = []
+        for s in seqs:
+            flat += list(s) + [0] * (stride - len(s))
+            lens.append(len(s))
+        ins = (State * max(1, n))(*states)
+        outs = (State * max(1, n))()
+        self._check(lib().z80b_exec(self._h, ins, _u32(flat), _u8(lens), 0, stride, n, outs))
+        return [outs[i] for i in range(n)]
+
+    # gpu.NewCUDAProcess
+    def load_candidates(self, cands, seq_len=1):
+        flat = [w for c in cands for w in (c if isinstance(c, (list, tuple)) else [c])]
+        n = len(flat) // seq_len
+        self._check(lib().z80b_load_candidates(self._h, _u32(flat), n, seq_len))
+
+    # CUDAProcess.QuickCheckGPU
+    def quickcheck_gpu(self, fp, dead_flags=0, cap=1 << 20):
+        hits = (ctypes.c_uint32 * cap)()
+        nh = ctypes.c_uint32()
+        fpb = (ctypes.c_uint8 * 80)(*fp)
+        self._check(lib().z80b_quickcheck(self._h, fpb, dead_flags, hits, cap, ctypes.byref(nh)))
+        return list(hits[:nh.value])
+
+    def verify_pairs(self, pairs, dead=None, tiers=TIER_QC | TIER_MID | TIER_EXH, stride=4):
+        """pairs: [(target_seq, cand_seq)]; returns [(tier_bits, flagdiff)]."""
+        n = len(pairs)
+        t, c, tl, cl = [], [], [], []
+        for a, b in pairs:
+            t += list(a) + [0] * (stride - len(a))
+            c += list(b) + [0] * (stride - len(b))
+            tl.append(len(a))
+            cl.append(len(b))
+        out = (ctypes.c_uint8 * max(1, n))()
+        fd = (ctypes.c_uint8 * max(1, n))()
+        dd = _u8(dead) if dead is not None else None
+        self._check(lib().z80b_verify_pairs(self._h, _u32(t), _u8(tl), _u32(c), _u8(cl), stride, n,
+                                            dd, tiers, out, fd))
+        return [(out[i], fd[i]) for i in range(n)]
+
+    @staticmethod
+    def make_job(targets, dead_flags=0, mode=MODE_FIRST, path=PATH_BATCHED, per_target_dead=None,
+                 dead_regs=None, stride=4, max_cand_len=1):
+        """Builds a Job plus the ctypes buffers it points to."""
+        n = len(targets)
+        flat = (ctypes.c_uint32 * max(1, n * stride))()
+        lens = (ctypes.c_uint8 * max(1, n))()
+        for i, t in enumerate(targets):
+            lens[i] = len(t)
+            for j, w in enumerate(t):
+                flat[i * stride + j] = w
+        job = Job()
+        job.targets = ctypes.cast(flat, ctypes.POINTER(ctypes.c_uint32))
+        job.target_lens = ctypes.cast(lens, ctypes.POINTER(ctypes.c_uint8))
+        keep = [flat, lens]
+        if per_target_dead is not None:
+            d = _u8(per_target_dead)
+            keep.append(d)
+            job.dead_flags = ctypes.cast(d, ctypes.POINTER(ctypes.c_uint8))
+        if dead_regs is not None:
+            r = _u8(dead_regs)
+            keep.append(r)
+            job.dead_regs = ctypes.cast(r, ctypes.POINTER(ctypes.c_uint8))
+        job.n_targets = n
+        job.target_len = 0
+        job.target_stride = stride
+        job.max_cand_len = max_cand_len
+        job.global_dead_flags = dead_flags
+        job.mode = mode
+        job.path = path
+        return job, keep
+
+    def search(self, targets, dead_flags=0, mode=MODE_FIRST, path=PATH_BATCHED,
+               per_target_dead=None, dead_regs=None, max_cand_len=1):
+        job, keep = self.make_job(targets, dead_flags, mode, path, per_target_dead, dead_regs,
+                                  max_cand_len=max_cand_len)
+        return self.run_job(job)
+
+    def run_job(self, job, cap=None):
+        cap = cap or (2 * job.n_targets + 1024)
+        while True:
+            out = (Rule * cap)()
+            nr = ctypes.c_uint64()
+            st = Stats()
+            s = lib().z80b_search(self._h, ctypes.byref(job), out, cap, ctypes.byref(nr),
+                                  ctypes.byref(st))
+            if s == ECAPACITY and nr.value > cap:
+                cap = nr.value
+                continue
+            self._check(s)
+            return [out[i] for i in range(nr.value)], st
+
+    def stage(self, job):
+        self._check(lib().z80b_stage_job(self._h, ctypes.byref(job)))
+
+    def run_staged(self):
+        nr = ctypes.c_uint64()
+        st = Stats()
+        self._check(lib().z80b_run_staged(self._h, ctypes.byref(nr), ctypes.byref(st)))
+        return nr.value, st
+
+    def fetch_rules(self, n):
+        out = (Rule * max(1, n))()
+        nr = ctypes.c_uint64()
+        self._check(lib().z80b_fetch_rules(self._h, out, max(1, n), ctypes.byref(nr)))
+        return [out[i] for i in range(nr.value)]
+
+
+def _sort_rules(rules):
+    # result.Table.Rules (pkg/result/table.go:38-50): bytes saved, then cycles
+    # saved, both descending; insertion order breaks ties (full rule first)
+    return sorted(rules, key=lambda r: (-r.bytes_saved, -r.cycles_saved))
+
+
+def search_single(ctx, target, max_cand_len=1):
+    """search.SearchSingle (pkg/search/search.go:82-94)."""
+    rules, _ = ctx.search([target], max_cand_len=max_cand_len)
+    rules = _sort_rules(rules)
+    return rules[0] if rules else None
+
+
+def search_single_masked(ctx, target, max_cand_len, dead_flags):
+    """search.SearchSingleMasked (pkg/search/search.go:97-110)."""
+    rules, _ = ctx.search([target], dead_flags=dead_flags, max_cand_len=max_cand_len)
+    rules = _sort_rules(rules)
+    return rules[0] if rules else None
