@@ -124,6 +124,22 @@ int orc_instructions8(uint32_t* out, int cap) {
   for (int i = 0; i < int(p.size()) && i < cap; i++) out[i] = pack(p[size_t(i)]);
   return int(p.size());
 }
+// Indices (enumeration order) of the 8-bit instructions passing
+// QuickCheckMasked against a target; writes up to cap, returns the count.
+int orc_qc_survivors(const uint32_t* t, int tn, int dead, uint32_t* out, int cap) {
+  Init();
+  auto tv = seqOf(t, tn);
+  const auto& pool = Instructions8();
+  int k = 0;
+  for (size_t i = 0; i < pool.size(); i++) {
+    if (QuickCheckMasked(tv.data(), tn, &pool[i], 1, FlagMask(dead))) {
+      if (k < cap) out[k] = uint32_t(i);
+      k++;
+    }
+  }
+  return k;
+}
+
 void orc_test_vectors(orc_state* qc8, orc_state* mid32) {
   for (int i = 0; i < 8; i++) qc8[i] = fromS(TestVectors[i]);
   for (int i = 0; i < 32; i++) mid32[i] = fromS(MidCheckVectors[i]);

@@ -248,3 +248,9 @@ def mul_run(seq, x, b, c, f):
 
 def mul_tstates(i):
     return lib().orc_mul_tstates(i)
+
+
+def qc_survivors(target, dead=0):
+    buf = (ctypes.c_uint32 * 8192)()
+    n = lib().orc_qc_survivors(arr(target), len(target), dead, buf, 8192)
+    return list(buf[:n])

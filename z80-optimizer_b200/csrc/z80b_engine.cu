@@ -16,6 +16,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
+#include <cstdlib>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -97,6 +99,22 @@ struct z80b_ctx {
 };
 
 namespace {
+
+// Stage tracing to stderr when Z80B_TRACE is set (timestamps from the
+// first traced event).
+void trace(const char* fmt, ...) {
+  static const bool on = std::getenv("Z80B_TRACE") != nullptr;
+  if (!on) return;
+  static const auto t0 = std::chrono::steady_clock::now();
+  double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  std::fprintf(stderr, "[z80b %9.4fs] %s\n", dt, buf);
+  std::fflush(stderr);
+}
 
 int fail(z80b_ctx* c, int code, const char* fmt, ...) {
   char buf[512];
@@ -185,10 +203,13 @@ int build_pool(z80b_ctx* ctx, PoolBufs& P, const uint32_t* insn, uint32_t n, uin
     // pool kernel requires a fixed length
     return fail(ctx, Z80B_EINVAL, "candidate pools need a fixed sequence length");
   }
+  trace("pool: %u candidates uploaded", n);
   launch_pool_outputs(P.insn.as<uint32_t>(), n, len, P.qc.as<uint4>(), with_mid ? P.mid.as<uint4>() : nullptr,
                       ctx->stream);
   CKR(check_launch(ctx, "pool_outputs"));
+  trace("pool: kernel launched");
   CK(cudaStreamSynchronize(ctx->stream));
+  trace("pool: outputs ready");
   P.dev = DevPool{};
   P.dev.insn = P.insn.as<uint32_t>();
   P.dev.qc = P.qc.as<uint4>();
@@ -314,6 +335,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, uint32_t mode, z80b_stats* 
   CK(cudaMemsetAsync(ctx->checked.p, 0, 8, s));
   CK(cudaMemsetAsync(ctx->states.p, 0, 8, s));
 
+  trace("pipeline: %u targets, mode %u, pool %u", n, mode, P.n);
   Timer tall{ctx, 0, 1};
   ctx->kev_used = 0;
   tall.start();
@@ -334,6 +356,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, uint32_t mode, z80b_stats* 
   CK(cudaMemcpyAsync(&last[2], ctx->cnt_m.as<uint32_t>() + (n - 1), 4, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   const uint64_t nsurv = uint64_t(last[0]) + last[1] + last[2];
+  trace("qc count done: %llu survivors", (unsigned long long)nsurv);
   if (nsurv > 0xFFFFFFF0ull) return fail(ctx, Z80B_ECAPACITY, "too many QuickCheck survivors (%llu)", (unsigned long long)nsurv);
   CK(ctx->surv.ensure(4ull * std::max<uint64_t>(nsurv, 1)));
   CK(ctx->sdiff.ensure(2ull * std::max<uint64_t>(nsurv, 1)));
@@ -377,6 +400,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, uint32_t mode, z80b_stats* 
         CKR(check_launch(ctx, "round_build"));
         uint32_t np = 0;
         CKR(fetch(ctx, &np, R.npairs));
+        trace("round %u: %u pairs", rounds, np);
         if (np == 0) break;
         rounds++;
         exh_pairs += np;
@@ -386,6 +410,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, uint32_t mode, z80b_stats* 
         CK(cudaMemcpyAsync(&lastn, R.nchunks + (np - 1), 8, cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         CK(cudaMemsetAsync(R.counter, 0, 8, s));
+        trace("round %u: %llu chunks", rounds, lastb + lastn);
         int ke = kbegin(ctx, 1);
         launch_exhaustive(T, P, R, np, lastb + lastn, s);
         kend(ctx, ke);
@@ -470,6 +495,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, uint32_t mode, z80b_stats* 
   }
   tall.stop();
   CK(cudaStreamSynchronize(s));
+  trace("pipeline done: %llu rules, %u rounds", (unsigned long long)*nr, rounds);
   if (st) {
     unsigned long long checks = 0, checked = 0, states = 0;
     CKR(fetch(ctx, &checks, ctx->checks.as<unsigned long long>()));
@@ -645,6 +671,8 @@ int z80b_init(int device, z80b_ctx** out) {
   cudaDeviceProp prop{};
   if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return Z80B_ENODEV;
   if (prop.major < 10) return Z80B_ENODEV;  // built for sm_100a only
+  trace("init device %d (%s, cc %d.%d, %d SMs)", device, prop.name, prop.major, prop.minor,
+        prop.multiProcessorCount);
   z80b_ctx* ctx = new z80b_ctx();
   ctx->device = device;
   if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
@@ -652,13 +680,16 @@ int z80b_init(int device, z80b_ctx** out) {
     return Z80B_ECUDA;
   }
   for (auto& e : ctx->ev) cudaEventCreate(&e);
+  trace("init: stream and events");
   dev_upload_tables(ctx->stream);
+  trace("init: tables queued");
   const auto& p8 = pool8();
   int r = build_pool(ctx, ctx->pool8, p8.data(), uint32_t(p8.size()), 1, nullptr, false);
   if (r != Z80B_OK) {
     z80b_destroy(ctx);
     return r;
   }
+  trace("init done");
   *out = ctx;
   return Z80B_OK;
 }

@@ -22,6 +22,8 @@
 // depend on it.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "z80b_kernels.cuh"
 
 namespace z80b {
@@ -31,8 +33,14 @@ constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr uint32_t kResolved = 0x80000000u;
 constexpr int kBlock = 256;
 
-__constant__ OpInfo c_ops[kNumOps];
-__constant__ uint32_t c_vec[32][3];  // MidCheck vectors; the first 8 are the QuickCheck vectors
+// Tables that lanes index with different values live in global memory (L1
+// cached); __constant__ is kept for the reduced-sweep values, whose index is
+// the same in every lane of a warp.  Every kernel that runs z_step gives all
+// lanes of a warp the same opcode: divergent dispatch of the 455-way switch
+// combined with lane-indexed constant loads in the same loop failed on this
+// toolchain (illegal address / no progress), so neither pattern is used.
+__device__ OpInfo g_ops[kNumOps];
+__device__ uint32_t g_vec[32][3];  // MidCheck vectors; the first 8 are the QuickCheck vectors
 __constant__ uint8_t c_rep[32];
 __constant__ uint16_t c_repsp[16];
 
@@ -54,7 +62,7 @@ __device__ __forceinline__ void run_lanes(Z80S& s, uint32_t lane_word, int first
 }
 
 __device__ __forceinline__ Z80S vec_state(int v) {
-  return z_unpack(c_vec[v][0], c_vec[v][1], c_vec[v][2]);
+  return z_unpack(g_vec[v][0], g_vec[v][1], g_vec[v][2]);
 }
 
 // Byte masks of compared registers from keepR bits (B,C,D,E,H,L).
@@ -105,57 +113,66 @@ __device__ __forceinline__ unsigned long long chunks_for(unsigned long long nb) 
 
 // ------------------------------------------------------------------ kernels
 
+// Warp per candidate, lane v runs the candidate on vector v (lanes 0..7
+// QuickCheck, 0..31 MidCheck); the opcode is the same in every lane.
 __global__ void k_pool_outputs(const uint32_t* __restrict__ insn, uint32_t n, uint32_t len,
                                uint4* __restrict__ qc, uint4* __restrict__ mid) {
-  uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= n) return;
-  uint32_t prog[kMaxSeq];
-  for (uint32_t i = 0; i < kMaxSeq; i++) prog[i] = i < len ? insn[(size_t)c * len + i] : 0u;
-  const int nv = mid ? 32 : 8;
-  for (int v = 0; v < nv; v++) {
-    Z80S s = vec_state(v);
-    for (uint32_t i = 0; i < len; i++) z_step(s, prog[i] & 0xFFFFu, prog[i] >> 16);
+  const unsigned lane = lane_id();
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t c = gw; c < n; c += nw) {
+    const uint32_t pw = lane < len ? insn[(size_t)c * len + lane] : 0u;
+    Z80S s = vec_state(int(lane));
+    run_lanes(s, pw, 0, int(len));
     uint32_t w[3];
     z_pack(s, w);
-    uint4 q = make_uint4(w[0], w[1], w[2], 0u);
-    if (v < 8) qc[(size_t)v * n + c] = q;
-    if (mid) mid[(size_t)v * n + c] = q;
+    const uint4 q = make_uint4(w[0], w[1], w[2], 0u);
+    if (lane < 8) qc[(size_t)lane * n + c] = q;
+    if (mid) mid[(size_t)lane * n + c] = q;
   }
 }
 
+// One warp per sequence; lane 0 runs it (arbitrary per-item opcodes would
+// otherwise diverge inside the dispatch loop).
 __global__ void k_exec(const uint32_t* __restrict__ in, const uint32_t* __restrict__ seqs,
                        const uint8_t* __restrict__ lens, uint32_t len, uint32_t stride, uint32_t n,
                        uint32_t* __restrict__ out) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  Z80S s = z_unpack(in[3 * i], in[3 * i + 1], in[3 * i + 2]);
-  uint32_t l = lens ? lens[i] : len;
-  for (uint32_t k = 0; k < l && k < kMaxSeq; k++) {
-    uint32_t w = seqs[(size_t)i * stride + k];
-    z_step(s, w & 0xFFFFu, w >> 16);
+  const unsigned lane = lane_id();
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t i = gw; i < n; i += nw) {
+    const uint32_t l = lens ? lens[i] : len;
+    const uint32_t pw = lane < l ? seqs[(size_t)i * stride + lane] : 0u;
+    Z80S s = z_unpack(in[3 * i], in[3 * i + 1], in[3 * i + 2]);
+    run_lanes(s, pw, 0, int(l));
+    if (lane == 0) {
+      uint32_t w[3];
+      z_pack(s, w);
+      out[3 * i] = w[0];
+      out[3 * i + 1] = w[1];
+      out[3 * i + 2] = w[2];
+    }
   }
-  uint32_t w[3];
-  z_pack(s, w);
-  out[3 * i] = w[0];
-  out[3 * i + 1] = w[1];
-  out[3 * i + 2] = w[2];
 }
 
-// search.Fingerprint: 8 x {A,F,B,C,D,E,H,L,SP_hi,SP_lo}.
+// search.Fingerprint: 8 x {A,F,B,C,D,E,H,L,SP_hi,SP_lo}; warp per sequence,
+// lane v (< 8) on test vector v.
 __global__ void k_fingerprints(const uint32_t* __restrict__ seqs, uint32_t n, uint32_t len,
                                uint8_t* __restrict__ out) {
-  uint32_t gid = blockIdx.x * blockDim.x + threadIdx.x;
-  uint32_t i = gid >> 3, v = gid & 7u;
-  if (i >= n) return;
-  Z80S s = vec_state(int(v));
-  for (uint32_t k = 0; k < len; k++) {
-    uint32_t w = seqs[(size_t)i * len + k];
-    z_step(s, w & 0xFFFFu, w >> 16);
+  const unsigned lane = lane_id();
+  const uint32_t gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nw = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t i = gw; i < n; i += nw) {
+    const uint32_t pw = lane < len ? seqs[(size_t)i * len + lane] : 0u;
+    Z80S s = vec_state(int(lane & 7u));
+    run_lanes(s, pw, 0, int(len));
+    if (lane < 8) {
+      uint8_t* p = out + (size_t)i * 80 + lane * 10;
+      p[0] = uint8_t(s.a); p[1] = uint8_t(s.f); p[2] = uint8_t(s.b); p[3] = uint8_t(s.c);
+      p[4] = uint8_t(s.d); p[5] = uint8_t(s.e); p[6] = uint8_t(s.h); p[7] = uint8_t(s.l);
+      p[8] = uint8_t(s.sp >> 8); p[9] = uint8_t(s.sp);
+    }
   }
-  uint8_t* p = out + (size_t)i * 80 + v * 10;
-  p[0] = uint8_t(s.a); p[1] = uint8_t(s.f); p[2] = uint8_t(s.b); p[3] = uint8_t(s.c);
-  p[4] = uint8_t(s.d); p[5] = uint8_t(s.e); p[6] = uint8_t(s.h); p[7] = uint8_t(s.l);
-  p[8] = uint8_t(s.sp >> 8); p[9] = uint8_t(s.sp);
 }
 
 // z80qc query semantics (cuda/z80_quickcheck.cu:666-681 over pkg/cpu
@@ -214,7 +231,7 @@ __global__ void __launch_bounds__(kBlock) k_qc_scan(DevTargets T, DevPool P, QCC
     const uint32_t pw = lane < tl ? T.insn[(size_t)t * T.stride + lane] : 0u;
     uint32_t sz = 0, ts = 0, rd = 0;
     if (lane < tl) {
-      const OpInfo& oi = c_ops[pw & 0xFFFFu];
+      const OpInfo oi = g_ops[pw & 0xFFFFu];
       sz = oi.size;
       ts = oi.tstates;
       rd = oi.reads;
@@ -420,7 +437,10 @@ __global__ void __launch_bounds__(kBlock) k_exhaustive(DevTargets T, DevPool P, 
       else hi = mid - 1;
     }
     const uint32_t p = lo;
-    if (*reinterpret_cast<volatile uint32_t*>(&R.rejected[p])) continue;
+    // lane 0 reads the flag and the warp acts on one value, so the
+    // shuffles below always see all 32 lanes
+    if (__shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0))
+      continue;
     const PairRec pr = R.pairs[p];
     const unsigned long long nch = (p + 1 < npairs ? R.cbase[p + 1] : total) - R.cbase[p];
     const unsigned long long bpc = (pr.nblocks + nch - 1) / nch;
@@ -452,20 +472,39 @@ __global__ void __launch_bounds__(kBlock) k_exhaustive(DevTargets T, DevPool P, 
     const Keep keep = make_keep(pr.keepF, pr.keepR, true);
 
     bool bad = false;
+    // Block index fields, fastest first: SP (reduced sweeps), the swept
+    // registers from the last to the first, carry.  The reference nests its
+    // loops as A, carry, first register, ..., last register, SP
+    // (verifier.go:498-531,578-610), so block b covers the reference's
+    // states (A, b) for every A at once and a sweep that the reference
+    // abandons early is abandoned at least as early here.
     for (unsigned long long ab = b0; ab < b1; ab++) {
-      const uint32_t carry = uint32_t(ab & 1ull);
-      const unsigned long long rest = ab >> 1;
+      unsigned long long rest = ab;
+      uint32_t sp = 0;
+      if (spw) {
+        sp = c_repsp[uint32_t(rest & 15ull)];
+        rest >>= 4;
+      }
+      uint32_t fieldv[7];
+#pragma unroll
+      for (int k = 6; k >= 0; k--) {
+        fieldv[k] = 0;
+        if (k < nx) {
+          const uint32_t f = uint32_t(rest) & (reduced ? 31u : 255u);
+          fieldv[k] = reduced ? c_rep[f] : f;
+          rest >>= fw;
+        }
+      }
+      const uint32_t carry = uint32_t(rest & 1ull);
       uint32_t rv[7];
 #pragma unroll
       for (int r = 0; r < 7; r++) {
-        if (slot[r] < 0) {
-          rv[r] = 0;
-        } else {
-          uint32_t f = uint32_t(rest >> (fw * slot[r]));
-          rv[r] = reduced ? c_rep[f & 31u] : (f & 0xFFu);
-        }
+        uint32_t v = 0;
+#pragma unroll
+        for (int k = 0; k < 7; k++)
+          if (slot[r] == k) v = fieldv[k];
+        rv[r] = v;
       }
-      const uint32_t sp = spw ? c_repsp[uint32_t(rest >> (5 * nx)) & 15u] : 0u;
 #pragma unroll 1
       for (uint32_t i = 0; i < 8; i++) {
         Z80S x;
@@ -480,7 +519,9 @@ __global__ void __launch_bounds__(kBlock) k_exhaustive(DevTargets T, DevPool P, 
       }
       my_states += 256;
       if (__any_sync(kFull, bad)) break;
-      if ((ab & 15ull) == 15ull && *reinterpret_cast<volatile uint32_t*>(&R.rejected[p])) break;
+      if ((ab & 15ull) == 15ull &&
+          __shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0))
+        break;
     }
     if (__any_sync(kFull, bad) && lane == 0) atomicExch(&R.rejected[p], 1u);
   }
@@ -647,8 +688,8 @@ int dev_num_sms() {
 namespace z80b {
 
 void dev_upload_tables(cudaStream_t s) {
-  cudaMemcpyToSymbolAsync(c_ops, op_table(), sizeof(OpInfo) * kNumOps, 0, cudaMemcpyHostToDevice, s);
-  cudaMemcpyToSymbolAsync(c_vec, mid_vectors(), sizeof(uint32_t) * 32 * 3, 0, cudaMemcpyHostToDevice, s);
+  cudaMemcpyToSymbolAsync(g_ops, op_table(), sizeof(OpInfo) * kNumOps, 0, cudaMemcpyHostToDevice, s);
+  cudaMemcpyToSymbolAsync(g_vec, mid_vectors(), sizeof(uint32_t) * 32 * 3, 0, cudaMemcpyHostToDevice, s);
   cudaMemcpyToSymbolAsync(c_rep, rep_values(), 32, 0, cudaMemcpyHostToDevice, s);
   cudaMemcpyToSymbolAsync(c_repsp, rep_sp(), 32, 0, cudaMemcpyHostToDevice, s);
 }
@@ -656,16 +697,19 @@ void dev_upload_tables(cudaStream_t s) {
 void launch_pool_outputs(const uint32_t* insn, uint32_t n, uint32_t len, uint4* qc, uint4* mid,
                          cudaStream_t s) {
   if (!n) return;
-  k_pool_outputs<<<grid_for(n, 128), 128, 0, s>>>(insn, n, len, qc, mid);
+  unsigned grid = std::min<unsigned>(grid_for(n, 4), unsigned(dev_num_sms() * 16));
+  k_pool_outputs<<<grid, 128, 0, s>>>(insn, n, len, qc, mid);
 }
 void launch_exec(const uint32_t* in, const uint32_t* seqs, const uint8_t* lens, uint32_t len,
                  uint32_t stride, uint32_t n, uint32_t* out, cudaStream_t s) {
   if (!n) return;
-  k_exec<<<grid_for(n, 128), 128, 0, s>>>(in, seqs, lens, len, stride, n, out);
+  unsigned grid = std::min<unsigned>(grid_for(n, 4), unsigned(dev_num_sms() * 16));
+  k_exec<<<grid, 128, 0, s>>>(in, seqs, lens, len, stride, n, out);
 }
 void launch_fingerprints(const uint32_t* seqs, uint32_t n, uint32_t len, uint8_t* out, cudaStream_t s) {
   if (!n) return;
-  k_fingerprints<<<grid_for(n * 8, 256), 256, 0, s>>>(seqs, n, len, out);
+  unsigned grid = std::min<unsigned>(grid_for(n, 4), unsigned(dev_num_sms() * 16));
+  k_fingerprints<<<grid, 128, 0, s>>>(seqs, n, len, out);
 }
 void launch_fp_query(const DevPool& P, const uint32_t* fp, uint32_t dead, uint32_t* hits,
                      uint32_t* nhits, uint32_t cap, cudaStream_t s) {

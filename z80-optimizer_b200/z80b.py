@@ -310,6 +310,7 @@ class Context:
                  dead_regs=None, stride=4, max_cand_len=1):
         """Builds a Job plus the ctypes buffers it points to."""
         n = len(targets)
+        stride = max([stride] + [len(t) for t in targets])
         flat = (ctypes.c_uint32 * max(1, n * stride))()
         lens = (ctypes.c_uint8 * max(1, n))()
         for i, t in enumerate(targets):
