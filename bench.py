@@ -1,10 +1,11 @@
 """Benchmark of the candidate-verification path on B200.
 
-Workload (default): every unpruned length-2 target over the reference's
-8-bit instruction list (9,818,041 targets), candidates of length 1, the
+Workload (default): a seeded uniform sample (1,000,000 targets, seed 0, by
+index) of every unpruned length-2 target over the reference's 8-bit
+instruction list (9,818,041 targets), candidates of length 1, the
 first-found semantics of pkg/search (QuickCheck -> ExhaustiveCheck per
 target, shortest/first candidate wins).  One step = one pass of the whole
-pipeline over the whole target set.
+pipeline over the sample.  `--targets 0` runs the full target set.
 
 Metric: candidate checks/s = (target, candidate) pairs of the workload that
 pass the byte-size and prune filters (the QuickCheck unit of work), per
@@ -38,13 +39,23 @@ METRIC = "Z80 candidate checks/s on 1 B200, batched vs plain GPU; p50/p99 query 
 UNIT = "candidate checks/s"
 
 
+T0 = time.perf_counter()
+
+
+def progress(*a):
+    print(f"[bench {time.perf_counter() - T0:8.2f}s]", *a, file=sys.stderr, flush=True)
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--targets", type=int, default=0, help="limit the target count (0 = all)")
+    ap.add_argument("--targets", type=int, default=1000000,
+                    help="seeded uniform sample of the C2 targets (0 = all 9,818,041)")
+    ap.add_argument("--plain-sample", type=int, default=2000,
+                    help="targets of the plain-vs-batched comparison (0 = skip)")
     ap.add_argument("--dead-flags", default="none")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=0, help="targets in the CPU sample (0 = auto)")
@@ -135,7 +146,7 @@ def cpu_run(sample, dead, workers):
     return time.perf_counter() - t0, len(rules)
 
 
-def cpu_baseline(all_targets, dead, n_sample, seed=0):
+def cpu_baseline(all_targets, dead, n_sample, seed=1):
     workers = os.cpu_count() or 1
     rng = np.random.default_rng(seed)
     idx = np.sort(rng.choice(len(all_targets), size=min(n_sample, len(all_targets)), replace=False))
@@ -148,8 +159,10 @@ def cpu_baseline(all_targets, dead, n_sample, seed=0):
 
 
 def auto_cpu_sample():
-    # about 20 core-seconds of oracle work (~0.8 ms per target per core)
-    return max(2000, min(60000, 25000 * (os.cpu_count() or 1) // 8))
+    # a few core-seconds of oracle work on a typical sample; the sweep-size
+    # tail (true equivalences with 2^34-state reduced sweeps, ~1 in 100k
+    # targets) makes larger samples unbounded on the CPU
+    return 4000
 
 
 def main():
@@ -161,10 +174,11 @@ def main():
     import z80b
     import workloads
     dead = z80b.parse_dead_flags(args.dead_flags)
-    allt = workloads.c2_targets()
-    if args.targets:
-        allt = allt[:args.targets]
-    workload = {"workload": "full length-2 (C2)", "targets": int(len(allt)), "target_len": 2,
+    full = workloads.c2_targets()
+    allt = workloads.c2_subset(args.targets, seed=0) if args.targets else full
+    workload = {"workload": "length-2 targets (C2)" + (f", seeded sample of {len(allt)} / {len(full)}"
+                                                     if args.targets else ", all"),
+                "targets": int(len(allt)), "target_len": 2,
                 "max_cand_len": 1, "candidates": 4531, "semantics": "pkg/search first-found",
                 "dead_flags": dead, "vectors": "reference QuickCheck 8 (verifier.go:19-28)",
                 "l2": "flushed between steps (512 MiB write)"}
@@ -210,14 +224,16 @@ def main():
     mine = np.ascontiguousarray(allt[lo:hi])
     ctx = z80b.Context(local if world > 1 else 0)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    progress(f"rank {rank}: {len(mine)} targets staged")
 
     # ---- value: targets resident in HBM
     job = make_job(z80b, mine, dead)
     ctx.stage(job)
-    for _ in range(args.warmup):
+    for i in range(args.warmup):
         flush.fill_(1)
         torch.cuda.synchronize()
-        ctx.run_staged()
+        _, wst = ctx.run_staged()
+        progress(f"warmup {i}: {wst.device_ms:.1f} ms, {wst.exhaustive_states:.3e} states, {wst.rounds} rounds")
     dev_ms, exh_ms, qc_ms, launches, checks, states, rules = 0.0, 0.0, 0.0, 0, 0, 0, 0
     stats_last = None
     if dist:
@@ -237,6 +253,7 @@ def main():
             states += st.exhaustive_states
             rules = n
             stats_last = st
+            progress(f"step: {st.device_ms:.1f} ms (qc {st.qc_ms:.1f}, exhaustive {st.exh_ms:.1f})")
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     t_step = dev_ms / args.steps
@@ -276,6 +293,7 @@ def main():
         e2e_t += time.perf_counter() - t1
         e2e_checks += st2.checks
     e2e_step = e2e_t / args.steps
+    progress(f"e2e: {1e3 * e2e_step:.1f} ms per step")
     if dist:
         t = torch.tensor([e2e_step], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -312,9 +330,31 @@ def main():
                 "algorithmic_ops_per_state": per_state,
                 "exhaustive_ms_per_step": exh_ms / args.steps, "qc_ms_per_step": qc_ms / args.steps}
 
+    # ---- plain (one target per launch) vs batched on the same sample
+    plain = None
+    if args.plain_sample and rank == 0:
+        ps = np.ascontiguousarray(workloads.c2_subset(args.plain_sample, seed=7))
+        pjob = make_job(z80b, ps, dead)
+        pjob.path = z80b.PATH_PLAIN
+        _, stp = ctx.run_job(pjob)
+        t1 = time.perf_counter()
+        _, stp = ctx.run_job(pjob)
+        tp = time.perf_counter() - t1
+        bjob = make_job(z80b, ps, dead)
+        _, stb = ctx.run_job(bjob)
+        t1 = time.perf_counter()
+        _, stb = ctx.run_job(bjob)
+        tb = time.perf_counter() - t1
+        progress(f"plain {tp:.2f} s vs batched {tb:.2f} s on {len(ps)} targets")
+        plain = {"targets": int(len(ps)), "plain_checks_per_s": stp.checks / tp,
+                 "batched_checks_per_s": stb.checks / tb, "batched_over_plain": tp / tb,
+                 "plain_launches": stp.launches, "batched_launches": stb.launches,
+                 "timing": "host wall clock around z80b_search (both synchronous)"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(allt, dead, args.cpu_sample or auto_cpu_sample())
+        progress(f"cpu baseline: {cpu['sample']}")
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_step, "higher_is_better": True,
@@ -323,7 +363,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": 1e3 * e2e_step},
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
-            "gpu_launches": launches,
+            "gpu_launches": launches, "plain_vs_batched": plain,
             "detail": {"rules": rules, "checked_ref": stats_last.checked_ref if stats_last else None,
                        "qc_survivors": stats_last.qc_survivors if stats_last else None,
                        "exhaustive_pairs": stats_last.exhaustive_pairs if stats_last else None,
