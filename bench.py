@@ -226,6 +226,14 @@ def main():
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
     progress(f"rank {rank}: {len(mine)} targets staged")
 
+    # ---- autotune (states per lane x chunk size) on a 200k-target sample
+    tune_arr = np.ascontiguousarray(workloads.c2_subset(200000, seed=11))
+    tr = ctx.autotune(make_job(z80b, tune_arr, dead))
+    tuning = {"lane_states": tr.lane_states, "chunk_blocks": tr.chunk_blocks,
+              "trial_ms": [[round(tr.ms[a][b], 2) for b in range(4)] for a in range(4)],
+              "grid": "lane states 1,2,4,8 x chunk blocks 8,32,128,512 on 200k targets"}
+    progress(f"autotune: lane states {tr.lane_states}, chunk blocks {tr.chunk_blocks}")
+
     # ---- value: targets resident in HBM
     job = make_job(z80b, mine, dead)
     ctx.stage(job)
@@ -363,7 +371,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": 1e3 * e2e_step},
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
-            "gpu_launches": launches, "plain_vs_batched": plain,
+            "gpu_launches": launches, "plain_vs_batched": plain, "autotune": tuning,
             "detail": {"rules": rules, "checked_ref": stats_last.checked_ref if stats_last else None,
                        "qc_survivors": stats_last.qc_survivors if stats_last else None,
                        "exhaustive_pairs": stats_last.exhaustive_pairs if stats_last else None,

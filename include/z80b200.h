@@ -162,6 +162,22 @@ int z80b_stage_job(z80b_ctx* ctx, const z80b_job* job);
 int z80b_run_staged(z80b_ctx* ctx, uint64_t* n_rules, z80b_stats* stats);
 int z80b_fetch_rules(z80b_ctx* ctx, z80b_rule* out, uint64_t cap, uint64_t* n_rules);
 
+/* ---- tuning -------------------------------------------------------------- */
+#define Z80B_OPT_EXH_LANE_STATES 1  /* ExhaustiveCheck states per lane per dispatch: 1, 2, 4, 8 */
+#define Z80B_OPT_EXH_CHUNK_BLOCKS 2 /* A-blocks (256 states) per work chunk: 1..4096 */
+int z80b_set_option(z80b_ctx* ctx, int option, int value);
+int z80b_get_option(const z80b_ctx* ctx, int option, int* value);
+
+typedef struct z80b_tune_result {
+  int lane_states;            /* chosen Z80B_OPT_EXH_LANE_STATES */
+  int chunk_blocks;           /* chosen Z80B_OPT_EXH_CHUNK_BLOCKS */
+  double ms[4][4];            /* device ms of the trial runs [lane_states 1,2,4,8][chunk 8,32,128,512] */
+} z80b_tune_result;
+/* Runs the job (a representative sample) for every combination of the
+ * tuning options, keeps the fastest for this context and reports the
+ * timings.  The rules of the trials are discarded. */
+int z80b_autotune(z80b_ctx* ctx, const z80b_job* sample, z80b_tune_result* out);
+
 /* ---- host helpers (no device work) ---------------------------------------- */
 /* inst.Catalog entry (pkg/inst/catalog.go:4-145): mnemonic with n/nn
  * placeholders, encoded size incl. immediate, T-states, immediate kind

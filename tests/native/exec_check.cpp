@@ -64,6 +64,29 @@ int main() {
       }
     }
   }
+  // z_stepK with several states per dispatch (the sweep kernel's form)
+  for (int op = 0; op < orc::OpCodeCount; op++) {
+    for (int i = 0; i < 2000; i++) {
+      orc::State o[3];
+      z80b::Z80S d[3];
+      uint16_t iv = uint16_t(rng());
+      for (int k = 0; k < 3; k++) {
+        uint64_t r = rng();
+        o[k] = orc::State{uint8_t(r), uint8_t(r >> 8), uint8_t(r >> 16), uint8_t(r >> 24), uint8_t(r >> 32),
+                          uint8_t(r >> 40), uint8_t(r >> 48), uint8_t(r >> 56), uint16_t(rng()), uint8_t(rng())};
+        d[k] = z80b::Z80S{o[k].A, o[k].F, o[k].B, o[k].C, o[k].D, o[k].E, o[k].H, o[k].L, o[k].SP, o[k].M};
+        orc::Exec(o[k], uint16_t(op), iv);
+      }
+      z80b::z_stepK<3>(d, uint32_t(op), iv);
+      for (int k = 0; k < 3; k++) {
+        checked++;
+        if (!same(o[k], d[k])) {
+          std::printf("MISMATCH K=3 op=%d (%s) state %d\n", op, orc::OpName(uint16_t(op)), k);
+          return 1;
+        }
+      }
+    }
+  }
   std::printf("OK %lld states\n", checked);
   return 0;
 }

@@ -244,3 +244,28 @@ def test_staged_equals_search(ctx):
     staged = ctx.fetch_rules(n)
     rules, _ = ctx.search(targets, dead_flags=0xFF)
     assert rule_keys(staged) == rule_keys(rules)
+
+
+@pytest.mark.parametrize("lane_states,chunk", [(1, 8), (2, 32), (4, 128), (8, 512), (4, 1)])
+def test_tuning_options_keep_parity(ctx, O, lane_states, chunk):
+    targets = workloads.to_lists(workloads.c2_subset(2500, seed=12))
+    old = (ctx.get_option(z80b.OPT_EXH_LANE_STATES), ctx.get_option(z80b.OPT_EXH_CHUNK_BLOCKS))
+    ctx.set_option(z80b.OPT_EXH_LANE_STATES, lane_states)
+    ctx.set_option(z80b.OPT_EXH_CHUNK_BLOCKS, chunk)
+    try:
+        rules, st = ctx.search(targets, dead_flags=0xFF)
+    finally:
+        ctx.set_option(z80b.OPT_EXH_LANE_STATES, old[0])
+        ctx.set_option(z80b.OPT_EXH_CHUNK_BLOCKS, old[1])
+    exp, checked = O.search(targets, 1, dead=0xFF)
+    assert rule_keys(rules) == rule_keys(exp)
+    assert st.checked_ref == checked
+
+
+def test_autotune_picks_a_valid_setting(ctx):
+    targets = workloads.to_lists(workloads.c2_subset(2000, seed=13))
+    job, keep = ctx.make_job(targets)
+    r = ctx.autotune(job)
+    assert r.lane_states in (1, 2, 4, 8) and r.chunk_blocks in (8, 32, 128, 512)
+    assert ctx.get_option(z80b.OPT_EXH_LANE_STATES) == r.lane_states
+    assert all(r.ms[a][b] > 0 for a in range(4) for b in range(4))

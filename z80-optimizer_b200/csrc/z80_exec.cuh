@@ -1,11 +1,12 @@
 // z80_exec.cuh -- the Z80 step function shared by every kernel.
 //
 // One instruction of the reference emulator (pkg/cpu/exec.go:8-1034, helpers
-// exec.go:1038-1264) over a register-resident state.  Each Z80 register
-// lives in its own 32-bit register (8-bit values, SP 16-bit), so a switch on
-// the opcode compiles to a jump table whose cases touch named registers only;
-// inside a warp that verifies one (target, candidate) pair every lane runs the
-// same opcode, so the dispatch never diverges.
+// exec.go:1038-1264) over register-resident states.  Each Z80 register
+// lives in its own 32-bit register (8-bit values, SP 16-bit), so the opcode
+// switch's cases touch named registers only; z_stepK applies one dispatch to
+// K states, which amortizes the dispatch over the K states a lane carries
+// through a sweep.  Inside a warp every lane runs the same opcode, so the
+// dispatch never diverges.
 //
 // The flag lookups of pkg/cpu/flags.go are computed instead of loaded:
 //   Sz53Table[v]   = (v & 0xA8) | (v == 0 ? Z : 0)
@@ -177,39 +178,49 @@ Z80_HD void z_sbchl(Z80S& s, uint32_t v) {
 #define Z80B_S7(M, base) M((base) + 0, b) M((base) + 1, c) M((base) + 2, d) M((base) + 3, e) \
   M((base) + 4, h) M((base) + 5, l) M((base) + 6, a)
 
-#define Z_LDA(o, r) case (o): s.a = s.r; break;
-#define Z_LDB(o, r) case (o): s.b = s.r; break;
-#define Z_LDC(o, r) case (o): s.c = s.r; break;
-#define Z_LDD(o, r) case (o): s.d = s.r; break;
-#define Z_LDE(o, r) case (o): s.e = s.r; break;
-#define Z_LDH(o, r) case (o): s.h = s.r; break;
-#define Z_LDL(o, r) case (o): s.l = s.r; break;
-#define Z_LDN(o, r) case (o): s.r = imm & 0xFFu; break;
-#define Z_ADD(o, r) case (o): z_add(s, s.r); break;
-#define Z_ADC(o, r) case (o): z_adc(s, s.r); break;
-#define Z_SUB(o, r) case (o): z_sub(s, s.r); break;
-#define Z_SBC(o, r) case (o): z_sbc(s, s.r); break;
-#define Z_AND(o, r) case (o): z_and(s, s.r); break;
-#define Z_XOR(o, r) case (o): z_xor(s, s.r); break;
-#define Z_OR(o, r) case (o): z_or(s, s.r); break;
-#define Z_CP(o, r) case (o): z_cp(s, s.r); break;
-#define Z_INC(o, r) case (o): z_inc(s, s.r); break;
-#define Z_DEC(o, r) case (o): z_dec(s, s.r); break;
-#define Z_RLC(o, r) case (o): s.r = z_rlc(s, s.r); break;
-#define Z_RRC(o, r) case (o): s.r = z_rrc(s, s.r); break;
-#define Z_RL(o, r) case (o): s.r = z_rl(s, s.r); break;
-#define Z_RR(o, r) case (o): s.r = z_rr(s, s.r); break;
-#define Z_SLA(o, r) case (o): s.r = z_sla(s, s.r); break;
-#define Z_SRA(o, r) case (o): s.r = z_sra(s, s.r); break;
-#define Z_SRL(o, r) case (o): s.r = z_srl(s, s.r); break;
-#define Z_SLL(o, r) case (o): s.r = z_sll(s, s.r); break;
-#define Z_BIT(o, r) case (o): z_bit(s, s.r, uint32_t(((o) - BIT_0_A) / 7)); break;
-#define Z_RES(o, r) case (o): s.r &= ~(1u << (((o) - RES_0_A) / 7)); break;
-#define Z_SET(o, r) case (o): s.r |= 1u << (((o) - SET_0_A) / 7); break;
+// Applies a statement to every state S[0..K) (named s inside).
+#define Z80B_EACH(...)                 \
+  _Pragma("unroll") for (int k_ = 0; k_ < K; k_++) { \
+    Z80S& s = S[k_];                   \
+    __VA_ARGS__;                       \
+  }
 
-// Executes one instruction.  Opcodes outside 0..454 leave the state alone
-// (the host rejects them before any launch).
-Z80_HD void z_step(Z80S& s, uint32_t op, uint32_t imm) {
+#define Z_LDA(o, r) case (o): Z80B_EACH(s.a = s.r); break;
+#define Z_LDB(o, r) case (o): Z80B_EACH(s.b = s.r); break;
+#define Z_LDC(o, r) case (o): Z80B_EACH(s.c = s.r); break;
+#define Z_LDD(o, r) case (o): Z80B_EACH(s.d = s.r); break;
+#define Z_LDE(o, r) case (o): Z80B_EACH(s.e = s.r); break;
+#define Z_LDH(o, r) case (o): Z80B_EACH(s.h = s.r); break;
+#define Z_LDL(o, r) case (o): Z80B_EACH(s.l = s.r); break;
+#define Z_LDN(o, r) case (o): Z80B_EACH(s.r = imm & 0xFFu); break;
+#define Z_ADD(o, r) case (o): Z80B_EACH(z_add(s, s.r)); break;
+#define Z_ADC(o, r) case (o): Z80B_EACH(z_adc(s, s.r)); break;
+#define Z_SUB(o, r) case (o): Z80B_EACH(z_sub(s, s.r)); break;
+#define Z_SBC(o, r) case (o): Z80B_EACH(z_sbc(s, s.r)); break;
+#define Z_AND(o, r) case (o): Z80B_EACH(z_and(s, s.r)); break;
+#define Z_XOR(o, r) case (o): Z80B_EACH(z_xor(s, s.r)); break;
+#define Z_OR(o, r) case (o): Z80B_EACH(z_or(s, s.r)); break;
+#define Z_CP(o, r) case (o): Z80B_EACH(z_cp(s, s.r)); break;
+#define Z_INC(o, r) case (o): Z80B_EACH(z_inc(s, s.r)); break;
+#define Z_DEC(o, r) case (o): Z80B_EACH(z_dec(s, s.r)); break;
+#define Z_RLC(o, r) case (o): Z80B_EACH(s.r = z_rlc(s, s.r)); break;
+#define Z_RRC(o, r) case (o): Z80B_EACH(s.r = z_rrc(s, s.r)); break;
+#define Z_RL(o, r) case (o): Z80B_EACH(s.r = z_rl(s, s.r)); break;
+#define Z_RR(o, r) case (o): Z80B_EACH(s.r = z_rr(s, s.r)); break;
+#define Z_SLA(o, r) case (o): Z80B_EACH(s.r = z_sla(s, s.r)); break;
+#define Z_SRA(o, r) case (o): Z80B_EACH(s.r = z_sra(s, s.r)); break;
+#define Z_SRL(o, r) case (o): Z80B_EACH(s.r = z_srl(s, s.r)); break;
+#define Z_SLL(o, r) case (o): Z80B_EACH(s.r = z_sll(s, s.r)); break;
+#define Z_BIT(o, r) case (o): Z80B_EACH(z_bit(s, s.r, uint32_t(((o) - BIT_0_A) / 7))); break;
+#define Z_RES(o, r) case (o): Z80B_EACH(s.r &= ~(1u << (((o) - RES_0_A) / 7))); break;
+#define Z_SET(o, r) case (o): Z80B_EACH(s.r |= 1u << (((o) - SET_0_A) / 7)); break;
+
+// Executes one instruction on K states at once: one dispatch on the opcode,
+// then the case body for each state (the "vectors per lane" of a sweep).
+// Opcodes outside 0..454 leave the states alone (the host rejects them
+// before any launch).
+template <int K>
+Z80_HD void z_stepK(Z80S (&S)[K], uint32_t op, uint32_t imm) {
   switch (op) {
     Z80B_S7(Z_LDA, LD_A_B)
     Z80B_R7(Z_LDB, LD_B_A)
@@ -220,58 +231,43 @@ Z80_HD void z_step(Z80S& s, uint32_t op, uint32_t imm) {
     Z80B_R7(Z_LDL, LD_L_A)
     Z80B_R7(Z_LDN, LD_A_N)
     Z80B_S7(Z_ADD, ADD_A_B)
-    case ADD_A_N: z_add(s, imm & 0xFFu); break;
+    case ADD_A_N: Z80B_EACH(z_add(s, imm & 0xFFu)); break;
     Z80B_S7(Z_ADC, ADC_A_B)
-    case ADC_A_N: z_adc(s, imm & 0xFFu); break;
+    case ADC_A_N: Z80B_EACH(z_adc(s, imm & 0xFFu)); break;
     Z80B_S7(Z_SUB, SUB_B)
-    case SUB_N: z_sub(s, imm & 0xFFu); break;
+    case SUB_N: Z80B_EACH(z_sub(s, imm & 0xFFu)); break;
     Z80B_S7(Z_SBC, SBC_A_B)
-    case SBC_A_N: z_sbc(s, imm & 0xFFu); break;
+    case SBC_A_N: Z80B_EACH(z_sbc(s, imm & 0xFFu)); break;
     Z80B_S7(Z_AND, AND_B)
-    case AND_N: z_and(s, imm & 0xFFu); break;
+    case AND_N: Z80B_EACH(z_and(s, imm & 0xFFu)); break;
     Z80B_S7(Z_XOR, XOR_B)
-    case XOR_N: z_xor(s, imm & 0xFFu); break;
+    case XOR_N: Z80B_EACH(z_xor(s, imm & 0xFFu)); break;
     Z80B_S7(Z_OR, OR_B)
-    case OR_N: z_or(s, imm & 0xFFu); break;
+    case OR_N: Z80B_EACH(z_or(s, imm & 0xFFu)); break;
     Z80B_S7(Z_CP, CP_B)
-    case CP_N: z_cp(s, imm & 0xFFu); break;
+    case CP_N: Z80B_EACH(z_cp(s, imm & 0xFFu)); break;
     Z80B_R7(Z_INC, INC_A)
     Z80B_R7(Z_DEC, DEC_A)
     case RLCA:
-      s.a = ((s.a << 1) | (s.a >> 7)) & 0xFFu;
-      s.f = (s.f & 0xC4u) | (s.a & 0x29u);
+      Z80B_EACH(s.a = ((s.a << 1) | (s.a >> 7)) & 0xFFu; s.f = (s.f & 0xC4u) | (s.a & 0x29u));
       break;
-    case RRCA: {
-      uint32_t c = s.a & 1u;
-      s.a = ((s.a >> 1) | (s.a << 7)) & 0xFFu;
-      s.f = (s.f & 0xC4u) | c | (s.a & 0x28u);
+    case RRCA:
+      Z80B_EACH(const uint32_t c = s.a & 1u; s.a = ((s.a >> 1) | (s.a << 7)) & 0xFFu;
+                s.f = (s.f & 0xC4u) | c | (s.a & 0x28u));
       break;
-    }
-    case RLA: {
-      uint32_t old = s.a;
-      s.a = ((s.a << 1) | (s.f & 1u)) & 0xFFu;
-      s.f = (s.f & 0xC4u) | (s.a & 0x28u) | (old >> 7);
+    case RLA:
+      Z80B_EACH(const uint32_t old = s.a; s.a = ((s.a << 1) | (s.f & 1u)) & 0xFFu;
+                s.f = (s.f & 0xC4u) | (s.a & 0x28u) | (old >> 7));
       break;
-    }
-    case RRA: {
-      uint32_t old = s.a;
-      s.a = (s.a >> 1) | ((s.f & 1u) << 7);
-      s.f = (s.f & 0xC4u) | (s.a & 0x28u) | (old & 1u);
+    case RRA:
+      Z80B_EACH(const uint32_t old = s.a; s.a = (s.a >> 1) | ((s.f & 1u) << 7);
+                s.f = (s.f & 0xC4u) | (s.a & 0x28u) | (old & 1u));
       break;
-    }
-    case DAA: z_daa(s); break;
-    case CPL:
-      s.a ^= 0xFFu;
-      s.f = (s.f & 0xC5u) | (s.a & 0x28u) | 0x12u;
-      break;
-    case SCF: s.f = (s.f & 0xC4u) | (s.a & 0x28u) | 1u; break;
-    case CCF: s.f = (s.f & 0xC4u) | (s.a & 0x28u) | ((s.f & 1u) ? 0x10u : 1u); break;
-    case NEG: {
-      uint32_t v = s.a;
-      s.a = 0;
-      z_sub(s, v);
-      break;
-    }
+    case DAA: Z80B_EACH(z_daa(s)); break;
+    case CPL: Z80B_EACH(s.a ^= 0xFFu; s.f = (s.f & 0xC5u) | (s.a & 0x28u) | 0x12u); break;
+    case SCF: Z80B_EACH(s.f = (s.f & 0xC4u) | (s.a & 0x28u) | 1u); break;
+    case CCF: Z80B_EACH(s.f = (s.f & 0xC4u) | (s.a & 0x28u) | ((s.f & 1u) ? 0x10u : 1u)); break;
+    case NEG: Z80B_EACH(const uint32_t v = s.a; s.a = 0; z_sub(s, v)); break;
     case NOP: break;
     Z80B_R7(Z_RLC, RLC_A)
     Z80B_R7(Z_RRC, RRC_A)
@@ -287,86 +283,90 @@ Z80_HD void z_step(Z80S& s, uint32_t op, uint32_t imm) {
     Z80B_R7(Z_RES, RES_4_A) Z80B_R7(Z_RES, RES_5_A) Z80B_R7(Z_RES, RES_6_A) Z80B_R7(Z_RES, RES_7_A)
     Z80B_R7(Z_SET, SET_0_A) Z80B_R7(Z_SET, SET_1_A) Z80B_R7(Z_SET, SET_2_A) Z80B_R7(Z_SET, SET_3_A)
     Z80B_R7(Z_SET, SET_4_A) Z80B_R7(Z_SET, SET_5_A) Z80B_R7(Z_SET, SET_6_A) Z80B_R7(Z_SET, SET_7_A)
-    case INC_BC: { uint32_t v = (((s.b << 8) | s.c) + 1u) & 0xFFFFu; s.b = v >> 8; s.c = v & 0xFFu; break; }
-    case INC_DE: { uint32_t v = (((s.d << 8) | s.e) + 1u) & 0xFFFFu; s.d = v >> 8; s.e = v & 0xFFu; break; }
-    case INC_HL: { uint32_t v = (((s.h << 8) | s.l) + 1u) & 0xFFFFu; s.h = v >> 8; s.l = v & 0xFFu; break; }
-    case INC_SP: s.sp = (s.sp + 1u) & 0xFFFFu; break;
-    case DEC_BC: { uint32_t v = (((s.b << 8) | s.c) - 1u) & 0xFFFFu; s.b = v >> 8; s.c = v & 0xFFu; break; }
-    case DEC_DE: { uint32_t v = (((s.d << 8) | s.e) - 1u) & 0xFFFFu; s.d = v >> 8; s.e = v & 0xFFu; break; }
-    case DEC_HL: { uint32_t v = (((s.h << 8) | s.l) - 1u) & 0xFFFFu; s.h = v >> 8; s.l = v & 0xFFu; break; }
-    case DEC_SP: s.sp = (s.sp - 1u) & 0xFFFFu; break;
-    case ADD_HL_BC: z_addhl(s, (s.b << 8) | s.c); break;
-    case ADD_HL_DE: z_addhl(s, (s.d << 8) | s.e); break;
-    case ADD_HL_HL: z_addhl(s, (s.h << 8) | s.l); break;
-    case ADD_HL_SP: z_addhl(s, s.sp); break;
-    case EX_DE_HL: {
-      uint32_t d = s.d, e = s.e;
-      s.d = s.h; s.e = s.l; s.h = d; s.l = e;
+    case INC_BC: Z80B_EACH(const uint32_t v = (((s.b << 8) | s.c) + 1u) & 0xFFFFu; s.b = v >> 8; s.c = v & 0xFFu); break;
+    case INC_DE: Z80B_EACH(const uint32_t v = (((s.d << 8) | s.e) + 1u) & 0xFFFFu; s.d = v >> 8; s.e = v & 0xFFu); break;
+    case INC_HL: Z80B_EACH(const uint32_t v = (((s.h << 8) | s.l) + 1u) & 0xFFFFu; s.h = v >> 8; s.l = v & 0xFFu); break;
+    case INC_SP: Z80B_EACH(s.sp = (s.sp + 1u) & 0xFFFFu); break;
+    case DEC_BC: Z80B_EACH(const uint32_t v = (((s.b << 8) | s.c) - 1u) & 0xFFFFu; s.b = v >> 8; s.c = v & 0xFFu); break;
+    case DEC_DE: Z80B_EACH(const uint32_t v = (((s.d << 8) | s.e) - 1u) & 0xFFFFu; s.d = v >> 8; s.e = v & 0xFFu); break;
+    case DEC_HL: Z80B_EACH(const uint32_t v = (((s.h << 8) | s.l) - 1u) & 0xFFFFu; s.h = v >> 8; s.l = v & 0xFFu); break;
+    case DEC_SP: Z80B_EACH(s.sp = (s.sp - 1u) & 0xFFFFu); break;
+    case ADD_HL_BC: Z80B_EACH(z_addhl(s, (s.b << 8) | s.c)); break;
+    case ADD_HL_DE: Z80B_EACH(z_addhl(s, (s.d << 8) | s.e)); break;
+    case ADD_HL_HL: Z80B_EACH(z_addhl(s, (s.h << 8) | s.l)); break;
+    case ADD_HL_SP: Z80B_EACH(z_addhl(s, s.sp)); break;
+    case EX_DE_HL:
+      Z80B_EACH(const uint32_t d = s.d; const uint32_t e = s.e; s.d = s.h; s.e = s.l; s.h = d; s.l = e);
       break;
-    }
-    case LD_SP_HL: s.sp = (s.h << 8) | s.l; break;
-    case LD_BC_NN: s.b = (imm >> 8) & 0xFFu; s.c = imm & 0xFFu; break;
-    case LD_DE_NN: s.d = (imm >> 8) & 0xFFu; s.e = imm & 0xFFu; break;
-    case LD_HL_NN: s.h = (imm >> 8) & 0xFFu; s.l = imm & 0xFFu; break;
-    case LD_SP_NN: s.sp = imm & 0xFFFFu; break;
-    case ADC_HL_BC: z_adchl(s, (s.b << 8) | s.c); break;
-    case ADC_HL_DE: z_adchl(s, (s.d << 8) | s.e); break;
-    case ADC_HL_HL: z_adchl(s, (s.h << 8) | s.l); break;
-    case ADC_HL_SP: z_adchl(s, s.sp); break;
-    case SBC_HL_BC: z_sbchl(s, (s.b << 8) | s.c); break;
-    case SBC_HL_DE: z_sbchl(s, (s.d << 8) | s.e); break;
-    case SBC_HL_HL: z_sbchl(s, (s.h << 8) | s.l); break;
-    case SBC_HL_SP: z_sbchl(s, s.sp); break;
+    case LD_SP_HL: Z80B_EACH(s.sp = (s.h << 8) | s.l); break;
+    case LD_BC_NN: Z80B_EACH(s.b = (imm >> 8) & 0xFFu; s.c = imm & 0xFFu); break;
+    case LD_DE_NN: Z80B_EACH(s.d = (imm >> 8) & 0xFFu; s.e = imm & 0xFFu); break;
+    case LD_HL_NN: Z80B_EACH(s.h = (imm >> 8) & 0xFFu; s.l = imm & 0xFFu); break;
+    case LD_SP_NN: Z80B_EACH(s.sp = imm & 0xFFFFu); break;
+    case ADC_HL_BC: Z80B_EACH(z_adchl(s, (s.b << 8) | s.c)); break;
+    case ADC_HL_DE: Z80B_EACH(z_adchl(s, (s.d << 8) | s.e)); break;
+    case ADC_HL_HL: Z80B_EACH(z_adchl(s, (s.h << 8) | s.l)); break;
+    case ADC_HL_SP: Z80B_EACH(z_adchl(s, s.sp)); break;
+    case SBC_HL_BC: Z80B_EACH(z_sbchl(s, (s.b << 8) | s.c)); break;
+    case SBC_HL_DE: Z80B_EACH(z_sbchl(s, (s.d << 8) | s.e)); break;
+    case SBC_HL_HL: Z80B_EACH(z_sbchl(s, (s.h << 8) | s.l)); break;
+    case SBC_HL_SP: Z80B_EACH(z_sbchl(s, s.sp)); break;
     // memory ops on the single byte M (exec.go:883-1028)
-    case LD_A_HLI: s.a = s.m; break;
-    case LD_B_HLI: s.b = s.m; break;
-    case LD_C_HLI: s.c = s.m; break;
-    case LD_D_HLI: s.d = s.m; break;
-    case LD_E_HLI: s.e = s.m; break;
-    case LD_H_HLI: s.h = s.m; break;
-    case LD_L_HLI: s.l = s.m; break;
-    case LD_HLI_A: s.m = s.a; break;
-    case LD_HLI_B: s.m = s.b; break;
-    case LD_HLI_C: s.m = s.c; break;
-    case LD_HLI_D: s.m = s.d; break;
-    case LD_HLI_E: s.m = s.e; break;
-    case LD_HLI_H: s.m = s.h; break;
-    case LD_HLI_L: s.m = s.l; break;
-    case LD_HLI_N: s.m = imm & 0xFFu; break;
-    case LD_A_BCI: case LD_A_DEI: s.a = s.m; break;
-    case LD_BCI_A: case LD_DEI_A: s.m = s.a; break;
-    case ADD_A_HLI: z_add(s, s.m); break;
-    case ADC_A_HLI: z_adc(s, s.m); break;
-    case SUB_HLI: z_sub(s, s.m); break;
-    case SBC_A_HLI: z_sbc(s, s.m); break;
-    case AND_HLI: z_and(s, s.m); break;
-    case XOR_HLI: z_xor(s, s.m); break;
-    case OR_HLI: z_or(s, s.m); break;
-    case CP_HLI: z_cp(s, s.m); break;
-    case INC_HLI: z_inc(s, s.m); break;
-    case DEC_HLI: z_dec(s, s.m); break;
-    case RLC_HLI: s.m = z_rlc(s, s.m); break;
-    case RRC_HLI: s.m = z_rrc(s, s.m); break;
-    case RL_HLI: s.m = z_rl(s, s.m); break;
-    case RR_HLI: s.m = z_rr(s, s.m); break;
-    case SLA_HLI: s.m = z_sla(s, s.m); break;
-    case SRA_HLI: s.m = z_sra(s, s.m); break;
-    case SRL_HLI: s.m = z_srl(s, s.m); break;
-    case SLL_HLI: s.m = z_sll(s, s.m); break;
+    case LD_A_HLI: Z80B_EACH(s.a = s.m); break;
+    case LD_B_HLI: Z80B_EACH(s.b = s.m); break;
+    case LD_C_HLI: Z80B_EACH(s.c = s.m); break;
+    case LD_D_HLI: Z80B_EACH(s.d = s.m); break;
+    case LD_E_HLI: Z80B_EACH(s.e = s.m); break;
+    case LD_H_HLI: Z80B_EACH(s.h = s.m); break;
+    case LD_L_HLI: Z80B_EACH(s.l = s.m); break;
+    case LD_HLI_A: Z80B_EACH(s.m = s.a); break;
+    case LD_HLI_B: Z80B_EACH(s.m = s.b); break;
+    case LD_HLI_C: Z80B_EACH(s.m = s.c); break;
+    case LD_HLI_D: Z80B_EACH(s.m = s.d); break;
+    case LD_HLI_E: Z80B_EACH(s.m = s.e); break;
+    case LD_HLI_H: Z80B_EACH(s.m = s.h); break;
+    case LD_HLI_L: Z80B_EACH(s.m = s.l); break;
+    case LD_HLI_N: Z80B_EACH(s.m = imm & 0xFFu); break;
+    case LD_A_BCI: case LD_A_DEI: Z80B_EACH(s.a = s.m); break;
+    case LD_BCI_A: case LD_DEI_A: Z80B_EACH(s.m = s.a); break;
+    case ADD_A_HLI: Z80B_EACH(z_add(s, s.m)); break;
+    case ADC_A_HLI: Z80B_EACH(z_adc(s, s.m)); break;
+    case SUB_HLI: Z80B_EACH(z_sub(s, s.m)); break;
+    case SBC_A_HLI: Z80B_EACH(z_sbc(s, s.m)); break;
+    case AND_HLI: Z80B_EACH(z_and(s, s.m)); break;
+    case XOR_HLI: Z80B_EACH(z_xor(s, s.m)); break;
+    case OR_HLI: Z80B_EACH(z_or(s, s.m)); break;
+    case CP_HLI: Z80B_EACH(z_cp(s, s.m)); break;
+    case INC_HLI: Z80B_EACH(z_inc(s, s.m)); break;
+    case DEC_HLI: Z80B_EACH(z_dec(s, s.m)); break;
+    case RLC_HLI: Z80B_EACH(s.m = z_rlc(s, s.m)); break;
+    case RRC_HLI: Z80B_EACH(s.m = z_rrc(s, s.m)); break;
+    case RL_HLI: Z80B_EACH(s.m = z_rl(s, s.m)); break;
+    case RR_HLI: Z80B_EACH(s.m = z_rr(s, s.m)); break;
+    case SLA_HLI: Z80B_EACH(s.m = z_sla(s, s.m)); break;
+    case SRA_HLI: Z80B_EACH(s.m = z_sra(s, s.m)); break;
+    case SRL_HLI: Z80B_EACH(s.m = z_srl(s, s.m)); break;
+    case SLL_HLI: Z80B_EACH(s.m = z_sll(s, s.m)); break;
     case BIT_0_HLI: case BIT_1_HLI: case BIT_2_HLI: case BIT_3_HLI:
     case BIT_4_HLI: case BIT_5_HLI: case BIT_6_HLI: case BIT_7_HLI:
-      z_bit(s, s.m, op - BIT_0_HLI);
+      Z80B_EACH(z_bit(s, s.m, op - BIT_0_HLI));
       break;
     case RES_0_HLI: case RES_1_HLI: case RES_2_HLI: case RES_3_HLI:
     case RES_4_HLI: case RES_5_HLI: case RES_6_HLI: case RES_7_HLI:
-      s.m &= ~(1u << (op - RES_0_HLI));
+      Z80B_EACH(s.m &= ~(1u << (op - RES_0_HLI)));
       break;
     case SET_0_HLI: case SET_1_HLI: case SET_2_HLI: case SET_3_HLI:
     case SET_4_HLI: case SET_5_HLI: case SET_6_HLI: case SET_7_HLI:
-      s.m |= 1u << (op - SET_0_HLI);
+      Z80B_EACH(s.m |= 1u << (op - SET_0_HLI));
       break;
     default: break;
   }
+}
+
+Z80_HD void z_step(Z80S& s, uint32_t op, uint32_t imm) {
+  Z80S S[1] = {s};
+  z_stepK<1>(S, op, imm);
+  s = S[0];
 }
 
 Z80_HD void z_run(Z80S& s, const uint32_t* prog, int n) {

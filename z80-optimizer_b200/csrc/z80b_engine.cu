@@ -96,6 +96,8 @@ struct z80b_ctx {
   DBuf v_tgt, v_cand, v_tl, v_cl, v_dead, v_out, v_fd, v_in, v_outs;
   uint64_t n_rules_dev = 0;
   uint32_t launches = 0;
+  int exh_k = 4;              // ExhaustiveCheck states per lane per dispatch (z80b_set_option)
+  int chunk_blocks = 32;      // A-blocks per ExhaustiveCheck work chunk
 };
 
 namespace {
@@ -393,6 +395,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, uint32_t mode, z80b_stats* 
     R.npairs = ctx->npairs.as<uint32_t>();
     R.counter = ctx->counter.as<unsigned long long>();
     R.states = ctx->states.as<unsigned long long>();
+    R.chunk_blocks = uint32_t(ctx->chunk_blocks);
     if (nsurv) {
       for (;;) {
         CK(cudaMemsetAsync(R.npairs, 0, 4, s));
@@ -412,7 +415,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, uint32_t mode, z80b_stats* 
         CK(cudaMemsetAsync(R.counter, 0, 8, s));
         trace("round %u: %llu chunks", rounds, lastb + lastn);
         int ke = kbegin(ctx, 1);
-        launch_exhaustive(T, P, R, np, lastb + lastn, s);
+        launch_exhaustive(T, P, R, np, lastb + lastn, ctx->exh_k, s);
         kend(ctx, ke);
         CKR(check_launch(ctx, "exhaustive"));
         launch_round_resolve(R, np, q, L, s);
@@ -453,6 +456,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, uint32_t mode, z80b_stats* 
     R.npairs = ctx->npairs.as<uint32_t>();
     R.counter = ctx->counter.as<unsigned long long>();
     R.states = ctx->states.as<unsigned long long>();
+    R.chunk_blocks = uint32_t(ctx->chunk_blocks);
     if (S) {
       launch_surv_targets(q, n, ctx->surv_target.as<uint32_t>(), s);
       CKR(check_launch(ctx, "surv_targets"));
@@ -475,7 +479,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, uint32_t mode, z80b_stats* 
         CK(cudaStreamSynchronize(s));
         CK(cudaMemsetAsync(R.counter, 0, 8, s));
         int ke = kbegin(ctx, 1);
-        launch_exhaustive(T, P, R, np, lastb + lastn, s);
+        launch_exhaustive(T, P, R, np, lastb + lastn, ctx->exh_k, s);
         kend(ctx, ke);
         CKR(check_launch(ctx, "exhaustive"));
         launch_rule_count_all(R, np, ctx->flag.as<uint32_t>(), s);
@@ -871,7 +875,7 @@ int z80b_verify_pairs(z80b_ctx* ctx, const uint32_t* tgt, const uint8_t* tlens, 
       pr[i].nblocks = w.states / 256;
       pr[i].keepF = uint8_t(~(dead ? dead[i] : 0u));
       pr[i].keepR = 0x3F;
-      unsigned long long c = (pr[i].nblocks + 31) / 32;
+      unsigned long long c = (pr[i].nblocks + ctx->chunk_blocks - 1) / uint64_t(ctx->chunk_blocks);
       nch[i] = c > 65536 ? 65536 : c;
       cb[i] = tot;
       tot += nch[i];
@@ -891,7 +895,7 @@ int z80b_verify_pairs(z80b_ctx* ctx, const uint32_t* tgt, const uint8_t* tlens, 
     R.rejected = ctx->rejected.as<uint32_t>();
     R.counter = ctx->counter.as<unsigned long long>();
     R.states = ctx->states.as<unsigned long long>();
-    launch_exhaustive(T, P, R, n, tot, s);
+    launch_exhaustive(T, P, R, n, tot, ctx->exh_k, s);
     CKR(check_launch(ctx, "exhaustive"));
     std::vector<uint32_t> rej(n);
     CK(cudaMemcpyAsync(rej.data(), ctx->rejected.p, 4ull * n, cudaMemcpyDeviceToHost, s));
@@ -901,6 +905,69 @@ int z80b_verify_pairs(z80b_ctx* ctx, const uint32_t* tgt, const uint8_t* tlens, 
   }
   std::memcpy(out, res.data(), n);
   if (flagdiff) std::memcpy(flagdiff, fd.data(), n);
+  return Z80B_OK;
+}
+
+int z80b_set_option(z80b_ctx* ctx, int option, int value) {
+  if (!ctx) return Z80B_EINVAL;
+  switch (option) {
+    case Z80B_OPT_EXH_LANE_STATES:
+      if (value != 1 && value != 2 && value != 4 && value != 8)
+        return fail(ctx, Z80B_EINVAL, "lane states must be 1, 2, 4 or 8");
+      ctx->exh_k = value;
+      return Z80B_OK;
+    case Z80B_OPT_EXH_CHUNK_BLOCKS:
+      if (value < 1 || value > 4096) return fail(ctx, Z80B_EINVAL, "chunk blocks must be 1..4096");
+      ctx->chunk_blocks = value;
+      return Z80B_OK;
+  }
+  return fail(ctx, Z80B_EINVAL, "unknown option %d", option);
+}
+
+int z80b_get_option(const z80b_ctx* ctx, int option, int* value) {
+  if (!ctx || !value) return Z80B_EINVAL;
+  switch (option) {
+    case Z80B_OPT_EXH_LANE_STATES: *value = ctx->exh_k; return Z80B_OK;
+    case Z80B_OPT_EXH_CHUNK_BLOCKS: *value = ctx->chunk_blocks; return Z80B_OK;
+  }
+  return Z80B_EINVAL;
+}
+
+// Tries every (lane states, chunk size) pair on the sample job and keeps the
+// fastest (device time of the whole pipeline).
+int z80b_autotune(z80b_ctx* ctx, const z80b_job* sample, z80b_tune_result* out) {
+  if (!ctx) return Z80B_EINVAL;
+  CKR(validate_job(ctx, sample));
+  if (sample->path != Z80B_PATH_BATCHED) return fail(ctx, Z80B_EINVAL, "autotune runs the batched path");
+  cudaSetDevice(ctx->device);
+  DevTargets T;
+  CKR(upload_targets(ctx, ctx->staged, sample, &T, true));
+  const int ks[4] = {1, 2, 4, 8}, cs[4] = {8, 32, 128, 512};
+  double best = 1e300;
+  int bk = ctx->exh_k, bc = ctx->chunk_blocks;
+  z80b_tune_result r{};
+  for (int a = 0; a < 4; a++)
+    for (int b = 0; b < 4; b++) {
+      ctx->exh_k = ks[a];
+      ctx->chunk_blocks = cs[b];
+      z80b_stats st{};
+      uint64_t nr = 0;
+      CKR(run_pipeline(ctx, T, sample->mode, &st, &nr));  // warm
+      std::memset(&st, 0, sizeof st);
+      CKR(run_pipeline(ctx, T, sample->mode, &st, &nr));
+      r.ms[a][b] = st.device_ms;
+      if (st.device_ms < best) {
+        best = st.device_ms;
+        bk = ks[a];
+        bc = cs[b];
+      }
+    }
+  ctx->exh_k = bk;
+  ctx->chunk_blocks = bc;
+  r.lane_states = bk;
+  r.chunk_blocks = bc;
+  if (out) *out = r;
+  trace("autotune: lane states %d, chunk blocks %d (%.3f ms)", bk, bc, best);
   return Z80B_OK;
 }
 

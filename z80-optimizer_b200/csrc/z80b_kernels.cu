@@ -104,10 +104,11 @@ __device__ __forceinline__ unsigned long long sweep_blocks(uint32_t reads) {
   if (n <= 2 && !sp) return 2ull << (8 * n);
   return (2ull << (5 * n)) * (sp ? 16ull : 1ull);
 }
-constexpr unsigned long long kChunkBlocks = 32;  // 8192 states
 constexpr unsigned long long kMaxChunks = 65536;
-__device__ __forceinline__ unsigned long long chunks_for(unsigned long long nb) {
-  unsigned long long c = (nb + kChunkBlocks - 1) / kChunkBlocks;
+// Work chunks of a sweep: cb A-blocks each (cb is the tuning option), at
+// most kMaxChunks per pair.
+__device__ __forceinline__ unsigned long long chunks_for(unsigned long long nb, uint32_t cb) {
+  unsigned long long c = (nb + cb - 1) / cb;
   return c > kMaxChunks ? kMaxChunks : c;
 }
 
@@ -381,7 +382,7 @@ __global__ void k_round_build(DevTargets T, DevPool P, QCOut q, Lanes L, RoundBu
       uint32_t p = base + __popc(b & lanemask_lt());
       R.pairs[p] = pr[kind];
       R.pair_src[p] = src[kind];
-      R.nchunks[p] = chunks_for(pr[kind].nblocks);
+      R.nchunks[p] = chunks_for(pr[kind].nblocks, R.chunk_blocks);
       R.rejected[p] = 0;
     }
   }
@@ -415,13 +416,18 @@ __global__ void k_pairs_from_survivors(DevTargets T, DevPool P, QCOut q, const u
     uint32_t p = base + __popc(b & lanemask_lt());
     R.pairs[p] = pr;
     R.pair_src[p] = i;
-    R.nchunks[p] = chunks_for(pr.nblocks);
+    R.nchunks[p] = chunks_for(pr.nblocks, R.chunk_blocks);
     R.rejected[p] = 0;
   }
 }
 
-__global__ void __launch_bounds__(kBlock) k_exhaustive(DevTargets T, DevPool P, RoundBuf R, uint32_t npairs,
+// K = states per lane per dispatch ("vectors per lane").  One warp
+// iteration covers 32*K values of A; an A-block (256 states) takes 8/K
+// iterations.
+template <int K>
+__global__ void __launch_bounds__(kBlock, K <= 4 ? 2 : 1) k_exhaustive(DevTargets T, DevPool P, RoundBuf R, uint32_t npairs,
                                                        unsigned long long total) {
+  static_assert(K == 1 || K == 2 || K == 4 || K == 8, "K divides 8");
   const unsigned lane = lane_id();
   unsigned long long my_states = 0;
   for (;;) {
@@ -454,6 +460,7 @@ __global__ void __launch_bounds__(kBlock) k_exhaustive(DevTargets T, DevPool P, 
     uint32_t pw = 0;
     if (lane < tl) pw = T.insn[(size_t)pr.target * T.stride + lane];
     else if (lane < tl + cl) pw = P.insn[(size_t)pr.cand * P.stride + (lane - tl)];
+    const int nsteps = int(tl + cl);
 
     // sweep shape (verifier.go:428-476): extra registers in B,C,D,E,H,L,M order
     const uint32_t ext = pr.reads & (kRegB | kRegC | kRegD | kRegE | kRegH | kRegL | kRegM);
@@ -461,7 +468,6 @@ __global__ void __launch_bounds__(kBlock) k_exhaustive(DevTargets T, DevPool P, 
     const bool spw = (pr.reads & kRegSP) != 0;
     const bool reduced = spw || nx > 2;
     const int fw = reduced ? 5 : 8;  // bits per swept register in the block index
-    // slot of each register (-1 = not swept)
     int slot[7];
     {
       int k2 = 0;
@@ -469,7 +475,11 @@ __global__ void __launch_bounds__(kBlock) k_exhaustive(DevTargets T, DevPool P, 
 #pragma unroll
       for (int r = 0; r < 7; r++) slot[r] = (ext & bits[r]) ? k2++ : -1;
     }
-    const Keep keep = make_keep(pr.keepF, pr.keepR, true);
+    // compared bytes of the packed words (A F B C / D E H L / SP M)
+    const uint32_t keep0 = 0xFFu | (uint32_t(pr.keepF) << 8) | ((pr.keepR & 1u) ? 0xFF0000u : 0u) |
+                           ((pr.keepR & 2u) ? 0xFF000000u : 0u);
+    const uint32_t keep1 = ((pr.keepR & 4u) ? 0xFFu : 0u) | ((pr.keepR & 8u) ? 0xFF00u : 0u) |
+                           ((pr.keepR & 16u) ? 0xFF0000u : 0u) | ((pr.keepR & 32u) ? 0xFF000000u : 0u);
 
     bool bad = false;
     // Block index fields, fastest first: SP (reduced sweeps), the swept
@@ -487,11 +497,11 @@ __global__ void __launch_bounds__(kBlock) k_exhaustive(DevTargets T, DevPool P, 
       }
       uint32_t fieldv[7];
 #pragma unroll
-      for (int k = 6; k >= 0; k--) {
-        fieldv[k] = 0;
-        if (k < nx) {
-          const uint32_t f = uint32_t(rest) & (reduced ? 31u : 255u);
-          fieldv[k] = reduced ? c_rep[f] : f;
+      for (int f = 6; f >= 0; f--) {
+        fieldv[f] = 0;
+        if (f < nx) {
+          const uint32_t x = uint32_t(rest) & (reduced ? 31u : 255u);
+          fieldv[f] = reduced ? c_rep[x] : x;
           rest >>= fw;
         }
       }
@@ -501,21 +511,50 @@ __global__ void __launch_bounds__(kBlock) k_exhaustive(DevTargets T, DevPool P, 
       for (int r = 0; r < 7; r++) {
         uint32_t v = 0;
 #pragma unroll
-        for (int k = 0; k < 7; k++)
-          if (slot[r] == k) v = fieldv[k];
+        for (int f = 0; f < 7; f++)
+          if (slot[r] == f) v = fieldv[f];
         rv[r] = v;
       }
 #pragma unroll 1
-      for (uint32_t i = 0; i < 8; i++) {
-        Z80S x;
-        x.a = i * 32u + lane;
-        x.f = carry;
-        x.b = rv[0]; x.c = rv[1]; x.d = rv[2]; x.e = rv[3]; x.h = rv[4]; x.l = rv[5]; x.m = rv[6];
-        x.sp = sp;
-        Z80S y = x;
-        run_lanes(x, pw, 0, int(tl));
-        run_lanes(y, pw, int(tl), int(cl));
-        bad = bad || !eq_keep(x, y, keep);
+      for (uint32_t i = 0; i < 8u / K; i++) {
+        Z80S X[K];
+        uint32_t P0[K], P1[K], P2[K];
+        // one dispatch site: the candidate runs first; its output is packed
+        // into three words per state, the registers are re-initialised and
+        // the target runs on them
+#pragma unroll 1
+        for (int st = -1; st < nsteps; st++) {
+          if (st == -1 || st == int(cl)) {
+            if (st == int(cl)) {
+#pragma unroll
+              for (int q = 0; q < K; q++) {
+                P0[q] = X[q].a | (X[q].f << 8) | (X[q].b << 16) | (X[q].c << 24);
+                P1[q] = X[q].d | (X[q].e << 8) | (X[q].h << 16) | (X[q].l << 24);
+                P2[q] = X[q].sp | (X[q].m << 16);
+              }
+            }
+#pragma unroll
+            for (int q = 0; q < K; q++) {
+              X[q].a = (i * K + q) * 32u + lane;
+              X[q].f = carry;
+              X[q].b = rv[0]; X[q].c = rv[1]; X[q].d = rv[2]; X[q].e = rv[3];
+              X[q].h = rv[4]; X[q].l = rv[5]; X[q].m = rv[6];
+              X[q].sp = sp;
+            }
+            if (st == -1) continue;
+          }
+          // lanes tl.. hold the candidate, lanes 0.. the target
+          const int src = st < int(cl) ? int(tl) + st : st - int(cl);
+          const uint32_t w = __shfl_sync(kFull, pw, src);
+          z_stepK<K>(X, w & 0xFFFFu, w >> 16);
+        }
+#pragma unroll
+        for (int q = 0; q < K; q++) {
+          const uint32_t d0 = (X[q].a | (X[q].f << 8) | (X[q].b << 16) | (X[q].c << 24)) ^ P0[q];
+          const uint32_t d1 = (X[q].d | (X[q].e << 8) | (X[q].h << 16) | (X[q].l << 24)) ^ P1[q];
+          const uint32_t d2 = (X[q].sp | (X[q].m << 16)) ^ P2[q];
+          bad = bad || ((d0 & keep0) | (d1 & keep1) | d2) != 0;
+        }
       }
       my_states += 256;
       if (__any_sync(kFull, bad)) break;
@@ -749,16 +788,29 @@ void launch_pairs_from_survivors(const DevTargets& T, const DevPool& P, const QC
   if (!nsurv) return;
   k_pairs_from_survivors<<<grid_for(nsurv, 256), 256, 0, s>>>(T, P, q, midpass, nsurv, surv_target, R);
 }
-void launch_exhaustive(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
-                       unsigned long long total, cudaStream_t s) {
-  if (!npairs || !total) return;
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_exhaustive, kBlock, 0);
-  if (per_sm < 1) per_sm = 1;
+template <int K>
+void launch_exhaustive_k(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
+                         unsigned long long total, cudaStream_t s) {
+  static int per_sm = 0;
+  if (!per_sm) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_exhaustive<K>, kBlock, 0);
+    if (per_sm < 1) per_sm = 1;
+  }
   unsigned long long need = (total + (kBlock / 32) - 1) / (kBlock / 32);
   unsigned long long grid = (unsigned long long)dev_num_sms() * per_sm;
   if (grid > need) grid = need;
-  k_exhaustive<<<unsigned(grid), kBlock, 0, s>>>(T, P, R, npairs, total);
+  k_exhaustive<K><<<unsigned(grid), kBlock, 0, s>>>(T, P, R, npairs, total);
+}
+
+void launch_exhaustive(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
+                       unsigned long long total, int k, cudaStream_t s) {
+  if (!npairs || !total) return;
+  switch (k) {
+    case 1: launch_exhaustive_k<1>(T, P, R, npairs, total, s); break;
+    case 2: launch_exhaustive_k<2>(T, P, R, npairs, total, s); break;
+    case 8: launch_exhaustive_k<8>(T, P, R, npairs, total, s); break;
+    default: launch_exhaustive_k<4>(T, P, R, npairs, total, s); break;
+  }
 }
 void launch_round_resolve(const RoundBuf& R, uint32_t npairs, const QCOut& q, const Lanes& L,
                           cudaStream_t s) {

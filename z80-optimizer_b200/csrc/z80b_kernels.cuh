@@ -42,6 +42,7 @@ struct RoundBuf {
   uint32_t* npairs;                // device counter
   unsigned long long* counter;     // chunk dispenser
   unsigned long long* states;      // states verified (stat)
+  uint32_t chunk_blocks;           // A-blocks per work chunk
 };
 
 struct DevRule {
@@ -69,8 +70,9 @@ void launch_round_build(const DevTargets& T, const DevPool& P, const QCOut& q, c
 void launch_pairs_from_survivors(const DevTargets& T, const DevPool& P, const QCOut& q,
                                  const uint8_t* midpass, uint32_t nsurv, const uint32_t* surv_target,
                                  const RoundBuf& R, cudaStream_t s);
+// k = states per lane per dispatch: 1, 2, 4 or 8.
 void launch_exhaustive(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
-                       unsigned long long total_chunks, cudaStream_t s);
+                       unsigned long long total_chunks, int k, cudaStream_t s);
 void launch_round_resolve(const RoundBuf& R, uint32_t npairs, const QCOut& q, const Lanes& L,
                           cudaStream_t s);
 void launch_midcheck(const DevTargets& T, const DevPool& P, const uint32_t* surv,

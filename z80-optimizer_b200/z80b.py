@@ -97,7 +97,14 @@ EXPORTS = [
     "z80b_verify_pairs", "z80b_search", "z80b_stage_job", "z80b_run_staged", "z80b_fetch_rules",
     "z80b_op_info", "z80b_disasm_seq", "z80b_parse_assembly", "z80b_parse_dead_flags",
     "z80b_dead_flag_desc", "z80b_should_prune", "z80b_pool8", "z80b_rules_json",
+    "z80b_set_option", "z80b_get_option", "z80b_autotune", "z80b_enumerate",
 ]
+OPT_EXH_LANE_STATES, OPT_EXH_CHUNK_BLOCKS = 1, 2
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [("lane_states", ctypes.c_int), ("chunk_blocks", ctypes.c_int),
+                ("ms", (ctypes.c_double * 4) * 4)]
 
 
 def lib():
@@ -141,6 +148,11 @@ def lib():
         L.z80b_rules_json.argtypes = [ctypes.POINTER(Rule), ctypes.c_uint64, ctypes.c_char_p,
                                       ctypes.c_uint64]
         L.z80b_rules_json.restype = ctypes.c_longlong
+        L.z80b_set_option.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+        L.z80b_get_option.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        L.z80b_autotune.argtypes = [vp, ctypes.POINTER(Job), ctypes.POINTER(TuneResult)]
+        L.z80b_enumerate.restype = ctypes.c_uint64
+        L.z80b_enumerate.argtypes = [u32p, ctypes.c_uint32, ctypes.c_uint32, u32p, ctypes.c_uint64]
         _lib = L
     return _lib
 
@@ -357,6 +369,20 @@ class Context:
                 continue
             self._check(s)
             return [out[i] for i in range(nr.value)], st
+
+    def set_option(self, option, value):
+        self._check(lib().z80b_set_option(self._h, option, value))
+
+    def get_option(self, option):
+        v = ctypes.c_int()
+        self._check(lib().z80b_get_option(self._h, option, ctypes.byref(v)))
+        return v.value
+
+    def autotune(self, job):
+        """Tries every (lane states, chunk size) on a sample job; keeps the fastest."""
+        r = TuneResult()
+        self._check(lib().z80b_autotune(self._h, ctypes.byref(job), ctypes.byref(r)))
+        return r
 
     def stage(self, job):
         self._check(lib().z80b_stage_job(self._h, ctypes.byref(job)))
