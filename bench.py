@@ -219,8 +219,7 @@ def main():
     else:
         torch.cuda.set_device(0)
     # strong scaling: the fixed target set is split into contiguous shards
-    lo = len(allt) * rank // world
-    hi = len(allt) * (rank + 1) // world
+    lo, hi = workloads.shard_bounds(len(allt), rank, world)
     mine = np.ascontiguousarray(allt[lo:hi])
     ctx = z80b.Context(local if world > 1 else 0)
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")

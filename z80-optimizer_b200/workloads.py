@@ -138,3 +138,9 @@ def c2_subset(k, seed=0):
 
 def to_lists(arr):
     return [list(map(int, row)) for row in arr]
+
+
+def shard_bounds(n, rank, world):
+    """Contiguous shard [lo, hi) of n independent targets for one rank (the
+    reference splits its outer target loop the same way across processes)."""
+    return n * rank // world, n * (rank + 1) // world
