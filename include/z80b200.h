@@ -162,6 +162,30 @@ int z80b_stage_job(z80b_ctx* ctx, const z80b_job* job);
 int z80b_run_staged(z80b_ctx* ctx, uint64_t* n_rules, z80b_stats* stats);
 int z80b_fetch_rules(z80b_ctx* ctx, z80b_rule* out, uint64_t cap, uint64_t* n_rules);
 
+/* ---- allocation-free ExhaustiveCheck -------------------------------------- */
+/* No counterpart in the reference: an entry point for callers that cannot
+ * allocate device memory -- a process whose GPU memory is budgeted by another
+ * component, a latency path that must not pay for an allocation or for the
+ * synchronization cudaFree implies, a plugin host that forbids allocator
+ * calls.  It needs no context and allocates nothing (device or host heap):
+ * its device scratch is a fixed 288 KiB array inside the library that every
+ * GPU loading the library keeps until the process exits.
+ *
+ * ExhaustiveCheck[Masked] (pkg/search/verifier.go:159-171,642-654) of n
+ * (target, candidate) pairs given as host arrays (as z80b_verify_pairs):
+ * pass[i] = 1 when pair i is equivalent over the sweep, else 0.  At most
+ * Z80B_NOALLOC_MAX_PAIRS pairs per call (larger n returns Z80B_ECAPACITY and
+ * does nothing); stride <= 4.  stream may be NULL (default stream).
+ * The first call on a device sets the scratch up on that device (symbol
+ * address, lookup tables); make that first call before any stream capture.
+ * Every call reuses the same scratch: calls are serialized on the host, and
+ * calls from separate processes or other threads' streams whose GPU work
+ * overlaps would race on it. */
+#define Z80B_NOALLOC_MAX_PAIRS 4096
+int z80b_exhaustive_noalloc(int device, const uint32_t* tgt, const uint8_t* tlens, const uint32_t* cand,
+                            const uint8_t* clens, uint32_t stride, uint32_t n, const uint8_t* dead,
+                            uint8_t* pass, void* stream);
+
 /* ---- tuning -------------------------------------------------------------- */
 #define Z80B_OPT_EXH_LANE_STATES 1  /* ExhaustiveCheck states per lane per dispatch: 1, 2, 4, 8 */
 #define Z80B_OPT_EXH_CHUNK_BLOCKS 2 /* A-blocks (256 states) per work chunk: 1..4096 */
