@@ -159,10 +159,10 @@ def cpu_baseline(all_targets, dead, n_sample, seed=1):
 
 
 def auto_cpu_sample():
-    # a few core-seconds of oracle work on a typical sample; the sweep-size
-    # tail (true equivalences with 2^34-state reduced sweeps, ~1 in 100k
-    # targets) makes larger samples unbounded on the CPU
-    return 4000
+    # 16,000 targets (seed 1) are ~200 core-seconds of oracle work; the
+    # sweep-size tail (true equivalences with 2^34-state reduced sweeps, ~1 in
+    # 100k targets) makes much larger samples unbounded on the CPU
+    return 16000
 
 
 def main():
@@ -186,13 +186,13 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        n_sample = args.cpu_sample or max(1000, auto_cpu_sample() // 4)
+        n_sample = args.cpu_sample or auto_cpu_sample()
         workers = os.cpu_count() or 1
         times, checks = [], 0
         rng = np.random.default_rng(1)
+        idx = np.sort(rng.choice(len(allt), size=min(n_sample, len(allt)), replace=False))
+        sample = allt[idx]
         for i in range(args.warmup + args.steps):
-            idx = np.sort(rng.choice(len(allt), size=n_sample, replace=False))
-            sample = allt[idx]
             secs, _ = cpu_run(sample, dead, workers)
             if i >= args.warmup:
                 times.append(secs)
@@ -204,7 +204,8 @@ def main():
                 "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u8",
                 "data": "synthetic", "config": dict(workload, sample_targets_per_step=n_sample),
                 "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port",
-                                 "sample": f"{n_sample} targets per step, seeded draws by index"},
+                                 "sample": f"{len(sample)} targets per step (the same seeded draw by index, "
+                                           f"seed 1, every step)"},
                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return 0
@@ -323,12 +324,15 @@ def main():
     per_state = 3 * rl["ops_per_emulated_insn"] + rl["ops_per_state"]  # 2-insn target + 1-insn candidate
     achieved = states / args.steps * per_state / (exh_ms / args.steps / 1e3) / 1e12 if exh_ms else 0.0
     peak = rl["sms"] * rl["int32_lanes_per_sm"] * sm_mhz * 1e6 / 1e12
+    # DRAM bytes per sweep launch: the measured bytes per ExhaustiveCheck pair
+    # of an ncu capture (profiles/exhaustive_c2_traffic.txt) times this run's
+    # pairs per launch; the kernel reads per-pair records and sequences only
     traffic = None
     tf = os.path.join(ROOT, "profiles", "exhaustive_c2_traffic.txt")
-    if os.path.exists(tf):
+    if os.path.exists(tf) and stats_last is not None and stats_last.rounds:
         for line in open(tf):
-            if line.startswith("dram_bytes_per_launch:"):
-                traffic = float(line.split(":")[1])
+            if line.startswith("dram_bytes_per_pair:"):
+                traffic = float(line.split(":")[1]) * stats_last.exhaustive_pairs / stats_last.rounds
     roofline = {"bound": "issue", "kernel": "k_exhaustive", "achieved": achieved, "peak": peak,
                 "unit": "Tops/s (INT32 lane-ops)", "frac": achieved / peak if peak else None,
                 "traffic": traffic,

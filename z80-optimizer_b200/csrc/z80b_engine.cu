@@ -28,6 +28,7 @@
 #include "../../include/z80b200.h"
 #include "z80_tables.h"
 #include "z80b_kernels.cuh"
+#include "z80b_mulopt.cuh"
 
 using namespace z80b;
 
@@ -94,6 +95,7 @@ struct z80b_ctx {
   DBuf cub_tmp;
   DBuf hits, nhits, fpq;
   DBuf v_tgt, v_cand, v_tl, v_cl, v_dead, v_out, v_fd, v_in, v_outs;
+  DBuf mul_best, mul_stats;   // constant-multiply search: best key per K, counters
   uint64_t n_rules_dev = 0;
   uint32_t launches = 0;
   int exh_k = 4;              // ExhaustiveCheck states per lane per dispatch (z80b_set_option)
@@ -157,7 +159,7 @@ int scan(z80b_ctx* ctx, const T* in, T* out, uint32_t n) {
   CK(cub::DeviceScan::ExclusiveSum(nullptr, tmp, in, out, n, ctx->stream));
   CK(ctx->cub_tmp.ensure(tmp));
   CK(cub::DeviceScan::ExclusiveSum(ctx->cub_tmp.p, tmp, in, out, n, ctx->stream));
-  ctx->launches++;
+  ctx->launches += 2;  // tile-state init + scan kernel
   return Z80B_OK;
 }
 
@@ -1048,6 +1050,113 @@ int z80b_search(z80b_ctx* ctx, const z80b_job* job, z80b_rule* out, uint64_t cap
     CK(cudaStreamSynchronize(ctx->stream));
   }
   to_rules(ctx, dr, job->targets, job->target_lens, job->target_len, job->target_stride, job->mode, 0, out);
+  return Z80B_OK;
+}
+
+
+int z80b_mul_pool(int pool, int* n_ops, int* max_len, const char** names, int* tstates, int cap) {
+  if (pool < 0 || pool >= mul::kNumPools) return Z80B_EINVAL;
+  const mul::PoolInfo& pi = mul::pool_info(pool);
+  if (n_ops) *n_ops = pi.n;
+  if (max_len) *max_len = pi.max_len;
+  for (int i = 0; i < pi.n && i < cap; i++) {
+    if (names) names[i] = pi.names[i];
+    if (tstates) tstates[i] = pi.tstates[i];
+  }
+  return Z80B_OK;
+}
+
+int z80b_mul_search(z80b_ctx* ctx, int pool, uint8_t init_b, uint8_t init_c, uint8_t init_f, int min_len,
+                    int max_len, const int32_t* ks, uint32_t n_k, z80b_mul_result* out, z80b_mul_stats* stats) {
+  if (!ctx) return Z80B_EINVAL;
+  if (pool < 0 || pool >= mul::kNumPools) return fail(ctx, Z80B_EINVAL, "unknown pool %d", pool);
+  const mul::PoolInfo& pi = mul::pool_info(pool);
+  if (min_len < 1 || max_len < min_len || max_len > pi.max_len)
+    return fail(ctx, Z80B_EINVAL, "lengths %d..%d outside 1..%d", min_len, max_len, pi.max_len);
+  std::vector<int> kl;
+  if (ks) {
+    for (uint32_t i = 0; i < n_k; i++) {
+      if (ks[i] < 2 || ks[i] > 255) return fail(ctx, Z80B_EINVAL, "constant %d outside 2..255", ks[i]);
+      kl.push_back(ks[i]);
+    }
+  } else {
+    for (int k = 2; k <= 255; k++) kl.push_back(k);
+  }
+  if (!kl.empty() && !out) return fail(ctx, Z80B_EINVAL, "null output");
+  cudaSetDevice(ctx->device);
+  int sms = 0;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+  CK(ctx->mul_best.ensure(256 * sizeof(unsigned long long)));
+  CK(ctx->mul_stats.ensure(sizeof(mul::LenStats)));
+  mul::SearchArgs a{};
+  a.pool = pool;
+  a.b = init_b;
+  a.c = init_c;
+  a.f = init_f;
+  a.min_len = min_len;
+  a.max_len = max_len;
+  for (int k : kl) a.want[k >> 5] |= 1u << (k & 31);
+  for (size_t i = 0; i < kl.size(); i++) {
+    std::memset(&out[i], 0, sizeof out[i]);
+    out[i].k = kl[i];
+  }
+  z80b_mul_stats st{};
+  int found_len[256] = {};
+  unsigned long long found_key[256] = {};
+  double nl = 1;
+  for (int i = 0; i < min_len - 1; i++) nl *= pi.n;
+  for (int len = min_len; len <= max_len; len++) {
+    nl *= pi.n;
+    bool any = false;
+    for (int w = 0; w < 8; w++) any = any || a.want[w];
+    if (!any) break;
+    CK(cudaMemsetAsync(ctx->mul_best.p, 0xFF, 256 * sizeof(unsigned long long), ctx->stream));
+    CK(cudaMemsetAsync(ctx->mul_stats.p, 0, sizeof(mul::LenStats), ctx->stream));
+    Timer tm{ctx, 0, 1};
+    tm.start();
+    cudaError_t e = mul::launch_length(a, len, ctx->mul_best.as<unsigned long long>(),
+                                       ctx->mul_stats.as<mul::LenStats>(), sms, ctx->stream);
+    if (e != cudaSuccess) return fail(ctx, Z80B_ECUDA, "mulopt length %d launch: %s", len, cudaGetErrorString(e));
+    tm.stop();
+    st.launches++;
+    unsigned long long best[256];
+    mul::LenStats ls{};
+    CK(cudaMemcpyAsync(best, ctx->mul_best.p, sizeof best, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaMemcpyAsync(&ls, ctx->mul_stats.p, sizeof ls, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    st.device_ms += tm.ms();
+    st.lengths++;
+    st.sequences += (uint64_t)nl;
+    st.filter_nodes += ls.filter_nodes;
+    st.full_checks += ls.full_checks;
+    st.full_pass += ls.full_pass;
+    for (int k = 2; k < 256; k++) {
+      if (!((a.want[k >> 5] >> (k & 31)) & 1u)) continue;
+      st.per_k_sequences += (uint64_t)nl;
+      if (best[k] != mul::kNoKey) {
+        found_len[k] = len;
+        found_key[k] = best[k];
+        a.want[k >> 5] &= ~(1u << (k & 31));
+      }
+    }
+    trace("mulopt pool %d length %d: %.3f ms, %llu nodes filtered, %llu full checks", pool, len, st.device_ms,
+          (unsigned long long)ls.filter_nodes, (unsigned long long)ls.full_checks);
+  }
+  for (size_t i = 0; i < kl.size(); i++) {
+    const int k = kl[i];
+    if (!found_len[k]) continue;
+    z80b_mul_result& r = out[i];
+    r.found = 1;
+    r.length = found_len[k];
+    r.tstates = int32_t(found_key[k] >> mul::kKeyShift);
+    r.index = found_key[k] & ((1ull << mul::kKeyShift) - 1);
+    unsigned long long v = r.index;
+    for (int j = r.length - 1; j >= 0; j--) {
+      r.ops[j] = uint8_t(v % unsigned(pi.n));
+      v /= unsigned(pi.n);
+    }
+  }
+  if (stats) *stats = st;
   return Z80B_OK;
 }
 
