@@ -202,6 +202,49 @@ typedef struct z80b_tune_result {
  * timings.  The rules of the trials are discarded. */
 int z80b_autotune(z80b_ctx* ctx, const z80b_job* sample, z80b_tune_result* out);
 
+/* ---- constant-multiply search (cmd/mulopt) ---------------------------------
+ * Replaces findOptimal (cmd/mulopt/main.go:186-229) for every requested
+ * constant at once, and the reference's per-K CUDA searchers
+ * (cuda/z80_mulopt.cu:232-303, cuda/z80_mulopt_fast.cu).  Per K the result is
+ * the shortest sequence with A_out = A_in * K (mod 256) for all 256 inputs,
+ * then the fewest T-states, then the first in odometer order (main.go:194-207),
+ * so ops are deterministic (the CUDA searchers pick among equal-cost ties by a
+ * race). */
+#define Z80B_MULPOOL_MULOPT 0 /* cmd/mulopt/main.go:25-49, 14 ops, state zero but A */
+#define Z80B_MULPOOL_WIDE21 1 /* the 21-op constant-multiply workload pool (pkg/cpu semantics) */
+#define Z80B_MULPOOL_FAST14 2 /* cuda/z80_mulopt_fast.cu:20-51, 14 ops */
+#define Z80B_MULPOOL_CUDA21 3 /* cuda/z80_mulopt.cu:19-48, 21 ops */
+
+typedef struct z80b_mul_result {   /* MulResult (cmd/mulopt/main.go:162-167) */
+  int32_t k;
+  int32_t found;       /* 0: no sequence up to max_len ("NOT FOUND") */
+  int32_t length;
+  int32_t tstates;
+  uint8_t ops[16];     /* pool indices, `length` entries (names: z80b_mul_pool) */
+  uint64_t index;      /* odometer index of ops among the pool^length sequences */
+} z80b_mul_result;
+
+typedef struct z80b_mul_stats {
+  uint64_t sequences;      /* sequences walked: sum of pool^L over the lengths searched */
+  uint64_t per_k_sequences;/* sequences the per-K odometers would test: sum over K of its lengths' pool^L */
+  uint64_t filter_nodes;   /* warp-level tree nodes whose leaves passed the x=2/x=255 filter */
+  uint64_t full_checks;    /* all-256-input tests run */
+  uint64_t full_pass;      /* tests passed */
+  int32_t lengths;         /* lengths searched */
+  int32_t launches;
+  double device_ms;        /* device time of the search kernels */
+} z80b_mul_stats;
+
+/* Pool description: instruction count, longest searchable length, and (when
+ * names / tstates are not NULL) up to `cap` names and T-state costs. */
+int z80b_mul_pool(int pool, int* n_ops, int* max_len, const char** names, int* tstates, int cap);
+/* Searches lengths min_len..max_len for the constants ks[0..n_k) (each 2..255;
+ * ks = NULL searches 2..255 and writes 254 results).  init_b, init_c, init_f
+ * are the initial B, C, F (0, 0, 0 for the reference's pools); A', F' and
+ * the shadow B' start at 0.  out[i] answers ks[i]. */
+int z80b_mul_search(z80b_ctx* ctx, int pool, uint8_t init_b, uint8_t init_c, uint8_t init_f, int min_len,
+                    int max_len, const int32_t* ks, uint32_t n_k, z80b_mul_result* out, z80b_mul_stats* stats);
+
 /* ---- host helpers (no device work) ---------------------------------------- */
 /* inst.Catalog entry (pkg/inst/catalog.go:4-145): mnemonic with n/nn
  * placeholders, encoded size incl. immediate, T-states, immediate kind

@@ -247,4 +247,22 @@ int orc_mul_run(const int* seq, int n, int x, int b, int c, int f) {
 }
 int orc_mul_tstates(int i) { return MulOpTStates(i); }
 
+// Pool-generic forms (pool ids of z80_oracle_mulopt.h).
+int orc_mul_pool_size(int pool) { return MulPoolSize(pool); }
+int orc_mul_find_pool(int pool, int k, int minLen, int maxLen, int b, int c, int f, int* len, int* tstates,
+                      int* ops) {
+  MulResult r;
+  if (!MulFindOptimalPool(pool, uint8_t(k), minLen, maxLen, MulInit{uint8_t(b), uint8_t(c), uint8_t(f)}, &r))
+    return 0;
+  *len = r.length;
+  *tstates = r.tstates;
+  for (int i = 0; i < r.length; i++) ops[i] = r.ops[size_t(i)];
+  return 1;
+}
+int orc_mul_run_pool(int pool, const int* seq, int n, int x, int b, int c, int f) {
+  return MulRunPool(pool, seq, n, uint8_t(x), MulInit{uint8_t(b), uint8_t(c), uint8_t(f)});
+}
+int orc_mul_tstates_pool(int pool, int i) { return MulOpTStatesPool(pool, i); }
+const char* orc_mul_op_name(int pool, int i) { return MulOpName(pool, i); }
+
 }  // extern "C"

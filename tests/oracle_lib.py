@@ -54,6 +54,7 @@ def lib():
         L.orc_search_gpu.argtypes = [u32p, ctypes.POINTER(ctypes.c_int), ctypes.c_int, u32p,
                                      ctypes.c_int, ctypes.c_int, ctypes.POINTER(OrcRule),
                                      ctypes.c_longlong]
+        L.orc_mul_op_name.restype = ctypes.c_char_p
         L.orc_init()
         _lib = L
     return _lib
@@ -248,6 +249,36 @@ def mul_run(seq, x, b, c, f):
 
 def mul_tstates(i):
     return lib().orc_mul_tstates(i)
+
+
+MUL_POOL_REFERENCE, MUL_POOL_WIDE, MUL_POOL_FAST, MUL_POOL_CUDA = 0, 1, 2, 3
+
+
+def mul_pool_size(pool):
+    return lib().orc_mul_pool_size(pool)
+
+
+def mul_find_pool(pool, k, min_len, max_len, b=0, c=0, f=0):
+    """(length, tstates, ops) of cmd/mulopt findOptimal over `pool`, or None."""
+    ln, t = ctypes.c_int(), ctypes.c_int()
+    ops_ = (ctypes.c_int * 16)()
+    ok = lib().orc_mul_find_pool(pool, k, min_len, max_len, b, c, f, ctypes.byref(ln), ctypes.byref(t), ops_)
+    if not ok:
+        return None
+    return ln.value, t.value, list(ops_[:ln.value])
+
+
+def mul_run_pool(pool, seq, x, b=0, c=0, f=0):
+    a = (ctypes.c_int * max(1, len(seq)))(*seq)
+    return lib().orc_mul_run_pool(pool, a, len(seq), x, b, c, f)
+
+
+def mul_tstates_pool(pool, i):
+    return lib().orc_mul_tstates_pool(pool, i)
+
+
+def mul_op_name(pool, i):
+    return lib().orc_mul_op_name(pool, i).decode()
 
 
 def qc_survivors(target, dead=0):

@@ -144,3 +144,10 @@ def shard_bounds(n, rank, world):
     """Contiguous shard [lo, hi) of n independent targets for one rank (the
     reference splits its outer target loop the same way across processes)."""
     return n * rank // world, n * (rank + 1) // world
+
+
+def mul_init(seed=2):
+    """Initial B, C, F of the constant-multiply workload: the low bytes of the
+    first three splitmix64 outputs of `seed`."""
+    g = splitmix64(seed)
+    return next(g) & 0xFF, next(g) & 0xFF, next(g) & 0xFF

@@ -98,8 +98,28 @@ EXPORTS = [
     "z80b_op_info", "z80b_disasm_seq", "z80b_parse_assembly", "z80b_parse_dead_flags",
     "z80b_dead_flag_desc", "z80b_should_prune", "z80b_pool8", "z80b_rules_json",
     "z80b_set_option", "z80b_get_option", "z80b_autotune", "z80b_enumerate",
+    "z80b_mul_pool", "z80b_mul_search",
 ]
 OPT_EXH_LANE_STATES, OPT_EXH_CHUNK_BLOCKS = 1, 2
+
+
+MULPOOL_MULOPT, MULPOOL_WIDE21, MULPOOL_FAST14, MULPOOL_CUDA21 = 0, 1, 2, 3
+
+
+class MulResult(ctypes.Structure):
+    """MulResult (cmd/mulopt/main.go:162-167) with pool indices for ops."""
+    _fields_ = [("k", ctypes.c_int32), ("found", ctypes.c_int32), ("length", ctypes.c_int32),
+                ("tstates", ctypes.c_int32), ("ops", ctypes.c_uint8 * 16), ("index", ctypes.c_uint64)]
+
+
+class MulStats(ctypes.Structure):
+    _fields_ = [("sequences", ctypes.c_uint64), ("per_k_sequences", ctypes.c_uint64),
+                ("filter_nodes", ctypes.c_uint64), ("full_checks", ctypes.c_uint64),
+                ("full_pass", ctypes.c_uint64), ("lengths", ctypes.c_int32),
+                ("launches", ctypes.c_int32), ("device_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class TuneResult(ctypes.Structure):
@@ -153,6 +173,11 @@ def lib():
         L.z80b_autotune.argtypes = [vp, ctypes.POINTER(Job), ctypes.POINTER(TuneResult)]
         L.z80b_enumerate.restype = ctypes.c_uint64
         L.z80b_enumerate.argtypes = [u32p, ctypes.c_uint32, ctypes.c_uint32, u32p, ctypes.c_uint64]
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.z80b_mul_pool.argtypes = [ctypes.c_int, ip, ip, ctypes.POINTER(ctypes.c_char_p), ip, ctypes.c_int]
+        L.z80b_mul_search.argtypes = [vp, ctypes.c_int, ctypes.c_uint8, ctypes.c_uint8, ctypes.c_uint8,
+                                      ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int32),
+                                      ctypes.c_uint32, ctypes.POINTER(MulResult), ctypes.POINTER(MulStats)]
         _lib = L
     return _lib
 
@@ -384,6 +409,21 @@ class Context:
         self._check(lib().z80b_autotune(self._h, ctypes.byref(job), ctypes.byref(r)))
         return r
 
+    def mul_search(self, pool, init=(0, 0, 0), min_len=1, max_len=8, ks=None):
+        """cmd/mulopt findOptimal for the constants ks (default 2..255) at once.
+        Returns ([{k, found, length, tstates, ops, index}], MulStats)."""
+        kl = list(range(2, 256)) if ks is None else list(ks)
+        karr = (ctypes.c_int32 * max(1, len(kl)))(*kl)
+        out = (MulResult * max(1, len(kl)))()
+        st = MulStats()
+        b, c, f = init
+        self._check(lib().z80b_mul_search(self._h, pool, b, c, f, min_len, max_len,
+                                          None if ks is None else karr, len(kl), out, ctypes.byref(st)))
+        res = [{"k": out[i].k, "found": bool(out[i].found), "length": out[i].length,
+                "tstates": out[i].tstates, "ops": list(out[i].ops[:out[i].length]),
+                "index": out[i].index} for i in range(len(kl))]
+        return res, st
+
     def stage(self, job):
         self._check(lib().z80b_stage_job(self._h, ctypes.byref(job)))
 
@@ -398,6 +438,27 @@ class Context:
         nr = ctypes.c_uint64()
         self._check(lib().z80b_fetch_rules(self._h, out, max(1, n), ctypes.byref(nr)))
         return [out[i] for i in range(nr.value)]
+
+
+def mul_pool(pool):
+    """(names, tstates, max_len) of a constant-multiply pool."""
+    n, ml = ctypes.c_int(), ctypes.c_int()
+    names = (ctypes.c_char_p * 32)()
+    ts = (ctypes.c_int * 32)()
+    st = lib().z80b_mul_pool(pool, ctypes.byref(n), ctypes.byref(ml), names, ts, 32)
+    if st != OK:
+        raise Z80BError(st, f"unknown pool {pool}")
+    return [names[i].decode() for i in range(n.value)], list(ts[:n.value]), ml.value
+
+
+def mul_results_json(results, pool):
+    """cmd/mulopt -json output (main.go:336-350): the found results as a JSON
+    array of {k, ops, length, tstates}, two-space indent."""
+    import json
+    names = mul_pool(pool)[0]
+    out = [{"k": r["k"], "ops": [names[i] for i in r["ops"]], "length": r["length"],
+            "tstates": r["tstates"]} for r in results if r["found"]]
+    return json.dumps(out, indent=2) + "\n"
 
 
 def _sort_rules(rules):
