@@ -10,9 +10,13 @@
 // inputs.  A warp takes 32 consecutive odometer prefixes (one per lane) and
 // walks the same suffix tree in lock step, so every lane dispatches the same
 // instruction at the same time; the last level is unrolled per pool.  A leaf
-// is filtered on x = 2 and x = 255 (A must be 2k and -k, k = A at x = 1);
-// survivors are re-checked on x = 127 and on the wanted-constant mask, and
-// then the whole warp runs the sequence on all 256 inputs (8 per lane).
+// is filtered by one shared-memory lookup: with k = A at x = 1, the table
+// row of k holds the A that x = 2, 255, 127 must give (2k, -k, 127k) when k
+// is a wanted constant, and an impossible value otherwise, so constants
+// already solved at a shorter length (and k = 0, 1) cost nothing further.
+// The table has one copy per lane (row k, column lane), so the lookups of a
+// warp never share a bank.  Survivors get the whole warp: it runs the
+// sequence on all 256 inputs (8 per lane).
 #include <cuda_runtime.h>
 
 #include "z80b_mul_ops.cuh"
@@ -39,7 +43,7 @@ struct Walk {
   uint32_t pidx;                 // this lane's prefix (odometer digits 0..plen-1)
   uint32_t pcost;
   bool active;
-  const uint32_t* want;          // shared
+  const uint32_t* tab;           // shared expected-A table, this lane's column
   const Params* p;
   unsigned long long n_slow, n_full, n_pass;  // warp-level counters (lane 0 adds them)
 };
@@ -88,8 +92,8 @@ __device__ bool full_check(const Params& p, uint32_t pidx, uint32_t sidx, uint32
 }
 
 // Rare path: some lane of the warp has a leaf under this parent that passes
-// the x = 2 / x = 255 filter.  Re-derives the N leaves with the complete
-// quick test and runs the full test on each candidate, one at a time.
+// the table filter.  Re-derives the N leaves and runs the full test on each
+// passing leaf whose key beats the best so far, one at a time.
 template <class P, int D>
 __device__ __noinline__ void slow_parent(const S4& s, uint32_t sidx_parent, uint32_t scost_parent, Walk& w) {
   const Params& p = *w.p;
@@ -101,10 +105,7 @@ __device__ __noinline__ void slow_parent(const S4& s, uint32_t sidx_parent, uint
     const uint32_t a = t.a;
     const uint32_t k = a & 0xFFu;
     const uint32_t sidx = sidx_parent * P::N + uint32_t(i);
-    // x = 2 -> 2k, x = 255 -> -k, x = 127 -> 127k (mod 256)
-    bool q = w.active && k >= 2u && ((a >> 8) & 0xFFu) == ((2u * k) & 0xFFu) &&
-             ((a >> 16) & 0xFFu) == ((0u - k) & 0xFFu) && (a >> 24) == ((127u * k) & 0xFFu) &&
-             ((w.want[k >> 5] >> (k & 31u)) & 1u);
+    bool q = w.active && (a >> 8) == w.tab[k << 5];
     unsigned long long key = 0;
     if (q) {
       const unsigned long long cost = w.pcost + scost_parent + cost_of<P>(i);
@@ -127,27 +128,22 @@ __device__ __noinline__ void slow_parent(const S4& s, uint32_t sidx_parent, uint
   }
 }
 
-// x = 2 / x = 255 filter of one leaf: 0 in the low byte iff it passes.
-__device__ __forceinline__ uint32_t leaf_filter(uint32_t a) {
-  return (((a >> 8) ^ (a << 1)) | ((a >> 16) + a)) & 0xFFu;
-}
-
 template <class P, int I>
-__device__ __forceinline__ void leaves(const S4& s, uint32_t& acc) {
+__device__ __forceinline__ void leaves(const S4& s, const uint32_t* tab, bool& hit) {
   if constexpr (I < P::N) {
     S4 t = s;
     apply<P::kind[I]>(t);
-    acc = min(acc, leaf_filter(t.a));
-    leaves<P, I + 1>(s, acc);
+    hit |= (t.a >> 8) == tab[(t.a & 0xFFu) << 5];
+    leaves<P, I + 1>(s, tab, hit);
   }
 }
 
 template <class P, int LVL, int D>
 __device__ __forceinline__ void walk(const S4& s, uint32_t sidx, uint32_t scost, Walk& w) {
   if constexpr (LVL == D - 1) {
-    uint32_t acc = 0xFFu;
-    leaves<P, 0>(s, acc);
-    if (__any_sync(FULL, w.active && acc == 0)) slow_parent<P, D>(s, sidx, scost, w);
+    bool hit = false;
+    leaves<P, 0>(s, w.tab, hit);
+    if (__any_sync(FULL, w.active && hit)) slow_parent<P, D>(s, sidx, scost, w);
   } else {
 #pragma unroll 1
     for (int i = 0; i < P::N; i++) {
@@ -160,14 +156,21 @@ __device__ __forceinline__ void walk(const S4& s, uint32_t sidx, uint32_t scost,
 
 template <class P, int D>
 __global__ void __launch_bounds__(256) k_mul_length(Params p) {
-  __shared__ uint32_t want[8];
-  if (threadIdx.x < 8) want[threadIdx.x] = p.want[threadIdx.x];
+  // Row k: the A of x = 2, 255, 127 (bytes 0..2) for a wanted k >= 2, else
+  // all ones (no A >> 8 equals it); 32 copies of each row, one per lane.
+  __shared__ uint32_t expect[256 * 32];
+  for (int i = threadIdx.x; i < 256 * 32; i += blockDim.x) {
+    const uint32_t k = uint32_t(i) >> 5;
+    const bool wanted = k >= 2u && ((p.want[k >> 5] >> (k & 31u)) & 1u);
+    expect[i] = wanted ? (((2u * k) & 0xFFu) | (((0u - k) & 0xFFu) << 8) | (((127u * k) & 0xFFu) << 16))
+                       : 0xFFFFFFFFu;
+  }
   __syncthreads();
   const int lane = threadIdx.x & 31;
   const unsigned long long groups = (p.n_prefix + 31) / 32;
   const unsigned long long warps = (unsigned long long)gridDim.x * (blockDim.x / 32);
   Walk w;
-  w.want = want;
+  w.tab = expect + lane;
   w.p = &p;
   w.n_slow = w.n_full = w.n_pass = 0;
   for (unsigned long long g = (unsigned long long)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32; g < groups;
