@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--dead-flags", default="none")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=0, help="targets in the CPU sample (0 = auto)")
+    ap.add_argument("--no-mulopt", action="store_true", help="skip the constant-multiply leg")
+    ap.add_argument("--mulopt-max-len", type=int, default=9)
     return ap.parse_args()
 
 
@@ -156,6 +158,59 @@ def cpu_baseline(all_targets, dead, n_sample, seed=1):
     return {"value": checks / secs, "unit": UNIT, "cores": workers, "kind": "port",
             "sample": f"{len(sample)} targets drawn by index (seed {seed}) from the workload; "
                       f"{checks} candidate checks in {secs:.2f} s with {workers} threads"}
+
+
+def mulopt_leg(ctx, z80b, workloads, args, with_cpu):
+    """Constant-multiply workload: every K = 2..255 over the 21-op pool with
+    B, C, F from seed 2, lengths 1..max_len, one z80b_mul_search per step
+    (device time of its kernels); the CPU oracle's findOptimal on a bounded
+    set of constants beside it."""
+    import torch
+    init = workloads.mul_init(2)
+    ml = args.mulopt_max_len
+    for _ in range(args.warmup):
+        ctx.mul_search(z80b.MULPOOL_WIDE21, init, 1, ml)
+    ms, res, st = [], None, None
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        res, st = ctx.mul_search(z80b.MULPOOL_WIDE21, init, 1, ml)
+        ms.append(st.device_ms)
+    t = statistics.median(ms)
+    hist = {}
+    for r in res:
+        if r["found"]:
+            hist[r["length"]] = hist.get(r["length"], 0) + 1
+    out = {"workload": f"K=2..255, 21-op pool, B,C,F=({init[0]:#04x},{init[1]:#04x},{init[2]:#04x}) from seed 2, "
+                       f"lengths 1..{ml}",
+           "device_ms_per_step": t, "launches_per_step": st.launches,
+           "sequences_per_step": st.sequences, "sequences_per_s": st.sequences / (t / 1e3),
+           "per_k_sequences_per_step": st.per_k_sequences,
+           "per_k_sequences_per_s": st.per_k_sequences / (t / 1e3),
+           "unit_note": "a sequence is one odometer entry walked once for all K; per-K sequences are what one "
+                        "odometer per constant (cmd/mulopt findOptimal) tests",
+           "found": sum(hist.values()), "not_found": 254 - sum(hist.values()),
+           "lengths": {str(k): hist[k] for k in sorted(hist)},
+           "full_checks": st.full_checks, "full_pass": st.full_pass}
+    if with_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_lib
+        from concurrent.futures import ThreadPoolExecutor
+        ks = list(range(2, 19))   # constants whose optimum has <= 6 instructions
+        seqs = 0
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(max_workers=os.cpu_count() or 1) as ex:
+            cres = list(ex.map(lambda k: oracle_lib.mul_find_pool(1, k, 1, 6, *init), ks))
+        secs = time.perf_counter() - t0
+        for r in cres:
+            seqs += sum(21 ** L for L in range(1, (r[0] if r else 6) + 1))
+        gpu_by_k = {r["k"]: r for r in res}
+        agree = all(c is not None and (c[0], c[1], c[2]) == (gpu_by_k[k]["length"], gpu_by_k[k]["tstates"],
+                                                            gpu_by_k[k]["ops"]) for k, c in zip(ks, cres))
+        out["cpu_baseline"] = {"value": seqs / secs, "unit": "per-K sequences/s", "cores": os.cpu_count() or 1,
+                               "kind": "port", "sample": f"findOptimal for K=2..18 (lengths 1..6) in {secs:.2f} s, "
+                                                         f"{seqs} per-K sequences, one thread per K",
+                               "agrees_with_device": agree}
+    return out
 
 
 def auto_cpu_sample():
@@ -362,6 +417,11 @@ def main():
                  "plain_launches": stp.launches, "batched_launches": stb.launches,
                  "timing": "host wall clock around z80b_search (both synchronous)"}
 
+    mulopt = None
+    if rank == 0 and not args.no_mulopt:
+        mulopt = mulopt_leg(ctx, z80b, workloads, args, world == 1 and not args.no_cpu_baseline)
+        progress(f"mulopt: {mulopt['device_ms_per_step']:.1f} ms per step, {mulopt['found']} constants found")
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(allt, dead, args.cpu_sample or auto_cpu_sample())
@@ -374,7 +434,7 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": 1e3 * e2e_step},
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
-            "gpu_launches": launches, "plain_vs_batched": plain, "autotune": tuning,
+            "gpu_launches": launches, "plain_vs_batched": plain, "autotune": tuning, "mulopt": mulopt,
             "detail": {"rules": rules, "checked_ref": stats_last.checked_ref if stats_last else None,
                        "qc_survivors": stats_last.qc_survivors if stats_last else None,
                        "exhaustive_pairs": stats_last.exhaustive_pairs if stats_last else None,

@@ -1,0 +1,129 @@
+// search_api.h -- C++ host mirror of the reference's Go search API for the
+// candidate-verification path, on top of libz80b200.so's C ABI.
+//
+//   search::Config, Run, SearchSingle, SearchSingleMasked   pkg/search/search.go:13-110
+//   search::ExhaustiveCheck[Masked]                        pkg/search/verifier.go:159,642
+//   search::ShouldPrune, EnumerateSequences8 order         pkg/search/pruner.go, enumerator.go
+//   gpu::SearchConfig, SearchGPU                           pkg/gpu/search.go:13-199
+//   result::Rule, Table, WriteJSON, DeadFlagDesc           pkg/result/table.go, output.go
+//   mul::FindAll (findOptimal for many K)                  cmd/mulopt/main.go:186-229
+//
+// Errors that the Go code returns as `error` are thrown as search::Error
+// (status and the library's message).  Every call runs on one lazily created
+// process-wide device context; there is no CPU fallback.
+#pragma once
+#include <cstdint>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "z80b200.h"
+
+namespace z80opt {
+
+struct Instruction {
+  uint16_t op = 0;
+  uint16_t imm = 0;
+  uint32_t packed() const { return uint32_t(op) | uint32_t(imm) << 16; }
+  static Instruction unpack(uint32_t w) { return {uint16_t(w & 0xFFFF), uint16_t(w >> 16)}; }
+};
+using Seq = std::vector<Instruction>;
+
+class Error : public std::runtime_error {
+ public:
+  Error(int status, const std::string& msg) : std::runtime_error(msg), status(status) {}
+  int status;
+};
+
+namespace inst {
+int SeqByteSize(const Seq& s);
+int SeqTStates(const Seq& s);
+std::string Disassemble(const Instruction& i);
+std::string DisasmSeq(const Seq& s);  // " : "-joined (pkg/search/worker.go:273-282)
+}  // namespace inst
+
+namespace result {
+struct Rule {
+  Seq Source, Replacement;
+  int BytesSaved = 0, CyclesSaved = 0;
+  uint8_t DeadFlags = 0;
+  uint8_t DeadRegs = 0;  // extension: dead-register mask (bit0..5 = B,C,D,E,H,L)
+};
+// result.Table (pkg/result/table.go:20-57): Rules() sorted by bytes saved,
+// then cycles saved, both descending.
+class Table {
+ public:
+  void Add(const Rule& r) { rules_.push_back(r); }
+  size_t Len() const { return rules_.size(); }
+  std::vector<Rule> Rules() const;
+
+ private:
+  std::vector<Rule> rules_;
+};
+std::string DeadFlagDesc(uint8_t mask);
+void WriteJSON(std::FILE* f, const std::vector<Rule>& rules);
+}  // namespace result
+
+namespace search {
+using FlagMask = uint8_t;
+constexpr FlagMask DeadNone = 0x00, DeadUndoc = 0x28, DeadAll = 0xFF;
+
+struct Config {
+  int MaxTargetLen = 2;  // targets of length 2..MaxTargetLen
+  int MaxCandLen = 0;    // 0: MaxTargetLen - 1
+  int NumWorkers = 0;    // accepted for compatibility; the device runs every target
+  bool Verbose = false;
+  FlagMask DeadFlags = DeadNone;
+  // Extension: draw a seeded uniform sample of this many targets per length
+  // (by enumeration index) instead of all of them; 0 = all.
+  uint64_t SampleTargets = 0;
+  uint64_t Seed = 0;
+};
+
+struct Stats {  // accumulated over Run's jobs
+  uint64_t targets = 0, checks = 0, checked = 0, rules = 0;
+  double device_ms = 0;
+};
+
+result::Table Run(const Config& cfg, Stats* stats = nullptr);
+bool SearchSingle(const Seq& target, int maxCandLen, bool verbose, result::Rule* out);
+bool SearchSingleMasked(const Seq& target, int maxCandLen, FlagMask deadFlags, bool verbose, result::Rule* out);
+bool ExhaustiveCheck(const Seq& target, const Seq& cand);
+bool ExhaustiveCheckMasked(const Seq& target, const Seq& cand, FlagMask deadFlags);
+// Batched form of the two above: verdict per pair (the verify-jsonl path).
+std::vector<uint8_t> ExhaustiveCheckBatch(const std::vector<Seq>& targets, const std::vector<Seq>& cands,
+                                          FlagMask deadFlags);
+bool ShouldPrune(const Seq& s);
+bool ParseAssembly(const std::string& text, Seq* out);      // cmd/z80opt/main.go:325-397
+bool ParseDeadFlags(const std::string& text, FlagMask* out);  // cmd/z80opt/main.go:305-322
+}  // namespace search
+
+namespace gpu {
+struct SearchConfig {
+  int MaxTargetLen = 2;
+  bool Verbose = false;
+  search::FlagMask DeadFlags = search::DeadNone;
+  uint64_t SampleTargets = 0;  // extension, as in search::Config
+  uint64_t Seed = 0;
+};
+result::Table SearchGPU(const SearchConfig& cfg);
+}  // namespace gpu
+
+namespace mul {
+struct Result {
+  int K = 0;
+  bool Found = false;
+  int Length = 0, TStates = 0;
+  std::vector<std::string> Ops;
+};
+// findOptimal for every constant of ks (2..255) over `pool` (Z80B_MULPOOL_*).
+std::vector<Result> FindAll(int pool, uint8_t b, uint8_t c, uint8_t f, int minLen, int maxLen,
+                            const std::vector<int>& ks, z80b_mul_stats* stats = nullptr);
+void WriteJSON(std::FILE* f, const std::vector<Result>& results);  // cmd/mulopt -json
+}  // namespace mul
+
+// The process-wide device context (created on first use).
+z80b_ctx* context();
+
+}  // namespace z80opt
