@@ -100,7 +100,10 @@ typedef struct z80b_job {
   uint32_t n_targets;
   uint32_t target_len;
   uint32_t target_stride;       /* words per target, >= the longest target */
-  uint32_t max_cand_len;        /* 1 (candidates are the 4,531 8-bit instructions) */
+  uint32_t max_cand_len;        /* 1: candidates are the 4,531 8-bit instructions;
+                                   2 (Z80B_MODE_FIRST): then, for targets without a
+                                   length-1 winner, the 4,531^2 instruction pairs in
+                                   EnumerateSequences8(2) order */
   uint32_t global_dead_flags;   /* search.FlagMask applied to every target */
   uint32_t mode;                /* Z80B_MODE_* */
   uint32_t path;                /* Z80B_PATH_* */
@@ -264,6 +267,9 @@ int z80b_parse_dead_flags(const char* text, uint32_t* out);
 int z80b_dead_flag_desc(uint32_t mask, char* buf, uint32_t cap);
 /* search.ShouldPrune (pkg/search/pruner.go:7-35): 1, 0, or -1 on a bad opcode. */
 int z80b_should_prune(const uint32_t* seq, uint32_t n);
+/* ShouldPrune of n sequences (lens[i] words at seqs + i*stride): out[i] = 1, 0,
+ * or 0xFF on a bad opcode or length. */
+int z80b_should_prune_batch(const uint32_t* seqs, const uint8_t* lens, uint32_t stride, uint64_t n, uint8_t* out);
 /* The 8-bit instruction list in EnumerateSequences8 order
  * (pkg/search/enumerator.go:319-345); returns its length (4531). */
 uint32_t z80b_pool8(uint32_t* out, uint32_t cap);

@@ -166,6 +166,13 @@ bool ExhaustiveCheckMasked(const Instruction* t, int tn, const Instruction* c, i
 FlagMask FlagDiff(const Instruction* t, int tn, const Instruction* c, int cn);
 void Fingerprint(const Instruction* seq, int n, uint8_t out[80]);
 bool StatesEqualMasked(const State& a, const State& b, FlagMask dead);
+// Dead-register extension: registers of deadRegs (bit0..5 = B,C,D,E,H,L) are
+// not compared either.
+bool StatesEqualMaskedRegs(const State& a, const State& b, FlagMask dead, uint8_t deadRegs);
+bool QuickCheckMaskedRegs(const Instruction* t, int tn, const Instruction* c, int cn, FlagMask dead,
+                          uint8_t deadRegs);
+bool ExhaustiveCheckMaskedRegs(const Instruction* t, int tn, const Instruction* c, int cn, FlagMask dead,
+                               uint8_t deadRegs);
 
 // Register masks (verifier.go:175-188)
 enum : uint16_t {
@@ -192,6 +199,7 @@ struct Rule {
   std::vector<Instruction> Source, Replacement;
   int BytesSaved = 0, CyclesSaved = 0;
   uint8_t DeadFlags = 0;
+  uint8_t DeadRegs = 0;  // extension: registers (bit0..5 = B,C,D,E,H,L) that differ
 };
 
 struct SearchStats {
@@ -203,6 +211,11 @@ struct SearchStats {
 // Appends 0..2 rules (full first, then masked) in reference order.
 void ProcessTask(const Instruction* target, int tn, int maxCandLen,
                  FlagMask deadFlags, std::vector<Rule>& out, SearchStats* st);
+// The same with the dead-register extension: the masked pass runs when dead
+// flags or dead registers are set, compares without both, and a rule records
+// the flags (OR of F differences) and registers that differ on the 8 vectors.
+void ProcessTaskExt(const Instruction* target, int tn, int maxCandLen, FlagMask deadFlags, uint8_t deadRegs,
+                    std::vector<Rule>& out, SearchStats* st);
 
 // Many targets with a thread pool (worker.go:48-121).  Rules are returned
 // grouped by target index order (deterministic, unlike the reference table).

@@ -25,7 +25,7 @@ struct orc_state {  // 12 bytes, C layout
 struct orc_rule {
   uint32_t src[4];
   uint32_t rep[4];
-  int32_t src_len, rep_len, bytes_saved, cycles_saved, dead_flags, target_index;
+  int32_t src_len, rep_len, bytes_saved, cycles_saved, dead_flags, target_index, dead_regs;
 };
 
 static inline Instruction unpack(uint32_t w) { return {uint16_t(w & 0xFFFF), uint16_t(w >> 16)}; }
@@ -155,6 +155,7 @@ static void toRule(const Rule& r, int ti, orc_rule* o) {
   o->cycles_saved = r.CyclesSaved;
   o->dead_flags = r.DeadFlags;
   o->target_index = ti;
+  o->dead_regs = r.DeadRegs;
 }
 
 // Targets: n sequences, stride 4 words, lengths in lens[].  Rules come out
@@ -176,6 +177,39 @@ long long orc_search(const uint32_t* seqs, const int* lens, int n, int maxCandLe
       size_t i;
       while ((i = next.fetch_add(1)) < tg.size())
         ProcessTask(tg[i].data(), int(tg[i].size()), maxCandLen, FlagMask(dead), per[i], &st[i]);
+    });
+  for (auto& t : th) t.join();
+  long long k = 0;
+  unsigned long long ch = 0;
+  for (size_t i = 0; i < per.size(); i++) {
+    ch += st[i].checked;
+    for (auto& r : per[i]) {
+      if (k >= cap) return -1;
+      toRule(r, int(i), &out[k++]);
+    }
+  }
+  if (checked) *checked = ch;
+  return k;
+}
+
+// orc_search with per-target dead flags and dead registers (extension);
+// dead / dregs may be NULL (0 for every target).
+long long orc_search_ext(const uint32_t* seqs, const int* lens, int n, int maxCandLen, const uint8_t* dead,
+                         const uint8_t* dregs, int workers, orc_rule* out, long long cap, unsigned long long* checked) {
+  Init();
+  std::vector<std::vector<Instruction>> tg(size_t(n > 0 ? n : 0));
+  for (int i = 0; i < n; i++) tg[size_t(i)] = seqOf(seqs + size_t(i) * 4, lens[i]);
+  std::vector<std::vector<Rule>> per(tg.size());
+  std::vector<SearchStats> st(tg.size());
+  if (workers <= 0) workers = 1;
+  std::vector<std::thread> th;
+  std::atomic<size_t> next{0};
+  for (int w = 0; w < workers; w++)
+    th.emplace_back([&] {
+      size_t i;
+      while ((i = next.fetch_add(1)) < tg.size())
+        ProcessTaskExt(tg[i].data(), int(tg[i].size()), maxCandLen, FlagMask(dead ? dead[i] : 0),
+                       uint8_t(dregs ? dregs[i] : 0), per[i], &st[i]);
     });
   for (auto& t : th) t.join();
   long long k = 0;

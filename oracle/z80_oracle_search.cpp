@@ -73,6 +73,20 @@ bool StatesEqualMasked(const State& a, const State& b, FlagMask dead) {
          a.D == b.D && a.E == b.E && a.H == b.H && a.L == b.L && a.SP == b.SP && a.M == b.M;
 }
 
+bool StatesEqualMaskedRegs(const State& a, const State& b, FlagMask dead, uint8_t deadRegs) {
+  const uint8_t keep = uint8_t(~dead);
+  auto eq = [&](int bit, uint8_t x, uint8_t y) { return ((deadRegs >> bit) & 1) || x == y; };
+  return a.A == b.A && (a.F & keep) == (b.F & keep) && eq(0, a.B, b.B) && eq(1, a.C, b.C) &&
+         eq(2, a.D, b.D) && eq(3, a.E, b.E) && eq(4, a.H, b.H) && eq(5, a.L, b.L) && a.SP == b.SP && a.M == b.M;
+}
+
+bool QuickCheckMaskedRegs(const Instruction* t, int tn, const Instruction* c, int cn, FlagMask dead,
+                          uint8_t deadRegs) {
+  for (const State& v : TestVectors)
+    if (!StatesEqualMaskedRegs(ExecSeq(v, t, tn), ExecSeq(v, c, cn), dead, deadRegs)) return false;
+  return true;
+}
+
 // verifier.go:85-94
 bool QuickCheck(const Instruction* t, int tn, const Instruction* c, int cn) {
   for (const State& v : TestVectors)
@@ -251,8 +265,9 @@ struct Pair {
   const Instruction* c;
   int cn;
   FlagMask dead;
+  uint8_t dregs;
   bool cmp(const State& s) const {
-    return StatesEqualMasked(ExecSeq(s, t, tn), ExecSeq(s, c, cn), dead);
+    return StatesEqualMaskedRegs(ExecSeq(s, t, tn), ExecSeq(s, c, cn), dead, dregs);
   }
 };
 
@@ -343,10 +358,14 @@ static bool exhaustive(const Pair& p) {
 }
 
 bool ExhaustiveCheck(const Instruction* t, int tn, const Instruction* c, int cn) {
-  return exhaustive(Pair{t, tn, c, cn, 0});
+  return exhaustive(Pair{t, tn, c, cn, 0, 0});
 }
 bool ExhaustiveCheckMasked(const Instruction* t, int tn, const Instruction* c, int cn, FlagMask dead) {
-  return exhaustive(Pair{t, tn, c, cn, dead});
+  return exhaustive(Pair{t, tn, c, cn, dead, 0});
+}
+bool ExhaustiveCheckMaskedRegs(const Instruction* t, int tn, const Instruction* c, int cn, FlagMask dead,
+                               uint8_t deadRegs) {
+  return exhaustive(Pair{t, tn, c, cn, dead, deadRegs});
 }
 
 uint64_t ExhaustiveStates(const Instruction* t, int tn, const Instruction* c, int cn) {
@@ -434,6 +453,11 @@ static void enumerate8(int n, Fn fn) {
 // worker.go:124-192 + 195-265
 void ProcessTask(const Instruction* target, int tn, int maxCandLen, FlagMask deadFlags,
                  std::vector<Rule>& out, SearchStats* st) {
+  ProcessTaskExt(target, tn, maxCandLen, deadFlags, 0, out, st);
+}
+
+void ProcessTaskExt(const Instruction* target, int tn, int maxCandLen, FlagMask deadFlags, uint8_t deadRegs,
+                    std::vector<Rule>& out, SearchStats* st) {
   Init();
   const int tBytes = SeqByteSize(target, tn), tT = SeqTStates(target, tn);
   uint64_t checked = 0, found = 0;
@@ -459,7 +483,7 @@ void ProcessTask(const Instruction* target, int tn, int maxCandLen, FlagMask dea
     });
     if (hit) break;
   }
-  if (deadFlags != DeadNone) {
+  if (deadFlags != DeadNone || deadRegs != 0) {
     for (int cl = 1; cl <= maxCandLen; cl++) {
       bool hit = false;
       enumerate8(cl, [&](const Instruction* c) {
@@ -468,10 +492,20 @@ void ProcessTask(const Instruction* target, int tn, int maxCandLen, FlagMask dea
         if (cb >= tBytes) return true;
         if (ShouldPrune(c, cl)) return true;
         if (QuickCheck(target, tn, c, cl)) return true;
-        if (!QuickCheckMasked(target, tn, c, cl, deadFlags)) return true;
-        if (!ExhaustiveCheckMasked(target, tn, c, cl, deadFlags)) return true;
-        FlagMask fd = FlagDiff(target, tn, c, cl);
-        if (fd == 0) return true;
+        if (!QuickCheckMaskedRegs(target, tn, c, cl, deadFlags, deadRegs)) return true;
+        if (!ExhaustiveCheckMaskedRegs(target, tn, c, cl, deadFlags, deadRegs)) return true;
+        // FlagDiff (verifier.go:658-673); with dead registers the registers
+        // that differ are recorded beside the flags
+        FlagMask fd = 0;
+        uint8_t rd = 0;
+        for (const State& v : TestVectors) {
+          State a = ExecSeq(v, target, tn), b = ExecSeq(v, c, cl);
+          fd |= uint8_t(a.F ^ b.F);
+          rd |= uint8_t((a.B != b.B ? 1 : 0) | (a.C != b.C ? 2 : 0) | (a.D != b.D ? 4 : 0) | (a.E != b.E ? 8 : 0) |
+                        (a.H != b.H ? 16 : 0) | (a.L != b.L ? 32 : 0));
+        }
+        if (deadRegs == 0 && rd != 0) fd = 0;  // FlagDiff is 0 when a register differs
+        if (fd == 0 && rd == 0) return true;
         found++;
         Rule r;
         r.Source = tgt;
@@ -479,6 +513,7 @@ void ProcessTask(const Instruction* target, int tn, int maxCandLen, FlagMask dea
         r.BytesSaved = tBytes - cb;
         r.CyclesSaved = tT - SeqTStates(c, cl);
         r.DeadFlags = fd;
+        r.DeadRegs = deadRegs ? rd : 0;
         out.push_back(std::move(r));
         hit = true;
         return false;

@@ -24,11 +24,15 @@ class OrcRule(ctypes.Structure):
     _fields_ = [("src", ctypes.c_uint32 * 4), ("rep", ctypes.c_uint32 * 4),
                 ("src_len", ctypes.c_int32), ("rep_len", ctypes.c_int32),
                 ("bytes_saved", ctypes.c_int32), ("cycles_saved", ctypes.c_int32),
-                ("dead_flags", ctypes.c_int32), ("target_index", ctypes.c_int32)]
+                ("dead_flags", ctypes.c_int32), ("target_index", ctypes.c_int32),
+                ("dead_regs", ctypes.c_int32)]
 
     def key(self):
         return (self.target_index, tuple(self.src[:self.src_len]), tuple(self.rep[:self.rep_len]),
                 self.bytes_saved, self.cycles_saved, self.dead_flags)
+
+    def key_regs(self):
+        return self.key() + (self.dead_regs,)
 
 
 _lib = None
@@ -50,6 +54,11 @@ def lib():
         L.orc_search.argtypes = [u32p, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
                                  ctypes.c_int, ctypes.c_int, ctypes.POINTER(OrcRule),
                                  ctypes.c_longlong, ctypes.POINTER(ctypes.c_ulonglong)]
+        L.orc_search_ext.restype = ctypes.c_longlong
+        L.orc_search_ext.argtypes = [u32p, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
+                                     ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_uint8), ctypes.c_int,
+                                     ctypes.POINTER(OrcRule), ctypes.c_longlong,
+                                     ctypes.POINTER(ctypes.c_ulonglong)]
         L.orc_search_gpu.restype = ctypes.c_longlong
         L.orc_search_gpu.argtypes = [u32p, ctypes.POINTER(ctypes.c_int), ctypes.c_int, u32p,
                                      ctypes.c_int, ctypes.c_int, ctypes.POINTER(OrcRule),
@@ -192,6 +201,21 @@ def search(targets, max_cand_len, dead=0, workers=0, cap=None):
     w = workers or os.cpu_count() or 1
     n = lib().orc_search(flat, lens, len(targets), max_cand_len, dead, w, out, cap,
                          ctypes.byref(checked))
+    assert n >= 0, "rule buffer too small"
+    return [out[i] for i in range(n)], checked.value
+
+
+def search_ext(targets, max_cand_len, dead=None, dregs=None, workers=0, cap=None):
+    """worker.go semantics with per-target dead flags and dead registers
+    (extension); returns (rules, checked)."""
+    flat, lens = _targets(targets)
+    cap = cap or (2 * len(targets) + 16)
+    out = (OrcRule * cap)()
+    checked = ctypes.c_ulonglong()
+    w = workers or os.cpu_count() or 1
+    d = (ctypes.c_uint8 * len(targets))(*dead) if dead is not None else None
+    r = (ctypes.c_uint8 * len(targets))(*dregs) if dregs is not None else None
+    n = lib().orc_search_ext(flat, lens, len(targets), max_cand_len, d, r, w, out, cap, ctypes.byref(checked))
     assert n >= 0, "rule buffer too small"
     return [out[i] for i in range(n)], checked.value
 

@@ -1,0 +1,55 @@
+"""Length-2 candidates with per-target dead flags and dead registers (the
+batched uneven workload) on the device against the CPU oracle.
+
+Rules are compared bit for bit (target, source, replacement, byte and cycle
+savings, dead flags, dead registers) together with the reference's
+'checked' counter."""
+import json
+import os
+
+import pytest
+
+import z80b
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+
+
+def fixture():
+    return json.load(open(os.path.join(ROOT, "tests", "golden", "c3_oracle.json")))
+
+
+def dev_keys(rules):
+    return [(r.target_index, list(r.src[:r.src_len]), list(r.rep[:r.rep_len]), r.bytes_saved, r.cycles_saved,
+             r.dead_flags, r.dead_regs) for r in rules]
+
+
+def run(ctx, fx, idx=None, path=z80b.PATH_BATCHED):
+    idx = range(fx["n"]) if idx is None else idx
+    targets = [fx["targets"][i] for i in idx]
+    return ctx.search(targets, per_target_dead=[fx["dead_flags"][i] for i in idx],
+                      dead_regs=[fx["dead_regs"][i] for i in idx], max_cand_len=2, path=path)
+
+
+def test_c3_sample_rules_and_checked(ctx):
+    fx = fixture()
+    rules, st = run(ctx, fx)
+    got = [tuple([k[0], tuple(k[1]), tuple(k[2])] + list(k[3:])) for k in dev_keys(rules)]
+    want = [tuple([r[0], tuple(r[1]), tuple(r[2])] + list(r[3:])) for r in fx["rules"]]
+    assert got == want
+    assert st.checked_ref == fx["checked"]
+    assert any(len(r.rep[:r.rep_len]) == 2 for r in rules)
+
+
+def test_c3_plain_equals_batched(ctx):
+    fx = fixture()
+    idx = list(range(0, fx["n"], 8))
+    a, _ = run(ctx, fx, idx)
+    b, _ = run(ctx, fx, idx, path=z80b.PATH_PLAIN)
+    assert dev_keys(a) == dev_keys(b)
+
+
+def test_length2_needs_first_mode(ctx):
+    with pytest.raises(z80b.Z80BError) as e:
+        ctx.search([[z80b.pack(0), z80b.pack(1)]], mode=z80b.MODE_ALL, max_cand_len=2)
+    assert e.value.status == z80b.EINVAL

@@ -21,8 +21,10 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/z80b200.h"
@@ -65,7 +67,15 @@ struct PoolBufs {
   bool loaded = false;
 };
 
+// What a pipeline run needs to know about its job beyond the device arrays.
+struct PipeOpts {
+  uint32_t mode = Z80B_MODE_FIRST;
+  uint32_t max_cand = 1;        // longest candidate (1 or 2 instructions)
+  uint64_t dreg_masks = 1;      // bit m: dead-register mask m occurs in a masked pass (bit 0 always)
+};
+
 struct Staged {
+  PipeOpts opts;
   std::vector<uint32_t> targets;
   std::vector<uint8_t> lens, dead, dregs;
   z80b_job job{};
@@ -96,6 +106,15 @@ struct z80b_ctx {
   DBuf hits, nhits, fpq;
   DBuf v_tgt, v_cand, v_tl, v_cl, v_dead, v_out, v_fd, v_in, v_outs;
   DBuf mul_best, mul_stats;   // constant-multiply search: best key per K, counters
+  // length-2 candidates: the 4,531^2 pair pool, its bucket indexes (one per
+  // dead-register mask, built on first use) and the per-lane pass state
+  PoolBufs pairs2;
+  uint32_t pairs2_valid = 0;
+  std::vector<unsigned long long> pairs2_eligible;  // [16]
+  DBuf pidx[64];
+  bool pidx_ok[64] = {};
+  DBuf pidx_ptrs, pkeys_tmp, psort_tmp, peligible;
+  DBuf next2, win2, windiff2, cnt2, resume2, surv2, sdiff2, refill2, checks2;
   uint64_t n_rules_dev = 0;
   uint32_t launches = 0;
   int exh_k = 4;              // ExhaustiveCheck states per lane per dispatch (z80b_set_option)
@@ -182,13 +201,20 @@ int build_pool(z80b_ctx* ctx, PoolBufs& P, const uint32_t* insn, uint32_t n, uin
   if (lens) P.host_lens.assign(lens, lens + n);
   std::vector<uint8_t> size(n), prune(n);
   std::vector<uint16_t> reads(n);
-  for (uint32_t i = 0; i < n; i++) {
-    const uint32_t* s = insn + (size_t)i * len;
-    int l = lens ? lens[i] : int(len);
-    size[i] = uint8_t(seq_bytes(s, l));
-    prune[i] = should_prune(s, l) ? 1 : 0;
-    reads[i] = seq_reads(s, l);
-  }
+  auto fill = [&](uint32_t lo, uint32_t hi) {
+    for (uint32_t i = lo; i < hi; i++) {
+      const uint32_t* s = insn + (size_t)i * len;
+      int l = lens ? lens[i] : int(len);
+      size[i] = uint8_t(seq_bytes(s, l));
+      prune[i] = should_prune(s, l) ? 1 : 0;
+      reads[i] = seq_reads(s, l);
+    }
+  };
+  const uint32_t nth = n > (1u << 16) ? std::max(1u, std::min(32u, std::thread::hardware_concurrency())) : 1u;
+  std::vector<std::thread> th;
+  for (uint32_t k = 0; k < nth; k++)
+    th.emplace_back(fill, uint32_t(uint64_t(n) * k / nth), uint32_t(uint64_t(n) * (k + 1) / nth));
+  for (auto& t : th) t.join();
   CK(P.insn.ensure(sizeof(uint32_t) * n * len));
   CK(P.qc.ensure(sizeof(uint4) * 8 * n));
   if (with_mid) CK(P.mid.ensure(sizeof(uint4) * 32 * n));
@@ -241,13 +267,79 @@ bool valid_seq(const uint32_t* s, int n) {
   return true;
 }
 
+// The length-2 candidate pool: every odometer pair of the 8-bit list
+// (pair index = first * 4531 + second, EnumerateSequences8(2) order), with
+// its QuickCheck outputs, built once per context.
+int ensure_pairpool(z80b_ctx* ctx) {
+  if (ctx->pairs2.loaded) return Z80B_OK;
+  const auto& p8 = pool8();
+  const uint32_t n1 = uint32_t(p8.size());
+  const uint32_t n = n1 * n1;
+  std::vector<uint32_t> insn(size_t(n) * 2);
+  for (uint32_t a = 0; a < n1; a++)
+    for (uint32_t b = 0; b < n1; b++) {
+      insn[(size_t(a) * n1 + b) * 2] = p8[a];
+      insn[(size_t(a) * n1 + b) * 2 + 1] = p8[b];
+    }
+  trace("pair pool: %u pairs", n);
+  CKR(build_pool(ctx, ctx->pairs2, insn.data(), n, 2, nullptr, false));
+  // unpruned pairs by encoded size, for the eligible-pair count per target
+  std::vector<uint8_t> size(n), prune(n);
+  CK(cudaMemcpy(size.data(), ctx->pairs2.size.p, n, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(prune.data(), ctx->pairs2.prune.p, n, cudaMemcpyDeviceToHost));
+  std::vector<unsigned long long> by_size(17, 0);
+  uint32_t valid = 0;
+  for (uint32_t q = 0; q < n; q++)
+    if (!prune[q]) {
+      valid++;
+      by_size[std::min<uint32_t>(size[q], 16)]++;
+    }
+  ctx->pairs2_valid = valid;
+  ctx->pairs2_eligible.assign(16, 0);
+  for (int b = 1; b < 16; b++) ctx->pairs2_eligible[size_t(b)] = ctx->pairs2_eligible[size_t(b - 1)] + by_size[size_t(b - 1)];
+  CK(ctx->peligible.ensure(16 * sizeof(unsigned long long)));
+  CK(cudaMemcpy(ctx->peligible.p, ctx->pairs2_eligible.data(), 16 * sizeof(unsigned long long), cudaMemcpyHostToDevice));
+  CK(ctx->pidx_ptrs.ensure(64 * sizeof(void*)));
+  CK(cudaMemset(ctx->pidx_ptrs.p, 0, 64 * sizeof(void*)));
+  trace("pair pool ready: %u unpruned", valid);
+  return Z80B_OK;
+}
+
+// Bucket index of the pair pool for one dead-register mask: the pairs'
+// (hash of the masked vector-0 output, pair index) keys, sorted.
+int ensure_pair_index(z80b_ctx* ctx, uint32_t m) {
+  if (ctx->pidx_ok[m]) return Z80B_OK;
+  const DevPool& P = ctx->pairs2.dev;
+  const size_t n = P.n;
+  CK(ctx->pkeys_tmp.ensure(n * 8));
+  CK(ctx->pidx[m].ensure(n * 8));
+  launch_pair_keys(P, m, ctx->pkeys_tmp.as<unsigned long long>(), ctx->stream);
+  CKR(check_launch(ctx, "pair_keys"));
+  size_t tmp = 0;
+  CK(cub::DeviceRadixSort::SortKeys(nullptr, tmp, ctx->pkeys_tmp.as<unsigned long long>(),
+                                    ctx->pidx[m].as<unsigned long long>(), int(n), 0, 64, ctx->stream));
+  CK(ctx->psort_tmp.ensure(tmp));
+  CK(cub::DeviceRadixSort::SortKeys(ctx->psort_tmp.p, tmp, ctx->pkeys_tmp.as<unsigned long long>(),
+                                    ctx->pidx[m].as<unsigned long long>(), int(n), 0, 64, ctx->stream));
+  ctx->launches += 2;
+  void* ptr = ctx->pidx[m].p;
+  CK(cudaMemcpyAsync(ctx->pidx_ptrs.as<void*>() + m, &ptr, sizeof ptr, cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  ctx->pidx_ok[m] = true;
+  trace("pair index for dead-register mask %02X built", m);
+  return Z80B_OK;
+}
+
 int validate_job(z80b_ctx* ctx, const z80b_job* job) {
   if (!job) return fail(ctx, Z80B_EINVAL, "job is null");
   if (job->n_targets && !job->targets) return fail(ctx, Z80B_EINVAL, "targets is null");
   if (job->target_stride < 1 || job->target_stride > 64) return fail(ctx, Z80B_EINVAL, "bad target_stride");
   if (job->mode != Z80B_MODE_FIRST && job->mode != Z80B_MODE_ALL) return fail(ctx, Z80B_EINVAL, "bad mode");
   if (job->path != Z80B_PATH_BATCHED && job->path != Z80B_PATH_PLAIN) return fail(ctx, Z80B_EINVAL, "bad path");
-  if (job->max_cand_len != 1) return fail(ctx, Z80B_EINVAL, "max_cand_len must be 1");
+  if (job->max_cand_len < 1 || job->max_cand_len > 2)
+    return fail(ctx, Z80B_EINVAL, "max_cand_len must be 1 or 2");
+  if (job->max_cand_len == 2 && job->mode != Z80B_MODE_FIRST)
+    return fail(ctx, Z80B_EINVAL, "length-2 candidates need Z80B_MODE_FIRST");
   if (job->global_dead_flags > 0xFF) return fail(ctx, Z80B_EINVAL, "dead flags > 0xFF");
   for (uint32_t i = 0; i < job->n_targets; i++) {
     uint32_t l = job->target_lens ? job->target_lens[i] : job->target_len;
@@ -306,7 +398,8 @@ struct Timer {
 
 // Runs the pipeline on device-resident targets.  Rules stay in ctx->rules
 // (DevRule), count in *nr.
-int run_pipeline(z80b_ctx* ctx, const DevTargets& T, uint32_t mode, z80b_stats* st, uint64_t* nr) {
+int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_stats* st, uint64_t* nr) {
+  const uint32_t mode = opts.mode;
   const uint32_t n = T.n;
   cudaStream_t s = ctx->stream;
   PoolBufs* pool = &ctx->pool8;
@@ -424,10 +517,81 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, uint32_t mode, z80b_stats* 
         CKR(check_launch(ctx, "round_resolve"));
       }
     }
+    Lanes L2{nullptr, nullptr, nullptr};
+    unsigned long long pool2_enum = 0;
+    if (opts.max_cand >= 2) {
+      // Length-2 candidates for the lanes the length-1 pass left without a
+      // winner (worker.go:131-184: candLen 2 after candLen 1).
+      CKR(ensure_pairpool(ctx));
+      const DevPool& P2 = ctx->pairs2.dev;
+      pool2_enum = (unsigned long long)P2.n;
+      for (uint32_t m = 0; m < 64; m++)
+        if ((opts.dreg_masks >> m) & 1u) CKR(ensure_pair_index(ctx, m));
+      CK(ctx->next2.ensure(8ull * n));
+      CK(ctx->win2.ensure(8ull * n));
+      CK(ctx->windiff2.ensure(4ull * n));
+      CK(ctx->cnt2.ensure(8ull * n));
+      CK(ctx->resume2.ensure(8ull * n));
+      CK(ctx->surv2.ensure(8ull * n * kSlots2));
+      CK(ctx->sdiff2.ensure(4ull * n * kSlots2));
+      CK(ctx->refill2.ensure(4));
+      L2 = Lanes{ctx->next2.as<uint32_t>(), ctx->win2.as<uint32_t>(), ctx->windiff2.as<uint16_t>()};
+      PairScan ps{};
+      ps.idx = reinterpret_cast<const unsigned long long* const*>(ctx->pidx_ptrs.p);
+      ps.n_valid = ctx->pairs2_valid;
+      ps.cnt = ctx->cnt2.as<uint32_t>();
+      ps.resume = ctx->resume2.as<uint32_t>();
+      ps.surv = ctx->surv2.as<uint32_t>();
+      ps.sdiff = ctx->sdiff2.as<uint16_t>();
+      ps.refill = ctx->refill2.as<uint32_t>();
+      ps.eligible = ctx->peligible.as<unsigned long long>();
+      ps.checks = ctx->checks.as<unsigned long long>();
+      QCOut q2 = q;
+      q2.sdiff = ps.sdiff;
+      launch_pair_lanes_init(T, L, q, L2, ps, s);
+      CKR(check_launch(ctx, "pair_lanes_init"));
+      int kq2 = kbegin(ctx, 0);
+      launch_pair_scan(T, P2, q, L2, ps, s);
+      kend(ctx, kq2);
+      CKR(check_launch(ctx, "pair_scan"));
+      for (;;) {
+        CK(cudaMemsetAsync(R.npairs, 0, 4, s));
+        CK(cudaMemsetAsync(ps.refill, 0, 4, s));
+        launch_pair_round_build(T, P2, q, L2, ps, R, s);
+        CKR(check_launch(ctx, "pair_round_build"));
+        uint32_t np = 0, nref = 0;
+        CK(cudaMemcpyAsync(&np, R.npairs, 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(&nref, ps.refill, 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        trace("length-2 round %u: %u pairs, %u lanes to rescan", rounds, np, nref);
+        if (np == 0) {
+          if (nref == 0) break;
+          int kr = kbegin(ctx, 0);
+          launch_pair_scan(T, P2, q, L2, ps, s);
+          kend(ctx, kr);
+          CKR(check_launch(ctx, "pair_scan"));
+          continue;
+        }
+        rounds++;
+        exh_pairs += np;
+        CKR(scan(ctx, R.nchunks, R.cbase, np));
+        unsigned long long lastb = 0, lastn = 0;
+        CK(cudaMemcpyAsync(&lastb, R.cbase + (np - 1), 8, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(&lastn, R.nchunks + (np - 1), 8, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        CK(cudaMemsetAsync(R.counter, 0, 8, s));
+        int ke = kbegin(ctx, 1);
+        launch_exhaustive(T, P2, R, np, lastb + lastn, ctx->exh_k, s);
+        kend(ctx, ke);
+        CKR(check_launch(ctx, "exhaustive"));
+        launch_round_resolve(R, np, q2, L2, s);
+        CKR(check_launch(ctx, "round_resolve"));
+      }
+    }
     CK(ctx->rcnt.ensure(4ull * n));
     CK(ctx->rbase.ensure(4ull * n));
-    launch_rule_count_first(L, n, ctx->rcnt.as<uint32_t>(), T, ctx->checked.as<unsigned long long>(),
-                            uint32_t(pool8().size()), s);
+    launch_rule_count_first(L, L2, n, ctx->rcnt.as<uint32_t>(), T, ctx->checked.as<unsigned long long>(),
+                            uint32_t(pool8().size()), pool2_enum, s);
     CKR(check_launch(ctx, "rule_count"));
     CKR(scan(ctx, ctx->rcnt.as<uint32_t>(), ctx->rbase.as<uint32_t>(), n));
     uint32_t lb = 0, lc = 0;
@@ -436,7 +600,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, uint32_t mode, z80b_stats* 
     CK(cudaStreamSynchronize(s));
     *nr = uint64_t(lb) + lc;
     CK(ctx->rules.ensure(sizeof(DevRule) * std::max<uint64_t>(*nr, 1)));
-    launch_rule_write_first(L, n, ctx->rbase.as<uint32_t>(), ctx->rules.as<DevRule>(), s);
+    launch_rule_write_first(L, L2, n, ctx->rbase.as<uint32_t>(), ctx->rules.as<DevRule>(), s);
     CKR(check_launch(ctx, "rule_write"));
   } else {
     // all-hits: MidCheck on every survivor, one ExhaustiveCheck pass
@@ -536,8 +700,9 @@ void to_rules(z80b_ctx* ctx, const std::vector<DevRule>& dr, const uint32_t* tar
     std::memset(&o, 0, sizeof o);
     const uint32_t* t = targets + (size_t)r.target * stride;
     int tl = tlens ? tlens[r.target] : int(tlen);
-    const uint32_t* c = P.host_insn.data() + (size_t)r.cand * P.len;
-    int cl = int(P.len);
+    const PoolBufs& PC = (r.clen == 2) ? ctx->pairs2 : P;
+    const uint32_t* c = PC.host_insn.data() + (size_t)r.cand * PC.len;
+    int cl = int(PC.len);
     o.src_len = tl;
     o.rep_len = cl;
     for (int k = 0; k < tl; k++) o.src[k] = t[k];
@@ -566,6 +731,15 @@ int upload_targets(z80b_ctx* ctx, Staged& S, const z80b_job* job, DevTargets* T,
   if (job->dead_flags) S.dead.assign(job->dead_flags, job->dead_flags + n);
   if (job->dead_regs) S.dregs.assign(job->dead_regs, job->dead_regs + n);
   S.job = *job;
+  S.opts = PipeOpts{};
+  S.opts.mode = job->mode;
+  S.opts.max_cand = job->max_cand_len;
+  if (job->max_cand_len >= 2)
+    for (uint32_t i = 0; i < n; i++) {
+      const uint32_t dr = job->dead_regs ? job->dead_regs[i] & 0x3Fu : 0u;
+      const uint32_t df = job->dead_flags ? job->dead_flags[i] : job->global_dead_flags;
+      if (dr || df) S.opts.dreg_masks |= 1ull << dr;
+    }
   cudaStream_t s = ctx->stream;
   CK(S.d_targets.ensure(4ull * std::max<size_t>(words, 1)));
   if (n) CK(cudaMemcpyAsync(S.d_targets.p, job->targets, 4ull * words, cudaMemcpyHostToDevice, s));
@@ -614,7 +788,7 @@ int run_staged(z80b_ctx* ctx, z80b_stats* st, uint64_t* nr, std::vector<z80b_rul
   Staged& S = ctx->staged;
   DevTargets T = staged_targets(S);
   const z80b_job& job = S.job;
-  if (job.path == Z80B_PATH_BATCHED) return run_pipeline(ctx, T, job.mode, st, nr);
+  if (job.path == Z80B_PATH_BATCHED) return run_pipeline(ctx, T, S.opts, st, nr);
   // plain: one target per pipeline launch, synchronizing in between
   uint64_t total = 0;
   std::vector<DevRule> dr;
@@ -626,7 +800,7 @@ int run_staged(z80b_ctx* ctx, z80b_stats* st, uint64_t* nr, std::vector<z80b_rul
     if (T.dead) one.dead = T.dead + i;
     if (T.dead_regs) one.dead_regs = T.dead_regs + i;
     uint64_t k = 0;
-    CKR(run_pipeline(ctx, one, job.mode, st, &k));
+    CKR(run_pipeline(ctx, one, S.opts, st, &k));
     if (k) {
       dr.resize(k);
       CK(cudaMemcpyAsync(dr.data(), ctx->rules.p, sizeof(DevRule) * k, cudaMemcpyDeviceToHost, ctx->stream));
@@ -954,9 +1128,9 @@ int z80b_autotune(z80b_ctx* ctx, const z80b_job* sample, z80b_tune_result* out) 
       ctx->chunk_blocks = cs[b];
       z80b_stats st{};
       uint64_t nr = 0;
-      CKR(run_pipeline(ctx, T, sample->mode, &st, &nr));  // warm
+      CKR(run_pipeline(ctx, T, ctx->staged.opts, &st, &nr));  // warm
       std::memset(&st, 0, sizeof st);
-      CKR(run_pipeline(ctx, T, sample->mode, &st, &nr));
+      CKR(run_pipeline(ctx, T, ctx->staged.opts, &st, &nr));
       r.ms[a][b] = st.device_ms;
       if (st.device_ms < best) {
         best = st.device_ms;
@@ -1038,7 +1212,7 @@ int z80b_search(z80b_ctx* ctx, const z80b_job* job, z80b_rule* out, uint64_t cap
                            (unsigned long long)cap)
                     : Z80B_OK;
   }
-  CKR(run_pipeline(ctx, T, job->mode, stats, &nr));
+  CKR(run_pipeline(ctx, T, ctx->staged.opts, stats, &nr));
   if (stats) stats->launches = ctx->launches;
   *n_rules = nr;
   if (nr > cap)

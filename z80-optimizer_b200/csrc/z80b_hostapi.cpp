@@ -84,6 +84,17 @@ int z80b_should_prune(const uint32_t* seq, uint32_t n) {
   return should_prune(seq, int(n)) ? 1 : 0;
 }
 
+int z80b_should_prune_batch(const uint32_t* seqs, const uint8_t* lens, uint32_t stride, uint64_t n, uint8_t* out) {
+  if (n && (!seqs || !lens || !out)) return Z80B_EINVAL;
+  if (stride < 1 || stride > 64) return Z80B_EINVAL;
+  for (uint64_t i = 0; i < n; i++) {
+    const uint32_t* s = seqs + i * stride;
+    const uint32_t l = lens[i];
+    out[i] = (l < 1 || l > stride || !ok_seq(s, l)) ? 0xFF : (should_prune(s, int(l)) ? 1 : 0);
+  }
+  return Z80B_OK;
+}
+
 uint32_t z80b_pool8(uint32_t* out, uint32_t cap) {
   const auto& p = pool8();
   for (size_t i = 0; i < p.size() && i < cap; i++) out[i] = p[i];

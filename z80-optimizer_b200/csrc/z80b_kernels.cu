@@ -608,37 +608,48 @@ __global__ void k_surv_targets(QCOut q, uint32_t n, uint32_t* __restrict__ st) {
   for (uint32_t j = 0; j < c; j++) st[b + j] = t;
 }
 
-__global__ void k_rule_count_first(Lanes L, uint32_t n, uint32_t* __restrict__ cnt, DevTargets T,
-                                   unsigned long long* checked, uint32_t pool_enum) {
+__global__ void k_rule_count_first(Lanes L, Lanes L2, uint32_t n, uint32_t* __restrict__ cnt, DevTargets T,
+                                   unsigned long long* checked, uint32_t pool_enum,
+                                   unsigned long long pool2_enum) {
   uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long ch = 0;
   if (t < n) {
-    uint32_t wf = L.win[2 * t], wm = L.win[2 * t + 1];
-    cnt[t] = (wf != kNone ? 1u : 0u) + (wm != kNone ? 1u : 0u);
-    // worker.go:134 counts every enumerated candidate up to and including
-    // the winner (the pool index is the enumeration ordinal)
-    ch = (wf != kNone) ? (unsigned long long)wf + 1ull : pool_enum;
-    if (target_dead(T, t) != 0 || target_dead_regs(T, t) != 0)
-      ch += (wm != kNone) ? (unsigned long long)wm + 1ull : pool_enum;
+    uint32_t c = 0;
+    const bool masked = target_dead(T, t) != 0 || target_dead_regs(T, t) != 0;
+    for (int kind = 0; kind < 2; kind++) {
+      const uint32_t w1 = L.win[2 * t + kind];
+      const uint32_t w2 = L2.win ? L2.win[2 * t + kind] : kNone;
+      c += (w1 != kNone || w2 != kNone) ? 1u : 0u;
+      // worker.go:134 counts every enumerated candidate up to and including
+      // the winner (the pool index is the enumeration ordinal): all of the
+      // shorter lengths, then the winner's own length
+      if (kind == 0 || masked) {
+        if (w1 != kNone) ch += (unsigned long long)w1 + 1ull;
+        else if (L2.win) ch += pool_enum + ((w2 != kNone) ? (unsigned long long)w2 + 1ull : pool2_enum);
+        else ch += pool_enum;
+      }
+    }
+    cnt[t] = c;
   }
   for (int off = 16; off; off >>= 1) ch += __shfl_down_sync(kFull, ch, off);
   if (lane_id() == 0 && ch) atomicAdd(checked, ch);
 }
-
-__global__ void k_rule_write_first(Lanes L, uint32_t n, const uint32_t* __restrict__ base,
+__global__ void k_rule_write_first(Lanes L, Lanes L2, uint32_t n, const uint32_t* __restrict__ base,
                                    DevRule* __restrict__ out) {
   uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
   uint32_t b = base[t];
   for (int kind = 0; kind < 2; kind++) {
-    uint32_t w = L.win[2 * t + kind];
-    if (w == kNone) continue;
+    const uint32_t idx = 2 * t + kind;
+    const uint32_t w1 = L.win[idx];
+    const uint32_t w2 = L2.win ? L2.win[idx] : kNone;
+    if (w1 == kNone && w2 == kNone) continue;
     DevRule r;
     r.target = t;
-    r.cand = w;
-    r.diff = kind ? L.windiff[2 * t + kind] : uint16_t(0);
+    r.cand = w1 != kNone ? w1 : w2;
+    r.diff = kind ? (w1 != kNone ? L.windiff[idx] : L2.windiff[idx]) : uint16_t(0);
     r.kind = uint8_t(kind);
-    r.pad = 0;
+    r.clen = w1 != kNone ? 1 : 2;
     out[b++] = r;
   }
 }
@@ -661,7 +672,7 @@ __global__ void k_rule_write_all(const uint32_t* __restrict__ flag, const uint32
   r.cand = surv[i];
   r.diff = sdiff[i];
   r.kind = 2;
-  r.pad = 0;
+  r.clen = 1;
   out[base[i]] = r;
 }
 
@@ -702,6 +713,241 @@ __global__ void k_verify_small(const uint32_t* __restrict__ tgt, const uint8_t* 
     }
   }
 }
+
+// ------------------------------------------------- length-2 candidates
+//
+// The candidates of length 2 are the 4,531^2 odometer pairs of the 8-bit
+// list (pair index = first * 4531 + second, the EnumerateSequences8 order),
+// held as a pool whose QuickCheck outputs are precomputed like the length-1
+// pool.  Instead of comparing every target with all 20.5M pairs, each pair
+// is filed in a sorted index under a hash of its vector-0 output with F left
+// out and the dead registers zeroed (one index per dead-register mask in
+// use).  A target hashes its own vector-0 output the same way, finds its
+// bucket by binary search, and QuickChecks only the bucket's pairs, which
+// the index keeps in enumeration order.  Survivors go to fixed slots per
+// (target, kind) lane; a lane whose slots are used up without a winner
+// rescans its bucket from where it stopped.
+
+// Bytes of the packed vector-0 word 0 / word 1 kept in the bucket key.
+__device__ __forceinline__ uint32_t key_keep0(uint32_t dregs) {
+  return 0xFFu | ((dregs & 1u) ? 0u : 0xFF0000u) | ((dregs & 2u) ? 0u : 0xFF000000u);
+}
+__device__ __forceinline__ uint32_t key_keep1(uint32_t dregs) {
+  return ((dregs & 4u) ? 0u : 0xFFu) | ((dregs & 8u) ? 0u : 0xFF00u) | ((dregs & 16u) ? 0u : 0xFF0000u) |
+         ((dregs & 32u) ? 0u : 0xFF000000u);
+}
+// 32-bit bucket hash of a masked output (splitmix64 finalizer).
+__device__ __forceinline__ uint32_t bucket_hash(uint32_t w0, uint32_t w1, uint32_t w2) {
+  unsigned long long h = ((unsigned long long)w0 << 32) | w1;
+  h ^= (unsigned long long)w2 * 0x9E3779B97F4A7C15ull;
+  h ^= h >> 30;
+  h *= 0xBF58476D1CE4E5B9ull;
+  h ^= h >> 27;
+  h *= 0x94D049BB133111EBull;
+  h ^= h >> 31;
+  return uint32_t(h >> 32);
+}
+
+__global__ void k_pair_keys(DevPool P, uint32_t dregs, unsigned long long* __restrict__ keys) {
+  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= P.n) return;
+  if (P.prune[q]) {
+    keys[q] = ~0ull;  // sorts after every real entry
+    return;
+  }
+  const uint4 o = P.qc[q];
+  keys[q] = ((unsigned long long)bucket_hash(o.x & key_keep0(dregs), o.y & key_keep1(dregs), o.z) << 32) | q;
+}
+
+// Lanes of the length-2 pass: a (target, kind) lane takes part when the
+// length-1 pass found no candidate for it, the target is long enough in
+// bytes for a 2-instruction replacement, and (masked kind) the target has
+// dead flags or registers.
+__global__ void k_pair_lanes_init(DevTargets T, Lanes L1, QCOut q1, Lanes L2, PairScan ps) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long chk = 0;
+  if (t < T.n) {
+    const uint32_t tb = q1.meta[t].bytes;
+    const bool masked = target_dead(T, t) != 0 || target_dead_regs(T, t) != 0;
+    bool any = false;
+    for (int kind = 0; kind < 2; kind++) {
+      const uint32_t idx = 2 * t + kind;
+      const bool need = L1.win[idx] == kNone && tb >= 3 && (kind == 0 || masked);
+      L2.next[idx] = need ? 0u : kResolved;
+      L2.win[idx] = kNone;
+      L2.windiff[idx] = 0;
+      ps.cnt[idx] = 0;
+      ps.resume[idx] = need ? 0u : kNone;
+      any = any || need;
+    }
+    if (any) chk = ps.eligible[tb < 16 ? tb : 15];
+  }
+  for (int off = 16; off; off >>= 1) chk += __shfl_down_sync(kFull, chk, off);
+  if (lane_id() == 0 && chk) atomicAdd(ps.checks, chk);
+}
+
+__device__ __forceinline__ uint32_t lower_bound_u64(const unsigned long long* a, uint32_t n, unsigned long long v) {
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint32_t mid = lo + ((hi - lo) >> 1);
+    if (a[mid] < v) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Warp per target: (re)fills the slots of each lane whose slots are used up
+// and whose bucket has pairs left.
+__global__ void __launch_bounds__(kBlock) k_pair_scan(DevTargets T, DevPool P, QCOut q1, Lanes L2, PairScan ps) {
+  const unsigned lane = lane_id();
+  const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const uint32_t nw = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t t = gw; t < T.n; t += nw) {
+    bool need[2];
+#pragma unroll
+    for (int kind = 0; kind < 2; kind++) {
+      const uint32_t idx = 2 * t + kind;
+      const uint32_t nx = L2.next[idx];
+      need[kind] = !(nx & kResolved) && nx >= ps.cnt[idx] && ps.resume[idx] != kNone;
+    }
+    if (!need[0] && !need[1]) continue;
+    const uint32_t tl = target_len(T, t);
+    const uint32_t pw = lane < tl ? T.insn[(size_t)t * T.stride + lane] : 0u;
+    Z80S st = vec_state(int(lane & 7u));
+    run_lanes(st, pw, 0, int(tl));
+    uint32_t w[3];
+    z_pack(st, w);
+    uint32_t tw[8][3];
+#pragma unroll
+    for (int v = 0; v < 8; v++) {
+      tw[v][0] = __shfl_sync(kFull, w[0], v);
+      tw[v][1] = __shfl_sync(kFull, w[1], v);
+      tw[v][2] = __shfl_sync(kFull, w[2], v);
+    }
+    const uint32_t tb = q1.meta[t].bytes;
+    const uint32_t dead = target_dead(T, t) & 0xFFu;
+    const uint32_t dregs = target_dead_regs(T, t) & 0x3Fu;
+    for (int kind = 0; kind < 2; kind++) {
+      if (!need[kind]) continue;
+      const uint32_t idx = 2 * t + kind;
+      const uint32_t m = kind ? dregs : 0u;
+      const unsigned long long* ix = ps.idx[m];
+      const uint32_t h = bucket_hash(tw[0][0] & key_keep0(m), tw[0][1] & key_keep1(m), tw[0][2]);
+      uint32_t lo = 0, hi = 0;
+      if (lane == 0) {
+        lo = lower_bound_u64(ix, ps.n_valid, (unsigned long long)h << 32);
+        hi = (h == 0xFFFFFFFFu) ? ps.n_valid : lower_bound_u64(ix, ps.n_valid, (unsigned long long)(h + 1u) << 32);
+      }
+      lo = __shfl_sync(kFull, lo, 0);
+      hi = __shfl_sync(kFull, hi, 0);
+      // compared bytes: kind 0 everything; kind 1 without the dead flags and registers
+      const uint32_t keep0 = kind ? (0xFFu | ((~dead & 0xFFu) << 8) | ((dregs & 1u) ? 0u : 0xFF0000u) |
+                                     ((dregs & 2u) ? 0u : 0xFF000000u))
+                                  : 0xFFFFFFFFu;
+      const uint32_t keep1 = kind ? key_keep1(dregs) : 0xFFFFFFFFu;
+      uint32_t pos = lo + ps.resume[idx];
+      uint32_t found = 0;
+      bool capped = false;
+      while (pos < hi && !capped) {
+        const uint32_t j = pos + lane;
+        bool pass = false;
+        uint32_t c = 0, diff = 0;
+        if (j < hi) {
+          c = uint32_t(ix[j]);
+          if (P.size[c] < tb) {
+            const uint4 o = P.qc[c];
+            const uint32_t d0 = o.x ^ tw[0][0], d1 = o.y ^ tw[0][1], d2 = o.z ^ tw[0][2];
+            if (((d0 & keep0) | (d1 & keep1) | d2) == 0) {
+              bool full = (d0 | d1 | d2) == 0;
+              uint32_t fd = (d0 >> 8) & 0xFFu, rdf = reg_diff(d0, d1);
+              bool ok = true;
+#pragma unroll
+              for (int v = 1; v < 8; v++) {
+                const uint4 ov = P.qc[(size_t)v * P.n + c];
+                const uint32_t e0 = ov.x ^ tw[v][0], e1 = ov.y ^ tw[v][1], e2 = ov.z ^ tw[v][2];
+                ok = ok && (((e0 & keep0) | (e1 & keep1) | e2) == 0);
+                full = full && ((e0 | e1 | e2) == 0);
+                fd |= (e0 >> 8) & 0xFFu;
+                rdf |= reg_diff(e0, e1);
+              }
+              pass = ok && (kind ? !full : full);
+              diff = fd | (rdf << 8);
+            }
+          }
+        }
+        const unsigned b = __ballot_sync(kFull, pass);
+        const uint32_t room = kSlots2 - found;
+        const uint32_t r = __popc(b & lanemask_lt());
+        if (pass && r < room) {
+          ps.surv[(size_t)idx * kSlots2 + found + r] = c;
+          ps.sdiff[(size_t)idx * kSlots2 + found + r] = uint16_t(diff);
+        }
+        const uint32_t nb = __popc(b);
+        if (nb > room) {
+          // resume after the last survivor that fit
+          uint32_t bb = b;
+          for (uint32_t k = 0; k < room; k++) bb &= bb - 1;
+          pos += uint32_t(__ffs(bb)) - 1u;
+          found = kSlots2;
+          capped = true;
+        } else {
+          found += nb;
+          pos += 32;
+          capped = found == kSlots2;
+        }
+      }
+      if (lane == 0) {
+        ps.cnt[idx] = found;
+        L2.next[idx] = 0;
+        ps.resume[idx] = pos >= hi ? kNone : pos - lo;
+      }
+    }
+  }
+}
+
+// One pair per length-2 lane with an untried survivor; lanes with no slot
+// left either end without a winner (bucket exhausted) or wait for a rescan.
+__global__ void k_pair_round_build(DevTargets T, DevPool P, QCOut q1, Lanes L2, PairScan ps, RoundBuf R) {
+  const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+  bool have = false;
+  PairRec pr;
+  uint32_t src = 0;
+  if (idx < 2 * T.n) {
+    const uint32_t nx = L2.next[idx];
+    if (!(nx & kResolved)) {
+      const uint32_t t = idx >> 1, kind = idx & 1u;
+      if (nx < ps.cnt[idx]) {
+        src = idx * kSlots2 + nx;
+        const uint32_t c = ps.surv[src];
+        const uint32_t reads = q1.meta[t].reads | P.reads[c];
+        pr.target = t;
+        pr.cand = c;
+        pr.reads = uint16_t(reads);
+        pr.nblocks = sweep_blocks(reads);
+        pr.keepF = kind ? uint8_t(~target_dead(T, t)) : uint8_t(0xFFu);
+        pr.keepR = kind ? uint8_t((~target_dead_regs(T, t) & 0x3Fu) | 0x80u) : uint8_t(0x3Fu);
+        have = true;
+      } else if (ps.resume[idx] == kNone) {
+        L2.next[idx] = nx | kResolved;
+      } else {
+        atomicAdd(ps.refill, 1u);
+      }
+    }
+  }
+  const unsigned b = __ballot_sync(kFull, have);
+  if (!b) return;
+  uint32_t base = 0;
+  if (lane_id() == 0) base = atomicAdd(R.npairs, (uint32_t)__popc(b));
+  base = __shfl_sync(kFull, base, 0);
+  if (have) {
+    const uint32_t p = base + __popc(b & lanemask_lt());
+    R.pairs[p] = pr;
+    R.pair_src[p] = src;
+    R.nchunks[p] = chunks_for(pr.nblocks, R.chunk_blocks);
+    R.rejected[p] = 0;
+  }
+}
+
 
 unsigned grid_for(uint32_t n, unsigned block) { return (n + block - 1) / block; }
 
@@ -830,15 +1076,16 @@ void launch_surv_targets(const QCOut& q, uint32_t n, uint32_t* st, cudaStream_t 
   if (!n) return;
   k_surv_targets<<<grid_for(n, 256), 256, 0, s>>>(q, n, st);
 }
-void launch_rule_count_first(const Lanes& L, uint32_t n, uint32_t* cnt, const DevTargets& T,
-                             unsigned long long* checked, uint32_t pool_enum, cudaStream_t s) {
-  if (!n) return;
-  k_rule_count_first<<<grid_for(n, 256), 256, 0, s>>>(L, n, cnt, T, checked, pool_enum);
-}
-void launch_rule_write_first(const Lanes& L, uint32_t n, const uint32_t* base, DevRule* out,
+void launch_rule_count_first(const Lanes& L, const Lanes& L2, uint32_t n, uint32_t* cnt, const DevTargets& T,
+                             unsigned long long* checked, uint32_t pool_enum, unsigned long long pool2_enum,
                              cudaStream_t s) {
   if (!n) return;
-  k_rule_write_first<<<grid_for(n, 256), 256, 0, s>>>(L, n, base, out);
+  k_rule_count_first<<<grid_for(n, 256), 256, 0, s>>>(L, L2, n, cnt, T, checked, pool_enum, pool2_enum);
+}
+void launch_rule_write_first(const Lanes& L, const Lanes& L2, uint32_t n, const uint32_t* base, DevRule* out,
+                             cudaStream_t s) {
+  if (!n) return;
+  k_rule_write_first<<<grid_for(n, 256), 256, 0, s>>>(L, L2, n, base, out);
 }
 void launch_rule_count_all(const RoundBuf& R, uint32_t npairs, uint32_t* flag, cudaStream_t s) {
   if (!npairs) return;
@@ -859,5 +1106,27 @@ void launch_verify_small(const uint32_t* tgt, const uint8_t* tlens, const uint32
   if (grid > cap) grid = cap;
   k_verify_small<<<grid, 256, 0, s>>>(tgt, tlens, cand, clens, stride, n, dead, tiers, out, flagdiff);
 }
+
+void launch_pair_keys(const DevPool& P, uint32_t dregs, unsigned long long* keys, cudaStream_t s) {
+  if (!P.n) return;
+  k_pair_keys<<<grid_for(P.n, 256), 256, 0, s>>>(P, dregs, keys);
+}
+void launch_pair_lanes_init(const DevTargets& T, const Lanes& L1, const QCOut& q1, const Lanes& L2,
+                            const PairScan& ps, cudaStream_t s) {
+  if (!T.n) return;
+  k_pair_lanes_init<<<grid_for(T.n, 256), 256, 0, s>>>(T, L1, q1, L2, ps);
+}
+void launch_pair_scan(const DevTargets& T, const DevPool& P, const QCOut& q1, const Lanes& L2, const PairScan& ps,
+                      cudaStream_t s) {
+  if (!T.n) return;
+  unsigned grid = std::min<unsigned>(grid_for(T.n, kBlock / 32), unsigned(dev_num_sms() * 8));
+  k_pair_scan<<<grid, kBlock, 0, s>>>(T, P, q1, L2, ps);
+}
+void launch_pair_round_build(const DevTargets& T, const DevPool& P, const QCOut& q1, const Lanes& L2,
+                             const PairScan& ps, const RoundBuf& R, cudaStream_t s) {
+  if (!T.n) return;
+  k_pair_round_build<<<grid_for(2 * T.n, 256), 256, 0, s>>>(T, P, q1, L2, ps, R);
+}
+
 
 }  // namespace z80b

@@ -45,12 +45,26 @@ struct RoundBuf {
   uint32_t chunk_blocks;           // A-blocks per work chunk
 };
 
+// Length-2 candidate pass (pair pool): bucket indexes and per-lane slots.
+constexpr uint32_t kSlots2 = 32;  // survivors held per (target, kind) lane
+struct PairScan {
+  const unsigned long long* const* idx;  // [64] sorted bucket keys per dead-register mask
+  uint32_t n_valid;                      // entries of each index (the unpruned pairs)
+  uint32_t* cnt;                         // [2n] survivors in the lane's slots
+  uint32_t* resume;                      // [2n] bucket offset to rescan from; kNone: exhausted
+  uint32_t* surv;                        // [2n * kSlots2] pair-pool indices
+  uint16_t* sdiff;                       // [2n * kSlots2]
+  uint32_t* refill;                      // lanes waiting for a rescan (round build)
+  const unsigned long long* eligible;    // [16] unpruned pairs shorter than b bytes
+  unsigned long long* checks;            // QuickCheck units (eligible pairs per target)
+};
+
 struct DevRule {
   uint32_t target;
   uint32_t cand;
   uint16_t diff;   // flag diff | reg diff << 8
   uint8_t kind;    // 0 full, 1 masked, 2 all-hits
-  uint8_t pad;
+  uint8_t clen;    // candidate length: 1 (pool index) or 2 (pair-pool index)
 };
 
 void dev_upload_tables(cudaStream_t s);
@@ -78,14 +92,24 @@ void launch_round_resolve(const RoundBuf& R, uint32_t npairs, const QCOut& q, co
 void launch_midcheck(const DevTargets& T, const DevPool& P, const uint32_t* surv,
                      const uint32_t* surv_target, uint32_t nsurv, uint8_t* pass, cudaStream_t s);
 void launch_surv_targets(const QCOut& q, uint32_t n, uint32_t* surv_target, cudaStream_t s);
-void launch_rule_count_first(const Lanes& L, uint32_t n, uint32_t* cnt, const DevTargets& T,
-                             unsigned long long* checked, uint32_t pool_enum, cudaStream_t s);
-void launch_rule_write_first(const Lanes& L, uint32_t n, const uint32_t* base, DevRule* out,
+// L2: the lanes of the length-2 candidate pass (all pointers null when the
+// job stops at length 1); pool2_enum: the enumerated length-2 sequences.
+void launch_rule_count_first(const Lanes& L, const Lanes& L2, uint32_t n, uint32_t* cnt, const DevTargets& T,
+                             unsigned long long* checked, uint32_t pool_enum, unsigned long long pool2_enum,
+                             cudaStream_t s);
+void launch_rule_write_first(const Lanes& L, const Lanes& L2, uint32_t n, const uint32_t* base, DevRule* out,
                              cudaStream_t s);
 void launch_rule_write_all(const uint32_t* flag, const uint32_t* base, uint32_t nsurv,
                            const uint32_t* surv, const uint16_t* sdiff, const uint32_t* surv_target,
                            DevRule* out, cudaStream_t s);
 void launch_rule_count_all(const RoundBuf& R, uint32_t npairs, uint32_t* flag, cudaStream_t s);
+void launch_pair_keys(const DevPool& P, uint32_t dregs, unsigned long long* keys, cudaStream_t s);
+void launch_pair_lanes_init(const DevTargets& T, const Lanes& L1, const QCOut& q1, const Lanes& L2,
+                            const PairScan& ps, cudaStream_t s);
+void launch_pair_scan(const DevTargets& T, const DevPool& P, const QCOut& q1, const Lanes& L2, const PairScan& ps,
+                      cudaStream_t s);
+void launch_pair_round_build(const DevTargets& T, const DevPool& P, const QCOut& q1, const Lanes& L2,
+                             const PairScan& ps, const RoundBuf& R, cudaStream_t s);
 void launch_verify_small(const uint32_t* tgt, const uint8_t* tlens, const uint32_t* cand,
                          const uint8_t* clens, uint32_t stride, uint32_t n, const uint8_t* dead,
                          uint32_t tiers, uint8_t* out, uint8_t* flagdiff, cudaStream_t s);

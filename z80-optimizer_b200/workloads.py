@@ -8,6 +8,10 @@ C1  small plain: targets = every unpruned length-2 sequence over a reduced
 C2  full length-2: every unpruned length-2 sequence over the reference's
     8-bit instruction list (9,818,041 targets); subsets are drawn by index
     with a seeded generator.
+C3  batched uneven: unpruned targets drawn instruction by instruction from
+    the 8-bit list (60% length 2, 40% length 3), each with a dead-register
+    mask over B,C,D,E,H,L and a dead-flag mask over the six documented flags
+    S,Z,H,P/V,N,C; candidates up to 2 instructions.
 The reference publishes no benchmark dataset for this path; these
 generators are the inputs of the parity tests and of bench.py.
 """
@@ -151,3 +155,42 @@ def mul_init(seed=2):
     first three splitmix64 outputs of `seed`."""
     g = splitmix64(seed)
     return next(g) & 0xFF, next(g) & 0xFF, next(g) & 0xFF
+
+
+DOC_FLAGS = (0x80, 0x40, 0x10, 0x04, 0x02, 0x01)  # S, Z, H, P/V, N, C
+
+
+def prune_mask(arr, lens):
+    """ShouldPrune of every row of arr (uint32 [n, stride]) with lengths lens."""
+    L = z80b.lib()
+    arr = np.ascontiguousarray(arr, dtype=np.uint32)
+    lens = np.ascontiguousarray(lens, dtype=np.uint8)
+    out = np.zeros(len(arr), dtype=np.uint8)
+    st = L.z80b_should_prune_batch(arr.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)),
+                                   lens.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), arr.shape[1], len(arr),
+                                   out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
+    assert st == 0 and not (out == 0xFF).any()
+    return out.astype(bool)
+
+
+def c3_targets(n, seed=1):
+    """n C3 targets: (targets uint32 [n, 4], lens uint8 [n], dead_flags uint8 [n],
+    dead_regs uint8 [n]).  Length 2 with probability 0.6, else 3; every
+    instruction uniform over the 4,531-entry 8-bit list; pruned draws are
+    redrawn; masks uniform over their 64 subsets."""
+    pool = np.array(z80b.pool8(), dtype=np.uint32)
+    rng = np.random.default_rng(seed)
+    out = np.zeros((n, 4), dtype=np.uint32)
+    lens = np.where(rng.random(n) < 0.6, 2, 3).astype(np.uint8)
+    todo = np.arange(n)
+    while len(todo):
+        out[todo, :3] = pool[rng.integers(0, len(pool), size=(len(todo), 3))]
+        out[todo[lens[todo] == 2], 2] = 0
+        bad = prune_mask(out[todo], lens[todo])
+        todo = todo[bad]
+    bits = rng.integers(0, 64, size=n)
+    dead = np.zeros(n, dtype=np.uint8)
+    for i, f in enumerate(DOC_FLAGS):
+        dead |= np.where((bits >> i) & 1, f, 0).astype(np.uint8)
+    dregs = rng.integers(0, 64, size=n).astype(np.uint8)
+    return out, lens, dead, dregs

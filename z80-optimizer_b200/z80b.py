@@ -98,7 +98,7 @@ EXPORTS = [
     "z80b_op_info", "z80b_disasm_seq", "z80b_parse_assembly", "z80b_parse_dead_flags",
     "z80b_dead_flag_desc", "z80b_should_prune", "z80b_pool8", "z80b_rules_json",
     "z80b_set_option", "z80b_get_option", "z80b_autotune", "z80b_enumerate",
-    "z80b_mul_pool", "z80b_mul_search",
+    "z80b_mul_pool", "z80b_mul_search", "z80b_should_prune_batch",
 ]
 OPT_EXH_LANE_STATES, OPT_EXH_CHUNK_BLOCKS = 1, 2
 
@@ -173,6 +173,7 @@ def lib():
         L.z80b_autotune.argtypes = [vp, ctypes.POINTER(Job), ctypes.POINTER(TuneResult)]
         L.z80b_enumerate.restype = ctypes.c_uint64
         L.z80b_enumerate.argtypes = [u32p, ctypes.c_uint32, ctypes.c_uint32, u32p, ctypes.c_uint64]
+        L.z80b_should_prune_batch.argtypes = [u32p, u8p, ctypes.c_uint32, ctypes.c_uint64, u8p]
         ip = ctypes.POINTER(ctypes.c_int)
         L.z80b_mul_pool.argtypes = [ctypes.c_int, ip, ip, ctypes.POINTER(ctypes.c_char_p), ip, ctypes.c_int]
         L.z80b_mul_search.argtypes = [vp, ctypes.c_int, ctypes.c_uint8, ctypes.c_uint8, ctypes.c_uint8,
