@@ -60,6 +60,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=0, help="targets in the CPU sample (0 = auto)")
     ap.add_argument("--no-mulopt", action="store_true", help="skip the constant-multiply leg")
+    ap.add_argument("--c3-targets", type=int, default=100000, help="C3 sample size (0 = skip the C3 leg)")
+    ap.add_argument("--serve-seconds", type=float, default=10.0, help="served-query leg length (0 = skip)")
+    ap.add_argument("--serve-rate", type=float, default=2000.0, help="Poisson arrival rate of the served leg")
     ap.add_argument("--mulopt-max-len", type=int, default=9)
     return ap.parse_args()
 
@@ -213,6 +216,63 @@ def mulopt_leg(ctx, z80b, workloads, args, with_cpu):
     return out
 
 
+def c3_leg(ctx, z80b, workloads, args):
+    """Batched uneven workload: seeded C3 targets (60% length 2, 40% length
+    3, per-target dead-register and dead-flag masks), candidates up to 2
+    instructions, first-found semantics; one search per step (device time of
+    the pipeline).  Beside it, the same targets' first 200 through the
+    one-target-per-launch path."""
+    import torch
+    n = args.c3_targets
+    arr, lens, dead, dregs = workloads.c3_targets(n, seed=1)
+    arr = np.ascontiguousarray(arr)
+
+    def job_for(lo, hi, path):
+        j = z80b.Job()
+        a = np.ascontiguousarray(arr[lo:hi])
+        ln, d, r = (np.ascontiguousarray(x[lo:hi]) for x in (lens, dead, dregs))
+        j.targets = a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))
+        j.target_lens = ln.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+        j.dead_flags = d.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+        j.dead_regs = r.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8))
+        j.n_targets = hi - lo
+        j.target_stride = 4
+        j.max_cand_len = 2
+        j.mode = z80b.MODE_FIRST
+        j.path = path
+        return j, (a, ln, d, r)
+
+    job, keep = job_for(0, n, z80b.PATH_BATCHED)
+    ctx.run_job(job)  # builds the pair pool and its bucket indexes once
+    ms, st, nrules = [], None, 0
+    for _ in range(max(1, min(args.steps, 2))):
+        torch.cuda.synchronize()
+        rules, st = ctx.run_job(job)
+        ms.append(st.device_ms)
+        nrules = len(rules)
+    t = statistics.median(ms)
+    out = {"workload": f"C3: {n} targets from seed 1 (60% length 2 / 40% length 3, dead-register and dead-flag "
+                       f"mask per target), candidates up to 2 instructions",
+           "value": st.checks / (t / 1e3), "unit": UNIT, "device_ms_per_step": t, "rules": nrules,
+           "qc_survivors": st.qc_survivors, "exhaustive_pairs": st.exhaustive_pairs,
+           "exhaustive_states": st.exhaustive_states, "rounds": st.rounds, "launches": st.launches,
+           "exhaustive_ms": st.exh_ms, "checks": st.checks}
+    if args.plain_sample:
+        m = min(1000, n)
+        pj, keep2 = job_for(0, m, z80b.PATH_PLAIN)
+        bj, keep3 = job_for(0, m, z80b.PATH_BATCHED)
+        t1 = time.perf_counter()
+        _, stp = ctx.run_job(pj)
+        tp = time.perf_counter() - t1
+        t1 = time.perf_counter()
+        _, stb = ctx.run_job(bj)
+        tb = time.perf_counter() - t1
+        out["plain_vs_batched"] = {"targets": m, "plain_checks_per_s": stp.checks / tp,
+                                   "batched_checks_per_s": stb.checks / tb, "batched_over_plain": tp / tb,
+                                   "timing": "host wall clock around z80b_search (both synchronous)"}
+    return out
+
+
 def auto_cpu_sample():
     # 16,000 targets (seed 1) are ~200 core-seconds of oracle work; the
     # sweep-size tail (true equivalences with 2^34-state reduced sweeps, ~1 in
@@ -330,6 +390,8 @@ def main():
     else:
         checks_all = float(checks)
     value = checks_all / args.steps / (t_step / 1e3)
+    # algorithmic emulated instructions of the steps (length-2 targets, length-1 candidates)
+    emulated = 8.0 * checks + 16.0 * len(mine) * args.steps + 3.0 * states
 
     # ---- e2e: public API with pinned host buffers
     pinned = torch.from_numpy(mine).pin_memory()
@@ -417,6 +479,17 @@ def main():
                  "plain_launches": stp.launches, "batched_launches": stb.launches,
                  "timing": "host wall clock around z80b_search (both synchronous)"}
 
+    c3 = None
+    if rank == 0 and args.c3_targets:
+        c3 = c3_leg(ctx, z80b, workloads, args)
+        progress(f"c3: {c3['device_ms_per_step']:.1f} ms per step, {c3['rules']} rules")
+
+    serve = None
+    if rank == 0 and args.serve_seconds > 0:
+        import serve_load
+        serve, _ = serve_load.run(rate=args.serve_rate, seconds=args.serve_seconds, seed=3, verify=True)
+        progress(f"serve: p50 {serve['p50_ms']:.2f} ms, p99 {serve['p99_ms']:.2f} ms, {serve['qps']:.0f} q/s")
+
     mulopt = None
     if rank == 0 and not args.no_mulopt:
         mulopt = mulopt_leg(ctx, z80b, workloads, args, world == 1 and not args.no_cpu_baseline)
@@ -434,7 +507,11 @@ def main():
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": 1e3 * e2e_step},
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),
-            "gpu_launches": launches, "plain_vs_batched": plain, "autotune": tuning, "mulopt": mulopt,
+            "gpu_launches": launches, "plain_vs_batched": plain, "autotune": tuning,
+            "emulated_instructions": {"value": emulated / args.steps / (t_step / 1e3), "unit": "emulated Z80 instructions/s",
+                                      "model": "8 per length-1 check + 8 per target instruction + (target + "
+                                               "candidate instructions) per swept state"},
+            "c3": c3, "mulopt": mulopt, "serve": serve,
             "detail": {"rules": rules, "checked_ref": stats_last.checked_ref if stats_last else None,
                        "qc_survivors": stats_last.qc_survivors if stats_last else None,
                        "exhaustive_pairs": stats_last.exhaustive_pairs if stats_last else None,

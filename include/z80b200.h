@@ -248,6 +248,55 @@ int z80b_mul_pool(int pool, int* n_ops, int* max_len, const char** names, int* t
 int z80b_mul_search(z80b_ctx* ctx, int pool, uint8_t init_b, uint8_t init_c, uint8_t init_f, int min_len,
                     int max_len, const int32_t* ks, uint32_t n_k, z80b_mul_result* out, z80b_mul_stats* stats);
 
+/* ---- serving loop ---------------------------------------------------------
+ * Queries (a target of 1..4 instructions plus its dead flags and dead
+ * registers) are answered like SearchSingle[Masked] (pkg/search/search.go:
+ * 82-110) with candidates shorter than the target, up to max_cand_len
+ * instructions.  Several workers, each with its own context and stream, run
+ * batches of waiting queries concurrently (continuous batching: queries that
+ * arrive while batches are in flight are admitted by the next free worker);
+ * admission charges each query's device frontier memory against
+ * memory_budget.  No counterpart in the reference (its serving is one query
+ * per z80opt target call). */
+typedef struct z80b_server z80b_server;
+typedef struct z80b_server_config {
+  int device;
+  int workers;               /* concurrent batches (contexts); 0: 3 */
+  uint32_t max_batch;        /* queries per batch; 0: 4096 */
+  uint64_t memory_budget;    /* device bytes of admitted query frontiers; 0: 64 GiB */
+  uint32_t max_cand_len;     /* 1 or 2; 0: 2 */
+} z80b_server_config;
+typedef struct z80b_query {
+  uint64_t id;
+  uint32_t target[4];        /* packed op | imm << 16 */
+  uint8_t len;               /* 1..4 */
+  uint8_t dead_flags;
+  uint8_t dead_regs;         /* bit0..5 = B,C,D,E,H,L */
+  uint8_t reserved;
+} z80b_query;
+typedef struct z80b_answer {
+  uint64_t id;
+  int32_t status;            /* Z80B_OK or the status of the query's batch */
+  int32_t n_rules;           /* 0..2: the full-equivalence rule first, then the masked one */
+  z80b_rule rules[2];
+  double queued_ms;          /* submit -> batch start */
+  double service_ms;         /* batch start -> answer */
+  double latency_ms;         /* submit -> answer */
+  uint32_t batch_size;       /* 0: answered without device work (length-1 target) */
+  uint32_t reserved;
+} z80b_answer;
+typedef struct z80b_server_stats {
+  uint64_t submitted, answered, errors, batches, max_batch_seen, pending, inflight_bytes;
+  double device_ms;          /* summed pipeline device time of the batches */
+} z80b_server_stats;
+int z80b_server_start(const z80b_server_config* cfg, z80b_server** out);
+int z80b_server_submit(z80b_server* s, const z80b_query* q, uint32_t n);  /* thread-safe */
+/* Completed answers (any order), up to cap; waits up to timeout_ms for the first. */
+int z80b_server_poll(z80b_server* s, z80b_answer* out, uint32_t cap, uint32_t* n, int timeout_ms);
+int z80b_server_get_stats(z80b_server* s, z80b_server_stats* out);
+/* Answers every submitted query, joins the workers and frees the server. */
+int z80b_server_stop(z80b_server* s);
+
 /* ---- host helpers (no device work) ---------------------------------------- */
 /* inst.Catalog entry (pkg/inst/catalog.go:4-145): mnemonic with n/nn
  * placeholders, encoded size incl. immediate, T-states, immediate kind

@@ -99,6 +99,11 @@ int orc_exhaustive(const uint32_t* t, int tn, const uint32_t* c, int cn, int dea
   auto tv = seqOf(t, tn), cv = seqOf(c, cn);
   return ExhaustiveCheckMasked(tv.data(), tn, cv.data(), cn, FlagMask(dead));
 }
+int orc_exhaustive_regs(const uint32_t* t, int tn, const uint32_t* c, int cn, int dead, int dregs) {
+  Init();
+  auto tv = seqOf(t, tn), cv = seqOf(c, cn);
+  return ExhaustiveCheckMaskedRegs(tv.data(), tn, cv.data(), cn, FlagMask(dead), uint8_t(dregs));
+}
 unsigned long long orc_exhaustive_states(const uint32_t* t, int tn, const uint32_t* c, int cn) {
   Init();
   auto tv = seqOf(t, tn), cv = seqOf(c, cn);

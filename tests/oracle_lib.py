@@ -142,6 +142,11 @@ def exhaustive(t, c, dead=0):
     return bool(lib().orc_exhaustive(arr(t), len(t), arr(c), len(c), dead))
 
 
+def exhaustive_regs(t, c, dead=0, dregs=0):
+    """ExhaustiveCheckMasked with the dead-register extension."""
+    return bool(lib().orc_exhaustive_regs(arr(t), len(t), arr(c), len(c), dead, dregs))
+
+
 def exhaustive_states(t, c):
     return int(lib().orc_exhaustive_states(arr(t), len(t), arr(c), len(c)))
 

@@ -1,0 +1,73 @@
+"""The serving loop (z80b_server_*): continuous batching of queries that
+arrive while other batches run.  Every answer must equal the offline
+batched answer of the same query (alone vs in the mix), and the served rules
+re-verify under the CPU oracle."""
+import os
+
+import numpy as np
+import pytest
+
+import serve_load
+import z80b
+
+
+def has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def test_query_mix_distribution():
+    arr, lens, dead, dregs = serve_load.make_queries(20000, 3)
+    frac = np.bincount(lens, minlength=5)[1:] / len(lens)
+    assert np.allclose(frac, serve_load.LEN_P, atol=0.02)
+    assert (dregs < 64).all() and ((dead & 0x28) == 0).all()
+    for k in range(4):
+        assert (arr[lens <= k, k] == 0).all()
+
+
+def test_server_fails_loudly_without_device():
+    if has_gpu():
+        pytest.skip("a GPU is present")
+    with pytest.raises(z80b.Z80BError) as e:
+        z80b.Server()
+    assert e.value.status == z80b.ENODEV
+
+
+@pytest.mark.gpu
+def test_served_answers_equal_offline_and_oracle(O):
+    out, (arr, lens, dead, dregs, answers) = serve_load.run(rate=2000, seconds=2.0, seed=3, verify=True)
+    assert out["answered"] == out["queries"] and out["errors"] == 0
+    assert out["same_as_offline"] == out["queries"]
+    assert out["server"]["batches"] >= 2
+    # re-verify served rules with small sweeps on the CPU oracle
+    checked = 0
+    for k, a in answers.items():
+        for j in range(a.n_rules):
+            r = a.rules[j]
+            t, c = list(r.src[:r.src_len]), list(r.rep[:r.rep_len])
+            if O.exhaustive_states(t, c) > (1 << 22):
+                continue
+            masked = r.dead_flags != 0 or r.dead_regs != 0
+            assert O.exhaustive_regs(t, c, int(dead[k]) if masked else 0, int(dregs[k]) if masked else 0), (k, j)
+            checked += 1
+        if checked >= 300:
+            break
+    assert checked >= 50
+
+
+@pytest.mark.gpu
+def test_server_rejects_bad_queries():
+    srv = z80b.Server(workers=1)
+    try:
+        with pytest.raises(z80b.Z80BError):
+            srv.submit([(1, [z80b.pack(500)], 0, 0)])
+        with pytest.raises(z80b.Z80BError):
+            srv.submit([(2, [z80b.pack(0)] * 5, 0, 0)])
+        srv.submit([(3, [z80b.pack(0)], 0, 0)])  # length 1: answered without device work
+        a = srv.poll(16, 1000)
+        assert len(a) == 1 and a[0].id == 3 and a[0].n_rules == 0 and a[0].batch_size == 0
+    finally:
+        srv.stop()

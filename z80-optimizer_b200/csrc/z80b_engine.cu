@@ -23,6 +23,9 @@
 #include <cstring>
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -74,6 +77,32 @@ struct PipeOpts {
   uint64_t dreg_masks = 1;      // bit m: dead-register mask m occurs in a masked pass (bit 0 always)
 };
 
+// The 4,531^2 pair pool, its QuickCheck outputs and its bucket indexes (one
+// per dead-register mask, built on first use).  Read-only once built, so all
+// contexts of a device share one copy; mu serializes the builds.
+struct PairShared {
+  std::mutex mu;
+  PoolBufs pool;
+  uint32_t valid = 0;                          // unpruned pairs
+  std::vector<unsigned long long> eligible;    // [16] unpruned pairs shorter than b bytes
+  DBuf idx[64];
+  bool ok[64] = {};
+  DBuf ptrs, eligible_dev, keys_tmp, sort_tmp;
+};
+
+std::mutex g_pairs_mu;
+std::map<int, std::weak_ptr<PairShared>> g_pairs;
+
+std::shared_ptr<PairShared> pair_shared(int device) {
+  std::lock_guard<std::mutex> lk(g_pairs_mu);
+  std::shared_ptr<PairShared> p = g_pairs[device].lock();
+  if (!p) {
+    p = std::make_shared<PairShared>();
+    g_pairs[device] = p;
+  }
+  return p;
+}
+
 struct Staged {
   PipeOpts opts;
   std::vector<uint32_t> targets;
@@ -106,15 +135,10 @@ struct z80b_ctx {
   DBuf hits, nhits, fpq;
   DBuf v_tgt, v_cand, v_tl, v_cl, v_dead, v_out, v_fd, v_in, v_outs;
   DBuf mul_best, mul_stats;   // constant-multiply search: best key per K, counters
-  // length-2 candidates: the 4,531^2 pair pool, its bucket indexes (one per
-  // dead-register mask, built on first use) and the per-lane pass state
-  PoolBufs pairs2;
-  uint32_t pairs2_valid = 0;
-  std::vector<unsigned long long> pairs2_eligible;  // [16]
-  DBuf pidx[64];
-  bool pidx_ok[64] = {};
-  DBuf pidx_ptrs, pkeys_tmp, psort_tmp, peligible;
-  DBuf next2, win2, windiff2, cnt2, resume2, surv2, sdiff2, refill2, checks2;
+  // length-2 candidates: the pair pool and its indexes, shared by the
+  // contexts of a device; the per-lane pass state is per context
+  std::shared_ptr<PairShared> pairpool;
+  DBuf next2, win2, windiff2, cnt2, resume2, surv2, sdiff2, refill2;
   uint64_t n_rules_dev = 0;
   uint32_t launches = 0;
   int exh_k = 4;              // ExhaustiveCheck states per lane per dispatch (z80b_set_option)
@@ -271,7 +295,10 @@ bool valid_seq(const uint32_t* s, int n) {
 // (pair index = first * 4531 + second, EnumerateSequences8(2) order), with
 // its QuickCheck outputs, built once per context.
 int ensure_pairpool(z80b_ctx* ctx) {
-  if (ctx->pairs2.loaded) return Z80B_OK;
+  if (!ctx->pairpool) ctx->pairpool = pair_shared(ctx->device);
+  PairShared& S = *ctx->pairpool;
+  std::lock_guard<std::mutex> lk(S.mu);
+  if (S.pool.loaded) return Z80B_OK;
   const auto& p8 = pool8();
   const uint32_t n1 = uint32_t(p8.size());
   const uint32_t n = n1 * n1;
@@ -282,11 +309,11 @@ int ensure_pairpool(z80b_ctx* ctx) {
       insn[(size_t(a) * n1 + b) * 2 + 1] = p8[b];
     }
   trace("pair pool: %u pairs", n);
-  CKR(build_pool(ctx, ctx->pairs2, insn.data(), n, 2, nullptr, false));
+  CKR(build_pool(ctx, S.pool, insn.data(), n, 2, nullptr, false));
   // unpruned pairs by encoded size, for the eligible-pair count per target
   std::vector<uint8_t> size(n), prune(n);
-  CK(cudaMemcpy(size.data(), ctx->pairs2.size.p, n, cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(prune.data(), ctx->pairs2.prune.p, n, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(size.data(), S.pool.size.p, n, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(prune.data(), S.pool.prune.p, n, cudaMemcpyDeviceToHost));
   std::vector<unsigned long long> by_size(17, 0);
   uint32_t valid = 0;
   for (uint32_t q = 0; q < n; q++)
@@ -294,13 +321,13 @@ int ensure_pairpool(z80b_ctx* ctx) {
       valid++;
       by_size[std::min<uint32_t>(size[q], 16)]++;
     }
-  ctx->pairs2_valid = valid;
-  ctx->pairs2_eligible.assign(16, 0);
-  for (int b = 1; b < 16; b++) ctx->pairs2_eligible[size_t(b)] = ctx->pairs2_eligible[size_t(b - 1)] + by_size[size_t(b - 1)];
-  CK(ctx->peligible.ensure(16 * sizeof(unsigned long long)));
-  CK(cudaMemcpy(ctx->peligible.p, ctx->pairs2_eligible.data(), 16 * sizeof(unsigned long long), cudaMemcpyHostToDevice));
-  CK(ctx->pidx_ptrs.ensure(64 * sizeof(void*)));
-  CK(cudaMemset(ctx->pidx_ptrs.p, 0, 64 * sizeof(void*)));
+  S.valid = valid;
+  S.eligible.assign(16, 0);
+  for (int b = 1; b < 16; b++) S.eligible[size_t(b)] = S.eligible[size_t(b - 1)] + by_size[size_t(b - 1)];
+  CK(S.eligible_dev.ensure(16 * sizeof(unsigned long long)));
+  CK(cudaMemcpy(S.eligible_dev.p, S.eligible.data(), 16 * sizeof(unsigned long long), cudaMemcpyHostToDevice));
+  CK(S.ptrs.ensure(64 * sizeof(void*)));
+  CK(cudaMemset(S.ptrs.p, 0, 64 * sizeof(void*)));
   trace("pair pool ready: %u unpruned", valid);
   return Z80B_OK;
 }
@@ -308,24 +335,26 @@ int ensure_pairpool(z80b_ctx* ctx) {
 // Bucket index of the pair pool for one dead-register mask: the pairs'
 // (hash of the masked vector-0 output, pair index) keys, sorted.
 int ensure_pair_index(z80b_ctx* ctx, uint32_t m) {
-  if (ctx->pidx_ok[m]) return Z80B_OK;
-  const DevPool& P = ctx->pairs2.dev;
+  PairShared& S = *ctx->pairpool;
+  std::lock_guard<std::mutex> lk(S.mu);
+  if (S.ok[m]) return Z80B_OK;
+  const DevPool& P = S.pool.dev;
   const size_t n = P.n;
-  CK(ctx->pkeys_tmp.ensure(n * 8));
-  CK(ctx->pidx[m].ensure(n * 8));
-  launch_pair_keys(P, m, ctx->pkeys_tmp.as<unsigned long long>(), ctx->stream);
+  CK(S.keys_tmp.ensure(n * 8));
+  CK(S.idx[m].ensure(n * 8));
+  launch_pair_keys(P, m, S.keys_tmp.as<unsigned long long>(), ctx->stream);
   CKR(check_launch(ctx, "pair_keys"));
   size_t tmp = 0;
-  CK(cub::DeviceRadixSort::SortKeys(nullptr, tmp, ctx->pkeys_tmp.as<unsigned long long>(),
-                                    ctx->pidx[m].as<unsigned long long>(), int(n), 0, 64, ctx->stream));
-  CK(ctx->psort_tmp.ensure(tmp));
-  CK(cub::DeviceRadixSort::SortKeys(ctx->psort_tmp.p, tmp, ctx->pkeys_tmp.as<unsigned long long>(),
-                                    ctx->pidx[m].as<unsigned long long>(), int(n), 0, 64, ctx->stream));
+  CK(cub::DeviceRadixSort::SortKeys(nullptr, tmp, S.keys_tmp.as<unsigned long long>(),
+                                    S.idx[m].as<unsigned long long>(), int(n), 0, 64, ctx->stream));
+  CK(S.sort_tmp.ensure(tmp));
+  CK(cub::DeviceRadixSort::SortKeys(S.sort_tmp.p, tmp, S.keys_tmp.as<unsigned long long>(),
+                                    S.idx[m].as<unsigned long long>(), int(n), 0, 64, ctx->stream));
   ctx->launches += 2;
-  void* ptr = ctx->pidx[m].p;
-  CK(cudaMemcpyAsync(ctx->pidx_ptrs.as<void*>() + m, &ptr, sizeof ptr, cudaMemcpyHostToDevice, ctx->stream));
+  void* ptr = S.idx[m].p;
+  CK(cudaMemcpyAsync(S.ptrs.as<void*>() + m, &ptr, sizeof ptr, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
-  ctx->pidx_ok[m] = true;
+  S.ok[m] = true;
   trace("pair index for dead-register mask %02X built", m);
   return Z80B_OK;
 }
@@ -523,7 +552,8 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
       // Length-2 candidates for the lanes the length-1 pass left without a
       // winner (worker.go:131-184: candLen 2 after candLen 1).
       CKR(ensure_pairpool(ctx));
-      const DevPool& P2 = ctx->pairs2.dev;
+      const PairShared& PS = *ctx->pairpool;
+      const DevPool& P2 = PS.pool.dev;
       pool2_enum = (unsigned long long)P2.n;
       for (uint32_t m = 0; m < 64; m++)
         if ((opts.dreg_masks >> m) & 1u) CKR(ensure_pair_index(ctx, m));
@@ -537,14 +567,14 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
       CK(ctx->refill2.ensure(4));
       L2 = Lanes{ctx->next2.as<uint32_t>(), ctx->win2.as<uint32_t>(), ctx->windiff2.as<uint16_t>()};
       PairScan ps{};
-      ps.idx = reinterpret_cast<const unsigned long long* const*>(ctx->pidx_ptrs.p);
-      ps.n_valid = ctx->pairs2_valid;
+      ps.idx = reinterpret_cast<const unsigned long long* const*>(PS.ptrs.p);
+      ps.n_valid = PS.valid;
       ps.cnt = ctx->cnt2.as<uint32_t>();
       ps.resume = ctx->resume2.as<uint32_t>();
       ps.surv = ctx->surv2.as<uint32_t>();
       ps.sdiff = ctx->sdiff2.as<uint16_t>();
       ps.refill = ctx->refill2.as<uint32_t>();
-      ps.eligible = ctx->peligible.as<unsigned long long>();
+      ps.eligible = PS.eligible_dev.as<unsigned long long>();
       ps.checks = ctx->checks.as<unsigned long long>();
       QCOut q2 = q;
       q2.sdiff = ps.sdiff;
@@ -700,7 +730,7 @@ void to_rules(z80b_ctx* ctx, const std::vector<DevRule>& dr, const uint32_t* tar
     std::memset(&o, 0, sizeof o);
     const uint32_t* t = targets + (size_t)r.target * stride;
     int tl = tlens ? tlens[r.target] : int(tlen);
-    const PoolBufs& PC = (r.clen == 2) ? ctx->pairs2 : P;
+    const PoolBufs& PC = (r.clen == 2) ? ctx->pairpool->pool : P;
     const uint32_t* c = PC.host_insn.data() + (size_t)r.cand * PC.len;
     int cl = int(PC.len);
     o.src_len = tl;

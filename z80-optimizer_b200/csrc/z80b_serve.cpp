@@ -1,0 +1,255 @@
+// z80b_serve.cpp -- serving loop over the C ABI: optimisation queries (a
+// target plus its dead flags / dead registers) arrive one by one and are
+// answered with the shortest equivalent, as z80opt target / SearchSingle
+// would answer them, while other queries are on the device.
+//
+// Continuous batching at batch granularity: `workers` threads each own a
+// context (its own stream and device buffers; the length-2 pair pool is
+// shared per device).  A free worker takes every waiting query of one class
+// (candidates up to 1 or up to 2 instructions) up to max_batch and runs them
+// as one first-found job, so new arrivals are admitted by the next free
+// worker while earlier batches are still in flight and their work overlaps
+// on the GPU.  Admission also charges each query's frontier memory (its
+// lanes, survivor slots and rule records on the device) against the budget
+// and waits while the in-flight total would exceed it.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "../../include/z80b200.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+// Device bytes one query holds while its batch runs: target and masks,
+// metadata, two first-found lanes, the length-1 survivor range, the
+// length-2 survivor slots and rule records (z80b_engine.cu's buffers).
+constexpr uint64_t kFrontierBytes = 64 + 16 + 2 * 16 + 2 * 4531 * 6 + 2 * 32 * 6 + 2 * 12;
+
+struct Pending {
+  z80b_query q;
+  Clock::time_point t_submit;
+  uint32_t cand;  // candidate length cap of this query
+};
+
+}  // namespace
+
+struct z80b_server {
+  z80b_server_config cfg{};
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  std::deque<Pending> pending;
+  std::deque<z80b_answer> done;
+  uint64_t inflight_bytes = 0;
+  bool stopping = false;
+  std::vector<std::thread> workers;
+  std::vector<z80b_ctx*> ctxs;
+  z80b_server_stats stats{};
+};
+
+namespace {
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+  return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+void worker_loop(z80b_server* S, z80b_ctx* ctx) {
+  std::vector<Pending> batch;
+  std::vector<uint32_t> tg;
+  std::vector<uint8_t> lens, dead, dregs;
+  std::vector<z80b_rule> rules;
+  for (;;) {
+    batch.clear();
+    uint32_t cand = 1;
+    {
+      std::unique_lock<std::mutex> lk(S->mu);
+      S->cv_work.wait(lk, [&] {
+        return S->stopping ||
+               (!S->pending.empty() && S->inflight_bytes + kFrontierBytes <= S->cfg.memory_budget);
+      });
+      if (S->pending.empty()) return;  // stopping and drained
+      // the class of the oldest query; take its class-mates in arrival order
+      cand = S->pending.front().cand;
+      for (auto it = S->pending.begin(); it != S->pending.end() && batch.size() < S->cfg.max_batch;) {
+        if (it->cand == cand && S->inflight_bytes + kFrontierBytes <= S->cfg.memory_budget) {
+          batch.push_back(*it);
+          S->inflight_bytes += kFrontierBytes;
+          it = S->pending.erase(it);
+        } else {
+          ++it;
+        }
+      }
+      if (!batch.empty()) {
+        S->stats.batches++;
+        S->stats.max_batch_seen = std::max<uint64_t>(S->stats.max_batch_seen, batch.size());
+      }
+    }
+    if (batch.empty()) {  // nothing of this class fits the budget yet
+      std::this_thread::sleep_for(std::chrono::milliseconds(1));
+      continue;
+    }
+    const auto t_start = Clock::now();
+    const uint32_t n = uint32_t(batch.size());
+    tg.assign(size_t(n) * 4, 0);
+    lens.resize(n);
+    dead.resize(n);
+    dregs.resize(n);
+    for (uint32_t i = 0; i < n; i++) {
+      std::memcpy(&tg[size_t(i) * 4], batch[i].q.target, sizeof batch[i].q.target);
+      lens[i] = batch[i].q.len;
+      dead[i] = batch[i].q.dead_flags;
+      dregs[i] = batch[i].q.dead_regs;
+    }
+    z80b_job job{};
+    job.targets = tg.data();
+    job.target_lens = lens.data();
+    job.dead_flags = dead.data();
+    job.dead_regs = dregs.data();
+    job.n_targets = n;
+    job.target_stride = 4;
+    job.max_cand_len = cand;
+    job.mode = Z80B_MODE_FIRST;
+    job.path = Z80B_PATH_BATCHED;
+    rules.resize(size_t(n) * 2 + 16);
+    uint64_t nr = 0;
+    z80b_stats st{};
+    int status = z80b_search(ctx, &job, rules.data(), rules.size(), &nr, &st);
+    const auto t_end = Clock::now();
+    std::vector<z80b_answer> ans(n);
+    for (uint32_t i = 0; i < n; i++) {
+      z80b_answer& a = ans[i];
+      std::memset(&a, 0, sizeof a);
+      a.id = batch[i].q.id;
+      a.status = status;
+      a.batch_size = n;
+      a.queued_ms = ms_between(batch[i].t_submit, t_start);
+      a.service_ms = ms_between(t_start, t_end);
+      a.latency_ms = ms_between(batch[i].t_submit, t_end);
+    }
+    if (status == Z80B_OK)
+      for (uint64_t k = 0; k < nr; k++) {
+        const z80b_rule& r = rules[k];
+        z80b_answer& a = ans[uint32_t(r.target_index)];
+        if (a.n_rules < 2) a.rules[a.n_rules++] = r;
+      }
+    {
+      std::lock_guard<std::mutex> lk(S->mu);
+      S->inflight_bytes -= uint64_t(n) * kFrontierBytes;
+      for (auto& a : ans) S->done.push_back(a);
+      S->stats.answered += n;
+      S->stats.device_ms += st.device_ms;
+      if (status != Z80B_OK) S->stats.errors += n;
+    }
+    S->cv_done.notify_all();
+    S->cv_work.notify_all();
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int z80b_server_start(const z80b_server_config* cfg, z80b_server** out) {
+  if (!out) return Z80B_EINVAL;
+  *out = nullptr;
+  z80b_server_config c{};
+  if (cfg) c = *cfg;
+  if (c.workers <= 0) c.workers = 3;
+  if (c.workers > 16) return Z80B_EINVAL;
+  if (c.max_batch == 0) c.max_batch = 4096;
+  if (c.memory_budget == 0) c.memory_budget = 64ull << 30;
+  if (c.max_cand_len == 0) c.max_cand_len = 2;
+  if (c.max_cand_len > 2) return Z80B_EINVAL;
+  if (c.memory_budget < kFrontierBytes) return Z80B_EINVAL;
+  z80b_server* S = new z80b_server();
+  S->cfg = c;
+  for (int w = 0; w < c.workers; w++) {
+    z80b_ctx* ctx = nullptr;
+    int st = z80b_init(c.device, &ctx);
+    if (st != Z80B_OK) {
+      for (auto* x : S->ctxs) z80b_destroy(x);
+      delete S;
+      return st;
+    }
+    S->ctxs.push_back(ctx);
+  }
+  for (auto* ctx : S->ctxs) S->workers.emplace_back(worker_loop, S, ctx);
+  *out = S;
+  return Z80B_OK;
+}
+
+int z80b_server_submit(z80b_server* S, const z80b_query* q, uint32_t n) {
+  if (!S || (n && !q)) return Z80B_EINVAL;
+  for (uint32_t i = 0; i < n; i++) {
+    if (q[i].len < 1 || q[i].len > 4 || (q[i].dead_regs & ~0x3Fu)) return Z80B_EINVAL;
+    for (uint32_t k = 0; k < q[i].len; k++)
+      if ((q[i].target[k] & 0xFFFFu) >= Z80B_NUM_OPS) return Z80B_EINVAL;
+  }
+  const auto now = Clock::now();
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (S->stopping) return Z80B_ESTATE;
+    for (uint32_t i = 0; i < n; i++) {
+      S->stats.submitted++;
+      const uint32_t cap = std::min<uint32_t>(uint32_t(q[i].len) - 1, S->cfg.max_cand_len);
+      if (cap == 0) {
+        // a single instruction has no shorter equivalent (MaxCandLen = 0)
+        z80b_answer a;
+        std::memset(&a, 0, sizeof a);
+        a.id = q[i].id;
+        a.status = Z80B_OK;
+        S->done.push_back(a);
+        S->stats.answered++;
+        continue;
+      }
+      S->pending.push_back(Pending{q[i], now, cap});
+    }
+  }
+  S->cv_work.notify_all();
+  S->cv_done.notify_all();
+  return Z80B_OK;
+}
+
+int z80b_server_poll(z80b_server* S, z80b_answer* out, uint32_t cap, uint32_t* n, int timeout_ms) {
+  if (!S || !n || (cap && !out)) return Z80B_EINVAL;
+  std::unique_lock<std::mutex> lk(S->mu);
+  if (S->done.empty() && timeout_ms > 0)
+    S->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] { return !S->done.empty(); });
+  uint32_t k = 0;
+  while (k < cap && !S->done.empty()) {
+    out[k++] = S->done.front();
+    S->done.pop_front();
+  }
+  *n = k;
+  return Z80B_OK;
+}
+
+int z80b_server_get_stats(z80b_server* S, z80b_server_stats* out) {
+  if (!S || !out) return Z80B_EINVAL;
+  std::lock_guard<std::mutex> lk(S->mu);
+  *out = S->stats;
+  out->pending = S->pending.size();
+  out->inflight_bytes = S->inflight_bytes;
+  return Z80B_OK;
+}
+
+int z80b_server_stop(z80b_server* S) {
+  if (!S) return Z80B_EINVAL;
+  {
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->stopping = true;
+  }
+  S->cv_work.notify_all();
+  for (auto& t : S->workers) t.join();
+  for (auto* c : S->ctxs) z80b_destroy(c);
+  delete S;
+  return Z80B_OK;
+}
+
+}  // extern "C"

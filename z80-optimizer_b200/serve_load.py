@@ -1,0 +1,154 @@
+"""Served-query load: Poisson arrivals of optimisation queries against the
+serving loop (z80b_server_*), with latency percentiles and the check that
+every answer equals the offline batched answer of the same query.
+
+Query mix (seeded): target length 1/2/3/4 with probabilities 0.5/0.3/0.15/
+0.05, each instruction uniform over the 4,531-entry 8-bit list (pruned draws
+redrawn), a dead-register mask over B..L and a dead-flag mask over the six
+documented flags; a query asks for the shortest equivalent shorter than the
+target, with candidates of up to 2 instructions.
+
+    python z80-optimizer_b200/serve_load.py --rate 2000 --seconds 60 --seed 3
+"""
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+
+import numpy as np  # noqa: E402
+
+import workloads  # noqa: E402
+import z80b  # noqa: E402
+
+LEN_P = (0.5, 0.3, 0.15, 0.05)
+
+
+def make_queries(n, seed):
+    """n queries: (targets uint32 [n, 4], lens, dead_flags, dead_regs)."""
+    pool = np.array(z80b.pool8(), dtype=np.uint32)
+    rng = np.random.default_rng(seed)
+    lens = rng.choice(4, size=n, p=LEN_P).astype(np.uint8) + 1
+    out = np.zeros((n, 4), dtype=np.uint32)
+    todo = np.arange(n)
+    while len(todo):
+        out[todo] = pool[rng.integers(0, len(pool), size=(len(todo), 4))]
+        for k in range(4):
+            out[todo[lens[todo] <= k], k] = 0
+        bad = workloads.prune_mask(out[todo], lens[todo])
+        todo = todo[bad]
+    bits = rng.integers(0, 64, size=n)
+    dead = np.zeros(n, dtype=np.uint8)
+    for i, f in enumerate(workloads.DOC_FLAGS):
+        dead |= np.where((bits >> i) & 1, f, 0).astype(np.uint8)
+    dregs = rng.integers(0, 64, size=n).astype(np.uint8)
+    return out, lens, dead, dregs
+
+
+def rule_key(r):
+    return (tuple(r.src[:r.src_len]), tuple(r.rep[:r.rep_len]), r.bytes_saved, r.cycles_saved, r.dead_flags,
+            r.dead_regs)
+
+
+def offline_answers(ctx, arr, lens, dead, dregs, idx):
+    """The batched offline path on the same queries: rule keys per query."""
+    res = {}
+    for cand in (1, 2):
+        sel = [i for i in idx if min(int(lens[i]) - 1, 2) == cand]
+        for lo in range(0, len(sel), 200000):
+            part = sel[lo:lo + 200000]
+            targets = [list(map(int, arr[i, :lens[i]])) for i in part]
+            rules, _ = ctx.search(targets, per_target_dead=[int(dead[i]) for i in part],
+                                  dead_regs=[int(dregs[i]) for i in part], max_cand_len=cand)
+            for i in part:
+                res[i] = []
+            for r in rules:
+                res[part[r.target_index]].append(rule_key(r))
+    for i in idx:
+        res.setdefault(i, [])
+    return res
+
+
+def run(rate, seconds, seed, workers=3, max_batch=4096, verify=True, progress=None):
+    n = int(rate * seconds)
+    arr, lens, dead, dregs = make_queries(n, seed)
+    rng = np.random.default_rng(seed + 1000)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n))
+    srv = z80b.Server(workers=workers, max_batch=max_batch)
+    # warm-up: builds the length-2 pair pool and its indexes once
+    warm_arr, warm_lens, warm_dead, warm_dregs = make_queries(256, seed + 7)
+    srv.submit((10**9 + i, list(map(int, warm_arr[i, :warm_lens[i]])), int(warm_dead[i]), int(warm_dregs[i]))
+               for i in range(256))
+    got = 0
+    while got < 256:
+        got += len(srv.poll(4096, 100))
+    answers = {}
+    done = threading.Event()
+
+    def poller():
+        while not done.is_set() or len(answers) < n:
+            for a in srv.poll(4096, 20):
+                answers[a.id] = a
+            if done.is_set() and len(answers) >= n:
+                break
+
+    th = threading.Thread(target=poller, daemon=True)
+    th.start()
+    t0 = time.perf_counter()
+    i = 0
+    while i < n:
+        now = time.perf_counter() - t0
+        j = i
+        while j < n and arrivals[j] <= now:
+            j += 1
+        if j > i:
+            srv.submit((k, list(map(int, arr[k, :lens[k]])), int(dead[k]), int(dregs[k])) for k in range(i, j))
+            i = j
+        else:
+            time.sleep(min(0.0005, max(0.0, arrivals[i] - now)))
+    t_submit_end = time.perf_counter() - t0
+    done.set()
+    th.join(timeout=600)
+    t_end = time.perf_counter() - t0
+    stats = srv.stats().as_dict()
+    srv.stop()
+    lat = np.array([answers[k].latency_ms for k in range(n) if k in answers])
+    served = np.array([answers[k].latency_ms for k in range(n) if k in answers and answers[k].batch_size > 0])
+    bsz = [answers[k].batch_size for k in range(n) if k in answers and answers[k].batch_size > 0]
+    out = {"queries": n, "answered": len(answers), "rate_offered_qps": rate, "seconds": seconds, "seed": seed,
+           "qps": len(answers) / t_end, "submit_span_s": t_submit_end, "wall_s": t_end,
+           "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+           "device_queries": int(len(served)),
+           "p50_ms_device_queries": float(np.percentile(served, 50)) if len(served) else None,
+           "p99_ms_device_queries": float(np.percentile(served, 99)) if len(served) else None,
+           "mean_batch": statistics.mean(bsz) if bsz else 0, "server": stats,
+           "errors": int(sum(1 for a in answers.values() if a.status != 0)),
+           "rules": int(sum(a.n_rules for a in answers.values()))}
+    if verify:
+        ctx = z80b.Context(0)
+        off = offline_answers(ctx, arr, lens, dead, dregs, list(range(n)))
+        ctx.close()
+        same = sum(1 for k in range(n)
+                   if k in answers and [rule_key(answers[k].rules[j]) for j in range(answers[k].n_rules)] == off[k])
+        out["same_as_offline"] = same
+    return out, (arr, lens, dead, dregs, answers)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--rate", type=float, default=2000)
+    ap.add_argument("--seconds", type=float, default=60)
+    ap.add_argument("--seed", type=int, default=3)
+    ap.add_argument("--workers", type=int, default=3)
+    ap.add_argument("--no-verify", action="store_true")
+    a = ap.parse_args()
+    out, _ = run(a.rate, a.seconds, a.seed, a.workers, verify=not a.no_verify)
+    print(json.dumps(out))
+
+
+if __name__ == "__main__":
+    main()

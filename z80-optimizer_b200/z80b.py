@@ -99,6 +99,7 @@ EXPORTS = [
     "z80b_dead_flag_desc", "z80b_should_prune", "z80b_pool8", "z80b_rules_json",
     "z80b_set_option", "z80b_get_option", "z80b_autotune", "z80b_enumerate",
     "z80b_mul_pool", "z80b_mul_search", "z80b_should_prune_batch",
+    "z80b_server_start", "z80b_server_submit", "z80b_server_poll", "z80b_server_get_stats", "z80b_server_stop",
 ]
 OPT_EXH_LANE_STATES, OPT_EXH_CHUNK_BLOCKS = 1, 2
 
@@ -117,6 +118,30 @@ class MulStats(ctypes.Structure):
                 ("filter_nodes", ctypes.c_uint64), ("full_checks", ctypes.c_uint64),
                 ("full_pass", ctypes.c_uint64), ("lengths", ctypes.c_int32),
                 ("launches", ctypes.c_int32), ("device_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Query(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_uint64), ("target", ctypes.c_uint32 * 4), ("len", ctypes.c_uint8),
+                ("dead_flags", ctypes.c_uint8), ("dead_regs", ctypes.c_uint8), ("reserved", ctypes.c_uint8)]
+
+
+class Answer(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_uint64), ("status", ctypes.c_int32), ("n_rules", ctypes.c_int32),
+                ("rules", Rule * 2), ("queued_ms", ctypes.c_double), ("service_ms", ctypes.c_double),
+                ("latency_ms", ctypes.c_double), ("batch_size", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("workers", ctypes.c_int), ("max_batch", ctypes.c_uint32),
+                ("memory_budget", ctypes.c_uint64), ("max_cand_len", ctypes.c_uint32)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_uint64) for k in ("submitted", "answered", "errors", "batches", "max_batch_seen",
+                                               "pending", "inflight_bytes")] + [("device_ms", ctypes.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -174,6 +199,12 @@ def lib():
         L.z80b_enumerate.restype = ctypes.c_uint64
         L.z80b_enumerate.argtypes = [u32p, ctypes.c_uint32, ctypes.c_uint32, u32p, ctypes.c_uint64]
         L.z80b_should_prune_batch.argtypes = [u32p, u8p, ctypes.c_uint32, ctypes.c_uint64, u8p]
+        L.z80b_server_start.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
+        L.z80b_server_submit.argtypes = [vp, ctypes.POINTER(Query), ctypes.c_uint32]
+        L.z80b_server_poll.argtypes = [vp, ctypes.POINTER(Answer), ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32),
+                                       ctypes.c_int]
+        L.z80b_server_get_stats.argtypes = [vp, ctypes.POINTER(ServerStats)]
+        L.z80b_server_stop.argtypes = [vp]
         ip = ctypes.POINTER(ctypes.c_int)
         L.z80b_mul_pool.argtypes = [ctypes.c_int, ip, ip, ctypes.POINTER(ctypes.c_char_p), ip, ctypes.c_int]
         L.z80b_mul_search.argtypes = [vp, ctypes.c_int, ctypes.c_uint8, ctypes.c_uint8, ctypes.c_uint8,
@@ -460,6 +491,51 @@ def mul_results_json(results, pool):
     out = [{"k": r["k"], "ops": [names[i] for i in r["ops"]], "length": r["length"],
             "tstates": r["tstates"]} for r in results if r["found"]]
     return json.dumps(out, indent=2) + "\n"
+
+
+class Server:
+    """Serving loop (z80b_server_*): submit queries from any thread, poll answers."""
+
+    def __init__(self, device=0, workers=3, max_batch=4096, memory_budget=0, max_cand_len=2):
+        cfg = ServerConfig(device, workers, max_batch, memory_budget, max_cand_len)
+        h = ctypes.c_void_p()
+        st = lib().z80b_server_start(ctypes.byref(cfg), ctypes.byref(h))
+        if st != OK:
+            raise Z80BError(st, "z80b_server_start failed")
+        self._h = h
+
+    def submit(self, queries):
+        """queries: iterable of (id, target instruction list, dead_flags, dead_regs)."""
+        qs = list(queries)
+        arr = (Query * max(1, len(qs)))()
+        for i, (qid, tgt, df, dr) in enumerate(qs):
+            arr[i].id = qid
+            arr[i].len = len(tgt)
+            for k, w in enumerate(tgt):
+                arr[i].target[k] = w
+            arr[i].dead_flags = df
+            arr[i].dead_regs = dr
+        st = lib().z80b_server_submit(self._h, arr, len(qs))
+        if st != OK:
+            raise Z80BError(st, "z80b_server_submit failed")
+
+    def poll(self, cap=4096, timeout_ms=10):
+        out = (Answer * cap)()
+        n = ctypes.c_uint32()
+        st = lib().z80b_server_poll(self._h, out, cap, ctypes.byref(n), timeout_ms)
+        if st != OK:
+            raise Z80BError(st, "z80b_server_poll failed")
+        return [out[i] for i in range(n.value)]
+
+    def stats(self):
+        s = ServerStats()
+        lib().z80b_server_get_stats(self._h, ctypes.byref(s))
+        return s
+
+    def stop(self):
+        if self._h:
+            lib().z80b_server_stop(self._h)
+            self._h = None
 
 
 def _sort_rules(rules):
