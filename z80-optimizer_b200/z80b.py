@@ -509,6 +509,8 @@ class Server:
         qs = list(queries)
         arr = (Query * max(1, len(qs)))()
         for i, (qid, tgt, df, dr) in enumerate(qs):
+            if not 1 <= len(tgt) <= 4:
+                raise Z80BError(EINVAL, f"query {qid}: target length {len(tgt)} outside 1..4")
             arr[i].id = qid
             arr[i].len = len(tgt)
             for k, w in enumerate(tgt):
