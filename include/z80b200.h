@@ -78,6 +78,8 @@ typedef struct z80b_stats {
   double device_ms;         /* whole pipeline, first to last event on the context's stream */
   double qc_ms, exh_ms;     /* summed durations of the QuickCheck scan kernels and of the
                                ExhaustiveCheck kernels (CUDA events around each launch) */
+  uint64_t exhaustive_evaluated; /* states the sweep kernel ran: exhaustive_states less what
+                               the A-independent sweeps skip (2 of 256 values of A decide) */
 } z80b_stats;
 
 /* Semantics of a search job. */

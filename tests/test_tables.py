@@ -1,10 +1,12 @@
 """Host-side tables of the product library (catalog, masks, pruning,
 enumeration order, disassembly, parsing, JSON) against the CPU oracle."""
 import json
+import os
 import random
 
 import z80b
 import workloads
+from conftest import ROOT
 
 
 def test_op_info_matches_oracle(O):
@@ -81,3 +83,19 @@ def test_rules_json_matches_oracle(O):
     assert z80b.write_json(mine) == O.write_json(rules)
     assert any(r.dead_flags for r in rules)
     json.loads(z80b.write_json(mine))
+
+
+def test_a_dependence_classes_against_oracle(tmp_path):
+    """The A-dependence class of every opcode (used to sweep A-independent
+    pairs at two values of A) holds under the oracle's Exec, and two values
+    of A decide random A-independent pairs exactly as all 256 do."""
+    import subprocess
+    exe = tmp_path / "aclass_check"
+    srcs = [os.path.join(ROOT, "tests", "native", "aclass_check.cpp"),
+            os.path.join(ROOT, "z80-optimizer_b200", "csrc", "z80_tables.cpp"),
+            os.path.join(ROOT, "oracle", "z80_oracle_isa_cpu.cpp"),
+            os.path.join(ROOT, "oracle", "z80_oracle_search.cpp")]
+    subprocess.run(["g++", "-O2", "-std=c++17", "-o", str(exe)] + srcs + ["-lpthread"], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.startswith("OK")

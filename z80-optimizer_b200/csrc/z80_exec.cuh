@@ -179,8 +179,13 @@ Z80_HD void z_sbchl(Z80S& s, uint32_t v) {
   M((base) + 4, h) M((base) + 5, l) M((base) + 6, a)
 
 // Applies a statement to every state S[0..K) (named s inside).
+#if defined(__CUDACC__)
+#define Z80B_UNROLL _Pragma("unroll")
+#else
+#define Z80B_UNROLL
+#endif
 #define Z80B_EACH(...)                 \
-  _Pragma("unroll") for (int k_ = 0; k_ < K; k_++) { \
+  Z80B_UNROLL for (int k_ = 0; k_ < K; k_++) { \
     Z80S& s = S[k_];                   \
     __VA_ARGS__;                       \
   }

@@ -2,6 +2,8 @@
 // See z80_tables.h for the reference files each part follows.
 #include "z80_tables.h"
 
+#include "z80_exec.cuh"
+
 #include <cctype>
 #include <cstdio>
 #include <cstring>
@@ -180,6 +182,73 @@ void hex2(std::string& o, unsigned v, int digits) {
 }  // namespace
 
 const OpInfo* op_table() { return tables().info; }
+
+namespace {
+// Class of one opcode: for sampled input states (all registers, F, SP and M
+// random, plus all-zero and all-one states) and several immediates, run the
+// step on all 256 values of A and compare the outputs.
+uint8_t classify_a(uint16_t op) {
+  uint64_t x = 0x9E3779B97F4A7C15ull ^ (uint64_t(op) << 32);
+  auto rnd = [&]() {
+    x += 0x9E3779B97F4A7C15ull;
+    uint64_t z = x;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+  };
+  const int kind = op_table()[op].imm;
+  const uint16_t imms[5] = {0x0000, 0x0001, 0x0080, 0xFFFF, 0x5A3C};
+  bool pass = true, over = true;
+  for (int ii = 0; ii < (kind ? 5 : 1); ii++) {
+    const uint16_t imm = kind == 1 ? uint16_t(imms[ii] & 0xFFu) : imms[ii];
+    for (int k = 0; k < 66; k++) {
+      const uint64_t r = k == 0 ? 0 : (k == 1 ? ~0ull : rnd());
+      const uint64_t r2 = k == 0 ? 0 : (k == 1 ? ~0ull : rnd());
+      z80b::Z80S base{0, uint32_t(r & 0xFF), uint32_t((r >> 8) & 0xFF), uint32_t((r >> 16) & 0xFF),
+                      uint32_t((r >> 24) & 0xFF), uint32_t((r >> 32) & 0xFF), uint32_t((r >> 40) & 0xFF),
+                      uint32_t((r >> 48) & 0xFF), uint32_t(r2 & 0xFFFF), uint32_t((r2 >> 16) & 0xFF)};
+      z80b::Z80S out0{};
+      uint32_t a_first = 0;
+      for (uint32_t a = 0; a < 256; a++) {
+        z80b::Z80S s = base;
+        s.a = a;
+        z80b::z_step(s, op, imm);
+        if (a == 0) {
+          out0 = s;
+          a_first = s.a;
+        } else if (s.f != out0.f || s.b != out0.b || s.c != out0.c || s.d != out0.d || s.e != out0.e ||
+                   s.h != out0.h || s.l != out0.l || s.sp != out0.sp || s.m != out0.m) {
+          return kADepends;
+        }
+        if (s.a != a) pass = false;
+        if (s.a != a_first) over = false;
+      }
+      if (!pass && !over) return kADepends;
+    }
+  }
+  return pass ? kAPass : (over ? kAOverwrite : kADepends);
+}
+}  // namespace
+
+const uint8_t* op_aclass() {
+  static uint8_t cls[kNumOps];
+  static std::once_flag once;
+  std::call_once(once, [] {
+    for (int op = 0; op < kNumOps; op++) cls[op] = classify_a(uint16_t(op));
+  });
+  return cls;
+}
+
+uint32_t seq_aflow(const uint32_t* s, int n) {
+  const uint8_t* c = op_aclass();
+  bool a_is_x = true;
+  for (int i = 0; i < n; i++) {
+    const uint8_t k = c[insn_op(s[i])];
+    if (k == kADepends && a_is_x) return 0;
+    if (k == kAOverwrite) a_is_x = false;
+  }
+  return a_is_x ? 3u : 1u;
+}
 const char* op_mnemonic(uint16_t op) { return tables().cat[op].mnem.c_str(); }
 const uint8_t* op_encoding(uint16_t op, int* n) {
   *n = tables().cat[op].nenc;

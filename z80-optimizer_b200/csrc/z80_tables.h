@@ -15,6 +15,17 @@
 namespace z80b {
 
 const OpInfo* op_table();                 // kNumOps entries
+
+// How an instruction's outputs depend on the input value of A (derived by
+// running the step function on every A value of sampled input states):
+//   kADepends    some output other than A, or A itself, depends on A
+//   kAPass       A passes through unchanged, nothing else depends on A
+//   kAOverwrite  A is written from other inputs, nothing depends on A
+enum AClass : uint8_t { kADepends = 0, kAPass = 1, kAOverwrite = 2 };
+const uint8_t* op_aclass();               // kNumOps entries
+// Folds the classes over a sequence: 0 when some output depends on the input
+// A; else 1 (A is overwritten) or 3 (A passes through to the output).
+uint32_t seq_aflow(const uint32_t* s, int n);
 const char* op_mnemonic(uint16_t op);     // "ADD A, n" style with placeholders
 const uint8_t* op_encoding(uint16_t op, int* n);
 std::string disassemble(uint32_t insn);   // catalog.go:73-127

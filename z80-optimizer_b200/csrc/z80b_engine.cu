@@ -454,12 +454,12 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
   CK(ctx->meta.ensure(sizeof(TargetMeta) * n));
   CK(ctx->checks.ensure(8));
   CK(ctx->checked.ensure(8));
-  CK(ctx->states.ensure(8));
+  CK(ctx->states.ensure(16));
   CK(ctx->npairs.ensure(4));
   CK(ctx->counter.ensure(8));
   CK(cudaMemsetAsync(ctx->checks.p, 0, 8, s));
   CK(cudaMemsetAsync(ctx->checked.p, 0, 8, s));
-  CK(cudaMemsetAsync(ctx->states.p, 0, 8, s));
+  CK(cudaMemsetAsync(ctx->states.p, 0, 16, s));
 
   trace("pipeline: %u targets, mode %u, pool %u", n, mode, P.n);
   Timer tall{ctx, 0, 1};
@@ -697,17 +697,18 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
   CK(cudaStreamSynchronize(s));
   trace("pipeline done: %llu rules, %u rounds", (unsigned long long)*nr, rounds);
   if (st) {
-    unsigned long long checks = 0, checked = 0, states = 0;
+    unsigned long long checks = 0, checked = 0, states[2] = {0, 0};
     CKR(fetch(ctx, &checks, ctx->checks.as<unsigned long long>()));
     CKR(fetch(ctx, &checked, ctx->checked.as<unsigned long long>()));
-    CKR(fetch(ctx, &states, ctx->states.as<unsigned long long>()));
+    CKR(fetch(ctx, states, ctx->states.as<unsigned long long>(), 2));
     st->targets += n;
     st->checks += checks;
     st->checked_ref += (mode == Z80B_MODE_FIRST) ? checked : 0;
     st->qc_survivors += nsurv;
     st->mid_survivors += mid_surv;
     st->exhaustive_pairs += exh_pairs;
-    st->exhaustive_states += states;
+    st->exhaustive_states += states[0];
+    st->exhaustive_evaluated += states[1];
     st->rules += *nr;
     st->rounds += rounds;
     double a = 0, b = 0;
@@ -1081,7 +1082,13 @@ int z80b_verify_pairs(z80b_ctx* ctx, const uint32_t* tgt, const uint8_t* tlens, 
       pr[i].nblocks = w.states / 256;
       pr[i].keepF = uint8_t(~(dead ? dead[i] : 0u));
       pr[i].keepR = 0x3F;
-      unsigned long long c = (pr[i].nblocks + ctx->chunk_blocks - 1) / uint64_t(ctx->chunk_blocks);
+      // A-independent pairs are swept in units of 128 blocks (see the sweep kernel)
+      unsigned long long units = pr[i].nblocks;
+      if (seq_aflow(tgt + (size_t)i * stride, tlens[i]) && seq_aflow(cand + (size_t)i * stride, clens[i])) {
+        pr[i].keepR |= 0x40;
+        units = (pr[i].nblocks + 127) / 128;
+      }
+      unsigned long long c = (units + ctx->chunk_blocks - 1) / uint64_t(ctx->chunk_blocks);
       nch[i] = c > 65536 ? 65536 : c;
       cb[i] = tot;
       tot += nch[i];
@@ -1090,7 +1097,7 @@ int z80b_verify_pairs(z80b_ctx* ctx, const uint32_t* tgt, const uint8_t* tlens, 
     CK(ctx->cbase.ensure(8ull * n));
     CK(ctx->rejected.ensure(4ull * n));
     CK(ctx->counter.ensure(8));
-    CK(ctx->states.ensure(8));
+    CK(ctx->states.ensure(16));
     CK(cudaMemcpyAsync(ctx->pairs.p, pr.data(), sizeof(PairRec) * n, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(ctx->cbase.p, cb.data(), 8ull * n, cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(ctx->rejected.p, 0, 4ull * n, s));

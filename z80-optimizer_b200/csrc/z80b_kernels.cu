@@ -43,6 +43,11 @@ __device__ OpInfo g_ops[kNumOps];
 __device__ uint32_t g_vec[32][3];  // MidCheck vectors; the first 8 are the QuickCheck vectors
 __constant__ uint8_t c_rep[32];
 __constant__ uint16_t c_repsp[16];
+// Lane-indexed copies of the sweep values and the A-dependence class per
+// opcode (AClass of z80_tables.h).
+__device__ uint8_t g_rep[32];
+__device__ uint16_t g_repsp[16];
+__device__ uint8_t g_aclass[kNumOps];
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 __device__ __forceinline__ unsigned lanemask_lt() {
@@ -103,6 +108,34 @@ __device__ __forceinline__ unsigned long long sweep_blocks(uint32_t reads) {
   if (n == 0 && !sp) return 2ull;
   if (n <= 2 && !sp) return 2ull << (8 * n);
   return (2ull << (5 * n)) * (sp ? 16ull : 1ull);
+}
+// A-independent sweeps.  When no output of either sequence depends on the
+// input A except A itself passing through (AClass folds of both sequences),
+// every output but A is the same for all 256 values of A, and A_out is
+// either A_in or a value independent of A_in in each sequence; two values of
+// A then decide the verdict of all 256 (equal outputs at A = 0 and A = 1
+// imply equal non-A outputs and either both pass A through or both write the
+// same constant; a sequence passing A through against one writing a
+// constant differs at one of the two).  Such a pair is swept as "units" of
+// 128 A-blocks with A in {0, 1}: 256 states evaluated per unit instead of
+// 32,768.  PairRec.keepR bit 6 marks it.
+constexpr uint32_t kXIndep = 0x40u;
+constexpr unsigned long long kUnitBlocks = 128;
+__device__ __forceinline__ uint32_t dev_seq_aflow(const uint32_t* w, uint32_t n) {
+  bool a_is_x = true;
+  for (uint32_t i = 0; i < n; i++) {
+    const uint32_t k = g_aclass[w[i] & 0xFFFFu];
+    if (k == 0u && a_is_x) return 0u;
+    if (k == 2u) a_is_x = false;
+  }
+  return a_is_x ? 3u : 1u;
+}
+__device__ __forceinline__ bool pair_xindep(const DevTargets& T, uint32_t t, const DevPool& P, uint32_t c) {
+  return dev_seq_aflow(T.insn + (size_t)t * T.stride, target_len(T, t)) != 0u &&
+         dev_seq_aflow(P.insn + (size_t)c * P.stride, pool_len(P, c)) != 0u;
+}
+__device__ __forceinline__ unsigned long long pair_units(unsigned long long nblocks, uint32_t keepR) {
+  return (keepR & kXIndep) ? (nblocks + kUnitBlocks - 1) / kUnitBlocks : nblocks;
 }
 constexpr unsigned long long kMaxChunks = 65536;
 // Work chunks of a sweep: cb A-blocks each (cb is the tuning option), at
@@ -367,6 +400,7 @@ __global__ void k_round_build(DevTargets T, DevPool P, QCOut q, Lanes L, RoundBu
       pr[kind].nblocks = sweep_blocks(reads);
       pr[kind].keepF = kind ? uint8_t(~target_dead(T, t)) : uint8_t(0xFFu);
       pr[kind].keepR = kind ? uint8_t((~target_dead_regs(T, t) & 0x3Fu) | 0x80u) : uint8_t(0x3Fu);
+      if (pair_xindep(T, t, P, c)) pr[kind].keepR |= uint8_t(kXIndep);
       src[kind] = sidx;
       have[kind] = true;
     }
@@ -382,7 +416,7 @@ __global__ void k_round_build(DevTargets T, DevPool P, QCOut q, Lanes L, RoundBu
       uint32_t p = base + __popc(b & lanemask_lt());
       R.pairs[p] = pr[kind];
       R.pair_src[p] = src[kind];
-      R.nchunks[p] = chunks_for(pr[kind].nblocks, R.chunk_blocks);
+      R.nchunks[p] = chunks_for(pair_units(pr[kind].nblocks, pr[kind].keepR), R.chunk_blocks);
       R.rejected[p] = 0;
     }
   }
@@ -405,6 +439,7 @@ __global__ void k_pairs_from_survivors(DevTargets T, DevPool P, QCOut q, const u
     pr.nblocks = sweep_blocks(reads);
     pr.keepF = uint8_t(~target_dead(T, t));
     pr.keepR = uint8_t(~target_dead_regs(T, t) & 0x3Fu);
+    if (pair_xindep(T, t, P, c)) pr.keepR |= uint8_t(kXIndep);
     have = true;
   }
   unsigned b = __ballot_sync(kFull, have);
@@ -416,7 +451,7 @@ __global__ void k_pairs_from_survivors(DevTargets T, DevPool P, QCOut q, const u
     uint32_t p = base + __popc(b & lanemask_lt());
     R.pairs[p] = pr;
     R.pair_src[p] = i;
-    R.nchunks[p] = chunks_for(pr.nblocks, R.chunk_blocks);
+    R.nchunks[p] = chunks_for(pair_units(pr.nblocks, pr.keepR), R.chunk_blocks);
     R.rejected[p] = 0;
   }
 }
@@ -424,12 +459,125 @@ __global__ void k_pairs_from_survivors(DevTargets T, DevPool P, QCOut q, const u
 // K = states per lane per dispatch ("vectors per lane").  One warp
 // iteration covers 32*K values of A; an A-block (256 states) takes 8/K
 // iterations.
+// Initial register values of A-block ab (everything but A and F's carry):
+// block index fields fastest first: SP (reduced sweeps), the swept registers
+// from the last to the first, carry.  UNIFORM selects the __constant__
+// tables (the index is the same in every lane) or their global copies
+// (lane-dependent index).
+template <bool UNIFORM>
+__device__ __forceinline__ void decode_block(unsigned long long ab, bool spw, bool reduced, int nx, int fw,
+                                             const int (&slot)[7], Z80S& init) {
+  unsigned long long rest = ab;
+  uint32_t sp = 0;
+  if (spw) {
+    sp = UNIFORM ? c_repsp[uint32_t(rest & 15ull)] : g_repsp[uint32_t(rest & 15ull)];
+    rest >>= 4;
+  }
+  uint32_t fieldv[7];
+#pragma unroll
+  for (int f = 6; f >= 0; f--) {
+    fieldv[f] = 0;
+    if (f < nx) {
+      const uint32_t x = uint32_t(rest) & (reduced ? 31u : 255u);
+      fieldv[f] = reduced ? (UNIFORM ? c_rep[x] : g_rep[x]) : x;
+      rest >>= fw;
+    }
+  }
+  uint32_t rv[7];
+#pragma unroll
+  for (int r = 0; r < 7; r++) {
+    uint32_t v = 0;
+#pragma unroll
+    for (int f = 0; f < 7; f++)
+      if (slot[r] == f) v = fieldv[f];
+    rv[r] = v;
+  }
+  init.a = 0;
+  init.f = uint32_t(rest & 1ull);
+  init.b = rv[0]; init.c = rv[1]; init.d = rv[2]; init.e = rv[3];
+  init.h = rv[4]; init.l = rv[5]; init.m = rv[6];
+  init.sp = sp;
+}
+
+// Runs the candidate then the target from K initial states (init(q, x)
+// writes state q) and reports whether any compared output differs (only
+// states with valid[q]).
+template <int K, class Init>
+__device__ __forceinline__ bool run_compare(const Init& init, const bool (&valid)[K], uint32_t pw, int tl, int cl,
+                                            uint32_t keep0, uint32_t keep1) {
+  Z80S X[K];
+  uint32_t P0[K], P1[K], P2[K];
+  const int nsteps = tl + cl;
+  // one dispatch site: the candidate runs first; its output is packed into
+  // three words per state, the registers are re-initialised and the target
+  // runs on them
+#pragma unroll 1
+  for (int st = -1; st < nsteps; st++) {
+    if (st == -1 || st == cl) {
+      if (st == cl) {
+#pragma unroll
+        for (int q = 0; q < K; q++) {
+          P0[q] = X[q].a | (X[q].f << 8) | (X[q].b << 16) | (X[q].c << 24);
+          P1[q] = X[q].d | (X[q].e << 8) | (X[q].h << 16) | (X[q].l << 24);
+          P2[q] = X[q].sp | (X[q].m << 16);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < K; q++) init(q, X[q]);
+      if (st == -1) continue;
+    }
+    // lanes tl.. hold the candidate, lanes 0.. the target
+    const int src = st < cl ? tl + st : st - cl;
+    const uint32_t w = __shfl_sync(kFull, pw, src);
+    z_stepK<K>(X, w & 0xFFFFu, w >> 16);
+  }
+  bool bad = false;
+#pragma unroll
+  for (int q = 0; q < K; q++) {
+    const uint32_t d0 = (X[q].a | (X[q].f << 8) | (X[q].b << 16) | (X[q].c << 24)) ^ P0[q];
+    const uint32_t d1 = (X[q].d | (X[q].e << 8) | (X[q].h << 16) | (X[q].l << 24)) ^ P1[q];
+    const uint32_t d2 = (X[q].sp | (X[q].m << 16)) ^ P2[q];
+    bad = bad || (valid[q] && ((d0 & keep0) | (d1 & keep1) | d2) != 0);
+  }
+  return bad;
+}
+
+// One unit (128 A-blocks at A = 0, 1) of an A-independent sweep; kept out of
+// line so its registers do not weigh on the A-block loop.
+template <int K>
+__device__ __noinline__ bool xindep_unit(unsigned long long first, unsigned long long nb, bool spw, bool reduced,
+                                         int nx, int fw, const int* slotp, uint32_t pw, int tl, int cl,
+                                         uint32_t keep0, uint32_t keep1) {
+  const unsigned lane = lane_id();
+  int slot[7];
+#pragma unroll
+  for (int r = 0; r < 7; r++) slot[r] = slotp[r];
+  bool bad = false;
+#pragma unroll 1
+  for (uint32_t i = 0; i < 8u / K; i++) {
+    uint32_t W[K][3];  // initial states, packed
+    bool valid[K];
+#pragma unroll
+    for (int q = 0; q < K; q++) {
+      const uint32_t sl = (i * K + q) * 32u + lane;
+      valid[q] = (sl >> 1) < nb;
+      Z80S x;
+      decode_block<false>(valid[q] ? first + (sl >> 1) : first, spw, reduced, nx, fw, slot, x);
+      x.a = sl & 1u;
+      z_pack(x, W[q]);
+    }
+    auto init = [&](int q, Z80S& x) { x = z_unpack(W[q][0], W[q][1], W[q][2]); };
+    bad = run_compare<K>(init, valid, pw, tl, cl, keep0, keep1) || bad;
+  }
+  return bad;
+}
+
 template <int K>
 __global__ void __launch_bounds__(kBlock, K <= 4 ? 2 : 1) k_exhaustive(DevTargets T, DevPool P, RoundBuf R, uint32_t npairs,
                                                        unsigned long long total) {
   static_assert(K == 1 || K == 2 || K == 4 || K == 8, "K divides 8");
   const unsigned lane = lane_id();
-  unsigned long long my_states = 0;
+  unsigned long long my_states = 0, my_eval = 0;
   for (;;) {
     unsigned long long k = 0;
     if (lane == 0) k = atomicAdd(R.counter, 1ull);
@@ -448,19 +596,20 @@ __global__ void __launch_bounds__(kBlock, K <= 4 ? 2 : 1) k_exhaustive(DevTarget
     if (__shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0))
       continue;
     const PairRec pr = R.pairs[p];
+    const bool xind = (pr.keepR & kXIndep) != 0;
+    const unsigned long long nunits = pair_units(pr.nblocks, pr.keepR);
     const unsigned long long nch = (p + 1 < npairs ? R.cbase[p + 1] : total) - R.cbase[p];
-    const unsigned long long bpc = (pr.nblocks + nch - 1) / nch;
+    const unsigned long long upc = (nunits + nch - 1) / nch;
     const unsigned long long j = k - R.cbase[p];
-    const unsigned long long b0 = j * bpc;
-    unsigned long long b1 = b0 + bpc;
-    if (b1 > pr.nblocks) b1 = pr.nblocks;
+    const unsigned long long u0 = j * upc;
+    unsigned long long u1 = u0 + upc;
+    if (u1 > nunits) u1 = nunits;
 
     // programs: lanes 0..tl-1 target, tl..tl+cl-1 candidate
     const uint32_t tl = target_len(T, pr.target), cl = pool_len(P, pr.cand);
     uint32_t pw = 0;
     if (lane < tl) pw = T.insn[(size_t)pr.target * T.stride + lane];
     else if (lane < tl + cl) pw = P.insn[(size_t)pr.cand * P.stride + (lane - tl)];
-    const int nsteps = int(tl + cl);
 
     // sweep shape (verifier.go:428-476): extra registers in B,C,D,E,H,L,M order
     const uint32_t ext = pr.reads & (kRegB | kRegC | kRegD | kRegE | kRegH | kRegL | kRegM);
@@ -482,91 +631,58 @@ __global__ void __launch_bounds__(kBlock, K <= 4 ? 2 : 1) k_exhaustive(DevTarget
                            ((pr.keepR & 16u) ? 0xFF0000u : 0u) | ((pr.keepR & 32u) ? 0xFF000000u : 0u);
 
     bool bad = false;
-    // Block index fields, fastest first: SP (reduced sweeps), the swept
-    // registers from the last to the first, carry.  The reference nests its
-    // loops as A, carry, first register, ..., last register, SP
-    // (verifier.go:498-531,578-610), so block b covers the reference's
-    // states (A, b) for every A at once and a sweep that the reference
-    // abandons early is abandoned at least as early here.
-    for (unsigned long long ab = b0; ab < b1; ab++) {
-      unsigned long long rest = ab;
-      uint32_t sp = 0;
-      if (spw) {
-        sp = c_repsp[uint32_t(rest & 15ull)];
-        rest >>= 4;
-      }
-      uint32_t fieldv[7];
+    if (!xind) {
+      // Unit = one A-block: the 256 values of A for one assignment of carry,
+      // swept registers and SP; lanes take 32 consecutive A values per
+      // dispatch.  The reference nests its loops as A, carry, first
+      // register, ..., last register, SP (verifier.go:498-531,578-610), so
+      // block b covers the reference's states (A, b) for every A at once and
+      // a sweep the reference abandons early is abandoned at least as early
+      // here.
+      bool valid[K];
 #pragma unroll
-      for (int f = 6; f >= 0; f--) {
-        fieldv[f] = 0;
-        if (f < nx) {
-          const uint32_t x = uint32_t(rest) & (reduced ? 31u : 255u);
-          fieldv[f] = reduced ? c_rep[x] : x;
-          rest >>= fw;
-        }
-      }
-      const uint32_t carry = uint32_t(rest & 1ull);
-      uint32_t rv[7];
-#pragma unroll
-      for (int r = 0; r < 7; r++) {
-        uint32_t v = 0;
-#pragma unroll
-        for (int f = 0; f < 7; f++)
-          if (slot[r] == f) v = fieldv[f];
-        rv[r] = v;
-      }
+      for (int q = 0; q < K; q++) valid[q] = true;
+      for (unsigned long long ab = u0; ab < u1; ab++) {
+        Z80S base;
+        decode_block<true>(ab, spw, reduced, nx, fw, slot, base);
 #pragma unroll 1
-      for (uint32_t i = 0; i < 8u / K; i++) {
-        Z80S X[K];
-        uint32_t P0[K], P1[K], P2[K];
-        // one dispatch site: the candidate runs first; its output is packed
-        // into three words per state, the registers are re-initialised and
-        // the target runs on them
-#pragma unroll 1
-        for (int st = -1; st < nsteps; st++) {
-          if (st == -1 || st == int(cl)) {
-            if (st == int(cl)) {
-#pragma unroll
-              for (int q = 0; q < K; q++) {
-                P0[q] = X[q].a | (X[q].f << 8) | (X[q].b << 16) | (X[q].c << 24);
-                P1[q] = X[q].d | (X[q].e << 8) | (X[q].h << 16) | (X[q].l << 24);
-                P2[q] = X[q].sp | (X[q].m << 16);
-              }
-            }
-#pragma unroll
-            for (int q = 0; q < K; q++) {
-              X[q].a = (i * K + q) * 32u + lane;
-              X[q].f = carry;
-              X[q].b = rv[0]; X[q].c = rv[1]; X[q].d = rv[2]; X[q].e = rv[3];
-              X[q].h = rv[4]; X[q].l = rv[5]; X[q].m = rv[6];
-              X[q].sp = sp;
-            }
-            if (st == -1) continue;
-          }
-          // lanes tl.. hold the candidate, lanes 0.. the target
-          const int src = st < int(cl) ? int(tl) + st : st - int(cl);
-          const uint32_t w = __shfl_sync(kFull, pw, src);
-          z_stepK<K>(X, w & 0xFFFFu, w >> 16);
+        for (uint32_t i = 0; i < 8u / K; i++) {
+          auto init = [&](int q, Z80S& x) {
+            x = base;
+            x.a = (i * K + uint32_t(q)) * 32u + lane;
+          };
+          bad = run_compare<K>(init, valid, pw, int(tl), int(cl), keep0, keep1) || bad;
         }
-#pragma unroll
-        for (int q = 0; q < K; q++) {
-          const uint32_t d0 = (X[q].a | (X[q].f << 8) | (X[q].b << 16) | (X[q].c << 24)) ^ P0[q];
-          const uint32_t d1 = (X[q].d | (X[q].e << 8) | (X[q].h << 16) | (X[q].l << 24)) ^ P1[q];
-          const uint32_t d2 = (X[q].sp | (X[q].m << 16)) ^ P2[q];
-          bad = bad || ((d0 & keep0) | (d1 & keep1) | d2) != 0;
-        }
+        my_states += 256;
+        my_eval += 256;
+        if (__any_sync(kFull, bad)) break;
+        if ((ab & 15ull) == 15ull &&
+            __shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0))
+          break;
       }
-      my_states += 256;
-      if (__any_sync(kFull, bad)) break;
-      if ((ab & 15ull) == 15ull &&
-          __shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0))
-        break;
+    } else {
+      // Unit = 128 A-blocks, each evaluated at A = 0 and A = 1: state slot s
+      // of the warp (s = (i*K + q)*32 + lane) takes block unit*128 + s/2 with
+      // A = s & 1.
+      for (unsigned long long u = u0; u < u1; u++) {
+        const unsigned long long first = u * kUnitBlocks;
+        const unsigned long long nb = (pr.nblocks - first < kUnitBlocks) ? pr.nblocks - first : kUnitBlocks;
+        bad = xindep_unit<K>(first, nb, spw, reduced, nx, fw, slot, pw, int(tl), int(cl), keep0, keep1) || bad;
+        my_states += 256ull * nb;
+        my_eval += 2ull * nb;
+        if (__any_sync(kFull, bad)) break;
+        if ((u & 3ull) == 3ull &&
+            __shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0))
+          break;
+      }
     }
     if (__any_sync(kFull, bad) && lane == 0) atomicExch(&R.rejected[p], 1u);
   }
-  if (lane == 0 && my_states) atomicAdd(R.states, my_states);
+  if (lane == 0 && my_states) {
+    atomicAdd(R.states, my_states);
+    atomicAdd(R.states + 1, my_eval);
+  }
 }
-
 __global__ void k_round_resolve(RoundBuf R, uint32_t npairs, QCOut q, Lanes L) {
   uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npairs) return;
@@ -926,6 +1042,7 @@ __global__ void k_pair_round_build(DevTargets T, DevPool P, QCOut q1, Lanes L2, 
         pr.nblocks = sweep_blocks(reads);
         pr.keepF = kind ? uint8_t(~target_dead(T, t)) : uint8_t(0xFFu);
         pr.keepR = kind ? uint8_t((~target_dead_regs(T, t) & 0x3Fu) | 0x80u) : uint8_t(0x3Fu);
+        if (pair_xindep(T, t, P, c)) pr.keepR |= uint8_t(kXIndep);
         have = true;
       } else if (ps.resume[idx] == kNone) {
         L2.next[idx] = nx | kResolved;
@@ -943,7 +1060,7 @@ __global__ void k_pair_round_build(DevTargets T, DevPool P, QCOut q1, Lanes L2, 
     const uint32_t p = base + __popc(b & lanemask_lt());
     R.pairs[p] = pr;
     R.pair_src[p] = src;
-    R.nchunks[p] = chunks_for(pr.nblocks, R.chunk_blocks);
+    R.nchunks[p] = chunks_for(pair_units(pr.nblocks, pr.keepR), R.chunk_blocks);
     R.rejected[p] = 0;
   }
 }
@@ -977,6 +1094,9 @@ void dev_upload_tables(cudaStream_t s) {
   cudaMemcpyToSymbolAsync(g_vec, mid_vectors(), sizeof(uint32_t) * 32 * 3, 0, cudaMemcpyHostToDevice, s);
   cudaMemcpyToSymbolAsync(c_rep, rep_values(), 32, 0, cudaMemcpyHostToDevice, s);
   cudaMemcpyToSymbolAsync(c_repsp, rep_sp(), 32, 0, cudaMemcpyHostToDevice, s);
+  cudaMemcpyToSymbolAsync(g_rep, rep_values(), 32, 0, cudaMemcpyHostToDevice, s);
+  cudaMemcpyToSymbolAsync(g_repsp, rep_sp(), 32, 0, cudaMemcpyHostToDevice, s);
+  cudaMemcpyToSymbolAsync(g_aclass, op_aclass(), kNumOps, 0, cudaMemcpyHostToDevice, s);
 }
 
 void launch_pool_outputs(const uint32_t* insn, uint32_t n, uint32_t len, uint4* qc, uint4* mid,

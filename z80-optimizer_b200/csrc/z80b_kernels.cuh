@@ -41,7 +41,7 @@ struct RoundBuf {
   uint32_t* rejected;              // per pair
   uint32_t* npairs;                // device counter
   unsigned long long* counter;     // chunk dispenser
-  unsigned long long* states;      // states verified (stat)
+  unsigned long long* states;      // [2]: states of the reference's sweeps covered, states evaluated
   uint32_t chunk_blocks;           // A-blocks per work chunk
 };
 

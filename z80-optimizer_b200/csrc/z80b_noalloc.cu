@@ -38,7 +38,7 @@ constexpr size_t kOffCbase = align256(kOffPairs + sizeof(PairRec) * kMaxPairs);
 constexpr size_t kOffRej = align256(kOffCbase + 8ull * kMaxPairs);
 constexpr size_t kOffCounter = align256(kOffRej + 4ull * kMaxPairs);
 constexpr size_t kOffStates = kOffCounter + 8;
-constexpr size_t kNoAllocBytes = align256(kOffStates + 8);
+constexpr size_t kNoAllocBytes = align256(kOffStates + 16);
 static_assert(kNoAllocBytes <= 320 * 1024, "the scratch stays modest");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
@@ -110,7 +110,13 @@ extern "C" int z80b_exhaustive_noalloc(int device, const uint32_t* tgt, const ui
     p.nblocks = sweep_for(rd).states / 256;
     p.keepF = uint8_t(~(dead ? dead[i] : 0u));
     p.keepR = 0x3F;
-    unsigned long long ch = (p.nblocks + 31) / 32;
+    // A-independent pairs are swept in units of 128 blocks (see the sweep kernel)
+    unsigned long long units = p.nblocks;
+    if (seq_aflow(&h_tgt[size_t(i) * kStride], int(tl)) && seq_aflow(&h_cand[size_t(i) * kStride], int(cl))) {
+      p.keepR |= 0x40;
+      units = (p.nblocks + 127) / 128;
+    }
+    unsigned long long ch = (units + 31) / 32;
     if (ch > 65536) ch = 65536;
     h_cbase[i] = total;
     total += ch;
@@ -131,7 +137,7 @@ extern "C" int z80b_exhaustive_noalloc(int device, const uint32_t* tgt, const ui
             cudaMemcpyAsync(base + kOffPairs, h_pairs, sizeof(PairRec) * n, cudaMemcpyHostToDevice, s) == cudaSuccess &&
             cudaMemcpyAsync(base + kOffCbase, h_cbase, 8ull * n, cudaMemcpyHostToDevice, s) == cudaSuccess &&
             cudaMemsetAsync(base + kOffRej, 0, 4ull * n, s) == cudaSuccess &&
-            cudaMemsetAsync(base + kOffCounter, 0, 16, s) == cudaSuccess;
+            cudaMemsetAsync(base + kOffCounter, 0, 24, s) == cudaSuccess;
   if (dead) ok = ok && cudaMemcpyAsync(base + kOffDead, dead, n, cudaMemcpyHostToDevice, s) == cudaSuccess;
   else ok = ok && cudaMemsetAsync(base + kOffDead, 0, n, s) == cudaSuccess;
   if (!ok) return Z80B_ECUDA;

@@ -1,9 +1,14 @@
-"""Small, fixed search case for profiler captures of the sweep kernel.
+"""Small, fixed cases for profiler captures, through the library's public API.
 
-Runs the first-found search (pkg/search/worker.go:124-265 semantics) on a
-seeded sample of the length-2 target set through the library's public API,
-`--steps` times, and prints one line of statistics per step.  The case is
-sized to keep a full-metric-set capture of one k_exhaustive launch short:
+  --case c2      first-found search (pkg/search/worker.go:124-265) on a seeded
+                 sample of the length-2 targets (the sweep kernel k_exhaustive)
+  --case c3      the batched uneven workload: seeded C3 targets with dead
+                 masks, candidates up to 2 instructions (k_pair_scan)
+  --case mulopt  constant multiply, all K over one pool up to --max-len
+                 (k_mul_length; one launch per length)
+
+Each runs `--steps` times and prints one line of statistics per step; sizes
+keep a full-metric-set capture of one launch short, e.g.
 
     python z80-optimizer_b200/profile_case.py --targets 30000 --seed 3 --steps 2
 
@@ -33,7 +38,33 @@ def main():
     ap.add_argument("--lane-states", type=int, default=4)
     ap.add_argument("--chunk-blocks", type=int, default=32)
     ap.add_argument("--dead-flags", default="none")
+    ap.add_argument("--case", default="c2", choices=["c2", "c3", "mulopt"])
+    ap.add_argument("--pool", type=int, default=2, help="mulopt pool (Z80B_MULPOOL_*)")
+    ap.add_argument("--max-len", type=int, default=9, help="mulopt: longest sequence")
     a = ap.parse_args()
+    if a.case == "mulopt":
+        ctx = z80b.Context(0)
+        init = workloads.mul_init(2) if a.pool == 1 else (0, 0, 0)
+        for i in range(a.steps):
+            res, st = ctx.mul_search(a.pool, init, 1, a.max_len)
+            print(f"step {i}: {sum(r['found'] for r in res)} constants found, {st.sequences:.4e} sequences, "
+                  f"{st.launches} launches, device {st.device_ms:.2f} ms", flush=True)
+        ctx.close()
+        return 0
+    if a.case == "c3":
+        ctx = z80b.Context(0)
+        ctx.set_option(OPT_LANE_STATES, a.lane_states)
+        ctx.set_option(OPT_CHUNK_BLOCKS, a.chunk_blocks)
+        arr, lens, dead, dregs = workloads.c3_targets(a.targets, seed=1)
+        targets = [list(map(int, arr[i, :lens[i]])) for i in range(a.targets)]
+        job, keep = ctx.make_job(targets, per_target_dead=list(map(int, dead)), dead_regs=list(map(int, dregs)),
+                                 max_cand_len=2)
+        for i in range(a.steps):
+            rules, st = ctx.run_job(job)
+            print(f"step {i}: {len(rules)} rules, {st.checks} checks, {st.exhaustive_pairs} exhaustive pairs, "
+                  f"{st.rounds} rounds, {st.launches} launches, device {st.device_ms:.2f} ms", flush=True)
+        ctx.close()
+        return 0
     arr = np.ascontiguousarray(workloads.c2_subset(a.targets, seed=a.seed))
     ctx = z80b.Context(0)
     ctx.set_option(OPT_LANE_STATES, a.lane_states)

@@ -73,7 +73,7 @@ class Stats(ctypes.Structure):
                 ("exhaustive_states", ctypes.c_uint64), ("rules", ctypes.c_uint64),
                 ("rounds", ctypes.c_uint32), ("launches", ctypes.c_uint32),
                 ("device_ms", ctypes.c_double), ("qc_ms", ctypes.c_double),
-                ("exh_ms", ctypes.c_double)]
+                ("exh_ms", ctypes.c_double), ("exhaustive_evaluated", ctypes.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
