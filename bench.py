@@ -357,7 +357,7 @@ def main():
         torch.cuda.synchronize()
         _, wst = ctx.run_staged()
         progress(f"warmup {i}: {wst.device_ms:.1f} ms, {wst.exhaustive_states:.3e} states, {wst.rounds} rounds")
-    dev_ms, exh_ms, qc_ms, launches, checks, states, rules = 0.0, 0.0, 0.0, 0, 0, 0, 0
+    dev_ms, exh_ms, qc_ms, launches, checks, states, evaluated, rules = 0.0, 0.0, 0.0, 0, 0, 0, 0, 0
     stats_last = None
     if dist:
         dist.barrier()
@@ -374,6 +374,7 @@ def main():
             launches += st.launches
             checks += st.checks
             states += st.exhaustive_states
+            evaluated += st.exhaustive_evaluated
             rules = n
             stats_last = st
             progress(f"step: {st.device_ms:.1f} ms (qc {st.qc_ms:.1f}, exhaustive {st.exh_ms:.1f})")
@@ -391,7 +392,7 @@ def main():
         checks_all = float(checks)
     value = checks_all / args.steps / (t_step / 1e3)
     # algorithmic emulated instructions of the steps (length-2 targets, length-1 candidates)
-    emulated = 8.0 * checks + 16.0 * len(mine) * args.steps + 3.0 * states
+    emulated = 8.0 * checks + 16.0 * len(mine) * args.steps + 3.0 * evaluated
 
     # ---- e2e: public API with pinned host buffers
     pinned = torch.from_numpy(mine).pin_memory()
@@ -439,7 +440,10 @@ def main():
         pass
     sm_mhz = peaks.get("sm_max_mhz", 1965.0)
     per_state = 3 * rl["ops_per_emulated_insn"] + rl["ops_per_state"]  # 2-insn target + 1-insn candidate
-    achieved = states / args.steps * per_state / (exh_ms / args.steps / 1e3) / 1e12 if exh_ms else 0.0
+    # states the sweep kernel actually ran (A-independent pairs run 2 of
+    # every 256 values of A), so the fraction measures the kernel, not the
+    # states it skips
+    achieved = evaluated / args.steps * per_state / (exh_ms / args.steps / 1e3) / 1e12 if exh_ms else 0.0
     peak = rl["sms"] * rl["int32_lanes_per_sm"] * sm_mhz * 1e6 / 1e12
     # DRAM bytes per sweep launch: the measured bytes per ExhaustiveCheck pair
     # of an ncu capture (profiles/exhaustive_c2_traffic.txt) times this run's
@@ -515,7 +519,9 @@ def main():
             "detail": {"rules": rules, "checked_ref": stats_last.checked_ref if stats_last else None,
                        "qc_survivors": stats_last.qc_survivors if stats_last else None,
                        "exhaustive_pairs": stats_last.exhaustive_pairs if stats_last else None,
-                       "exhaustive_states_per_step": states / args.steps, "rounds": stats_last.rounds if stats_last else None,
+                       "exhaustive_states_per_step": states / args.steps,
+                       "exhaustive_evaluated_per_step": evaluated / args.steps,
+                       "rounds": stats_last.rounds if stats_last else None,
                        "wall_s_timed": wall}}
     ctx.close()
     if dist:
