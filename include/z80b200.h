@@ -256,14 +256,16 @@ int z80b_mul_search(z80b_ctx* ctx, int pool, uint8_t init_b, uint8_t init_c, uin
  * 82-110) with candidates shorter than the target, up to max_cand_len
  * instructions.  Several workers, each with its own context and stream, run
  * batches of waiting queries concurrently (continuous batching: queries that
- * arrive while batches are in flight are admitted by the next free worker);
+ * arrive while batches are in flight are admitted by the next free worker;
+ * queries whose target alone implies a long ExhaustiveCheck sweep are
+ * batched apart from the others);
  * admission charges each query's device frontier memory against
  * memory_budget.  No counterpart in the reference (its serving is one query
  * per z80opt target call). */
 typedef struct z80b_server z80b_server;
 typedef struct z80b_server_config {
   int device;
-  int workers;               /* concurrent batches (contexts); 0: 3 */
+  int workers;               /* concurrent batches (contexts); 0: 4 */
   uint32_t max_batch;        /* queries per batch; 0: 4096 */
   uint64_t memory_budget;    /* device bytes of admitted query frontiers; 0: 64 GiB */
   uint32_t max_cand_len;     /* 1 or 2; 0: 2 */

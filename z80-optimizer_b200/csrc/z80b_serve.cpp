@@ -6,10 +6,13 @@
 // Continuous batching at batch granularity: `workers` threads each own a
 // context (its own stream and device buffers; the length-2 pair pool is
 // shared per device).  A free worker takes every waiting query of one class
-// (candidates up to 1 or up to 2 instructions) up to max_batch and runs them
-// as one first-found job, so new arrivals are admitted by the next free
-// worker while earlier batches are still in flight and their work overlaps
-// on the GPU.  Admission also charges each query's frontier memory (its
+// up to max_batch and runs them as one first-found job, so new arrivals are
+// admitted by the next free worker while earlier batches are still in
+// flight and their work overlaps on the GPU.  A class is the candidate
+// length cap (1 or 2 instructions) and whether the target alone already
+// reads enough registers for an ExhaustiveCheck sweep of 2^26 states or
+// more: such heavy queries are batched apart, so the light ones do not wait
+// behind a long sweep.  Admission also charges each query's frontier memory (its
 // lanes, survivor slots and rule records on the device) against the budget
 // and waits while the in-flight total would exceed it.
 #include <algorithm>
@@ -22,6 +25,7 @@
 #include <vector>
 
 #include "../../include/z80b200.h"
+#include "z80_tables.h"
 
 namespace {
 
@@ -35,8 +39,11 @@ constexpr uint64_t kFrontierBytes = 64 + 16 + 2 * 16 + 2 * 4531 * 6 + 2 * 32 * 6
 struct Pending {
   z80b_query q;
   Clock::time_point t_submit;
-  uint32_t cand;  // candidate length cap of this query
+  uint32_t cand;   // candidate length cap of this query
+  uint32_t klass;  // batch class: cand | heavy << 2
 };
+
+constexpr uint64_t kHeavyStates = 1ull << 26;
 
 }  // namespace
 
@@ -76,8 +83,9 @@ void worker_loop(z80b_server* S, z80b_ctx* ctx) {
       if (S->pending.empty()) return;  // stopping and drained
       // the class of the oldest query; take its class-mates in arrival order
       cand = S->pending.front().cand;
+      const uint32_t klass = S->pending.front().klass;
       for (auto it = S->pending.begin(); it != S->pending.end() && batch.size() < S->cfg.max_batch;) {
-        if (it->cand == cand && S->inflight_bytes + kFrontierBytes <= S->cfg.memory_budget) {
+        if (it->klass == klass && S->inflight_bytes + kFrontierBytes <= S->cfg.memory_budget) {
           batch.push_back(*it);
           S->inflight_bytes += kFrontierBytes;
           it = S->pending.erase(it);
@@ -160,7 +168,7 @@ int z80b_server_start(const z80b_server_config* cfg, z80b_server** out) {
   *out = nullptr;
   z80b_server_config c{};
   if (cfg) c = *cfg;
-  if (c.workers <= 0) c.workers = 3;
+  if (c.workers <= 0) c.workers = 4;
   if (c.workers > 16) return Z80B_EINVAL;
   if (c.max_batch == 0) c.max_batch = 4096;
   if (c.memory_budget == 0) c.memory_budget = 64ull << 30;
@@ -208,7 +216,9 @@ int z80b_server_submit(z80b_server* S, const z80b_query* q, uint32_t n) {
         S->stats.answered++;
         continue;
       }
-      S->pending.push_back(Pending{q[i], now, cap});
+      const bool heavy =
+          z80b::sweep_for(z80b::seq_reads(q[i].target, int(q[i].len))).states >= kHeavyStates;
+      S->pending.push_back(Pending{q[i], now, cap, cap | (heavy ? 4u : 0u)});
     }
   }
   S->cv_work.notify_all();

@@ -73,7 +73,7 @@ def offline_answers(ctx, arr, lens, dead, dregs, idx):
     return res
 
 
-def run(rate, seconds, seed, workers=3, max_batch=4096, verify=True, progress=None):
+def run(rate, seconds, seed, workers=4, max_batch=4096, verify=True, progress=None):
     n = int(rate * seconds)
     arr, lens, dead, dregs = make_queries(n, seed)
     rng = np.random.default_rng(seed + 1000)
@@ -143,7 +143,7 @@ def main():
     ap.add_argument("--rate", type=float, default=2000)
     ap.add_argument("--seconds", type=float, default=60)
     ap.add_argument("--seed", type=int, default=3)
-    ap.add_argument("--workers", type=int, default=3)
+    ap.add_argument("--workers", type=int, default=4)
     ap.add_argument("--no-verify", action="store_true")
     a = ap.parse_args()
     out, _ = run(a.rate, a.seconds, a.seed, a.workers, verify=not a.no_verify)

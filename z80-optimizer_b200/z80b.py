@@ -496,7 +496,7 @@ def mul_results_json(results, pool):
 class Server:
     """Serving loop (z80b_server_*): submit queries from any thread, poll answers."""
 
-    def __init__(self, device=0, workers=3, max_batch=4096, memory_budget=0, max_cand_len=2):
+    def __init__(self, device=0, workers=4, max_batch=4096, memory_budget=0, max_cand_len=2):
         cfg = ServerConfig(device, workers, max_batch, memory_budget, max_cand_len)
         h = ctypes.c_void_p()
         st = lib().z80b_server_start(ctypes.byref(cfg), ctypes.byref(h))
