@@ -194,6 +194,7 @@ int z80b_exhaustive_noalloc(int device, const uint32_t* tgt, const uint8_t* tlen
 /* ---- tuning -------------------------------------------------------------- */
 #define Z80B_OPT_EXH_LANE_STATES 1  /* ExhaustiveCheck states per lane per dispatch: 1, 2, 4, 8 */
 #define Z80B_OPT_EXH_CHUNK_BLOCKS 2 /* A-blocks (256 states) per work chunk: 1..4096 */
+#define Z80B_OPT_STREAM_PRIORITY 3  /* the context's stream: -1 high, 0 default, 1 low priority */
 int z80b_set_option(z80b_ctx* ctx, int option, int value);
 int z80b_get_option(const z80b_ctx* ctx, int option, int* value);
 
@@ -266,7 +267,7 @@ typedef struct z80b_server z80b_server;
 typedef struct z80b_server_config {
   int device;
   int workers;               /* concurrent batches (contexts); 0: 4 */
-  uint32_t max_batch;        /* queries per batch; 0: 4096 */
+  uint32_t max_batch;        /* queries per batch; 0: 512 */
   uint64_t memory_budget;    /* device bytes of admitted query frontiers; 0: 64 GiB */
   uint32_t max_cand_len;     /* 1 or 2; 0: 2 */
 } z80b_server_config;

@@ -143,6 +143,7 @@ struct z80b_ctx {
   uint32_t launches = 0;
   int exh_k = 4;              // ExhaustiveCheck states per lane per dispatch (z80b_set_option)
   int chunk_blocks = 32;      // A-blocks per ExhaustiveCheck work chunk
+  int priority = 0;           // Z80B_OPT_STREAM_PRIORITY
 };
 
 namespace {
@@ -1133,6 +1134,20 @@ int z80b_set_option(z80b_ctx* ctx, int option, int value) {
       if (value < 1 || value > 4096) return fail(ctx, Z80B_EINVAL, "chunk blocks must be 1..4096");
       ctx->chunk_blocks = value;
       return Z80B_OK;
+    case Z80B_OPT_STREAM_PRIORITY: {
+      if (value < -1 || value > 1) return fail(ctx, Z80B_EINVAL, "stream priority must be -1, 0 or 1");
+      int lo = 0, hi = 0;  // numerically lower is higher priority
+      CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+      const int prio = value < 0 ? hi : (value > 0 ? lo : 0);
+      cudaSetDevice(ctx->device);
+      CK(cudaStreamSynchronize(ctx->stream));
+      cudaStream_t ns = nullptr;
+      CK(cudaStreamCreateWithPriority(&ns, cudaStreamNonBlocking, prio));
+      CK(cudaStreamDestroy(ctx->stream));
+      ctx->stream = ns;
+      ctx->priority = value;
+      return Z80B_OK;
+    }
   }
   return fail(ctx, Z80B_EINVAL, "unknown option %d", option);
 }
@@ -1142,6 +1157,7 @@ int z80b_get_option(const z80b_ctx* ctx, int option, int* value) {
   switch (option) {
     case Z80B_OPT_EXH_LANE_STATES: *value = ctx->exh_k; return Z80B_OK;
     case Z80B_OPT_EXH_CHUNK_BLOCKS: *value = ctx->chunk_blocks; return Z80B_OK;
+    case Z80B_OPT_STREAM_PRIORITY: *value = ctx->priority; return Z80B_OK;
   }
   return Z80B_EINVAL;
 }

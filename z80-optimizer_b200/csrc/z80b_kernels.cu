@@ -138,6 +138,7 @@ __device__ __forceinline__ unsigned long long pair_units(unsigned long long nblo
   return (keepR & kXIndep) ? (nblocks + kUnitBlocks - 1) / kUnitBlocks : nblocks;
 }
 constexpr unsigned long long kMaxChunks = 65536;
+constexpr int kChunksPerWarp = 64;
 // Work chunks of a sweep: cb A-blocks each (cb is the tuning option), at
 // most kMaxChunks per pair.
 __device__ __forceinline__ unsigned long long chunks_for(unsigned long long nb, uint32_t cb) {
@@ -578,7 +579,10 @@ __global__ void __launch_bounds__(kBlock, K <= 4 ? 2 : 1) k_exhaustive(DevTarget
   static_assert(K == 1 || K == 2 || K == 4 || K == 8, "K divides 8");
   const unsigned lane = lane_id();
   unsigned long long my_states = 0, my_eval = 0;
-  for (;;) {
+  // At most kChunksPerWarp chunks per warp, then the block retires: the grid
+  // covers all chunks, and blocks of kernels on other streams (with a higher
+  // priority) get SMs as soon as blocks of a long sweep retire.
+  for (int taken = 0; taken < kChunksPerWarp; taken++) {
     unsigned long long k = 0;
     if (lane == 0) k = atomicAdd(R.counter, 1ull);
     k = __shfl_sync(kFull, k, 0);
@@ -1162,9 +1166,14 @@ void launch_exhaustive_k(const DevTargets& T, const DevPool& P, const RoundBuf& 
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_exhaustive<K>, kBlock, 0);
     if (per_sm < 1) per_sm = 1;
   }
-  unsigned long long need = (total + (kBlock / 32) - 1) / (kBlock / 32);
+  // resident blocks, or more when the chunks exceed kChunksPerWarp per warp
+  const unsigned long long wpb = kBlock / 32;
+  unsigned long long need = (total + wpb - 1) / wpb;
   unsigned long long grid = (unsigned long long)dev_num_sms() * per_sm;
   if (grid > need) grid = need;
+  const unsigned long long cover = (total + wpb * kChunksPerWarp - 1) / (wpb * kChunksPerWarp);
+  if (grid < cover) grid = cover;
+  if (grid > 0x7FFFFFFFull) grid = 0x7FFFFFFFull;
   k_exhaustive<K><<<unsigned(grid), kBlock, 0, s>>>(T, P, R, npairs, total);
 }
 

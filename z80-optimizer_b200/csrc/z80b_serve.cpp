@@ -11,8 +11,11 @@
 // flight and their work overlaps on the GPU.  A class is the candidate
 // length cap (1 or 2 instructions) and whether the target alone already
 // reads enough registers for an ExhaustiveCheck sweep of 2^26 states or
-// more: such heavy queries are batched apart, so the light ones do not wait
-// behind a long sweep.  Admission also charges each query's frontier memory (its
+// more.  With two or more workers, worker 0 serves the heavy classes first
+// on a low-priority stream and the others serve only the light classes on
+// high-priority streams; since the sweep kernel's blocks retire every few
+// chunks, the block scheduler hands SMs to the light batches' kernels while a
+// heavy sweep runs.  Admission also charges each query's frontier memory (its
 // lanes, survivor slots and rule records on the device) against the budget
 // and waits while the in-flight total would exceed it.
 #include <algorithm>
@@ -66,7 +69,8 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
   return std::chrono::duration<double, std::milli>(b - a).count();
 }
 
-void worker_loop(z80b_server* S, z80b_ctx* ctx) {
+// role: 0 any class (single worker), 1 heavy first, 2 light classes only
+void worker_loop(z80b_server* S, z80b_ctx* ctx, int role) {
   std::vector<Pending> batch;
   std::vector<uint32_t> tg;
   std::vector<uint8_t> lens, dead, dregs;
@@ -76,14 +80,28 @@ void worker_loop(z80b_server* S, z80b_ctx* ctx) {
     uint32_t cand = 1;
     {
       std::unique_lock<std::mutex> lk(S->mu);
+      // the oldest query this worker may take: its class is the batch's
+      auto pick = [&]() -> const Pending* {
+        const Pending* first_any = nullptr;
+        for (const Pending& p : S->pending) {
+          const bool heavy = (p.klass & 4u) != 0;
+          if (role == 2 && heavy) continue;
+          if (role == 1 && heavy) return &p;
+          if (!first_any) first_any = &p;
+          if (role != 1) return first_any;
+        }
+        return first_any;
+      };
       S->cv_work.wait(lk, [&] {
-        return S->stopping ||
-               (!S->pending.empty() && S->inflight_bytes + kFrontierBytes <= S->cfg.memory_budget);
+        return S->stopping || (pick() && S->inflight_bytes + kFrontierBytes <= S->cfg.memory_budget);
       });
-      if (S->pending.empty()) return;  // stopping and drained
-      // the class of the oldest query; take its class-mates in arrival order
-      cand = S->pending.front().cand;
-      const uint32_t klass = S->pending.front().klass;
+      const Pending* head = pick();
+      if (!head) {
+        if (S->stopping) return;  // stopping and nothing left for this worker
+        continue;
+      }
+      cand = head->cand;
+      const uint32_t klass = head->klass;
       for (auto it = S->pending.begin(); it != S->pending.end() && batch.size() < S->cfg.max_batch;) {
         if (it->klass == klass && S->inflight_bytes + kFrontierBytes <= S->cfg.memory_budget) {
           batch.push_back(*it);
@@ -170,7 +188,7 @@ int z80b_server_start(const z80b_server_config* cfg, z80b_server** out) {
   if (cfg) c = *cfg;
   if (c.workers <= 0) c.workers = 4;
   if (c.workers > 16) return Z80B_EINVAL;
-  if (c.max_batch == 0) c.max_batch = 4096;
+  if (c.max_batch == 0) c.max_batch = 512;
   if (c.memory_budget == 0) c.memory_budget = 64ull << 30;
   if (c.max_cand_len == 0) c.max_cand_len = 2;
   if (c.max_cand_len > 2) return Z80B_EINVAL;
@@ -187,7 +205,11 @@ int z80b_server_start(const z80b_server_config* cfg, z80b_server** out) {
     }
     S->ctxs.push_back(ctx);
   }
-  for (auto* ctx : S->ctxs) S->workers.emplace_back(worker_loop, S, ctx);
+  for (size_t w = 0; w < S->ctxs.size(); w++) {
+    const int role = S->ctxs.size() < 2 ? 0 : (w == 0 ? 1 : 2);
+    z80b_set_option(S->ctxs[w], Z80B_OPT_STREAM_PRIORITY, role == 1 ? 1 : (role == 2 ? -1 : 0));
+    S->workers.emplace_back(worker_loop, S, S->ctxs[w], role);
+  }
   *out = S;
   return Z80B_OK;
 }

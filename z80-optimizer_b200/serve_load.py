@@ -73,7 +73,7 @@ def offline_answers(ctx, arr, lens, dead, dregs, idx):
     return res
 
 
-def run(rate, seconds, seed, workers=4, max_batch=4096, verify=True, progress=None):
+def run(rate, seconds, seed, workers=4, max_batch=512, verify=True, progress=None):
     n = int(rate * seconds)
     arr, lens, dead, dregs = make_queries(n, seed)
     rng = np.random.default_rng(seed + 1000)
@@ -126,6 +126,10 @@ def run(rate, seconds, seed, workers=4, max_batch=4096, verify=True, progress=No
            "p50_ms_device_queries": float(np.percentile(served, 50)) if len(served) else None,
            "p99_ms_device_queries": float(np.percentile(served, 99)) if len(served) else None,
            "mean_batch": statistics.mean(bsz) if bsz else 0, "server": stats,
+           "slowest": [{"len": int(lens[k]), "dead_flags": int(dead[k]), "dead_regs": int(dregs[k]),
+                        "latency_ms": answers[k].latency_ms, "queued_ms": answers[k].queued_ms,
+                        "service_ms": answers[k].service_ms, "batch": answers[k].batch_size}
+                       for k in sorted(answers, key=lambda k: -answers[k].latency_ms)[:12]],
            "errors": int(sum(1 for a in answers.values() if a.status != 0)),
            "rules": int(sum(a.n_rules for a in answers.values()))}
     if verify:

@@ -101,7 +101,7 @@ EXPORTS = [
     "z80b_mul_pool", "z80b_mul_search", "z80b_should_prune_batch",
     "z80b_server_start", "z80b_server_submit", "z80b_server_poll", "z80b_server_get_stats", "z80b_server_stop",
 ]
-OPT_EXH_LANE_STATES, OPT_EXH_CHUNK_BLOCKS = 1, 2
+OPT_EXH_LANE_STATES, OPT_EXH_CHUNK_BLOCKS, OPT_STREAM_PRIORITY = 1, 2, 3
 
 
 MULPOOL_MULOPT, MULPOOL_WIDE21, MULPOOL_FAST14, MULPOOL_CUDA21 = 0, 1, 2, 3
@@ -496,7 +496,7 @@ def mul_results_json(results, pool):
 class Server:
     """Serving loop (z80b_server_*): submit queries from any thread, poll answers."""
 
-    def __init__(self, device=0, workers=4, max_batch=4096, memory_budget=0, max_cand_len=2):
+    def __init__(self, device=0, workers=4, max_batch=512, memory_budget=0, max_cand_len=2):
         cfg = ServerConfig(device, workers, max_batch, memory_budget, max_cand_len)
         h = ctypes.c_void_p()
         st = lib().z80b_server_start(ctypes.byref(cfg), ctypes.byref(h))
