@@ -258,8 +258,8 @@ int z80b_mul_search(z80b_ctx* ctx, int pool, uint8_t init_b, uint8_t init_c, uin
  * instructions.  Several workers, each with its own context and stream, run
  * batches of waiting queries concurrently (continuous batching: queries that
  * arrive while batches are in flight are admitted by the next free worker;
- * queries whose target alone implies a long ExhaustiveCheck sweep are
- * batched apart from the others);
+ * queries whose target alone implies an ExhaustiveCheck sweep of 2^32
+ * states or more run alone on a low-priority stream);
  * admission charges each query's device frontier memory against
  * memory_budget.  No counterpart in the reference (its serving is one query
  * per z80opt target call). */

@@ -10,12 +10,14 @@
 // admitted by the next free worker while earlier batches are still in
 // flight and their work overlaps on the GPU.  A class is the candidate
 // length cap (1 or 2 instructions) and whether the target alone already
-// reads enough registers for an ExhaustiveCheck sweep of 2^26 states or
-// more.  With two or more workers, worker 0 serves the heavy classes first
-// on a low-priority stream and the others serve only the light classes on
+// reads enough registers for an ExhaustiveCheck sweep of 2^32 states or
+// more (a "giant": e.g. SET 1, D : SBC HL, BC : XOR (HL) : OR 0C0h sweeps
+// 2^39 states, several seconds of the whole GPU).  With two or more
+// workers, worker 0 serves giants first, one query per batch, on a
+// low-priority stream, and the others serve every other query on
 // high-priority streams; since the sweep kernel's blocks retire every few
-// chunks, the block scheduler hands SMs to the light batches' kernels while a
-// heavy sweep runs.  Admission also charges each query's frontier memory (its
+// chunks, the block scheduler hands SMs to their kernels while a giant sweep
+// runs.  Admission also charges each query's frontier memory (its
 // lanes, survivor slots and rule records on the device) against the budget
 // and waits while the in-flight total would exceed it.
 #include <algorithm>
@@ -43,10 +45,10 @@ struct Pending {
   z80b_query q;
   Clock::time_point t_submit;
   uint32_t cand;   // candidate length cap of this query
-  uint32_t klass;  // batch class: cand | heavy << 2
+  uint32_t klass;  // batch class: cand | giant << 2
 };
 
-constexpr uint64_t kHeavyStates = 1ull << 26;
+constexpr uint64_t kGiantStates = 1ull << 32;
 
 }  // namespace
 
@@ -69,7 +71,7 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
   return std::chrono::duration<double, std::milli>(b - a).count();
 }
 
-// role: 0 any class (single worker), 1 heavy first, 2 light classes only
+// role: 0 any class (single worker), 1 giants first, 2 everything but giants
 void worker_loop(z80b_server* S, z80b_ctx* ctx, int role) {
   std::vector<Pending> batch;
   std::vector<uint32_t> tg;
@@ -84,9 +86,9 @@ void worker_loop(z80b_server* S, z80b_ctx* ctx, int role) {
       auto pick = [&]() -> const Pending* {
         const Pending* first_any = nullptr;
         for (const Pending& p : S->pending) {
-          const bool heavy = (p.klass & 4u) != 0;
-          if (role == 2 && heavy) continue;
-          if (role == 1 && heavy) return &p;
+          const bool giant = (p.klass & 4u) != 0;
+          if (role == 2 && giant) continue;
+          if (role == 1 && giant) return &p;
           if (!first_any) first_any = &p;
           if (role != 1) return first_any;
         }
@@ -102,7 +104,8 @@ void worker_loop(z80b_server* S, z80b_ctx* ctx, int role) {
       }
       cand = head->cand;
       const uint32_t klass = head->klass;
-      for (auto it = S->pending.begin(); it != S->pending.end() && batch.size() < S->cfg.max_batch;) {
+      const uint32_t cap = (klass & 4u) ? 1u : S->cfg.max_batch;  // giants run alone
+      for (auto it = S->pending.begin(); it != S->pending.end() && batch.size() < cap;) {
         if (it->klass == klass && S->inflight_bytes + kFrontierBytes <= S->cfg.memory_budget) {
           batch.push_back(*it);
           S->inflight_bytes += kFrontierBytes;
@@ -238,9 +241,9 @@ int z80b_server_submit(z80b_server* S, const z80b_query* q, uint32_t n) {
         S->stats.answered++;
         continue;
       }
-      const bool heavy =
-          z80b::sweep_for(z80b::seq_reads(q[i].target, int(q[i].len))).states >= kHeavyStates;
-      S->pending.push_back(Pending{q[i], now, cap, cap | (heavy ? 4u : 0u)});
+      const bool giant =
+          z80b::sweep_for(z80b::seq_reads(q[i].target, int(q[i].len))).states >= kGiantStates;
+      S->pending.push_back(Pending{q[i], now, cap, cap | (giant ? 4u : 0u)});
     }
   }
   S->cv_work.notify_all();
