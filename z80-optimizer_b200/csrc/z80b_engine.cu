@@ -1090,7 +1090,7 @@ int z80b_verify_pairs(z80b_ctx* ctx, const uint32_t* tgt, const uint8_t* tlens, 
         units = (pr[i].nblocks + 127) / 128;
       }
       unsigned long long c = (units + ctx->chunk_blocks - 1) / uint64_t(ctx->chunk_blocks);
-      nch[i] = c > 65536 ? 65536 : c;
+      nch[i] = c > (1ull << 20) ? (1ull << 20) : c;
       cb[i] = tot;
       tot += nch[i];
     }

@@ -137,8 +137,8 @@ __device__ __forceinline__ bool pair_xindep(const DevTargets& T, uint32_t t, con
 __device__ __forceinline__ unsigned long long pair_units(unsigned long long nblocks, uint32_t keepR) {
   return (keepR & kXIndep) ? (nblocks + kUnitBlocks - 1) / kUnitBlocks : nblocks;
 }
-constexpr unsigned long long kMaxChunks = 65536;
-constexpr int kChunksPerWarp = 64;
+constexpr unsigned long long kMaxChunks = 1ull << 20;
+constexpr int kChunksPerWarp = 16;
 // Work chunks of a sweep: cb A-blocks each (cb is the tuning option), at
 // most kMaxChunks per pair.
 __device__ __forceinline__ unsigned long long chunks_for(unsigned long long nb, uint32_t cb) {
@@ -574,7 +574,7 @@ __device__ __noinline__ bool xindep_unit(unsigned long long first, unsigned long
 }
 
 template <int K>
-__global__ void __launch_bounds__(kBlock, K <= 4 ? 2 : 1) k_exhaustive(DevTargets T, DevPool P, RoundBuf R, uint32_t npairs,
+__global__ void __launch_bounds__(kBlock, K <= 2 ? 3 : (K <= 4 ? 2 : 1)) k_exhaustive(DevTargets T, DevPool P, RoundBuf R, uint32_t npairs,
                                                        unsigned long long total) {
   static_assert(K == 1 || K == 2 || K == 4 || K == 8, "K divides 8");
   const unsigned lane = lane_id();

@@ -117,7 +117,7 @@ extern "C" int z80b_exhaustive_noalloc(int device, const uint32_t* tgt, const ui
       units = (p.nblocks + 127) / 128;
     }
     unsigned long long ch = (units + 31) / 32;
-    if (ch > 65536) ch = 65536;
+    if (ch > (1ull << 20)) ch = 1ull << 20;
     h_cbase[i] = total;
     total += ch;
   }
