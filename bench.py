@@ -242,6 +242,12 @@ def c3_leg(ctx, z80b, workloads, args):
         j.path = path
         return j, (a, ln, d, r)
 
+    # tune the sweep kernel for this workload on its first 4,000 targets
+    # (longer sequences than C2's, so another setting may win); the C2
+    # setting is restored after the leg
+    k0, c0 = ctx.get_option(z80b.OPT_EXH_LANE_STATES), ctx.get_option(z80b.OPT_EXH_CHUNK_BLOCKS)
+    tj, tkeep = job_for(0, min(4000, n), z80b.PATH_BATCHED)
+    tr = ctx.autotune(tj)
     job, keep = job_for(0, n, z80b.PATH_BATCHED)
     ctx.run_job(job)  # builds the pair pool and its bucket indexes once
     ms, st, nrules = [], None, 0
@@ -256,7 +262,9 @@ def c3_leg(ctx, z80b, workloads, args):
            "value": st.checks / (t / 1e3), "unit": UNIT, "device_ms_per_step": t, "rules": nrules,
            "qc_survivors": st.qc_survivors, "exhaustive_pairs": st.exhaustive_pairs,
            "exhaustive_states": st.exhaustive_states, "rounds": st.rounds, "launches": st.launches,
-           "exhaustive_ms": st.exh_ms, "checks": st.checks}
+           "exhaustive_ms": st.exh_ms, "checks": st.checks,
+           "autotune": {"lane_states": tr.lane_states, "chunk_blocks": tr.chunk_blocks,
+                        "sample": "first 4,000 targets of the leg"}}
     if args.plain_sample:
         m = min(1000, n)
         pj, keep2 = job_for(0, m, z80b.PATH_PLAIN)
@@ -270,6 +278,8 @@ def c3_leg(ctx, z80b, workloads, args):
         out["plain_vs_batched"] = {"targets": m, "plain_checks_per_s": stp.checks / tp,
                                    "batched_checks_per_s": stb.checks / tb, "batched_over_plain": tp / tb,
                                    "timing": "host wall clock around z80b_search (both synchronous)"}
+    ctx.set_option(z80b.OPT_EXH_LANE_STATES, k0)
+    ctx.set_option(z80b.OPT_EXH_CHUNK_BLOCKS, c0)
     return out
 
 

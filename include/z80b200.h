@@ -159,6 +159,17 @@ int z80b_verify_pairs(z80b_ctx* ctx, const uint32_t* tgt, const uint8_t* tlens,
 int z80b_search(z80b_ctx* ctx, const z80b_job* job, z80b_rule* out, uint64_t cap,
                 uint64_t* n_rules, z80b_stats* stats);
 
+/* z80b_search with each target's answer handed to cb as soon as it is final
+ * (both its full and its masked lane have a winner or have no candidate left
+ * to try), before the whole job ends: cb(user, target_index, rules, n) with
+ * the target's 0..2 rules in z80b_search's order; called once per target, on
+ * the calling thread.  Batched first-found jobs only.  For callers that
+ * answer queries individually (the serving loop), so one slow target does
+ * not hold the answers of the others. */
+typedef void (*z80b_rule_cb)(void* user, uint32_t target_index, const z80b_rule* rules, uint32_t n_rules);
+int z80b_search_cb(z80b_ctx* ctx, const z80b_job* job, z80b_rule* out, uint64_t cap, uint64_t* n_rules,
+                   z80b_stats* stats, z80b_rule_cb cb, void* user);
+
 /* Device-resident variant for timing the pipeline without host copies:
  * z80b_stage_job uploads the job's targets once; z80b_run_staged runs the
  * pipeline on them and keeps the rules on the device (count in *n_rules);

@@ -53,3 +53,19 @@ def test_length2_needs_first_mode(ctx):
     with pytest.raises(z80b.Z80BError) as e:
         ctx.search([[z80b.pack(0), z80b.pack(1)]], mode=z80b.MODE_ALL, max_cand_len=2)
     assert e.value.status == z80b.EINVAL
+
+
+def test_streaming_answers_equal_final_rules(ctx):
+    """z80b_search_cb hands every target's rules to the callback exactly
+    once, and they are the rules z80b_search returns for it."""
+    fx = fixture()
+    idx = list(range(0, fx["n"], 2))
+    targets = [fx["targets"][i] for i in idx]
+    rules, st, events = ctx.search_streaming(targets, per_target_dead=[fx["dead_flags"][i] for i in idx],
+                                             dead_regs=[fx["dead_regs"][i] for i in idx], max_cand_len=2)
+    assert sorted(t for t, _ in events) == list(range(len(targets)))
+    by_t = {}
+    for r in rules:
+        by_t.setdefault(r.target_index, []).append(r.key())
+    for t, keys in events:
+        assert keys == by_t.get(t, []), t

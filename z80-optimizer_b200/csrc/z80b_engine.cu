@@ -70,11 +70,14 @@ struct PoolBufs {
   bool loaded = false;
 };
 
+struct Reporter;
+
 // What a pipeline run needs to know about its job beyond the device arrays.
 struct PipeOpts {
   uint32_t mode = Z80B_MODE_FIRST;
   uint32_t max_cand = 1;        // longest candidate (1 or 2 instructions)
   uint64_t dreg_masks = 1;      // bit m: dead-register mask m occurs in a masked pass (bit 0 always)
+  Reporter* rep = nullptr;      // per-target answers as they become final (first-found mode)
 };
 
 // The 4,531^2 pair pool, its QuickCheck outputs and its bucket indexes (one
@@ -426,6 +429,28 @@ struct Timer {
   }
 };
 
+void to_rules(z80b_ctx* ctx, const std::vector<DevRule>& dr, const uint32_t* targets, const uint8_t* tlens,
+              uint32_t tlen, uint32_t stride, uint32_t mode, uint32_t tindex_offset, z80b_rule* out);
+
+// Hands each target's rules to a callback as soon as both of its
+// (target, kind) lanes are final: a lane is final once it has a winner, or
+// it is resolved without one and no longer candidates remain to try.  The
+// pipeline calls update() after every ExhaustiveCheck round; each call
+// copies the lane arrays (a few words per target) to the host.
+struct Reporter {
+  z80b_rule_cb cb = nullptr;
+  void* user = nullptr;
+  const uint32_t* targets = nullptr;
+  const uint8_t* tlens = nullptr;
+  uint32_t tlen = 0, stride = 0;
+  std::vector<uint8_t> done;
+  std::vector<uint32_t> n1, w1, n2, w2;
+  std::vector<uint16_t> d1, d2;
+
+  int update(z80b_ctx* ctx, uint32_t n, const Lanes& L, const Lanes& L2, uint32_t max_cand, bool phase2,
+             bool last);
+};
+
 // Runs the pipeline on device-resident targets.  Rules stay in ctx->rules
 // (DevRule), count in *nr.
 int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_stats* st, uint64_t* nr) {
@@ -545,6 +570,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
         CKR(check_launch(ctx, "exhaustive"));
         launch_round_resolve(R, np, q, L, s);
         CKR(check_launch(ctx, "round_resolve"));
+        if (opts.rep) CKR(opts.rep->update(ctx, n, L, Lanes{nullptr, nullptr, nullptr}, opts.max_cand, false, false));
       }
     }
     Lanes L2{nullptr, nullptr, nullptr};
@@ -617,8 +643,10 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
         CKR(check_launch(ctx, "exhaustive"));
         launch_round_resolve(R, np, q2, L2, s);
         CKR(check_launch(ctx, "round_resolve"));
+        if (opts.rep) CKR(opts.rep->update(ctx, n, L, L2, opts.max_cand, true, false));
       }
     }
+    if (opts.rep) CKR(opts.rep->update(ctx, n, L, L2, opts.max_cand, opts.max_cand >= 2, true));
     CK(ctx->rcnt.ensure(4ull * n));
     CK(ctx->rbase.ensure(4ull * n));
     launch_rule_count_first(L, L2, n, ctx->rcnt.as<uint32_t>(), T, ctx->checked.as<unsigned long long>(),
@@ -745,6 +773,67 @@ void to_rules(z80b_ctx* ctx, const std::vector<DevRule>& dr, const uint32_t* tar
     o.dead_regs = (r.kind == 0) ? 0 : int(r.diff >> 8);
     o.target_index = int(r.target + tindex_offset);
   }
+}
+
+int Reporter::update(z80b_ctx* ctx, uint32_t n, const Lanes& L, const Lanes& L2, uint32_t max_cand, bool phase2,
+                     bool last) {
+  if (!cb || n == 0) return Z80B_OK;
+  cudaStream_t s = ctx->stream;
+  if (done.size() != n) done.assign(n, 0);
+  n1.resize(2 * size_t(n));
+  w1.resize(2 * size_t(n));
+  d1.resize(2 * size_t(n));
+  CK(cudaMemcpyAsync(n1.data(), L.next, 8ull * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(w1.data(), L.win, 8ull * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(d1.data(), L.windiff, 4ull * n, cudaMemcpyDeviceToHost, s));
+  if (phase2 && L2.win) {
+    n2.resize(2 * size_t(n));
+    w2.resize(2 * size_t(n));
+    d2.resize(2 * size_t(n));
+    CK(cudaMemcpyAsync(n2.data(), L2.next, 8ull * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(w2.data(), L2.win, 8ull * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(d2.data(), L2.windiff, 4ull * n, cudaMemcpyDeviceToHost, s));
+  }
+  CK(cudaStreamSynchronize(s));
+  const uint32_t kResolvedBit = 0x80000000u;
+  std::vector<DevRule> dr;
+  std::vector<z80b_rule> out;
+  for (uint32_t t = 0; t < n; t++) {
+    if (done[t]) continue;
+    bool final_all = true;
+    dr.clear();
+    for (int kind = 0; kind < 2 && final_all; kind++) {
+      const size_t i = 2 * size_t(t) + size_t(kind);
+      DevRule r{};
+      r.target = t;
+      r.kind = uint8_t(kind);
+      if (w1[i] != kNone) {
+        r.cand = w1[i];
+        r.diff = kind ? d1[i] : uint16_t(0);
+        r.clen = 1;
+        dr.push_back(r);
+      } else if (!(n1[i] & kResolvedBit)) {
+        final_all = last;
+      } else if (max_cand >= 2) {
+        if (!phase2 || !L2.win) {
+          final_all = false;
+        } else if (w2[i] != kNone) {
+          r.cand = w2[i];
+          r.diff = kind ? d2[i] : uint16_t(0);
+          r.clen = 2;
+          dr.push_back(r);
+        } else if (!(n2[i] & kResolvedBit)) {
+          final_all = last;
+        }
+      }
+    }
+    if (!final_all) continue;
+    done[t] = 1;
+    out.resize(dr.size());
+    if (!dr.empty()) to_rules(ctx, dr, targets, tlens, tlen, stride, Z80B_MODE_FIRST, 0, out.data());
+    cb(user, t, out.data(), uint32_t(out.size()));
+  }
+  return Z80B_OK;
 }
 
 // Uploads the job's arrays straight from the caller's buffers (pinned
@@ -1243,8 +1332,8 @@ int z80b_fetch_rules(z80b_ctx* ctx, z80b_rule* out, uint64_t cap, uint64_t* n_ru
   return Z80B_OK;
 }
 
-int z80b_search(z80b_ctx* ctx, const z80b_job* job, z80b_rule* out, uint64_t cap, uint64_t* n_rules,
-                z80b_stats* stats) {
+static int search_impl(z80b_ctx* ctx, const z80b_job* job, z80b_rule* out, uint64_t cap, uint64_t* n_rules,
+                       z80b_stats* stats, Reporter* rep) {
   if (!ctx) return Z80B_EINVAL;
   if (!n_rules) return fail(ctx, Z80B_EINVAL, "n_rules is null");
   CKR(validate_job(ctx, job));
@@ -1265,7 +1354,16 @@ int z80b_search(z80b_ctx* ctx, const z80b_job* job, z80b_rule* out, uint64_t cap
                            (unsigned long long)cap)
                     : Z80B_OK;
   }
-  CKR(run_pipeline(ctx, T, ctx->staged.opts, stats, &nr));
+  PipeOpts opts = ctx->staged.opts;
+  if (rep && job->mode == Z80B_MODE_FIRST) {
+    rep->targets = job->targets;
+    rep->tlens = job->target_lens;
+    rep->tlen = job->target_len;
+    rep->stride = job->target_stride;
+    rep->done.assign(job->n_targets, 0);
+    opts.rep = rep;
+  }
+  CKR(run_pipeline(ctx, T, opts, stats, &nr));
   if (stats) stats->launches = ctx->launches;
   *n_rules = nr;
   if (nr > cap)
@@ -1278,6 +1376,22 @@ int z80b_search(z80b_ctx* ctx, const z80b_job* job, z80b_rule* out, uint64_t cap
   }
   to_rules(ctx, dr, job->targets, job->target_lens, job->target_len, job->target_stride, job->mode, 0, out);
   return Z80B_OK;
+}
+
+int z80b_search(z80b_ctx* ctx, const z80b_job* job, z80b_rule* out, uint64_t cap, uint64_t* n_rules,
+                z80b_stats* stats) {
+  return search_impl(ctx, job, out, cap, n_rules, stats, nullptr);
+}
+
+int z80b_search_cb(z80b_ctx* ctx, const z80b_job* job, z80b_rule* out, uint64_t cap, uint64_t* n_rules,
+                   z80b_stats* stats, z80b_rule_cb cb, void* user) {
+  if (!cb) return search_impl(ctx, job, out, cap, n_rules, stats, nullptr);
+  if (job && (job->mode != Z80B_MODE_FIRST || job->path != Z80B_PATH_BATCHED))
+    return fail(ctx, Z80B_EINVAL, "per-target answers need the batched first-found path");
+  Reporter rep;
+  rep.cb = cb;
+  rep.user = user;
+  return search_impl(ctx, job, out, cap, n_rules, stats, &rep);
 }
 
 

@@ -301,6 +301,7 @@ __global__ void __launch_bounds__(kBlock) k_qc_scan(DevTargets T, DevPool P, QCC
     const uint32_t keep2 = cfg.w2mask;
 
     uint32_t nf = 0, nm = 0;
+    uint32_t lf = 0, lm = 0, lc = 0;  // count pass: per-lane tallies, reduced once per target
     for (uint32_t base = 0; base < P.n; base += 32) {
       const uint32_t c = base + lane;
       bool el = false;
@@ -337,13 +338,14 @@ __global__ void __launch_bounds__(kBlock) k_qc_scan(DevTargets T, DevPool P, QCC
           }
         }
       }
-      if (!COLLECT) {
-        const unsigned be = __ballot_sync(kFull, el);
-        if (lane == 0) my_checks += __popc(be);
-      }
-      const unsigned bf = __ballot_sync(kFull, fp);
-      const unsigned bm = __ballot_sync(kFull, mp);
-      if (COLLECT) {
+      if constexpr (!COLLECT) {
+        lc += el ? 1u : 0u;
+        lf += fp ? 1u : 0u;
+        lm += mp ? 1u : 0u;
+      } else {
+        // ballots give the survivors their enumeration-ordered slots
+        const unsigned bf = __ballot_sync(kFull, fp);
+        const unsigned bm = __ballot_sync(kFull, mp);
         if (fp) {
           uint32_t idx = obase + nf + __popc(bf & lanemask_lt());
           o.surv[idx] = c;
@@ -354,9 +356,15 @@ __global__ void __launch_bounds__(kBlock) k_qc_scan(DevTargets T, DevPool P, QCC
           o.surv[idx] = c;
           o.sdiff[idx] = uint16_t(diff);
         }
+        nf += __popc(bf);
+        nm += __popc(bm);
       }
-      nf += __popc(bf);
-      nm += __popc(bm);
+    }
+    if constexpr (!COLLECT) {
+      nf = __reduce_add_sync(kFull, lf);
+      nm = __reduce_add_sync(kFull, lm);
+      const uint32_t nc = __reduce_add_sync(kFull, lc);
+      if (lane == 0) my_checks += nc;
     }
     if (!COLLECT && lane == 0) {
       o.cnt_f[t] = nf;

@@ -71,6 +71,37 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
   return std::chrono::duration<double, std::milli>(b - a).count();
 }
 
+// One running batch: answers leave as soon as z80b_search_cb reports a
+// target final, so a slow target does not hold the others of its batch.
+struct BatchRun {
+  z80b_server* S;
+  const std::vector<Pending>* batch;
+  Clock::time_point t_start;
+  std::vector<uint8_t> answered;
+};
+
+void on_target(void* user, uint32_t t, const z80b_rule* rules, uint32_t n) {
+  BatchRun* b = static_cast<BatchRun*>(user);
+  const Pending& p = (*b->batch)[t];
+  const auto now = Clock::now();
+  z80b_answer a;
+  std::memset(&a, 0, sizeof a);
+  a.id = p.q.id;
+  a.status = Z80B_OK;
+  a.batch_size = uint32_t(b->batch->size());
+  a.queued_ms = ms_between(p.t_submit, b->t_start);
+  a.service_ms = ms_between(b->t_start, now);
+  a.latency_ms = ms_between(p.t_submit, now);
+  for (uint32_t k = 0; k < n && k < 2; k++) a.rules[a.n_rules++] = rules[k];
+  b->answered[t] = 1;
+  {
+    std::lock_guard<std::mutex> lk(b->S->mu);
+    b->S->done.push_back(a);
+    b->S->stats.answered++;
+  }
+  b->S->cv_done.notify_all();
+}
+
 // role: 0 any class (single worker), 1 giants first, 2 everything but giants
 void worker_loop(z80b_server* S, z80b_ctx* ctx, int role) {
   std::vector<Pending> batch;
@@ -148,32 +179,30 @@ void worker_loop(z80b_server* S, z80b_ctx* ctx, int role) {
     rules.resize(size_t(n) * 2 + 16);
     uint64_t nr = 0;
     z80b_stats st{};
-    int status = z80b_search(ctx, &job, rules.data(), rules.size(), &nr, &st);
+    BatchRun run{S, &batch, t_start, std::vector<uint8_t>(n, 0)};
+    const int status = z80b_search_cb(ctx, &job, rules.data(), rules.size(), &nr, &st, on_target, &run);
     const auto t_end = Clock::now();
-    std::vector<z80b_answer> ans(n);
+    // targets the callback did not answer (the batch failed)
+    std::vector<z80b_answer> ans;
     for (uint32_t i = 0; i < n; i++) {
-      z80b_answer& a = ans[i];
+      if (run.answered[i]) continue;
+      z80b_answer a;
       std::memset(&a, 0, sizeof a);
       a.id = batch[i].q.id;
-      a.status = status;
+      a.status = status == Z80B_OK ? Z80B_ESTATE : status;
       a.batch_size = n;
       a.queued_ms = ms_between(batch[i].t_submit, t_start);
       a.service_ms = ms_between(t_start, t_end);
       a.latency_ms = ms_between(batch[i].t_submit, t_end);
+      ans.push_back(a);
     }
-    if (status == Z80B_OK)
-      for (uint64_t k = 0; k < nr; k++) {
-        const z80b_rule& r = rules[k];
-        z80b_answer& a = ans[uint32_t(r.target_index)];
-        if (a.n_rules < 2) a.rules[a.n_rules++] = r;
-      }
     {
       std::lock_guard<std::mutex> lk(S->mu);
       S->inflight_bytes -= uint64_t(n) * kFrontierBytes;
       for (auto& a : ans) S->done.push_back(a);
-      S->stats.answered += n;
+      S->stats.answered += ans.size();
       S->stats.device_ms += st.device_ms;
-      if (status != Z80B_OK) S->stats.errors += n;
+      S->stats.errors += ans.size();
     }
     S->cv_done.notify_all();
     S->cv_work.notify_all();

@@ -100,7 +100,9 @@ EXPORTS = [
     "z80b_set_option", "z80b_get_option", "z80b_autotune", "z80b_enumerate",
     "z80b_mul_pool", "z80b_mul_search", "z80b_should_prune_batch",
     "z80b_server_start", "z80b_server_submit", "z80b_server_poll", "z80b_server_get_stats", "z80b_server_stop",
+    "z80b_search_cb",
 ]
+RULE_CB = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32)
 OPT_EXH_LANE_STATES, OPT_EXH_CHUNK_BLOCKS, OPT_STREAM_PRIORITY = 1, 2, 3
 
 
@@ -199,6 +201,8 @@ def lib():
         L.z80b_enumerate.restype = ctypes.c_uint64
         L.z80b_enumerate.argtypes = [u32p, ctypes.c_uint32, ctypes.c_uint32, u32p, ctypes.c_uint64]
         L.z80b_should_prune_batch.argtypes = [u32p, u8p, ctypes.c_uint32, ctypes.c_uint64, u8p]
+        L.z80b_search_cb.argtypes = [vp, ctypes.POINTER(Job), ctypes.POINTER(Rule), ctypes.c_uint64,
+                                     ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(Stats), RULE_CB, vp]
         L.z80b_server_start.argtypes = [ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)]
         L.z80b_server_submit.argtypes = [vp, ctypes.POINTER(Query), ctypes.c_uint32]
         L.z80b_server_poll.argtypes = [vp, ctypes.POINTER(Answer), ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32),
@@ -426,6 +430,26 @@ class Context:
                 continue
             self._check(s)
             return [out[i] for i in range(nr.value)], st
+
+    def search_streaming(self, targets, per_target_dead=None, dead_regs=None, max_cand_len=1):
+        """z80b_search_cb: returns (rules, stats, events) where events lists
+        (target_index, [rule keys]) in the order the callback delivered them."""
+        job, keep = self.make_job(targets, 0, MODE_FIRST, PATH_BATCHED, per_target_dead, dead_regs,
+                                  max_cand_len=max_cand_len)
+        events = []
+
+        def cb(user, t, rules, n):
+            rs = ctypes.cast(rules, ctypes.POINTER(Rule))
+            events.append((t, [rs[i].key() for i in range(n)]))
+
+        fn = RULE_CB(cb)
+        cap = 2 * len(targets) + 16
+        out = (Rule * cap)()
+        nr = ctypes.c_uint64()
+        st = Stats()
+        self._check(lib().z80b_search_cb(self._h, ctypes.byref(job), out, cap, ctypes.byref(nr), ctypes.byref(st),
+                                         fn, None))
+        return [out[i] for i in range(nr.value)], st, events
 
     def set_option(self, option, value):
         self._check(lib().z80b_set_option(self._h, option, value))
