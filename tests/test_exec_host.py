@@ -15,3 +15,14 @@ def test_exec_header_matches_oracle(tmp_path):
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.startswith("OK")
+
+
+def test_bitsliced_step_matches_scalar(tmp_path):
+    """The bit-sliced step (z80_bits.cuh, 32 states per step) agrees with the
+    scalar step on every opcode, random full states and all values of A."""
+    exe = tmp_path / "bits_check"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-o", str(exe),
+                    os.path.join(ROOT, "tests", "native", "bits_check.cpp")], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.startswith("OK")

@@ -812,9 +812,9 @@ int Reporter::update(z80b_ctx* ctx, uint32_t n, const Lanes& L, const Lanes& L2,
         r.diff = kind ? d1[i] : uint16_t(0);
         r.clen = 1;
         dr.push_back(r);
-      } else if (!(n1[i] & kResolvedBit)) {
-        final_all = last;
       } else if (max_cand >= 2) {
+        // no length-1 winner: the answer is the length-2 pass's, which starts
+        // once every length-1 lane is done
         if (!phase2 || !L2.win) {
           final_all = false;
         } else if (w2[i] != kNone) {
@@ -825,6 +825,8 @@ int Reporter::update(z80b_ctx* ctx, uint32_t n, const Lanes& L, const Lanes& L2,
         } else if (!(n2[i] & kResolvedBit)) {
           final_all = last;
         }
+      } else if (!(n1[i] & kResolvedBit)) {
+        final_all = last;  // a lane without survivors is never offered to a round
       }
     }
     if (!final_all) continue;
@@ -1172,8 +1174,9 @@ int z80b_verify_pairs(z80b_ctx* ctx, const uint32_t* tgt, const uint8_t* tlens, 
       pr[i].nblocks = w.states / 256;
       pr[i].keepF = uint8_t(~(dead ? dead[i] : 0u));
       pr[i].keepR = 0x3F;
-      // A-independent pairs are swept in units of 128 blocks (see the sweep kernel)
-      unsigned long long units = pr[i].nblocks;
+      // sweep units (see the sweep kernel): 128 A-blocks for A-independent
+      // pairs, 4 A-blocks (bit-sliced) for the others
+      unsigned long long units = (pr[i].nblocks + 3) / 4;
       if (seq_aflow(tgt + (size_t)i * stride, tlens[i]) && seq_aflow(cand + (size_t)i * stride, clens[i])) {
         pr[i].keepR |= 0x40;
         units = (pr[i].nblocks + 127) / 128;

@@ -24,6 +24,7 @@
 
 #include <algorithm>
 
+#include "z80_bits.cuh"
 #include "z80b_kernels.cuh"
 
 namespace z80b {
@@ -134,8 +135,13 @@ __device__ __forceinline__ bool pair_xindep(const DevTargets& T, uint32_t t, con
   return dev_seq_aflow(T.insn + (size_t)t * T.stride, target_len(T, t)) != 0u &&
          dev_seq_aflow(P.insn + (size_t)c * P.stride, pool_len(P, c)) != 0u;
 }
+// A-dependent pairs run bit-sliced (z80_bits.cuh): a unit is 4 A-blocks, a
+// lane takes 32 consecutive values of A of one block.
+constexpr unsigned long long kBitsBlocks = 4;
+constexpr int kBitsWords = 88;  // planes of one ZB (A F B C D E H L M: 8 each, SP: 16)
 __device__ __forceinline__ unsigned long long pair_units(unsigned long long nblocks, uint32_t keepR) {
-  return (keepR & kXIndep) ? (nblocks + kUnitBlocks - 1) / kUnitBlocks : nblocks;
+  return (keepR & kXIndep) ? (nblocks + kUnitBlocks - 1) / kUnitBlocks
+                           : (nblocks + kBitsBlocks - 1) / kBitsBlocks;
 }
 constexpr unsigned long long kMaxChunks = 1ull << 20;
 constexpr int kChunksPerWarp = 16;
@@ -551,8 +557,92 @@ __device__ __forceinline__ bool run_compare(const Init& init, const bool (&valid
   return bad;
 }
 
+// Planes of the 32 states A = a0 .. a0+31 (a0 a multiple of 32) with the
+// other registers of x.
+__device__ __forceinline__ void zb_init(ZB& z, const Z80S& x, uint32_t a0) {
+  z.a[0] = 0xAAAAAAAAu;
+  z.a[1] = 0xCCCCCCCCu;
+  z.a[2] = 0xF0F0F0F0u;
+  z.a[3] = 0xFF00FF00u;
+  z.a[4] = 0xFFFF0000u;
+  z.a[5] = (a0 & 32u) ? kZBOnes : 0u;
+  z.a[6] = (a0 & 64u) ? kZBOnes : 0u;
+  z.a[7] = (a0 & 128u) ? kZBOnes : 0u;
+  zb_set8(z.f, x.f);
+  zb_set8(z.b, x.b);
+  zb_set8(z.c, x.c);
+  zb_set8(z.d, x.d);
+  zb_set8(z.e, x.e);
+  zb_set8(z.h, x.h);
+  zb_set8(z.l, x.l);
+  zb_set8(z.m, x.m);
+#pragma unroll
+  for (int i = 0; i < 16; i++) z.sp[i] = ((x.sp >> i) & 1u) ? kZBOnes : 0u;
+}
+// Saves / compares the planes (s: this lane's column, stride 32 words).
+__device__ __forceinline__ void zb_save(const ZB& z, uint32_t* s) {
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    s[(0 + i) * 32] = z.a[i];
+    s[(8 + i) * 32] = z.f[i];
+    s[(16 + i) * 32] = z.b[i];
+    s[(24 + i) * 32] = z.c[i];
+    s[(32 + i) * 32] = z.d[i];
+    s[(40 + i) * 32] = z.e[i];
+    s[(48 + i) * 32] = z.h[i];
+    s[(56 + i) * 32] = z.l[i];
+    s[(64 + i) * 32] = z.m[i];
+  }
+#pragma unroll
+  for (int i = 0; i < 16; i++) s[(72 + i) * 32] = z.sp[i];
+}
+__device__ __forceinline__ uint32_t zb_diff(const ZB& z, const uint32_t* s, uint32_t keepF, uint32_t keepR) {
+  uint32_t d = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    d |= z.a[i] ^ s[(0 + i) * 32];
+    if ((keepF >> i) & 1u) d |= z.f[i] ^ s[(8 + i) * 32];
+    if (keepR & 1u) d |= z.b[i] ^ s[(16 + i) * 32];
+    if (keepR & 2u) d |= z.c[i] ^ s[(24 + i) * 32];
+    if (keepR & 4u) d |= z.d[i] ^ s[(32 + i) * 32];
+    if (keepR & 8u) d |= z.e[i] ^ s[(40 + i) * 32];
+    if (keepR & 16u) d |= z.h[i] ^ s[(48 + i) * 32];
+    if (keepR & 32u) d |= z.l[i] ^ s[(56 + i) * 32];
+    d |= z.m[i] ^ s[(64 + i) * 32];
+  }
+#pragma unroll
+  for (int i = 0; i < 16; i++) d |= z.sp[i] ^ s[(72 + i) * 32];
+  return d;
+}
+// One unit (4 A-blocks) of an A-dependent sweep, bit-sliced: lane l takes
+// block unit*4 + l/8 and A = (l%8)*32 .. +31; the candidate's outputs wait in
+// shared memory while the target runs.  One dispatch site for both programs.
+__device__ __forceinline__ bool bits_unit(unsigned long long u, unsigned long long nblocks, bool spw, bool reduced,
+                                          int nx, int fw, const int (&slot)[7], uint32_t pw, int tl, int cl,
+                                          uint32_t keepF, uint32_t keepR, uint32_t* sm) {
+  const unsigned lane = lane_id();
+  const unsigned long long blk = u * kBitsBlocks + (lane >> 3);
+  const bool valid = blk < nblocks;
+  Z80S x;
+  decode_block<false>(valid ? blk : u * kBitsBlocks, spw, reduced, nx, fw, slot, x);
+  const uint32_t a0 = (lane & 7u) * 32u;
+  ZB z;
+#pragma unroll 1
+  for (int st = -1; st < tl + cl; st++) {
+    if (st == -1 || st == cl) {
+      if (st == cl) zb_save(z, sm);
+      zb_init(z, x, a0);
+      if (st == -1) continue;
+    }
+    const int src = st < cl ? tl + st : st - cl;
+    const uint32_t w = __shfl_sync(kFull, pw, src);
+    zb_step(z, w & 0xFFFFu, w >> 16);
+  }
+  return valid && zb_diff(z, sm, keepF, keepR) != 0u;
+}
+
 // One unit (128 A-blocks at A = 0, 1) of an A-independent sweep; kept out of
-// line so its registers do not weigh on the A-block loop.
+// line so its registers do not weigh on the bit-sliced path.
 template <int K>
 __device__ __noinline__ bool xindep_unit(unsigned long long first, unsigned long long nb, bool spw, bool reduced,
                                          int nx, int fw, const int* slotp, uint32_t pw, int tl, int cl,
@@ -582,7 +672,7 @@ __device__ __noinline__ bool xindep_unit(unsigned long long first, unsigned long
 }
 
 template <int K>
-__global__ void __launch_bounds__(kBlock, K <= 2 ? 3 : (K <= 4 ? 2 : 1)) k_exhaustive(DevTargets T, DevPool P, RoundBuf R, uint32_t npairs,
+__global__ void __launch_bounds__(kBlock, 1) k_exhaustive(DevTargets T, DevPool P, RoundBuf R, uint32_t npairs,
                                                        unsigned long long total) {
   static_assert(K == 1 || K == 2 || K == 4 || K == 8, "K divides 8");
   const unsigned lane = lane_id();
@@ -644,31 +734,22 @@ __global__ void __launch_bounds__(kBlock, K <= 2 ? 3 : (K <= 4 ? 2 : 1)) k_exhau
 
     bool bad = false;
     if (!xind) {
-      // Unit = one A-block: the 256 values of A for one assignment of carry,
-      // swept registers and SP; lanes take 32 consecutive A values per
-      // dispatch.  The reference nests its loops as A, carry, first
-      // register, ..., last register, SP (verifier.go:498-531,578-610), so
-      // block b covers the reference's states (A, b) for every A at once and
-      // a sweep the reference abandons early is abandoned at least as early
-      // here.
-      bool valid[K];
-#pragma unroll
-      for (int q = 0; q < K; q++) valid[q] = true;
-      for (unsigned long long ab = u0; ab < u1; ab++) {
-        Z80S base;
-        decode_block<true>(ab, spw, reduced, nx, fw, slot, base);
-#pragma unroll 1
-        for (uint32_t i = 0; i < 8u / K; i++) {
-          auto init = [&](int q, Z80S& x) {
-            x = base;
-            x.a = (i * K + uint32_t(q)) * 32u + lane;
-          };
-          bad = run_compare<K>(init, valid, pw, int(tl), int(cl), keep0, keep1) || bad;
-        }
-        my_states += 256;
-        my_eval += 256;
+      // Unit = 4 A-blocks, bit-sliced (256 states of each block in 8 lanes).
+      // The reference nests its loops as A, carry, first register, ...,
+      // last register, SP (verifier.go:498-531,578-610); the block index
+      // varies SP and the last register fastest, so a sweep the reference
+      // abandons early is abandoned early here too.
+      extern __shared__ uint32_t zsm[];
+      uint32_t* sm = zsm + (threadIdx.x >> 5) * (kBitsWords * 32) + lane;
+      for (unsigned long long u = u0; u < u1; u++) {
+        const unsigned long long first = u * kBitsBlocks;
+        const unsigned long long nb = (pr.nblocks - first < kBitsBlocks) ? pr.nblocks - first : kBitsBlocks;
+        bad = bits_unit(u, pr.nblocks, spw, reduced, nx, fw, slot, pw, int(tl), int(cl), pr.keepF, pr.keepR, sm) ||
+              bad;
+        my_states += 256ull * nb;
+        my_eval += 256ull * nb;
         if (__any_sync(kFull, bad)) break;
-        if ((ab & 15ull) == 15ull &&
+        if ((u & 15ull) == 15ull &&
             __shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0))
           break;
       }
@@ -1169,9 +1250,12 @@ void launch_pairs_from_survivors(const DevTargets& T, const DevPool& P, const QC
 template <int K>
 void launch_exhaustive_k(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
                          unsigned long long total, cudaStream_t s) {
+  // shared memory: the candidate's output planes, kBitsWords words per lane
+  constexpr int smem = kBlock * kBitsWords * 4;
   static int per_sm = 0;
   if (!per_sm) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_exhaustive<K>, kBlock, 0);
+    cudaFuncSetAttribute(k_exhaustive<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_exhaustive<K>, kBlock, smem);
     if (per_sm < 1) per_sm = 1;
   }
   // resident blocks, or more when the chunks exceed kChunksPerWarp per warp
@@ -1182,7 +1266,7 @@ void launch_exhaustive_k(const DevTargets& T, const DevPool& P, const RoundBuf& 
   const unsigned long long cover = (total + wpb * kChunksPerWarp - 1) / (wpb * kChunksPerWarp);
   if (grid < cover) grid = cover;
   if (grid > 0x7FFFFFFFull) grid = 0x7FFFFFFFull;
-  k_exhaustive<K><<<unsigned(grid), kBlock, 0, s>>>(T, P, R, npairs, total);
+  k_exhaustive<K><<<unsigned(grid), kBlock, smem, s>>>(T, P, R, npairs, total);
 }
 
 void launch_exhaustive(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,

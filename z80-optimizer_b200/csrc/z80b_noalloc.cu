@@ -110,8 +110,9 @@ extern "C" int z80b_exhaustive_noalloc(int device, const uint32_t* tgt, const ui
     p.nblocks = sweep_for(rd).states / 256;
     p.keepF = uint8_t(~(dead ? dead[i] : 0u));
     p.keepR = 0x3F;
-    // A-independent pairs are swept in units of 128 blocks (see the sweep kernel)
-    unsigned long long units = p.nblocks;
+    // sweep units (see the sweep kernel): 128 A-blocks for A-independent
+    // pairs, 4 A-blocks (bit-sliced) for the others
+    unsigned long long units = (p.nblocks + 3) / 4;
     if (seq_aflow(&h_tgt[size_t(i) * kStride], int(tl)) && seq_aflow(&h_cand[size_t(i) * kStride], int(cl))) {
       p.keepR |= 0x40;
       units = (p.nblocks + 127) / 128;
