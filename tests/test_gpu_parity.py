@@ -246,6 +246,36 @@ def test_staged_equals_search(ctx):
     assert rule_keys(staged) == rule_keys(rules)
 
 
+@pytest.mark.parametrize("all_hits", [False, True])
+def test_qc_index_equals_full_scan(ctx, O, all_hits):
+    """QuickCheck through the pool's bucket index gives the rules, survivor
+    counts and QuickCheck unit counts of the scan over every candidate, under
+    per-target dead flags and dead registers (and, in all-hits mode, the
+    80-byte fingerprint compare over a loaded pool)."""
+    targets = workloads.to_lists(workloads.c2_subset(4000, seed=21))
+    g = workloads.splitmix64(5)
+    dead = [next(g) & 0xFF for _ in targets]
+    dregs = [next(g) & 0x3F if i % 3 else 0 for i in range(len(targets))]
+    kw = dict(per_target_dead=dead, dead_regs=dregs)
+    if all_hits:
+        ctx.load_candidates(z80b.pool8(), 1)
+        kw = dict(dead_flags=0xFF, mode=z80b.MODE_ALL)
+    out = []
+    try:
+        for on in (0, 1):
+            ctx.set_option(z80b.OPT_QC_INDEX, on)
+            rules, st = ctx.search(targets, **kw)
+            out.append((rule_keys(rules), st.checks, st.checked_ref, st.qc_survivors, st.exhaustive_pairs))
+    finally:
+        ctx.set_option(z80b.OPT_QC_INDEX, 1)
+    assert out[0] == out[1]
+    assert len(out[1][0]) > 100
+    if not all_hits:
+        exp, checked = O.search_ext(targets, 1, dead=dead, dregs=dregs)
+        assert out[1][0] == rule_keys(exp)
+        assert out[1][2] == checked
+
+
 @pytest.mark.parametrize("lane_states,chunk", [(1, 8), (2, 32), (4, 128), (8, 512), (4, 1)])
 def test_tuning_options_keep_parity(ctx, O, lane_states, chunk):
     targets = workloads.to_lists(workloads.c2_subset(2500, seed=12))

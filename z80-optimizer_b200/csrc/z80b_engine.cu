@@ -63,6 +63,10 @@ struct DBuf {
 
 struct PoolBufs {
   DBuf insn, qc, mid, size, prune, reads, lens;
+  // QuickCheck bucket index (pools of at most kQCIndexMax candidates)
+  DBuf qkeys, qkeys_tmp, qtop, qelig, qsort_tmp;
+  int qstate = 0;          // 0 not built, 1 built, -1 pool too large
+  uint32_t qw2 = 0;        // word-2 mask the index hashes
   DevPool dev{};
   std::vector<uint32_t> host_insn;
   std::vector<uint8_t> host_lens;
@@ -147,6 +151,7 @@ struct z80b_ctx {
   int exh_k = 4;              // ExhaustiveCheck states per lane per dispatch (z80b_set_option)
   int chunk_blocks = 32;      // A-blocks per ExhaustiveCheck work chunk
   int priority = 0;           // Z80B_OPT_STREAM_PRIORITY
+  int qc_index = 1;           // Z80B_OPT_QC_INDEX
 };
 
 namespace {
@@ -363,6 +368,55 @@ int ensure_pair_index(z80b_ctx* ctx, uint32_t m) {
   return Z80B_OK;
 }
 
+// QuickCheck bucket index of a pool: every candidate's (dead-register mask,
+// hash of its masked vector-0 output, index) key for all 64 masks in one
+// sort, the per-mask top tables, and the eligible-candidate counts by
+// target size.  Pools above kQCIndexMax candidates keep the full scan.
+int ensure_qc_index(z80b_ctx* ctx, PoolBufs& P, uint32_t w2mask) {
+  if (P.qstate == -1) return Z80B_OK;
+  if (P.qstate == 1 && P.qw2 == w2mask) return Z80B_OK;
+  const uint32_t n = P.dev.n;
+  if (n == 0 || n > kQCIndexMax) {
+    P.qstate = -1;
+    return Z80B_OK;
+  }
+  cudaStream_t s = ctx->stream;
+  std::vector<uint8_t> size(n), prune(n);
+  CK(cudaMemcpyAsync(size.data(), P.size.p, n, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(prune.data(), P.prune.p, n, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  std::vector<uint32_t> by_size(257, 0), elig(256, 0);
+  uint32_t nv = 0;
+  for (uint32_t q = 0; q < n; q++)
+    if (!prune[q]) {
+      nv++;
+      by_size[size[q]]++;
+    }
+  for (int b = 1; b < 256; b++) elig[size_t(b)] = elig[size_t(b - 1)] + by_size[size_t(b - 1)];
+  const size_t nk = 64ull * n;
+  CK(P.qkeys_tmp.ensure(nk * 8));
+  CK(P.qkeys.ensure(nk * 8));
+  CK(P.qtop.ensure(64ull * (kQCTop + 1) * 4));
+  CK(P.qelig.ensure(256 * 4));
+  launch_qc_keys(P.dev, w2mask, P.qkeys_tmp.as<unsigned long long>(), s);
+  CKR(check_launch(ctx, "qc_keys"));
+  size_t tmp = 0;
+  CK(cub::DeviceRadixSort::SortKeys(nullptr, tmp, P.qkeys_tmp.as<unsigned long long>(),
+                                    P.qkeys.as<unsigned long long>(), int(nk), 0, 64, s));
+  CK(P.qsort_tmp.ensure(tmp));
+  CK(cub::DeviceRadixSort::SortKeys(P.qsort_tmp.p, tmp, P.qkeys_tmp.as<unsigned long long>(),
+                                    P.qkeys.as<unsigned long long>(), int(nk), 0, 64, s));
+  launch_qc_top(P.qkeys.as<unsigned long long>(), nv, P.qtop.as<uint32_t>(), s);
+  CKR(check_launch(ctx, "qc_top"));
+  CK(cudaMemcpyAsync(P.qelig.p, elig.data(), 256 * 4, cudaMemcpyHostToDevice, s));
+  CK(cudaStreamSynchronize(s));
+  ctx->launches += 3;
+  P.qstate = 1;
+  P.qw2 = w2mask;
+  trace("QuickCheck index: %u candidates, %u unpruned, 64 masks", n, nv);
+  return Z80B_OK;
+}
+
 int validate_job(z80b_ctx* ctx, const z80b_job* job) {
   if (!job) return fail(ctx, Z80B_EINVAL, "job is null");
   if (job->n_targets && !job->targets) return fail(ctx, Z80B_EINVAL, "targets is null");
@@ -487,6 +541,17 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
   CK(cudaMemsetAsync(ctx->checked.p, 0, 8, s));
   CK(cudaMemsetAsync(ctx->states.p, 0, 16, s));
 
+  QCIndex qix{};
+  bool use_ix = false;
+  if (ctx->qc_index) {
+    CKR(ensure_qc_index(ctx, *pool, cfg.w2mask));
+    if (pool->qstate == 1) {
+      use_ix = true;
+      qix.keys = pool->qkeys.as<unsigned long long>();
+      qix.top = pool->qtop.as<uint32_t>();
+      qix.elig_lt = pool->qelig.as<uint32_t>();
+    }
+  }
   trace("pipeline: %u targets, mode %u, pool %u", n, mode, P.n);
   Timer tall{ctx, 0, 1};
   ctx->kev_used = 0;
@@ -498,7 +563,8 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
   q.cnt_all = ctx->cnt_all.as<uint32_t>();
   q.meta = ctx->meta.as<TargetMeta>();
   q.checks = ctx->checks.as<unsigned long long>();
-  launch_qc_scan(T, P, cfg, q, false, s);
+  if (use_ix) launch_qc_bucket(T, P, cfg, qix, q, false, s);
+  else launch_qc_scan(T, P, cfg, q, false, s);
   kend(ctx, kq);
   CKR(check_launch(ctx, "qc_count"));
   CKR(scan(ctx, ctx->cnt_all.as<uint32_t>(), ctx->base.as<uint32_t>(), n));
@@ -517,7 +583,8 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
   q.sdiff = ctx->sdiff.as<uint16_t>();
   if (nsurv) {
     int kc = kbegin(ctx, 0);
-    launch_qc_scan(T, P, cfg, q, true, s);
+    if (use_ix) launch_qc_bucket(T, P, cfg, qix, q, true, s);
+    else launch_qc_scan(T, P, cfg, q, true, s);
     kend(ctx, kc);
     CKR(check_launch(ctx, "qc_collect"));
   }
@@ -1240,6 +1307,10 @@ int z80b_set_option(z80b_ctx* ctx, int option, int value) {
       ctx->priority = value;
       return Z80B_OK;
     }
+    case Z80B_OPT_QC_INDEX:
+      if (value != 0 && value != 1) return fail(ctx, Z80B_EINVAL, "QuickCheck index option must be 0 or 1");
+      ctx->qc_index = value;
+      return Z80B_OK;
   }
   return fail(ctx, Z80B_EINVAL, "unknown option %d", option);
 }
@@ -1250,6 +1321,7 @@ int z80b_get_option(const z80b_ctx* ctx, int option, int* value) {
     case Z80B_OPT_EXH_LANE_STATES: *value = ctx->exh_k; return Z80B_OK;
     case Z80B_OPT_EXH_CHUNK_BLOCKS: *value = ctx->chunk_blocks; return Z80B_OK;
     case Z80B_OPT_STREAM_PRIORITY: *value = ctx->priority; return Z80B_OK;
+    case Z80B_OPT_QC_INDEX: *value = ctx->qc_index; return Z80B_OK;
   }
   return Z80B_EINVAL;
 }

@@ -243,6 +243,123 @@ __global__ void k_fp_query(DevPool P, const uint32_t* __restrict__ fp, uint32_t 
   }
 }
 
+// Target side of a QuickCheck: encoded bytes, T-states and reads of the
+// target (summed over its lanes), its outputs on the 8 vectors (warp-uniform
+// copies) and the compared bytes of the packed words under its dead masks.
+struct QCTarget {
+  uint32_t tb, tts, trd, tl;
+  uint32_t tw[8][3];
+  uint32_t keep0, keep1;
+};
+__device__ __forceinline__ void qc_target(const DevTargets& T, uint32_t t, QCTarget& g) {
+  const unsigned lane = lane_id();
+  const uint32_t tl = target_len(T, t);
+  const uint32_t pw = lane < tl ? T.insn[(size_t)t * T.stride + lane] : 0u;
+  uint32_t sz = 0, ts = 0, rd = 0;
+  if (lane < tl) {
+    const OpInfo oi = g_ops[pw & 0xFFFFu];
+    sz = oi.size;
+    ts = oi.tstates;
+    rd = oi.reads;
+  }
+#pragma unroll
+  for (int off = 2; off >= 1; off >>= 1) {
+    sz += __shfl_down_sync(kFull, sz, off);
+    ts += __shfl_down_sync(kFull, ts, off);
+    rd |= __shfl_down_sync(kFull, rd, off);
+  }
+  g.tl = tl;
+  g.tb = __shfl_sync(kFull, sz, 0);
+  g.tts = __shfl_sync(kFull, ts, 0);
+  g.trd = __shfl_sync(kFull, rd, 0);
+  Z80S s = vec_state(int(lane & 7u));
+  run_lanes(s, pw, 0, int(tl));
+  uint32_t w[3];
+  z_pack(s, w);
+#pragma unroll
+  for (int v = 0; v < 8; v++) {
+    g.tw[v][0] = __shfl_sync(kFull, w[0], v);
+    g.tw[v][1] = __shfl_sync(kFull, w[1], v);
+    g.tw[v][2] = __shfl_sync(kFull, w[2], v);
+  }
+  const uint32_t dead = target_dead(T, t) & 0xFFu;
+  const uint32_t dregs = target_dead_regs(T, t) & 0x3Fu;
+  g.keep0 = 0xFFu | ((~dead & 0xFFu) << 8) | ((dregs & 1u) ? 0u : 0xFF0000u) | ((dregs & 2u) ? 0u : 0xFF000000u);
+  g.keep1 = ((dregs & 4u) ? 0u : 0xFFu) | ((dregs & 8u) ? 0u : 0xFF00u) | ((dregs & 16u) ? 0u : 0xFF0000u) |
+            ((dregs & 32u) ? 0u : 0xFF000000u);
+}
+
+// QuickCheck of candidate c (vector-0 output q) against the target: fp
+// (full equivalence; every pass in all-hits mode), mp (passes only under the
+// dead masks), diff (FlagDiff | differing registers << 8 over the vectors).
+__device__ __forceinline__ void qc_candidate(const DevPool& P, uint4 q, uint32_t c, const QCTarget& g,
+                                             uint32_t keep2, bool all_hits, bool& fp, bool& mp, uint32_t& diff) {
+  const uint32_t d0 = q.x ^ g.tw[0][0], d1 = q.y ^ g.tw[0][1], d2 = q.z ^ g.tw[0][2];
+  if (((d0 & g.keep0) | (d1 & g.keep1) | (d2 & keep2)) != 0) return;
+  bool full = (d0 | d1 | (d2 & keep2)) == 0;
+  uint32_t fd = (d0 >> 8) & 0xFFu, rdf = reg_diff(d0, d1);
+  bool ok = true;
+#pragma unroll
+  for (int v = 1; v < 8; v++) {
+    const uint4 qv = P.qc[(size_t)v * P.n + c];
+    const uint32_t e0 = qv.x ^ g.tw[v][0], e1 = qv.y ^ g.tw[v][1], e2 = qv.z ^ g.tw[v][2];
+    ok = ok && (((e0 & g.keep0) | (e1 & g.keep1) | (e2 & keep2)) == 0);
+    full = full && ((e0 | e1 | (e2 & keep2)) == 0);
+    fd |= (e0 >> 8) & 0xFFu;
+    rdf |= reg_diff(e0, e1);
+  }
+  if (!ok) return;
+  if (all_hits) {
+    fp = true;
+  } else {
+    fp = full;
+    mp = !full;
+  }
+  diff = fd | (rdf << 8);
+}
+
+// Appends this warp's survivors of one 32-candidate step in enumeration
+// order (collect pass) or tallies them per lane (count pass).
+template <bool COLLECT>
+__device__ __forceinline__ void qc_emit(const QCOut& o, bool fp, bool mp, uint32_t c, uint32_t diff, uint32_t obase,
+                                        uint32_t nf_total, uint32_t& nf, uint32_t& nm, uint32_t& lf,
+                                        uint32_t& lm) {
+  if constexpr (!COLLECT) {
+    lf += fp ? 1u : 0u;
+    lm += mp ? 1u : 0u;
+  } else {
+    const unsigned bf = __ballot_sync(kFull, fp);
+    const unsigned bm = __ballot_sync(kFull, mp);
+    if (fp) {
+      const uint32_t idx = obase + nf + __popc(bf & lanemask_lt());
+      o.surv[idx] = c;
+      o.sdiff[idx] = uint16_t(diff);
+    }
+    if (mp) {
+      const uint32_t idx = obase + nf_total + nm + __popc(bm & lanemask_lt());
+      o.surv[idx] = c;
+      o.sdiff[idx] = uint16_t(diff);
+    }
+    nf += __popc(bf);
+    nm += __popc(bm);
+  }
+}
+
+// Count-pass epilogue: survivor counts and the target's metadata.
+__device__ __forceinline__ void qc_count_out(const QCOut& o, uint32_t t, const QCTarget& g, uint32_t nf,
+                                             uint32_t nm) {
+  o.cnt_f[t] = nf;
+  o.cnt_m[t] = nm;
+  o.cnt_all[t] = nf + nm;
+  TargetMeta m;
+  m.tstates = uint16_t(g.tts);
+  m.bytes = uint8_t(g.tb);
+  m.len = uint8_t(g.tl);
+  m.reads = uint16_t(g.trd);
+  m.pad = 0;
+  o.meta[t] = m;
+}
+
 template <bool COLLECT>
 __global__ void __launch_bounds__(kBlock) k_qc_scan(DevTargets T, DevPool P, QCConfig cfg, QCOut o) {
   extern __shared__ uint4 smem[];
@@ -268,44 +385,8 @@ __global__ void __launch_bounds__(kBlock) k_qc_scan(DevTargets T, DevPool P, QCC
       if (nf_total + o.cnt_m[t] == 0) continue;
       obase = o.base[t];
     }
-    const uint32_t tl = target_len(T, t);
-    const uint32_t pw = lane < tl ? T.insn[(size_t)t * T.stride + lane] : 0u;
-    uint32_t sz = 0, ts = 0, rd = 0;
-    if (lane < tl) {
-      const OpInfo oi = g_ops[pw & 0xFFFFu];
-      sz = oi.size;
-      ts = oi.tstates;
-      rd = oi.reads;
-    }
-#pragma unroll
-    for (int off = 2; off >= 1; off >>= 1) {
-      sz += __shfl_down_sync(kFull, sz, off);
-      ts += __shfl_down_sync(kFull, ts, off);
-      rd |= __shfl_down_sync(kFull, rd, off);
-    }
-    const uint32_t tb = __shfl_sync(kFull, sz, 0);
-    const uint32_t tts = __shfl_sync(kFull, ts, 0);
-    const uint32_t trd = __shfl_sync(kFull, rd, 0);
-
-    Z80S s = vec_state(int(lane & 7u));
-    run_lanes(s, pw, 0, int(tl));
-    uint32_t w[3];
-    z_pack(s, w);
-    uint32_t tw[8][3];
-#pragma unroll
-    for (int v = 0; v < 8; v++) {
-      tw[v][0] = __shfl_sync(kFull, w[0], v);
-      tw[v][1] = __shfl_sync(kFull, w[1], v);
-      tw[v][2] = __shfl_sync(kFull, w[2], v);
-    }
-    const uint32_t dead = target_dead(T, t) & 0xFFu;
-    const uint32_t dregs = target_dead_regs(T, t) & 0x3Fu;
-    const uint32_t keep0 = 0xFFu | ((~dead & 0xFFu) << 8) | ((dregs & 1u) ? 0u : 0xFF0000u) |
-                           ((dregs & 2u) ? 0u : 0xFF000000u);
-    const uint32_t keep1 = ((dregs & 4u) ? 0u : 0xFFu) | ((dregs & 8u) ? 0u : 0xFF00u) |
-                           ((dregs & 16u) ? 0u : 0xFF0000u) | ((dregs & 32u) ? 0u : 0xFF000000u);
-    const uint32_t keep2 = cfg.w2mask;
-
+    QCTarget g;
+    qc_target(T, t, g);
     uint32_t nf = 0, nm = 0;
     uint32_t lf = 0, lm = 0, lc = 0;  // count pass: per-lane tallies, reduced once per target
     for (uint32_t base = 0; base < P.n; base += 32) {
@@ -313,76 +394,22 @@ __global__ void __launch_bounds__(kBlock) k_qc_scan(DevTargets T, DevPool P, QCC
       bool el = false;
       if (c < P.n) {
         uint32_t e = cfg.use_smem ? s_el[c] : (P.size[c] | (P.prune[c] ? 0x80u : 0u));
-        el = (e & 0x7Fu) < tb && !(e & 0x80u);
+        el = (e & 0x7Fu) < g.tb && !(e & 0x80u);
       }
       bool fp = false, mp = false;
       uint32_t diff = 0;
-      if (el) {
-        uint4 q = cfg.use_smem ? s_q0[c] : P.qc[c];
-        uint32_t d0 = q.x ^ tw[0][0], d1 = q.y ^ tw[0][1], d2 = q.z ^ tw[0][2];
-        if (((d0 & keep0) | (d1 & keep1) | (d2 & keep2)) == 0) {
-          bool full = (d0 | d1 | (d2 & keep2)) == 0;
-          uint32_t fd = (d0 >> 8) & 0xFFu, rdf = reg_diff(d0, d1);
-          bool ok = true;
-#pragma unroll
-          for (int v = 1; v < 8; v++) {
-            uint4 qv = P.qc[(size_t)v * P.n + c];
-            uint32_t e0 = qv.x ^ tw[v][0], e1 = qv.y ^ tw[v][1], e2 = qv.z ^ tw[v][2];
-            ok = ok && (((e0 & keep0) | (e1 & keep1) | (e2 & keep2)) == 0);
-            full = full && ((e0 | e1 | (e2 & keep2)) == 0);
-            fd |= (e0 >> 8) & 0xFFu;
-            rdf |= reg_diff(e0, e1);
-          }
-          if (ok) {
-            if (cfg.all_hits) {
-              fp = true;
-            } else {
-              fp = full;
-              mp = !full;
-            }
-            diff = fd | (rdf << 8);
-          }
-        }
-      }
-      if constexpr (!COLLECT) {
-        lc += el ? 1u : 0u;
-        lf += fp ? 1u : 0u;
-        lm += mp ? 1u : 0u;
-      } else {
-        // ballots give the survivors their enumeration-ordered slots
-        const unsigned bf = __ballot_sync(kFull, fp);
-        const unsigned bm = __ballot_sync(kFull, mp);
-        if (fp) {
-          uint32_t idx = obase + nf + __popc(bf & lanemask_lt());
-          o.surv[idx] = c;
-          o.sdiff[idx] = uint16_t(diff);
-        }
-        if (mp) {
-          uint32_t idx = obase + nf_total + nm + __popc(bm & lanemask_lt());
-          o.surv[idx] = c;
-          o.sdiff[idx] = uint16_t(diff);
-        }
-        nf += __popc(bf);
-        nm += __popc(bm);
-      }
+      if (el) qc_candidate(P, cfg.use_smem ? s_q0[c] : P.qc[c], c, g, cfg.w2mask, cfg.all_hits != 0, fp, mp, diff);
+      if constexpr (!COLLECT) lc += el ? 1u : 0u;
+      qc_emit<COLLECT>(o, fp, mp, c, diff, obase, nf_total, nf, nm, lf, lm);
     }
     if constexpr (!COLLECT) {
       nf = __reduce_add_sync(kFull, lf);
       nm = __reduce_add_sync(kFull, lm);
       const uint32_t nc = __reduce_add_sync(kFull, lc);
-      if (lane == 0) my_checks += nc;
-    }
-    if (!COLLECT && lane == 0) {
-      o.cnt_f[t] = nf;
-      o.cnt_m[t] = nm;
-      o.cnt_all[t] = nf + nm;
-      TargetMeta m;
-      m.tstates = uint16_t(tts);
-      m.bytes = uint8_t(tb);
-      m.len = uint8_t(tl);
-      m.reads = uint16_t(trd);
-      m.pad = 0;
-      o.meta[t] = m;
+      if (lane == 0) {
+        my_checks += nc;
+        qc_count_out(o, t, g, nf, nm);
+      }
     }
   }
   if (!COLLECT && lane == 0 && my_checks) atomicAdd(o.checks, my_checks);
@@ -1005,6 +1032,81 @@ __device__ __forceinline__ uint32_t lower_bound_u64(const unsigned long long* a,
   return lo;
 }
 
+// QuickCheck bucket index of a candidate pool (at most 65,536 entries): one
+// segment per dead-register mask m, keys m << 48 | bucket hash << 16 | index
+// sorted, pruned candidates left out (their keys sort past the last
+// segment); a top table per segment holds the first entry of each 4,096th of
+// the hash range.
+__global__ void k_qc_keys(DevPool P, uint32_t w2mask, unsigned long long* __restrict__ keys) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 64u * P.n) return;
+  const uint32_t m = i / P.n, q = i - m * P.n;
+  if (P.prune[q]) {
+    keys[i] = ~0ull;
+    return;
+  }
+  const uint4 o = P.qc[q];
+  const uint32_t h = bucket_hash(o.x & key_keep0(m), o.y & key_keep1(m), o.z & w2mask);
+  keys[i] = ((unsigned long long)m << 48) | ((unsigned long long)h << 16) | q;
+}
+__global__ void k_qc_top(const unsigned long long* __restrict__ keys, uint32_t nv, uint32_t* __restrict__ top) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 64u * (kQCTop + 1)) return;
+  const uint32_t m = i / (kQCTop + 1), b = i - m * (kQCTop + 1);
+  top[i] = b == kQCTop ? (m + 1) * nv
+                       : m * nv + lower_bound_u64(keys + (size_t)m * nv, nv,
+                                                  ((unsigned long long)m << 48) | ((unsigned long long)b << 36));
+}
+
+// QuickCheck through the bucket index: a target only meets the candidates
+// whose vector-0 output agrees with its own on A, the live registers and
+// word 2 (the flags are compared per candidate, under the dead flags), which
+// is every candidate that can pass.  Entries of a bucket are in pool order,
+// so survivors come out in enumeration order as in the full scan.
+template <bool COLLECT>
+__global__ void __launch_bounds__(kBlock) k_qc_bucket(DevTargets T, DevPool P, QCConfig cfg, QCIndex ix, QCOut o) {
+  const unsigned lane = lane_id();
+  const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const uint32_t nw = gridDim.x * (blockDim.x >> 5);
+  unsigned long long my_checks = 0;
+  for (uint32_t t = gw; t < T.n; t += nw) {
+    uint32_t nf_total = 0, obase = 0;
+    if (COLLECT) {
+      nf_total = o.cnt_f[t];
+      if (nf_total + o.cnt_m[t] == 0) continue;
+      obase = o.base[t];
+    }
+    QCTarget g;
+    qc_target(T, t, g);
+    const uint32_t m = target_dead_regs(T, t) & 0x3Fu;
+    const uint32_t h = bucket_hash(g.tw[0][0] & key_keep0(m), g.tw[0][1] & key_keep1(m), g.tw[0][2] & cfg.w2mask);
+    const uint32_t* top = ix.top + m * (kQCTop + 1) + (h >> (32 - kQCTopBits));
+    const uint32_t r0 = top[0], r1 = top[1];
+    uint32_t nf = 0, nm = 0, lf = 0, lm = 0;
+    for (uint32_t base = r0; base < r1; base += 32) {
+      const uint32_t i = base + lane;
+      bool fp = false, mp = false;
+      uint32_t diff = 0, c = 0;
+      if (i < r1) {
+        const unsigned long long key = ix.keys[i];
+        c = uint32_t(key) & 0xFFFFu;
+        if (uint32_t(key >> 16) == h && P.size[c] < g.tb)
+          qc_candidate(P, P.qc[c], c, g, cfg.w2mask, cfg.all_hits != 0, fp, mp, diff);
+      }
+      qc_emit<COLLECT>(o, fp, mp, c, diff, obase, nf_total, nf, nm, lf, lm);
+    }
+    if constexpr (!COLLECT) {
+      nf = __reduce_add_sync(kFull, lf);
+      nm = __reduce_add_sync(kFull, lm);
+      if (lane == 0) {
+        my_checks += ix.elig_lt[g.tb < 255u ? g.tb : 255u];
+        qc_count_out(o, t, g, nf, nm);
+      }
+    }
+  }
+  if (!COLLECT && lane == 0 && my_checks) atomicAdd(o.checks, my_checks);
+}
+
 // Warp per target: (re)fills the slots of each lane whose slots are used up
 // and whose bucket has pairs left.
 __global__ void __launch_bounds__(kBlock) k_pair_scan(DevTargets T, DevPool P, QCOut q1, Lanes L2, PairScan ps) {
@@ -1235,6 +1337,27 @@ void launch_qc_scan(const DevTargets& T, const DevPool& P, const QCConfig& cfg, 
   if (grid > need) grid = need;
   if (collect) k_qc_scan<true><<<grid, kBlock, smem, s>>>(T, P, cfg, o);
   else k_qc_scan<false><<<grid, kBlock, smem, s>>>(T, P, cfg, o);
+}
+void launch_qc_keys(const DevPool& P, uint32_t w2mask, unsigned long long* keys, cudaStream_t s) {
+  const uint32_t n = 64u * P.n;
+  if (n) k_qc_keys<<<grid_for(n, 256), 256, 0, s>>>(P, w2mask, keys);
+}
+void launch_qc_top(const unsigned long long* keys, uint32_t nv, uint32_t* top, cudaStream_t s) {
+  const uint32_t n = 64u * (kQCTop + 1);
+  k_qc_top<<<grid_for(n, 256), 256, 0, s>>>(keys, nv, top);
+}
+void launch_qc_bucket(const DevTargets& T, const DevPool& P, const QCConfig& cfg, const QCIndex& ix,
+                      const QCOut& o, bool collect, cudaStream_t s) {
+  if (!T.n) return;
+  int per_sm = 0;
+  if (collect) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_qc_bucket<true>, kBlock, 0);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_qc_bucket<false>, kBlock, 0);
+  if (per_sm < 1) per_sm = 1;
+  unsigned need = grid_for(T.n, kBlock / 32);
+  unsigned grid = unsigned(dev_num_sms() * per_sm);
+  if (grid > need) grid = need;
+  if (collect) k_qc_bucket<true><<<grid, kBlock, 0, s>>>(T, P, cfg, ix, o);
+  else k_qc_bucket<false><<<grid, kBlock, 0, s>>>(T, P, cfg, ix, o);
 }
 void launch_round_build(const DevTargets& T, const DevPool& P, const QCOut& q, const Lanes& L,
                         const RoundBuf& R, cudaStream_t s) {

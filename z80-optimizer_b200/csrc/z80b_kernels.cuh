@@ -26,6 +26,19 @@ struct QCConfig {
   int use_smem;      // pool QC0 staged in shared memory
 };
 
+// QuickCheck bucket index of a candidate pool (pools of at most 65,536
+// candidates): 64 segments (one per dead-register mask) of sorted keys
+// m << 48 | hash << 16 | index over the unpruned candidates, a top table of
+// kQCTop + 1 offsets per segment, and the unpruned candidates shorter than b
+// bytes (the count of QuickCheck units a target of b bytes evaluates).
+constexpr uint32_t kQCTopBits = 12, kQCTop = 1u << kQCTopBits;
+constexpr uint32_t kQCIndexMax = 65536;
+struct QCIndex {
+  const unsigned long long* keys;  // [64 * n_valid]
+  const uint32_t* top;             // [64 * (kQCTop + 1)]
+  const uint32_t* elig_lt;         // [256]
+};
+
 // Per-(target, kind) progress of the first-found rounds.
 struct Lanes {
   uint32_t* next;    // [2n] survivor index to try next; bit31 = resolved
@@ -79,6 +92,10 @@ void launch_qc_scan(const DevTargets& T, const DevPool& P, const QCConfig& cfg, 
                     bool collect, cudaStream_t s);
 void launch_fp_query(const DevPool& P, const uint32_t* fp3x8, uint32_t dead, uint32_t* hits,
                      uint32_t* nhits, uint32_t cap, cudaStream_t s);
+void launch_qc_keys(const DevPool& P, uint32_t w2mask, unsigned long long* keys, cudaStream_t s);
+void launch_qc_top(const unsigned long long* keys, uint32_t nv, uint32_t* top, cudaStream_t s);
+void launch_qc_bucket(const DevTargets& T, const DevPool& P, const QCConfig& cfg, const QCIndex& ix,
+                      const QCOut& o, bool collect, cudaStream_t s);
 void launch_round_build(const DevTargets& T, const DevPool& P, const QCOut& q, const Lanes& L,
                         const RoundBuf& R, cudaStream_t s);
 void launch_pairs_from_survivors(const DevTargets& T, const DevPool& P, const QCOut& q,

@@ -103,7 +103,7 @@ EXPORTS = [
     "z80b_search_cb",
 ]
 RULE_CB = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32)
-OPT_EXH_LANE_STATES, OPT_EXH_CHUNK_BLOCKS, OPT_STREAM_PRIORITY = 1, 2, 3
+OPT_EXH_LANE_STATES, OPT_EXH_CHUNK_BLOCKS, OPT_STREAM_PRIORITY, OPT_QC_INDEX = 1, 2, 3, 4
 
 
 MULPOOL_MULOPT, MULPOOL_WIDE21, MULPOOL_FAST14, MULPOOL_CUDA21 = 0, 1, 2, 3
