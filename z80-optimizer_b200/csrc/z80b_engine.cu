@@ -135,7 +135,7 @@ struct z80b_ctx {
   Staged staged;
   // pipeline scratch
   DBuf cnt_f, cnt_m, cnt_all, base, meta, surv, sdiff, checks;
-  DBuf next, win, windiff;
+  DBuf next, win, windiff, spec, spec2, wlen;
   DBuf pairs, pair_src, nchunks, cbase, rejected, npairs, counter, states;
   DBuf rcnt, rbase, rules, checked, surv_target, midpass, flag;
   DBuf cub_tmp;
@@ -596,19 +596,26 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
     CK(ctx->next.ensure(8ull * n));
     CK(ctx->win.ensure(8ull * n));
     CK(ctx->windiff.ensure(4ull * n));
-    CK(ctx->pairs.ensure(sizeof(PairRec) * 2ull * n));
-    CK(ctx->pair_src.ensure(8ull * n));
-    CK(ctx->nchunks.ensure(16ull * n));
-    CK(ctx->cbase.ensure(16ull * n));
-    CK(ctx->rejected.ensure(8ull * n));
+    // pair slots per round: every lane once, and room for survivor windows
+    const uint64_t cap = std::max<uint64_t>(2ull * n, std::min<uint64_t>(128ull * n, 1ull << 20));
+    CK(ctx->pairs.ensure(sizeof(PairRec) * cap));
+    CK(ctx->pair_src.ensure(4 * cap));
+    CK(ctx->nchunks.ensure(8 * cap));
+    CK(ctx->cbase.ensure(8 * cap));
+    CK(ctx->rejected.ensure(4 * cap));
+    CK(ctx->wlen.ensure(cap));
+    CK(ctx->spec.ensure(2ull * n));
+    CK(cudaMemsetAsync(ctx->spec.p, 0, 2ull * n, s));
     CK(cudaMemsetAsync(ctx->next.p, 0, 8ull * n, s));
     CK(cudaMemsetAsync(ctx->win.p, 0xFF, 8ull * n, s));
-    Lanes L{ctx->next.as<uint32_t>(), ctx->win.as<uint32_t>(), ctx->windiff.as<uint16_t>()};
+    Lanes L{ctx->next.as<uint32_t>(), ctx->win.as<uint32_t>(), ctx->windiff.as<uint16_t>(), ctx->spec.as<uint8_t>()};
     R.pairs = ctx->pairs.as<PairRec>();
     R.pair_src = ctx->pair_src.as<uint32_t>();
     R.nchunks = ctx->nchunks.as<unsigned long long>();
     R.cbase = ctx->cbase.as<unsigned long long>();
     R.rejected = ctx->rejected.as<uint32_t>();
+    R.wlen = ctx->wlen.as<uint8_t>();
+    R.cap = uint32_t(cap);
     R.npairs = ctx->npairs.as<uint32_t>();
     R.counter = ctx->counter.as<unsigned long long>();
     R.states = ctx->states.as<unsigned long long>();
@@ -620,6 +627,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
         CKR(check_launch(ctx, "round_build"));
         uint32_t np = 0;
         CKR(fetch(ctx, &np, R.npairs));
+        np = std::min(np, R.cap);
         trace("round %u: %u pairs", rounds, np);
         if (np == 0) break;
         rounds++;
@@ -635,7 +643,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
         launch_exhaustive(T, P, R, np, lastb + lastn, ctx->exh_k, s);
         kend(ctx, ke);
         CKR(check_launch(ctx, "exhaustive"));
-        launch_round_resolve(R, np, q, L, s);
+        launch_round_resolve(R, np, q, L, kMaxSpec1, s);
         CKR(check_launch(ctx, "round_resolve"));
         if (opts.rep) CKR(opts.rep->update(ctx, n, L, Lanes{nullptr, nullptr, nullptr}, opts.max_cand, false, false));
       }
@@ -659,7 +667,9 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
       CK(ctx->surv2.ensure(8ull * n * kSlots2));
       CK(ctx->sdiff2.ensure(4ull * n * kSlots2));
       CK(ctx->refill2.ensure(4));
-      L2 = Lanes{ctx->next2.as<uint32_t>(), ctx->win2.as<uint32_t>(), ctx->windiff2.as<uint16_t>()};
+      CK(ctx->spec2.ensure(2ull * n));
+      L2 = Lanes{ctx->next2.as<uint32_t>(), ctx->win2.as<uint32_t>(), ctx->windiff2.as<uint16_t>(),
+                 ctx->spec2.as<uint8_t>()};
       PairScan ps{};
       ps.idx = reinterpret_cast<const unsigned long long* const*>(PS.ptrs.p);
       ps.n_valid = PS.valid;
@@ -687,6 +697,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
         CK(cudaMemcpyAsync(&np, R.npairs, 4, cudaMemcpyDeviceToHost, s));
         CK(cudaMemcpyAsync(&nref, ps.refill, 4, cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
+        np = std::min(np, R.cap);
         trace("length-2 round %u: %u pairs, %u lanes to rescan", rounds, np, nref);
         if (np == 0) {
           if (nref == 0) break;
@@ -708,7 +719,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
         launch_exhaustive(T, P2, R, np, lastb + lastn, ctx->exh_k, s);
         kend(ctx, ke);
         CKR(check_launch(ctx, "exhaustive"));
-        launch_round_resolve(R, np, q2, L2, s);
+        launch_round_resolve(R, np, q2, L2, kMaxSpec2, s);
         CKR(check_launch(ctx, "round_resolve"));
         if (opts.rep) CKR(opts.rep->update(ctx, n, L, L2, opts.max_cand, true, false));
       }

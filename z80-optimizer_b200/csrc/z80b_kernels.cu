@@ -416,51 +416,70 @@ __global__ void __launch_bounds__(kBlock) k_qc_scan(DevTargets T, DevPool P, QCC
 }
 
 // Appends one pair per unresolved (target, kind) lane with an untried survivor.
-__global__ void k_round_build(DevTargets T, DevPool P, QCOut q, Lanes L, RoundBuf R) {
-  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  bool have[2] = {false, false};
-  PairRec pr[2];
-  uint32_t src[2] = {0, 0};
-  if (t < T.n) {
-    const uint32_t cf = q.cnt_f[t], cm = q.cnt_m[t];
+// Allocates w consecutive pair slots for this thread (one atomic per warp;
+// every lane of the warp takes part); returns the first slot.
+__device__ __forceinline__ uint32_t alloc_pairs(uint32_t* counter, uint32_t w) {
+  const unsigned lane = lane_id();
+  uint32_t incl = w;
 #pragma unroll
-    for (int kind = 0; kind < 2; kind++) {
-      const uint32_t idx = 2 * t + kind;
-      uint32_t nx = L.next[idx];
-      if (nx & kResolved) continue;
-      const uint32_t cnt = kind ? cm : cf;
-      if (nx >= cnt) {
-        L.next[idx] = nx | kResolved;
-        continue;
-      }
-      const uint32_t sidx = q.base[t] + (kind ? cf : 0u) + nx;
-      const uint32_t c = q.surv[sidx];
-      const uint32_t reads = q.meta[t].reads | P.reads[c];
-      pr[kind].target = t;
-      pr[kind].cand = c;
-      pr[kind].reads = uint16_t(reads);
-      pr[kind].nblocks = sweep_blocks(reads);
-      pr[kind].keepF = kind ? uint8_t(~target_dead(T, t)) : uint8_t(0xFFu);
-      pr[kind].keepR = kind ? uint8_t((~target_dead_regs(T, t) & 0x3Fu) | 0x80u) : uint8_t(0x3Fu);
-      if (pair_xindep(T, t, P, c)) pr[kind].keepR |= uint8_t(kXIndep);
-      src[kind] = sidx;
-      have[kind] = true;
-    }
+  for (int off = 1; off < 32; off <<= 1) {
+    const uint32_t v = __shfl_up_sync(kFull, incl, off);
+    if (lane >= unsigned(off)) incl += v;
   }
+  const uint32_t total = __shfl_sync(kFull, incl, 31);
+  uint32_t base = 0;
+  if (lane == 31 && total) base = atomicAdd(counter, total);
+  base = __shfl_sync(kFull, base, 31);
+  return base + incl - w;
+}
+
+// Writes one pair of a round.
+__device__ __forceinline__ void put_pair(const RoundBuf& R, uint32_t p, const DevTargets& T, const DevPool& P,
+                                         const QCOut& q, uint32_t t, uint32_t kind, uint32_t c, uint32_t src,
+                                         uint8_t wlen) {
+  PairRec pr;
+  const uint32_t reads = q.meta[t].reads | P.reads[c];
+  pr.target = t;
+  pr.cand = c;
+  pr.reads = uint16_t(reads);
+  pr.nblocks = sweep_blocks(reads);
+  pr.keepF = kind ? uint8_t(~target_dead(T, t)) : uint8_t(0xFFu);
+  pr.keepR = kind ? uint8_t((~target_dead_regs(T, t) & 0x3Fu) | 0x80u) : uint8_t(0x3Fu);
+  if (pair_xindep(T, t, P, c)) pr.keepR |= uint8_t(kXIndep);
+  R.pairs[p] = pr;
+  R.pair_src[p] = src;
+  R.nchunks[p] = chunks_for(pair_units(pr.nblocks, pr.keepR), R.chunk_blocks);
+  R.rejected[p] = 0;
+  R.wlen[p] = wlen;
+}
+
+// One round of the length-1 pass: each unresolved (target, kind) lane puts
+// its window of next survivors into the round (pairs past the buffer's
+// capacity wait for the next round).
+__global__ void k_round_build(DevTargets T, DevPool P, QCOut q, Lanes L, RoundBuf R) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
 #pragma unroll
-  for (int kind = 0; kind < 2; kind++) {
-    unsigned b = __ballot_sync(kFull, have[kind]);
-    if (!b) continue;
-    uint32_t base = 0;
-    if (lane_id() == 0) base = atomicAdd(R.npairs, (uint32_t)__popc(b));
-    base = __shfl_sync(kFull, base, 0);
-    if (have[kind]) {
-      uint32_t p = base + __popc(b & lanemask_lt());
-      R.pairs[p] = pr[kind];
-      R.pair_src[p] = src[kind];
-      R.nchunks[p] = chunks_for(pair_units(pr[kind].nblocks, pr[kind].keepR), R.chunk_blocks);
-      R.rejected[p] = 0;
+  for (uint32_t kind = 0; kind < 2; kind++) {
+    uint32_t w = 0, nx = 0, sbase = 0;
+    if (t < T.n) {
+      const uint32_t cf = q.cnt_f[t], cm = q.cnt_m[t];
+      const uint32_t idx = 2 * t + kind;
+      nx = L.next[idx];
+      if (!(nx & kResolved)) {
+        const uint32_t cnt = kind ? cm : cf;
+        if (nx >= cnt) {
+          L.next[idx] = nx | kResolved;
+        } else {
+          w = min(1u << L.spec[idx], cnt - nx);
+          sbase = q.base[t] + (kind ? cf : 0u) + nx;
+        }
+      }
     }
+    if (!__any_sync(kFull, w != 0)) continue;
+    const uint32_t p0 = alloc_pairs(R.npairs, w);
+    const uint32_t fit = p0 >= R.cap ? 0u : min(w, R.cap - p0);
+    for (uint32_t j = 0; j < fit; j++)
+      put_pair(R, p0 + j, T, P, q, t, kind, q.surv[sbase + j], sbase + j, j == 0 ? uint8_t(fit) : uint8_t(0));
   }
 }
 
@@ -803,18 +822,26 @@ __global__ void __launch_bounds__(kBlock, 1) k_exhaustive(DevTargets T, DevPool 
     atomicAdd(R.states + 1, my_eval);
   }
 }
-__global__ void k_round_resolve(RoundBuf R, uint32_t npairs, QCOut q, Lanes L) {
-  uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+// Window heads settle their lane: the first pair of the window that passed
+// wins; if none did, the lane moves past the window and the next window
+// doubles (up to 2^max_spec).
+__global__ void k_round_resolve(RoundBuf R, uint32_t npairs, QCOut q, Lanes L, uint32_t max_spec) {
+  const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npairs) return;
+  const uint32_t w = R.wlen[p];
+  if (w == 0) return;
   const PairRec pr = R.pairs[p];
   const uint32_t idx = 2 * pr.target + ((pr.keepR & 0x80u) ? 1u : 0u);
-  if (R.rejected[p] == 0) {
-    L.win[idx] = pr.cand;
-    L.windiff[idx] = q.sdiff[R.pair_src[p]];
-    L.next[idx] |= kResolved;
-  } else {
-    L.next[idx] += 1;
+  for (uint32_t j = 0; j < w; j++) {
+    if (R.rejected[p + j] == 0) {
+      L.win[idx] = R.pairs[p + j].cand;
+      L.windiff[idx] = q.sdiff[R.pair_src[p + j]];
+      L.next[idx] = (L.next[idx] + j) | kResolved;
+      return;
+    }
   }
+  L.next[idx] += w;
+  if (L.spec[idx] < max_spec) L.spec[idx] += 1;
 }
 
 __global__ void k_midcheck(DevTargets T, DevPool P, const uint32_t* __restrict__ surv,
@@ -1010,6 +1037,7 @@ __global__ void k_pair_lanes_init(DevTargets T, Lanes L1, QCOut q1, Lanes L2, Pa
       const uint32_t idx = 2 * t + kind;
       const bool need = L1.win[idx] == kNone && tb >= 3 && (kind == 0 || masked);
       L2.next[idx] = need ? 0u : kResolved;
+      L2.spec[idx] = 0;
       L2.win[idx] = kNone;
       L2.windiff[idx] = 0;
       ps.cnt[idx] = 0;
@@ -1218,27 +1246,17 @@ __global__ void __launch_bounds__(kBlock) k_pair_scan(DevTargets T, DevPool P, Q
 
 // One pair per length-2 lane with an untried survivor; lanes with no slot
 // left either end without a winner (bucket exhausted) or wait for a rescan.
+// One round of the length-2 pass: windows over the lane's slots; a lane
+// with its slots used up and its bucket not exhausted asks for a rescan.
 __global__ void k_pair_round_build(DevTargets T, DevPool P, QCOut q1, Lanes L2, PairScan ps, RoundBuf R) {
   const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
-  bool have = false;
-  PairRec pr;
-  uint32_t src = 0;
+  uint32_t w = 0, sbase = 0;
   if (idx < 2 * T.n) {
     const uint32_t nx = L2.next[idx];
     if (!(nx & kResolved)) {
-      const uint32_t t = idx >> 1, kind = idx & 1u;
       if (nx < ps.cnt[idx]) {
-        src = idx * kSlots2 + nx;
-        const uint32_t c = ps.surv[src];
-        const uint32_t reads = q1.meta[t].reads | P.reads[c];
-        pr.target = t;
-        pr.cand = c;
-        pr.reads = uint16_t(reads);
-        pr.nblocks = sweep_blocks(reads);
-        pr.keepF = kind ? uint8_t(~target_dead(T, t)) : uint8_t(0xFFu);
-        pr.keepR = kind ? uint8_t((~target_dead_regs(T, t) & 0x3Fu) | 0x80u) : uint8_t(0x3Fu);
-        if (pair_xindep(T, t, P, c)) pr.keepR |= uint8_t(kXIndep);
-        have = true;
+        w = min(1u << L2.spec[idx], ps.cnt[idx] - nx);
+        sbase = idx * kSlots2 + nx;
       } else if (ps.resume[idx] == kNone) {
         L2.next[idx] = nx | kResolved;
       } else {
@@ -1246,18 +1264,12 @@ __global__ void k_pair_round_build(DevTargets T, DevPool P, QCOut q1, Lanes L2, 
       }
     }
   }
-  const unsigned b = __ballot_sync(kFull, have);
-  if (!b) return;
-  uint32_t base = 0;
-  if (lane_id() == 0) base = atomicAdd(R.npairs, (uint32_t)__popc(b));
-  base = __shfl_sync(kFull, base, 0);
-  if (have) {
-    const uint32_t p = base + __popc(b & lanemask_lt());
-    R.pairs[p] = pr;
-    R.pair_src[p] = src;
-    R.nchunks[p] = chunks_for(pair_units(pr.nblocks, pr.keepR), R.chunk_blocks);
-    R.rejected[p] = 0;
-  }
+  if (!__any_sync(kFull, w != 0)) return;
+  const uint32_t p0 = alloc_pairs(R.npairs, w);
+  const uint32_t fit = p0 >= R.cap ? 0u : min(w, R.cap - p0);
+  for (uint32_t j = 0; j < fit; j++)
+    put_pair(R, p0 + j, T, P, q1, idx >> 1, idx & 1u, ps.surv[sbase + j], sbase + j,
+             j == 0 ? uint8_t(fit) : uint8_t(0));
 }
 
 
@@ -1402,10 +1414,10 @@ void launch_exhaustive(const DevTargets& T, const DevPool& P, const RoundBuf& R,
     default: launch_exhaustive_k<4>(T, P, R, npairs, total, s); break;
   }
 }
-void launch_round_resolve(const RoundBuf& R, uint32_t npairs, const QCOut& q, const Lanes& L,
+void launch_round_resolve(const RoundBuf& R, uint32_t npairs, const QCOut& q, const Lanes& L, uint32_t max_spec,
                           cudaStream_t s) {
   if (!npairs) return;
-  k_round_resolve<<<grid_for(npairs, 256), 256, 0, s>>>(R, npairs, q, L);
+  k_round_resolve<<<grid_for(npairs, 256), 256, 0, s>>>(R, npairs, q, L, max_spec);
 }
 void launch_midcheck(const DevTargets& T, const DevPool& P, const uint32_t* surv,
                      const uint32_t* surv_target, uint32_t nsurv, uint8_t* pass, cudaStream_t s) {

@@ -44,7 +44,15 @@ struct Lanes {
   uint32_t* next;    // [2n] survivor index to try next; bit31 = resolved
   uint32_t* win;     // [2n] winning pool index or kNone
   uint16_t* windiff; // [2n] sdiff of the winner
+  uint8_t* spec;     // [2n] log2 of the lane's survivor window in the next round
 };
+
+// Survivor windows: a lane whose survivors keep failing ExhaustiveCheck
+// takes 1, 2, 4, ... of its next survivors (in enumeration order) into one
+// round, up to these caps; the first one that passes wins, as if they had
+// been tried one per round.
+constexpr uint32_t kMaxSpec1 = 6;  // length-1 pass: windows up to 64
+constexpr uint32_t kMaxSpec2 = 5;  // length-2 pass: windows up to 32 (the lane's slots)
 
 struct RoundBuf {
   PairRec* pairs;
@@ -52,6 +60,8 @@ struct RoundBuf {
   unsigned long long* nchunks;     // per pair (scan input)
   unsigned long long* cbase;       // exclusive prefix of nchunks
   uint32_t* rejected;              // per pair
+  uint8_t* wlen;                   // per pair: survivors in the window it heads (0: not a head)
+  uint32_t cap;                    // pair slots of the buffers
   uint32_t* npairs;                // device counter
   unsigned long long* counter;     // chunk dispenser
   unsigned long long* states;      // [2]: states of the reference's sweeps covered, states evaluated
@@ -104,7 +114,7 @@ void launch_pairs_from_survivors(const DevTargets& T, const DevPool& P, const QC
 // k = states per lane per dispatch: 1, 2, 4 or 8.
 void launch_exhaustive(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
                        unsigned long long total_chunks, int k, cudaStream_t s);
-void launch_round_resolve(const RoundBuf& R, uint32_t npairs, const QCOut& q, const Lanes& L,
+void launch_round_resolve(const RoundBuf& R, uint32_t npairs, const QCOut& q, const Lanes& L, uint32_t max_spec,
                           cudaStream_t s);
 void launch_midcheck(const DevTargets& T, const DevPool& P, const uint32_t* surv,
                      const uint32_t* surv_target, uint32_t nsurv, uint8_t* pass, cudaStream_t s);
