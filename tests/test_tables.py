@@ -99,19 +99,3 @@ def test_a_dependence_classes_against_oracle(tmp_path):
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.startswith("OK")
-
-
-def test_write_masks_against_oracle(tmp_path):
-    """No opcode changes a state field outside its sampled write mask (the
-    bit-sliced sweep re-initialises only the fields a pair can change): every
-    16-bit pair of fields swept over all values under the oracle's Exec."""
-    import subprocess
-    exe = tmp_path / "wmask_check"
-    srcs = [os.path.join(ROOT, "tests", "native", "wmask_check.cpp"),
-            os.path.join(ROOT, "z80-optimizer_b200", "csrc", "z80_tables.cpp"),
-            os.path.join(ROOT, "oracle", "z80_oracle_isa_cpu.cpp"),
-            os.path.join(ROOT, "oracle", "z80_oracle_search.cpp")]
-    subprocess.run(["g++", "-O2", "-std=c++17", "-o", str(exe)] + srcs + ["-lpthread"], check=True)
-    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
-    assert r.returncode == 0, r.stdout + r.stderr
-    assert r.stdout.startswith("OK")

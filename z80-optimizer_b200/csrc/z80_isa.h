@@ -102,11 +102,6 @@ struct OpInfo {
   uint16_t writes;  // pruner.go:66-236 (opWrites; memory ops report 0)
 };
 
-// State fields an instruction can change, as a bit set (A F B C D E H L SP
-// M); the per-opcode table is sampled from the step function (op_wmask).
-enum : uint16_t { kWA = 1, kWF = 2, kWB = 4, kWC = 8, kWD = 16, kWE = 32, kWH = 64, kWL = 128, kWSP = 256,
-                  kWM = 512 };
-
 inline constexpr uint16_t insn_op(uint32_t w) { return uint16_t(w & 0xFFFFu); }
 inline constexpr uint16_t insn_imm(uint32_t w) { return uint16_t(w >> 16); }
 inline constexpr uint32_t insn(uint16_t op, uint16_t imm = 0) { return uint32_t(op) | (uint32_t(imm) << 16); }

@@ -239,65 +239,6 @@ const uint8_t* op_aclass() {
   return cls;
 }
 
-namespace {
-// Fields one opcode changes: the union over sampled input states (all-zero,
-// all-one and random ones, with every value of A, the low byte of each pair
-// and M at least once) and immediates (every 8-bit value; for 16-bit ones
-// 0, FFFF and sampled values) of the fields whose output differs from input.
-uint16_t sample_wmask(uint16_t op) {
-  uint64_t x = 0xD1B54A32D192ED03ull ^ (uint64_t(op) << 32);
-  auto rnd = [&]() {
-    x += 0x9E3779B97F4A7C15ull;
-    uint64_t z = x;
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    return z ^ (z >> 31);
-  };
-  const int kind = op_table()[op].imm;
-  uint16_t m = 0;
-  for (int k = 0; k < 4096; k++) {
-    const uint64_t r = k == 0 ? 0 : (k == 1 ? ~0ull : rnd());
-    const uint64_t r2 = k == 0 ? 0 : (k == 1 ? ~0ull : rnd());
-    z80b::Z80S s{uint32_t(r & 0xFF), uint32_t((r >> 8) & 0xFF), uint32_t((r >> 16) & 0xFF),
-                 uint32_t((r >> 24) & 0xFF), uint32_t((r >> 32) & 0xFF), uint32_t((r >> 40) & 0xFF),
-                 uint32_t((r >> 48) & 0xFF), uint32_t((r >> 56) & 0xFF), uint32_t(r2 & 0xFFFF),
-                 uint32_t((r2 >> 16) & 0xFF)};
-    if (k >= 2 && k < 258) {  // every byte value in A, C, E, L, M and the low byte of SP
-      const uint32_t v = uint32_t(k - 2);
-      s.a = v;
-      s.c = v;
-      s.e = v;
-      s.l = v;
-      s.m = v;
-      s.sp = (s.sp & 0xFF00u) | v;
-    }
-    const uint16_t imm = kind == 0 ? 0 : kind == 1 ? uint16_t(k & 0xFF) : (k < 256 ? uint16_t(k * 257) : uint16_t(r2 >> 32));
-    const z80b::Z80S in = s;
-    z80b::z_step(s, op, imm);
-    if (s.a != in.a) m |= kWA;
-    if (s.f != in.f) m |= kWF;
-    if (s.b != in.b) m |= kWB;
-    if (s.c != in.c) m |= kWC;
-    if (s.d != in.d) m |= kWD;
-    if (s.e != in.e) m |= kWE;
-    if (s.h != in.h) m |= kWH;
-    if (s.l != in.l) m |= kWL;
-    if (s.sp != in.sp) m |= kWSP;
-    if (s.m != in.m) m |= kWM;
-  }
-  return m;
-}
-}  // namespace
-
-const uint16_t* op_wmask() {
-  static uint16_t wm[kNumOps];
-  static std::once_flag once;
-  std::call_once(once, [] {
-    for (int op = 0; op < kNumOps; op++) wm[op] = sample_wmask(uint16_t(op));
-  });
-  return wm;
-}
-
 uint32_t seq_aflow(const uint32_t* s, int n) {
   const uint8_t* c = op_aclass();
   bool a_is_x = true;

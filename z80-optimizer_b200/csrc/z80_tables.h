@@ -26,10 +26,6 @@ const uint8_t* op_aclass();               // kNumOps entries
 // Folds the classes over a sequence: 0 when some output depends on the input
 // A; else 1 (A is overwritten) or 3 (A passes through to the output).
 uint32_t seq_aflow(const uint32_t* s, int n);
-// State fields an instruction can change (kWA..kWM bits), found by running
-// the step function on sampled states and immediates; a field outside the
-// mask is left unchanged by the instruction.
-const uint16_t* op_wmask();               // kNumOps entries
 const char* op_mnemonic(uint16_t op);     // "ADD A, n" style with placeholders
 const uint8_t* op_encoding(uint16_t op, int* n);
 std::string disassemble(uint32_t insn);   // catalog.go:73-127
