@@ -184,7 +184,7 @@ int z80b_fetch_rules(z80b_ctx* ctx, z80b_rule* out, uint64_t cap, uint64_t* n_ru
  * component, a latency path that must not pay for an allocation or for the
  * synchronization cudaFree implies, a plugin host that forbids allocator
  * calls.  It needs no context and allocates nothing (device or host heap):
- * its device scratch is a fixed 288 KiB array inside the library that every
+ * its device scratch is a fixed 316 KiB array inside the library that every
  * GPU loading the library keeps until the process exits.
  *
  * ExhaustiveCheck[Masked] (pkg/search/verifier.go:159-171,642-654) of n

@@ -136,7 +136,7 @@ struct z80b_ctx {
   // pipeline scratch
   DBuf cnt_f, cnt_m, cnt_all, base, meta, surv, sdiff, checks;
   DBuf next, win, windiff, spec, spec2, wlen;
-  DBuf pairs, pair_src, nchunks, cbase, rejected, npairs, counter, states;
+  DBuf pairs, pair_src, nchunks, cbase, nchunks_x, cbase_x, rejected, npairs, counter, states;
   DBuf rcnt, rbase, rules, checked, surv_target, midpass, flag;
   DBuf cub_tmp;
   DBuf hits, nhits, fpq;
@@ -505,6 +505,28 @@ struct Reporter {
              bool last);
 };
 
+// ExhaustiveCheck of the np pairs of a round: chunk prefixes of both pair
+// classes, then the sweep kernel of each class that has chunks.
+int sweep_round(z80b_ctx* ctx, const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t np) {
+  cudaStream_t s = ctx->stream;
+  CKR(scan(ctx, R.nchunks, R.cbase, np));
+  CKR(scan(ctx, R.nchunks_x, R.cbase_x, np));
+  unsigned long long last[4] = {0, 0, 0, 0};
+  CK(cudaMemcpyAsync(&last[0], R.cbase + (np - 1), 8, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&last[1], R.nchunks + (np - 1), 8, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&last[2], R.cbase_x + (np - 1), 8, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&last[3], R.nchunks_x + (np - 1), 8, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  CK(cudaMemsetAsync(R.counter, 0, 16, s));
+  trace("sweep: %u pairs, %llu + %llu chunks", np, last[0] + last[1], last[2] + last[3]);
+  int ke = kbegin(ctx, 1);
+  const int nl = launch_exhaustive(T, P, R, np, last[0] + last[1], last[2] + last[3], ctx->exh_k, s);
+  kend(ctx, ke);
+  CKR(check_launch(ctx, "exhaustive"));
+  if (nl > 1) ctx->launches += uint32_t(nl - 1);
+  return Z80B_OK;
+}
+
 // Runs the pipeline on device-resident targets.  Rules stay in ctx->rules
 // (DevRule), count in *nr.
 int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_stats* st, uint64_t* nr) {
@@ -536,7 +558,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
   CK(ctx->checked.ensure(8));
   CK(ctx->states.ensure(16));
   CK(ctx->npairs.ensure(4));
-  CK(ctx->counter.ensure(8));
+  CK(ctx->counter.ensure(16));
   CK(cudaMemsetAsync(ctx->checks.p, 0, 8, s));
   CK(cudaMemsetAsync(ctx->checked.p, 0, 8, s));
   CK(cudaMemsetAsync(ctx->states.p, 0, 16, s));
@@ -602,6 +624,8 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
     CK(ctx->pair_src.ensure(4 * cap));
     CK(ctx->nchunks.ensure(8 * cap));
     CK(ctx->cbase.ensure(8 * cap));
+    CK(ctx->nchunks_x.ensure(8 * cap));
+    CK(ctx->cbase_x.ensure(8 * cap));
     CK(ctx->rejected.ensure(4 * cap));
     CK(ctx->wlen.ensure(cap));
     CK(ctx->spec.ensure(2ull * n));
@@ -613,6 +637,8 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
     R.pair_src = ctx->pair_src.as<uint32_t>();
     R.nchunks = ctx->nchunks.as<unsigned long long>();
     R.cbase = ctx->cbase.as<unsigned long long>();
+    R.nchunks_x = ctx->nchunks_x.as<unsigned long long>();
+    R.cbase_x = ctx->cbase_x.as<unsigned long long>();
     R.rejected = ctx->rejected.as<uint32_t>();
     R.wlen = ctx->wlen.as<uint8_t>();
     R.cap = uint32_t(cap);
@@ -632,17 +658,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
         if (np == 0) break;
         rounds++;
         exh_pairs += np;
-        CKR(scan(ctx, R.nchunks, R.cbase, np));
-        unsigned long long lastb = 0, lastn = 0;
-        CK(cudaMemcpyAsync(&lastb, R.cbase + (np - 1), 8, cudaMemcpyDeviceToHost, s));
-        CK(cudaMemcpyAsync(&lastn, R.nchunks + (np - 1), 8, cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        CK(cudaMemsetAsync(R.counter, 0, 8, s));
-        trace("round %u: %llu chunks", rounds, lastb + lastn);
-        int ke = kbegin(ctx, 1);
-        launch_exhaustive(T, P, R, np, lastb + lastn, ctx->exh_k, s);
-        kend(ctx, ke);
-        CKR(check_launch(ctx, "exhaustive"));
+        CKR(sweep_round(ctx, T, P, R, np));
         launch_round_resolve(R, np, q, L, kMaxSpec1, s);
         CKR(check_launch(ctx, "round_resolve"));
         if (opts.rep) CKR(opts.rep->update(ctx, n, L, Lanes{nullptr, nullptr, nullptr}, opts.max_cand, false, false));
@@ -709,16 +725,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
         }
         rounds++;
         exh_pairs += np;
-        CKR(scan(ctx, R.nchunks, R.cbase, np));
-        unsigned long long lastb = 0, lastn = 0;
-        CK(cudaMemcpyAsync(&lastb, R.cbase + (np - 1), 8, cudaMemcpyDeviceToHost, s));
-        CK(cudaMemcpyAsync(&lastn, R.nchunks + (np - 1), 8, cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        CK(cudaMemsetAsync(R.counter, 0, 8, s));
-        int ke = kbegin(ctx, 1);
-        launch_exhaustive(T, P2, R, np, lastb + lastn, ctx->exh_k, s);
-        kend(ctx, ke);
-        CKR(check_launch(ctx, "exhaustive"));
+        CKR(sweep_round(ctx, T, P2, R, np));
         launch_round_resolve(R, np, q2, L2, kMaxSpec2, s);
         CKR(check_launch(ctx, "round_resolve"));
         if (opts.rep) CKR(opts.rep->update(ctx, n, L, L2, opts.max_cand, true, false));
@@ -750,11 +757,15 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
     CK(ctx->pair_src.ensure(4ull * std::max<uint32_t>(S, 1)));
     CK(ctx->nchunks.ensure(8ull * std::max<uint32_t>(S, 1)));
     CK(ctx->cbase.ensure(8ull * std::max<uint32_t>(S, 1)));
+    CK(ctx->nchunks_x.ensure(8ull * std::max<uint32_t>(S, 1)));
+    CK(ctx->cbase_x.ensure(8ull * std::max<uint32_t>(S, 1)));
     CK(ctx->rejected.ensure(4ull * std::max<uint32_t>(S, 1)));
     R.pairs = ctx->pairs.as<PairRec>();
     R.pair_src = ctx->pair_src.as<uint32_t>();
     R.nchunks = ctx->nchunks.as<unsigned long long>();
     R.cbase = ctx->cbase.as<unsigned long long>();
+    R.nchunks_x = ctx->nchunks_x.as<unsigned long long>();
+    R.cbase_x = ctx->cbase_x.as<unsigned long long>();
     R.rejected = ctx->rejected.as<uint32_t>();
     R.npairs = ctx->npairs.as<uint32_t>();
     R.counter = ctx->counter.as<unsigned long long>();
@@ -775,16 +786,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
       CK(cudaMemsetAsync(ctx->flag.p, 0, 4ull * S, s));
       if (np) {
         rounds = 1;
-        CKR(scan(ctx, R.nchunks, R.cbase, np));
-        unsigned long long lastb = 0, lastn = 0;
-        CK(cudaMemcpyAsync(&lastb, R.cbase + (np - 1), 8, cudaMemcpyDeviceToHost, s));
-        CK(cudaMemcpyAsync(&lastn, R.nchunks + (np - 1), 8, cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        CK(cudaMemsetAsync(R.counter, 0, 8, s));
-        int ke = kbegin(ctx, 1);
-        launch_exhaustive(T, P, R, np, lastb + lastn, ctx->exh_k, s);
-        kend(ctx, ke);
-        CKR(check_launch(ctx, "exhaustive"));
+        CKR(sweep_round(ctx, T, P, R, np));
         launch_rule_count_all(R, np, ctx->flag.as<uint32_t>(), s);
         CKR(check_launch(ctx, "rule_count_all"));
       }
@@ -1240,8 +1242,8 @@ int z80b_verify_pairs(z80b_ctx* ctx, const uint32_t* tgt, const uint8_t* tlens, 
     P.n = n;
     P.stride = stride;
     std::vector<PairRec> pr(n);
-    std::vector<unsigned long long> nch(n), cb(n);
-    unsigned long long tot = 0;
+    std::vector<unsigned long long> cb(n), cbx(n);
+    unsigned long long tot = 0, totx = 0;  // chunks of the bit-sliced / A-independent pairs
     for (uint32_t i = 0; i < n; i++) {
       uint16_t rd = uint16_t(seq_reads(tgt + (size_t)i * stride, tlens[i]) | seq_reads(cand + (size_t)i * stride, clens[i]));
       Sweep w = sweep_for(rd);
@@ -1260,27 +1262,33 @@ int z80b_verify_pairs(z80b_ctx* ctx, const uint32_t* tgt, const uint8_t* tlens, 
         units = (pr[i].nblocks + 127) / 128;
       }
       unsigned long long c = (units + ctx->chunk_blocks - 1) / uint64_t(ctx->chunk_blocks);
-      nch[i] = c > (1ull << 20) ? (1ull << 20) : c;
+      if (c > (1ull << 20)) c = 1ull << 20;
       cb[i] = tot;
-      tot += nch[i];
+      cbx[i] = totx;
+      if (pr[i].keepR & 0x40) totx += c;
+      else tot += c;
     }
     CK(ctx->pairs.ensure(sizeof(PairRec) * n));
     CK(ctx->cbase.ensure(8ull * n));
+    CK(ctx->cbase_x.ensure(8ull * n));
     CK(ctx->rejected.ensure(4ull * n));
-    CK(ctx->counter.ensure(8));
+    CK(ctx->counter.ensure(16));
     CK(ctx->states.ensure(16));
     CK(cudaMemcpyAsync(ctx->pairs.p, pr.data(), sizeof(PairRec) * n, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(ctx->cbase.p, cb.data(), 8ull * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(ctx->cbase_x.p, cbx.data(), 8ull * n, cudaMemcpyHostToDevice, s));
     CK(cudaMemsetAsync(ctx->rejected.p, 0, 4ull * n, s));
-    CK(cudaMemsetAsync(ctx->counter.p, 0, 8, s));
+    CK(cudaMemsetAsync(ctx->counter.p, 0, 16, s));
     RoundBuf R{};
     R.pairs = ctx->pairs.as<PairRec>();
     R.cbase = ctx->cbase.as<unsigned long long>();
+    R.cbase_x = ctx->cbase_x.as<unsigned long long>();
     R.rejected = ctx->rejected.as<uint32_t>();
     R.counter = ctx->counter.as<unsigned long long>();
     R.states = ctx->states.as<unsigned long long>();
-    launch_exhaustive(T, P, R, n, tot, ctx->exh_k, s);
+    const int nl = launch_exhaustive(T, P, R, n, tot, totx, ctx->exh_k, s);
     CKR(check_launch(ctx, "exhaustive"));
+    if (nl > 1) ctx->launches += uint32_t(nl - 1);
     std::vector<uint32_t> rej(n);
     CK(cudaMemcpyAsync(rej.data(), ctx->rejected.p, 4ull * n, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));

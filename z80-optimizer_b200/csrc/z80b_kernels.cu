@@ -147,6 +147,14 @@ constexpr unsigned long long kMaxChunks = 1ull << 20;
 constexpr int kChunksPerWarp = 16;
 // Work chunks of a sweep: cb A-blocks each (cb is the tuning option), at
 // most kMaxChunks per pair.
+__device__ __forceinline__ unsigned long long chunks_for(unsigned long long nb, uint32_t cb);
+// Chunks of pair p in the numbering of its class (zero in the other one).
+__device__ __forceinline__ void set_chunks(const RoundBuf& R, uint32_t p, const PairRec& pr) {
+  const unsigned long long c = chunks_for(pair_units(pr.nblocks, pr.keepR), R.chunk_blocks);
+  const bool xind = (pr.keepR & kXIndep) != 0;
+  R.nchunks[p] = xind ? 0ull : c;
+  R.nchunks_x[p] = xind ? c : 0ull;
+}
 __device__ __forceinline__ unsigned long long chunks_for(unsigned long long nb, uint32_t cb) {
   unsigned long long c = (nb + cb - 1) / cb;
   return c > kMaxChunks ? kMaxChunks : c;
@@ -448,7 +456,7 @@ __device__ __forceinline__ void put_pair(const RoundBuf& R, uint32_t p, const De
   if (pair_xindep(T, t, P, c)) pr.keepR |= uint8_t(kXIndep);
   R.pairs[p] = pr;
   R.pair_src[p] = src;
-  R.nchunks[p] = chunks_for(pair_units(pr.nblocks, pr.keepR), R.chunk_blocks);
+  set_chunks(R, p, pr);
   R.rejected[p] = 0;
   R.wlen[p] = wlen;
 }
@@ -512,7 +520,7 @@ __global__ void k_pairs_from_survivors(DevTargets T, DevPool P, QCOut q, const u
     uint32_t p = base + __popc(b & lanemask_lt());
     R.pairs[p] = pr;
     R.pair_src[p] = i;
-    R.nchunks[p] = chunks_for(pair_units(pr.nblocks, pr.keepR), R.chunk_blocks);
+    set_chunks(R, p, pr);
     R.rejected[p] = 0;
   }
 }
@@ -717,10 +725,15 @@ __device__ __noinline__ bool xindep_unit(unsigned long long first, unsigned long
   return bad;
 }
 
-template <int K>
+// One kernel per pair class: XI = false runs the bit-sliced pairs, XI = true
+// the A-independent ones (K states per lane per dispatch); each draws chunks
+// from its own numbering and dispenser.  Kept apart so that neither path's
+// registers weigh on the other.
+template <int K, bool XI>
 __global__ void __launch_bounds__(kBlock, 1) k_exhaustive(DevTargets T, DevPool P, RoundBuf R, uint32_t npairs,
                                                        unsigned long long total) {
   static_assert(K == 1 || K == 2 || K == 4 || K == 8, "K divides 8");
+  const unsigned long long* __restrict__ cbase = XI ? R.cbase_x : R.cbase;
   const unsigned lane = lane_id();
   unsigned long long my_states = 0, my_eval = 0;
   // At most kChunksPerWarp chunks per warp, then the block retires: the grid
@@ -728,14 +741,14 @@ __global__ void __launch_bounds__(kBlock, 1) k_exhaustive(DevTargets T, DevPool 
   // priority) get SMs as soon as blocks of a long sweep retire.
   for (int taken = 0; taken < kChunksPerWarp; taken++) {
     unsigned long long k = 0;
-    if (lane == 0) k = atomicAdd(R.counter, 1ull);
+    if (lane == 0) k = atomicAdd(R.counter + (XI ? 1 : 0), 1ull);
     k = __shfl_sync(kFull, k, 0);
     if (k >= total) break;
     // pair p: cbase[p] <= k < cbase[p + 1]
     uint32_t lo = 0, hi = npairs - 1;
     while (lo < hi) {
       uint32_t mid = (lo + hi + 1) >> 1;
-      if (R.cbase[mid] <= k) lo = mid;
+      if (cbase[mid] <= k) lo = mid;
       else hi = mid - 1;
     }
     const uint32_t p = lo;
@@ -744,11 +757,10 @@ __global__ void __launch_bounds__(kBlock, 1) k_exhaustive(DevTargets T, DevPool 
     if (__shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0))
       continue;
     const PairRec pr = R.pairs[p];
-    const bool xind = (pr.keepR & kXIndep) != 0;
     const unsigned long long nunits = pair_units(pr.nblocks, pr.keepR);
-    const unsigned long long nch = (p + 1 < npairs ? R.cbase[p + 1] : total) - R.cbase[p];
+    const unsigned long long nch = (p + 1 < npairs ? cbase[p + 1] : total) - cbase[p];
     const unsigned long long upc = (nunits + nch - 1) / nch;
-    const unsigned long long j = k - R.cbase[p];
+    const unsigned long long j = k - cbase[p];
     const unsigned long long u0 = j * upc;
     unsigned long long u1 = u0 + upc;
     if (u1 > nunits) u1 = nunits;
@@ -779,7 +791,7 @@ __global__ void __launch_bounds__(kBlock, 1) k_exhaustive(DevTargets T, DevPool 
                            ((pr.keepR & 16u) ? 0xFF0000u : 0u) | ((pr.keepR & 32u) ? 0xFF000000u : 0u);
 
     bool bad = false;
-    if (!xind) {
+    if constexpr (!XI) {
       // Unit = 4 A-blocks, bit-sliced (256 states of each block in 8 lanes).
       // The reference nests its loops as A, carry, first register, ...,
       // last register, SP (verifier.go:498-531,578-610); the block index
@@ -1382,15 +1394,16 @@ void launch_pairs_from_survivors(const DevTargets& T, const DevPool& P, const QC
   if (!nsurv) return;
   k_pairs_from_survivors<<<grid_for(nsurv, 256), 256, 0, s>>>(T, P, q, midpass, nsurv, surv_target, R);
 }
-template <int K>
+template <int K, bool XI>
 void launch_exhaustive_k(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
                          unsigned long long total, cudaStream_t s) {
-  // shared memory: the candidate's output planes, kBitsWords words per lane
-  constexpr int smem = kBlock * kBitsWords * 4;
+  // shared memory (bit-sliced class): the candidate's output planes,
+  // kBitsWords words per lane
+  constexpr int smem = XI ? 0 : kBlock * kBitsWords * 4;
   static int per_sm = 0;
   if (!per_sm) {
-    cudaFuncSetAttribute(k_exhaustive<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_exhaustive<K>, kBlock, smem);
+    if (smem) cudaFuncSetAttribute(k_exhaustive<K, XI>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_exhaustive<K, XI>, kBlock, smem);
     if (per_sm < 1) per_sm = 1;
   }
   // resident blocks, or more when the chunks exceed kChunksPerWarp per warp
@@ -1401,18 +1414,27 @@ void launch_exhaustive_k(const DevTargets& T, const DevPool& P, const RoundBuf& 
   const unsigned long long cover = (total + wpb * kChunksPerWarp - 1) / (wpb * kChunksPerWarp);
   if (grid < cover) grid = cover;
   if (grid > 0x7FFFFFFFull) grid = 0x7FFFFFFFull;
-  k_exhaustive<K><<<unsigned(grid), kBlock, smem, s>>>(T, P, R, npairs, total);
+  k_exhaustive<K, XI><<<unsigned(grid), kBlock, smem, s>>>(T, P, R, npairs, total);
 }
 
-void launch_exhaustive(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
-                       unsigned long long total, int k, cudaStream_t s) {
-  if (!npairs || !total) return;
-  switch (k) {
-    case 1: launch_exhaustive_k<1>(T, P, R, npairs, total, s); break;
-    case 2: launch_exhaustive_k<2>(T, P, R, npairs, total, s); break;
-    case 8: launch_exhaustive_k<8>(T, P, R, npairs, total, s); break;
-    default: launch_exhaustive_k<4>(T, P, R, npairs, total, s); break;
+int launch_exhaustive(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
+                      unsigned long long total_b, unsigned long long total_x, int k, cudaStream_t s) {
+  if (!npairs) return 0;
+  int n = 0;
+  if (total_b) {
+    launch_exhaustive_k<1, false>(T, P, R, npairs, total_b, s);
+    n++;
   }
+  if (total_x) {
+    switch (k) {
+      case 1: launch_exhaustive_k<1, true>(T, P, R, npairs, total_x, s); break;
+      case 2: launch_exhaustive_k<2, true>(T, P, R, npairs, total_x, s); break;
+      case 8: launch_exhaustive_k<8, true>(T, P, R, npairs, total_x, s); break;
+      default: launch_exhaustive_k<4, true>(T, P, R, npairs, total_x, s); break;
+    }
+    n++;
+  }
+  return n;
 }
 void launch_round_resolve(const RoundBuf& R, uint32_t npairs, const QCOut& q, const Lanes& L, uint32_t max_spec,
                           cudaStream_t s) {

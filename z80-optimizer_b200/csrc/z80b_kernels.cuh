@@ -57,13 +57,18 @@ constexpr uint32_t kMaxSpec2 = 5;  // length-2 pass: windows up to 32 (the lane'
 struct RoundBuf {
   PairRec* pairs;
   uint32_t* pair_src;              // index of the (target, kind) lane or survivor
-  unsigned long long* nchunks;     // per pair (scan input)
+  // Two sweep kernels share a round: one runs the bit-sliced pairs (outputs
+  // depend on A), the other the A-independent ones; each class has its own
+  // chunk numbering (pairs of the other class count zero chunks in it).
+  unsigned long long* nchunks;     // per pair (scan input), bit-sliced class
   unsigned long long* cbase;       // exclusive prefix of nchunks
+  unsigned long long* nchunks_x;   // per pair, A-independent class
+  unsigned long long* cbase_x;     // exclusive prefix of nchunks_x
   uint32_t* rejected;              // per pair
   uint8_t* wlen;                   // per pair: survivors in the window it heads (0: not a head)
   uint32_t cap;                    // pair slots of the buffers
   uint32_t* npairs;                // device counter
-  unsigned long long* counter;     // chunk dispenser
+  unsigned long long* counter;     // chunk dispensers: [0] bit-sliced class, [1] A-independent class
   unsigned long long* states;      // [2]: states of the reference's sweeps covered, states evaluated
   uint32_t chunk_blocks;           // A-blocks per work chunk
 };
@@ -112,8 +117,10 @@ void launch_pairs_from_survivors(const DevTargets& T, const DevPool& P, const QC
                                  const uint8_t* midpass, uint32_t nsurv, const uint32_t* surv_target,
                                  const RoundBuf& R, cudaStream_t s);
 // k = states per lane per dispatch: 1, 2, 4 or 8.
-void launch_exhaustive(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
-                       unsigned long long total_chunks, int k, cudaStream_t s);
+// Launches the sweep kernel of each class that has chunks (total_b
+// bit-sliced, total_x A-independent); returns the number of launches.
+int launch_exhaustive(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
+                      unsigned long long total_b, unsigned long long total_x, int k, cudaStream_t s);
 void launch_round_resolve(const RoundBuf& R, uint32_t npairs, const QCOut& q, const Lanes& L, uint32_t max_spec,
                           cudaStream_t s);
 void launch_midcheck(const DevTargets& T, const DevPool& P, const uint32_t* surv,

@@ -35,9 +35,10 @@ constexpr size_t kOffCLen = align256(kOffTLen + kMaxPairs);
 constexpr size_t kOffDead = align256(kOffCLen + kMaxPairs);
 constexpr size_t kOffPairs = align256(kOffDead + kMaxPairs);
 constexpr size_t kOffCbase = align256(kOffPairs + sizeof(PairRec) * kMaxPairs);
-constexpr size_t kOffRej = align256(kOffCbase + 8ull * kMaxPairs);
+constexpr size_t kOffCbaseX = align256(kOffCbase + 8ull * kMaxPairs);
+constexpr size_t kOffRej = align256(kOffCbaseX + 8ull * kMaxPairs);
 constexpr size_t kOffCounter = align256(kOffRej + 4ull * kMaxPairs);
-constexpr size_t kOffStates = kOffCounter + 8;
+constexpr size_t kOffStates = kOffCounter + 16;
 constexpr size_t kNoAllocBytes = align256(kOffStates + 16);
 static_assert(kNoAllocBytes <= 320 * 1024, "the scratch stays modest");
 
@@ -47,7 +48,7 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 std::mutex g_mu;
 uint32_t h_tgt[kStride * kMaxPairs], h_cand[kStride * kMaxPairs], h_rej[kMaxPairs];
 PairRec h_pairs[kMaxPairs];
-unsigned long long h_cbase[kMaxPairs];
+unsigned long long h_cbase[kMaxPairs], h_cbase_x[kMaxPairs];  // chunk prefixes: bit-sliced / A-independent pairs
 
 constexpr int kMaxDevices = 64;
 unsigned char* g_dev_ptr[kMaxDevices] = {};  // device address of the scratch on each device
@@ -86,7 +87,7 @@ extern "C" int z80b_exhaustive_noalloc(int device, const uint32_t* tgt, const ui
   // (pkg/search/verifier.go:159-171,428-476) and the chunk prefix.
   std::memset(h_tgt, 0, 4ull * kStride * n);
   std::memset(h_cand, 0, 4ull * kStride * n);
-  unsigned long long total = 0;
+  unsigned long long total = 0, total_x = 0;
   for (uint32_t i = 0; i < n; i++) {
     const uint32_t tl = tlens[i], cl = clens[i];
     if (tl < 1 || tl > kStride || tl > stride || cl < 1 || cl > 3 || cl > stride) return Z80B_EINVAL;
@@ -120,7 +121,9 @@ extern "C" int z80b_exhaustive_noalloc(int device, const uint32_t* tgt, const ui
     unsigned long long ch = (units + 31) / 32;
     if (ch > (1ull << 20)) ch = 1ull << 20;
     h_cbase[i] = total;
-    total += ch;
+    h_cbase_x[i] = total_x;
+    if (p.keepR & 0x40) total_x += ch;
+    else total += ch;
   }
   if (cudaSetDevice(device) != cudaSuccess) return Z80B_ECUDA;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -137,8 +140,9 @@ extern "C" int z80b_exhaustive_noalloc(int device, const uint32_t* tgt, const ui
             cudaMemcpyAsync(base + kOffCLen, clens, n, cudaMemcpyHostToDevice, s) == cudaSuccess &&
             cudaMemcpyAsync(base + kOffPairs, h_pairs, sizeof(PairRec) * n, cudaMemcpyHostToDevice, s) == cudaSuccess &&
             cudaMemcpyAsync(base + kOffCbase, h_cbase, 8ull * n, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+            cudaMemcpyAsync(base + kOffCbaseX, h_cbase_x, 8ull * n, cudaMemcpyHostToDevice, s) == cudaSuccess &&
             cudaMemsetAsync(base + kOffRej, 0, 4ull * n, s) == cudaSuccess &&
-            cudaMemsetAsync(base + kOffCounter, 0, 24, s) == cudaSuccess;
+            cudaMemsetAsync(base + kOffCounter, 0, 32, s) == cudaSuccess;
   if (dead) ok = ok && cudaMemcpyAsync(base + kOffDead, dead, n, cudaMemcpyHostToDevice, s) == cudaSuccess;
   else ok = ok && cudaMemsetAsync(base + kOffDead, 0, n, s) == cudaSuccess;
   if (!ok) return Z80B_ECUDA;
@@ -157,11 +161,12 @@ extern "C" int z80b_exhaustive_noalloc(int device, const uint32_t* tgt, const ui
   RoundBuf R{};
   R.pairs = reinterpret_cast<PairRec*>(base + kOffPairs);
   R.cbase = reinterpret_cast<unsigned long long*>(base + kOffCbase);
+  R.cbase_x = reinterpret_cast<unsigned long long*>(base + kOffCbaseX);
   R.rejected = reinterpret_cast<uint32_t*>(base + kOffRej);
   R.counter = reinterpret_cast<unsigned long long*>(base + kOffCounter);
   R.states = reinterpret_cast<unsigned long long*>(base + kOffStates);
   R.chunk_blocks = 32;
-  launch_exhaustive(T, P, R, n, total, 4, s);
+  launch_exhaustive(T, P, R, n, total, total_x, 4, s);
   if (cudaGetLastError() != cudaSuccess) return Z80B_ECUDA;
   if (cudaMemcpyAsync(h_rej, base + kOffRej, 4ull * n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess)
