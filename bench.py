@@ -457,16 +457,18 @@ def main():
     # states it skips
     achieved = evaluated / args.steps * per_state / (exh_ms / args.steps / 1e3) / 1e12 if exh_ms else 0.0
     peak = rl["sms"] * rl["int32_lanes_per_sm"] * sm_mhz * 1e6 / 1e12
-    # DRAM bytes per sweep launch: the measured bytes per ExhaustiveCheck pair
-    # of an ncu capture (profiles/exhaustive_c2_traffic.txt) times this run's
-    # pairs per launch; the kernel reads per-pair records and sequences only
+    # DRAM bytes per sweep round (its bit-sliced and A-independent kernels):
+    # the measured bytes per ExhaustiveCheck pair of an ncu capture
+    # (profiles/exhaustive_c2_traffic.txt) times this run's pairs per round;
+    # the kernels read per-pair records and sequences only
     traffic = None
     tf = os.path.join(ROOT, "profiles", "exhaustive_c2_traffic.txt")
     if os.path.exists(tf) and stats_last is not None and stats_last.rounds:
         for line in open(tf):
             if line.startswith("dram_bytes_per_pair:"):
                 traffic = float(line.split(":")[1]) * stats_last.exhaustive_pairs / stats_last.rounds
-    roofline = {"bound": "issue", "kernel": "k_exhaustive", "achieved": achieved, "peak": peak,
+    roofline = {"bound": "issue", "kernel": "k_exhaustive (bit-sliced and A-independent pair kernels of a round)",
+                "achieved": achieved, "peak": peak,
                 "unit": "Tops/s (INT32 lane-ops)", "frac": achieved / peak if peak else None,
                 "traffic": traffic,
                 "peak_source": f"{rl['sms']} SMs x {rl['int32_lanes_per_sm']} INT32 lanes x "
