@@ -695,8 +695,9 @@ __device__ __forceinline__ bool bits_unit(unsigned long long u, unsigned long lo
   return valid && zb_diff(z, sm, keepF, keepR) != 0u;
 }
 
-// One unit (128 A-blocks at A = 0, 1) of an A-independent sweep; kept out of
-// line so its registers do not weigh on the bit-sliced path.
+// One unit (128 A-blocks at A = 0, 1) of an A-independent sweep, for the
+// A-independent sweep kernel; kept out of line (that kernel compiles without
+// register spills at every K this way).
 template <int K>
 __device__ __noinline__ bool xindep_unit(unsigned long long first, unsigned long long nb, bool spw, bool reduced,
                                          int nx, int fw, const int* slotp, uint32_t pw, int tl, int cl,
