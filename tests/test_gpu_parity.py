@@ -276,6 +276,27 @@ def test_qc_index_equals_full_scan(ctx, O, all_hits):
         assert out[1][2] == checked
 
 
+def test_qc_index_follows_reloaded_pool(ctx):
+    """Loading another candidate pool replaces the QuickCheck index built for
+    the previous one: the bucket index and the full scan agree on each pool."""
+    targets = workloads.to_lists(workloads.c2_subset(1500, seed=23))
+    pool = z80b.pool8()
+    out = []
+    try:
+        for cands in (pool[:2000], pool[1000:]):
+            ctx.load_candidates(cands, 1)
+            got = []
+            for on in (1, 0):
+                ctx.set_option(z80b.OPT_QC_INDEX, on)
+                rules, st = ctx.search(targets, dead_flags=0xFF, mode=z80b.MODE_ALL)
+                got.append((rule_keys(rules), st.checks, st.qc_survivors))
+            assert got[0] == got[1]
+            out.append(got[0])
+    finally:
+        ctx.set_option(z80b.OPT_QC_INDEX, 1)
+    assert out[0] != out[1]
+
+
 @pytest.mark.parametrize("lane_states,chunk", [(1, 8), (2, 32), (4, 128), (8, 512), (4, 1)])
 def test_tuning_options_keep_parity(ctx, O, lane_states, chunk):
     targets = workloads.to_lists(workloads.c2_subset(2500, seed=12))

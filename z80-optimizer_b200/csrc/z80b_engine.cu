@@ -227,6 +227,7 @@ int fetch(z80b_ctx* ctx, T* host, const T* dev, size_t n = 1) {
 int build_pool(z80b_ctx* ctx, PoolBufs& P, const uint32_t* insn, uint32_t n, uint32_t len,
                const uint8_t* lens, bool with_mid) {
   P.loaded = false;
+  P.qstate = 0;  // a QuickCheck index of the previous contents is stale
   P.n = n;
   P.len = len;
   P.host_insn.assign(insn, insn + (size_t)n * len);
