@@ -1,0 +1,106 @@
+"""Rule export formats: `z80opt export` (result.WriteGoCode text and the
+generated peephole table package) and the JSON reader and peephole table
+functions of the C++ host API.  No device is needed."""
+import json
+import os
+import subprocess
+
+from conftest import ROOT
+
+EXE = os.path.join(ROOT, "z80-optimizer_b200", "_build", "z80opt")
+
+RULES = [
+    {"source_asm": "SUB A : LD A, 00h", "replacement_asm": "SUB A", "source_bytes": 3,
+     "replacement_bytes": 1, "bytes_saved": 2, "cycles_saved": 7},
+    {"source_asm": "OR A : AND A", "replacement_asm": "AND A", "source_bytes": 2,
+     "replacement_bytes": 1, "bytes_saved": 1, "cycles_saved": 4, "dead_flags": "10",
+     "dead_flag_desc": "H"},
+    {"source_asm": "LD B, 0A5h : LD C, 0FFh", "replacement_asm": "LD C, 0FFh : LD B, 0A5h",
+     "source_bytes": 4, "replacement_bytes": 4, "bytes_saved": 0, "cycles_saved": 0, "dead_flags": "FF",
+     "dead_flag_desc": "all"},
+]
+
+DESC = {0x10: "H", 0xFF: "all"}
+
+
+def expected_go(rules):
+    """output.go:95-125's text for these rules, written out independently."""
+    out = ["// Code generated by z80opt. DO NOT EDIT.", "", "package optimizer", "",
+           "// Z80OptRules contains peephole optimization rules discovered by the superoptimizer.",
+           "var Z80OptRules = []PeepholeRule{"]
+    for r in rules:
+        dead = int(r.get("dead_flags", "0"), 16)
+        head = f"\t// {r['source_asm']} -> {r['replacement_asm']} (-{r['bytes_saved']} bytes, -{r['cycles_saved']} cycles)"
+        out.append(head + (f" [dead: {DESC[dead]}]" if dead else ""))
+        out.append("\t{")
+        q = lambda asm: ", ".join(json.dumps(x) for x in asm.split(" : "))
+        out.append(f"\t\tMatch: []string{{{q(r['source_asm'])}}},")
+        out.append(f"\t\tReplace: []string{{{q(r['replacement_asm'])}}},")
+        if dead:
+            out.append(f"\t\tDeadFlags: 0x{dead:02X}, // {DESC[dead]}")
+        out.append("\t},")
+    out.append("}")
+    return "\n".join(out) + "\n"
+
+
+def run(*args):
+    return subprocess.run([EXE, *args], capture_output=True, text=True, timeout=60)
+
+
+def test_export_go_code(tmp_path):
+    f = tmp_path / "rules.json"
+    f.write_text(json.dumps(RULES, indent=2))
+    r = run("export", str(f))
+    assert r.returncode == 0, r.stderr
+    assert r.stdout == expected_go(RULES)
+    out = tmp_path / "rules.go"
+    r = run("export", str(f), "-f", "go", "-o", str(out))
+    assert r.returncode == 0 and out.read_text() == expected_go(RULES)
+
+
+def test_export_peephole_table(tmp_path):
+    f = tmp_path / "top.json"
+    f.write_text(json.dumps(RULES))
+    r = run("export", str(f), "-f", "peephole", "--var", "Top3")
+    assert r.returncode == 0, r.stderr
+    lines = r.stdout.splitlines()
+    assert lines[0] == "// Code generated from top.json. DO NOT EDIT."
+    assert lines[1] == "package peephole"
+    body = lines[lines.index("var Top3 = map[string]Rule{") + 1:]
+    body = body[:body.index("}")]
+    assert body == [f"\t{json.dumps(x['source_asm'])}: {{{json.dumps(x['replacement_asm'])}, "
+                    f"{x['cycles_saved']}, {x['bytes_saved']}}}," for x in RULES]
+    assert "func Lookup(source string) *Rule {" in lines
+    assert "func LoadRules(path string) (map[string]Rule, error) {" in lines
+
+
+def test_export_rejects_bad_input(tmp_path):
+    bad = tmp_path / "bad.json"
+    bad.write_text('{"source_asm": "NOP"}')
+    r = run("export", str(bad))
+    assert r.returncode == 1 and "not an array" in r.stderr
+    unparsable = tmp_path / "u.json"
+    unparsable.write_text('[{"source_asm": "FROB A", "replacement_asm": "NOP"}]')
+    r = run("export", str(unparsable))
+    assert r.returncode == 1 and "cannot parse source assembly" in r.stderr
+    good = tmp_path / "g.json"
+    good.write_text(json.dumps(RULES))
+    r = run("export", str(good), "-f", "yaml")
+    assert r.returncode == 1 and "unknown format: yaml" in r.stderr
+
+
+def test_json_reader_and_peephole_api(tmp_path):
+    """ReadJSON follows encoding/json on rule files (case-insensitive keys,
+    unknown keys skipped, null values, escapes, integers only), LoadRules
+    keeps the last entry of a source, Lookup finds entries."""
+    exe = tmp_path / "export_check"
+    build = os.path.join(ROOT, "z80-optimizer_b200", "_build")
+    subprocess.run(["g++", "-O1", "-std=c++17", "-o", str(exe),
+                    os.path.join(ROOT, "tests", "native", "export_check.cpp"),
+                    os.path.join(ROOT, "z80-optimizer_b200", "csrc", "host", "search_api.cpp"),
+                    "-I" + os.path.join(ROOT, "z80-optimizer_b200", "csrc", "host"),
+                    "-I" + os.path.join(ROOT, "include"), "-L" + build, "-lz80b200",
+                    "-Wl,-rpath," + build, "-lpthread"], check=True)
+    r = subprocess.run([str(exe), str(tmp_path)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.startswith("OK")

@@ -2,9 +2,15 @@
 #include "search_api.h"
 
 #include <algorithm>
+#include <cctype>
+#include <cerrno>
+#include <climits>
+#include <cmath>
 #include <cstring>
+#include <fstream>
 #include <mutex>
 #include <random>
+#include <sstream>
 
 namespace z80opt {
 
@@ -21,6 +27,289 @@ z80b_ctx* g_ctx = nullptr;
 
 void check(int st, const char* what) {
   if (st != Z80B_OK) raise(st, what);
+}
+
+// A JSON value, as much of JSON as rule files need (RFC 8259 grammar).
+struct JVal {
+  enum Kind { kNull, kBool, kNum, kStr, kArr, kObj } k = kNull;
+  bool b = false;
+  double num = 0;
+  bool integral = false;  // a number without fraction or exponent that fits in long long
+  long long i = 0;
+  std::string s;
+  std::vector<JVal> arr;
+  std::vector<std::pair<std::string, JVal>> obj;
+};
+
+class JParser {
+ public:
+  explicit JParser(const std::string& t) : t_(t) {}
+  JVal parse() {
+    JVal v = value(0);
+    ws();
+    if (p_ != t_.size()) fail("data after the top-level value");
+    return v;
+  }
+
+ private:
+  const std::string& t_;
+  size_t p_ = 0;
+
+  [[noreturn]] void fail(const char* what) const {
+    throw Error(Z80B_EINVAL, std::string("ReadJSON: ") + what + " at byte " + std::to_string(p_));
+  }
+  bool at(char c) const { return p_ < t_.size() && t_[p_] == c; }
+  void ws() {
+    while (p_ < t_.size() && (t_[p_] == ' ' || t_[p_] == '\t' || t_[p_] == '\n' || t_[p_] == '\r')) p_++;
+  }
+  bool word(const char* w) {
+    const size_t n = std::strlen(w);
+    if (t_.compare(p_, n, w) != 0) return false;
+    p_ += n;
+    return true;
+  }
+  JVal value(int depth) {
+    if (depth > 256) fail("nesting too deep");
+    ws();
+    if (p_ >= t_.size()) fail("unexpected end of input");
+    JVal v;
+    const char c = t_[p_];
+    if (c == '{') {
+      p_++;
+      v.k = JVal::kObj;
+      ws();
+      if (at('}')) {
+        p_++;
+        return v;
+      }
+      for (;;) {
+        ws();
+        if (!at('"')) fail("expected an object key");
+        std::string key = str();
+        ws();
+        if (!at(':')) fail("expected ':'");
+        p_++;
+        v.obj.emplace_back(std::move(key), value(depth + 1));
+        ws();
+        if (at(',')) {
+          p_++;
+          continue;
+        }
+        if (at('}')) {
+          p_++;
+          return v;
+        }
+        fail("expected ',' or '}'");
+      }
+    }
+    if (c == '[') {
+      p_++;
+      v.k = JVal::kArr;
+      ws();
+      if (at(']')) {
+        p_++;
+        return v;
+      }
+      for (;;) {
+        v.arr.push_back(value(depth + 1));
+        ws();
+        if (at(',')) {
+          p_++;
+          continue;
+        }
+        if (at(']')) {
+          p_++;
+          return v;
+        }
+        fail("expected ',' or ']'");
+      }
+    }
+    if (c == '"') {
+      v.k = JVal::kStr;
+      v.s = str();
+      return v;
+    }
+    if (word("true")) {
+      v.k = JVal::kBool;
+      v.b = true;
+      return v;
+    }
+    if (word("false")) {
+      v.k = JVal::kBool;
+      return v;
+    }
+    if (word("null")) return v;
+    return number();
+  }
+  unsigned hex4() {
+    if (p_ + 4 > t_.size()) fail("short \\u escape");
+    unsigned v = 0;
+    for (int k = 0; k < 4; k++) {
+      const char h = t_[p_++];
+      v <<= 4;
+      if (h >= '0' && h <= '9') v |= unsigned(h - '0');
+      else if (h >= 'a' && h <= 'f') v |= unsigned(h - 'a' + 10);
+      else if (h >= 'A' && h <= 'F') v |= unsigned(h - 'A' + 10);
+      else fail("bad \\u escape");
+    }
+    return v;
+  }
+  static void utf8(std::string& o, unsigned cp) {
+    if (cp < 0x80) {
+      o += char(cp);
+    } else if (cp < 0x800) {
+      o += char(0xC0 | (cp >> 6));
+      o += char(0x80 | (cp & 0x3F));
+    } else if (cp < 0x10000) {
+      o += char(0xE0 | (cp >> 12));
+      o += char(0x80 | ((cp >> 6) & 0x3F));
+      o += char(0x80 | (cp & 0x3F));
+    } else {
+      o += char(0xF0 | (cp >> 18));
+      o += char(0x80 | ((cp >> 12) & 0x3F));
+      o += char(0x80 | ((cp >> 6) & 0x3F));
+      o += char(0x80 | (cp & 0x3F));
+    }
+  }
+  std::string str() {
+    p_++;  // opening quote
+    std::string out;
+    while (p_ < t_.size()) {
+      const char c = t_[p_++];
+      if (c == '"') return out;
+      if (static_cast<unsigned char>(c) < 0x20) fail("control character in a string");
+      if (c != '\\') {
+        out += c;
+        continue;
+      }
+      if (p_ >= t_.size()) break;
+      const char e = t_[p_++];
+      switch (e) {
+        case '"': out += '"'; break;
+        case '\\': out += '\\'; break;
+        case '/': out += '/'; break;
+        case 'b': out += '\b'; break;
+        case 'f': out += '\f'; break;
+        case 'n': out += '\n'; break;
+        case 'r': out += '\r'; break;
+        case 't': out += '\t'; break;
+        case 'u': {
+          unsigned cp = hex4();
+          if (cp >= 0xD800 && cp < 0xDC00) {  // a surrogate pair, else U+FFFD
+            const size_t save = p_;
+            if (word("\\u")) {
+              const unsigned lo = hex4();
+              if (lo >= 0xDC00 && lo < 0xE000) {
+                cp = 0x10000 + ((cp - 0xD800) << 10) + (lo - 0xDC00);
+              } else {
+                cp = 0xFFFD;
+                p_ = save;
+              }
+            } else {
+              cp = 0xFFFD;
+            }
+          } else if (cp >= 0xDC00 && cp < 0xE000) {
+            cp = 0xFFFD;
+          }
+          utf8(out, cp);
+          break;
+        }
+        default: fail("bad escape in a string");
+      }
+    }
+    fail("unterminated string");
+  }
+  JVal number() {
+    const size_t b = p_;
+    bool integral = true;
+    if (at('-')) p_++;
+    if (at('0')) {
+      p_++;
+    } else if (p_ < t_.size() && t_[p_] >= '1' && t_[p_] <= '9') {
+      while (p_ < t_.size() && std::isdigit(static_cast<unsigned char>(t_[p_]))) p_++;
+    } else {
+      fail("invalid value");
+    }
+    if (at('.')) {
+      integral = false;
+      p_++;
+      if (!(p_ < t_.size() && std::isdigit(static_cast<unsigned char>(t_[p_])))) fail("bad number");
+      while (p_ < t_.size() && std::isdigit(static_cast<unsigned char>(t_[p_]))) p_++;
+    }
+    if (at('e') || at('E')) {
+      integral = false;
+      p_++;
+      if (at('+') || at('-')) p_++;
+      if (!(p_ < t_.size() && std::isdigit(static_cast<unsigned char>(t_[p_])))) fail("bad number");
+      while (p_ < t_.size() && std::isdigit(static_cast<unsigned char>(t_[p_]))) p_++;
+    }
+    JVal v;
+    v.k = JVal::kNum;
+    const std::string text = t_.substr(b, p_ - b);
+    v.num = std::strtod(text.c_str(), nullptr);
+    if (integral) {
+      errno = 0;
+      char* end = nullptr;
+      v.i = std::strtoll(text.c_str(), &end, 10);
+      v.integral = errno == 0;
+    }
+    return v;
+  }
+};
+
+// Go %q of a string (strconv.Quote): printable ASCII as is, quote and
+// backslash escaped, the rest as escapes.
+std::string go_quote(const std::string& s) {
+  std::string o = "\"";
+  for (unsigned char c : s) {
+    if (c == '"' || c == '\\') {
+      o += '\\';
+      o += char(c);
+    } else if (c >= 0x20 && c < 0x7F) {
+      o += char(c);
+    } else if (c == '\n') {
+      o += "\\n";
+    } else if (c == '\t') {
+      o += "\\t";
+    } else if (c == '\r') {
+      o += "\\r";
+    } else {
+      char buf[8];
+      std::snprintf(buf, sizeof buf, "\\x%02x", c);
+      o += buf;
+    }
+  }
+  return o + "\"";
+}
+
+std::string read_all(std::FILE* f) {
+  std::string t;
+  char buf[65536];
+  size_t n;
+  while ((n = std::fread(buf, 1, sizeof buf, f)) > 0) t.append(buf, n);
+  return t;
+}
+
+bool key_is(const std::string& key, const char* tag) {
+  const size_t n = std::strlen(tag);
+  if (key.size() != n) return false;
+  for (size_t i = 0; i < n; i++)
+    if (std::tolower(static_cast<unsigned char>(key[i])) != std::tolower(static_cast<unsigned char>(tag[i])))
+      return false;
+  return true;
+}
+
+void json_string_field(const JVal& v, std::string* out, const char* key) {
+  if (v.k == JVal::kNull) return;
+  if (v.k != JVal::kStr) throw Error(Z80B_EINVAL, std::string("ReadJSON: field ") + key + " is not a string");
+  *out = v.s;
+}
+
+void json_int_field(const JVal& v, int* out, const char* key) {
+  if (v.k == JVal::kNull) return;
+  if (v.k != JVal::kNum || !v.integral || v.i < INT_MIN || v.i > INT_MAX)
+    throw Error(Z80B_EINVAL, std::string("ReadJSON: field ") + key + " is not an integer in range");
+  *out = int(v.i);
 }
 
 std::vector<uint32_t> pack(const Seq& s) {
@@ -208,7 +497,162 @@ void WriteJSON(std::FILE* f, const std::vector<Rule>& rules) {
   z80b_rules_json(rr.data(), rr.size(), &s[0], s.size());
   std::fwrite(s.data(), 1, size_t(n), f);
 }
+
+std::vector<JSONRule> ReadJSON(const std::string& text) {
+  const JVal top = JParser(text).parse();
+  std::vector<JSONRule> out;
+  if (top.k == JVal::kNull) return out;
+  if (top.k != JVal::kArr) throw Error(Z80B_EINVAL, "ReadJSON: the top-level value is not an array");
+  for (const JVal& e : top.arr) {
+    JSONRule r;
+    if (e.k == JVal::kNull) {
+      out.push_back(r);
+      continue;
+    }
+    if (e.k != JVal::kObj) throw Error(Z80B_EINVAL, "ReadJSON: an array element is not an object");
+    for (const auto& kv : e.obj) {
+      const std::string& k = kv.first;
+      if (key_is(k, "source_asm")) json_string_field(kv.second, &r.SourceASM, "source_asm");
+      else if (key_is(k, "replacement_asm")) json_string_field(kv.second, &r.ReplacementASM, "replacement_asm");
+      else if (key_is(k, "source_bytes")) json_int_field(kv.second, &r.SourceBytes, "source_bytes");
+      else if (key_is(k, "replacement_bytes")) json_int_field(kv.second, &r.ReplacementBytes, "replacement_bytes");
+      else if (key_is(k, "bytes_saved")) json_int_field(kv.second, &r.BytesSaved, "bytes_saved");
+      else if (key_is(k, "cycles_saved")) json_int_field(kv.second, &r.CyclesSaved, "cycles_saved");
+      else if (key_is(k, "dead_flags")) json_string_field(kv.second, &r.DeadFlags, "dead_flags");
+      else if (key_is(k, "dead_flag_desc")) json_string_field(kv.second, &r.DeadFlagDesc, "dead_flag_desc");
+    }
+    out.push_back(r);
+  }
+  return out;
+}
+
+std::vector<JSONRule> ReadJSON(std::FILE* f) { return ReadJSON(read_all(f)); }
+
+Rule FromJSON(const JSONRule& j) {
+  Rule r;
+  if (!search::ParseAssembly(j.SourceASM, &r.Source) || r.Source.empty())
+    throw Error(Z80B_EINVAL, "cannot parse source assembly: " + j.SourceASM);
+  if (!j.ReplacementASM.empty() && !search::ParseAssembly(j.ReplacementASM, &r.Replacement))
+    throw Error(Z80B_EINVAL, "cannot parse replacement assembly: " + j.ReplacementASM);
+  r.BytesSaved = j.BytesSaved;
+  r.CyclesSaved = j.CyclesSaved;
+  if (!j.DeadFlags.empty()) {
+    char* end = nullptr;
+    const unsigned long m = std::strtoul(j.DeadFlags.c_str(), &end, 16);
+    if (*end != '\0' || m > 0xFF) throw Error(Z80B_EINVAL, "bad dead_flags: " + j.DeadFlags);
+    r.DeadFlags = uint8_t(m);
+  }
+  return r;
+}
+
+void WriteGoCode(std::FILE* f, const std::vector<Rule>& rules) {
+  auto seq_text = [](const Seq& s) { return s.empty() ? std::string() : inst::DisasmSeq(s); };
+  auto go_slice = [](const Seq& s) {
+    std::string o;
+    for (size_t i = 0; i < s.size(); i++) {
+      if (i) o += ", ";
+      o += go_quote(inst::Disassemble(s[i]));
+    }
+    return o;
+  };
+  std::fputs("// Code generated by z80opt. DO NOT EDIT.\n\npackage optimizer\n\n"
+             "// Z80OptRules contains peephole optimization rules discovered by the superoptimizer.\n"
+             "var Z80OptRules = []PeepholeRule{\n",
+             f);
+  for (const Rule& r : rules) {
+    const std::string src = seq_text(r.Source), rep = seq_text(r.Replacement);
+    if (r.DeadFlags)
+      std::fprintf(f, "\t// %s -> %s (-%d bytes, -%d cycles) [dead: %s]\n", src.c_str(), rep.c_str(), r.BytesSaved,
+                   r.CyclesSaved, DeadFlagDesc(r.DeadFlags).c_str());
+    else
+      std::fprintf(f, "\t// %s -> %s (-%d bytes, -%d cycles)\n", src.c_str(), rep.c_str(), r.BytesSaved,
+                   r.CyclesSaved);
+    std::fprintf(f, "\t{\n\t\tMatch: []string{%s},\n\t\tReplace: []string{%s},\n", go_slice(r.Source).c_str(),
+                 go_slice(r.Replacement).c_str());
+    if (r.DeadFlags) std::fprintf(f, "\t\tDeadFlags: 0x%02X, // %s\n", r.DeadFlags, DeadFlagDesc(r.DeadFlags).c_str());
+    std::fputs("\t},\n", f);
+  }
+  std::fputs("}\n", f);
+}
 }  // namespace result
+
+namespace peephole {
+const Rule* Lookup(const Table& t, const std::string& source) {
+  const auto it = t.find(source);
+  return it == t.end() ? nullptr : &it->second;
+}
+
+Table LoadRules(const std::string& path) {
+  std::ifstream in(path, std::ios::binary);
+  if (!in) throw Error(Z80B_EINVAL, "LoadRules: cannot open " + path);
+  std::stringstream ss;
+  ss << in.rdbuf();
+  const JVal top = JParser(ss.str()).parse();
+  Table t;
+  if (top.k == JVal::kNull) return t;
+  if (top.k != JVal::kArr) throw Error(Z80B_EINVAL, "LoadRules: the top-level value is not an array");
+  for (const JVal& e : top.arr) {
+    if (e.k == JVal::kNull) {
+      t[""] = Rule{};
+      continue;
+    }
+    if (e.k != JVal::kObj) throw Error(Z80B_EINVAL, "LoadRules: an array element is not an object");
+    std::string src;
+    Rule r;
+    for (const auto& kv : e.obj) {
+      if (key_is(kv.first, "source")) json_string_field(kv.second, &src, "source");
+      else if (key_is(kv.first, "replacement")) json_string_field(kv.second, &r.Replacement, "replacement");
+      else if (key_is(kv.first, "cycles_saved")) json_int_field(kv.second, &r.CyclesSaved, "cycles_saved");
+      else if (key_is(kv.first, "bytes_saved")) json_int_field(kv.second, &r.BytesSaved, "bytes_saved");
+    }
+    t[src] = r;
+  }
+  return t;
+}
+
+void WriteTable(std::FILE* f, const std::vector<std::pair<std::string, Rule>>& entries, const std::string& from,
+                const std::string& var_name) {
+  std::fprintf(f,
+               "// Code generated from %s. DO NOT EDIT.\n"
+               "package peephole\n\n"
+               "import (\n\t\"encoding/json\"\n\t\"os\"\n)\n\n"
+               "// Rule is a peephole replacement: the replacement assembly and what it saves.\n"
+               "type Rule struct {\n\tReplacement string\n\tCyclesSaved int\n\tBytesSaved  int\n}\n\n"
+               "// %s maps source assembly to its replacement.\n"
+               "var %s = map[string]Rule{\n",
+               from.c_str(), var_name.c_str(), var_name.c_str());
+  for (const auto& e : entries)
+    std::fprintf(f, "\t%s: {%s, %d, %d},\n", go_quote(e.first).c_str(), go_quote(e.second.Replacement).c_str(),
+                 e.second.CyclesSaved, e.second.BytesSaved);
+  std::fprintf(f,
+               "}\n\n"
+               "// Lookup returns the replacement recorded for source, or nil.\n"
+               "func Lookup(source string) *Rule {\n"
+               "\tr, ok := %s[source]\n"
+               "\tif !ok {\n\t\treturn nil\n\t}\n"
+               "\treturn &r\n"
+               "}\n\n"
+               "// LoadRules reads a JSON array of {\"source\", \"replacement\", \"cycles_saved\",\n"
+               "// \"bytes_saved\"} objects into a table; a later source replaces an earlier one.\n"
+               "func LoadRules(path string) (map[string]Rule, error) {\n"
+               "\traw, err := os.ReadFile(path)\n"
+               "\tif err != nil {\n\t\treturn nil, err\n\t}\n"
+               "\tvar in []struct {\n"
+               "\t\tSource      string `json:\"source\"`\n"
+               "\t\tReplacement string `json:\"replacement\"`\n"
+               "\t\tCyclesSaved int    `json:\"cycles_saved\"`\n"
+               "\t\tBytesSaved  int    `json:\"bytes_saved\"`\n"
+               "\t}\n"
+               "\tif err := json.Unmarshal(raw, &in); err != nil {\n\t\treturn nil, err\n\t}\n"
+               "\tt := make(map[string]Rule, len(in))\n"
+               "\tfor _, e := range in {\n"
+               "\t\tt[e.Source] = Rule{Replacement: e.Replacement, CyclesSaved: e.CyclesSaved, BytesSaved: e.BytesSaved}\n"
+               "\t}\n"
+               "\treturn t, nil\n"
+               "}\n",
+               var_name.c_str());
+}
+}  // namespace peephole
 
 namespace search {
 

@@ -6,6 +6,8 @@
 //   search::ShouldPrune, EnumerateSequences8 order         pkg/search/pruner.go, enumerator.go
 //   gpu::SearchConfig, SearchGPU                           pkg/gpu/search.go:13-199
 //   result::Rule, Table, WriteJSON, DeadFlagDesc           pkg/result/table.go, output.go
+//   result::JSONRule, ReadJSON, WriteGoCode                pkg/result/output.go:12-22,86-141
+//   peephole::Rule, Lookup, LoadRules, WriteTable          pkg/peephole/rules.go
 //   mul::FindAll (findOptimal for many K)                  cmd/mulopt/main.go:186-229
 //
 // Errors that the Go code returns as `error` are thrown as search::Error
@@ -14,6 +16,7 @@
 #pragma once
 #include <cstdint>
 #include <cstdio>
+#include <map>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -63,7 +66,45 @@ class Table {
 };
 std::string DeadFlagDesc(uint8_t mask);
 void WriteJSON(std::FILE* f, const std::vector<Rule>& rules);
+
+// The JSON form of a rule (output.go:12-22); DeadFlags is "%02X" or empty.
+struct JSONRule {
+  std::string SourceASM, ReplacementASM;
+  int SourceBytes = 0, ReplacementBytes = 0, BytesSaved = 0, CyclesSaved = 0;
+  std::string DeadFlags, DeadFlagDesc;
+};
+// ReadJSON (output.go:86-93): a JSON array of rule objects.  Keys match the
+// struct tags case-insensitively and unknown keys are skipped, as
+// encoding/json does; malformed input throws Error(Z80B_EINVAL).
+std::vector<JSONRule> ReadJSON(std::FILE* f);
+std::vector<JSONRule> ReadJSON(const std::string& text);
+// Back from the JSON form: the assembly parsed into instructions and the
+// dead-flag mask from its hex text (the reference has no such parse-back;
+// throws Error(Z80B_EINVAL) on text that does not parse).
+Rule FromJSON(const JSONRule& j);
+// WriteGoCode (output.go:95-125): the rules as MinZ PeepholeRule entries.
+void WriteGoCode(std::FILE* f, const std::vector<Rule>& rules);
 }  // namespace result
+
+// The generated peephole table package (pkg/peephole/rules.go): a map from
+// the source assembly to its replacement.
+namespace peephole {
+struct Rule {
+  std::string Replacement;
+  int CyclesSaved = 0, BytesSaved = 0;
+};
+using Table = std::map<std::string, Rule>;
+// Lookup (rules.go:522-527): the replacement of a source sequence, or null.
+const Rule* Lookup(const Table& t, const std::string& source);
+// LoadRules (rules.go:529-550): [{"source", "replacement", "cycles_saved",
+// "bytes_saved"}]; a later entry for the same source replaces an earlier one.
+Table LoadRules(const std::string& path);
+// Writes the Go source of the table package, entries in the given order
+// (the layout of rules.go: the Rule type, the table under `var_name`,
+// Lookup and LoadRules); `from` names the rule file in the header line.
+void WriteTable(std::FILE* f, const std::vector<std::pair<std::string, Rule>>& entries, const std::string& from,
+                const std::string& var_name = "Top500");
+}  // namespace peephole
 
 namespace search {
 using FlagMask = uint8_t;

@@ -7,9 +7,13 @@
 //   z80opt verify-jsonl FILE [--dead-flags M] [-v]
 //   z80opt mulopt [--pool mulopt|wide21|fast14|cuda21] [--max-len N] [--min-len N]
 //                 [--k K] [--json] [--init B,C,F]
+//   z80opt export FILE [-f go|peephole] [--output OUT] [--var NAME]
 //
 // Output text follows the reference commands.  --sample/--seed (search a
-// seeded uniform sample of the targets) and --pool/--init are extensions.
+// seeded uniform sample of the targets) and --pool/--init are extensions, and
+// so is `export`'s output (the reference command prints a placeholder line):
+// result.WriteGoCode text, or the generated source of the peephole table
+// package.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -47,6 +51,8 @@ Args parse(int argc, char** argv, const std::vector<std::string>& flags) {
   for (int i = 0; i < argc; i++) {
     std::string s = argv[i];
     if (s == "-v") s = "--verbose";
+    if (s == "-f") s = "--format";
+    if (s == "-o") s = "--output";
     if (s.rfind("--", 0) == 0) {
       const size_t eq = s.find('=');
       std::string k = s.substr(2, eq == std::string::npos ? std::string::npos : eq - 2);
@@ -308,13 +314,60 @@ int cmd_mulopt(const Args& a) {
   return 0;
 }
 
+// export (cmd/z80opt/main.go:173-201): a rules JSON file (result.WriteJSON
+// form) written as Go code.  -f go: result.WriteGoCode (pkg/result/
+// output.go:95-125), the rules parsed back from their assembly with the
+// reference's parser (which, like the reference's, does not take 16-bit
+// immediates: such a rule is an error); -f peephole:
+// the generated table package of pkg/peephole/rules.go, keyed by source
+// assembly in file order (--var names the table, default Top500).  Needs no
+// device.
+int cmd_export(const Args& a) {
+  if (a.pos.size() != 1) throw Error(Z80B_EINVAL, "export: exactly one rules file is required");
+  std::FILE* in = std::fopen(a.pos[0].c_str(), "rb");
+  if (!in) throw Error(Z80B_EINVAL, "cannot open " + a.pos[0]);
+  std::vector<result::JSONRule> js;
+  try {
+    js = result::ReadJSON(in);
+  } catch (...) {
+    std::fclose(in);
+    throw;
+  }
+  std::fclose(in);
+  const std::string format = a.get("format", "go");
+  if (format != "go" && format != "peephole") throw Error(Z80B_EINVAL, "unknown format: " + format);
+  std::FILE* out = stdout;
+  const std::string path = a.get("output", "");
+  if (!path.empty()) {
+    out = std::fopen(path.c_str(), "wb");
+    if (!out) throw Error(Z80B_EINVAL, "cannot create " + path);
+  }
+  if (format == "go") {
+    std::vector<result::Rule> rules;
+    rules.reserve(js.size());
+    for (const auto& j : js) rules.push_back(result::FromJSON(j));
+    result::WriteGoCode(out, rules);
+  } else {
+    std::vector<std::pair<std::string, peephole::Rule>> entries;
+    entries.reserve(js.size());
+    for (const auto& j : js) entries.push_back({j.SourceASM, peephole::Rule{j.ReplacementASM, j.CyclesSaved, j.BytesSaved}});
+    std::string from = a.pos[0];
+    const size_t slash = from.find_last_of('/');
+    if (slash != std::string::npos) from = from.substr(slash + 1);
+    peephole::WriteTable(out, entries, from, a.get("var", "Top500"));
+  }
+  if (out != stdout) std::fclose(out);
+  return 0;
+}
+
 void usage() {
   std::fprintf(stderr,
-               "usage: z80opt enumerate|target|verify-jsonl|mulopt [flags]\n"
+               "usage: z80opt enumerate|target|verify-jsonl|mulopt|export [flags]\n"
                "  enumerate    --max-target N --output FILE --dead-flags none|undoc|all|0xNN --gpu -v\n"
                "  target       \"ASM : ASM\" --max-candidate N\n"
                "  verify-jsonl FILE --dead-flags M -v\n"
-               "  mulopt       --pool mulopt|wide21|fast14|cuda21 --max-len N --k K --json\n");
+               "  mulopt       --pool mulopt|wide21|fast14|cuda21 --max-len N --k K --json\n"
+               "  export       FILE -f go|peephole --output OUT --var NAME\n");
 }
 
 }  // namespace
@@ -331,6 +384,7 @@ int main(int argc, char** argv) {
     if (cmd == "target") return cmd_target(a);
     if (cmd == "verify-jsonl") return cmd_verify_jsonl(a);
     if (cmd == "mulopt") return cmd_mulopt(a);
+    if (cmd == "export") return cmd_export(a);
     usage();
     return 2;
   } catch (const Error& e) {
