@@ -109,8 +109,12 @@ typedef struct z80b_job {
   uint32_t global_dead_flags;   /* search.FlagMask applied to every target */
   uint32_t mode;                /* Z80B_MODE_* */
   uint32_t path;                /* Z80B_PATH_* */
-  uint32_t reserved;
+  uint32_t flags;               /* Z80B_JOB_* bits, 0 for the default pipeline */
 } z80b_job;
+/* Z80B_MODE_ALL only: report every MidCheck survivor without the
+ * ExhaustiveCheck tier (cuda/z80_search_v2.cu --no-exhaust,
+ * z80_search_v2.cu:944-948); such rules are candidates, not proofs. */
+#define Z80B_JOB_NO_EXHAUSTIVE 1u
 
 /* ---- context ---------------------------------------------------------- */
 int z80b_init(int device, z80b_ctx** out);

@@ -1,6 +1,8 @@
-"""Rule export formats: `z80opt export` (result.WriteGoCode text and the
-generated peephole table package) and the JSON reader and peephole table
-functions of the C++ host API.  No device is needed."""
+"""Host-side parts of the enumeration and export rows: `z80opt export`
+(result.WriteGoCode text and the generated peephole table package), the
+JSON reader and peephole table functions of the C++ host API, and the ranged
+target enumeration behind `enumerate --first-op-start/--first-op-end`.  No
+device is needed."""
 import json
 import os
 import subprocess
@@ -104,3 +106,33 @@ def test_json_reader_and_peephole_api(tmp_path):
     r = subprocess.run([str(exe), str(tmp_path)], capture_output=True, text=True, timeout=60)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.startswith("OK")
+
+
+def _native(tmp_path, name, extra=()):
+    exe = tmp_path / name
+    build = os.path.join(ROOT, "z80-optimizer_b200", "_build")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-o", str(exe),
+                    os.path.join(ROOT, "tests", "native", name + ".cpp"),
+                    os.path.join(ROOT, "z80-optimizer_b200", "csrc", "host", "search_api.cpp"), *extra,
+                    "-I" + os.path.join(ROOT, "z80-optimizer_b200", "csrc", "host"),
+                    "-I" + os.path.join(ROOT, "include"), "-L" + build, "-lz80b200",
+                    "-Wl,-rpath," + build, "-lpthread"], check=True)
+    return exe
+
+
+def test_ranged_target_enumeration(tmp_path):
+    """EnumerateTargets: whole and split ranges equal the full enumeration,
+    samples follow Floyd's algorithm (length 2) or are uniform distinct
+    unpruned draws (length 3), length-3 ranges match the oracle's pruner."""
+    exe = _native(tmp_path, "enum_check", [os.path.join(ROOT, "oracle", "z80_oracle_isa_cpu.cpp"),
+                                           os.path.join(ROOT, "oracle", "z80_oracle_search.cpp")])
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.startswith("OK")
+
+
+def test_enumerate_flag_checks():
+    r = run("enumerate", "--max-target", "4")
+    assert r.returncode == 1 and "--max-target must be 2 or 3" in r.stderr
+    r = run("enumerate", "--no-exhaust")
+    assert r.returncode == 1 and "--no-exhaust needs --gpu" in r.stderr

@@ -11,6 +11,8 @@
 #include <mutex>
 #include <random>
 #include <sstream>
+#include <thread>
+#include <unordered_set>
 
 namespace z80opt {
 
@@ -338,10 +340,12 @@ result::Rule to_rule(const z80b_rule& r) {
 // One z80b_search over packed targets (stride words each); rules appended
 // to `table` in target order.
 void run_job(const std::vector<uint32_t>& targets, const std::vector<uint8_t>& lens, uint32_t stride,
-             int maxCand, search::FlagMask dead, uint32_t mode, result::Table* table, search::Stats* stats) {
+             int maxCand, search::FlagMask dead, uint32_t mode, uint32_t flags,
+             const std::function<void(const result::Rule&)>& emit, search::Stats* stats) {
   const uint32_t n = uint32_t(lens.size());
   if (n == 0) return;
   z80b_job job{};
+  job.flags = flags;
   job.targets = targets.data();
   job.target_lens = lens.data();
   job.n_targets = n;
@@ -360,7 +364,7 @@ void run_job(const std::vector<uint32_t>& targets, const std::vector<uint8_t>& l
     s = z80b_search(context(), &job, out.data(), out.size(), &nr, &st);
   }
   check(s, "z80b_search");
-  for (uint64_t i = 0; i < nr; i++) table->Add(to_rule(out[i]));
+  for (uint64_t i = 0; i < nr; i++) emit(to_rule(out[i]));
   if (stats) {
     stats->targets += st.targets;
     stats->checks += st.checks;
@@ -370,55 +374,37 @@ void run_job(const std::vector<uint32_t>& targets, const std::vector<uint8_t>& l
   }
 }
 
-// The unpruned targets of one length over the 8-bit list, in
-// EnumerateSequences8 order, or a seeded sample of them by index.
-void collect_targets(int len, uint64_t sample, uint64_t seed, std::vector<uint32_t>* out, uint64_t* count) {
-  std::vector<uint32_t> pool(4531);
-  pool.resize(z80b_pool8(pool.data(), uint32_t(pool.size())));
-  const uint64_t total = z80b_enumerate(pool.data(), uint32_t(pool.size()), uint32_t(len), nullptr, 0);
-  std::vector<uint32_t> all(total * uint64_t(len));
-  z80b_enumerate(pool.data(), uint32_t(pool.size()), uint32_t(len), all.data(), total);
-  if (sample == 0 || sample >= total) {
-    *out = std::move(all);
-    *count = total;
-    return;
-  }
-  // Floyd's algorithm: `sample` distinct indices, then index order.
-  std::mt19937_64 rng(seed);
-  std::vector<uint64_t> pick;
-  pick.reserve(sample);
-  std::vector<uint8_t> taken(total, 0);
-  for (uint64_t j = total - sample; j < total; j++) {
-    uint64_t t = std::uniform_int_distribution<uint64_t>(0, j)(rng);
-    if (taken[t]) t = j;
-    taken[t] = 1;
-    pick.push_back(t);
-  }
-  std::sort(pick.begin(), pick.end());
-  out->resize(sample * uint64_t(len));
-  for (uint64_t i = 0; i < sample; i++)
-    std::memcpy(out->data() + i * uint64_t(len), all.data() + pick[i] * uint64_t(len), 4u * uint32_t(len));
-  *count = sample;
-}
+// What run_lengths searches: target lengths 2..maxTarget (each over the
+// first-instruction range, whole or sampled) as first-found or all-hits
+// jobs of at most 4M targets.
+struct RunSpec {
+  int maxTarget = 2, maxCand = 1;
+  search::FlagMask dead = 0;
+  uint32_t mode = Z80B_MODE_FIRST, flags = 0;
+  uint64_t sample = 0, seed = 0;
+  bool verbose = false;
+  int first0 = 0, first1 = -1;
+  search::RuleSink sink;
+};
 
-result::Table run_lengths(int maxTarget, int maxCand, search::FlagMask dead, uint32_t mode, uint64_t sample,
-                          uint64_t seed, bool verbose, search::Stats* stats) {
+result::Table run_lengths(const RunSpec& r, search::Stats* stats) {
   result::Table table;
-  for (int len = 2; len <= maxTarget; len++) {
-    std::vector<uint32_t> t;
+  const std::function<void(const result::Rule&)> emit =
+      r.sink ? r.sink : std::function<void(const result::Rule&)>([&](const result::Rule& x) { table.Add(x); });
+  for (int len = 2; len <= r.maxTarget; len++) {
+    if (r.verbose) std::printf("=== Searching target length %d ===\n", len);
     uint64_t n = 0;
-    collect_targets(len, sample, seed, &t, &n);
-    if (verbose) std::printf("=== Searching target length %d ===\n  Generated %llu target sequences (after pruning)\n",
-                             len, (unsigned long long)n);
     // jobs of at most 4M targets keep the per-job device buffers modest
-    const uint64_t chunk = 1u << 22;
-    for (uint64_t lo = 0; lo < n; lo += chunk) {
-      const uint64_t hi = std::min(n, lo + chunk);
-      std::vector<uint32_t> part(t.begin() + long(lo * uint64_t(len)), t.begin() + long(hi * uint64_t(len)));
-      std::vector<uint8_t> lens(hi - lo, uint8_t(len));
-      run_job(part, lens, uint32_t(len), maxCand, dead, mode, &table, stats);
+    search::EnumerateTargets(len, r.first0, r.first1, r.sample, r.seed, 1u << 22,
+                             [&](const std::vector<uint32_t>& w, uint64_t m) {
+                               n += m;
+                               const std::vector<uint8_t> lens(m, uint8_t(len));
+                               run_job(w, lens, uint32_t(len), r.maxCand, r.dead, r.mode, r.flags, emit, stats);
+                             });
+    if (r.verbose) {
+      std::printf("  Generated %llu target sequences (after pruning)\n", (unsigned long long)n);
+      if (!r.sink) std::printf("  Found: %zu\n", table.Len());
     }
-    if (verbose) std::printf("  Found: %zu\n", table.Len());
   }
   return table;
 }
@@ -658,15 +644,26 @@ namespace search {
 
 result::Table Run(const Config& cfg, Stats* stats) {
   const int maxCand = cfg.MaxCandLen > 0 ? cfg.MaxCandLen : cfg.MaxTargetLen - 1;
-  return run_lengths(cfg.MaxTargetLen, maxCand, cfg.DeadFlags, Z80B_MODE_FIRST, cfg.SampleTargets, cfg.Seed,
-                     cfg.Verbose, stats);
+  RunSpec r;
+  r.maxTarget = cfg.MaxTargetLen;
+  r.maxCand = maxCand;
+  r.dead = cfg.DeadFlags;
+  r.mode = Z80B_MODE_FIRST;
+  r.sample = cfg.SampleTargets;
+  r.seed = cfg.Seed;
+  r.verbose = cfg.Verbose;
+  r.first0 = cfg.FirstOpStart;
+  r.first1 = cfg.FirstOpEnd;
+  r.sink = cfg.Sink;
+  return run_lengths(r, stats);
 }
 
 static bool single(const Seq& target, int maxCandLen, FlagMask dead, result::Rule* out) {
   if (target.empty() || target.size() > 4) throw Error(Z80B_EINVAL, "target length must be 1..4");
   result::Table t;
   const auto w = pack(target);
-  run_job(w, {uint8_t(target.size())}, uint32_t(target.size()), maxCandLen, dead, Z80B_MODE_FIRST, &t, nullptr);
+  run_job(w, {uint8_t(target.size())}, uint32_t(target.size()), maxCandLen, dead, Z80B_MODE_FIRST, 0,
+          [&](const result::Rule& x) { t.Add(x); }, nullptr);
   const auto rules = t.Rules();
   if (rules.empty()) return false;
   if (out) *out = rules[0];
@@ -729,6 +726,125 @@ bool ParseAssembly(const std::string& text, Seq* out) {
   return true;
 }
 
+void EnumerateTargets(int len, int firstStart, int firstEnd, uint64_t sample, uint64_t seed, uint64_t batch,
+                      const std::function<void(const std::vector<uint32_t>&, uint64_t)>& fn) {
+  if (len < 1 || len > 3) throw Error(Z80B_EINVAL, "EnumerateTargets: lengths 1..3");
+  if (batch == 0) throw Error(Z80B_EINVAL, "EnumerateTargets: batch must be positive");
+  std::vector<uint32_t> pool(4531);
+  pool.resize(z80b_pool8(pool.data(), uint32_t(pool.size())));
+  const uint64_t P = pool.size();
+  const uint64_t lo = uint64_t(std::max(0, firstStart));
+  const uint64_t hi = firstEnd < 0 ? P : std::min<uint64_t>(P, uint64_t(firstEnd));
+  if (lo >= hi) return;
+  const uint64_t per_first = len == 1 ? 1 : (len == 2 ? P : P * P);
+  const uint64_t L = uint64_t(len);
+  auto seq_at = [&](uint64_t raw, uint32_t* w) {  // raw index within the range
+    uint64_t rest = raw;
+    for (int k = len - 1; k >= 1; k--) {
+      w[k] = pool[rest % P];
+      rest /= P;
+    }
+    w[0] = pool[lo + rest];
+  };
+  {
+    const uint32_t one = pool[0];  // builds the library's tables before any threads
+    (void)z80b_should_prune(&one, 1);
+  }
+  // the unpruned sequences of one first instruction, in order (length 3:
+  // the second instruction's range split over threads)
+  auto of_first = [&](uint64_t i0, std::vector<uint32_t>* out) {
+    out->clear();
+    const uint64_t nth =
+        len == 3 ? std::max<uint64_t>(1, std::min<uint64_t>(32, std::thread::hardware_concurrency())) : 1;
+    std::vector<std::vector<uint32_t>> part(nth);
+    auto work = [&](uint64_t t) {
+      const uint64_t a = per_first * t / nth, b = per_first * (t + 1) / nth;
+      uint32_t w[3];
+      for (uint64_t r = a; r < b; r++) {
+        seq_at((i0 - lo) * per_first + r, w);
+        if (z80b_should_prune(w, uint32_t(len)) == 0) part[t].insert(part[t].end(), w, w + len);
+      }
+    };
+    if (nth == 1) {
+      work(0);
+    } else {
+      std::vector<std::thread> th;
+      for (uint64_t t = 0; t < nth; t++) th.emplace_back(work, t);
+      for (auto& x : th) x.join();
+    }
+    for (auto& v : part) out->insert(out->end(), v.begin(), v.end());
+  };
+  std::vector<uint32_t> buf;
+  uint64_t nbuf = 0;
+  auto push = [&](const uint32_t* w, uint64_t n) {
+    while (n) {
+      const uint64_t take = std::min(n, batch - nbuf);
+      buf.insert(buf.end(), w, w + take * L);
+      nbuf += take;
+      w += take * L;
+      n -= take;
+      if (nbuf == batch) {
+        fn(buf, nbuf);
+        buf.clear();
+        nbuf = 0;
+      }
+    }
+  };
+  if (sample == 0 || len < 3) {
+    // every unpruned sequence of the range (and, for a sample of length 1
+    // or 2, Floyd's algorithm over their indices, kept in index order)
+    std::vector<uint32_t> all, one;
+    for (uint64_t i0 = lo; i0 < hi; i0++) {
+      of_first(i0, &one);
+      if (sample == 0) push(one.data(), one.size() / L);
+      else all.insert(all.end(), one.begin(), one.end());
+    }
+    if (sample) {
+      const uint64_t total = all.size() / L;
+      if (sample >= total) {
+        push(all.data(), total);
+      } else {
+        std::mt19937_64 rng(seed);
+        std::vector<uint64_t> pick;
+        pick.reserve(sample);
+        std::vector<uint8_t> taken(total, 0);
+        for (uint64_t j = total - sample; j < total; j++) {
+          uint64_t t = std::uniform_int_distribution<uint64_t>(0, j)(rng);
+          if (taken[t]) t = j;
+          taken[t] = 1;
+          pick.push_back(t);
+        }
+        std::sort(pick.begin(), pick.end());
+        for (uint64_t t : pick) push(all.data() + t * L, 1);
+      }
+    }
+  } else {
+    // length 3, sampled: distinct raw indices of the range drawn uniformly
+    // until `sample` unpruned ones are in hand (uniform over the unpruned
+    // sequences), then delivered in index order
+    const uint64_t raw = (hi - lo) * per_first;
+    if (sample > raw / 2)
+      throw Error(Z80B_EINVAL, "EnumerateTargets: a sample above half the range; enumerate the range whole");
+    std::mt19937_64 rng(seed);
+    std::unordered_set<uint64_t> seen;
+    std::vector<uint64_t> pick;
+    pick.reserve(sample);
+    uint32_t w[3];
+    while (pick.size() < sample && seen.size() < raw) {
+      const uint64_t t = std::uniform_int_distribution<uint64_t>(0, raw - 1)(rng);
+      if (!seen.insert(t).second) continue;
+      seq_at(t, w);
+      if (z80b_should_prune(w, 3) == 0) pick.push_back(t);
+    }
+    std::sort(pick.begin(), pick.end());
+    for (uint64_t t : pick) {
+      seq_at(t, w);
+      push(w, 1);
+    }
+  }
+  if (nbuf) fn(buf, nbuf);
+}
+
 bool ParseDeadFlags(const std::string& text, FlagMask* out) {
   uint32_t m = 0;
   if (z80b_parse_dead_flags(text.c_str(), &m) != Z80B_OK) return false;
@@ -740,8 +856,19 @@ bool ParseDeadFlags(const std::string& text, FlagMask* out) {
 
 namespace gpu {
 result::Table SearchGPU(const SearchConfig& cfg) {
-  return run_lengths(cfg.MaxTargetLen, 1, cfg.DeadFlags, Z80B_MODE_ALL, cfg.SampleTargets, cfg.Seed, cfg.Verbose,
-                     nullptr);
+  RunSpec r;
+  r.maxTarget = cfg.MaxTargetLen;
+  r.maxCand = 1;
+  r.dead = cfg.DeadFlags;
+  r.mode = Z80B_MODE_ALL;
+  r.flags = cfg.NoExhaust ? Z80B_JOB_NO_EXHAUSTIVE : 0u;
+  r.sample = cfg.SampleTargets;
+  r.seed = cfg.Seed;
+  r.verbose = cfg.Verbose;
+  r.first0 = cfg.FirstOpStart;
+  r.first1 = cfg.FirstOpEnd;
+  r.sink = cfg.Sink;
+  return run_lengths(r, nullptr);
 }
 }  // namespace gpu
 

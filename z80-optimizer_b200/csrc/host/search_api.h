@@ -16,6 +16,7 @@
 #pragma once
 #include <cstdint>
 #include <cstdio>
+#include <functional>
 #include <map>
 #include <stdexcept>
 #include <string>
@@ -110,6 +111,11 @@ namespace search {
 using FlagMask = uint8_t;
 constexpr FlagMask DeadNone = 0x00, DeadUndoc = 0x28, DeadAll = 0xFF;
 
+// Receives each rule as soon as its batch of targets is done (Run and
+// SearchGPU then return an empty table): the form for enumerations whose
+// rule sets do not fit in memory.
+using RuleSink = std::function<void(const result::Rule&)>;
+
 struct Config {
   int MaxTargetLen = 2;  // targets of length 2..MaxTargetLen
   int MaxCandLen = 0;    // 0: MaxTargetLen - 1
@@ -120,6 +126,12 @@ struct Config {
   // (by enumeration index) instead of all of them; 0 = all.
   uint64_t SampleTargets = 0;
   uint64_t Seed = 0;
+  // Extension (cuda/z80_search_v2.cu --first-op-start/--first-op-end): only
+  // targets whose first instruction has an index in [FirstOpStart,
+  // FirstOpEnd) of the 8-bit list; -1 = to the end.  Disjoint ranges shard
+  // an enumeration over processes or GPUs.
+  int FirstOpStart = 0, FirstOpEnd = -1;
+  RuleSink Sink;  // extension, see RuleSink
 };
 
 struct Stats {  // accumulated over Run's jobs
@@ -138,6 +150,17 @@ std::vector<uint8_t> ExhaustiveCheckBatch(const std::vector<Seq>& targets, const
 bool ShouldPrune(const Seq& s);
 bool ParseAssembly(const std::string& text, Seq* out);      // cmd/z80opt/main.go:325-397
 bool ParseDeadFlags(const std::string& text, FlagMask* out);  // cmd/z80opt/main.go:305-322
+
+// The unpruned sequences of `len` instructions over the 8-bit list whose
+// first instruction has an index in [firstStart, firstEnd) (-1: to the
+// end), in EnumerateSequences8 order (pkg/search/enumerator.go:14-60), or a
+// seeded uniform sample of `sample` of them (0: all; drawn by index among
+// the unpruned ones, delivered in index order).  Delivered in batches of at
+// most `batch` sequences: packed words, `len` per sequence.  Lengths 1..3;
+// nothing is held beyond one batch and one first instruction's sequences,
+// so length 3 (93 billion sequences) can be walked range by range.
+void EnumerateTargets(int len, int firstStart, int firstEnd, uint64_t sample, uint64_t seed, uint64_t batch,
+                      const std::function<void(const std::vector<uint32_t>& words, uint64_t n)>& fn);
 }  // namespace search
 
 namespace gpu {
@@ -147,6 +170,11 @@ struct SearchConfig {
   search::FlagMask DeadFlags = search::DeadNone;
   uint64_t SampleTargets = 0;  // extension, as in search::Config
   uint64_t Seed = 0;
+  int FirstOpStart = 0, FirstOpEnd = -1;  // extension, as in search::Config
+  // Extension (cuda/z80_search_v2.cu --no-exhaust): every MidCheck survivor
+  // is reported, without the ExhaustiveCheck tier.
+  bool NoExhaust = false;
+  search::RuleSink Sink;  // extension, as in search::Config
 };
 result::Table SearchGPU(const SearchConfig& cfg);
 }  // namespace gpu

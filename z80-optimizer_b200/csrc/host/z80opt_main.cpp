@@ -3,6 +3,7 @@
 //
 //   z80opt enumerate [--max-target N] [--output FILE] [--dead-flags M] [--gpu]
 //                    [--workers N] [-v] [--sample N] [--seed S]
+//                    [--first-op-start M] [--first-op-end N] [--jsonl FILE] [--no-exhaust]
 //   z80opt target "ASM : ASM ..." [--max-candidate N] [--dead-flags M] [-v]
 //   z80opt verify-jsonl FILE [--dead-flags M] [-v]
 //   z80opt mulopt [--pool mulopt|wide21|fast14|cuda21] [--max-len N] [--min-len N]
@@ -10,7 +11,11 @@
 //   z80opt export FILE [-f go|peephole] [--output OUT] [--var NAME]
 //
 // Output text follows the reference commands.  --sample/--seed (search a
-// seeded uniform sample of the targets) and --pool/--init are extensions, and
+// seeded uniform sample of the targets), --first-op-start/--first-op-end
+// (shard by the first instruction's index), --jsonl (stream rules as JSON
+// lines) and --no-exhaust (with --gpu: MidCheck survivors without the
+// ExhaustiveCheck tier), after cuda/z80_search_v2.cu, and --pool/--init are
+// extensions, and
 // so is `export`'s output (the reference command prints a placeholder line):
 // result.WriteGoCode text, or the generated source of the peephole table
 // package.
@@ -76,10 +81,46 @@ search::FlagMask dead_flags(const Args& a) {
   return m;
 }
 
+// One rule as a JSON line, in cuda/z80_search_v2.cu's emit_jsonl form
+// (z80_search_v2.cu:923-942).
+void write_jsonl(std::FILE* f, const result::Rule& r) {
+  auto esc = [](const std::string& t) {
+    std::string o;
+    for (char c : t) {
+      if (c == '"' || c == '\\') o += '\\';
+      o += c;
+    }
+    return o;
+  };
+  std::fprintf(f,
+               "{\"source_asm\":\"%s\",\"replacement_asm\":\"%s\",\"source_bytes\":%d,\"replacement_bytes\":%d,"
+               "\"bytes_saved\":%d,\"cycles_saved\":%d",
+               esc(inst::DisasmSeq(r.Source)).c_str(), esc(inst::DisasmSeq(r.Replacement)).c_str(),
+               inst::SeqByteSize(r.Source), inst::SeqByteSize(r.Replacement), r.BytesSaved, r.CyclesSaved);
+  if (r.DeadFlags) std::fprintf(f, ",\"dead_flags\":\"0x%02X\"", r.DeadFlags);
+  std::fputs("}\n", f);
+}
+
 int cmd_enumerate(const Args& a) {
   const search::FlagMask dead = dead_flags(a);
   const int maxTarget = int(a.num("max-target", 2));
   const bool gpu = a.has("gpu"), verbose = a.has("verbose");
+  const int first0 = int(a.num("first-op-start", 0)), first1 = int(a.num("first-op-end", -1));
+  const bool noExhaust = a.has("no-exhaust");
+  if (noExhaust && !gpu) throw Error(Z80B_EINVAL, "--no-exhaust needs --gpu (all-hits mode)");
+  if (maxTarget < 2 || maxTarget > 3) throw Error(Z80B_EINVAL, "--max-target must be 2 or 3");
+  std::FILE* jl = nullptr;
+  uint64_t streamed = 0;
+  search::RuleSink sink;
+  const std::string jpath = a.get("jsonl", "");
+  if (!jpath.empty()) {
+    jl = std::fopen(jpath.c_str(), "w");
+    if (!jl) throw Error(Z80B_EINVAL, "cannot create " + jpath);
+    sink = [&](const result::Rule& r) {
+      write_jsonl(jl, r);
+      streamed++;
+    };
+  }
   std::printf("Z80 Superoptimizer\n");
   std::printf("  Max target length: %d\n", maxTarget);
   std::printf("  Target instructions: 4531 per position (8-bit only)\n");
@@ -94,6 +135,10 @@ int cmd_enumerate(const Args& a) {
     c.DeadFlags = dead;
     c.SampleTargets = uint64_t(a.num("sample", 0));
     c.Seed = uint64_t(a.num("seed", 0));
+    c.FirstOpStart = first0;
+    c.FirstOpEnd = first1;
+    c.NoExhaust = noExhaust;
+    c.Sink = sink;
     rules = gpu::SearchGPU(c).Rules();
   } else {
     search::Config c;
@@ -103,7 +148,15 @@ int cmd_enumerate(const Args& a) {
     c.DeadFlags = dead;
     c.SampleTargets = uint64_t(a.num("sample", 0));
     c.Seed = uint64_t(a.num("seed", 0));
+    c.FirstOpStart = first0;
+    c.FirstOpEnd = first1;
+    c.Sink = sink;
     rules = search::Run(c).Rules();
+  }
+  if (jl) {
+    std::fclose(jl);
+    std::printf("\nFound %llu optimizations (streamed to %s)\n", (unsigned long long)streamed, jpath.c_str());
+    return 0;
   }
   std::printf("\nFound %zu optimizations\n", rules.size());
   const std::string out = a.get("output", "");
@@ -364,6 +417,7 @@ void usage() {
   std::fprintf(stderr,
                "usage: z80opt enumerate|target|verify-jsonl|mulopt|export [flags]\n"
                "  enumerate    --max-target N --output FILE --dead-flags none|undoc|all|0xNN --gpu -v\n"
+               "               --sample N --seed S --first-op-start M --first-op-end N --jsonl FILE --no-exhaust\n"
                "  target       \"ASM : ASM\" --max-candidate N\n"
                "  verify-jsonl FILE --dead-flags M -v\n"
                "  mulopt       --pool mulopt|wide21|fast14|cuda21 --max-len N --k K --json\n"
@@ -378,7 +432,7 @@ int main(int argc, char** argv) {
     return 2;
   }
   const std::string cmd = argv[1];
-  const Args a = parse(argc - 2, argv + 2, {"verbose", "gpu", "json"});
+  const Args a = parse(argc - 2, argv + 2, {"verbose", "gpu", "json", "no-exhaust"});
   try {
     if (cmd == "enumerate") return cmd_enumerate(a);
     if (cmd == "target") return cmd_target(a);

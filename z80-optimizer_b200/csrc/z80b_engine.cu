@@ -81,6 +81,7 @@ struct PipeOpts {
   uint32_t mode = Z80B_MODE_FIRST;
   uint32_t max_cand = 1;        // longest candidate (1 or 2 instructions)
   uint64_t dreg_masks = 1;      // bit m: dead-register mask m occurs in a masked pass (bit 0 always)
+  bool no_exhaustive = false;   // all-hits mode: MidCheck survivors are the rules (Z80B_JOB_NO_EXHAUSTIVE)
   Reporter* rep = nullptr;      // per-target answers as they become final (first-found mode)
 };
 
@@ -428,6 +429,9 @@ int validate_job(z80b_ctx* ctx, const z80b_job* job) {
     return fail(ctx, Z80B_EINVAL, "max_cand_len must be 1 or 2");
   if (job->max_cand_len == 2 && job->mode != Z80B_MODE_FIRST)
     return fail(ctx, Z80B_EINVAL, "length-2 candidates need Z80B_MODE_FIRST");
+  if (job->flags & ~Z80B_JOB_NO_EXHAUSTIVE) return fail(ctx, Z80B_EINVAL, "unknown job flags %#x", job->flags);
+  if ((job->flags & Z80B_JOB_NO_EXHAUSTIVE) && job->mode != Z80B_MODE_ALL)
+    return fail(ctx, Z80B_EINVAL, "Z80B_JOB_NO_EXHAUSTIVE needs Z80B_MODE_ALL");
   if (job->global_dead_flags > 0xFF) return fail(ctx, Z80B_EINVAL, "dead flags > 0xFF");
   for (uint32_t i = 0; i < job->n_targets; i++) {
     uint32_t l = job->target_lens ? job->target_lens[i] : job->target_len;
@@ -787,7 +791,9 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
       CK(cudaMemsetAsync(ctx->flag.p, 0, 4ull * S, s));
       if (np) {
         rounds = 1;
-        CKR(sweep_round(ctx, T, P, R, np));
+        // without the ExhaustiveCheck tier every pair keeps the zero
+        // rejection flag its build wrote
+        if (!opts.no_exhaustive) CKR(sweep_round(ctx, T, P, R, np));
         launch_rule_count_all(R, np, ctx->flag.as<uint32_t>(), s);
         CKR(check_launch(ctx, "rule_count_all"));
       }
@@ -938,6 +944,7 @@ int upload_targets(z80b_ctx* ctx, Staged& S, const z80b_job* job, DevTargets* T,
   S.opts = PipeOpts{};
   S.opts.mode = job->mode;
   S.opts.max_cand = job->max_cand_len;
+  S.opts.no_exhaustive = (job->flags & Z80B_JOB_NO_EXHAUSTIVE) != 0;
   if (job->max_cand_len >= 2)
     for (uint32_t i = 0; i < n; i++) {
       const uint32_t dr = job->dead_regs ? job->dead_regs[i] & 0x3Fu : 0u;

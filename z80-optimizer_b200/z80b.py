@@ -87,7 +87,7 @@ class Job(ctypes.Structure):
                 ("n_targets", ctypes.c_uint32), ("target_len", ctypes.c_uint32),
                 ("target_stride", ctypes.c_uint32), ("max_cand_len", ctypes.c_uint32),
                 ("global_dead_flags", ctypes.c_uint32), ("mode", ctypes.c_uint32),
-                ("path", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("path", ctypes.c_uint32), ("flags", ctypes.c_uint32)]
 
 
 _lib = None
@@ -104,6 +104,7 @@ EXPORTS = [
 ]
 RULE_CB = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32)
 OPT_EXH_LANE_STATES, OPT_EXH_CHUNK_BLOCKS, OPT_STREAM_PRIORITY, OPT_QC_INDEX = 1, 2, 3, 4
+JOB_NO_EXHAUSTIVE = 1
 
 
 MULPOOL_MULOPT, MULPOOL_WIDE21, MULPOOL_FAST14, MULPOOL_CUDA21 = 0, 1, 2, 3
@@ -380,7 +381,7 @@ class Context:
 
     @staticmethod
     def make_job(targets, dead_flags=0, mode=MODE_FIRST, path=PATH_BATCHED, per_target_dead=None,
-                 dead_regs=None, stride=4, max_cand_len=1):
+                 dead_regs=None, stride=4, max_cand_len=1, no_exhaustive=False):
         """Builds a Job plus the ctypes buffers it points to."""
         n = len(targets)
         stride = max([stride] + [len(t) for t in targets])
@@ -409,12 +410,13 @@ class Context:
         job.global_dead_flags = dead_flags
         job.mode = mode
         job.path = path
+        job.flags = JOB_NO_EXHAUSTIVE if no_exhaustive else 0
         return job, keep
 
     def search(self, targets, dead_flags=0, mode=MODE_FIRST, path=PATH_BATCHED,
-               per_target_dead=None, dead_regs=None, max_cand_len=1):
+               per_target_dead=None, dead_regs=None, max_cand_len=1, no_exhaustive=False):
         job, keep = self.make_job(targets, dead_flags, mode, path, per_target_dead, dead_regs,
-                                  max_cand_len=max_cand_len)
+                                  max_cand_len=max_cand_len, no_exhaustive=no_exhaustive)
         return self.run_job(job)
 
     def run_job(self, job, cap=None):
