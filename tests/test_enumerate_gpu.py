@@ -74,3 +74,33 @@ def test_all_hits_without_exhaustive_tier(ctx, O):
         assert O.exhaustive(t, c, 0x28) == (k in fk)
     with pytest.raises(z80b.Z80BError):
         ctx.search(targets[:5], no_exhaustive=True)  # needs the all-hits mode
+
+
+@pytest.mark.gpu
+def test_stoke_verifier_calls_host_api(tmp_path, O):
+    """ExhaustiveCheck[Masked] and FlagDiff through the C++ host API, the
+    calls pkg/stoke/search.go:108-117 makes, against the oracle."""
+    build = os.path.join(ROOT, "z80-optimizer_b200", "_build")
+    exe = tmp_path / "stoke_check"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-o", str(exe), os.path.join(ROOT, "tests", "native", "stoke_check.cpp"),
+                    os.path.join(ROOT, "z80-optimizer_b200", "csrc", "host", "search_api.cpp"),
+                    "-I" + os.path.join(ROOT, "z80-optimizer_b200", "csrc", "host"),
+                    "-I" + os.path.join(ROOT, "include"), "-L" + build, "-lz80b200", "-Wl,-rpath," + build,
+                    "-lpthread"], check=True)
+    pool = z80b.pool8()
+    rng = __import__("random").Random(17)
+    o = O.ops()
+    pairs = [([O.pack(o["SUB_A"]), O.pack(o["LD_A_N"], 0)], [O.pack(o["SUB_A"])], 0),
+             ([O.pack(o["LD_A_N"], 0), O.pack(o["NEG"])], [O.pack(o["SUB_A"])], 0xFF),
+             ([O.pack(o["AND_N"], 0xFF)], [O.pack(o["OR_N"], 0)], 0x10)]
+    for _ in range(60):
+        t = [rng.choice(pool) for _ in range(rng.choice((1, 2)))]
+        pairs.append((t, [rng.choice(pool)], rng.choice((0, 0xFF, 0x28))))
+    f = tmp_path / "pairs.txt"
+    f.write_text("".join(f"{d:x} " + " ".join(f"{w:x}" for w in t) + " ; " + " ".join(f"{w:x}" for w in c) + "\n"
+                         for t, c, d in pairs))
+    r = subprocess.run([str(exe), str(f)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    got = [tuple(map(int, x.split())) for x in r.stdout.splitlines()]
+    assert got == [(int(O.exhaustive(t, c, d)), O.flagdiff(t, c)) for t, c, d in pairs]
+    assert any(g[0] for g in got)

@@ -713,6 +713,18 @@ bool ExhaustiveCheckMasked(const Seq& target, const Seq& cand, FlagMask deadFlag
   return ExhaustiveCheckBatch({target}, {cand}, deadFlags)[0] != 0;
 }
 
+uint8_t FlagDiff(const Seq& target, const Seq& cand) {
+  if (target.empty() || target.size() > 4 || cand.empty() || cand.size() > 3)
+    throw Error(Z80B_EINVAL, "FlagDiff: sequence lengths 1..4 (target), 1..3 (candidate)");
+  uint32_t tw[4] = {0, 0, 0, 0}, cw[4] = {0, 0, 0, 0};
+  for (size_t k = 0; k < target.size(); k++) tw[k] = target[k].packed();
+  for (size_t k = 0; k < cand.size(); k++) cw[k] = cand[k].packed();
+  const uint8_t tl = uint8_t(target.size()), cl = uint8_t(cand.size());
+  uint8_t bits = 0, fd = 0;
+  check(z80b_verify_pairs(context(), tw, &tl, cw, &cl, 4, 1, nullptr, 1u, &bits, &fd), "z80b_verify_pairs");
+  return fd;
+}
+
 bool ShouldPrune(const Seq& s) {
   const auto w = pack(s);
   return z80b_should_prune(w.data(), uint32_t(w.size())) == 1;

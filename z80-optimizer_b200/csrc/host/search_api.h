@@ -147,6 +147,11 @@ bool ExhaustiveCheckMasked(const Seq& target, const Seq& cand, FlagMask deadFlag
 // Batched form of the two above: verdict per pair (the verify-jsonl path).
 std::vector<uint8_t> ExhaustiveCheckBatch(const std::vector<Seq>& targets, const std::vector<Seq>& cands,
                                           FlagMask deadFlags);
+// FlagDiff (verifier.go:658-673), computed on the device: the flag bits in
+// which target and candidate differ over the QuickCheck vectors (0 when a
+// register differs).  With ExhaustiveCheck[Masked] it is what the STOKE
+// search (pkg/stoke/search.go:108-117) asks of the verifier.
+uint8_t FlagDiff(const Seq& target, const Seq& cand);
 bool ShouldPrune(const Seq& s);
 bool ParseAssembly(const std::string& text, Seq* out);      // cmd/z80opt/main.go:325-397
 bool ParseDeadFlags(const std::string& text, FlagMask* out);  // cmd/z80opt/main.go:305-322
