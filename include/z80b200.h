@@ -211,6 +211,7 @@ int z80b_exhaustive_noalloc(int device, const uint32_t* tgt, const uint8_t* tlen
 #define Z80B_OPT_EXH_CHUNK_BLOCKS 2 /* A-blocks (256 states) per work chunk: 1..4096 */
 #define Z80B_OPT_STREAM_PRIORITY 3  /* the context's stream: -1 high, 0 default, 1 low priority */
 #define Z80B_OPT_QC_INDEX 4         /* QuickCheck through the pool's bucket index: 1 (default) or 0 (scan every candidate) */
+#define Z80B_OPT_XINDEP_BITS 5      /* A-independent sweeps bit-sliced (1, default) or one state per lane slot (0) */
 int z80b_set_option(z80b_ctx* ctx, int option, int value);
 int z80b_get_option(const z80b_ctx* ctx, int option, int* value);
 

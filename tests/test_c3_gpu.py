@@ -69,3 +69,30 @@ def test_streaming_answers_equal_final_rules(ctx):
         by_t.setdefault(r.target_index, []).append(r.key())
     for t, keys in events:
         assert keys == by_t.get(t, []), t
+
+
+@pytest.mark.parametrize("xbits", [1, 0])
+def test_a_independent_sweep_kernels_keep_parity(ctx, O, xbits):
+    """Both A-independent sweep kernels (Z80B_OPT_XINDEP_BITS = 1: bit-sliced,
+    32 blocks per lane word, the default; 0: one state per lane slot): the C3
+    sample's rules and 'checked' counter, and a C2 sample against the
+    oracle."""
+    import workloads
+    fx = fixture()
+    old = ctx.get_option(z80b.OPT_XINDEP_BITS)
+    ctx.set_option(z80b.OPT_XINDEP_BITS, xbits)
+    try:
+        rules, st = run(ctx, fx)
+        targets = workloads.to_lists(workloads.c2_subset(3000, seed=12))
+        r2, st2 = ctx.search(targets, dead_flags=0xFF)
+    finally:
+        ctx.set_option(z80b.OPT_XINDEP_BITS, old)
+    got = [tuple([k[0], tuple(k[1]), tuple(k[2])] + list(k[3:])) for k in dev_keys(rules)]
+    want = [tuple([r[0], tuple(r[1]), tuple(r[2])] + list(r[3:])) for r in fx["rules"]]
+    assert got == want
+    assert st.checked_ref == fx["checked"]
+    exp, checked = O.search(targets, 1, dead=0xFF)
+    key = lambda r: (r.target_index, tuple(r.src[:r.src_len]), tuple(r.rep[:r.rep_len]), r.bytes_saved,
+                     r.cycles_saved, r.dead_flags)
+    assert [key(r) for r in r2] == [key(r) for r in exp]
+    assert st2.checked_ref == checked

@@ -153,6 +153,7 @@ struct z80b_ctx {
   int chunk_blocks = 32;      // A-blocks per ExhaustiveCheck work chunk
   int priority = 0;           // Z80B_OPT_STREAM_PRIORITY
   int qc_index = 1;           // Z80B_OPT_QC_INDEX
+  int xbits = 1;              // Z80B_OPT_XINDEP_BITS
 };
 
 namespace {
@@ -651,6 +652,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
     R.counter = ctx->counter.as<unsigned long long>();
     R.states = ctx->states.as<unsigned long long>();
     R.chunk_blocks = uint32_t(ctx->chunk_blocks);
+    R.xunit = ctx->xbits ? kXBitsBlocks : kXScalarBlocks;
     if (nsurv) {
       for (;;) {
         CK(cudaMemsetAsync(R.npairs, 0, 4, s));
@@ -776,6 +778,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
     R.counter = ctx->counter.as<unsigned long long>();
     R.states = ctx->states.as<unsigned long long>();
     R.chunk_blocks = uint32_t(ctx->chunk_blocks);
+    R.xunit = ctx->xbits ? kXBitsBlocks : kXScalarBlocks;
     if (S) {
       launch_surv_targets(q, n, ctx->surv_target.as<uint32_t>(), s);
       CKR(check_launch(ctx, "surv_targets"));
@@ -1338,6 +1341,10 @@ int z80b_set_option(z80b_ctx* ctx, int option, int value) {
       if (value != 0 && value != 1) return fail(ctx, Z80B_EINVAL, "QuickCheck index option must be 0 or 1");
       ctx->qc_index = value;
       return Z80B_OK;
+    case Z80B_OPT_XINDEP_BITS:
+      if (value != 0 && value != 1) return fail(ctx, Z80B_EINVAL, "A-independent sweep option must be 0 or 1");
+      ctx->xbits = value;
+      return Z80B_OK;
   }
   return fail(ctx, Z80B_EINVAL, "unknown option %d", option);
 }
@@ -1349,6 +1356,7 @@ int z80b_get_option(const z80b_ctx* ctx, int option, int* value) {
     case Z80B_OPT_EXH_CHUNK_BLOCKS: *value = ctx->chunk_blocks; return Z80B_OK;
     case Z80B_OPT_STREAM_PRIORITY: *value = ctx->priority; return Z80B_OK;
     case Z80B_OPT_QC_INDEX: *value = ctx->qc_index; return Z80B_OK;
+    case Z80B_OPT_XINDEP_BITS: *value = ctx->xbits; return Z80B_OK;
   }
   return Z80B_EINVAL;
 }

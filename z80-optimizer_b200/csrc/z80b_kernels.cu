@@ -139,9 +139,10 @@ __device__ __forceinline__ bool pair_xindep(const DevTargets& T, uint32_t t, con
 // lane takes 32 consecutive values of A of one block.
 constexpr unsigned long long kBitsBlocks = 4;
 constexpr int kBitsWords = 88;  // planes of one ZB (A F B C D E H L M: 8 each, SP: 16)
-__device__ __forceinline__ unsigned long long pair_units(unsigned long long nblocks, uint32_t keepR) {
-  return (keepR & kXIndep) ? (nblocks + kUnitBlocks - 1) / kUnitBlocks
-                           : (nblocks + kBitsBlocks - 1) / kBitsBlocks;
+__device__ __forceinline__ unsigned long long pair_units(unsigned long long nblocks, uint32_t keepR,
+                                                         uint32_t xunit) {
+  const unsigned long long xu = xunit ? xunit : kUnitBlocks;
+  return (keepR & kXIndep) ? (nblocks + xu - 1) / xu : (nblocks + kBitsBlocks - 1) / kBitsBlocks;
 }
 constexpr unsigned long long kMaxChunks = 1ull << 20;
 constexpr int kChunksPerWarp = 16;
@@ -150,7 +151,7 @@ constexpr int kChunksPerWarp = 16;
 __device__ __forceinline__ unsigned long long chunks_for(unsigned long long nb, uint32_t cb);
 // Chunks of pair p in the numbering of its class (zero in the other one).
 __device__ __forceinline__ void set_chunks(const RoundBuf& R, uint32_t p, const PairRec& pr) {
-  const unsigned long long c = chunks_for(pair_units(pr.nblocks, pr.keepR), R.chunk_blocks);
+  const unsigned long long c = chunks_for(pair_units(pr.nblocks, pr.keepR, R.xunit), R.chunk_blocks);
   const bool xind = (pr.keepR & kXIndep) != 0;
   R.nchunks[p] = xind ? 0ull : c;
   R.nchunks_x[p] = xind ? c : 0ull;
@@ -695,6 +696,112 @@ __device__ __forceinline__ bool bits_unit(unsigned long long u, unsigned long lo
   return valid && zb_diff(z, sm, keepF, keepR) != 0u;
 }
 
+// A-independent sweeps, bit-sliced: lane l of a unit takes the 32 A-blocks
+// u*1024 + 32l .. +31 as one state word (block j in bit j), first at A = 0,
+// then at A = 1 (two values decide these pairs).  In an aligned group of 32
+// blocks only the low 5 bits of the block index change, and they move one
+// thing: the last swept register's low 5 bits (full sweep), its 32
+// representative values (reduced sweep), SP's 16 representatives and one bit
+// of the next field (SP sweep), or the carry (no extra register).
+__device__ __forceinline__ void zb_set_reg(ZB& z, int r, const uint32_t (&pl)[8]) {
+  switch (r) {
+    case 0: zb_copy8(z.b, pl); break;
+    case 1: zb_copy8(z.c, pl); break;
+    case 2: zb_copy8(z.d, pl); break;
+    case 3: zb_copy8(z.e, pl); break;
+    case 4: zb_copy8(z.h, pl); break;
+    case 5: zb_copy8(z.l, pl); break;
+    case 6: zb_copy8(z.m, pl); break;
+    default: break;
+  }
+}
+__device__ __forceinline__ bool xbits_unit(unsigned long long u, unsigned long long nblocks, bool spw, bool reduced,
+                                           int nx, int fw, const int (&slot)[7], int rlast, uint32_t pw, int tl,
+                                           int cl, uint32_t keepF, uint32_t keepR, uint32_t* sm) {
+  const unsigned lane = lane_id();
+  const unsigned long long g0 = u * kXBitsBlocks + (unsigned long long)lane * 32ull;
+  const uint32_t valid = g0 >= nblocks ? 0u
+                         : (nblocks - g0 >= 32ull ? 0xFFFFFFFFu : ((1u << uint32_t(nblocks - g0)) - 1u));
+  Z80S x;
+  decode_block<false>(g0 < nblocks ? g0 : 0ull, spw, reduced, nx, fw, slot, x);
+  // planes of what the low 5 bits of the block index move
+  uint32_t vp[8], spp[16];
+  uint32_t fp0 = 0u;
+#pragma unroll
+  for (int i = 0; i < 16; i++) spp[i] = 0u;
+  if (spw) {
+    // SP: state j takes representative j mod 16; bit 4: the last field's x
+    // (even x0 in states 0-15, x0 + 1 in 16-31) or, with no field, the carry
+#pragma unroll
+    for (int i = 0; i < 16; i++) spp[i] = __ballot_sync(kFull, (g_repsp[lane & 15u] >> i) & 1u);
+    const uint32_t x0 = uint32_t(g0 >> 4) & 31u;
+    const uint32_t lo = g_rep[x0], hi = g_rep[(x0 + 1u) & 31u];
+#pragma unroll
+    for (int i = 0; i < 8; i++)
+      vp[i] = (((lo >> i) & 1u) ? 0x0000FFFFu : 0u) | (((hi >> i) & 1u) ? 0xFFFF0000u : 0u);
+    fp0 = 0xFFFF0000u;
+  } else if (reduced) {
+    // the last field's 32 representatives, state j = representative j
+#pragma unroll
+    for (int i = 0; i < 8; i++) vp[i] = __ballot_sync(kFull, (g_rep[lane] >> i) & 1u);
+  } else {
+    // full sweep: the last field's low 5 bits count the states, the rest is
+    // the group's value; with no extra register the carry is bit 0
+    uint32_t v = 0u;
+    switch (rlast) {
+      case 0: v = x.b; break;
+      case 1: v = x.c; break;
+      case 2: v = x.d; break;
+      case 3: v = x.e; break;
+      case 4: v = x.h; break;
+      case 5: v = x.l; break;
+      case 6: v = x.m; break;
+      default: break;
+    }
+    vp[0] = 0xAAAAAAAAu;
+    vp[1] = 0xCCCCCCCCu;
+    vp[2] = 0xF0F0F0F0u;
+    vp[3] = 0xFF00FF00u;
+    vp[4] = 0xFFFF0000u;
+#pragma unroll
+    for (int i = 5; i < 8; i++) vp[i] = ((v >> i) & 1u) ? kZBOnes : 0u;
+    fp0 = 0xAAAAAAAAu;
+  }
+  ZB z;
+  bool bad = false;
+#pragma unroll 1
+  for (uint32_t abit = 0; abit < 2u; abit++) {
+    auto init = [&]() {
+      zb_set8(z.a, abit);
+      zb_set8(z.f, x.f);
+      zb_set8(z.b, x.b);
+      zb_set8(z.c, x.c);
+      zb_set8(z.d, x.d);
+      zb_set8(z.e, x.e);
+      zb_set8(z.h, x.h);
+      zb_set8(z.l, x.l);
+      zb_set8(z.m, x.m);
+#pragma unroll
+      for (int i = 0; i < 16; i++) z.sp[i] = spw ? spp[i] : (((x.sp >> i) & 1u) ? kZBOnes : 0u);
+      if (nx >= 1) zb_set_reg(z, rlast, vp);
+      else z.f[0] = fp0;
+    };
+    init();
+#pragma unroll 1
+    for (int st = 0; st < tl + cl; st++) {
+      if (st == cl) {
+        zb_save(z, sm);
+        init();
+      }
+      const int src = st < cl ? tl + st : st - cl;
+      const uint32_t w = __shfl_sync(kFull, pw, src);
+      zb_step(z, w & 0xFFFFu, w >> 16);
+    }
+    bad = bad || (zb_diff(z, sm, keepF, keepR) & valid) != 0u;
+  }
+  return bad;
+}
+
 // One unit (128 A-blocks at A = 0, 1) of an A-independent sweep, for the
 // A-independent sweep kernel; kept out of line (that kernel compiles without
 // register spills at every K this way).
@@ -726,14 +833,16 @@ __device__ __noinline__ bool xindep_unit(unsigned long long first, unsigned long
   return bad;
 }
 
-// One kernel per pair class: XI = false runs the bit-sliced pairs, XI = true
-// the A-independent ones (K states per lane per dispatch); each draws chunks
+// One kernel per pair class: CLS 0 runs the bit-sliced pairs (outputs
+// depend on A), CLS 1 the A-independent ones (K states per lane per
+// dispatch), CLS 2 the A-independent ones bit-sliced; each class draws chunks
 // from its own numbering and dispenser.  Kept apart so that neither path's
 // registers weigh on the other.
-template <int K, bool XI>
+template <int K, int CLS>
 __global__ void __launch_bounds__(kBlock, 1) k_exhaustive(DevTargets T, DevPool P, RoundBuf R, uint32_t npairs,
                                                        unsigned long long total) {
   static_assert(K == 1 || K == 2 || K == 4 || K == 8, "K divides 8");
+  constexpr bool XI = CLS != 0;
   const unsigned long long* __restrict__ cbase = XI ? R.cbase_x : R.cbase;
   const unsigned lane = lane_id();
   unsigned long long my_states = 0, my_eval = 0;
@@ -758,7 +867,7 @@ __global__ void __launch_bounds__(kBlock, 1) k_exhaustive(DevTargets T, DevPool 
     if (__shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0))
       continue;
     const PairRec pr = R.pairs[p];
-    const unsigned long long nunits = pair_units(pr.nblocks, pr.keepR);
+    const unsigned long long nunits = pair_units(pr.nblocks, pr.keepR, R.xunit);
     const unsigned long long nch = (p + 1 < npairs ? cbase[p + 1] : total) - cbase[p];
     const unsigned long long upc = (nunits + nch - 1) / nch;
     const unsigned long long j = k - cbase[p];
@@ -811,6 +920,25 @@ __global__ void __launch_bounds__(kBlock, 1) k_exhaustive(DevTargets T, DevPool 
         if ((u & 15ull) == 15ull &&
             __shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0))
           break;
+      }
+    } else if constexpr (CLS == 2) {
+      // Unit = 1,024 A-blocks, 32 per lane, each at A = 0 and A = 1.
+      extern __shared__ uint32_t zsm[];
+      uint32_t* sm = zsm + (threadIdx.x >> 5) * (kBitsWords * 32) + lane;
+      int rlast = -1;  // the register of the last swept field (the fastest)
+#pragma unroll
+      for (int r = 0; r < 7; r++)
+        if (slot[r] == nx - 1) rlast = r;
+      for (unsigned long long u = u0; u < u1; u++) {
+        const unsigned long long first = u * kXBitsBlocks;
+        const unsigned long long nb = (pr.nblocks - first < kXBitsBlocks) ? pr.nblocks - first : kXBitsBlocks;
+        bad = xbits_unit(u, pr.nblocks, spw, reduced, nx, fw, slot, rlast, pw, int(tl), int(cl), pr.keepF,
+                         pr.keepR, sm) ||
+              bad;
+        my_states += 256ull * nb;
+        my_eval += 2ull * nb;
+        if (__any_sync(kFull, bad)) break;
+        if (__shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0)) break;
       }
     } else {
       // Unit = 128 A-blocks, each evaluated at A = 0 and A = 1: state slot s
@@ -1395,16 +1523,16 @@ void launch_pairs_from_survivors(const DevTargets& T, const DevPool& P, const QC
   if (!nsurv) return;
   k_pairs_from_survivors<<<grid_for(nsurv, 256), 256, 0, s>>>(T, P, q, midpass, nsurv, surv_target, R);
 }
-template <int K, bool XI>
+template <int K, int CLS>
 void launch_exhaustive_k(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
                          unsigned long long total, cudaStream_t s) {
-  // shared memory (bit-sliced class): the candidate's output planes,
+  // shared memory (bit-sliced kernels): the candidate's output planes,
   // kBitsWords words per lane
-  constexpr int smem = XI ? 0 : kBlock * kBitsWords * 4;
+  constexpr int smem = CLS == 1 ? 0 : kBlock * kBitsWords * 4;
   static int per_sm = 0;
   if (!per_sm) {
-    if (smem) cudaFuncSetAttribute(k_exhaustive<K, XI>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_exhaustive<K, XI>, kBlock, smem);
+    if (smem) cudaFuncSetAttribute(k_exhaustive<K, CLS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_exhaustive<K, CLS>, kBlock, smem);
     if (per_sm < 1) per_sm = 1;
   }
   // resident blocks, or more when the chunks exceed kChunksPerWarp per warp
@@ -1415,7 +1543,7 @@ void launch_exhaustive_k(const DevTargets& T, const DevPool& P, const RoundBuf& 
   const unsigned long long cover = (total + wpb * kChunksPerWarp - 1) / (wpb * kChunksPerWarp);
   if (grid < cover) grid = cover;
   if (grid > 0x7FFFFFFFull) grid = 0x7FFFFFFFull;
-  k_exhaustive<K, XI><<<unsigned(grid), kBlock, smem, s>>>(T, P, R, npairs, total);
+  k_exhaustive<K, CLS><<<unsigned(grid), kBlock, smem, s>>>(T, P, R, npairs, total);
 }
 
 int launch_exhaustive(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
@@ -1423,15 +1551,19 @@ int launch_exhaustive(const DevTargets& T, const DevPool& P, const RoundBuf& R, 
   if (!npairs) return 0;
   int n = 0;
   if (total_b) {
-    launch_exhaustive_k<1, false>(T, P, R, npairs, total_b, s);
+    launch_exhaustive_k<1, 0>(T, P, R, npairs, total_b, s);
     n++;
   }
   if (total_x) {
-    switch (k) {
-      case 1: launch_exhaustive_k<1, true>(T, P, R, npairs, total_x, s); break;
-      case 2: launch_exhaustive_k<2, true>(T, P, R, npairs, total_x, s); break;
-      case 8: launch_exhaustive_k<8, true>(T, P, R, npairs, total_x, s); break;
-      default: launch_exhaustive_k<4, true>(T, P, R, npairs, total_x, s); break;
+    if (R.xunit == kXBitsBlocks) {
+      launch_exhaustive_k<1, 2>(T, P, R, npairs, total_x, s);
+    } else {
+      switch (k) {
+        case 1: launch_exhaustive_k<1, 1>(T, P, R, npairs, total_x, s); break;
+        case 2: launch_exhaustive_k<2, 1>(T, P, R, npairs, total_x, s); break;
+        case 8: launch_exhaustive_k<8, 1>(T, P, R, npairs, total_x, s); break;
+        default: launch_exhaustive_k<4, 1>(T, P, R, npairs, total_x, s); break;
+      }
     }
     n++;
   }

@@ -47,6 +47,10 @@ struct Lanes {
   uint8_t* spec;     // [2n] log2 of the lane's survivor window in the next round
 };
 
+// A-independent sweeps: 128 A-blocks per unit in the scalar kernel, 1,024
+// (32 per lane, 32 states per lane word) in the bit-sliced one.
+constexpr uint32_t kXScalarBlocks = 128, kXBitsBlocks = 1024;
+
 // Survivor windows: a lane whose survivors keep failing ExhaustiveCheck
 // takes 1, 2, 4, ... of its next survivors (in enumeration order) into one
 // round, up to these caps; the first one that passes wins, as if they had
@@ -71,6 +75,8 @@ struct RoundBuf {
   unsigned long long* counter;     // chunk dispensers: [0] bit-sliced class, [1] A-independent class
   unsigned long long* states;      // [2]: states of the reference's sweeps covered, states evaluated
   uint32_t chunk_blocks;           // A-blocks per work chunk
+  uint32_t xunit;                  // A-blocks per unit of an A-independent sweep: kXBitsBlocks
+                                   // (bit-sliced kernel), else (0 too) the scalar kernel's 128
 };
 
 // Length-2 candidate pass (pair pool): bucket indexes and per-lane slots.

@@ -103,7 +103,7 @@ EXPORTS = [
     "z80b_search_cb",
 ]
 RULE_CB = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32)
-OPT_EXH_LANE_STATES, OPT_EXH_CHUNK_BLOCKS, OPT_STREAM_PRIORITY, OPT_QC_INDEX = 1, 2, 3, 4
+OPT_EXH_LANE_STATES, OPT_EXH_CHUNK_BLOCKS, OPT_STREAM_PRIORITY, OPT_QC_INDEX, OPT_XINDEP_BITS = 1, 2, 3, 4, 5
 JOB_NO_EXHAUSTIVE = 1
 
 
