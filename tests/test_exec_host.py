@@ -26,3 +26,19 @@ def test_bitsliced_step_matches_scalar(tmp_path):
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.startswith("OK")
+
+
+def test_bitsliced_a_independent_layout(tmp_path):
+    """The planes the bit-sliced A-independent sweep builds for a group of 32
+    A-blocks hold each block's decoded initial state (every sweep shape), and
+    sweeping random A-independent pairs that way at A = 0 and 1 reproduces
+    the oracle's ExhaustiveCheck[Masked] verdicts."""
+    exe = tmp_path / "xbits_check"
+    srcs = [os.path.join(ROOT, "tests", "native", "xbits_check.cpp"),
+            os.path.join(ROOT, "z80-optimizer_b200", "csrc", "z80_tables.cpp"),
+            os.path.join(ROOT, "oracle", "z80_oracle_isa_cpu.cpp"),
+            os.path.join(ROOT, "oracle", "z80_oracle_search.cpp")]
+    subprocess.run(["g++", "-O2", "-std=c++17", "-o", str(exe)] + srcs + ["-lpthread"], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.startswith("OK")
