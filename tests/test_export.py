@@ -136,3 +136,57 @@ def test_enumerate_flag_checks():
     assert r.returncode == 1 and "--max-target must be 2 or 3" in r.stderr
     r = run("enumerate", "--no-exhaust")
     assert r.returncode == 1 and "--no-exhaust needs --gpu" in r.stderr
+
+
+def test_json_reader_against_python_json(tmp_path):
+    """ReadJSON against Python's json module on generated rule files: random
+    strings (escapes, control characters, non-ASCII, surrogate pairs),
+    integers, nulls, unknown nested fields, random whitespace; and broken
+    files are rejected."""
+    import random
+    exe = _native(tmp_path, "json_echo")
+    rng = random.Random(5)
+    alphabet = "ABC :,'\"\\/\t\né中\U0001F600\x01"
+    fields = ["source_asm", "replacement_asm", "source_bytes", "replacement_bytes", "bytes_saved", "cycles_saved",
+              "dead_flags", "dead_flag_desc"]
+
+    def rstr():
+        return "".join(rng.choice(alphabet) for _ in range(rng.randint(0, 12)))
+
+    for case in range(40):
+        rules = []
+        for _ in range(rng.randint(0, 6)):
+            obj = {}
+            for k in fields:
+                if rng.random() < 0.8:
+                    if k.endswith(("bytes", "saved")):
+                        obj[k] = rng.choice([None, rng.randint(-2**31, 2**31 - 1)])
+                    else:
+                        obj[k] = rng.choice([None, rstr()])
+            if rng.random() < 0.5:
+                obj["extra"] = {"x": [1, 2.5, {"y": None}], "z": rstr()}
+            items = list(obj.items())
+            rng.shuffle(items)
+            rules.append(dict(items))
+        text = json.dumps(rules, ensure_ascii=rng.random() < 0.5, indent=rng.choice([None, 1, 4]))
+        f = tmp_path / f"c{case}.json"
+        f.write_bytes(text.encode("utf-8"))
+        r = subprocess.run([str(exe), str(f)], capture_output=True, text=True, timeout=60)
+        assert r.returncode == 0
+        want = []
+        for obj in rules:
+            row = []
+            for k in fields:
+                v = obj.get(k)
+                if k.endswith(("bytes", "saved")):
+                    row.append(str(v if v is not None else 0))
+                else:
+                    row.append((v or "").encode("utf-8").hex())
+            want.append("\t".join(row) + "\t")
+        assert r.stdout.splitlines() == want, (case, text)
+    for bad in ['[{"source_asm": "A"}', '[{"bytes_saved": 1e3}]', '[{"source_asm": "\\x"}]', '{}', '[1]',
+                '[{"source_asm": "a\x01"}]', '[] x', '[{"cycles_saved": 99999999999}]']:
+        f = tmp_path / "bad.json"
+        f.write_bytes(bad.encode())
+        r = subprocess.run([str(exe), str(f)], capture_output=True, text=True, timeout=60)
+        assert r.stdout.strip() == "ERROR", bad
