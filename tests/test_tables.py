@@ -4,6 +4,8 @@ import json
 import os
 import random
 
+import pytest
+
 import z80b
 import workloads
 from conftest import ROOT
@@ -57,8 +59,14 @@ def test_enumerate_counts():
 
 def test_parse_and_flags(O):
     for text in ["SUB A : LD A, 0", "AND 0FFh", "ld a, 0x00 : neg", "LD (HL), 12h", "BIT 7, (HL)",
-                 "EX DE, HL", "ADC HL, SP", "SLL (HL)"]:
+                 "EX DE, HL", "ADC HL, SP", "SLL (HL)", "LD A, 0A5h : LD C, 255"]:
         assert z80b.parse_assembly(text) == O.parse_assembly(text), text
+    # as in cmd/z80opt/main.go:348-395, a 16-bit immediate never parses (the
+    # mnemonic's "nn" leaves an "N" in the prefix it matches against)
+    for text in ["LD HL, 0C000h", "LD BC, 1234h", "LD SP, 0", "FROB A"]:
+        assert O.parse_assembly(text) is None, text
+        with pytest.raises(z80b.Z80BError):
+            z80b.parse_assembly(text)
     for s in ["none", "undoc", "all", "0x13", "FF", "0x00"]:
         assert z80b.parse_dead_flags(s) == O.parse_dead_flags(s)
     for m in range(256):
