@@ -1,12 +1,15 @@
-// Host check of the block layout behind the bit-sliced A-independent sweep
-// (xbits_unit in z80b_kernels.cu): for every sweep shape, the state planes
-// the kernel builds for an aligned group of 32 A-blocks (the moving field's
-// planes from counting patterns, transposed representative tables or
-// constants) hold, in bit j, exactly the initial state of block g0 + j as
-// the block decoder defines it; and sweeping random A-independent pairs this
-// way at A = 0 and 1 gives the CPU oracle's ExhaustiveCheck[Masked] verdict.
-// The decoder and the plane construction are restated here from the kernel
-// (warp ballots become loops over j).  Built and run by tests/test_exec_host.py.
+// Host check of the layouts behind the two bit-sliced sweeps
+// (z80b_kernels.cu).  A-independent pairs (xbits_unit): for every sweep
+// shape, the state planes the kernel builds for an aligned group of 32
+// A-blocks (the moving field's planes from counting patterns, transposed
+// representative tables or constants) hold, in bit j, exactly the initial
+// state of block g0 + j as the block decoder defines it, and sweeping random
+// A-independent pairs this way at A = 0 and 1 gives the CPU oracle's
+// ExhaustiveCheck[Masked] verdict.  A-dependent pairs (bits_unit): lane l of
+// a unit takes block 4u + l/8 and A = 32(l % 8) .. +31, and sweeping random
+// A-dependent pairs that way gives the oracle's verdict too.  The decoder
+// and the plane construction are restated here from the kernel (warp ballots
+// become loops over j).  Built and run by tests/test_exec_host.py.
 #include <cstdio>
 #include <random>
 #include <vector>
@@ -224,6 +227,81 @@ int main() {
     std::printf("too few pairs (%d) or equivalences (%d)\n", pairs, equal);
     return 1;
   }
-  std::printf("OK %lld states, %d pairs, %d equivalent verdicts\n", checked, pairs, equal);
+  // 3. A-dependent pairs: every block at all 256 values of A, 32 per word
+  // (lane l of a unit: block 4u + l/8, A from 32(l % 8)), against the oracle
+  int dpairs = 0, dequal = 0;
+  for (int trial = 0; trial < 400000 && dpairs < 1500; trial++) {
+    const int tn = 1 + int(rng() % 2);
+    uint32_t tw[2], cw[2];
+    orc::Instruction ti[2], ci[2];
+    for (int i = 0; i < tn; i++) {
+      ti[i] = I[rng() % I.size()];
+      tw[i] = uint32_t(ti[i].op) | uint32_t(ti[i].imm) << 16;
+    }
+    const int mode = int(rng() % 3);
+    int cl = 1 + int(rng() % 2);
+    for (int i = 0; i < cl; i++) ci[i] = I[rng() % I.size()];
+    if (mode == 1 || (mode == 2 && tn == 2)) {
+      cl = tn;
+      ci[0] = ti[mode == 2 ? 1 : 0];
+      ci[1] = ti[mode == 2 ? 0 : 1];
+    }
+    for (int i = 0; i < cl; i++) cw[i] = uint32_t(ci[i].op) | uint32_t(ci[i].imm) << 16;
+    if (seq_aflow(tw, tn) && seq_aflow(cw, cl)) continue;  // A-dependent pairs only
+    const uint16_t reads = uint16_t(seq_reads(tw, tn) | seq_reads(cw, cl));
+    const Shape s = shape_of(reads);
+    if (s.nblocks > (1u << 12)) continue;
+    dpairs++;
+    for (uint8_t dead : {uint8_t(0x00), uint8_t(0xFF)}) {
+      const uint32_t keepF = uint8_t(~dead);
+      bool bad = false;
+      for (uint64_t blk = 0; blk < s.nblocks && !bad; blk++) {
+        const Z80S x = decode(blk, s);
+        for (uint32_t a0 = 0; a0 < 256 && !bad; a0 += 32) {
+          ZB z;
+          z.a[0] = 0xAAAAAAAAu;
+          z.a[1] = 0xCCCCCCCCu;
+          z.a[2] = 0xF0F0F0F0u;
+          z.a[3] = 0xFF00FF00u;
+          z.a[4] = 0xFFFF0000u;
+          for (int i = 5; i < 8; i++) z.a[i] = ((a0 >> i) & 1u) ? kZBOnes : 0u;
+          zb_set8(z.f, x.f);
+          zb_set8(z.b, x.b);
+          zb_set8(z.c, x.c);
+          zb_set8(z.d, x.d);
+          zb_set8(z.e, x.e);
+          zb_set8(z.h, x.h);
+          zb_set8(z.l, x.l);
+          zb_set8(z.m, x.m);
+          for (int i = 0; i < 16; i++) z.sp[i] = ((x.sp >> i) & 1u) ? kZBOnes : 0u;
+          for (int j = 0; j < 32; j++) {
+            Z80S want = x;
+            want.a = a0 + uint32_t(j);
+            if (!same(zb_get(z, j), want)) {
+              std::printf("A-dependent layout mismatch: block %llu A %u\n", (unsigned long long)blk, a0 + j);
+              return 1;
+            }
+          }
+          ZB zc = z, zt = z;
+          for (int i = 0; i < cl; i++) zb_step(zc, cw[i] & 0xFFFFu, cw[i] >> 16);
+          for (int i = 0; i < tn; i++) zb_step(zt, tw[i] & 0xFFFFu, tw[i] >> 16);
+          bad = diff_mask(zc, zt, keepF) != 0;
+        }
+      }
+      const bool want = dead ? orc::ExhaustiveCheckMasked(ti, tn, ci, cl, dead) : orc::ExhaustiveCheck(ti, tn, ci, cl);
+      if (want != !bad) {
+        std::printf("A-dependent verdict mismatch: target %08x %08x (%d) candidate %08x %08x (%d) dead %02x\n", tw[0],
+                    tn > 1 ? tw[1] : 0, tn, cw[0], cl > 1 ? cw[1] : 0, cl, dead);
+        return 1;
+      }
+      dequal += want ? 1 : 0;
+    }
+  }
+  if (dpairs < 500 || dequal < 50) {
+    std::printf("too few A-dependent pairs (%d) or equivalences (%d)\n", dpairs, dequal);
+    return 1;
+  }
+  std::printf("OK %lld states, %d A-independent pairs (%d equivalent verdicts), %d A-dependent pairs (%d)\n", checked,
+              pairs, equal, dpairs, dequal);
   return 0;
 }

@@ -28,11 +28,12 @@ def test_bitsliced_step_matches_scalar(tmp_path):
     assert r.stdout.startswith("OK")
 
 
-def test_bitsliced_a_independent_layout(tmp_path):
+def test_bitsliced_sweep_layouts(tmp_path):
     """The planes the bit-sliced A-independent sweep builds for a group of 32
     A-blocks hold each block's decoded initial state (every sweep shape), and
-    sweeping random A-independent pairs that way at A = 0 and 1 reproduces
-    the oracle's ExhaustiveCheck[Masked] verdicts."""
+    sweeping random pairs the way both bit-sliced kernels lay them out
+    (A-independent: 32 blocks per word at A = 0 and 1; A-dependent: 32 values
+    of A per word) reproduces the oracle's ExhaustiveCheck[Masked] verdicts."""
     exe = tmp_path / "xbits_check"
     srcs = [os.path.join(ROOT, "tests", "native", "xbits_check.cpp"),
             os.path.join(ROOT, "z80-optimizer_b200", "csrc", "z80_tables.cpp"),
