@@ -100,6 +100,35 @@ int main() {
     }
     CHECK(seen.size() == 3000);
   }
+  // length 1: the unpruned instructions of the range; a sample as large as
+  // the range is the whole range
+  {
+    const uint64_t t1 = z80b_enumerate(pool.data(), P, 1, nullptr, 0);
+    std::vector<uint32_t> r1(t1);
+    z80b_enumerate(pool.data(), P, 1, r1.data(), t1);
+    CHECK(collect(1, 0, -1, 0, 0, 100) == r1);
+    CHECK(collect(1, 0, -1, t1 + 5, 3, 100) == r1);
+    std::vector<uint32_t> part;
+    for (uint32_t w : r1)
+      for (uint32_t i = 10; i < 20; i++)
+        if (pool[i] == w) part.push_back(w);
+    CHECK(collect(1, 10, 20, 0, 0, 3) == part);
+  }
+  // a length-2 sample of a sub-range comes from that range only, in order,
+  // without repeats
+  {
+    const std::vector<uint32_t> sub = collect(2, 40, 45, 0, 0, 1u << 20);
+    const std::vector<uint32_t> smp = collect(2, 40, 45, 700, 8, 64);
+    CHECK(smp.size() == 1400);
+    size_t pos = 0;
+    bool ordered = true;
+    for (size_t i = 0; i < smp.size(); i += 2) {
+      while (pos < sub.size() && !(sub[pos] == smp[i] && sub[pos + 1] == smp[i + 1])) pos += 2;
+      if (pos >= sub.size()) ordered = false;
+      pos += 2;
+    }
+    CHECK(ordered);
+  }
   // bad arguments
   bool threw = false;
   try {
