@@ -107,3 +107,19 @@ def test_a_dependence_classes_against_oracle(tmp_path):
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.startswith("OK")
+
+
+def test_register_renaming_against_oracle(tmp_path):
+    """op_rename: for every opcode and permutation of B..L, the renamed
+    opcode run on the permuted state gives the permuted result (oracle's
+    Exec); instructions with only 8-bit register operands always rename."""
+    import subprocess
+    exe = tmp_path / "rename_check"
+    srcs = [os.path.join(ROOT, "tests", "native", "rename_check.cpp"),
+            os.path.join(ROOT, "z80-optimizer_b200", "csrc", "z80_tables.cpp"),
+            os.path.join(ROOT, "oracle", "z80_oracle_isa_cpu.cpp"),
+            os.path.join(ROOT, "oracle", "z80_oracle_search.cpp")]
+    subprocess.run(["g++", "-O2", "-std=c++17", "-o", str(exe)] + srcs + ["-lpthread"], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.startswith("OK")

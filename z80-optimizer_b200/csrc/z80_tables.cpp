@@ -250,6 +250,45 @@ uint32_t seq_aflow(const uint32_t* s, int n) {
   return a_is_x ? 3u : 1u;
 }
 const char* op_mnemonic(uint16_t op) { return tables().cat[op].mnem.c_str(); }
+
+int op_rename(uint16_t op, const uint8_t (&map)[6]) {
+  static const char* kRegs = "BCDEHL";
+  static const char* kPairs[3] = {"BC", "DE", "HL"};
+  const std::string& m = tables().cat[op].mnem;
+  std::string out;
+  int depth = 0;
+  for (size_t i = 0; i < m.size(); i++) {
+    const char ch = m[i];
+    if (ch == '(') depth++;
+    if (ch == ')') depth--;
+    const bool word_start = i == 0 || m[i - 1] == ' ' || m[i - 1] == ',';
+    if (depth == 0 && word_start) {
+      // a register pair operand
+      bool done = false;
+      for (int p = 0; p < 3 && !done; p++) {
+        if (m.compare(i, 2, kPairs[p]) == 0 && (i + 2 == m.size() || m[i + 2] == ',' || m[i + 2] == ' ')) {
+          const uint8_t hi = map[2 * p], lo = map[2 * p + 1];
+          if (hi % 2 != 0 || lo != hi + 1) return -1;  // not onto a pair in order
+          out += kPairs[hi / 2];
+          i += 1;
+          done = true;
+        }
+      }
+      if (done) continue;
+      // an 8-bit register operand (mnemonic words like "SLA" are longer)
+      const char* r = std::strchr(kRegs, ch);
+      if (r && *r && (i + 1 == m.size() || m[i + 1] == ',' || m[i + 1] == ' ')) {
+        out += kRegs[map[r - kRegs]];
+        continue;
+      }
+    }
+    out += ch;
+  }
+  if (out == m) return op;
+  for (int o = 0; o < kNumOps; o++)
+    if (tables().cat[o].mnem == out && op_table()[o].imm == op_table()[op].imm) return o;
+  return -1;
+}
 const uint8_t* op_encoding(uint16_t op, int* n) {
   *n = tables().cat[op].nenc;
   return tables().cat[op].enc;

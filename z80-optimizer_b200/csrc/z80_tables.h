@@ -27,6 +27,15 @@ const uint8_t* op_aclass();               // kNumOps entries
 // A; else 1 (A is overwritten) or 3 (A passes through to the output).
 uint32_t seq_aflow(const uint32_t* s, int n);
 const char* op_mnemonic(uint16_t op);     // "ADD A, n" style with placeholders
+// The instruction that does op's work with the 8-bit registers renamed:
+// register r (0..5 = B, C, D, E, H, L) plays the part of map[r] (map is a
+// permutation).  A, F, SP and the memory byte keep their parts; a register
+// pair that op uses as one (BC, DE, HL outside parentheses) must map onto a
+// pair in order.  Returns -1 when the catalog has no such instruction (HL as
+// the fixed operand of ADD/ADC/SBC HL, EX DE,HL or LD SP,HL renamed away, or
+// a pair split).  Memory operands ((HL), (BC), (DE)) stay as they are: the
+// step function's memory byte does not depend on the address registers.
+int op_rename(uint16_t op, const uint8_t (&map)[6]);
 const uint8_t* op_encoding(uint16_t op, int* n);
 std::string disassemble(uint32_t insn);   // catalog.go:73-127
 std::string disasm_seq(const uint32_t* seq, int n);  // " : " joined
