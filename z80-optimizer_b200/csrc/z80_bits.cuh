@@ -22,7 +22,7 @@ struct ZB {
 
 constexpr uint32_t kZBOnes = 0xFFFFFFFFu;
 
-#if defined(__CUDACC__)
+#if defined(__CUDA_ARCH__)  // device pass only: host compilers do not know the pragma
 #define ZB_UNROLL _Pragma("unroll")
 #else
 #define ZB_UNROLL

@@ -179,7 +179,7 @@ Z80_HD void z_sbchl(Z80S& s, uint32_t v) {
   M((base) + 4, h) M((base) + 5, l) M((base) + 6, a)
 
 // Applies a statement to every state S[0..K) (named s inside).
-#if defined(__CUDACC__)
+#if defined(__CUDA_ARCH__)  // device pass only: host compilers do not know the pragma
 #define Z80B_UNROLL _Pragma("unroll")
 #else
 #define Z80B_UNROLL

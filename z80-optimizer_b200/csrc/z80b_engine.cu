@@ -668,10 +668,10 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
         CKR(sweep_round(ctx, T, P, R, np));
         launch_round_resolve(R, np, q, L, kMaxSpec1, s);
         CKR(check_launch(ctx, "round_resolve"));
-        if (opts.rep) CKR(opts.rep->update(ctx, n, L, Lanes{nullptr, nullptr, nullptr}, opts.max_cand, false, false));
+        if (opts.rep) CKR(opts.rep->update(ctx, n, L, Lanes{}, opts.max_cand, false, false));
       }
     }
-    Lanes L2{nullptr, nullptr, nullptr};
+    Lanes L2{};
     unsigned long long pool2_enum = 0;
     if (opts.max_cand >= 2) {
       // Length-2 candidates for the lanes the length-1 pass left without a
