@@ -1,0 +1,178 @@
+// Host check of the compact-state mapping (op_regs, compact_map in
+// z80_tables.cpp).  (1) op_regs is sound: a register or the memory byte an
+// instruction does not name keeps its value and changes no other output,
+// for every opcode, every value of that field and sampled states and
+// immediates (oracle's Exec).  (2) For random pairs that compact_map
+// accepts, running the renamed programs on the renamed states over the
+// reference's whole ExhaustiveCheck sweep, comparing A, F (under the dead
+// flags) and the registers B, C only, gives the oracle's verdict for the
+// original pair.  Built and run by tests/test_tables.py.
+#include <cstdio>
+#include <random>
+
+#include "../../oracle/z80_oracle.h"
+#include "../../z80-optimizer_b200/csrc/z80_exec.cuh"
+#include "../../z80-optimizer_b200/csrc/z80_tables.h"
+
+using namespace z80b;
+
+static uint8_t* field(orc::State& s, int i) {
+  switch (i) {
+    case 0: return &s.B;
+    case 1: return &s.C;
+    case 2: return &s.D;
+    case 3: return &s.E;
+    case 4: return &s.H;
+    case 5: return &s.L;
+    default: return &s.M;
+  }
+}
+
+// the reference sweep's states of a read mask, in block order, all A values
+struct Shape {
+  bool spw, reduced;
+  int nx, fw, slot[7];
+  uint64_t nblocks;
+};
+static Shape shape_of(uint16_t reads) {
+  Shape s{};
+  const uint32_t bits[7] = {kRegB, kRegC, kRegD, kRegE, kRegH, kRegL, kRegM};
+  int k = 0;
+  for (int r = 0; r < 7; r++) s.slot[r] = (reads & bits[r]) ? k++ : -1;
+  s.nx = k;
+  s.spw = (reads & kRegSP) != 0;
+  s.reduced = s.spw || s.nx > 2;
+  s.fw = s.reduced ? 5 : 8;
+  s.nblocks = sweep_for(reads).states / 256;
+  return s;
+}
+static Z80S decode(uint64_t ab, const Shape& s) {
+  const uint8_t* rep = rep_values();
+  const uint16_t* repsp = rep_sp();
+  uint64_t rest = ab;
+  uint32_t sp = 0;
+  if (s.spw) {
+    sp = repsp[rest & 15];
+    rest >>= 4;
+  }
+  uint32_t fv[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int f = 6; f >= 0; f--)
+    if (f < s.nx) {
+      const uint32_t x = uint32_t(rest) & (s.reduced ? 31u : 255u);
+      fv[f] = s.reduced ? rep[x] : x;
+      rest >>= s.fw;
+    }
+  uint32_t rv[7];
+  for (int r = 0; r < 7; r++) rv[r] = s.slot[r] >= 0 ? fv[s.slot[r]] : 0;
+  return Z80S{0, uint32_t(rest & 1), rv[0], rv[1], rv[2], rv[3], rv[4], rv[5], sp, rv[6]};
+}
+static uint32_t* zreg(Z80S& s, int r) {
+  switch (r) {
+    case 0: return &s.b;
+    case 1: return &s.c;
+    case 2: return &s.d;
+    case 3: return &s.e;
+    case 4: return &s.h;
+    default: return &s.l;
+  }
+}
+
+int main() {
+  orc::Init();
+  std::mt19937_64 rng(31);
+  // (1) soundness of op_regs
+  for (int op = 0; op < orc::OpCodeCount; op++) {
+    const uint8_t named = op_regs(uint16_t(op));
+    const bool imm16 = orc::HasImm16(uint16_t(op));
+    for (int fld = 0; fld < 8; fld++) {  // B..L, M (6), SP (7)
+      const uint8_t bit = fld < 6 ? uint8_t(1u << fld) : (fld == 6 ? 0x40 : 0x80);
+      if (named & bit) continue;
+      for (int k = 0; k < 24; k++) {
+        const uint64_t r = rng(), r2 = rng();
+        orc::State s{uint8_t(r), uint8_t(r >> 8), uint8_t(r >> 16), uint8_t(r >> 24), uint8_t(r >> 32),
+                     uint8_t(r >> 40), uint8_t(r >> 48), uint8_t(r >> 56), uint16_t(r2), uint8_t(r2 >> 16)};
+        const uint16_t imm = imm16 ? uint16_t(rng()) : uint16_t(rng() & 0xFF);
+        orc::State base = s;
+        orc::Exec(base, uint16_t(op), imm);
+        for (int v = 0; v < 256; v++) {
+          orc::State t = s;
+          if (fld == 7) t.SP = uint16_t((rng() & 0xFF00) | v);
+          else *field(t, fld) = uint8_t(v);
+          const orc::State in = t;
+          orc::Exec(t, uint16_t(op), imm);
+          // the field keeps its value and the others match the base run
+          orc::State u = t, b2 = base;
+          if (fld == 7) {
+            if (t.SP != in.SP) goto bad;
+            u.SP = b2.SP = 0;
+          } else {
+            if (*field(t, fld) != *field(const_cast<orc::State&>(in), fld)) goto bad;
+            *field(u, fld) = *field(b2, fld) = 0;
+          }
+          if (u != b2) goto bad;
+          continue;
+        bad:
+          std::printf("op %d (%s) uses field %d that it does not name\n", op, op_mnemonic(uint16_t(op)), fld);
+          return 1;
+        }
+      }
+    }
+  }
+  // (2) verdicts of compact pairs over the reference sweep
+  const auto& I = orc::Instructions8();
+  int pairs = 0, equal = 0, renamed = 0;
+  for (int trial = 0; trial < 2000000 && pairs < 600; trial++) {
+    const int tn = 1 + int(rng() % 2);
+    int cn = 1 + int(rng() % 2);
+    orc::Instruction ti[2], ci[2];
+    uint32_t tw[2], cw[2], tr[2], cr[2];
+    for (int i = 0; i < tn; i++) ti[i] = I[rng() % I.size()];
+    for (int i = 0; i < cn; i++) ci[i] = I[rng() % I.size()];
+    if (rng() % 3 == 0) {  // the target itself or swapped: equivalences
+      cn = tn;
+      ci[0] = ti[tn == 2 && (rng() & 1) ? 1 : 0];
+      if (tn == 2) ci[1] = ti[ci[0].op == ti[0].op && ci[0].imm == ti[0].imm ? 1 : 0];
+    }
+    for (int i = 0; i < tn; i++) tw[i] = uint32_t(ti[i].op) | uint32_t(ti[i].imm) << 16;
+    for (int i = 0; i < cn; i++) cw[i] = uint32_t(ci[i].op) | uint32_t(ci[i].imm) << 16;
+    uint8_t map[6];
+    if (!compact_map(tw, tn, cw, cn, map, tr, cr)) continue;
+    const uint16_t reads = uint16_t(seq_reads(tw, tn) | seq_reads(cw, cn));
+    const Shape s = shape_of(reads);
+    if (s.nblocks > 512) continue;
+    pairs++;
+    bool moved = false;
+    for (int r = 0; r < 6; r++) moved = moved || map[r] != r;
+    renamed += moved ? 1 : 0;
+    for (uint8_t dead : {uint8_t(0x00), uint8_t(0xFF)}) {
+      bool eq = true;
+      for (uint64_t b = 0; b < s.nblocks && eq; b++) {
+        const Z80S x = decode(b, s);
+        for (uint32_t a = 0; a < 256 && eq; a++) {
+          Z80S y = x;
+          y.a = a;
+          Z80S p = y;  // renamed state: register r's value in register map[r]
+          for (int r = 0; r < 6; r++) *zreg(p, map[r]) = *zreg(y, r);
+          Z80S pt = p, pc = p;
+          for (int i = 0; i < tn; i++) z_step(pt, insn_op(tr[i]), insn_imm(tr[i]));
+          for (int i = 0; i < cn; i++) z_step(pc, insn_op(cr[i]), insn_imm(cr[i]));
+          const uint32_t keepF = uint8_t(~dead);
+          eq = pt.a == pc.a && ((pt.f ^ pc.f) & keepF) == 0 && pt.b == pc.b && pt.c == pc.c;
+        }
+      }
+      const bool want = dead ? orc::ExhaustiveCheckMasked(ti, tn, ci, cn, dead) : orc::ExhaustiveCheck(ti, tn, ci, cn);
+      if (want != eq) {
+        std::printf("compact verdict differs: target %08x %08x (%d) candidate %08x %08x (%d) dead %02x oracle %d\n",
+                    tw[0], tn > 1 ? tw[1] : 0, tn, cw[0], cn > 1 ? cw[1] : 0, cn, dead, want ? 1 : 0);
+        return 1;
+      }
+      equal += want ? 1 : 0;
+    }
+  }
+  if (pairs < 300 || equal < 50 || renamed < 50) {
+    std::printf("too few pairs (%d), equivalences (%d) or renamed pairs (%d)\n", pairs, equal, renamed);
+    return 1;
+  }
+  std::printf("OK %d compact pairs (%d renamed), %d equivalent verdicts\n", pairs, renamed, equal);
+  return 0;
+}

@@ -123,3 +123,20 @@ def test_register_renaming_against_oracle(tmp_path):
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.startswith("OK")
+
+
+def test_compact_state_mapping_against_oracle(tmp_path):
+    """op_regs is sound (fields an instruction does not name never matter),
+    and pairs that compact_map renames onto B, C keep the oracle's
+    ExhaustiveCheck[Masked] verdict over the reference's whole sweep when only
+    A, F, B and C are compared."""
+    import subprocess
+    exe = tmp_path / "compact_check"
+    srcs = [os.path.join(ROOT, "tests", "native", "compact_check.cpp"),
+            os.path.join(ROOT, "z80-optimizer_b200", "csrc", "z80_tables.cpp"),
+            os.path.join(ROOT, "oracle", "z80_oracle_isa_cpu.cpp"),
+            os.path.join(ROOT, "oracle", "z80_oracle_search.cpp")]
+    subprocess.run(["g++", "-O2", "-std=c++17", "-o", str(exe)] + srcs + ["-lpthread"], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.startswith("OK")

@@ -251,6 +251,96 @@ uint32_t seq_aflow(const uint32_t* s, int n) {
 }
 const char* op_mnemonic(uint16_t op) { return tables().cat[op].mnem.c_str(); }
 
+uint8_t op_regs(uint16_t op) {
+  static const char* kRegs = "BCDEHL";
+  const std::string& m = tables().cat[op].mnem;
+  uint8_t r = 0;
+  int depth = 0;
+  for (size_t i = 0; i < m.size(); i++) {
+    const char ch = m[i];
+    if (ch == '(') {
+      depth++;
+      r |= 0x40;  // a memory operand
+      continue;
+    }
+    if (ch == ')') {
+      depth--;
+      continue;
+    }
+    const bool word_start = i == 0 || m[i - 1] == ' ' || m[i - 1] == ',';
+    if (depth != 0 || !word_start) continue;
+    size_t j = i;
+    while (j < m.size() && m[j] != ',' && m[j] != ' ') j++;
+    const std::string w = m.substr(i, j - i);
+    if (w == "SP") r |= 0x80;
+    else if (w == "BC") r |= 0x03;
+    else if (w == "DE") r |= 0x0C;
+    else if (w == "HL") r |= 0x30;
+    else if (w.size() == 1 && std::strchr(kRegs, w[0])) r |= uint8_t(1u << (std::strchr(kRegs, w[0]) - kRegs));
+  }
+  return r;
+}
+
+bool compact_map(const uint32_t* t, int tn, const uint32_t* c, int cn, uint8_t (&map)[6], uint32_t* tw,
+                 uint32_t* cw) {
+  uint8_t fp = 0;
+  bool pair_named[3] = {false, false, false};
+  auto scan = [&](const uint32_t* s, int n) {
+    for (int i = 0; i < n; i++) {
+      const uint16_t op = insn_op(s[i]);
+      fp |= op_regs(op);
+      const std::string& m = tables().cat[op].mnem;
+      const char* names[3] = {"BC", "DE", "HL"};
+      for (int p = 0; p < 3; p++) {
+        const size_t at = m.find(names[p]);
+        if (at != std::string::npos && (at == 0 || m[at - 1] != '(')) pair_named[p] = true;
+      }
+    }
+  };
+  scan(t, tn);
+  scan(c, cn);
+  if (fp & 0xC0) return false;  // SP or the memory byte
+  int regs[6], nr = 0;
+  for (int r = 0; r < 6; r++)
+    if (fp & (1u << r)) regs[nr++] = r;
+  if (nr > 2) return false;
+  // targets: a named pair moves onto BC as a pair; single registers onto B, C
+  int target[6] = {-1, -1, -1, -1, -1, -1};
+  if ((fp & 0x03u) == fp) {
+    for (int r = 0; r < 6; r++) target[r] = r;  // already in B, C
+  } else if (nr == 2 && regs[1] == regs[0] + 1 && regs[0] % 2 == 0 && pair_named[regs[0] / 2]) {
+    target[regs[0]] = 0;
+    target[regs[1]] = 1;
+  } else {
+    for (int k = 0; k < nr; k++) target[regs[k]] = k;
+  }
+  // the registers left over take the places left over, pairs kept together
+  // where they can be (they are not used, so any order would do)
+  bool used[6] = {false, false, false, false, false, false};
+  for (int r = 0; r < 6; r++)
+    if (target[r] >= 0) used[target[r]] = true;
+  for (int r = 0; r < 6; r++)
+    if (target[r] < 0)
+      for (int d = 0; d < 6; d++)
+        if (!used[d]) {
+          target[r] = d;
+          used[d] = true;
+          break;
+        }
+  for (int r = 0; r < 6; r++) map[r] = uint8_t(target[r]);
+  for (int i = 0; i < tn; i++) {
+    const int o = op_rename(insn_op(t[i]), map);
+    if (o < 0) return false;
+    tw[i] = insn(uint16_t(o), insn_imm(t[i]));
+  }
+  for (int i = 0; i < cn; i++) {
+    const int o = op_rename(insn_op(c[i]), map);
+    if (o < 0) return false;
+    cw[i] = insn(uint16_t(o), insn_imm(c[i]));
+  }
+  return true;
+}
+
 int op_rename(uint16_t op, const uint8_t (&map)[6]) {
   static const char* kRegs = "BCDEHL";
   static const char* kPairs[3] = {"BC", "DE", "HL"};

@@ -36,6 +36,17 @@ const char* op_mnemonic(uint16_t op);     // "ADD A, n" style with placeholders
 // a pair split).  Memory operands ((HL), (BC), (DE)) stay as they are: the
 // step function's memory byte does not depend on the address registers.
 int op_rename(uint16_t op, const uint8_t (&map)[6]);
+// Registers an instruction names, read or written: bit r (r = 0..5) for B,
+// C, D, E, H, L (a register pair counts both halves), bit 6 for the memory
+// byte (a parenthesised operand), bit 7 for SP.  A and F are left out.  The
+// catalog's instructions use no other registers implicitly.
+uint8_t op_regs(uint16_t op);
+// A pair whose two programs name at most two of B..L and neither SP nor the
+// memory byte, with its registers renamed onto B and C (pairs used as pairs
+// onto BC): map[r] is register r's new place, tw/cw the renamed programs.
+// False when the pair names more, or a renaming does not exist.
+bool compact_map(const uint32_t* t, int tn, const uint32_t* c, int cn, uint8_t (&map)[6], uint32_t* tw,
+                 uint32_t* cw);
 const uint8_t* op_encoding(uint16_t op, int* n);
 std::string disassemble(uint32_t insn);   // catalog.go:73-127
 std::string disasm_seq(const uint32_t* seq, int n);  // " : " joined
