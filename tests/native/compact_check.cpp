@@ -6,11 +6,15 @@
 // accepts, running the renamed programs on the renamed states over the
 // reference's whole ExhaustiveCheck sweep, comparing A, F (under the dead
 // flags) and the registers B, C only, gives the oracle's verdict for the
-// original pair.  Built and run by tests/test_tables.py.
+// original pair.  (3) The bit-sliced step on the compact state (ZBc: A, F,
+// B, C and shared scratch) gives the full state's A, F, B and C for every
+// opcode that names no register but B and C.  Built and run by
+// tests/test_tables.py.
 #include <cstdio>
 #include <random>
 
 #include "../../oracle/z80_oracle.h"
+#include "../../z80-optimizer_b200/csrc/z80_bits.cuh"
 #include "../../z80-optimizer_b200/csrc/z80_exec.cuh"
 #include "../../z80-optimizer_b200/csrc/z80_tables.h"
 
@@ -169,10 +173,48 @@ int main() {
       equal += want ? 1 : 0;
     }
   }
+  // (3) the compact bit-sliced step
+  int compact_ops = 0;
+  for (uint32_t op = 0; op < uint32_t(kNumOps); op++) {
+    if (op_regs(uint16_t(op)) & ~0x03u) continue;
+    compact_ops++;
+    for (int rep = 0; rep < 32; rep++) {
+      Z80S st[32];
+      for (int j = 0; j < 32; j++) {
+        const uint64_t r = rng();
+        st[j] = Z80S{uint32_t(r & 0xFF), uint32_t((r >> 8) & 0xFF), uint32_t((r >> 16) & 0xFF),
+                     uint32_t((r >> 24) & 0xFF), 0, 0, 0, 0, 0, 0};
+      }
+      const uint32_t imm = uint32_t(rng() & 0xFFFF);
+      ZB full;
+      zb_from(full, st);
+      ZBc cz;
+      for (int i = 0; i < 8; i++) {
+        cz.a[i] = full.a[i];
+        cz.f[i] = full.f[i];
+        cz.b[i] = full.b[i];
+        cz.c[i] = full.c[i];
+        cz.x[i] = 0;
+      }
+      for (int i = 0; i < 16; i++) cz.sp[i] = 0;
+      zb_step(full, op, imm);
+      zb_step(cz, op, imm);
+      for (int i = 0; i < 8; i++)
+        if (cz.a[i] != full.a[i] || cz.f[i] != full.f[i] || cz.b[i] != full.b[i] || cz.c[i] != full.c[i]) {
+          std::printf("compact step differs on op %u (%s)\n", op, op_mnemonic(uint16_t(op)));
+          return 1;
+        }
+    }
+  }
+  if (compact_ops < 150) {
+    std::printf("too few compact opcodes (%d)\n", compact_ops);
+    return 1;
+  }
   if (pairs < 300 || equal < 50 || renamed < 50) {
     std::printf("too few pairs (%d), equivalences (%d) or renamed pairs (%d)\n", pairs, equal, renamed);
     return 1;
   }
-  std::printf("OK %d compact pairs (%d renamed), %d equivalent verdicts\n", pairs, renamed, equal);
+  std::printf("OK %d compact pairs (%d renamed), %d equivalent verdicts, %d opcodes on the compact step\n", pairs,
+              renamed, equal, compact_ops);
   return 0;
 }

@@ -19,6 +19,17 @@ struct ZB {
   uint32_t a[8], f[8], b[8], c[8], d[8], e[8], h[8], l[8], m[8];
   uint32_t sp[16];
 };
+// A compact state for pairs whose instructions name no register but B and C
+// (after renaming) and neither SP nor the memory byte: D, E, H, L and M
+// share one scratch array that such instructions never touch, SP another.
+// The step functions below are templates over the state type.
+struct ZBc {
+  uint32_t a[8], f[8], b[8], c[8];
+  union {
+    uint32_t x[8], d[8], e[8], h[8], l[8], m[8];
+  };
+  uint32_t sp[16];
+};
 
 constexpr uint32_t kZBOnes = 0xFFFFFFFFu;
 
@@ -43,7 +54,8 @@ Z80_HD void zb_copy8(uint32_t (&d)[8], const uint32_t (&s)[8]) {
   ZB_UNROLL for (int i = 0; i < 8; i++) d[i] = s[i];
 }
 // S, Z, 5, 3 of a result (z_sz53), P/V and H, N cleared.
-Z80_HD void zb_sz53p(ZB& z, const uint32_t (&r)[8], uint32_t carry) {
+template <class ZT>
+Z80_HD void zb_sz53p(ZT& z, const uint32_t (&r)[8], uint32_t carry) {
   z.f[0] = carry;
   z.f[1] = 0;
   z.f[2] = zb_even(r);
@@ -66,7 +78,8 @@ Z80_HD uint32_t zb_adder8(const uint32_t (&x)[8], const uint32_t (&y)[8], uint32
   }
   return c;
 }
-Z80_HD void zb_add(ZB& z, const uint32_t (&v)[8], uint32_t cin) {
+template <class ZT>
+Z80_HD void zb_add(ZT& z, const uint32_t (&v)[8], uint32_t cin) {
   uint32_t r[8], c4 = 0;
   const uint32_t co = zb_adder8(z.a, v, cin, r, &c4);
   z.f[0] = co;
@@ -89,7 +102,8 @@ Z80_HD uint32_t zb_suber8(const uint32_t (&x)[8], const uint32_t (&v)[8], uint32
   *h = ~c4;  // bit 4 of x ^ v ^ r
   return ~co;
 }
-Z80_HD void zb_sub(ZB& z, const uint32_t (&v)[8], uint32_t bin) {
+template <class ZT>
+Z80_HD void zb_sub(ZT& z, const uint32_t (&v)[8], uint32_t bin) {
   uint32_t r[8], h = 0;
   const uint32_t borrow = zb_suber8(z.a, v, bin, r, &h);
   z.f[0] = borrow;
@@ -102,7 +116,8 @@ Z80_HD void zb_sub(ZB& z, const uint32_t (&v)[8], uint32_t bin) {
   z.f[7] = r[7];
   zb_copy8(z.a, r);
 }
-Z80_HD void zb_cp(ZB& z, const uint32_t (&v)[8]) {
+template <class ZT>
+Z80_HD void zb_cp(ZT& z, const uint32_t (&v)[8]) {
   uint32_t r[8], h = 0;
   const uint32_t borrow = zb_suber8(z.a, v, 0u, r, &h);
   z.f[0] = borrow;
@@ -114,21 +129,25 @@ Z80_HD void zb_cp(ZB& z, const uint32_t (&v)[8]) {
   z.f[6] = ~zb_any(r);
   z.f[7] = r[7];
 }
-Z80_HD void zb_and(ZB& z, const uint32_t (&v)[8]) {
+template <class ZT>
+Z80_HD void zb_and(ZT& z, const uint32_t (&v)[8]) {
   ZB_UNROLL for (int i = 0; i < 8; i++) z.a[i] &= v[i];
   zb_sz53p(z, z.a, 0u);
   z.f[4] = kZBOnes;
 }
-Z80_HD void zb_xor(ZB& z, const uint32_t (&v)[8]) {
+template <class ZT>
+Z80_HD void zb_xor(ZT& z, const uint32_t (&v)[8]) {
   ZB_UNROLL for (int i = 0; i < 8; i++) z.a[i] ^= v[i];
   zb_sz53p(z, z.a, 0u);
 }
-Z80_HD void zb_or(ZB& z, const uint32_t (&v)[8]) {
+template <class ZT>
+Z80_HD void zb_or(ZT& z, const uint32_t (&v)[8]) {
   ZB_UNROLL for (int i = 0; i < 8; i++) z.a[i] |= v[i];
   zb_sz53p(z, z.a, 0u);
 }
 // z_inc / z_dec
-Z80_HD void zb_inc(ZB& z, uint32_t (&r)[8]) {
+template <class ZT>
+Z80_HD void zb_inc(ZT& z, uint32_t (&r)[8]) {
   uint32_t c = kZBOnes;
   ZB_UNROLL for (int i = 0; i < 8; i++) {
     const uint32_t t = r[i];
@@ -143,7 +162,8 @@ Z80_HD void zb_inc(ZB& z, uint32_t (&r)[8]) {
   z.f[6] = ~zb_any(r);
   z.f[7] = r[7];
 }
-Z80_HD void zb_dec(ZB& z, uint32_t (&r)[8]) {
+template <class ZT>
+Z80_HD void zb_dec(ZT& z, uint32_t (&r)[8]) {
   z.f[4] = ~(r[0] | r[1] | r[2] | r[3]);
   uint32_t c = kZBOnes;
   ZB_UNROLL for (int i = 0; i < 8; i++) {
@@ -159,7 +179,8 @@ Z80_HD void zb_dec(ZB& z, uint32_t (&r)[8]) {
   z.f[7] = r[7];
 }
 // z_daa: corrections chosen per state, the add or the subtract selected by N.
-Z80_HD void zb_daa(ZB& z) {
+template <class ZT>
+Z80_HD void zb_daa(ZT& z) {
   const uint32_t lo_gt9 = z.a[3] & (z.a[2] | z.a[1]);
   const uint32_t hi_gt9 = z.a[7] & (z.a[6] | z.a[5]);
   const uint32_t hi_eq9 = z.a[7] & ~z.a[6] & ~z.a[5] & z.a[4];
@@ -168,7 +189,7 @@ Z80_HD void zb_daa(ZB& z) {
   const uint32_t add60 = z.f[0] | gt99;
   const uint32_t carry = z.f[0] | gt99;
   uint32_t v[8] = {0u, add6, add6, 0u, 0u, add60, add60, 0u};
-  ZB za = z, zs = z;
+  ZT za = z, zs = z;
   zb_add(za, v, 0u);
   zb_sub(zs, v, 0u);
   const uint32_t n = z.f[1];
@@ -180,7 +201,8 @@ Z80_HD void zb_daa(ZB& z) {
   z.f[2] = zb_even(z.a);
 }
 // ---- CB rotates and shifts; results into r, flags from the new value
-Z80_HD void zb_rot(ZB& z, uint32_t (&r)[8], int kind) {
+template <class ZT>
+Z80_HD void zb_rot(ZT& z, uint32_t (&r)[8], int kind) {
   uint32_t n[8], co = 0;
   switch (kind) {
     case 0:  // RLC
@@ -227,7 +249,8 @@ Z80_HD void zb_rot(ZB& z, uint32_t (&r)[8], int kind) {
   zb_copy8(r, n);
   zb_sz53p(z, r, co);
 }
-Z80_HD void zb_bit(ZB& z, const uint32_t (&r)[8], int bit) {
+template <class ZT>
+Z80_HD void zb_bit(ZT& z, const uint32_t (&r)[8], int bit) {
   const uint32_t nb = ~r[bit];
   z.f[1] = 0;
   z.f[2] = nb;
@@ -260,7 +283,8 @@ Z80_HD void zb_incsp(uint32_t (&sp)[16], bool dec) {
   }
 }
 // HL + v (+ carry) / HL - v - carry over 16 planes; kind 0 ADD, 1 ADC, 2 SBC.
-Z80_HD void zb_hl16(ZB& z, const uint32_t (&v)[16], int kind) {
+template <class ZT>
+Z80_HD void zb_hl16(ZT& z, const uint32_t (&v)[16], int kind) {
   uint32_t x[16], y[16], r[16];
   ZB_UNROLL for (int i = 0; i < 8; i++) {
     x[i] = z.l[i];
@@ -347,7 +371,8 @@ Z80_HD void zb_pair(uint32_t (&v)[16], const uint32_t (&hi)[8], const uint32_t (
 #define ZB_SET(o, r) case (o): z.r[((o) - SET_0_A) / 7] = kZBOnes; break;
 
 // One instruction on the 32 states of z (op and imm are the same for all).
-Z80_HD void zb_step(ZB& z, uint32_t op, uint32_t imm) {
+template <class ZT>
+Z80_HD void zb_step(ZT& z, uint32_t op, uint32_t imm) {
   uint32_t t8[8];
   uint32_t t16[16];
   switch (op) {
@@ -527,7 +552,8 @@ Z80_HD void zb_step(ZB& z, uint32_t op, uint32_t imm) {
 }
 
 // Planes <-> scalar states (host tests; the sweep builds planes directly).
-Z80_HD void zb_from(ZB& z, const Z80S (&s)[32]) {
+template <class ZT>
+Z80_HD void zb_from(ZT& z, const Z80S (&s)[32]) {
   for (int i = 0; i < 8; i++) {
     z.a[i] = z.f[i] = z.b[i] = z.c[i] = z.d[i] = z.e[i] = z.h[i] = z.l[i] = z.m[i] = 0;
   }
@@ -549,7 +575,8 @@ Z80_HD void zb_from(ZB& z, const Z80S (&s)[32]) {
       if ((s[j].sp >> i) & 1u) z.sp[i] |= bit;
   }
 }
-Z80_HD Z80S zb_get(const ZB& z, int j) {
+template <class ZT>
+Z80_HD Z80S zb_get(const ZT& z, int j) {
   Z80S s{};
   for (int i = 0; i < 8; i++) {
     s.a |= ((z.a[i] >> j) & 1u) << i;
