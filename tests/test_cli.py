@@ -75,3 +75,42 @@ def test_cli_target_and_enumerate_sample(tmp_path):
     assert r.returncode == 0, r.stderr
     rules = json.load(open(out))
     assert rules and all(x["bytes_saved"] > 0 for x in rules)
+
+
+def test_cli_mulopt_resume_all_presolved(tmp_path):
+    """mulopt -resume (cmd/mulopt/main.go:238-302): constants in the resume
+    file are not searched again; with all 254 there, no device is needed and
+    the output is the file's results."""
+    res = [{"k": k, "ops": ["ADD A,A"] * (k % 5 + 1), "length": k % 5 + 1, "tstates": 4 * (k % 5 + 1)}
+           for k in range(2, 256)]
+    f = tmp_path / "prev.json"
+    f.write_text(json.dumps(res))
+    r = run("mulopt", "-resume", str(f), "-json")
+    assert r.returncode == 0, r.stderr
+    assert json.loads(r.stdout) == res
+    assert "Resumed 254 previous results" in r.stderr and "0 constants to check (254 pre-solved)" in r.stderr
+    r = run("mulopt", "--resume", str(f))
+    assert r.returncode == 0
+    assert r.stdout.splitlines()[0] == "×  2: " + "[ADD A,A ADD A,A ADD A,A]".ljust(80) + " (3 insts, 12T)"
+    bad = tmp_path / "bad.json"
+    bad.write_text('[{"k": 300, "ops": []}]')
+    r = run("mulopt", "--resume", str(bad))
+    assert r.returncode == 1 and "Error parsing resume file" in r.stderr
+    bad.write_text('{"k": 3')
+    r = run("mulopt", "--resume", str(bad))
+    assert r.returncode == 1 and "Error parsing resume file" in r.stderr
+
+
+@pytest.mark.gpu
+def test_cli_mulopt_resume_partial(tmp_path):
+    """Resuming from the first ten constants of a run gives the same output
+    as the run itself."""
+    r = run("mulopt", "--max-len", "4", "--json")
+    assert r.returncode == 0, r.stderr
+    full = json.loads(r.stdout)
+    f = tmp_path / "prev.json"
+    f.write_text(json.dumps(full[:10]))
+    r = run("mulopt", "--max-len", "4", "--json", "--resume", str(f))
+    assert r.returncode == 0, r.stderr
+    assert json.loads(r.stdout) == full
+    assert "(10 pre-solved)" in r.stderr

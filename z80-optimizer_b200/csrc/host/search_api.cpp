@@ -927,6 +927,34 @@ void WriteJSON(std::FILE* f, const std::vector<Result>& results) {
   }
   std::fprintf(f, "]\n");
 }
+std::vector<Result> ReadJSON(const std::string& text) {
+  const JVal top = JParser(text).parse();
+  std::vector<Result> out;
+  if (top.k == JVal::kNull) return out;
+  if (top.k != JVal::kArr) throw Error(Z80B_EINVAL, "mulopt results: the top-level value is not an array");
+  for (const JVal& e : top.arr) {
+    if (e.k == JVal::kNull) continue;
+    if (e.k != JVal::kObj) throw Error(Z80B_EINVAL, "mulopt results: an array element is not an object");
+    Result r;
+    r.Found = true;
+    for (const auto& kv : e.obj) {
+      if (key_is(kv.first, "k")) json_int_field(kv.second, &r.K, "k");
+      else if (key_is(kv.first, "length")) json_int_field(kv.second, &r.Length, "length");
+      else if (key_is(kv.first, "tstates")) json_int_field(kv.second, &r.TStates, "tstates");
+      else if (key_is(kv.first, "ops")) {
+        if (kv.second.k == JVal::kNull) continue;
+        if (kv.second.k != JVal::kArr) throw Error(Z80B_EINVAL, "mulopt results: ops is not an array");
+        for (const JVal& o : kv.second.arr) {
+          std::string op;
+          json_string_field(o, &op, "ops");
+          r.Ops.push_back(op);
+        }
+      }
+    }
+    out.push_back(r);
+  }
+  return out;
+}
 }  // namespace mul
 
 }  // namespace z80opt

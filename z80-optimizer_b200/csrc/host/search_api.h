@@ -195,6 +195,10 @@ struct Result {
 std::vector<Result> FindAll(int pool, uint8_t b, uint8_t c, uint8_t f, int minLen, int maxLen,
                             const std::vector<int>& ks, z80b_mul_stats* stats = nullptr);
 void WriteJSON(std::FILE* f, const std::vector<Result>& results);  // cmd/mulopt -json
+// The -json output read back (cmd/mulopt/main.go:238-256, the -resume file):
+// every entry found, keys as in MulResult; throws Error(Z80B_EINVAL) on
+// malformed input.
+std::vector<Result> ReadJSON(const std::string& text);
 }  // namespace mul
 
 // The process-wide device context (created on first use).

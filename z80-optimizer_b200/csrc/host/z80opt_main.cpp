@@ -7,7 +7,7 @@
 //   z80opt target "ASM : ASM ..." [--max-candidate N] [--dead-flags M] [-v]
 //   z80opt verify-jsonl FILE [--dead-flags M] [-v]
 //   z80opt mulopt [--pool mulopt|wide21|fast14|cuda21] [--max-len N] [--min-len N]
-//                 [--k K] [--json] [--init B,C,F]
+//                 [--k K] [--json] [--init B,C,F] [--resume FILE]
 //   z80opt export FILE [-f go|peephole] [--output OUT] [--var NAME]
 //
 // Output text follows the reference commands.  --sample/--seed (search a
@@ -23,6 +23,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -58,6 +59,8 @@ Args parse(int argc, char** argv, const std::vector<std::string>& flags) {
     if (s == "-v") s = "--verbose";
     if (s == "-f") s = "--format";
     if (s == "-o") s = "--output";
+    // Go's flag package (cmd/mulopt) also takes long flags with one dash
+    if (s.size() > 2 && s[0] == '-' && s[1] != '-' && !(s[1] >= '0' && s[1] <= '9')) s = "-" + s;
     if (s.rfind("--", 0) == 0) {
       const size_t eq = s.find('=');
       std::string k = s.substr(2, eq == std::string::npos ? std::string::npos : eq - 2);
@@ -320,16 +323,64 @@ int cmd_mulopt(const Args& a) {
     throw Error(Z80B_EINVAL, "--init wants B,C,F");
   const int maxLen = int(a.num("max-len", 8)), minLen = int(a.num("min-len", 1));
   const int k = int(a.num("k", 0));
+  // -resume (cmd/mulopt/main.go:238-256,283-302): constants solved in an
+  // earlier -json output are kept and not searched again
+  std::vector<mul::Result> prev;
+  const std::string resume = a.get("resume", "");
+  if (!resume.empty()) {
+    std::ifstream in(resume, std::ios::binary);
+    if (!in) {
+      std::fprintf(stderr, "Error reading resume file: cannot open %s\n", resume.c_str());
+      return 1;
+    }
+    std::stringstream ss;
+    ss << in.rdbuf();
+    try {
+      prev = mul::ReadJSON(ss.str());
+    } catch (const Error& e) {
+      std::fprintf(stderr, "Error parsing resume file: %s\n", e.what());
+      return 1;
+    }
+    for (const auto& r : prev)
+      if (r.K < 2 || r.K > 255) {
+        std::fprintf(stderr, "Error parsing resume file: constant %d outside 2..255\n", r.K);
+        return 1;
+      }
+    std::fprintf(stderr, "Resumed %zu previous results\n", prev.size());
+  }
   std::vector<int> ks;
+  std::vector<int> pre(256, -1);  // index into prev of a pre-solved constant
+  for (size_t i = 0; i < prev.size(); i++) pre[size_t(prev[i].K)] = int(i);
   if (k > 0) ks.push_back(k);
   else
-    for (int i = 2; i <= 255; i++) ks.push_back(i);
+    for (int i = 2; i <= 255; i++)
+      if (pre[size_t(i)] < 0) ks.push_back(i);
   int n = 0, ml = 0;
   z80b_mul_pool(pool, &n, &ml, nullptr, nullptr, 0);
+  int skipped = 0;
+  for (int i = 2; i <= 255; i++) skipped += pre[size_t(i)] >= 0;
   if (k > 0) std::fprintf(stderr, "Searching for mul×%d (len %d..%d, %d ops)...\n", k, minLen, maxLen, n);
-  else std::fprintf(stderr, "Searching len %d..%d, %zu constants to check (0 pre-solved)\n", minLen, maxLen, ks.size());
+  else
+    std::fprintf(stderr, "Searching len %d..%d, %zu constants to check (%d pre-solved)\n", minLen, maxLen, ks.size(),
+                 skipped);
   z80b_mul_stats st{};
-  const auto res = mul::FindAll(pool, uint8_t(b), uint8_t(c), uint8_t(f), minLen, maxLen, ks, &st);
+  std::vector<mul::Result> found;
+  if (!ks.empty()) found = mul::FindAll(pool, uint8_t(b), uint8_t(c), uint8_t(f), minLen, maxLen, ks, &st);
+  std::vector<mul::Result> res;
+  if (k > 0) {
+    res = found;
+  } else {
+    // 2..255 in order: pre-solved entries as loaded, the rest as searched
+    size_t j = 0;
+    for (int i = 2; i <= 255; i++) {
+      if (pre[size_t(i)] >= 0) {
+        res.push_back(prev[size_t(pre[size_t(i)])]);
+        res.back().K = i;
+      } else {
+        res.push_back(found[j++]);
+      }
+    }
+  }
   if (k > 0) {
     if (!res[0].Found) {
       std::fprintf(stderr, "No sequence found for ×%d within length %d\n", k, maxLen);
@@ -420,7 +471,7 @@ void usage() {
                "               --sample N --seed S --first-op-start M --first-op-end N --jsonl FILE --no-exhaust\n"
                "  target       \"ASM : ASM\" --max-candidate N\n"
                "  verify-jsonl FILE --dead-flags M -v\n"
-               "  mulopt       --pool mulopt|wide21|fast14|cuda21 --max-len N --k K --json\n"
+               "  mulopt       --pool mulopt|wide21|fast14|cuda21 --max-len N --k K --json --resume FILE\n"
                "  export       FILE -f go|peephole --output OUT --var NAME\n");
 }
 
