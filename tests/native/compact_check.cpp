@@ -8,8 +8,9 @@
 // flags) and the registers B, C only, gives the oracle's verdict for the
 // original pair.  (3) The bit-sliced step on the compact state (ZBc: A, F,
 // B, C and shared scratch) gives the full state's A, F, B and C for every
-// opcode that names no register but B and C.  Built and run by
-// tests/test_tables.py.
+// opcode that names no register but B and C.  (4) The device's tables
+// (compact_tables) accept, rename and place registers as compact_map does.
+// Built and run by tests/test_tables.py.
 #include <cstdio>
 #include <random>
 
@@ -204,6 +205,62 @@ int main() {
           std::printf("compact step differs on op %u (%s)\n", op, op_mnemonic(uint16_t(op)));
           return 1;
         }
+    }
+  }
+  // (4) the device's tables (compact_tables) decide and rename as
+  // compact_map does
+  {
+    const CompactTables& T = compact_tables();
+    int agreed = 0;
+    for (int trial = 0; trial < 200000; trial++) {
+      const int tn = 1 + int(rng() % 3), cn = 1 + int(rng() % 2);
+      uint32_t tw[3], cw[2], tr[3], cr[2];
+      for (int i = 0; i < tn; i++) {
+        const auto& x = I[rng() % I.size()];
+        tw[i] = uint32_t(x.op) | uint32_t(x.imm) << 16;
+      }
+      for (int i = 0; i < cn; i++) {
+        const auto& x = I[rng() % I.size()];
+        cw[i] = uint32_t(x.op) | uint32_t(x.imm) << 16;
+      }
+      uint8_t map[6];
+      const bool by_map = compact_map(tw, tn, cw, cn, map, tr, cr);
+      uint8_t fp = 0;
+      for (int i = 0; i < tn; i++) fp |= T.opregs[insn_op(tw[i])];
+      for (int i = 0; i < cn; i++) fp |= T.opregs[insn_op(cw[i])];
+      const int id = (fp & 0xC0) ? 0 : T.id_of_set[fp & 0x3F];
+      bool by_table = id != 0;
+      for (int i = 0; i < tn && by_table; i++) by_table = T.ren[id - 1][insn_op(tw[i])] >= 0;
+      for (int i = 0; i < cn && by_table; i++) by_table = T.ren[id - 1][insn_op(cw[i])] >= 0;
+      if (by_map != by_table) {
+        std::printf("compact tables disagree with compact_map (%d vs %d)\n", by_table, by_map);
+        return 1;
+      }
+      if (!by_map) continue;
+      agreed++;
+      for (int i = 0; i < tn; i++)
+        if (uint32_t(T.ren[id - 1][insn_op(tw[i])]) != insn_op(tr[i])) {
+          std::printf("compact table renames differently\n");
+          return 1;
+        }
+      for (int i = 0; i < cn; i++)
+        if (uint32_t(T.ren[id - 1][insn_op(cw[i])]) != insn_op(cr[i])) {
+          std::printf("compact table renames differently\n");
+          return 1;
+        }
+      for (int slot = 0; slot < 2; slot++) {
+        int want = -1;
+        for (int r = 0; r < 6; r++)
+          if ((fp & (1u << r)) && map[r] == slot) want = r;
+        if (T.orig[id - 1][slot] != want) {
+          std::printf("compact table origin differs\n");
+          return 1;
+        }
+      }
+    }
+    if (agreed < 1000) {
+      std::printf("too few compact pairs for the table check (%d)\n", agreed);
+      return 1;
     }
   }
   if (compact_ops < 150) {

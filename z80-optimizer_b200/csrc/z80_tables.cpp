@@ -284,38 +284,35 @@ uint8_t op_regs(uint16_t op) {
 bool compact_map(const uint32_t* t, int tn, const uint32_t* c, int cn, uint8_t (&map)[6], uint32_t* tw,
                  uint32_t* cw) {
   uint8_t fp = 0;
-  bool pair_named[3] = {false, false, false};
-  auto scan = [&](const uint32_t* s, int n) {
-    for (int i = 0; i < n; i++) {
-      const uint16_t op = insn_op(s[i]);
-      fp |= op_regs(op);
-      const std::string& m = tables().cat[op].mnem;
-      const char* names[3] = {"BC", "DE", "HL"};
-      for (int p = 0; p < 3; p++) {
-        const size_t at = m.find(names[p]);
-        if (at != std::string::npos && (at == 0 || m[at - 1] != '(')) pair_named[p] = true;
-      }
-    }
-  };
-  scan(t, tn);
-  scan(c, cn);
+  for (int i = 0; i < tn; i++) fp |= op_regs(insn_op(t[i]));
+  for (int i = 0; i < cn; i++) fp |= op_regs(insn_op(c[i]));
   if (fp & 0xC0) return false;  // SP or the memory byte
-  int regs[6], nr = 0;
-  for (int r = 0; r < 6; r++)
-    if (fp & (1u << r)) regs[nr++] = r;
-  if (nr > 2) return false;
-  // targets: a named pair moves onto BC as a pair; single registers onto B, C
-  int target[6] = {-1, -1, -1, -1, -1, -1};
-  if ((fp & 0x03u) == fp) {
-    for (int r = 0; r < 6; r++) target[r] = r;  // already in B, C
-  } else if (nr == 2 && regs[1] == regs[0] + 1 && regs[0] % 2 == 0 && pair_named[regs[0] / 2]) {
-    target[regs[0]] = 0;
-    target[regs[1]] = 1;
-  } else {
-    for (int k = 0; k < nr; k++) target[regs[k]] = k;
+  if (__builtin_popcount(fp) > 2) return false;
+  // a register pair that an instruction uses as one has both halves in the
+  // set; they land on B and C in order, so the pair becomes BC
+  compact_set_map(fp, map);
+  for (int i = 0; i < tn; i++) {
+    const int o = op_rename(insn_op(t[i]), map);
+    if (o < 0) return false;
+    tw[i] = insn(uint16_t(o), insn_imm(t[i]));
   }
-  // the registers left over take the places left over, pairs kept together
-  // where they can be (they are not used, so any order would do)
+  for (int i = 0; i < cn; i++) {
+    const int o = op_rename(insn_op(c[i]), map);
+    if (o < 0) return false;
+    cw[i] = insn(uint16_t(o), insn_imm(c[i]));
+  }
+  return true;
+}
+
+void compact_set_map(uint8_t set, uint8_t (&map)[6]) {
+  int target[6] = {-1, -1, -1, -1, -1, -1};
+  if ((set & 0x03u) == set) {
+    for (int r = 0; r < 6; r++) target[r] = r;  // already in B, C
+  } else {
+    int k = 0;
+    for (int r = 0; r < 6; r++)
+      if (set & (1u << r)) target[r] = k++;  // in order onto B, C (a pair's halves onto B, C)
+  }
   bool used[6] = {false, false, false, false, false, false};
   for (int r = 0; r < 6; r++)
     if (target[r] >= 0) used[target[r]] = true;
@@ -328,17 +325,30 @@ bool compact_map(const uint32_t* t, int tn, const uint32_t* c, int cn, uint8_t (
           break;
         }
   for (int r = 0; r < 6; r++) map[r] = uint8_t(target[r]);
-  for (int i = 0; i < tn; i++) {
-    const int o = op_rename(insn_op(t[i]), map);
-    if (o < 0) return false;
-    tw[i] = insn(uint16_t(o), insn_imm(t[i]));
-  }
-  for (int i = 0; i < cn; i++) {
-    const int o = op_rename(insn_op(c[i]), map);
-    if (o < 0) return false;
-    cw[i] = insn(uint16_t(o), insn_imm(c[i]));
-  }
-  return true;
+}
+
+const CompactTables& compact_tables() {
+  static CompactTables T;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    std::memset(T.id_of_set, 0, sizeof T.id_of_set);
+    int e = 0;
+    for (uint32_t set = 0; set < 64; set++) {
+      if (__builtin_popcount(set) > 2) continue;
+      T.id_of_set[set] = uint8_t(e + 1);
+      uint8_t map[6];
+      compact_set_map(uint8_t(set), map);
+      for (int op = 0; op < kNumOps; op++) T.ren[e][op] = int16_t(op_rename(uint16_t(op), map));
+      for (int slot = 0; slot < 2; slot++) {
+        T.orig[e][slot] = -1;
+        for (int r = 0; r < 6; r++)
+          if ((set & (1u << r)) && map[r] == slot) T.orig[e][slot] = int8_t(r);
+      }
+      e++;
+    }
+    for (int op = 0; op < kNumOps; op++) T.opregs[op] = op_regs(uint16_t(op));
+  });
+  return T;
 }
 
 int op_rename(uint16_t op, const uint8_t (&map)[6]) {

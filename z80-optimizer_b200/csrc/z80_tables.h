@@ -47,6 +47,23 @@ uint8_t op_regs(uint16_t op);
 // False when the pair names more, or a renaming does not exist.
 bool compact_map(const uint32_t* t, int tn, const uint32_t* c, int cn, uint8_t (&map)[6], uint32_t* tw,
                  uint32_t* cw);
+// The renaming compact_map uses for a set of at most two of B..L (bit r =
+// register r): the set's registers onto B and C (in order), the others onto
+// the places left.
+void compact_set_map(uint8_t set, uint8_t (&map)[6]);
+// The same mapping as tables for the device, one entry per set of at most
+// two registers (22 sets): id_of_set[set] = 1 + entry (0 for larger sets),
+// ren[entry][op] the renamed opcode or -1, orig[entry][s] the original
+// register (0..5) that plays B (s = 0) or C (s = 1), or -1, and op_regs of
+// every opcode.
+constexpr int kCompactSets = 22;
+struct CompactTables {
+  int16_t ren[kCompactSets][kNumOps];
+  int8_t orig[kCompactSets][2];
+  uint8_t id_of_set[64];
+  uint8_t opregs[kNumOps];
+};
+const CompactTables& compact_tables();
 const uint8_t* op_encoding(uint16_t op, int* n);
 std::string disassemble(uint32_t insn);   // catalog.go:73-127
 std::string disasm_seq(const uint32_t* seq, int n);  // " : " joined
