@@ -56,6 +56,7 @@ struct PairRec {
   uint16_t reads;      // union of regsRead
   uint8_t keepF;       // ~deadFlags
   uint8_t keepR;       // bits 0..5: register compared (B,C,D,E,H,L); bit 7: masked pass
+  uint8_t cmap;        // compact sweep: 1 + the register-set entry of its tables; 0: full state
 };
 
 __device__ __forceinline__ uint32_t target_len(const DevTargets& T, uint32_t t) {

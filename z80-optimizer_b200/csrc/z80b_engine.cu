@@ -137,7 +137,7 @@ struct z80b_ctx {
   // pipeline scratch
   DBuf cnt_f, cnt_m, cnt_all, base, meta, surv, sdiff, checks;
   DBuf next, win, windiff, spec, spec2, wlen;
-  DBuf pairs, pair_src, nchunks, cbase, nchunks_x, cbase_x, rejected, npairs, counter, states;
+  DBuf pairs, pair_src, nchunks, cbase, nchunks_x, cbase_x, nchunks_c, cbase_c, rejected, npairs, counter, states;
   DBuf rcnt, rbase, rules, checked, surv_target, midpass, flag;
   DBuf cub_tmp;
   DBuf hits, nhits, fpq;
@@ -154,6 +154,7 @@ struct z80b_ctx {
   int priority = 0;           // Z80B_OPT_STREAM_PRIORITY
   int qc_index = 1;           // Z80B_OPT_QC_INDEX
   int xbits = 1;              // Z80B_OPT_XINDEP_BITS
+  int compact = 0;            // Z80B_OPT_COMPACT_SWEEP
 };
 
 namespace {
@@ -517,16 +518,22 @@ int sweep_round(z80b_ctx* ctx, const DevTargets& T, const DevPool& P, const Roun
   cudaStream_t s = ctx->stream;
   CKR(scan(ctx, R.nchunks, R.cbase, np));
   CKR(scan(ctx, R.nchunks_x, R.cbase_x, np));
-  unsigned long long last[4] = {0, 0, 0, 0};
+  if (R.compact) CKR(scan(ctx, R.nchunks_c, R.cbase_c, np));
+  unsigned long long last[6] = {0, 0, 0, 0, 0, 0};
   CK(cudaMemcpyAsync(&last[0], R.cbase + (np - 1), 8, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(&last[1], R.nchunks + (np - 1), 8, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(&last[2], R.cbase_x + (np - 1), 8, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(&last[3], R.nchunks_x + (np - 1), 8, cudaMemcpyDeviceToHost, s));
+  if (R.compact) {
+    CK(cudaMemcpyAsync(&last[4], R.cbase_c + (np - 1), 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&last[5], R.nchunks_c + (np - 1), 8, cudaMemcpyDeviceToHost, s));
+  }
   CK(cudaStreamSynchronize(s));
-  CK(cudaMemsetAsync(R.counter, 0, 16, s));
-  trace("sweep: %u pairs, %llu + %llu chunks", np, last[0] + last[1], last[2] + last[3]);
+  CK(cudaMemsetAsync(R.counter, 0, 24, s));
+  trace("sweep: %u pairs, %llu + %llu + %llu chunks", np, last[0] + last[1], last[2] + last[3], last[4] + last[5]);
   int ke = kbegin(ctx, 1);
-  const int nl = launch_exhaustive(T, P, R, np, last[0] + last[1], last[2] + last[3], ctx->exh_k, s);
+  const int nl =
+      launch_exhaustive(T, P, R, np, last[0] + last[1], last[2] + last[3], last[4] + last[5], ctx->exh_k, s);
   kend(ctx, ke);
   CKR(check_launch(ctx, "exhaustive"));
   if (nl > 1) ctx->launches += uint32_t(nl - 1);
@@ -564,7 +571,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
   CK(ctx->checked.ensure(8));
   CK(ctx->states.ensure(16));
   CK(ctx->npairs.ensure(4));
-  CK(ctx->counter.ensure(16));
+  CK(ctx->counter.ensure(24));
   CK(cudaMemsetAsync(ctx->checks.p, 0, 8, s));
   CK(cudaMemsetAsync(ctx->checked.p, 0, 8, s));
   CK(cudaMemsetAsync(ctx->states.p, 0, 16, s));
@@ -632,6 +639,10 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
     CK(ctx->cbase.ensure(8 * cap));
     CK(ctx->nchunks_x.ensure(8 * cap));
     CK(ctx->cbase_x.ensure(8 * cap));
+    if (ctx->compact) {
+      CK(ctx->nchunks_c.ensure(8 * cap));
+      CK(ctx->cbase_c.ensure(8 * cap));
+    }
     CK(ctx->rejected.ensure(4 * cap));
     CK(ctx->wlen.ensure(cap));
     CK(ctx->spec.ensure(2ull * n));
@@ -653,6 +664,9 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
     R.states = ctx->states.as<unsigned long long>();
     R.chunk_blocks = uint32_t(ctx->chunk_blocks);
     R.xunit = ctx->xbits ? kXBitsBlocks : kXScalarBlocks;
+    R.compact = mode == Z80B_MODE_FIRST && ctx->compact ? 1u : 0u;
+    R.nchunks_c = R.compact ? ctx->nchunks_c.as<unsigned long long>() : nullptr;
+    R.cbase_c = R.compact ? ctx->cbase_c.as<unsigned long long>() : nullptr;
     if (nsurv) {
       for (;;) {
         CK(cudaMemsetAsync(R.npairs, 0, 4, s));
@@ -779,6 +793,9 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
     R.states = ctx->states.as<unsigned long long>();
     R.chunk_blocks = uint32_t(ctx->chunk_blocks);
     R.xunit = ctx->xbits ? kXBitsBlocks : kXScalarBlocks;
+    R.compact = mode == Z80B_MODE_FIRST && ctx->compact ? 1u : 0u;
+    R.nchunks_c = R.compact ? ctx->nchunks_c.as<unsigned long long>() : nullptr;
+    R.cbase_c = R.compact ? ctx->cbase_c.as<unsigned long long>() : nullptr;
     if (S) {
       launch_surv_targets(q, n, ctx->surv_target.as<uint32_t>(), s);
       CKR(check_launch(ctx, "surv_targets"));
@@ -1283,7 +1300,7 @@ int z80b_verify_pairs(z80b_ctx* ctx, const uint32_t* tgt, const uint8_t* tlens, 
     CK(ctx->cbase.ensure(8ull * n));
     CK(ctx->cbase_x.ensure(8ull * n));
     CK(ctx->rejected.ensure(4ull * n));
-    CK(ctx->counter.ensure(16));
+    CK(ctx->counter.ensure(24));
     CK(ctx->states.ensure(16));
     CK(cudaMemcpyAsync(ctx->pairs.p, pr.data(), sizeof(PairRec) * n, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(ctx->cbase.p, cb.data(), 8ull * n, cudaMemcpyHostToDevice, s));
@@ -1297,7 +1314,7 @@ int z80b_verify_pairs(z80b_ctx* ctx, const uint32_t* tgt, const uint8_t* tlens, 
     R.rejected = ctx->rejected.as<uint32_t>();
     R.counter = ctx->counter.as<unsigned long long>();
     R.states = ctx->states.as<unsigned long long>();
-    const int nl = launch_exhaustive(T, P, R, n, tot, totx, ctx->exh_k, s);
+    const int nl = launch_exhaustive(T, P, R, n, tot, totx, 0, ctx->exh_k, s);
     CKR(check_launch(ctx, "exhaustive"));
     if (nl > 1) ctx->launches += uint32_t(nl - 1);
     std::vector<uint32_t> rej(n);
@@ -1345,6 +1362,10 @@ int z80b_set_option(z80b_ctx* ctx, int option, int value) {
       if (value != 0 && value != 1) return fail(ctx, Z80B_EINVAL, "A-independent sweep option must be 0 or 1");
       ctx->xbits = value;
       return Z80B_OK;
+    case Z80B_OPT_COMPACT_SWEEP:
+      if (value != 0 && value != 1) return fail(ctx, Z80B_EINVAL, "compact sweep option must be 0 or 1");
+      ctx->compact = value;
+      return Z80B_OK;
   }
   return fail(ctx, Z80B_EINVAL, "unknown option %d", option);
 }
@@ -1357,6 +1378,7 @@ int z80b_get_option(const z80b_ctx* ctx, int option, int* value) {
     case Z80B_OPT_STREAM_PRIORITY: *value = ctx->priority; return Z80B_OK;
     case Z80B_OPT_QC_INDEX: *value = ctx->qc_index; return Z80B_OK;
     case Z80B_OPT_XINDEP_BITS: *value = ctx->xbits; return Z80B_OK;
+    case Z80B_OPT_COMPACT_SWEEP: *value = ctx->compact; return Z80B_OK;
   }
   return Z80B_EINVAL;
 }

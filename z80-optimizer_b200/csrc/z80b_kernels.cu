@@ -25,6 +25,7 @@
 #include <algorithm>
 
 #include "z80_bits.cuh"
+#include "z80_tables.h"
 #include "z80b_kernels.cuh"
 
 namespace z80b {
@@ -49,6 +50,12 @@ __constant__ uint16_t c_repsp[16];
 __device__ uint8_t g_rep[32];
 __device__ uint16_t g_repsp[16];
 __device__ uint8_t g_aclass[kNumOps];
+// compact sweep: renamed opcodes and register places per register set
+// (compact_tables), the registers each opcode names
+__device__ int16_t g_cren[kCompactSets][kNumOps];
+__device__ int8_t g_corig[kCompactSets][2];
+__device__ uint8_t g_cid[64];
+__device__ uint8_t g_opregs[kNumOps];
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 __device__ __forceinline__ unsigned lanemask_lt() {
@@ -135,6 +142,25 @@ __device__ __forceinline__ bool pair_xindep(const DevTargets& T, uint32_t t, con
   return dev_seq_aflow(T.insn + (size_t)t * T.stride, target_len(T, t)) != 0u &&
          dev_seq_aflow(P.insn + (size_t)c * P.stride, pool_len(P, c)) != 0u;
 }
+// Compact sweep: 1 + the register-set entry when the pair's instructions
+// name at most two of B..L, neither SP nor the memory byte, and all rename
+// onto B and C (compact_map); 0 otherwise.
+__device__ __forceinline__ uint8_t pair_cmap(const DevTargets& T, uint32_t t, const DevPool& P, uint32_t c) {
+  const uint32_t tl = target_len(T, t), cl = pool_len(P, c);
+  const uint32_t* tw = T.insn + (size_t)t * T.stride;
+  const uint32_t* cw = P.insn + (size_t)c * P.stride;
+  uint32_t fp = 0;
+  for (uint32_t i = 0; i < tl; i++) fp |= g_opregs[tw[i] & 0xFFFFu];
+  for (uint32_t i = 0; i < cl; i++) fp |= g_opregs[cw[i] & 0xFFFFu];
+  if (fp & 0xC0u) return 0;
+  const uint32_t id = g_cid[fp & 0x3Fu];
+  if (!id) return 0;
+  for (uint32_t i = 0; i < tl; i++)
+    if (g_cren[id - 1][tw[i] & 0xFFFFu] < 0) return 0;
+  for (uint32_t i = 0; i < cl; i++)
+    if (g_cren[id - 1][cw[i] & 0xFFFFu] < 0) return 0;
+  return uint8_t(id);
+}
 // A-dependent pairs run bit-sliced (z80_bits.cuh): a unit is 4 A-blocks, a
 // lane takes 32 consecutive values of A of one block.
 constexpr unsigned long long kBitsBlocks = 4;
@@ -153,8 +179,11 @@ __device__ __forceinline__ unsigned long long chunks_for(unsigned long long nb, 
 __device__ __forceinline__ void set_chunks(const RoundBuf& R, uint32_t p, const PairRec& pr) {
   const unsigned long long c = chunks_for(pair_units(pr.nblocks, pr.keepR, R.xunit), R.chunk_blocks);
   const bool xind = (pr.keepR & kXIndep) != 0;
-  R.nchunks[p] = xind ? 0ull : c;
+  const bool comp = pr.cmap != 0;  // only set when R.compact
+  R.nchunks[p] = (xind || comp) ? 0ull : c;
   R.nchunks_x[p] = xind ? c : 0ull;
+  if (comp) R.nchunks_c[p] = c;
+  else if (R.compact) R.nchunks_c[p] = 0ull;
 }
 __device__ __forceinline__ unsigned long long chunks_for(unsigned long long nb, uint32_t cb) {
   unsigned long long c = (nb + cb - 1) / cb;
@@ -455,6 +484,7 @@ __device__ __forceinline__ void put_pair(const RoundBuf& R, uint32_t p, const De
   pr.keepF = kind ? uint8_t(~target_dead(T, t)) : uint8_t(0xFFu);
   pr.keepR = kind ? uint8_t((~target_dead_regs(T, t) & 0x3Fu) | 0x80u) : uint8_t(0x3Fu);
   if (pair_xindep(T, t, P, c)) pr.keepR |= uint8_t(kXIndep);
+  pr.cmap = (R.compact && !(pr.keepR & kXIndep)) ? pair_cmap(T, t, P, c) : uint8_t(0);
   R.pairs[p] = pr;
   R.pair_src[p] = src;
   set_chunks(R, p, pr);
@@ -510,6 +540,7 @@ __global__ void k_pairs_from_survivors(DevTargets T, DevPool P, QCOut q, const u
     pr.keepF = uint8_t(~target_dead(T, t));
     pr.keepR = uint8_t(~target_dead_regs(T, t) & 0x3Fu);
     if (pair_xindep(T, t, P, c)) pr.keepR |= uint8_t(kXIndep);
+    pr.cmap = 0;
     have = true;
   }
   unsigned b = __ballot_sync(kFull, have);
@@ -696,6 +727,79 @@ __device__ __forceinline__ bool bits_unit(unsigned long long u, unsigned long lo
   return valid && zb_diff(z, sm, keepF, keepR) != 0u;
 }
 
+// One unit of a compact sweep: the layout of bits_unit (lane l: block 4u +
+// l/8, A = 32(l % 8) .. +31) on the compact state (A, F, B, C; ZBc).  The
+// pair's programs arrive renamed onto B and C; o0 / o1 are the original
+// registers (0..5 = B..L) that B and C stand for, or -1 where none does.
+// Only A, F (under keepF) and those registers (under keepR) can differ.
+constexpr int kCompactWords = 32;  // planes saved per lane: A, F, B, C
+__device__ __forceinline__ bool cbits_unit(unsigned long long u, unsigned long long nblocks, bool spw, bool reduced,
+                                           int nx, int fw, const int (&slot)[7], uint32_t pw, int tl, int cl,
+                                           uint32_t keepF, uint32_t keepR, int o0, int o1, uint32_t* sm) {
+  const unsigned lane = lane_id();
+  const unsigned long long blk = u * kBitsBlocks + (lane >> 3);
+  const bool valid = blk < nblocks;
+  Z80S x;
+  decode_block<false>(valid ? blk : u * kBitsBlocks, spw, reduced, nx, fw, slot, x);
+  const uint32_t a0 = (lane & 7u) * 32u;
+  auto regval = [&](int r) -> uint32_t {
+    switch (r) {
+      case 0: return x.b;
+      case 1: return x.c;
+      case 2: return x.d;
+      case 3: return x.e;
+      case 4: return x.h;
+      case 5: return x.l;
+      default: return 0u;
+    }
+  };
+  const uint32_t vb = regval(o0), vc = regval(o1);
+  ZBc z;
+  auto init = [&]() {
+    z.a[0] = 0xAAAAAAAAu;
+    z.a[1] = 0xCCCCCCCCu;
+    z.a[2] = 0xF0F0F0F0u;
+    z.a[3] = 0xFF00FF00u;
+    z.a[4] = 0xFFFF0000u;
+    z.a[5] = (a0 & 32u) ? kZBOnes : 0u;
+    z.a[6] = (a0 & 64u) ? kZBOnes : 0u;
+    z.a[7] = (a0 & 128u) ? kZBOnes : 0u;
+    zb_set8(z.f, x.f);
+    zb_set8(z.b, vb);
+    zb_set8(z.c, vc);
+    zb_set8(z.x, 0u);
+#pragma unroll
+    for (int i = 0; i < 16; i++) z.sp[i] = 0u;
+  };
+  init();
+#pragma unroll 1
+  for (int st = 0; st < tl + cl; st++) {
+    if (st == cl) {
+#pragma unroll
+      for (int i = 0; i < 8; i++) {
+        sm[(0 + i) * 32] = z.a[i];
+        sm[(8 + i) * 32] = z.f[i];
+        sm[(16 + i) * 32] = z.b[i];
+        sm[(24 + i) * 32] = z.c[i];
+      }
+      init();
+    }
+    const int src = st < cl ? tl + st : st - cl;
+    const uint32_t w = __shfl_sync(kFull, pw, src);
+    zb_step(z, w & 0xFFFFu, w >> 16);
+  }
+  const bool cmp_b = o0 >= 0 && ((keepR >> o0) & 1u), cmp_c = o1 >= 0 && ((keepR >> o1) & 1u);
+  uint32_t d = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    d |= z.a[i] ^ sm[(0 + i) * 32];
+    if ((keepF >> i) & 1u) d |= z.f[i] ^ sm[(8 + i) * 32];
+    if (cmp_b) d |= z.b[i] ^ sm[(16 + i) * 32];
+    if (cmp_c) d |= z.c[i] ^ sm[(24 + i) * 32];
+  }
+  return valid && d != 0u;
+}
+
 // A-independent sweeps, bit-sliced: lane l of a unit takes the 32 A-blocks
 // u*1024 + 32l .. +31 as one state word (block j in bit j), first at A = 0,
 // then at A = 1 (two values decide these pairs).  In an aligned group of 32
@@ -835,15 +939,16 @@ __device__ __noinline__ bool xindep_unit(unsigned long long first, unsigned long
 
 // One kernel per pair class: CLS 0 runs the bit-sliced pairs (outputs
 // depend on A), CLS 1 the A-independent ones (K states per lane per
-// dispatch), CLS 2 the A-independent ones bit-sliced; each class draws chunks
-// from its own numbering and dispenser.  Kept apart so that neither path's
-// registers weigh on the other.
+// dispatch), CLS 2 the A-independent ones bit-sliced, CLS 3 the A-dependent
+// ones whose registers fit the compact state (two blocks per SM); each class
+// draws chunks from its own numbering and dispenser.  Kept apart so that
+// neither path's registers weigh on the other.
 template <int K, int CLS>
-__global__ void __launch_bounds__(kBlock, 1) k_exhaustive(DevTargets T, DevPool P, RoundBuf R, uint32_t npairs,
-                                                       unsigned long long total) {
+__global__ void __launch_bounds__(kBlock, CLS == 3 ? 2 : 1)
+    k_exhaustive(DevTargets T, DevPool P, RoundBuf R, uint32_t npairs, unsigned long long total) {
   static_assert(K == 1 || K == 2 || K == 4 || K == 8, "K divides 8");
   constexpr bool XI = CLS != 0;
-  const unsigned long long* __restrict__ cbase = XI ? R.cbase_x : R.cbase;
+  const unsigned long long* __restrict__ cbase = CLS == 3 ? R.cbase_c : (XI ? R.cbase_x : R.cbase);
   const unsigned lane = lane_id();
   unsigned long long my_states = 0, my_eval = 0;
   // At most kChunksPerWarp chunks per warp, then the block retires: the grid
@@ -851,7 +956,7 @@ __global__ void __launch_bounds__(kBlock, 1) k_exhaustive(DevTargets T, DevPool 
   // priority) get SMs as soon as blocks of a long sweep retire.
   for (int taken = 0; taken < kChunksPerWarp; taken++) {
     unsigned long long k = 0;
-    if (lane == 0) k = atomicAdd(R.counter + (XI ? 1 : 0), 1ull);
+    if (lane == 0) k = atomicAdd(R.counter + (CLS == 3 ? 2 : (XI ? 1 : 0)), 1ull);
     k = __shfl_sync(kFull, k, 0);
     if (k >= total) break;
     // pair p: cbase[p] <= k < cbase[p + 1]
@@ -901,7 +1006,27 @@ __global__ void __launch_bounds__(kBlock, 1) k_exhaustive(DevTargets T, DevPool 
                            ((pr.keepR & 16u) ? 0xFF0000u : 0u) | ((pr.keepR & 32u) ? 0xFF000000u : 0u);
 
     bool bad = false;
-    if constexpr (!XI) {
+    if constexpr (CLS == 3) {
+      // the compact state, the programs renamed onto B and C
+      const uint32_t e = pr.cmap - 1u;
+      if (lane < tl + cl) pw = (uint32_t(uint16_t(g_cren[e][pw & 0xFFFFu]))) | (pw & 0xFFFF0000u);
+      const int o0 = g_corig[e][0], o1 = g_corig[e][1];
+      extern __shared__ uint32_t zsm[];
+      uint32_t* sm = zsm + (threadIdx.x >> 5) * (kCompactWords * 32) + lane;
+      for (unsigned long long u = u0; u < u1; u++) {
+        const unsigned long long first = u * kBitsBlocks;
+        const unsigned long long nb = (pr.nblocks - first < kBitsBlocks) ? pr.nblocks - first : kBitsBlocks;
+        bad = cbits_unit(u, pr.nblocks, spw, reduced, nx, fw, slot, pw, int(tl), int(cl), pr.keepF, pr.keepR, o0, o1,
+                         sm) ||
+              bad;
+        my_states += 256ull * nb;
+        my_eval += 256ull * nb;
+        if (__any_sync(kFull, bad)) break;
+        if ((u & 15ull) == 15ull &&
+            __shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0))
+          break;
+      }
+    } else if constexpr (!XI) {
       // Unit = 4 A-blocks, bit-sliced (256 states of each block in 8 lanes).
       // The reference nests its loops as A, carry, first register, ...,
       // last register, SP (verifier.go:498-531,578-610); the block index
@@ -1445,6 +1570,13 @@ void dev_upload_tables(cudaStream_t s) {
   cudaMemcpyToSymbolAsync(g_rep, rep_values(), 32, 0, cudaMemcpyHostToDevice, s);
   cudaMemcpyToSymbolAsync(g_repsp, rep_sp(), 32, 0, cudaMemcpyHostToDevice, s);
   cudaMemcpyToSymbolAsync(g_aclass, op_aclass(), kNumOps, 0, cudaMemcpyHostToDevice, s);
+  {
+    const CompactTables& C = compact_tables();
+    cudaMemcpyToSymbolAsync(g_cren, C.ren, sizeof C.ren, 0, cudaMemcpyHostToDevice, s);
+    cudaMemcpyToSymbolAsync(g_corig, C.orig, sizeof C.orig, 0, cudaMemcpyHostToDevice, s);
+    cudaMemcpyToSymbolAsync(g_cid, C.id_of_set, sizeof C.id_of_set, 0, cudaMemcpyHostToDevice, s);
+    cudaMemcpyToSymbolAsync(g_opregs, C.opregs, sizeof C.opregs, 0, cudaMemcpyHostToDevice, s);
+  }
 }
 
 void launch_pool_outputs(const uint32_t* insn, uint32_t n, uint32_t len, uint4* qc, uint4* mid,
@@ -1528,7 +1660,7 @@ void launch_exhaustive_k(const DevTargets& T, const DevPool& P, const RoundBuf& 
                          unsigned long long total, cudaStream_t s) {
   // shared memory (bit-sliced kernels): the candidate's output planes,
   // kBitsWords words per lane
-  constexpr int smem = CLS == 1 ? 0 : kBlock * kBitsWords * 4;
+  constexpr int smem = CLS == 1 ? 0 : kBlock * (CLS == 3 ? kCompactWords : kBitsWords) * 4;
   static int per_sm = 0;
   if (!per_sm) {
     if (smem) cudaFuncSetAttribute(k_exhaustive<K, CLS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -1547,9 +1679,14 @@ void launch_exhaustive_k(const DevTargets& T, const DevPool& P, const RoundBuf& 
 }
 
 int launch_exhaustive(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
-                      unsigned long long total_b, unsigned long long total_x, int k, cudaStream_t s) {
+                      unsigned long long total_b, unsigned long long total_x, unsigned long long total_c, int k,
+                      cudaStream_t s) {
   if (!npairs) return 0;
   int n = 0;
+  if (total_c) {
+    launch_exhaustive_k<1, 3>(T, P, R, npairs, total_c, s);
+    n++;
+  }
   if (total_b) {
     launch_exhaustive_k<1, 0>(T, P, R, npairs, total_b, s);
     n++;

@@ -68,11 +68,15 @@ struct RoundBuf {
   unsigned long long* cbase;       // exclusive prefix of nchunks
   unsigned long long* nchunks_x;   // per pair, A-independent class
   unsigned long long* cbase_x;     // exclusive prefix of nchunks_x
+  unsigned long long* nchunks_c;   // per pair, compact class (with compact set; else unused)
+  unsigned long long* cbase_c;     // exclusive prefix of nchunks_c
+  uint32_t compact;                // A-dependent pairs whose registers fit the compact state get
+                                   // their own class and kernel
   uint32_t* rejected;              // per pair
   uint8_t* wlen;                   // per pair: survivors in the window it heads (0: not a head)
   uint32_t cap;                    // pair slots of the buffers
   uint32_t* npairs;                // device counter
-  unsigned long long* counter;     // chunk dispensers: [0] bit-sliced class, [1] A-independent class
+  unsigned long long* counter;     // chunk dispensers: [0] bit-sliced, [1] A-independent, [2] compact class
   unsigned long long* states;      // [2]: states of the reference's sweeps covered, states evaluated
   uint32_t chunk_blocks;           // A-blocks per work chunk
   uint32_t xunit;                  // A-blocks per unit of an A-independent sweep: kXBitsBlocks
@@ -124,9 +128,11 @@ void launch_pairs_from_survivors(const DevTargets& T, const DevPool& P, const QC
                                  const RoundBuf& R, cudaStream_t s);
 // k = states per lane per dispatch: 1, 2, 4 or 8.
 // Launches the sweep kernel of each class that has chunks (total_b
-// bit-sliced, total_x A-independent); returns the number of launches.
+// bit-sliced, total_x A-independent, total_c compact); returns the number of
+// launches.
 int launch_exhaustive(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
-                      unsigned long long total_b, unsigned long long total_x, int k, cudaStream_t s);
+                      unsigned long long total_b, unsigned long long total_x, unsigned long long total_c, int k,
+                      cudaStream_t s);
 void launch_round_resolve(const RoundBuf& R, uint32_t npairs, const QCOut& q, const Lanes& L, uint32_t max_spec,
                           cudaStream_t s);
 void launch_midcheck(const DevTargets& T, const DevPool& P, const uint32_t* surv,

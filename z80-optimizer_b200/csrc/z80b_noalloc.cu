@@ -166,7 +166,7 @@ extern "C" int z80b_exhaustive_noalloc(int device, const uint32_t* tgt, const ui
   R.counter = reinterpret_cast<unsigned long long*>(base + kOffCounter);
   R.states = reinterpret_cast<unsigned long long*>(base + kOffStates);
   R.chunk_blocks = 32;
-  launch_exhaustive(T, P, R, n, total, total_x, 4, s);
+  launch_exhaustive(T, P, R, n, total, total_x, 0, 4, s);
   if (cudaGetLastError() != cudaSuccess) return Z80B_ECUDA;
   if (cudaMemcpyAsync(h_rej, base + kOffRej, 4ull * n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess)
