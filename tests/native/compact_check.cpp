@@ -10,7 +10,9 @@
 // B, C and shared scratch) gives the full state's A, F, B and C for every
 // opcode that names no register but B and C.  (4) The device's tables
 // (compact_tables) accept, rename and place registers as compact_map does.
-// Built and run by tests/test_tables.py.
+// (5) The compact kernel's sweep unit, restated with its plane layout and its
+// dead-flag and dead-register compares, gives the oracle's verdicts.  Built
+// and run by tests/test_tables.py.
 #include <cstdio>
 #include <random>
 
@@ -260,6 +262,89 @@ int main() {
     }
     if (agreed < 1000) {
       std::printf("too few compact pairs for the table check (%d)\n", agreed);
+      return 1;
+    }
+  }
+  // (5) the compact kernel's unit restated (cbits_unit in z80b_kernels.cu):
+  // per block and 32 values of A, the compact planes from the decoded state
+  // (B, C from the registers they stand for, 0 where none), renamed
+  // programs, A / F under the dead flags / B, C under the dead registers of
+  // the registers they stand for; against the oracle with dead registers
+  {
+    const CompactTables& T = compact_tables();
+    int cp = 0, ceq = 0;
+    for (int trial = 0; trial < 2000000 && cp < 400; trial++) {
+      const int tn = 1 + int(rng() % 2);
+      int cn = 1 + int(rng() % 2);
+      orc::Instruction ti[2], ci[2];
+      uint32_t tw[2], cw[2];
+      for (int i = 0; i < tn; i++) ti[i] = I[rng() % I.size()];
+      for (int i = 0; i < cn; i++) ci[i] = I[rng() % I.size()];
+      if (rng() % 3 == 0) {
+        ci[0] = ti[0];
+        cn = 1;
+      }
+      for (int i = 0; i < tn; i++) tw[i] = uint32_t(ti[i].op) | uint32_t(ti[i].imm) << 16;
+      for (int i = 0; i < cn; i++) cw[i] = uint32_t(ci[i].op) | uint32_t(ci[i].imm) << 16;
+      if (seq_aflow(tw, tn) && seq_aflow(cw, cn)) continue;  // the compact class takes A-dependent pairs
+      uint8_t fp = 0;
+      for (int i = 0; i < tn; i++) fp |= T.opregs[insn_op(tw[i])];
+      for (int i = 0; i < cn; i++) fp |= T.opregs[insn_op(cw[i])];
+      const int id = (fp & 0xC0) ? 0 : T.id_of_set[fp & 0x3F];
+      bool ok = id != 0;
+      for (int i = 0; i < tn && ok; i++) ok = T.ren[id - 1][insn_op(tw[i])] >= 0;
+      for (int i = 0; i < cn && ok; i++) ok = T.ren[id - 1][insn_op(cw[i])] >= 0;
+      if (!ok) continue;
+      const Shape s = shape_of(uint16_t(seq_reads(tw, tn) | seq_reads(cw, cn)));
+      if (s.nblocks > 512) continue;
+      cp++;
+      uint32_t tr[2], cr[2];
+      for (int i = 0; i < tn; i++) tr[i] = uint32_t(uint16_t(T.ren[id - 1][insn_op(tw[i])])) | (tw[i] & 0xFFFF0000u);
+      for (int i = 0; i < cn; i++) cr[i] = uint32_t(uint16_t(T.ren[id - 1][insn_op(cw[i])])) | (cw[i] & 0xFFFF0000u);
+      const int o0 = T.orig[id - 1][0], o1 = T.orig[id - 1][1];
+      const uint8_t dead = uint8_t(rng() & 0xFF), dregs = uint8_t(rng() & 0x3F);
+      const uint32_t keepF = uint8_t(~dead), keepR = ~uint32_t(dregs) & 0x3Fu;
+      const bool cmp_b = o0 >= 0 && ((keepR >> o0) & 1u), cmp_c = o1 >= 0 && ((keepR >> o1) & 1u);
+      bool bad = false;
+      for (uint64_t b = 0; b < s.nblocks && !bad; b++) {
+        const Z80S x = decode(b, s);
+        const uint32_t regs[6] = {x.b, x.c, x.d, x.e, x.h, x.l};
+        for (uint32_t a0 = 0; a0 < 256 && !bad; a0 += 32) {
+          ZBc z;
+          z.a[0] = 0xAAAAAAAAu;
+          z.a[1] = 0xCCCCCCCCu;
+          z.a[2] = 0xF0F0F0F0u;
+          z.a[3] = 0xFF00FF00u;
+          z.a[4] = 0xFFFF0000u;
+          for (int i = 5; i < 8; i++) z.a[i] = ((a0 >> i) & 1u) ? kZBOnes : 0u;
+          zb_set8(z.f, x.f);
+          zb_set8(z.b, o0 >= 0 ? regs[o0] : 0u);
+          zb_set8(z.c, o1 >= 0 ? regs[o1] : 0u);
+          zb_set8(z.x, 0u);
+          for (int i = 0; i < 16; i++) z.sp[i] = 0;
+          ZBc zc = z, zt = z;
+          for (int i = 0; i < cn; i++) zb_step(zc, insn_op(cr[i]), insn_imm(cr[i]));
+          for (int i = 0; i < tn; i++) zb_step(zt, insn_op(tr[i]), insn_imm(tr[i]));
+          uint32_t d = 0;
+          for (int i = 0; i < 8; i++) {
+            d |= zc.a[i] ^ zt.a[i];
+            if ((keepF >> i) & 1u) d |= zc.f[i] ^ zt.f[i];
+            if (cmp_b) d |= zc.b[i] ^ zt.b[i];
+            if (cmp_c) d |= zc.c[i] ^ zt.c[i];
+          }
+          bad = d != 0;
+        }
+      }
+      const bool want = orc::ExhaustiveCheckMaskedRegs(ti, tn, ci, cn, dead, dregs);
+      if (want == bad) {
+        std::printf("compact unit verdict differs: target %08x %08x (%d) candidate %08x %08x (%d) dead %02x regs %02x\n",
+                    tw[0], tn > 1 ? tw[1] : 0, tn, cw[0], cn > 1 ? cw[1] : 0, cn, dead, dregs);
+        return 1;
+      }
+      ceq += want ? 1 : 0;
+    }
+    if (cp < 200 || ceq < 30) {
+      std::printf("too few compact A-dependent pairs (%d) or equivalences (%d)\n", cp, ceq);
       return 1;
     }
   }
