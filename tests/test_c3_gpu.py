@@ -96,3 +96,30 @@ def test_a_independent_sweep_kernels_keep_parity(ctx, O, xbits):
                      r.cycles_saved, r.dead_flags)
     assert [key(r) for r in r2] == [key(r) for r in exp]
     assert st2.checked_ref == checked
+
+
+@pytest.mark.skipif(os.environ.get("Z80B_TEST_COMPACT") != "1",
+                    reason="the compact sweep kernel is off by default until it has run on a GPU "
+                           "(set Z80B_TEST_COMPACT=1)")
+def test_compact_sweep_keeps_parity(ctx, O):
+    """Z80B_OPT_COMPACT_SWEEP = 1: the C3 sample's rules and 'checked'
+    counter, and a C2 sample against the oracle, are unchanged."""
+    import workloads
+    fx = fixture()
+    old = ctx.get_option(z80b.OPT_COMPACT_SWEEP)
+    ctx.set_option(z80b.OPT_COMPACT_SWEEP, 1)
+    try:
+        rules, st = run(ctx, fx)
+        targets = workloads.to_lists(workloads.c2_subset(3000, seed=12))
+        r2, st2 = ctx.search(targets, dead_flags=0xFF)
+    finally:
+        ctx.set_option(z80b.OPT_COMPACT_SWEEP, old)
+    got = [tuple([k[0], tuple(k[1]), tuple(k[2])] + list(k[3:])) for k in dev_keys(rules)]
+    want = [tuple([r[0], tuple(r[1]), tuple(r[2])] + list(r[3:])) for r in fx["rules"]]
+    assert got == want
+    assert st.checked_ref == fx["checked"]
+    exp, checked = O.search(targets, 1, dead=0xFF)
+    key = lambda r: (r.target_index, tuple(r.src[:r.src_len]), tuple(r.rep[:r.rep_len]), r.bytes_saved,
+                     r.cycles_saved, r.dead_flags)
+    assert [key(r) for r in r2] == [key(r) for r in exp]
+    assert st2.checked_ref == checked
