@@ -360,7 +360,8 @@ def main():
               "trial_ms": [[round(tr.ms[a][b], 2) for b in range(4)] for a in range(4)],
               "grid": "lane states 1,2,4,8 x chunk blocks 8,32,128,512 on 200k targets",
               "a_independent_sweeps": ("bit-sliced" if ctx.get_option(z80b.OPT_XINDEP_BITS)
-                                       else "scalar (lane states apply)")}
+                                       else "scalar (lane states apply)"),
+              "compact_sweeps": bool(ctx.get_option(z80b.OPT_COMPACT_SWEEP))}
     progress(f"autotune: lane states {tr.lane_states}, chunk blocks {tr.chunk_blocks}")
 
     # ---- value: targets resident in HBM
