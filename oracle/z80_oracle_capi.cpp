@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <thread>
 #include <cstring>
+#include <ctime>
 #include <string>
 #include <vector>
 
@@ -124,6 +125,39 @@ int orc_should_prune(const uint32_t* seq, int n) {
   auto v = seqOf(seq, n);
   return ShouldPrune(v.data(), n);
 }
+// EnumerateSequences8's order (pkg/search/enumerator.go:319-345: an odometer
+// with position 0 most significant) over an arbitrary instruction pool,
+// keeping the sequences ShouldPrune (pruner.go:7-27) lets through.  Writes up
+// to cap sequences of n words to out and returns how many exist.
+long long orc_enumerate_pool(const uint32_t* pool, int npool, int n, uint32_t* out, long long cap) {
+  Init();
+  if (n < 1 || n > 4 || npool < 1) return 0;
+  std::vector<Instruction> P(static_cast<size_t>(npool));
+  for (int i = 0; i < npool; i++) P[size_t(i)] = unpack(pool[i]);
+  std::vector<int> idx(size_t(n), 0);
+  std::vector<Instruction> seq(size_t(n), P[0]);
+  long long k = 0;
+  while (true) {
+    if (!ShouldPrune(seq.data(), n)) {
+      if (k < cap)
+        for (int j = 0; j < n; j++) out[size_t(k) * size_t(n) + size_t(j)] = pack(seq[size_t(j)]);
+      k++;
+    }
+    int p = n - 1;
+    while (p >= 0) {
+      if (++idx[size_t(p)] < npool) {
+        seq[size_t(p)] = P[size_t(idx[size_t(p)])];
+        break;
+      }
+      idx[size_t(p)] = 0;
+      seq[size_t(p)] = P[0];
+      p--;
+    }
+    if (p < 0) break;
+  }
+  return k;
+}
+
 int orc_instructions8(uint32_t* out, int cap) {
   const auto& p = Instructions8();
   for (int i = 0; i < int(p.size()) && i < cap; i++) out[i] = pack(p[size_t(i)]);
@@ -166,8 +200,20 @@ static void toRule(const Rule& r, int ti, orc_rule* o) {
 // Targets: n sequences, stride 4 words, lengths in lens[].  Rules come out
 // grouped by target index (deterministic order).  Returns the rule count or
 // -1 if cap is too small.
+long long orc_search_timed(const uint32_t* seqs, const int* lens, int n, int maxCandLen, int dead, int workers,
+                           orc_rule* out, long long cap, unsigned long long* checked, double* secs);
 long long orc_search(const uint32_t* seqs, const int* lens, int n, int maxCandLen, int dead,
                      int workers, orc_rule* out, long long cap, unsigned long long* checked) {
+  return orc_search_timed(seqs, lens, n, maxCandLen, dead, workers, out, cap, checked, nullptr);
+}
+
+// orc_search that also reports, per target, the CPU time of its worker
+// thread spent on that target (secs[i], seconds; secs may be NULL).  The sum
+// over targets divided by the worker count is the wall time of a perfectly
+// balanced pool, which a large target set approaches; a small sample's wall
+// time is instead set by its slowest target.
+long long orc_search_timed(const uint32_t* seqs, const int* lens, int n, int maxCandLen, int dead, int workers,
+                           orc_rule* out, long long cap, unsigned long long* checked, double* secs) {
   Init();
   std::vector<std::vector<Instruction>> tg(size_t(n > 0 ? n : 0));
   for (int i = 0; i < n; i++) tg[size_t(i)] = seqOf(seqs + size_t(i) * 4, lens[i]);
@@ -180,8 +226,15 @@ long long orc_search(const uint32_t* seqs, const int* lens, int n, int maxCandLe
   for (int w = 0; w < workers; w++)
     th.emplace_back([&] {
       size_t i;
-      while ((i = next.fetch_add(1)) < tg.size())
+      while ((i = next.fetch_add(1)) < tg.size()) {
+        timespec a{}, b{};
+        if (secs) clock_gettime(CLOCK_THREAD_CPUTIME_ID, &a);
         ProcessTask(tg[i].data(), int(tg[i].size()), maxCandLen, FlagMask(dead), per[i], &st[i]);
+        if (secs) {
+          clock_gettime(CLOCK_THREAD_CPUTIME_ID, &b);
+          secs[i] = double(b.tv_sec - a.tv_sec) + 1e-9 * double(b.tv_nsec - a.tv_nsec);
+        }
+      }
     });
   for (auto& t : th) t.join();
   long long k = 0;

@@ -1,7 +1,7 @@
 """Regenerates the golden fixtures derived from the reference's data files.
 
-Run in a checkout where the reference is mounted (its path is the only
-argument, default /root/reference).  Writes:
+Usage: python tests/golden/make_fixtures.py REFERENCE_ROOT, where
+REFERENCE_ROOT is a checkout of oisee/z80-optimizer.  Writes:
   peephole_top500_pairs.json -- (source, replacement, bytes_saved,
       cycles_saved) of the reference's data/peephole_top500.json, the 500
       rules its CUDA pipeline reported for length-2 targets.  Every pair is
@@ -18,7 +18,9 @@ import json
 import os
 import sys
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit(__doc__)
+ref = sys.argv[1]
 here = os.path.dirname(os.path.abspath(__file__))
 src = json.load(open(os.path.join(ref, "data", "peephole_top500.json")))
 pairs = [{"source": r["source"], "replacement": r["replacement"],

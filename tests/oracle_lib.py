@@ -59,6 +59,13 @@ def lib():
                                      ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_uint8), ctypes.c_int,
                                      ctypes.POINTER(OrcRule), ctypes.c_longlong,
                                      ctypes.POINTER(ctypes.c_ulonglong)]
+        L.orc_search_timed.restype = ctypes.c_longlong
+        L.orc_search_timed.argtypes = [u32p, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_int, ctypes.POINTER(OrcRule),
+                                       ctypes.c_longlong, ctypes.POINTER(ctypes.c_ulonglong),
+                                       ctypes.POINTER(ctypes.c_double)]
+        L.orc_enumerate_pool.restype = ctypes.c_longlong
+        L.orc_enumerate_pool.argtypes = [u32p, ctypes.c_int, ctypes.c_int, u32p, ctypes.c_longlong]
         L.orc_search_gpu.restype = ctypes.c_longlong
         L.orc_search_gpu.argtypes = [u32p, ctypes.POINTER(ctypes.c_int), ctypes.c_int, u32p,
                                      ctypes.c_int, ctypes.c_int, ctypes.POINTER(OrcRule),
@@ -314,3 +321,105 @@ def qc_survivors(target, dead=0):
     buf = (ctypes.c_uint32 * 8192)()
     n = lib().orc_qc_survivors(arr(target), len(target), dead, buf, 8192)
     return list(buf[:n])
+
+
+def search_timed(targets, max_cand_len, dead=0, workers=0, cap=None):
+    """search() that also returns each target's worker-thread CPU seconds:
+    (rules, checked, secs list)."""
+    flat, lens = _targets(targets)
+    cap = cap or (2 * len(targets) + 16)
+    out = (OrcRule * cap)()
+    checked = ctypes.c_ulonglong()
+    secs = (ctypes.c_double * max(1, len(targets)))()
+    w = workers or os.cpu_count() or 1
+    n = lib().orc_search_timed(flat, lens, len(targets), max_cand_len, dead, w, out, cap,
+                               ctypes.byref(checked), secs)
+    assert n >= 0, "rule buffer too small"
+    return [out[i] for i in range(n)], checked.value, list(secs[:len(targets)])
+
+
+def enumerate_pool(pool, length):
+    """Unpruned sequences of `length` over `pool` in EnumerateSequences8
+    order, as a numpy uint32 array [n, length]."""
+    import numpy as np
+    p = arr(pool)
+    n = lib().orc_enumerate_pool(p, len(pool), length, None, 0)
+    out = np.zeros((n, length), dtype=np.uint32)
+    lib().orc_enumerate_pool(p, len(pool), length, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), n)
+    return out
+
+
+_C2 = None
+
+
+def c2_targets():
+    """Every unpruned length-2 sequence over the 8-bit instruction list."""
+    global _C2
+    if _C2 is None:
+        _C2 = enumerate_pool(instructions8(), 2)
+    return _C2
+
+
+def c2_subset(k, seed=0):
+    """k C2 targets drawn without replacement by index with numpy's seeded
+    generator, in index order (the same draw as the workload generator)."""
+    import numpy as np
+    allt = c2_targets()
+    rng = np.random.default_rng(seed)
+    idx = np.sort(rng.choice(len(allt), size=min(k, len(allt)), replace=False))
+    return allt[idx]
+
+
+def splitmix64(seed):
+    """The splitmix64 stream (Steele, Lea, Flood 2014)."""
+    m = (1 << 64) - 1
+    x = seed & m
+    while True:
+        x = (x + 0x9E3779B97F4A7C15) & m
+        z = x
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & m
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & m
+        yield z ^ (z >> 31)
+
+
+def c1_pool(seed=0):
+    """The small plain pool: register LD/ALU/INC/DEC, accumulator and CB
+    rotates/shifts on registers, SCF/CCF/CPL/NEG, and the immediate forms
+    with imm8 in {00,01,7F,80,FF} plus three bytes of splitmix64(seed), in
+    opcode order (immediate forms after the others)."""
+    o = ops()
+    regs = "ABCDEHL"
+    names = []
+    for d in regs:
+        names += [f"LD_{d}_{s}" for s in ("BCDEHLA" if d == "A" else regs)]
+    for pre in ["ADD_A_", "ADC_A_", "SUB_", "SBC_A_", "AND_", "XOR_", "OR_", "CP_"]:
+        names += [pre + s for s in "BCDEHLA"]
+    names += [f"INC_{r}" for r in regs] + [f"DEC_{r}" for r in regs]
+    names += ["RLCA", "RRCA", "RLA", "RRA"]
+    for k in ["RLC", "RRC", "RL", "RR", "SLA", "SRA", "SRL", "SLL"]:
+        names += [f"{k}_{r}" for r in regs]
+    names += ["SCF", "CCF", "CPL", "NEG"]
+    non_imm = sorted(o[n] for n in names)
+    imm_ops = sorted(o[n] for n in [f"LD_{d}_N" for d in regs] +
+                     ["ADD_A_N", "ADC_A_N", "SUB_N", "SBC_A_N", "AND_N", "XOR_N", "OR_N", "CP_N"])
+    g = splitmix64(seed)
+    imms = [0x00, 0x01, 0x7F, 0x80, 0xFF] + [next(g) & 0xFF for _ in range(3)]
+    return [pack(op) for op in non_imm] + [pack(op, v) for op in imm_ops for v in imms]
+
+
+def c1_targets(seed=0):
+    return enumerate_pool(c1_pool(seed), 2)
+
+
+def eligible_checks(targets):
+    """QuickCheck units of a target array (numpy uint32 [n, L]): for each
+    target, the 8-bit instructions with a shorter encoding than the target
+    that ShouldPrune keeps."""
+    import numpy as np
+    sizes = np.array([catalog(op)[3] for op in range(op_count())], dtype=np.int64)
+    pool = np.array(instructions8(), dtype=np.uint32)
+    psize = sizes[pool & 0xFFFF]
+    prune = np.array([should_prune([int(w)]) for w in pool])
+    tb = sizes[(targets & 0xFFFF)].sum(axis=1)
+    counts = np.array([np.count_nonzero((psize < b) & ~prune) for b in range(0, 16)], dtype=np.int64)
+    return int(counts[tb].sum())
