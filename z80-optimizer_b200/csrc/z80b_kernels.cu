@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 
 #include "z80_bits.cuh"
 #include "z80_tables.h"
@@ -1541,18 +1542,52 @@ __global__ void k_pair_round_build(DevTargets T, DevPool P, QCOut q1, Lanes L2, 
 
 unsigned grid_for(uint32_t n, unsigned block) { return (n + block - 1) / block; }
 
-int g_num_sms = 0;
+// Launch facts are properties of a device: its SM count, and per kernel the
+// dynamic shared-memory limit (cudaFuncSetAttribute acts on the current
+// device) and the resident blocks per SM.  They are cached per device, for
+// the device current at the launch; devices past kMaxCachedDevices are
+// queried on every launch.
+constexpr int kMaxCachedDevices = 64;
+std::atomic<int> g_num_sms[kMaxCachedDevices];
+
+int current_device() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+  return dev;
+}
+
+// Resident blocks per SM of kernel f on the current device with `smem`
+// bytes of dynamic shared memory, raising the kernel's shared-memory limit
+// to smem first when it is above the default; cache[] keeps one answer per
+// device.
+template <class F>
+int blocks_per_sm(std::atomic<int>* cache, F f, int block, size_t smem, size_t smem_limit) {
+  const int dev = current_device();
+  if (dev >= 0 && dev < kMaxCachedDevices) {
+    const int c = cache[dev].load(std::memory_order_relaxed);
+    if (c) return c;
+  }
+  if (smem_limit) cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_limit));
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, f, block, smem);
+  if (per_sm < 1) per_sm = 1;
+  if (dev >= 0 && dev < kMaxCachedDevices) cache[dev].store(per_sm, std::memory_order_relaxed);
+  return per_sm;
+}
 
 }  // namespace
 
 int dev_num_sms() {
-  if (!g_num_sms) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-    if (g_num_sms <= 0) g_num_sms = 1;
+  const int dev = current_device();
+  if (dev >= 0 && dev < kMaxCachedDevices) {
+    const int c = g_num_sms[dev].load(std::memory_order_relaxed);
+    if (c) return c;
   }
-  return g_num_sms;
+  int n = 0;
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+  if (n <= 0) n = 1;
+  if (dev >= 0 && dev < kMaxCachedDevices) g_num_sms[dev].store(n, std::memory_order_relaxed);
+  return n;
 }
 
 }  // namespace z80b
@@ -1605,11 +1640,15 @@ void launch_qc_scan(const DevTargets& T, const DevPool& P, const QCConfig& cfg, 
                     bool collect, cudaStream_t s) {
   if (!T.n) return;
   size_t smem = cfg.use_smem ? (size_t)P.n * 17 + 16 : 0;
-  static bool attr_done = false;
-  if (!attr_done) {
-    cudaFuncSetAttribute(k_qc_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_qc_scan<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_done = true;
+  // occupancy depends on smem (the pool's size), so it is cached per device
+  // only for the limit; the answer for this launch is computed each time
+  static std::atomic<int> limit_set[2][kMaxCachedDevices];
+  const int dev = current_device();
+  const bool cache_ok = dev >= 0 && dev < kMaxCachedDevices;
+  if (!cache_ok || !limit_set[collect][dev].load(std::memory_order_relaxed)) {
+    if (collect) cudaFuncSetAttribute(k_qc_scan<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    else cudaFuncSetAttribute(k_qc_scan<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (cache_ok) limit_set[collect][dev].store(1, std::memory_order_relaxed);
   }
   int per_sm = 0;
   if (collect)
@@ -1634,10 +1673,9 @@ void launch_qc_top(const unsigned long long* keys, uint32_t nv, uint32_t* top, c
 void launch_qc_bucket(const DevTargets& T, const DevPool& P, const QCConfig& cfg, const QCIndex& ix,
                       const QCOut& o, bool collect, cudaStream_t s) {
   if (!T.n) return;
-  int per_sm = 0;
-  if (collect) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_qc_bucket<true>, kBlock, 0);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_qc_bucket<false>, kBlock, 0);
-  if (per_sm < 1) per_sm = 1;
+  static std::atomic<int> occ[2][kMaxCachedDevices];
+  const int per_sm = collect ? blocks_per_sm(occ[1], k_qc_bucket<true>, kBlock, 0, 0)
+                             : blocks_per_sm(occ[0], k_qc_bucket<false>, kBlock, 0, 0);
   unsigned need = grid_for(T.n, kBlock / 32);
   unsigned grid = unsigned(dev_num_sms() * per_sm);
   if (grid > need) grid = need;
@@ -1661,12 +1699,8 @@ void launch_exhaustive_k(const DevTargets& T, const DevPool& P, const RoundBuf& 
   // shared memory (bit-sliced kernels): the candidate's output planes,
   // kBitsWords words per lane
   constexpr int smem = CLS == 1 ? 0 : kBlock * (CLS == 3 ? kCompactWords : kBitsWords) * 4;
-  static int per_sm = 0;
-  if (!per_sm) {
-    if (smem) cudaFuncSetAttribute(k_exhaustive<K, CLS>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_exhaustive<K, CLS>, kBlock, smem);
-    if (per_sm < 1) per_sm = 1;
-  }
+  static std::atomic<int> occ[kMaxCachedDevices];
+  const int per_sm = blocks_per_sm(occ, k_exhaustive<K, CLS>, kBlock, smem, smem);
   // resident blocks, or more when the chunks exceed kChunksPerWarp per warp
   const unsigned long long wpb = kBlock / 32;
   unsigned long long need = (total + wpb - 1) / wpb;
