@@ -5,7 +5,8 @@ memory (their GPU memory is budgeted elsewhere, or an allocation's implicit
 synchronization is not acceptable on their path).  It keeps its scratch in a
 fixed array inside the library, so these checks call it twice in a row (the
 second call must not see the first call's leftovers) and compare both
-results, bit for bit, with the regular context-based entry point.  This
+results, bit for bit, with the regular context-based entry point and with
+the CPU oracle's ExhaustiveCheck.  This
 file is collected last so that a failure here stops a -x run only after
 every other test has run.
 """
@@ -58,14 +59,25 @@ def _pairs(seed, n_random):
     return pairs, deads
 
 
-def test_noalloc_matches_verify_pairs_twice(ctx):
+def test_noalloc_matches_verify_pairs_twice(ctx, O):
     for call, seed in enumerate((1, 2)):
         pairs, deads = _pairs(seed, 300)
         st, got = _noalloc(pairs, deads)
         assert st == z80b.OK, st
         want = [(bits >> 2) & 1 for bits, _ in ctx.verify_pairs(pairs, dead=deads, tiers=z80b.TIER_EXH)]
         assert got == want, f"call {call}"
+        # and against the oracle's ExhaustiveCheckMasked (verifier.go:642-654) directly
+        assert got == [int(O.exhaustive(t, c, d)) for (t, c), d in zip(pairs, deads)], f"call {call}"
         assert any(got) and not all(got)
+
+
+def test_noalloc_keeps_the_callers_current_device(ctx):
+    import torch
+    before = torch.cuda.current_device()
+    pairs, deads = _pairs(4, 20)
+    st, _ = _noalloc(pairs, deads)
+    assert st == z80b.OK
+    assert torch.cuda.current_device() == before
 
 
 def test_noalloc_rejects_oversize(ctx):

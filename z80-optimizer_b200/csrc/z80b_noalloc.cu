@@ -68,6 +68,61 @@ int setup_device(int device, cudaStream_t s, unsigned char** out) {
   return Z80B_OK;
 }
 
+// The device part of z80b_exhaustive_noalloc, with `device` current and the
+// host staging (h_tgt, h_cand, h_pairs, chunk prefixes) filled; g_mu held.
+int run_on_device(int device, uint32_t n, const uint8_t* tlens, const uint8_t* clens, const uint8_t* dead,
+                  unsigned long long total, unsigned long long total_x, cudaStream_t s, uint8_t* pass) {
+  unsigned char* base = nullptr;
+  int r = setup_device(device, s, &base);
+  if (r != Z80B_OK) return r;
+
+  // The scratch keeps whatever the previous call left in it: the rejection
+  // flags and the work counters, which must start at zero, are cleared here.
+  // Calls in one process are serialized by g_mu and return only after their
+  // stream has finished, so their GPU work never overlaps; work enqueued by
+  // any other route that touched this array (e.g. a captured graph replayed
+  // later) would race with a call on it.
+  bool ok = cudaMemcpyAsync(base + kOffTgt, h_tgt, 4ull * kStride * n, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+            cudaMemcpyAsync(base + kOffCand, h_cand, 4ull * kStride * n, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+            cudaMemcpyAsync(base + kOffTLen, tlens, n, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+            cudaMemcpyAsync(base + kOffCLen, clens, n, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+            cudaMemcpyAsync(base + kOffPairs, h_pairs, sizeof(PairRec) * n, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+            cudaMemcpyAsync(base + kOffCbase, h_cbase, 8ull * n, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+            cudaMemcpyAsync(base + kOffCbaseX, h_cbase_x, 8ull * n, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+            cudaMemsetAsync(base + kOffRej, 0, 4ull * n, s) == cudaSuccess &&
+            cudaMemsetAsync(base + kOffCounter, 0, 32, s) == cudaSuccess;
+  if (dead) ok = ok && cudaMemcpyAsync(base + kOffDead, dead, n, cudaMemcpyHostToDevice, s) == cudaSuccess;
+  else ok = ok && cudaMemsetAsync(base + kOffDead, 0, n, s) == cudaSuccess;
+  if (!ok) return Z80B_ECUDA;
+
+  DevTargets T{};
+  T.insn = reinterpret_cast<const uint32_t*>(base + kOffTgt);
+  T.len = base + kOffTLen;
+  T.dead = base + kOffDead;
+  T.n = n;
+  T.stride = kStride;
+  DevPool P{};
+  P.insn = reinterpret_cast<const uint32_t*>(base + kOffCand);
+  P.lens = base + kOffCLen;
+  P.n = n;
+  P.stride = kStride;
+  RoundBuf R{};
+  R.pairs = reinterpret_cast<PairRec*>(base + kOffPairs);
+  R.cbase = reinterpret_cast<unsigned long long*>(base + kOffCbase);
+  R.cbase_x = reinterpret_cast<unsigned long long*>(base + kOffCbaseX);
+  R.rejected = reinterpret_cast<uint32_t*>(base + kOffRej);
+  R.counter = reinterpret_cast<unsigned long long*>(base + kOffCounter);
+  R.states = reinterpret_cast<unsigned long long*>(base + kOffStates);
+  R.chunk_blocks = 32;
+  launch_exhaustive(T, P, R, n, total, total_x, 0, 4, s);
+  if (cudaGetLastError() != cudaSuccess) return Z80B_ECUDA;
+  if (cudaMemcpyAsync(h_rej, base + kOffRej, 4ull * n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return Z80B_ECUDA;
+  for (uint32_t i = 0; i < n; i++) pass[i] = h_rej[i] ? 0 : 1;
+  return Z80B_OK;
+}
+
 }  // namespace
 }  // namespace z80b
 
@@ -125,52 +180,13 @@ extern "C" int z80b_exhaustive_noalloc(int device, const uint32_t* tgt, const ui
     if (p.keepR & 0x40) total_x += ch;
     else total += ch;
   }
-  if (cudaSetDevice(device) != cudaSuccess) return Z80B_ECUDA;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  unsigned char* base = nullptr;
-  int r = setup_device(device, s, &base);
-  if (r != Z80B_OK) return r;
-
-  // The scratch keeps whatever the previous call left in it: the rejection
-  // flags and the work counters, which must start at zero, are cleared here.
-  // Two calls whose work overlaps on the GPU race on this one array.
-  bool ok = cudaMemcpyAsync(base + kOffTgt, h_tgt, 4ull * kStride * n, cudaMemcpyHostToDevice, s) == cudaSuccess &&
-            cudaMemcpyAsync(base + kOffCand, h_cand, 4ull * kStride * n, cudaMemcpyHostToDevice, s) == cudaSuccess &&
-            cudaMemcpyAsync(base + kOffTLen, tlens, n, cudaMemcpyHostToDevice, s) == cudaSuccess &&
-            cudaMemcpyAsync(base + kOffCLen, clens, n, cudaMemcpyHostToDevice, s) == cudaSuccess &&
-            cudaMemcpyAsync(base + kOffPairs, h_pairs, sizeof(PairRec) * n, cudaMemcpyHostToDevice, s) == cudaSuccess &&
-            cudaMemcpyAsync(base + kOffCbase, h_cbase, 8ull * n, cudaMemcpyHostToDevice, s) == cudaSuccess &&
-            cudaMemcpyAsync(base + kOffCbaseX, h_cbase_x, 8ull * n, cudaMemcpyHostToDevice, s) == cudaSuccess &&
-            cudaMemsetAsync(base + kOffRej, 0, 4ull * n, s) == cudaSuccess &&
-            cudaMemsetAsync(base + kOffCounter, 0, 32, s) == cudaSuccess;
-  if (dead) ok = ok && cudaMemcpyAsync(base + kOffDead, dead, n, cudaMemcpyHostToDevice, s) == cudaSuccess;
-  else ok = ok && cudaMemsetAsync(base + kOffDead, 0, n, s) == cudaSuccess;
-  if (!ok) return Z80B_ECUDA;
-
-  DevTargets T{};
-  T.insn = reinterpret_cast<const uint32_t*>(base + kOffTgt);
-  T.len = base + kOffTLen;
-  T.dead = base + kOffDead;
-  T.n = n;
-  T.stride = kStride;
-  DevPool P{};
-  P.insn = reinterpret_cast<const uint32_t*>(base + kOffCand);
-  P.lens = base + kOffCLen;
-  P.n = n;
-  P.stride = kStride;
-  RoundBuf R{};
-  R.pairs = reinterpret_cast<PairRec*>(base + kOffPairs);
-  R.cbase = reinterpret_cast<unsigned long long*>(base + kOffCbase);
-  R.cbase_x = reinterpret_cast<unsigned long long*>(base + kOffCbaseX);
-  R.rejected = reinterpret_cast<uint32_t*>(base + kOffRej);
-  R.counter = reinterpret_cast<unsigned long long*>(base + kOffCounter);
-  R.states = reinterpret_cast<unsigned long long*>(base + kOffStates);
-  R.chunk_blocks = 32;
-  launch_exhaustive(T, P, R, n, total, total_x, 0, 4, s);
-  if (cudaGetLastError() != cudaSuccess) return Z80B_ECUDA;
-  if (cudaMemcpyAsync(h_rej, base + kOffRej, 4ull * n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-      cudaStreamSynchronize(s) != cudaSuccess)
-    return Z80B_ECUDA;
-  for (uint32_t i = 0; i < n; i++) pass[i] = h_rej[i] ? 0 : 1;
-  return Z80B_OK;
+  // The work runs with `device` current; the caller's current device is
+  // put back on every return path below.
+  int prev = -1;
+  if (cudaGetDevice(&prev) != cudaSuccess) return Z80B_ECUDA;
+  if (prev != device && cudaSetDevice(device) != cudaSuccess) return Z80B_ECUDA;
+  const int r = run_on_device(device, n, tlens, clens, dead, total, total_x, static_cast<cudaStream_t>(stream),
+                              pass);
+  if (prev != device && cudaSetDevice(prev) != cudaSuccess && r == Z80B_OK) return Z80B_ECUDA;
+  return r;
 }
