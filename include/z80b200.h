@@ -195,12 +195,17 @@ int z80b_fetch_rules(z80b_ctx* ctx, z80b_rule* out, uint64_t cap, uint64_t* n_ru
  * (target, candidate) pairs given as host arrays (as z80b_verify_pairs):
  * pass[i] = 1 when pair i is equivalent over the sweep, else 0.  At most
  * Z80B_NOALLOC_MAX_PAIRS pairs per call (larger n returns Z80B_ECAPACITY and
- * does nothing); stride <= 4.  stream may be NULL (default stream).
+ * does nothing); stride <= 4.  stream may be NULL (default stream).  The
+ * work runs on `device`; the calling thread's current device is the same
+ * after the call as before it.
  * The first call on a device sets the scratch up on that device (symbol
  * address, lookup tables); make that first call before any stream capture.
- * Every call reuses the same scratch: calls are serialized on the host, and
- * calls from separate processes or other threads' streams whose GPU work
- * overlaps would race on it. */
+ * Every call reuses the same scratch array (one per process and device, its
+ * contents left over from the previous call; what must start at zero is
+ * cleared by each call).  Calls in one process are serialized on the host and
+ * return only after their GPU work has finished, so they never overlap; GPU
+ * work that reaches the array by another route while a call runs (a captured
+ * copy of a call replayed later) would race with it. */
 #define Z80B_NOALLOC_MAX_PAIRS 4096
 int z80b_exhaustive_noalloc(int device, const uint32_t* tgt, const uint8_t* tlens, const uint32_t* cand,
                             const uint8_t* clens, uint32_t stride, uint32_t n, const uint8_t* dead,
@@ -278,9 +283,14 @@ int z80b_mul_search(z80b_ctx* ctx, int pool, uint8_t init_b, uint8_t init_c, uin
  * arrive while batches are in flight are admitted by the next free worker;
  * queries whose target alone implies an ExhaustiveCheck sweep of 2^32
  * states or more run alone on a low-priority stream);
- * admission charges each query's device frontier memory against
- * memory_budget.  No counterpart in the reference (its serving is one query
- * per z80opt target call). */
+ * admission charges each query the device memory its batch holds for it
+ * (lanes, survivor records at their bound for its target's size and passes,
+ * pair slots, length-2 slots, rule records) against memory_budget, and a
+ * query waits until its charge fits; z80b_server_submit returns
+ * Z80B_ECAPACITY for a query whose charge alone exceeds the budget.
+ * Answers of length-4 targets carry Z80B_ANSWER_TRUNCATED (candidates of 3
+ * instructions are not searched).  No counterpart in the reference (its
+ * serving is one query per z80opt target call). */
 typedef struct z80b_server z80b_server;
 typedef struct z80b_server_config {
   int device;
@@ -306,11 +316,18 @@ typedef struct z80b_answer {
   double service_ms;         /* batch start -> answer */
   double latency_ms;         /* submit -> answer */
   uint32_t batch_size;       /* 0: answered without device work (length-1 target) */
-  uint32_t reserved;
+  uint32_t flags;            /* Z80B_ANSWER_* */
 } z80b_answer;
+/* The query's own candidate limit (target length - 1, SearchSingle's
+ * MaxCandLen, pkg/search/search.go:27-29) is above the server's
+ * max_cand_len: only candidates of up to max_cand_len instructions were
+ * searched (length-4 targets: 3-instruction candidates were not), so a
+ * shorter 3-instruction equivalent may exist that the answer does not give. */
+#define Z80B_ANSWER_TRUNCATED 1u
 typedef struct z80b_server_stats {
   uint64_t submitted, answered, errors, batches, max_batch_seen, pending, inflight_bytes;
   double device_ms;          /* summed pipeline device time of the batches */
+  uint64_t peak_inflight_bytes; /* most frontier bytes admitted at once (never above memory_budget) */
 } z80b_server_stats;
 int z80b_server_start(const z80b_server_config* cfg, z80b_server** out);
 int z80b_server_submit(z80b_server* s, const z80b_query* q, uint32_t n);  /* thread-safe */

@@ -59,6 +59,47 @@ def test_served_answers_equal_offline_and_oracle(O):
 
 
 @pytest.mark.gpu
+def test_served_alone_equals_mixed():
+    """Continuous batching must not change answers: 240 queries that reach
+    the device, answered in a 2 s mix at 2,000 queries/s, are submitted
+    again one at a time and must get the same rules."""
+    out, (arr, lens, dead, dregs, answers) = serve_load.run(rate=2000, seconds=2.0, seed=5, verify=False)
+    assert out["answered"] == out["queries"] and out["errors"] == 0
+    idx = [k for k in sorted(answers) if lens[k] >= 2][:240]
+    assert len(idx) == 240
+    alone = serve_load.answers_alone(arr, lens, dead, dregs, idx)
+    for k in idx:
+        a = answers[k]
+        assert alone[k] == [serve_load.rule_key(a.rules[j]) for j in range(a.n_rules)], k
+    # length-4 targets are searched with candidates of at most 2 instructions and say so
+    for k, a in answers.items():
+        assert bool(a.flags & z80b.ANSWER_TRUNCATED) == (lens[k] == 4), k
+
+
+@pytest.mark.gpu
+def test_admission_budget_binds():
+    """With a 2 MiB frontier budget only a few dozen queries fit on the
+    device at once: admission waits, the in-flight charge never exceeds the
+    budget, and every answer still equals the offline answer."""
+    budget = 2 << 20
+    out, _ = serve_load.run(rate=2000, seconds=1.0, seed=6, verify=True, memory_budget=budget)
+    assert out["answered"] == out["queries"] and out["errors"] == 0
+    assert out["same_as_offline"] == out["queries"]
+    srv = out["server"]
+    assert 0 < srv["peak_inflight_bytes"] <= budget
+    assert srv["peak_inflight_bytes"] > budget // 2  # the budget was what limited admission
+    assert srv["inflight_bytes"] == 0
+    # a query whose own frontier exceeds the budget is refused at submission
+    tiny = z80b.Server(workers=1, memory_budget=4096)
+    try:
+        with pytest.raises(z80b.Z80BError) as e:
+            tiny.submit([(1, [z80b.pack(0), z80b.pack(1)], 0, 0)])
+        assert e.value.status == z80b.ECAPACITY
+    finally:
+        tiny.stop()
+
+
+@pytest.mark.gpu
 def test_server_rejects_bad_queries():
     srv = z80b.Server(workers=1)
     try:

@@ -33,6 +33,7 @@
 #include "../../include/z80b200.h"
 #include "z80_tables.h"
 #include "z80b_kernels.cuh"
+#include "z80b_engine.h"
 #include "z80b_mulopt.cuh"
 
 using namespace z80b;
@@ -1634,3 +1635,31 @@ int z80b_mul_search(z80b_ctx* ctx, int pool, uint8_t init_b, uint8_t init_c, uin
 }
 
 }  // extern "C"
+
+namespace z80b {
+
+uint64_t target_frontier_bytes(const uint32_t* seq, int len, int max_cand, bool masked) {
+  // unpruned 8-bit candidates per target byte size (the QuickCheck units of
+  // one pass), computed once
+  static const std::vector<uint32_t> elig_lt = [] {
+    std::vector<uint32_t> e(16, 0);
+    for (uint32_t w : pool8()) {
+      const int b = op_table()[insn_op(w)].size;
+      if (should_prune(&w, 1)) continue;
+      for (int t = b + 1; t < 16; t++) e[size_t(t)]++;
+    }
+    return e;
+  }();
+  const int tb = std::min(seq_bytes(seq, len), 15);
+  const uint64_t passes = masked ? 2 : 1;
+  uint64_t b = 4ull * 4 + 4 + 3;                          // target words, length, dead flags and registers
+  b += 4ull * 4 + sizeof(TargetMeta);                      // cnt_f, cnt_m, cnt_all, base, meta
+  b += passes * uint64_t(elig_lt[size_t(tb)]) * (4 + 2);   // survivor indices and flag differences
+  b += 8 + 8 + 4 + 2;                                      // next, win, windiff, spec
+  b += 128ull * (sizeof(PairRec) + 4 + 8 * 6 + 4 + 1);     // pair slots of the windows (cap 128 per target)
+  if (max_cand >= 2)
+    b += 8 + 8 + 4 + 8 + 8 + 2 + uint64_t(kSlots2) * 2 * (4 + 2);  // length-2 lanes and survivor slots
+  return b;
+}
+
+}  // namespace z80b

@@ -17,9 +17,11 @@
 // low-priority stream, and the others serve every other query on
 // high-priority streams; since the sweep kernel's blocks retire every few
 // chunks, the block scheduler hands SMs to their kernels while a giant sweep
-// runs.  Admission also charges each query's frontier memory (its
-// lanes, survivor slots and rule records on the device) against the budget
-// and waits while the in-flight total would exceed it.
+// runs.  Admission charges each query the device memory its batch holds for
+// it (z80b::target_frontier_bytes: its lanes, survivor records at their
+// bound for its target size and passes, pair slots, length-2 slots, rule
+// records) against the budget, and a query waits while the in-flight total
+// would exceed it.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -31,22 +33,23 @@
 
 #include "../../include/z80b200.h"
 #include "z80_tables.h"
+#include "z80b_engine.h"
 
 namespace {
 
 using Clock = std::chrono::steady_clock;
 
-// Device bytes one query holds while its batch runs: target and masks,
-// metadata, two first-found lanes, the length-1 survivor range, the
-// length-2 survivor slots and rule records (z80b_engine.cu's buffers).
-constexpr uint64_t kFrontierBytes = 64 + 16 + 2 * 16 + 2 * 4531 * 6 + 2 * 32 * 6 + 2 * 12;
-
 struct Pending {
   z80b_query q;
   Clock::time_point t_submit;
-  uint32_t cand;   // candidate length cap of this query
-  uint32_t klass;  // batch class: cand | giant << 2
+  uint32_t cand;    // candidate length cap of this query
+  uint32_t klass;   // batch class: cand | giant << 2
+  uint32_t flags;   // Z80B_ANSWER_* bits of its answer
+  uint64_t bytes;   // device frontier its batch holds for it (admission charge)
 };
+
+// Rule records of one query in the batch's output (full and masked rule).
+constexpr uint64_t kRuleBytes = 2 * sizeof(z80b_rule);
 
 constexpr uint64_t kGiantStates = 1ull << 32;
 
@@ -92,6 +95,7 @@ void on_target(void* user, uint32_t t, const z80b_rule* rules, uint32_t n) {
   a.queued_ms = ms_between(p.t_submit, b->t_start);
   a.service_ms = ms_between(b->t_start, now);
   a.latency_ms = ms_between(p.t_submit, now);
+  a.flags = p.flags;
   for (uint32_t k = 0; k < n && k < 2; k++) a.rules[a.n_rules++] = rules[k];
   b->answered[t] = 1;
   {
@@ -126,7 +130,8 @@ void worker_loop(z80b_server* S, z80b_ctx* ctx, int role) {
         return first_any;
       };
       S->cv_work.wait(lk, [&] {
-        return S->stopping || (pick() && S->inflight_bytes + kFrontierBytes <= S->cfg.memory_budget);
+        const Pending* h = pick();
+        return S->stopping || (h && S->inflight_bytes + h->bytes <= S->cfg.memory_budget);
       });
       const Pending* head = pick();
       if (!head) {
@@ -137,9 +142,10 @@ void worker_loop(z80b_server* S, z80b_ctx* ctx, int role) {
       const uint32_t klass = head->klass;
       const uint32_t cap = (klass & 4u) ? 1u : S->cfg.max_batch;  // giants run alone
       for (auto it = S->pending.begin(); it != S->pending.end() && batch.size() < cap;) {
-        if (it->klass == klass && S->inflight_bytes + kFrontierBytes <= S->cfg.memory_budget) {
+        if (it->klass == klass && S->inflight_bytes + it->bytes <= S->cfg.memory_budget) {
           batch.push_back(*it);
-          S->inflight_bytes += kFrontierBytes;
+          S->inflight_bytes += it->bytes;
+          S->stats.peak_inflight_bytes = std::max(S->stats.peak_inflight_bytes, S->inflight_bytes);
           it = S->pending.erase(it);
         } else {
           ++it;
@@ -194,11 +200,14 @@ void worker_loop(z80b_server* S, z80b_ctx* ctx, int role) {
       a.queued_ms = ms_between(batch[i].t_submit, t_start);
       a.service_ms = ms_between(t_start, t_end);
       a.latency_ms = ms_between(batch[i].t_submit, t_end);
+      a.flags = batch[i].flags;
       ans.push_back(a);
     }
+    uint64_t held = 0;
+    for (const Pending& p : batch) held += p.bytes;
     {
       std::lock_guard<std::mutex> lk(S->mu);
-      S->inflight_bytes -= uint64_t(n) * kFrontierBytes;
+      S->inflight_bytes -= held;
       for (auto& a : ans) S->done.push_back(a);
       S->stats.answered += ans.size();
       S->stats.device_ms += st.device_ms;
@@ -224,7 +233,6 @@ int z80b_server_start(const z80b_server_config* cfg, z80b_server** out) {
   if (c.memory_budget == 0) c.memory_budget = 64ull << 30;
   if (c.max_cand_len == 0) c.max_cand_len = 2;
   if (c.max_cand_len > 2) return Z80B_EINVAL;
-  if (c.memory_budget < kFrontierBytes) return Z80B_EINVAL;
   z80b_server* S = new z80b_server();
   S->cfg = c;
   for (int w = 0; w < c.workers; w++) {
@@ -252,6 +260,11 @@ int z80b_server_submit(z80b_server* S, const z80b_query* q, uint32_t n) {
     if (q[i].len < 1 || q[i].len > 4 || (q[i].dead_regs & ~0x3Fu)) return Z80B_EINVAL;
     for (uint32_t k = 0; k < q[i].len; k++)
       if ((q[i].target[k] & 0xFFFFu) >= Z80B_NUM_OPS) return Z80B_EINVAL;
+    // a query whose frontier alone exceeds the budget could never be admitted
+    const uint32_t cap = std::min<uint32_t>(uint32_t(q[i].len) - 1, S->cfg.max_cand_len);
+    if (cap && z80b::target_frontier_bytes(q[i].target, int(q[i].len), int(cap), q[i].dead_flags || q[i].dead_regs) +
+                       kRuleBytes > S->cfg.memory_budget)
+      return Z80B_ECAPACITY;
   }
   const auto now = Clock::now();
   {
@@ -259,7 +272,11 @@ int z80b_server_submit(z80b_server* S, const z80b_query* q, uint32_t n) {
     if (S->stopping) return Z80B_ESTATE;
     for (uint32_t i = 0; i < n; i++) {
       S->stats.submitted++;
-      const uint32_t cap = std::min<uint32_t>(uint32_t(q[i].len) - 1, S->cfg.max_cand_len);
+      // SearchSingle's MaxCandLen is the target length - 1 (pkg/search/search.go:27-29);
+      // the server searches at most max_cand_len (<= 2) and says so when it cut
+      const uint32_t want = uint32_t(q[i].len) - 1;
+      const uint32_t cap = std::min<uint32_t>(want, S->cfg.max_cand_len);
+      const uint32_t flags = cap < want ? Z80B_ANSWER_TRUNCATED : 0u;
       if (cap == 0) {
         // a single instruction has no shorter equivalent (MaxCandLen = 0)
         z80b_answer a;
@@ -272,7 +289,10 @@ int z80b_server_submit(z80b_server* S, const z80b_query* q, uint32_t n) {
       }
       const bool giant =
           z80b::sweep_for(z80b::seq_reads(q[i].target, int(q[i].len))).states >= kGiantStates;
-      S->pending.push_back(Pending{q[i], now, cap, cap | (giant ? 4u : 0u)});
+      const uint64_t bytes =
+          z80b::target_frontier_bytes(q[i].target, int(q[i].len), int(cap), q[i].dead_flags || q[i].dead_regs) +
+          kRuleBytes;
+      S->pending.push_back(Pending{q[i], now, cap, cap | (giant ? 4u : 0u), flags, bytes});
     }
   }
   S->cv_work.notify_all();

@@ -106,6 +106,7 @@ RULE_CB = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void
 OPT_EXH_LANE_STATES, OPT_EXH_CHUNK_BLOCKS, OPT_STREAM_PRIORITY, OPT_QC_INDEX, OPT_XINDEP_BITS = 1, 2, 3, 4, 5
 OPT_COMPACT_SWEEP = 6
 JOB_NO_EXHAUSTIVE = 1
+ANSWER_TRUNCATED = 1
 
 
 MULPOOL_MULOPT, MULPOOL_WIDE21, MULPOOL_FAST14, MULPOOL_CUDA21 = 0, 1, 2, 3
@@ -135,7 +136,7 @@ class Query(ctypes.Structure):
 class Answer(ctypes.Structure):
     _fields_ = [("id", ctypes.c_uint64), ("status", ctypes.c_int32), ("n_rules", ctypes.c_int32),
                 ("rules", Rule * 2), ("queued_ms", ctypes.c_double), ("service_ms", ctypes.c_double),
-                ("latency_ms", ctypes.c_double), ("batch_size", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("latency_ms", ctypes.c_double), ("batch_size", ctypes.c_uint32), ("flags", ctypes.c_uint32)]
 
 
 class ServerConfig(ctypes.Structure):
@@ -145,7 +146,8 @@ class ServerConfig(ctypes.Structure):
 
 class ServerStats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_uint64) for k in ("submitted", "answered", "errors", "batches", "max_batch_seen",
-                                               "pending", "inflight_bytes")] + [("device_ms", ctypes.c_double)]
+                                               "pending", "inflight_bytes")] + [("device_ms", ctypes.c_double),
+                                                                                 ("peak_inflight_bytes", ctypes.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
