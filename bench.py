@@ -1,11 +1,11 @@
 """Benchmark of the candidate-verification path on B200.
 
-Workload (default): a seeded uniform sample (1,000,000 targets, seed 0, by
-index) of every unpruned length-2 target over the reference's 8-bit
-instruction list (9,818,041 targets), candidates of length 1, the
-first-found semantics of pkg/search (QuickCheck -> ExhaustiveCheck per
-target, shortest/first candidate wins).  One step = one pass of the whole
-pipeline over the sample.  `--targets 0` runs the full target set.
+Workload (default): every unpruned length-2 target over the reference's
+8-bit instruction list (9,818,041 targets, the C2 configuration),
+candidates of length 1, the first-found semantics of pkg/search
+(QuickCheck -> ExhaustiveCheck per target, shortest/first candidate wins).
+One step = one pass of the whole pipeline over the targets.  `--targets N`
+runs a seeded sample of N of them instead.
 
 Metric: candidate checks/s = (target, candidate) pairs of the workload that
 pass the byte-size and prune filters (the QuickCheck unit of work), per
@@ -15,9 +15,16 @@ library's stream); `e2e` calls z80b_search with pinned host buffers, so
 every step includes the H2D copy of the targets and the D2H copy of the
 rules.  Between steps L2 is flushed by writing a 512 MiB buffer.
 
-`--impl reference` times the CPU oracle (the C++ restatement of the
-reference's Go search; the Go toolchain is not available) on a bounded
-sample of the same workload with all host threads.
+CPU figures (the `cpu_baseline` leg and `--impl reference`) come from the
+oracle, the C++ restatement of the reference's Go search (no Go toolchain
+exists on the box), run on one fixed CPU sample of the workload: the
+100,000 targets drawn by index with default_rng(0) (the C2 parity subset)
+on all host threads.  Their time is the worker threads' CPU time divided by
+the thread count (a balanced pool's wall time; one slow target does not
+serialise a small sample), and a target whose sweeps need more than
+CPU_TARGET_BUDGET_S of CPU is left out of checks and time alike (the sweep
+tail; its count is reported).  `--impl reference` loads only the oracle:
+the target set, the sample and the check count all come from it.
 """
 import argparse
 import ctypes
@@ -46,25 +53,26 @@ def progress(*a):
     print(f"[bench {time.perf_counter() - T0:8.2f}s]", *a, file=sys.stderr, flush=True)
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--targets", type=int, default=1000000,
+    ap.add_argument("--targets", type=int, default=0,
                     help="seeded uniform sample of the C2 targets (0 = all 9,818,041)")
     ap.add_argument("--plain-sample", type=int, default=2000,
                     help="targets of the plain-vs-batched comparison (0 = skip)")
     ap.add_argument("--dead-flags", default="none")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-sample", type=int, default=0, help="targets in the CPU sample (0 = auto)")
+    ap.add_argument("--cpu-sample", type=int, default=100000,
+                    help="targets in the CPU sample (drawn by index with default_rng(0))")
     ap.add_argument("--no-mulopt", action="store_true", help="skip the constant-multiply leg")
     ap.add_argument("--c3-targets", type=int, default=100000, help="C3 sample size (0 = skip the C3 leg)")
-    ap.add_argument("--serve-seconds", type=float, default=10.0, help="served-query leg length (0 = skip)")
+    ap.add_argument("--serve-seconds", type=float, default=60.0, help="served-query leg length (0 = skip)")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="Poisson arrival rate of the served leg")
     ap.add_argument("--mulopt-max-len", type=int, default=9)
-    return ap.parse_args()
+    return ap.parse_args(argv)
 
 
 class ClockSampler:
@@ -113,20 +121,6 @@ class ClockSampler:
                 "samples": len(self.rows)}
 
 
-def eligible_checks(targets):
-    """QuickCheck units of a target set: candidates of the 4,531-instruction
-    list shorter than the target and not pruned (162 one-byte ones for a
-    two-byte target, 4,523 otherwise)."""
-    import z80b
-    sizes = np.array([z80b.op_info(op)["size"] for op in range(455)], dtype=np.int32)
-    pool = np.array(z80b.pool8(), dtype=np.uint32)
-    psize = sizes[pool & 0xFFFF]
-    prune = np.array([z80b.should_prune([int(w)]) for w in pool])
-    tb = sizes[(targets & 0xFFFF)].sum(axis=1)
-    counts = np.array([np.count_nonzero((psize < b) & ~prune) for b in range(0, 9)], dtype=np.int64)
-    return int(counts[tb].sum())
-
-
 def make_job(z80b, arr, dead):
     n, L = arr.shape
     job = z80b.Job()
@@ -141,26 +135,61 @@ def make_job(z80b, arr, dead):
     return job
 
 
-def cpu_run(sample, dead, workers):
-    """Oracle (CPU restatement of the reference search) over a target sample;
-    returns (seconds, rules)."""
+def cpu_sample(allt, n, seed=0):
+    """The CPU sample: n targets of the workload drawn by index with
+    default_rng(seed), in index order (for all C2 targets and n = 100,000,
+    the C2 parity subset)."""
+    rng = np.random.default_rng(seed)
+    idx = np.sort(rng.choice(len(allt), size=min(n, len(allt)), replace=False))
+    return allt[idx]
+
+
+# CPU seconds one target may spend in its ExhaustiveCheck sweeps in the timed
+# CPU sample: the sweep tail (true equivalences swept over up to 2^34
+# states, about 10 minutes each on one core) would otherwise hold a pass for
+# many minutes.  Targets that run past it are left out of the checks and the
+# time alike, so the CPU rate shown is the rate without that tail (an upper
+# bound on the CPU's rate over the whole workload).
+CPU_TARGET_BUDGET_S = 2.0
+
+
+def cpu_pass(sample, dead, workers):
+    """The oracle (CPU restatement of pkg/search worker.go:124-265, one task
+    per target on `workers` threads) over `sample`.  Returns (balanced
+    seconds, wall seconds, per-target seconds (-1: abandoned), candidate
+    checks of the finished targets, rules): balanced seconds = the threads'
+    CPU time on the finished targets / workers, the wall time of a busy pool,
+    which the whole workload approaches; a small sample's wall time is
+    bounded below by its slowest target instead."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_lib
     t0 = time.perf_counter()
-    rules, _ = oracle_lib.search([list(map(int, r)) for r in sample], 1, dead=dead, workers=workers)
-    return time.perf_counter() - t0, len(rules)
+    rules, _, secs = oracle_lib.search_timed([list(map(int, r)) for r in sample], 1, dead=dead, workers=workers,
+                                             target_budget=CPU_TARGET_BUDGET_S)
+    wall = time.perf_counter() - t0
+    done = np.array([x >= 0 for x in secs], dtype=bool)
+    checks = oracle_lib.eligible_checks(sample[done]) if done.any() else 0
+    return sum(x for x in secs if x >= 0) / workers, wall, secs, checks, len(rules)
 
 
-def cpu_baseline(all_targets, dead, n_sample, seed=1):
+def tail_note(secs):
+    """The sweep-size tail of a sample: the targets abandoned at the budget,
+    and how much of the finished targets' CPU time the slowest ones take."""
+    fin = sorted((x for x in secs if x >= 0), reverse=True)
+    tot = sum(fin) or 1.0
+    return (f"{sum(1 for x in secs if x < 0)} targets abandoned after {CPU_TARGET_BUDGET_S:.0f} CPU s of sweeps "
+            f"and left out (sweep tail); of the finished ones the slowest took {fin[0] if fin else 0:.2f} s, the "
+            f"10 slowest {100 * sum(fin[:10]) / tot:.1f}% of the CPU time")
+
+
+def cpu_baseline(allt, dead, n_sample):
     workers = os.cpu_count() or 1
-    rng = np.random.default_rng(seed)
-    idx = np.sort(rng.choice(len(all_targets), size=min(n_sample, len(all_targets)), replace=False))
-    sample = all_targets[idx]
-    secs, _ = cpu_run(sample, dead, workers)
-    checks = eligible_checks(sample)
-    return {"value": checks / secs, "unit": UNIT, "cores": workers, "kind": "port",
-            "sample": f"{len(sample)} targets drawn by index (seed {seed}) from the workload; "
-                      f"{checks} candidate checks in {secs:.2f} s with {workers} threads"}
+    sample = cpu_sample(allt, n_sample)
+    bal, wall, secs, checks, _ = cpu_pass(sample, dead, workers)
+    return {"value": checks / bal, "unit": UNIT, "cores": workers, "kind": "port",
+            "sample": f"{len(sample)} targets drawn by index (default_rng(0)) from the workload, one pass on "
+                      f"{workers} threads: {checks} candidate checks, {bal:.2f} s balanced ({wall:.2f} s wall); "
+                      + tail_note(secs)}
 
 
 def mulopt_leg(ctx, z80b, workloads, args, with_cpu):
@@ -283,11 +312,61 @@ def c3_leg(ctx, z80b, workloads, args):
     return out
 
 
-def auto_cpu_sample():
-    # 16,000 targets (seed 1) are ~200 core-seconds of oracle work; the
-    # sweep-size tail (true equivalences with 2^34-state reduced sweeps, ~1 in
-    # 100k targets) makes much larger samples unbounded on the CPU
-    return 16000
+C2_TARGETS = 9818041  # unpruned length-2 targets over the 8-bit list (checked by the tests)
+
+
+def workload_config(args, world):
+    """The `config` object of both arms' JSON lines."""
+    nsel = min(args.targets, C2_TARGETS) if args.targets else C2_TARGETS
+    return {"workload": "length-2 targets (C2)" + (f", seeded sample of {nsel} / {C2_TARGETS}"
+                                                 if args.targets else ", all"),
+            "targets": nsel, "target_len": 2,
+            "max_cand_len": 1, "candidates": 4531, "semantics": "pkg/search first-found",
+            "dead_flags": args.dead_flags, "vectors": "reference QuickCheck 8 (verifier.go:19-28)",
+            "l2": "flushed between steps (512 MiB write)", "path": "batched",
+            "parallelism": f"targets sharded over {world} GPU(s)"}
+
+
+def reference_arm(args, rank, workload):
+    """The reference's CPU path (the oracle: the Go toolchain is absent) on
+    the workload's CPU sample, loading only the oracle.  Warm-up steps run
+    200 other targets; the timed steps split the CPU sample into `steps`
+    consecutive parts, so all timed steps together make one pass over it
+    (the same sample and the same time measure as the `cpu_baseline` leg of
+    the GPU arm).  Under torchrun only rank 0 runs."""
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib
+    dead = oracle_lib.parse_dead_flags(args.dead_flags)
+    if dead is None:
+        raise SystemExit(f"bad --dead-flags value {args.dead_flags!r}")
+    full = oracle_lib.c2_targets()
+    assert len(full) == C2_TARGETS
+    allt = oracle_lib.c2_subset(args.targets, seed=0) if args.targets else full
+    workers = os.cpu_count() or 1
+    sample = cpu_sample(allt, args.cpu_sample)
+    warm = cpu_sample(allt, 200, seed=99)
+    for i in range(args.warmup):
+        cpu_pass(warm, dead, workers)
+        progress(f"reference warmup {i}")
+    bal, wall, checks, secs = 0.0, 0.0, 0, []
+    for part in np.array_split(sample, args.steps):
+        b, w, s, c, _ = cpu_pass(part, dead, workers)
+        bal, wall, checks, secs = bal + b, wall + w, checks + c, secs + s
+        progress(f"reference step: {len(part)} targets, {b:.2f} s balanced, {w:.2f} s wall")
+    value = checks / bal
+    note = (f"{len(sample)} targets drawn by index (default_rng(0)) from the workload, split into {args.steps} "
+            f"steps of ~{len(sample) // args.steps} on {workers} threads: {checks} candidate checks, {bal:.2f} s "
+            f"balanced ({wall:.2f} s wall); " + tail_note(secs))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * bal / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic", "config": workload,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port", "sample": note},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
 
 
 def main():
@@ -296,46 +375,20 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
+    # The workload description is built before either arm loads anything, so
+    # both arms print the same config.
+    workload = workload_config(args, world)
+    ntot = C2_TARGETS
+
+    if args.impl == "reference":
+        return reference_arm(args, rank, workload)
+
     import z80b
     import workloads
     dead = z80b.parse_dead_flags(args.dead_flags)
     full = workloads.c2_targets()
+    assert len(full) == ntot
     allt = workloads.c2_subset(args.targets, seed=0) if args.targets else full
-    workload = {"workload": "length-2 targets (C2)" + (f", seeded sample of {len(allt)} / {len(full)}"
-                                                     if args.targets else ", all"),
-                "targets": int(len(allt)), "target_len": 2,
-                "max_cand_len": 1, "candidates": 4531, "semantics": "pkg/search first-found",
-                "dead_flags": dead, "vectors": "reference QuickCheck 8 (verifier.go:19-28)",
-                "l2": "flushed between steps (512 MiB write)"}
-
-    if args.impl == "reference":
-        if rank != 0:
-            return 0
-        n_sample = args.cpu_sample or auto_cpu_sample()
-        workers = os.cpu_count() or 1
-        times, checks = [], 0
-        rng = np.random.default_rng(1)
-        idx = np.sort(rng.choice(len(allt), size=min(n_sample, len(allt)), replace=False))
-        # every second target of the CPU-baseline sample: each step stays near
-        # 10 s on 16 threads, so the default 23 steps end within a few minutes
-        sample = allt[idx[::2]]
-        for i in range(args.warmup + args.steps):
-            secs, _ = cpu_run(sample, dead, workers)
-            if i >= args.warmup:
-                times.append(secs)
-                checks += eligible_checks(sample)
-        total = sum(times)
-        value = checks / total
-        line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
-                "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u8",
-                "data": "synthetic", "config": dict(workload, sample_targets_per_step=int(len(sample))),
-                "cpu_baseline": {"value": value, "unit": UNIT, "cores": workers, "kind": "port",
-                                 "sample": f"{len(sample)} targets per step (every second target of the seeded "
-                                           f"draw by index, seed 1, of the CPU-baseline sample; the same every step)"},
-                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-        print(json.dumps(line), flush=True)
-        return 0
 
     import torch
     dist = None
@@ -518,13 +571,13 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(allt, dead, args.cpu_sample or auto_cpu_sample())
+        cpu = cpu_baseline(allt, dead, args.cpu_sample)
         progress(f"cpu baseline: {cpu['sample']}")
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_step, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-            "config": dict(workload, path="batched", parallelism=f"targets sharded over {world} GPU(s)"),
+            "config": workload,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": 1e3 * e2e_step},
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(),

@@ -184,6 +184,13 @@ uint16_t OpWrites(uint16_t op);
 uint16_t RegsRead(const Instruction* seq, int n);
 // Sweep size of ExhaustiveCheck for a pair (number of compared states).
 uint64_t ExhaustiveStates(const Instruction* t, int tn, const Instruction* c, int cn);
+// A CPU-time budget (seconds of the calling thread, from now; <= 0: none)
+// for the thread's ExhaustiveCheck sweeps.  Once spent, sweeps report
+// "not equivalent" at once and SweepBudgetSpent() is true: the results the
+// thread computes from then on are void.  Bounds a timed CPU sample; the
+// parity tests never set it.
+void SetSweepBudget(double seconds);
+bool SweepBudgetSpent();
 
 // pkg/search/pruner.go
 bool ShouldPrune(const Instruction* seq, int n);

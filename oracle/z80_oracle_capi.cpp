@@ -201,19 +201,25 @@ static void toRule(const Rule& r, int ti, orc_rule* o) {
 // grouped by target index (deterministic order).  Returns the rule count or
 // -1 if cap is too small.
 long long orc_search_timed(const uint32_t* seqs, const int* lens, int n, int maxCandLen, int dead, int workers,
-                           orc_rule* out, long long cap, unsigned long long* checked, double* secs);
+                           orc_rule* out, long long cap, unsigned long long* checked, double* secs,
+                           double target_budget);
 long long orc_search(const uint32_t* seqs, const int* lens, int n, int maxCandLen, int dead,
                      int workers, orc_rule* out, long long cap, unsigned long long* checked) {
-  return orc_search_timed(seqs, lens, n, maxCandLen, dead, workers, out, cap, checked, nullptr);
+  return orc_search_timed(seqs, lens, n, maxCandLen, dead, workers, out, cap, checked, nullptr, 0);
 }
 
 // orc_search that also reports, per target, the CPU time of its worker
 // thread spent on that target (secs[i], seconds; secs may be NULL).  The sum
 // over targets divided by the worker count is the wall time of a perfectly
 // balanced pool, which a large target set approaches; a small sample's wall
-// time is instead set by its slowest target.
+// time is instead set by its slowest target.  With target_budget > 0 a
+// target whose ExhaustiveCheck sweeps run past that many CPU seconds is
+// abandoned: secs[i] = -1 and none of its rules or its `checked` count are
+// reported (a bounded CPU sample; the tail it leaves out is counted by the
+// caller from the -1 entries).
 long long orc_search_timed(const uint32_t* seqs, const int* lens, int n, int maxCandLen, int dead, int workers,
-                           orc_rule* out, long long cap, unsigned long long* checked, double* secs) {
+                           orc_rule* out, long long cap, unsigned long long* checked, double* secs,
+                           double target_budget) {
   Init();
   std::vector<std::vector<Instruction>> tg(size_t(n > 0 ? n : 0));
   for (int i = 0; i < n; i++) tg[size_t(i)] = seqOf(seqs + size_t(i) * 4, lens[i]);
@@ -229,10 +235,17 @@ long long orc_search_timed(const uint32_t* seqs, const int* lens, int n, int max
       while ((i = next.fetch_add(1)) < tg.size()) {
         timespec a{}, b{};
         if (secs) clock_gettime(CLOCK_THREAD_CPUTIME_ID, &a);
+        if (target_budget > 0) SetSweepBudget(target_budget);
         ProcessTask(tg[i].data(), int(tg[i].size()), maxCandLen, FlagMask(dead), per[i], &st[i]);
+        const bool abandoned = target_budget > 0 && SweepBudgetSpent();
+        SetSweepBudget(0);
+        if (abandoned) {
+          per[i].clear();
+          st[i] = SearchStats{};
+        }
         if (secs) {
           clock_gettime(CLOCK_THREAD_CPUTIME_ID, &b);
-          secs[i] = double(b.tv_sec - a.tv_sec) + 1e-9 * double(b.tv_nsec - a.tv_nsec);
+          secs[i] = abandoned ? -1.0 : double(b.tv_sec - a.tv_sec) + 1e-9 * double(b.tv_nsec - a.tv_nsec);
         }
       }
     });

@@ -6,6 +6,7 @@
 #include <cctype>
 #include <cstdio>
 #include <cstring>
+#include <ctime>
 #include <thread>
 
 #include "z80_oracle.h"
@@ -259,6 +260,28 @@ static void setReg(State& s, int off, uint8_t v) {
   }
 }
 
+// Optional CPU-time budget of the calling thread's ExhaustiveCheck sweeps
+// (SetSweepBudget; used to bound a timed CPU sample, never by the parity
+// tests).  Unset, every sweep runs to its end as the reference's does.
+struct SweepBudget {
+  double deadline = 0;  // thread CPU seconds; 0: no budget
+  uint32_t tick = 0;
+  bool spent = false;
+};
+static thread_local SweepBudget t_budget;
+
+static double threadCpuSeconds() {
+  timespec ts{};
+  clock_gettime(CLOCK_THREAD_CPUTIME_ID, &ts);
+  return double(ts.tv_sec) + 1e-9 * double(ts.tv_nsec);
+}
+
+void SetSweepBudget(double seconds) {
+  t_budget = SweepBudget{};
+  if (seconds > 0) t_budget.deadline = threadCpuSeconds() + seconds;
+}
+bool SweepBudgetSpent() { return t_budget.spent; }
+
 struct Pair {
   const Instruction* t;
   int tn;
@@ -267,6 +290,13 @@ struct Pair {
   FlagMask dead;
   uint8_t dregs;
   bool cmp(const State& s) const {
+    if (t_budget.deadline > 0) {
+      // every 65,536 states, look at the clock; once the budget is spent every
+      // sweep of this thread stops at its next state (the caller discards
+      // the target's result)
+      if ((++t_budget.tick & 0xFFFFu) == 0 && threadCpuSeconds() > t_budget.deadline) t_budget.spent = true;
+      if (t_budget.spent) return false;
+    }
     return StatesEqualMaskedRegs(ExecSeq(s, t, tn), ExecSeq(s, c, cn), dead, dregs);
   }
 };

@@ -63,7 +63,7 @@ def lib():
         L.orc_search_timed.argtypes = [u32p, ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int,
                                        ctypes.c_int, ctypes.c_int, ctypes.POINTER(OrcRule),
                                        ctypes.c_longlong, ctypes.POINTER(ctypes.c_ulonglong),
-                                       ctypes.POINTER(ctypes.c_double)]
+                                       ctypes.POINTER(ctypes.c_double), ctypes.c_double]
         L.orc_enumerate_pool.restype = ctypes.c_longlong
         L.orc_enumerate_pool.argtypes = [u32p, ctypes.c_int, ctypes.c_int, u32p, ctypes.c_longlong]
         L.orc_search_gpu.restype = ctypes.c_longlong
@@ -323,9 +323,11 @@ def qc_survivors(target, dead=0):
     return list(buf[:n])
 
 
-def search_timed(targets, max_cand_len, dead=0, workers=0, cap=None):
+def search_timed(targets, max_cand_len, dead=0, workers=0, cap=None, target_budget=0.0):
     """search() that also returns each target's worker-thread CPU seconds:
-    (rules, checked, secs list)."""
+    (rules, checked, secs list).  With target_budget > 0, a target whose
+    sweeps run past that many CPU seconds is abandoned: secs = -1, and its
+    rules and checked count are left out."""
     flat, lens = _targets(targets)
     cap = cap or (2 * len(targets) + 16)
     out = (OrcRule * cap)()
@@ -333,7 +335,7 @@ def search_timed(targets, max_cand_len, dead=0, workers=0, cap=None):
     secs = (ctypes.c_double * max(1, len(targets)))()
     w = workers or os.cpu_count() or 1
     n = lib().orc_search_timed(flat, lens, len(targets), max_cand_len, dead, w, out, cap,
-                               ctypes.byref(checked), secs)
+                               ctypes.byref(checked), secs, float(target_budget))
     assert n >= 0, "rule buffer too small"
     return [out[i] for i in range(n)], checked.value, list(secs[:len(targets)])
 
@@ -423,3 +425,4 @@ def eligible_checks(targets):
     tb = sizes[(targets & 0xFFFF)].sum(axis=1)
     counts = np.array([np.count_nonzero((psize < b) & ~prune) for b in range(0, 16)], dtype=np.int64)
     return int(counts[tb].sum())
+
