@@ -3,6 +3,8 @@
 Every comparison is bit-exact: states, fingerprints, verifier verdicts,
 FlagDiff masks, rule lists and the reference's 'checked' counter.
 """
+import hashlib
+import json
 import os
 import random
 
@@ -14,7 +16,20 @@ import z80b
 
 pytestmark = pytest.mark.gpu
 
-FULL = os.environ.get("Z80B_FULL_PARITY") == "1"
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def golden(name):
+    with open(os.path.join(GOLDEN, name)) as f:
+        return json.load(f)
+
+
+def digest(arr):
+    return hashlib.sha256(np.ascontiguousarray(arr, dtype="<u4").tobytes()).hexdigest()
+
+
+def fixture_keys(rules):
+    return [(r[0], tuple(r[1]), tuple(r[2]), r[3], r[4], r[5]) for r in rules]
 
 
 def rule_keys(rules):
@@ -153,22 +168,38 @@ def _search_both(ctx, O, targets, dead=0, path=z80b.PATH_BATCHED, per_target_dea
     return rules, st, exp, checked
 
 
-@pytest.mark.parametrize("dead", [0x00, 0xFF, 0x28])
-def test_search_first_c2_subset(ctx, O, dead):
-    n = 100000 if FULL else 6000
-    targets = workloads.to_lists(workloads.c2_subset(n, seed=0))
-    rules, st, exp, checked = _search_both(ctx, O, targets, dead)
-    assert rule_keys(rules) == rule_keys(exp)
-    assert st.checked_ref == checked
-    assert st.targets == n
+@pytest.mark.parametrize("pas", [0, 1], ids=["dead00", "deadFF"])
+def test_search_first_c2_100k(ctx, pas):
+    """The C2 parity subset at its configured size: 100,000 targets (seed 0),
+    against the oracle's rules and 'checked' counter for dead flags 0x00 and
+    0xFF (tests/golden/c2_100k_oracle.json, make_parity_fixtures.py)."""
+    fx = golden("c2_100k_oracle.json")
+    arr = workloads.c2_subset(100000, seed=0)
+    assert digest(arr) == fx["targets_sha256"]
+    p = fx["passes"][pas]
+    rules, st = ctx.search(workloads.to_lists(arr), dead_flags=p["dead_flags"])
+    assert rule_keys(rules) == fixture_keys(p["rules"])
+    assert st.checked_ref == p["checked"]
+    assert st.targets == 100000
 
 
-def test_search_first_c1(ctx, O):
-    t = workloads.c1_targets()
-    if not FULL:
-        t = t[np.sort(np.random.default_rng(0).choice(len(t), 8000, replace=False))]
-    targets = workloads.to_lists(t)
-    rules, st, exp, checked = _search_both(ctx, O, targets, 0)
+def test_search_first_c1_all(ctx):
+    """Every C1 target (53,951) against the oracle's rules and counter
+    (tests/golden/c1_full_oracle.json)."""
+    fx = golden("c1_full_oracle.json")
+    arr = workloads.c1_targets()
+    assert digest(arr) == fx["targets_sha256"] and len(arr) == fx["n_targets"]
+    p = fx["passes"][0]
+    rules, st = ctx.search(workloads.to_lists(arr), dead_flags=p["dead_flags"])
+    assert rule_keys(rules) == fixture_keys(p["rules"])
+    assert st.checked_ref == p["checked"]
+
+
+def test_search_first_c2_subset_dead28(ctx, O):
+    """A third dead-flag mask (the undocumented bits 3 and 5) on 6,000 C2
+    targets, the oracle run live."""
+    targets = workloads.to_lists(workloads.c2_subset(6000, seed=0))
+    rules, st, exp, checked = _search_both(ctx, O, targets, 0x28)
     assert rule_keys(rules) == rule_keys(exp)
     assert st.checked_ref == checked
 
@@ -313,10 +344,34 @@ def test_tuning_options_keep_parity(ctx, O, lane_states, chunk):
     assert st.checked_ref == checked
 
 
-def test_autotune_picks_a_valid_setting(ctx):
+def test_autotune_picks_a_valid_setting(ctx, O):
     targets = workloads.to_lists(workloads.c2_subset(2000, seed=13))
     job, keep = ctx.make_job(targets)
-    r = ctx.autotune(job)
-    assert r.lane_states in (1, 2, 4, 8) and r.chunk_blocks in (8, 32, 128, 512)
-    assert ctx.get_option(z80b.OPT_EXH_LANE_STATES) == r.lane_states
-    assert all(r.ms[a][b] > 0 for a in range(4) for b in range(4))
+    opts = [z80b.OPT_EXH_LANE_STATES, z80b.OPT_EXH_CHUNK_BLOCKS, z80b.OPT_XINDEP_BITS, z80b.OPT_COMPACT_SWEEP]
+    saved = [ctx.get_option(o) for o in opts]
+    try:
+        r = ctx.autotune(job)
+        assert r.lane_states in (1, 2, 4, 8) and r.chunk_blocks in (8, 32, 128, 512)
+        assert [ctx.get_option(o) for o in opts] == [r.lane_states, r.chunk_blocks, r.xindep_bits, r.compact]
+        trials = r.trial_list()
+        assert len(trials) == 40 and all(t["ms"] > 0 for t in trials)
+        # every cell is a distinct kernel configuration, and names what it ran
+        cells = {(t["xindep_bits"], t["lane_states"], t["chunk_blocks"], t["compact"]) for t in trials}
+        assert len(cells) == 40
+        scalar = ("k_exhaustive<1,1>", "k_exhaustive<2,1>", "k_exhaustive<4,1>", "k_exhaustive<8,1>")
+        for t in trials:
+            if t["xindep_bits"]:
+                assert not any(k in t["kernels"] for k in scalar), t
+            else:
+                assert "k_exhaustive<1,2>" not in t["kernels"], t
+                assert all(k not in t["kernels"] for k in scalar if k != f"k_exhaustive<{t['lane_states']},1>"), t
+            if t["compact"] == 0:
+                assert "k_exhaustive<1,3>" not in t["kernels"], t
+        assert any("k_exhaustive<1,3>" in t["kernels"] for t in trials if t["compact"])
+        # the chosen setting keeps parity
+        rules, st = ctx.search(targets, dead_flags=0xFF)
+        exp, checked = O.search(targets, 1, dead=0xFF)
+        assert rule_keys(rules) == rule_keys(exp) and st.checked_ref == checked
+    finally:
+        for o, v in zip(opts, saved):
+            ctx.set_option(o, v)
