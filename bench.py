@@ -245,6 +245,21 @@ def mulopt_leg(ctx, z80b, workloads, args, with_cpu):
     return out
 
 
+def tune_record(tr, sample):
+    """The autotuner's choice and its trial grid, each trial with the sweep
+    kernels it launched."""
+    trials = tr.trial_list()
+    best = min(trials, key=lambda t: t["ms"])
+    return {"chosen": {"xindep_bits": tr.xindep_bits, "lane_states": tr.lane_states,
+                       "chunk_blocks": tr.chunk_blocks, "compact": tr.compact, "kernels": best["kernels"]},
+            "grid": "A-independent kernel (bit-sliced; scalar at 1, 2, 4, 8 states per lane) x units per chunk "
+                    "(8, 32, 128, 512) x compact kernel (off, on)",
+            "sample": sample,
+            "trials": [[t["xindep_bits"], t["lane_states"], t["chunk_blocks"], t["compact"], round(t["ms"], 3),
+                        t["kernels"]] for t in trials],
+            "trial_fields": ["xindep_bits", "lane_states", "chunk_blocks", "compact", "device_ms", "kernels"]}
+
+
 def c3_leg(ctx, z80b, workloads, args):
     """Batched uneven workload: seeded C3 targets (60% length 2, 40% length
     3, per-target dead-register and dead-flag masks), candidates up to 2
@@ -274,7 +289,8 @@ def c3_leg(ctx, z80b, workloads, args):
     # tune the sweep kernel for this workload on its first 4,000 targets
     # (longer sequences than C2's, so another setting may win); the C2
     # setting is restored after the leg
-    k0, c0 = ctx.get_option(z80b.OPT_EXH_LANE_STATES), ctx.get_option(z80b.OPT_EXH_CHUNK_BLOCKS)
+    tuned = [z80b.OPT_EXH_LANE_STATES, z80b.OPT_EXH_CHUNK_BLOCKS, z80b.OPT_XINDEP_BITS, z80b.OPT_COMPACT_SWEEP]
+    saved = [ctx.get_option(o) for o in tuned]
     tj, tkeep = job_for(0, min(4000, n), z80b.PATH_BATCHED)
     tr = ctx.autotune(tj)
     job, keep = job_for(0, n, z80b.PATH_BATCHED)
@@ -292,8 +308,7 @@ def c3_leg(ctx, z80b, workloads, args):
            "qc_survivors": st.qc_survivors, "exhaustive_pairs": st.exhaustive_pairs,
            "exhaustive_states": st.exhaustive_states, "rounds": st.rounds, "launches": st.launches,
            "exhaustive_ms": st.exh_ms, "checks": st.checks,
-           "autotune": {"lane_states": tr.lane_states, "chunk_blocks": tr.chunk_blocks,
-                        "sample": "first 4,000 targets of the leg"}}
+           "autotune": tune_record(tr, "first 4,000 targets of the leg")}
     if args.plain_sample:
         m = min(1000, n)
         pj, keep2 = job_for(0, m, z80b.PATH_PLAIN)
@@ -307,8 +322,8 @@ def c3_leg(ctx, z80b, workloads, args):
         out["plain_vs_batched"] = {"targets": m, "plain_checks_per_s": stp.checks / tp,
                                    "batched_checks_per_s": stb.checks / tb, "batched_over_plain": tp / tb,
                                    "timing": "host wall clock around z80b_search (both synchronous)"}
-    ctx.set_option(z80b.OPT_EXH_LANE_STATES, k0)
-    ctx.set_option(z80b.OPT_EXH_CHUNK_BLOCKS, c0)
+    for o, v in zip(tuned, saved):
+        ctx.set_option(o, v)
     return out
 
 
@@ -406,16 +421,11 @@ def main():
     flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
     progress(f"rank {rank}: {len(mine)} targets staged")
 
-    # ---- autotune (states per lane x chunk size) on a 200k-target sample
+    # ---- autotune (sweep kernel configuration) on a 200k-target sample
     tune_arr = np.ascontiguousarray(workloads.c2_subset(200000, seed=11))
     tr = ctx.autotune(make_job(z80b, tune_arr, dead))
-    tuning = {"lane_states": tr.lane_states, "chunk_blocks": tr.chunk_blocks,
-              "trial_ms": [[round(tr.ms[a][b], 2) for b in range(4)] for a in range(4)],
-              "grid": "lane states 1,2,4,8 x chunk blocks 8,32,128,512 on 200k targets",
-              "a_independent_sweeps": ("bit-sliced" if ctx.get_option(z80b.OPT_XINDEP_BITS)
-                                       else "scalar (lane states apply)"),
-              "compact_sweeps": bool(ctx.get_option(z80b.OPT_COMPACT_SWEEP))}
-    progress(f"autotune: lane states {tr.lane_states}, chunk blocks {tr.chunk_blocks}")
+    tuning = tune_record(tr, "200,000 C2 targets (seed 11)")
+    progress(f"autotune: {tuning['chosen']}")
 
     # ---- value: targets resident in HBM
     job = make_job(z80b, mine, dead)

@@ -221,14 +221,30 @@ int z80b_exhaustive_noalloc(int device, const uint32_t* tgt, const uint8_t* tlen
 int z80b_set_option(z80b_ctx* ctx, int option, int value);
 int z80b_get_option(const z80b_ctx* ctx, int option, int* value);
 
+typedef struct z80b_tune_trial {
+  int xindep_bits;            /* Z80B_OPT_XINDEP_BITS of the trial */
+  int lane_states;            /* Z80B_OPT_EXH_LANE_STATES (scalar A-independent kernel); 0 when bit-sliced */
+  int chunk_blocks;           /* Z80B_OPT_EXH_CHUNK_BLOCKS: sweep units per work chunk */
+  int compact;                /* Z80B_OPT_COMPACT_SWEEP */
+  double ms;                  /* device ms of the pipeline on the sample */
+  char kernels[96];           /* the sweep kernels it launched, "k_exhaustive<K,CLS>" joined by '+' */
+} z80b_tune_trial;
+#define Z80B_TUNE_MAX_TRIALS 64
 typedef struct z80b_tune_result {
-  int lane_states;            /* chosen Z80B_OPT_EXH_LANE_STATES */
-  int chunk_blocks;           /* chosen Z80B_OPT_EXH_CHUNK_BLOCKS */
-  double ms[4][4];            /* device ms of the trial runs [lane_states 1,2,4,8][chunk 8,32,128,512] */
+  int lane_states;            /* the chosen setting, now the context's */
+  int chunk_blocks;
+  int xindep_bits;
+  int compact;
+  int n_trials;
+  z80b_tune_trial trials[Z80B_TUNE_MAX_TRIALS];
 } z80b_tune_result;
-/* Runs the job (a representative sample) for every combination of the
- * tuning options, keeps the fastest for this context and reports the
- * timings.  The rules of the trials are discarded. */
+/* Runs the job (a representative sample) once per sweep configuration --
+ * A-independent kernel (bit-sliced, or scalar with 1/2/4/8 states per lane
+ * per dispatch) x units per chunk (8, 32, 128, 512) x compact kernel off/on,
+ * 40 distinct kernel configurations -- keeps the fastest for this context
+ * and reports every trial with the kernels it launched.  The rules of the
+ * trials are discarded.  No counterpart in the reference (its launch shape
+ * is fixed, cuda/z80_search_v2.cu:900-948). */
 int z80b_autotune(z80b_ctx* ctx, const z80b_job* sample, z80b_tune_result* out);
 
 /* ---- constant-multiply search (cmd/mulopt) ---------------------------------

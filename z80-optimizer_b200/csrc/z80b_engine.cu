@@ -156,6 +156,7 @@ struct z80b_ctx {
   int qc_index = 1;           // Z80B_OPT_QC_INDEX
   int xbits = 1;              // Z80B_OPT_XINDEP_BITS
   int compact = 0;            // Z80B_OPT_COMPACT_SWEEP
+  uint32_t sweep_kernels = 0; // kSweep* bits of the sweep kernels launched since the last reset
 };
 
 namespace {
@@ -533,8 +534,8 @@ int sweep_round(z80b_ctx* ctx, const DevTargets& T, const DevPool& P, const Roun
   CK(cudaMemsetAsync(R.counter, 0, 24, s));
   trace("sweep: %u pairs, %llu + %llu + %llu chunks", np, last[0] + last[1], last[2] + last[3], last[4] + last[5]);
   int ke = kbegin(ctx, 1);
-  const int nl =
-      launch_exhaustive(T, P, R, np, last[0] + last[1], last[2] + last[3], last[4] + last[5], ctx->exh_k, s);
+  const int nl = launch_exhaustive(T, P, R, np, last[0] + last[1], last[2] + last[3], last[4] + last[5], ctx->exh_k,
+                                   s, &ctx->sweep_kernels);
   kend(ctx, ke);
   CKR(check_launch(ctx, "exhaustive"));
   if (nl > 1) ctx->launches += uint32_t(nl - 1);
@@ -1384,8 +1385,30 @@ int z80b_get_option(const z80b_ctx* ctx, int option, int* value) {
   return Z80B_EINVAL;
 }
 
-// Tries every (lane states, chunk size) pair on the sample job and keeps the
-// fastest (device time of the whole pipeline).
+// The sweep kernels of a kSweep* mask, by name ("k_exhaustive<K,CLS>" joined
+// by '+').
+static void sweep_kernel_names(uint32_t mask, char* out, size_t cap) {
+  std::string r;
+  auto add = [&](const char* n) {
+    if (!r.empty()) r += "+";
+    r += n;
+  };
+  if (mask & kSweepBits) add("k_exhaustive<1,0>");
+  if (mask & kSweepXBits) add("k_exhaustive<1,2>");
+  if (mask & kSweepCompact) add("k_exhaustive<1,3>");
+  const char* scalar[4] = {"k_exhaustive<1,1>", "k_exhaustive<2,1>", "k_exhaustive<4,1>", "k_exhaustive<8,1>"};
+  for (int i = 0; i < 4; i++)
+    if (mask & (kSweepScalarK1 << i)) add(scalar[i]);
+  std::snprintf(out, cap, "%s", r.c_str());
+}
+
+// Runs the sample job once for every sweep configuration of the grid and
+// keeps the fastest (device time of the whole pipeline): the kernel for
+// A-independent pairs (bit-sliced, or scalar with 1, 2, 4 or 8 states per
+// lane per dispatch), units per work chunk, and whether A-dependent pairs
+// that fit the compact state take the compact kernel.  Every cell of the
+// grid is a distinct kernel configuration; each trial records the sweep
+// kernels it launched.
 int z80b_autotune(z80b_ctx* ctx, const z80b_job* sample, z80b_tune_result* out) {
   if (!ctx) return Z80B_EINVAL;
   CKR(validate_job(ctx, sample));
@@ -1393,32 +1416,53 @@ int z80b_autotune(z80b_ctx* ctx, const z80b_job* sample, z80b_tune_result* out) 
   cudaSetDevice(ctx->device);
   DevTargets T;
   CKR(upload_targets(ctx, ctx->staged, sample, &T, true));
-  const int ks[4] = {1, 2, 4, 8}, cs[4] = {8, 32, 128, 512};
+  // A-independent kernel: {xbits, lane states}
+  const int xv[5][2] = {{1, 0}, {0, 1}, {0, 2}, {0, 4}, {0, 8}};
+  const int cs[4] = {8, 32, 128, 512};
+  const int k0 = ctx->exh_k;
   double best = 1e300;
-  int bk = ctx->exh_k, bc = ctx->chunk_blocks;
+  int bk = ctx->exh_k, bc = ctx->chunk_blocks, bx = ctx->xbits, bm = ctx->compact;
   z80b_tune_result r{};
-  for (int a = 0; a < 4; a++)
-    for (int b = 0; b < 4; b++) {
-      ctx->exh_k = ks[a];
-      ctx->chunk_blocks = cs[b];
-      z80b_stats st{};
-      uint64_t nr = 0;
-      CKR(run_pipeline(ctx, T, ctx->staged.opts, &st, &nr));  // warm
-      std::memset(&st, 0, sizeof st);
-      CKR(run_pipeline(ctx, T, ctx->staged.opts, &st, &nr));
-      r.ms[a][b] = st.device_ms;
-      if (st.device_ms < best) {
-        best = st.device_ms;
-        bk = ks[a];
-        bc = cs[b];
+  for (int m = 0; m < 2; m++)
+    for (int a = 0; a < 5; a++)
+      for (int b = 0; b < 4; b++) {
+        ctx->xbits = xv[a][0];
+        ctx->exh_k = xv[a][1] ? xv[a][1] : k0;
+        ctx->chunk_blocks = cs[b];
+        ctx->compact = m;
+        z80b_stats st{};
+        uint64_t nr = 0;
+        CKR(run_pipeline(ctx, T, ctx->staged.opts, &st, &nr));  // warm
+        std::memset(&st, 0, sizeof st);
+        ctx->sweep_kernels = 0;
+        CKR(run_pipeline(ctx, T, ctx->staged.opts, &st, &nr));
+        if (r.n_trials < Z80B_TUNE_MAX_TRIALS) {
+          z80b_tune_trial& t = r.trials[r.n_trials++];
+          t.xindep_bits = xv[a][0];
+          t.lane_states = xv[a][1];
+          t.chunk_blocks = cs[b];
+          t.compact = m;
+          t.ms = st.device_ms;
+          sweep_kernel_names(ctx->sweep_kernels, t.kernels, sizeof t.kernels);
+        }
+        if (st.device_ms < best) {
+          best = st.device_ms;
+          bk = ctx->exh_k;
+          bc = cs[b];
+          bx = xv[a][0];
+          bm = m;
+        }
       }
-    }
   ctx->exh_k = bk;
   ctx->chunk_blocks = bc;
+  ctx->xbits = bx;
+  ctx->compact = bm;
   r.lane_states = bk;
   r.chunk_blocks = bc;
+  r.xindep_bits = bx;
+  r.compact = bm;
   if (out) *out = r;
-  trace("autotune: lane states %d, chunk blocks %d (%.3f ms)", bk, bc, best);
+  trace("autotune: xbits %d, lane states %d, chunk %d, compact %d (%.3f ms)", bx, bk, bc, bm, best);
   return Z80B_OK;
 }
 

@@ -1714,30 +1714,35 @@ void launch_exhaustive_k(const DevTargets& T, const DevPool& P, const RoundBuf& 
 
 int launch_exhaustive(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
                       unsigned long long total_b, unsigned long long total_x, unsigned long long total_c, int k,
-                      cudaStream_t s) {
+                      cudaStream_t s, uint32_t* kernels) {
   if (!npairs) return 0;
   int n = 0;
+  uint32_t mask = 0;
   if (total_c) {
     launch_exhaustive_k<1, 3>(T, P, R, npairs, total_c, s);
+    mask |= kSweepCompact;
     n++;
   }
   if (total_b) {
     launch_exhaustive_k<1, 0>(T, P, R, npairs, total_b, s);
+    mask |= kSweepBits;
     n++;
   }
   if (total_x) {
     if (R.xunit == kXBitsBlocks) {
       launch_exhaustive_k<1, 2>(T, P, R, npairs, total_x, s);
+      mask |= kSweepXBits;
     } else {
       switch (k) {
-        case 1: launch_exhaustive_k<1, 1>(T, P, R, npairs, total_x, s); break;
-        case 2: launch_exhaustive_k<2, 1>(T, P, R, npairs, total_x, s); break;
-        case 8: launch_exhaustive_k<8, 1>(T, P, R, npairs, total_x, s); break;
-        default: launch_exhaustive_k<4, 1>(T, P, R, npairs, total_x, s); break;
+        case 1: launch_exhaustive_k<1, 1>(T, P, R, npairs, total_x, s); mask |= kSweepScalarK1; break;
+        case 2: launch_exhaustive_k<2, 1>(T, P, R, npairs, total_x, s); mask |= kSweepScalarK1 << 1; break;
+        case 8: launch_exhaustive_k<8, 1>(T, P, R, npairs, total_x, s); mask |= kSweepScalarK1 << 3; break;
+        default: launch_exhaustive_k<4, 1>(T, P, R, npairs, total_x, s); mask |= kSweepScalarK1 << 2; break;
       }
     }
     n++;
   }
+  if (kernels) *kernels |= mask;
   return n;
 }
 void launch_round_resolve(const RoundBuf& R, uint32_t npairs, const QCOut& q, const Lanes& L, uint32_t max_spec,

@@ -129,10 +129,13 @@ void launch_pairs_from_survivors(const DevTargets& T, const DevPool& P, const QC
 // k = states per lane per dispatch: 1, 2, 4 or 8.
 // Launches the sweep kernel of each class that has chunks (total_b
 // bit-sliced, total_x A-independent, total_c compact); returns the number of
-// launches.
+// launches and ORs the launched instantiations into *kernels (may be NULL):
+// kSweep* bits.
+constexpr uint32_t kSweepBits = 1u, kSweepXBits = 2u, kSweepCompact = 4u;
+constexpr uint32_t kSweepScalarK1 = 8u;  // scalar A-independent kernel, K = 1, 2, 4, 8: bits 3..6
 int launch_exhaustive(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
                       unsigned long long total_b, unsigned long long total_x, unsigned long long total_c, int k,
-                      cudaStream_t s);
+                      cudaStream_t s, uint32_t* kernels = nullptr);
 void launch_round_resolve(const RoundBuf& R, uint32_t npairs, const QCOut& q, const Lanes& L, uint32_t max_spec,
                           cudaStream_t s);
 void launch_midcheck(const DevTargets& T, const DevPool& P, const uint32_t* surv,

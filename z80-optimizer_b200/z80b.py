@@ -153,9 +153,25 @@ class ServerStats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class TuneTrial(ctypes.Structure):
+    _fields_ = [("xindep_bits", ctypes.c_int), ("lane_states", ctypes.c_int), ("chunk_blocks", ctypes.c_int),
+                ("compact", ctypes.c_int), ("ms", ctypes.c_double), ("kernels", ctypes.c_char * 96)]
+
+    def as_dict(self):
+        return {"xindep_bits": self.xindep_bits, "lane_states": self.lane_states,
+                "chunk_blocks": self.chunk_blocks, "compact": self.compact, "ms": self.ms,
+                "kernels": self.kernels.decode()}
+
+
+TUNE_MAX_TRIALS = 64
+
+
 class TuneResult(ctypes.Structure):
-    _fields_ = [("lane_states", ctypes.c_int), ("chunk_blocks", ctypes.c_int),
-                ("ms", (ctypes.c_double * 4) * 4)]
+    _fields_ = [("lane_states", ctypes.c_int), ("chunk_blocks", ctypes.c_int), ("xindep_bits", ctypes.c_int),
+                ("compact", ctypes.c_int), ("n_trials", ctypes.c_int), ("trials", TuneTrial * TUNE_MAX_TRIALS)]
+
+    def trial_list(self):
+        return [self.trials[i].as_dict() for i in range(self.n_trials)]
 
 
 def lib():
