@@ -57,6 +57,32 @@ def test_enumerate_range_length3_jsonl(tmp_path, O):
 
 
 @pytest.mark.gpu
+def test_enumerate_range_length3_equals_oracle(tmp_path, O):
+    """A sampled length-2/3 enumeration over the first-instruction range
+    [1200, 1210): the searched targets (--targets-out) run through the
+    oracle's first-found search (worker.go:124-265, candidates up to
+    MaxTargetLen - 1 = 2 instructions) give exactly the rule set the CLI
+    reports."""
+    tl, out = tmp_path / "t.jsonl", tmp_path / "r.json"
+    r = run("enumerate", "--max-target", "3", "--first-op-start", "1200", "--first-op-end", "1210",
+            "--sample", "300", "--seed", "5", "--targets-out", str(tl), "--output", str(out))
+    assert r.returncode == 0, r.stderr
+    targets = [json.loads(x) for x in open(tl)]
+    assert len(targets) == 600  # 300 per target length
+    assert {len(t) for t in targets} == {2, 3}
+    pool = z80b.pool8()
+    first = set(pool[1200:1210])
+    assert all(t[0] in first for t in targets)
+    got = sorted((x["source_asm"], x["replacement_asm"], x["bytes_saved"], x["cycles_saved"])
+                 for x in json.load(open(out)))
+    rules, _ = O.search(targets, 2)
+    want = sorted((O.disasm(list(x.src[:x.src_len])), O.disasm(list(x.rep[:x.rep_len])), x.bytes_saved,
+                   x.cycles_saved) for x in rules)
+    assert got == want
+    assert any(len(O.parse_assembly(g[0])) == 3 for g in got)
+
+
+@pytest.mark.gpu
 def test_all_hits_without_exhaustive_tier(ctx, O):
     """Z80B_JOB_NO_EXHAUSTIVE: the rules are every QuickCheck + MidCheck
     survivor, a superset of the verified rules; the extra ones fail the

@@ -1,10 +1,12 @@
 """Multi-rank host logic of bench.py on CPU with the gloo backend
 (world size 2): every target is owned by exactly one rank, and the reported
-step time is the maximum and the check count the sum over ranks."""
+step time is the maximum and the check count the sum over ranks.  On a GPU:
+two shards of an enumeration give together the rules of the whole."""
 import os
 import socket
 
 import numpy as np
+import pytest
 import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
@@ -62,3 +64,38 @@ def test_shard_bounds_partition():
             assert all(bounds[i][1] == bounds[i + 1][0] for i in range(world - 1))
             sizes = np.diff([0] + [b[1] for b in bounds])
             assert sizes.max() - sizes.min() <= 1
+
+
+@pytest.mark.gpu
+def test_range_shards_union_equals_whole(tmp_path):
+    """Sharding the enumeration by first instruction (the reference's
+    --first-op-start/--first-op-end split across processes or GPUs,
+    README.md:216-221): two ranks, run as two concurrent z80opt processes on
+    the same device, each search its shard_bounds part of [1000, 1040); the
+    union of their rule sets equals the rule set of one process over the
+    whole range."""
+    import json
+    import subprocess
+
+    exe = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "z80-optimizer_b200", "_build",
+                       "z80opt")
+    lo, hi, world = 1000, 1040, 2
+
+    def cmd(a, b, out):
+        return [exe, "enumerate", "--max-target", "2", "--first-op-start", str(a), "--first-op-end", str(b),
+                "--output", str(out)]
+
+    procs, outs = [], []
+    for rank in range(world):
+        a, b = workloads.shard_bounds(hi - lo, rank, world)
+        out = tmp_path / f"shard{rank}.json"
+        outs.append(out)
+        procs.append(subprocess.Popen(cmd(lo + a, lo + b, out), stdout=subprocess.DEVNULL, stderr=subprocess.PIPE))
+    for p in procs:
+        assert p.wait(timeout=600) == 0, p.stderr.read()
+    whole = tmp_path / "whole.json"
+    assert subprocess.run(cmd(lo, hi, whole), capture_output=True, timeout=600).returncode == 0
+    key = lambda x: (x["source_asm"], x["replacement_asm"], x["bytes_saved"], x["cycles_saved"])  # noqa: E731
+    union = sorted(key(x) for o in outs for x in json.load(open(o)))
+    assert union == sorted(key(x) for x in json.load(open(whole)))
+    assert len(union) > 100

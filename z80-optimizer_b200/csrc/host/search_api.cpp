@@ -385,6 +385,7 @@ struct RunSpec {
   bool verbose = false;
   int first0 = 0, first1 = -1;
   search::RuleSink sink;
+  search::TargetSink targets;
 };
 
 result::Table run_lengths(const RunSpec& r, search::Stats* stats) {
@@ -398,6 +399,7 @@ result::Table run_lengths(const RunSpec& r, search::Stats* stats) {
     search::EnumerateTargets(len, r.first0, r.first1, r.sample, r.seed, 1u << 22,
                              [&](const std::vector<uint32_t>& w, uint64_t m) {
                                n += m;
+                               if (r.targets) r.targets(w, len, m);
                                const std::vector<uint8_t> lens(m, uint8_t(len));
                                run_job(w, lens, uint32_t(len), r.maxCand, r.dead, r.mode, r.flags, emit, stats);
                              });
@@ -655,6 +657,7 @@ result::Table Run(const Config& cfg, Stats* stats) {
   r.first0 = cfg.FirstOpStart;
   r.first1 = cfg.FirstOpEnd;
   r.sink = cfg.Sink;
+  r.targets = cfg.Targets;
   return run_lengths(r, stats);
 }
 
@@ -880,6 +883,7 @@ result::Table SearchGPU(const SearchConfig& cfg) {
   r.first0 = cfg.FirstOpStart;
   r.first1 = cfg.FirstOpEnd;
   r.sink = cfg.Sink;
+  r.targets = cfg.Targets;
   return run_lengths(r, nullptr);
 }
 }  // namespace gpu

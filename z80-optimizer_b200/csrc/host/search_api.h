@@ -115,6 +115,10 @@ constexpr FlagMask DeadNone = 0x00, DeadUndoc = 0x28, DeadAll = 0xFF;
 // SearchGPU then return an empty table): the form for enumerations whose
 // rule sets do not fit in memory.
 using RuleSink = std::function<void(const result::Rule&)>;
+// Receives every batch of targets before it is searched: `n` sequences of
+// `len` packed words each (extension; records exactly which targets a
+// sampled or sharded enumeration searched).
+using TargetSink = std::function<void(const std::vector<uint32_t>& words, int len, uint64_t n)>;
 
 struct Config {
   int MaxTargetLen = 2;  // targets of length 2..MaxTargetLen
@@ -132,6 +136,7 @@ struct Config {
   // an enumeration over processes or GPUs.
   int FirstOpStart = 0, FirstOpEnd = -1;
   RuleSink Sink;  // extension, see RuleSink
+  TargetSink Targets;  // extension, see TargetSink
 };
 
 struct Stats {  // accumulated over Run's jobs
@@ -180,6 +185,7 @@ struct SearchConfig {
   // is reported, without the ExhaustiveCheck tier.
   bool NoExhaust = false;
   search::RuleSink Sink;  // extension, as in search::Config
+  search::TargetSink Targets;  // extension, as in search::Config
 };
 result::Table SearchGPU(const SearchConfig& cfg);
 }  // namespace gpu

@@ -4,6 +4,7 @@
 //   z80opt enumerate [--max-target N] [--output FILE] [--dead-flags M] [--gpu]
 //                    [--workers N] [-v] [--sample N] [--seed S]
 //                    [--first-op-start M] [--first-op-end N] [--jsonl FILE] [--no-exhaust]
+//                    [--targets-out FILE]
 //   z80opt target "ASM : ASM ..." [--max-candidate N] [--dead-flags M] [-v]
 //   z80opt verify-jsonl FILE [--dead-flags M] [-v]
 //   z80opt mulopt [--pool mulopt|wide21|fast14|cuda21] [--max-len N] [--min-len N]
@@ -124,6 +125,21 @@ int cmd_enumerate(const Args& a) {
       streamed++;
     };
   }
+  // --targets-out FILE: every searched target as a JSON array of packed words
+  std::FILE* tf = nullptr;
+  search::TargetSink tsink;
+  const std::string tpath = a.get("targets-out", "");
+  if (!tpath.empty()) {
+    tf = std::fopen(tpath.c_str(), "w");
+    if (!tf) throw Error(Z80B_EINVAL, "cannot create " + tpath);
+    tsink = [&](const std::vector<uint32_t>& w, int len, uint64_t n) {
+      for (uint64_t i = 0; i < n; i++) {
+        std::fputc('[', tf);
+        for (int k = 0; k < len; k++) std::fprintf(tf, k ? ",%u" : "%u", w[size_t(i) * size_t(len) + size_t(k)]);
+        std::fputs("]\n", tf);
+      }
+    };
+  }
   std::printf("Z80 Superoptimizer\n");
   std::printf("  Max target length: %d\n", maxTarget);
   std::printf("  Target instructions: 4531 per position (8-bit only)\n");
@@ -142,6 +158,7 @@ int cmd_enumerate(const Args& a) {
     c.FirstOpEnd = first1;
     c.NoExhaust = noExhaust;
     c.Sink = sink;
+    c.Targets = tsink;
     rules = gpu::SearchGPU(c).Rules();
   } else {
     search::Config c;
@@ -154,8 +171,10 @@ int cmd_enumerate(const Args& a) {
     c.FirstOpStart = first0;
     c.FirstOpEnd = first1;
     c.Sink = sink;
+    c.Targets = tsink;
     rules = search::Run(c).Rules();
   }
+  if (tf) std::fclose(tf);
   if (jl) {
     std::fclose(jl);
     std::printf("\nFound %llu optimizations (streamed to %s)\n", (unsigned long long)streamed, jpath.c_str());
@@ -469,6 +488,7 @@ void usage() {
                "usage: z80opt enumerate|target|verify-jsonl|mulopt|export [flags]\n"
                "  enumerate    --max-target N --output FILE --dead-flags none|undoc|all|0xNN --gpu -v\n"
                "               --sample N --seed S --first-op-start M --first-op-end N --jsonl FILE --no-exhaust\n"
+               "               --targets-out FILE\n"
                "  target       \"ASM : ASM\" --max-candidate N\n"
                "  verify-jsonl FILE --dead-flags M -v\n"
                "  mulopt       --pool mulopt|wide21|fast14|cuda21 --max-len N --k K --json --resume FILE\n"
