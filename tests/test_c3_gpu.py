@@ -123,3 +123,26 @@ def test_compact_sweep_keeps_parity(ctx, O):
                      r.cycles_saved, r.dead_flags)
     assert [key(r) for r in r2] == [key(r) for r in exp]
     assert st2.checked_ref == checked
+
+
+@pytest.mark.parametrize("case", ["c3", "c2"])
+def test_device_rounds_equal_host_rounds(ctx, case):
+    """The first-found rounds driven on the device (one CUDA graph, a WHILE
+    node over build / scan / sweep / resolve) and driven from the host give
+    the same rules, counters, rounds and swept pairs."""
+    import workloads
+    saved = ctx.get_option(z80b.OPT_GRAPH_ROUNDS)
+    try:
+        res = []
+        for g in (1, 0):
+            ctx.set_option(z80b.OPT_GRAPH_ROUNDS, g)
+            if case == "c3":
+                rules, st = run(ctx, fixture())
+            else:
+                rules, st = ctx.search(workloads.to_lists(workloads.c2_subset(6000, seed=4)), dead_flags=0xFF)
+            res.append((dev_keys(rules), st.checked_ref, st.checks, st.rounds, st.exhaustive_pairs,
+                        st.exhaustive_states))
+        assert res[0] == res[1]
+        assert res[0][3] > 1  # several rounds
+    finally:
+        ctx.set_option(z80b.OPT_GRAPH_ROUNDS, saved)

@@ -123,6 +123,25 @@ struct Staged {
 
 }  // namespace
 
+// An instantiated round loop (see rounds_on_device) and the launch
+// arguments it was captured with; a run with other arguments captures anew.
+struct RoundGraph {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::vector<unsigned char> key;
+  RoundGraph() = default;
+  RoundGraph(const RoundGraph&) = delete;
+  RoundGraph& operator=(const RoundGraph&) = delete;
+  ~RoundGraph() { reset(); }
+  void reset() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+    key.clear();
+  }
+};
+
 struct z80b_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -157,6 +176,9 @@ struct z80b_ctx {
   int xbits = 1;              // Z80B_OPT_XINDEP_BITS
   int compact = 0;            // Z80B_OPT_COMPACT_SWEEP
   uint32_t sweep_kernels = 0; // kSweep* bits of the sweep kernels launched since the last reset
+  int graph_rounds = 1;       // Z80B_OPT_GRAPH_ROUNDS
+  DBuf roundctl;              // RoundCtl of the device-driven rounds
+  RoundGraph rg1, rg2;        // instantiated round loops: length-1 and length-2 candidate passes
 };
 
 namespace {
@@ -542,6 +564,99 @@ int sweep_round(z80b_ctx* ctx, const DevTargets& T, const DevPool& P, const Roun
   return Z80B_OK;
 }
 
+template <class V>
+void key_put(std::vector<unsigned char>& k, const V& v) {
+  const unsigned char* b = reinterpret_cast<const unsigned char*>(&v);
+  k.insert(k.end(), b, b + sizeof v);
+}
+
+// The rounds of one first-found pass driven by the device: one CUDA graph
+// whose WHILE node repeats the round body -- clear the pair counter (and the
+// rescan counter), build the round's pairs, scan their chunk counts and set
+// the loop condition (k_round_scan), [rescan the length-2 buckets of lanes
+// whose slots ran out, only after an empty round], the sweep kernels of
+// every class on persistent grids, resolve -- until a round is empty with no
+// rescan pending.  The same work and order as the host loop of
+// run_pipeline, without a host round trip per round.  The graph is
+// captured once per set of launch arguments and replayed.
+int rounds_on_device(z80b_ctx* ctx, RoundGraph& g, const DevTargets& T, const DevPool& P, const QCOut& q,
+                     const Lanes& L, const RoundBuf& R, uint32_t max_spec, const PairScan* ps, const QCOut* qres,
+                     uint32_t* rounds, uint64_t* pairs) {
+  cudaStream_t s = ctx->stream;
+  CK(ctx->roundctl.ensure(sizeof(RoundCtl)));
+  RoundCtl* ctl = ctx->roundctl.as<RoundCtl>();
+  std::vector<unsigned char> key;
+  key_put(key, T);
+  key_put(key, P);
+  key_put(key, q);
+  key_put(key, L);
+  key_put(key, R);
+  key_put(key, max_spec);
+  key_put(key, ctx->exh_k);
+  key_put(key, ctl);
+  if (ps) {
+    key_put(key, *ps);
+    key_put(key, *qres);
+  }
+  if (!g.exec || g.key != key) {
+    g.reset();
+    warm_exhaustive_dev(R, ctx->exh_k);
+    CK(cudaGraphCreate(&g.graph, 0));
+    cudaGraphConditionalHandle loop;
+    CK(cudaGraphConditionalHandleCreate(&loop, g.graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = loop;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g.graph, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    CK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    cudaMemsetAsync(R.npairs, 0, 4, s);
+    if (ps) {
+      cudaMemsetAsync(ps->refill, 0, 4, s);
+      launch_pair_round_build(T, P, q, L, *ps, R, s);
+      launch_round_scan(R, ctl, ps->refill, loop, s);
+      launch_pair_scan_gated(T, P, q, L, *ps, ctl, s);
+    } else {
+      launch_round_build(T, P, q, L, R, s);
+      launch_round_scan(R, ctl, nullptr, loop, s);
+    }
+    launch_exhaustive_dev(T, P, R, ctl, ctx->exh_k, s);
+    launch_round_resolve_dev(R, ctl, ps ? *qres : q, L, max_spec, s);
+    cudaGraph_t captured = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(s, &captured);
+    if (ce != cudaSuccess) {
+      g.reset();
+      cudaGetLastError();
+      CK(ce);
+    }
+    CK(cudaGraphInstantiate(&g.exec, g.graph, 0));
+    g.key = key;
+    trace("round loop captured (%s pass)", ps ? "length-2" : "length-1");
+  }
+  const int per_iter = (ps ? 3 : 2) + 1 + (R.compact ? 3 : 2);  // build, scan, [rescan], sweeps, resolve
+  CK(cudaMemsetAsync(ctl, 0, sizeof(RoundCtl), s));
+  int ke = kbegin(ctx, 1);
+  CK(cudaGraphLaunch(g.exec, s));
+  kend(ctx, ke);
+  CKR(check_launch(ctx, "round loop"));
+  RoundCtl h{};
+  CK(cudaMemcpyAsync(&h, ctl, sizeof h, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (h.overrun) return fail(ctx, Z80B_ETIMEOUT, "device round loop did not end within %u iterations", kMaxRoundIters);
+  *rounds += h.rounds;
+  *pairs += h.pairs;
+  ctx->launches += h.iters * uint32_t(per_iter);
+  uint32_t mask = (R.compact ? kSweepCompact : 0u) | kSweepBits;
+  if (R.xunit == kXBitsBlocks) mask |= kSweepXBits;
+  else mask |= kSweepScalarK1 << (ctx->exh_k == 1 ? 0 : ctx->exh_k == 2 ? 1 : ctx->exh_k == 8 ? 3 : 2);
+  ctx->sweep_kernels |= mask;
+  trace("device rounds: %u rounds, %u iterations, %llu pairs", h.rounds, h.iters, (unsigned long long)h.pairs);
+  return Z80B_OK;
+}
+
 // Runs the pipeline on device-resident targets.  Rules stay in ctx->rules
 // (DevRule), count in *nr.
 int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_stats* st, uint64_t* nr) {
@@ -669,7 +784,12 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
     R.compact = mode == Z80B_MODE_FIRST && ctx->compact ? 1u : 0u;
     R.nchunks_c = R.compact ? ctx->nchunks_c.as<unsigned long long>() : nullptr;
     R.cbase_c = R.compact ? ctx->cbase_c.as<unsigned long long>() : nullptr;
-    if (nsurv) {
+    // rounds on the device (one graph) unless the caller takes answers
+    // round by round (streaming callbacks)
+    const bool dev_rounds = ctx->graph_rounds && !opts.rep;
+    if (nsurv && dev_rounds) {
+      CKR(rounds_on_device(ctx, ctx->rg1, T, P, q, L, R, kMaxSpec1, nullptr, nullptr, &rounds, &exh_pairs));
+    } else if (nsurv) {
       for (;;) {
         CK(cudaMemsetAsync(R.npairs, 0, 4, s));
         launch_round_build(T, P, q, L, R, s);
@@ -727,7 +847,9 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
       launch_pair_scan(T, P2, q, L2, ps, s);
       kend(ctx, kq2);
       CKR(check_launch(ctx, "pair_scan"));
-      for (;;) {
+      if (dev_rounds)
+        CKR(rounds_on_device(ctx, ctx->rg2, T, P2, q, L2, R, kMaxSpec2, &ps, &q2, &rounds, &exh_pairs));
+      for (; !dev_rounds;) {
         CK(cudaMemsetAsync(R.npairs, 0, 4, s));
         CK(cudaMemsetAsync(ps.refill, 0, 4, s));
         launch_pair_round_build(T, P2, q, L2, ps, R, s);
@@ -1368,6 +1490,10 @@ int z80b_set_option(z80b_ctx* ctx, int option, int value) {
       if (value != 0 && value != 1) return fail(ctx, Z80B_EINVAL, "compact sweep option must be 0 or 1");
       ctx->compact = value;
       return Z80B_OK;
+    case Z80B_OPT_GRAPH_ROUNDS:
+      if (value != 0 && value != 1) return fail(ctx, Z80B_EINVAL, "graph rounds option must be 0 or 1");
+      ctx->graph_rounds = value;
+      return Z80B_OK;
   }
   return fail(ctx, Z80B_EINVAL, "unknown option %d", option);
 }
@@ -1381,6 +1507,7 @@ int z80b_get_option(const z80b_ctx* ctx, int option, int* value) {
     case Z80B_OPT_QC_INDEX: *value = ctx->qc_index; return Z80B_OK;
     case Z80B_OPT_XINDEP_BITS: *value = ctx->xbits; return Z80B_OK;
     case Z80B_OPT_COMPACT_SWEEP: *value = ctx->compact; return Z80B_OK;
+    case Z80B_OPT_GRAPH_ROUNDS: *value = ctx->graph_rounds; return Z80B_OK;
   }
   return Z80B_EINVAL;
 }

@@ -944,10 +944,19 @@ __device__ __noinline__ bool xindep_unit(unsigned long long first, unsigned long
 // ones whose registers fit the compact state (two blocks per SM); each class
 // draws chunks from its own numbering and dispenser.  Kept apart so that
 // neither path's registers weigh on the other.
+// dev_total / dev_np (device-driven rounds): the class's chunk total and the
+// round's pair count are read from the device instead of total / npairs.
+// chunks_per_warp: chunks a warp takes before its block retires.
 template <int K, int CLS>
 __global__ void __launch_bounds__(kBlock, CLS == 3 ? 2 : 1)
-    k_exhaustive(DevTargets T, DevPool P, RoundBuf R, uint32_t npairs, unsigned long long total) {
+    k_exhaustive(DevTargets T, DevPool P, RoundBuf R, uint32_t npairs, unsigned long long total,
+                 const unsigned long long* __restrict__ dev_total, const uint32_t* __restrict__ dev_np,
+                 int chunks_per_warp) {
   static_assert(K == 1 || K == 2 || K == 4 || K == 8, "K divides 8");
+  if (dev_total) {
+    total = *dev_total;
+    npairs = *dev_np;
+  }
   constexpr bool XI = CLS != 0;
   const unsigned long long* __restrict__ cbase = CLS == 3 ? R.cbase_c : (XI ? R.cbase_x : R.cbase);
   const unsigned lane = lane_id();
@@ -955,7 +964,7 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 2 : 1)
   // At most kChunksPerWarp chunks per warp, then the block retires: the grid
   // covers all chunks, and blocks of kernels on other streams (with a higher
   // priority) get SMs as soon as blocks of a long sweep retire.
-  for (int taken = 0; taken < kChunksPerWarp; taken++) {
+  for (int taken = 0; taken < chunks_per_warp; taken++) {
     unsigned long long k = 0;
     if (lane == 0) k = atomicAdd(R.counter + (CLS == 3 ? 2 : (XI ? 1 : 0)), 1ull);
     k = __shfl_sync(kFull, k, 0);
@@ -1092,8 +1101,10 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 2 : 1)
 // Window heads settle their lane: the first pair of the window that passed
 // wins; if none did, the lane moves past the window and the next window
 // doubles (up to 2^max_spec).
-__global__ void k_round_resolve(RoundBuf R, uint32_t npairs, QCOut q, Lanes L, uint32_t max_spec) {
+__global__ void k_round_resolve(RoundBuf R, uint32_t npairs, QCOut q, Lanes L, uint32_t max_spec,
+                                const uint32_t* __restrict__ dev_np) {
   const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (dev_np) npairs = *dev_np;
   if (p >= npairs) return;
   const uint32_t w = R.wlen[p];
   if (w == 0) return;
@@ -1404,7 +1415,9 @@ __global__ void __launch_bounds__(kBlock) k_qc_bucket(DevTargets T, DevPool P, Q
 
 // Warp per target: (re)fills the slots of each lane whose slots are used up
 // and whose bucket has pairs left.
-__global__ void __launch_bounds__(kBlock) k_pair_scan(DevTargets T, DevPool P, QCOut q1, Lanes L2, PairScan ps) {
+__global__ void __launch_bounds__(kBlock) k_pair_scan(DevTargets T, DevPool P, QCOut q1, Lanes L2, PairScan ps,
+                                                      const RoundCtl* __restrict__ gate) {
+  if (gate && gate->np != 0) return;  // device-driven rounds: rescan only after an empty round
   const unsigned lane = lane_id();
   const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const uint32_t nw = gridDim.x * (blockDim.x >> 5);
@@ -1693,14 +1706,21 @@ void launch_pairs_from_survivors(const DevTargets& T, const DevPool& P, const QC
   if (!nsurv) return;
   k_pairs_from_survivors<<<grid_for(nsurv, 256), 256, 0, s>>>(T, P, q, midpass, nsurv, surv_target, R);
 }
+// Resident blocks per SM of a sweep kernel on the current device (its
+// shared-memory limit raised first), cached per device.
+template <int K, int CLS>
+int exhaustive_blocks_per_sm() {
+  constexpr int smem = CLS == 1 ? 0 : kBlock * (CLS == 3 ? kCompactWords : kBitsWords) * 4;
+  static std::atomic<int> occ[kMaxCachedDevices];
+  return blocks_per_sm(occ, k_exhaustive<K, CLS>, kBlock, smem, smem);
+}
 template <int K, int CLS>
 void launch_exhaustive_k(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
                          unsigned long long total, cudaStream_t s) {
   // shared memory (bit-sliced kernels): the candidate's output planes,
   // kBitsWords words per lane
   constexpr int smem = CLS == 1 ? 0 : kBlock * (CLS == 3 ? kCompactWords : kBitsWords) * 4;
-  static std::atomic<int> occ[kMaxCachedDevices];
-  const int per_sm = blocks_per_sm(occ, k_exhaustive<K, CLS>, kBlock, smem, smem);
+  const int per_sm = exhaustive_blocks_per_sm<K, CLS>();
   // resident blocks, or more when the chunks exceed kChunksPerWarp per warp
   const unsigned long long wpb = kBlock / 32;
   unsigned long long need = (total + wpb - 1) / wpb;
@@ -1709,7 +1729,19 @@ void launch_exhaustive_k(const DevTargets& T, const DevPool& P, const RoundBuf& 
   const unsigned long long cover = (total + wpb * kChunksPerWarp - 1) / (wpb * kChunksPerWarp);
   if (grid < cover) grid = cover;
   if (grid > 0x7FFFFFFFull) grid = 0x7FFFFFFFull;
-  k_exhaustive<K, CLS><<<unsigned(grid), kBlock, smem, s>>>(T, P, R, npairs, total);
+  k_exhaustive<K, CLS><<<unsigned(grid), kBlock, smem, s>>>(T, P, R, npairs, total, nullptr, nullptr,
+                                                               kChunksPerWarp);
+}
+
+// The same kernel on a persistent grid (resident blocks on every SM) whose
+// blocks take chunks until the class's device-side total is spent.
+template <int K, int CLS>
+void launch_exhaustive_dev_k(const DevTargets& T, const DevPool& P, const RoundBuf& R, const unsigned long long* total,
+                             const uint32_t* np, cudaStream_t s) {
+  constexpr int smem = CLS == 1 ? 0 : kBlock * (CLS == 3 ? kCompactWords : kBitsWords) * 4;
+  const int per_sm = exhaustive_blocks_per_sm<K, CLS>();
+  const unsigned grid = unsigned(dev_num_sms() * per_sm);
+  k_exhaustive<K, CLS><<<grid, kBlock, smem, s>>>(T, P, R, 0u, 0ull, total, np, 0x7FFFFFFF);
 }
 
 int launch_exhaustive(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
@@ -1748,8 +1780,118 @@ int launch_exhaustive(const DevTargets& T, const DevPool& P, const RoundBuf& R, 
 void launch_round_resolve(const RoundBuf& R, uint32_t npairs, const QCOut& q, const Lanes& L, uint32_t max_spec,
                           cudaStream_t s) {
   if (!npairs) return;
-  k_round_resolve<<<grid_for(npairs, 256), 256, 0, s>>>(R, npairs, q, L, max_spec);
+  k_round_resolve<<<grid_for(npairs, 256), 256, 0, s>>>(R, npairs, q, L, max_spec, nullptr);
 }
+
+// One block: the round's pair count, the exclusive prefix of each class's
+// chunk counts over the round's pairs (each thread sums a contiguous run,
+// the block scans the 1,024 run sums, each thread writes its run), the
+// classes' totals, cleared dispensers, and the loop condition.
+constexpr int kScanThreads = 1024;
+__global__ void __launch_bounds__(kScanThreads) k_round_scan(RoundBuf R, RoundCtl* __restrict__ ctl,
+                                                             const uint32_t* __restrict__ refill,
+                                                             cudaGraphConditionalHandle loop) {
+  __shared__ unsigned long long part[kScanThreads];
+  const uint32_t tid = threadIdx.x;
+  const uint32_t np = min(*R.npairs, R.cap);
+  const bool over = ctl->iters + 1 >= kMaxRoundIters;
+  __syncthreads();  // every thread has read ctl before thread 0 updates it
+  if (tid == 0) {
+    ctl->iters += 1;
+    if (over) {
+      // the loop has run far past any legitimate number of rounds: end it,
+      // sweep nothing more, and let the host report the error
+      ctl->overrun = 1;
+      cudaGraphSetConditional(loop, 0);
+    }
+    ctl->np = over ? 0u : np;
+    if (np && !over) {
+      ctl->rounds += 1;
+      ctl->pairs += np;
+    }
+    R.counter[0] = R.counter[1] = R.counter[2] = 0;
+    if (np == 0 || over) {
+      ctl->totals[0] = ctl->totals[1] = ctl->totals[2] = 0;
+      if (!refill || *refill == 0) cudaGraphSetConditional(loop, 0);
+    }
+  }
+  if (np == 0 || over) return;
+  const uint32_t per = (np + kScanThreads - 1) / kScanThreads;
+  const uint32_t lo = min(tid * per, np), hi = min(lo + per, np);
+  for (int c = 0; c < 3; c++) {
+    const unsigned long long* in = c == 0 ? R.nchunks : (c == 1 ? R.nchunks_x : R.nchunks_c);
+    unsigned long long* out = c == 0 ? R.cbase : (c == 1 ? R.cbase_x : R.cbase_c);
+    if (c == 2 && !R.compact) {
+      if (tid == 0) ctl->totals[2] = 0;
+      break;
+    }
+    unsigned long long sum = 0;
+    for (uint32_t i = lo; i < hi; i++) sum += in[i];
+    part[tid] = sum;
+    __syncthreads();
+    // inclusive Hillis-Steele scan of the run sums
+    for (uint32_t d = 1; d < kScanThreads; d <<= 1) {
+      const unsigned long long v = tid >= d ? part[tid - d] : 0ull;
+      __syncthreads();
+      part[tid] += v;
+      __syncthreads();
+    }
+    unsigned long long run = part[tid] - sum;
+    for (uint32_t i = lo; i < hi; i++) {
+      out[i] = run;
+      run += in[i];
+    }
+    if (tid == kScanThreads - 1) ctl->totals[c] = part[tid];
+    __syncthreads();
+  }
+}
+
+void launch_round_scan(const RoundBuf& R, RoundCtl* ctl, const uint32_t* refill, cudaGraphConditionalHandle loop,
+                       cudaStream_t s) {
+  k_round_scan<<<1, kScanThreads, 0, s>>>(R, ctl, refill, loop);
+}
+
+template <int K, int CLS>
+void warm_exhaustive_k() {
+  (void)exhaustive_blocks_per_sm<K, CLS>();
+}
+void warm_exhaustive_dev(const RoundBuf& R, int k) {
+  (void)dev_num_sms();
+  if (R.compact) warm_exhaustive_k<1, 3>();
+  warm_exhaustive_k<1, 0>();
+  if (R.xunit == kXBitsBlocks) warm_exhaustive_k<1, 2>();
+  else if (k == 1) warm_exhaustive_k<1, 1>();
+  else if (k == 2) warm_exhaustive_k<2, 1>();
+  else if (k == 8) warm_exhaustive_k<8, 1>();
+  else warm_exhaustive_k<4, 1>();
+}
+
+int launch_exhaustive_dev(const DevTargets& T, const DevPool& P, const RoundBuf& R, const RoundCtl* ctl, int k,
+                          cudaStream_t s) {
+  int n = 0;
+  if (R.compact) {
+    launch_exhaustive_dev_k<1, 3>(T, P, R, &ctl->totals[2], &ctl->np, s);
+    n++;
+  }
+  launch_exhaustive_dev_k<1, 0>(T, P, R, &ctl->totals[0], &ctl->np, s);
+  if (R.xunit == kXBitsBlocks) {
+    launch_exhaustive_dev_k<1, 2>(T, P, R, &ctl->totals[1], &ctl->np, s);
+  } else {
+    switch (k) {
+      case 1: launch_exhaustive_dev_k<1, 1>(T, P, R, &ctl->totals[1], &ctl->np, s); break;
+      case 2: launch_exhaustive_dev_k<2, 1>(T, P, R, &ctl->totals[1], &ctl->np, s); break;
+      case 8: launch_exhaustive_dev_k<8, 1>(T, P, R, &ctl->totals[1], &ctl->np, s); break;
+      default: launch_exhaustive_dev_k<4, 1>(T, P, R, &ctl->totals[1], &ctl->np, s); break;
+    }
+  }
+  return n + 2;
+}
+
+void launch_round_resolve_dev(const RoundBuf& R, const RoundCtl* ctl, const QCOut& q, const Lanes& L,
+                              uint32_t max_spec, cudaStream_t s) {
+  k_round_resolve<<<grid_for(R.cap, 256), 256, 0, s>>>(R, R.cap, q, L, max_spec, &ctl->np);
+}
+
 void launch_midcheck(const DevTargets& T, const DevPool& P, const uint32_t* surv,
                      const uint32_t* surv_target, uint32_t nsurv, uint8_t* pass, cudaStream_t s) {
   if (!nsurv) return;
@@ -1807,7 +1949,13 @@ void launch_pair_scan(const DevTargets& T, const DevPool& P, const QCOut& q1, co
                       cudaStream_t s) {
   if (!T.n) return;
   unsigned grid = std::min<unsigned>(grid_for(T.n, kBlock / 32), unsigned(dev_num_sms() * 8));
-  k_pair_scan<<<grid, kBlock, 0, s>>>(T, P, q1, L2, ps);
+  k_pair_scan<<<grid, kBlock, 0, s>>>(T, P, q1, L2, ps, nullptr);
+}
+void launch_pair_scan_gated(const DevTargets& T, const DevPool& P, const QCOut& q1, const Lanes& L2,
+                            const PairScan& ps, const RoundCtl* ctl, cudaStream_t s) {
+  if (!T.n) return;
+  unsigned grid = std::min<unsigned>(grid_for(T.n, kBlock / 32), unsigned(dev_num_sms() * 8));
+  k_pair_scan<<<grid, kBlock, 0, s>>>(T, P, q1, L2, ps, ctl);
 }
 void launch_pair_round_build(const DevTargets& T, const DevPool& P, const QCOut& q1, const Lanes& L2,
                              const PairScan& ps, const RoundBuf& R, cudaStream_t s) {

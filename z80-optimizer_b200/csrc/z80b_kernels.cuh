@@ -138,6 +138,39 @@ int launch_exhaustive(const DevTargets& T, const DevPool& P, const RoundBuf& R, 
                       cudaStream_t s, uint32_t* kernels = nullptr);
 void launch_round_resolve(const RoundBuf& R, uint32_t npairs, const QCOut& q, const Lanes& L, uint32_t max_spec,
                           cudaStream_t s);
+
+// ---- device-driven rounds (one CUDA graph, a WHILE node over the round body)
+// The round's pair count and chunk totals stay on the device: k_round_scan
+// takes the count the build left in R.npairs, scans the chunk counts of the
+// three classes, clears the dispensers and ends the loop (sets the graph's
+// condition to 0) when the round is empty and no lane waits for a rescan.
+struct RoundCtl {
+  unsigned long long totals[3];  // chunks of the current round: bit-sliced, A-independent, compact class
+  unsigned long long pairs;      // pairs swept, all rounds
+  uint32_t rounds;               // rounds with pairs
+  uint32_t iters;                // loop iterations (rounds, rescans, the last empty one)
+  uint32_t np;                   // pairs of the current round
+  uint32_t overrun;              // set when the loop stopped at kMaxRoundIters (an error)
+};
+// Bound on the iterations of one device-driven loop: a loop that has not
+// ended by then stops and reports an error instead of running on.
+constexpr uint32_t kMaxRoundIters = 1u << 20;
+void launch_round_scan(const RoundBuf& R, RoundCtl* ctl, const uint32_t* refill, cudaGraphConditionalHandle loop,
+                       cudaStream_t s);
+// The sweep kernels of the configured classes on a persistent grid, the
+// chunk totals and pair count read from ctl; returns the launches per round.
+int launch_exhaustive_dev(const DevTargets& T, const DevPool& P, const RoundBuf& R, const RoundCtl* ctl, int k,
+                          cudaStream_t s);
+// Sets up (outside any stream capture) the launch facts of the kernels
+// launch_exhaustive_dev will launch for R and k.
+void warm_exhaustive_dev(const RoundBuf& R, int k);
+// k_round_resolve over the pair slots, the pair count read from ctl.
+void launch_round_resolve_dev(const RoundBuf& R, const RoundCtl* ctl, const QCOut& q, const Lanes& L,
+                              uint32_t max_spec, cudaStream_t s);
+// k_pair_scan that does its work only when the current round is empty (the
+// rescan step of the length-2 pass).
+void launch_pair_scan_gated(const DevTargets& T, const DevPool& P, const QCOut& q1, const Lanes& L2,
+                            const PairScan& ps, const RoundCtl* ctl, cudaStream_t s);
 void launch_midcheck(const DevTargets& T, const DevPool& P, const uint32_t* surv,
                      const uint32_t* surv_target, uint32_t nsurv, uint8_t* pass, cudaStream_t s);
 void launch_surv_targets(const QCOut& q, uint32_t n, uint32_t* surv_target, cudaStream_t s);
