@@ -37,11 +37,14 @@ constexpr uint32_t kResolved = 0x80000000u;
 constexpr int kBlock = 256;
 
 // Tables that lanes index with different values live in global memory (L1
-// cached); __constant__ is kept for the reduced-sweep values, whose index is
-// the same in every lane of a warp.  Every kernel that runs z_step gives all
-// lanes of a warp the same opcode: divergent dispatch of the 455-way switch
-// combined with lane-indexed constant loads in the same loop failed on this
-// toolchain (illegal address / no progress), so neither pattern is used.
+// cached; lane-indexed __constant__ loads would serialise); __constant__ is
+// kept for the reduced-sweep values, whose index is the same in every lane
+// of a warp.  Every kernel that runs z_step gives all lanes of a warp the
+// same opcode (a per-lane 455-way switch serialises by opcode).  A flag that
+// other warps write (the pair's rejection flag) is read by lane 0 and
+// broadcast, never read per lane in front of a warp collective: lanes that
+// read it at different times would leave the warp split at the next
+// __shfl_sync / __any_sync, which is undefined.
 __device__ OpInfo g_ops[kNumOps];
 __device__ uint32_t g_vec[32][3];  // MidCheck vectors; the first 8 are the QuickCheck vectors
 __constant__ uint8_t c_rep[32];
