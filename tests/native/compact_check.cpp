@@ -6,9 +6,10 @@
 // accepts, running the renamed programs on the renamed states over the
 // reference's whole ExhaustiveCheck sweep, comparing A, F (under the dead
 // flags) and the registers B, C only, gives the oracle's verdict for the
-// original pair.  (3) The bit-sliced step on the compact state (ZBc: A, F,
-// B, C and shared scratch) gives the full state's A, F, B and C for every
-// opcode that names no register but B and C.  (4) The device's tables
+// original pair.  (3) The bit-sliced step on the compact states (ZBc: A, F,
+// B, C and shared scratch; ZB4: A, F, B, C with its own step zb4_step)
+// gives the full state's A, F, B and C for every opcode that names no
+// register but B and C.  (4) The device's tables
 // (compact_tables) accept, rename and place registers as compact_map does.
 // (5) The compact kernel's sweep unit, restated with its plane layout and its
 // dead-flag and dead-register compares, gives the oracle's verdicts.  Built
@@ -200,11 +201,24 @@ int main() {
         cz.x[i] = 0;
       }
       for (int i = 0; i < 16; i++) cz.sp[i] = 0;
+      ZB4 z4;
+      for (int i = 0; i < 8; i++) {
+        z4.a[i] = full.a[i];
+        z4.f[i] = full.f[i];
+        z4.b[i] = full.b[i];
+        z4.c[i] = full.c[i];
+      }
       zb_step(full, op, imm);
       zb_step(cz, op, imm);
+      zb4_step(z4, op, imm);
       for (int i = 0; i < 8; i++)
         if (cz.a[i] != full.a[i] || cz.f[i] != full.f[i] || cz.b[i] != full.b[i] || cz.c[i] != full.c[i]) {
           std::printf("compact step differs on op %u (%s)\n", op, op_mnemonic(uint16_t(op)));
+          return 1;
+        }
+      for (int i = 0; i < 8; i++)
+        if (z4.a[i] != full.a[i] || z4.f[i] != full.f[i] || z4.b[i] != full.b[i] || z4.c[i] != full.c[i]) {
+          std::printf("A/F/B/C step differs on op %u (%s)\n", op, op_mnemonic(uint16_t(op)));
           return 1;
         }
     }
@@ -310,7 +324,7 @@ int main() {
         const Z80S x = decode(b, s);
         const uint32_t regs[6] = {x.b, x.c, x.d, x.e, x.h, x.l};
         for (uint32_t a0 = 0; a0 < 256 && !bad; a0 += 32) {
-          ZBc z;
+          ZB4 z;
           z.a[0] = 0xAAAAAAAAu;
           z.a[1] = 0xCCCCCCCCu;
           z.a[2] = 0xF0F0F0F0u;
@@ -320,11 +334,9 @@ int main() {
           zb_set8(z.f, x.f);
           zb_set8(z.b, o0 >= 0 ? regs[o0] : 0u);
           zb_set8(z.c, o1 >= 0 ? regs[o1] : 0u);
-          zb_set8(z.x, 0u);
-          for (int i = 0; i < 16; i++) z.sp[i] = 0;
-          ZBc zc = z, zt = z;
-          for (int i = 0; i < cn; i++) zb_step(zc, insn_op(cr[i]), insn_imm(cr[i]));
-          for (int i = 0; i < tn; i++) zb_step(zt, insn_op(tr[i]), insn_imm(tr[i]));
+          ZB4 zc = z, zt = z;
+          for (int i = 0; i < cn; i++) zb4_step(zc, insn_op(cr[i]), insn_imm(cr[i]));
+          for (int i = 0; i < tn; i++) zb4_step(zt, insn_op(tr[i]), insn_imm(tr[i]));
           uint32_t d = 0;
           for (int i = 0; i < 8; i++) {
             d |= zc.a[i] ^ zt.a[i];

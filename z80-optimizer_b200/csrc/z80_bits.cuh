@@ -370,38 +370,12 @@ Z80_HD void zb_pair(uint32_t (&v)[16], const uint32_t (&hi)[8], const uint32_t (
 #define ZB_RES(o, r) case (o): z.r[((o) - RES_0_A) / 7] = 0u; break;
 #define ZB_SET(o, r) case (o): z.r[((o) - SET_0_A) / 7] = kZBOnes; break;
 
-// One instruction on the 32 states of z (op and imm are the same for all).
+// The instructions that touch only A and F (RLCA, RRCA, RLA, RRA, DAA,
+// CPL, SCF, CCF, NEG, NOP); false for any other opcode.
 template <class ZT>
-Z80_HD void zb_step(ZT& z, uint32_t op, uint32_t imm) {
+Z80_HD bool zb_acc_step(ZT& z, uint32_t op) {
   uint32_t t8[8];
-  uint32_t t16[16];
   switch (op) {
-    ZB_S7(ZB_LDA, LD_A_B)
-    ZB_R7(ZB_LDB, LD_B_A)
-    ZB_R7(ZB_LDC, LD_C_A)
-    ZB_R7(ZB_LDD, LD_D_A)
-    ZB_R7(ZB_LDE, LD_E_A)
-    ZB_R7(ZB_LDH, LD_H_A)
-    ZB_R7(ZB_LDL, LD_L_A)
-    ZB_R7(ZB_LDN, LD_A_N)
-    ZB_S7(ZB_ADD, ADD_A_B)
-    case ADD_A_N: zb_set8(t8, imm & 0xFFu); zb_add(z, t8, 0u); break;
-    ZB_S7(ZB_ADC, ADC_A_B)
-    case ADC_A_N: zb_set8(t8, imm & 0xFFu); zb_add(z, t8, z.f[0]); break;
-    ZB_S7(ZB_SUB, SUB_B)
-    case SUB_N: zb_set8(t8, imm & 0xFFu); zb_sub(z, t8, 0u); break;
-    ZB_S7(ZB_SBC, SBC_A_B)
-    case SBC_A_N: zb_set8(t8, imm & 0xFFu); zb_sub(z, t8, z.f[0]); break;
-    ZB_S7(ZB_AND, AND_B)
-    case AND_N: zb_set8(t8, imm & 0xFFu); zb_and(z, t8); break;
-    ZB_S7(ZB_XOR, XOR_B)
-    case XOR_N: zb_set8(t8, imm & 0xFFu); zb_xor(z, t8); break;
-    ZB_S7(ZB_OR, OR_B)
-    case OR_N: zb_set8(t8, imm & 0xFFu); zb_or(z, t8); break;
-    ZB_S7(ZB_CP, CP_B)
-    case CP_N: zb_set8(t8, imm & 0xFFu); zb_cp(z, t8); break;
-    ZB_R7(ZB_INC, INC_A)
-    ZB_R7(ZB_DEC, DEC_A)
     case RLCA: {
       const uint32_t o7 = z.a[7];
       for (int i = 7; i > 0; i--) z.a[i] = z.a[i - 1];
@@ -439,6 +413,43 @@ Z80_HD void zb_step(ZT& z, uint32_t op, uint32_t imm) {
       zb_sub(z, t8, 0u);
     } break;
     case NOP: break;
+    default: return false;
+  }
+  return true;
+}
+
+// One instruction on the 32 states of z (op and imm are the same for all).
+template <class ZT>
+Z80_HD void zb_step(ZT& z, uint32_t op, uint32_t imm) {
+  uint32_t t8[8];
+  uint32_t t16[16];
+  switch (op) {
+    ZB_S7(ZB_LDA, LD_A_B)
+    ZB_R7(ZB_LDB, LD_B_A)
+    ZB_R7(ZB_LDC, LD_C_A)
+    ZB_R7(ZB_LDD, LD_D_A)
+    ZB_R7(ZB_LDE, LD_E_A)
+    ZB_R7(ZB_LDH, LD_H_A)
+    ZB_R7(ZB_LDL, LD_L_A)
+    ZB_R7(ZB_LDN, LD_A_N)
+    ZB_S7(ZB_ADD, ADD_A_B)
+    case ADD_A_N: zb_set8(t8, imm & 0xFFu); zb_add(z, t8, 0u); break;
+    ZB_S7(ZB_ADC, ADC_A_B)
+    case ADC_A_N: zb_set8(t8, imm & 0xFFu); zb_add(z, t8, z.f[0]); break;
+    ZB_S7(ZB_SUB, SUB_B)
+    case SUB_N: zb_set8(t8, imm & 0xFFu); zb_sub(z, t8, 0u); break;
+    ZB_S7(ZB_SBC, SBC_A_B)
+    case SBC_A_N: zb_set8(t8, imm & 0xFFu); zb_sub(z, t8, z.f[0]); break;
+    ZB_S7(ZB_AND, AND_B)
+    case AND_N: zb_set8(t8, imm & 0xFFu); zb_and(z, t8); break;
+    ZB_S7(ZB_XOR, XOR_B)
+    case XOR_N: zb_set8(t8, imm & 0xFFu); zb_xor(z, t8); break;
+    ZB_S7(ZB_OR, OR_B)
+    case OR_N: zb_set8(t8, imm & 0xFFu); zb_or(z, t8); break;
+    ZB_S7(ZB_CP, CP_B)
+    case CP_N: zb_set8(t8, imm & 0xFFu); zb_cp(z, t8); break;
+    ZB_R7(ZB_INC, INC_A)
+    ZB_R7(ZB_DEC, DEC_A)
     ZB_R7(ZB_RLC, RLC_A)
     ZB_R7(ZB_RRC, RRC_A)
     ZB_R7(ZB_RL, RL_A)
@@ -547,7 +558,65 @@ Z80_HD void zb_step(ZT& z, uint32_t op, uint32_t imm) {
     case SET_5_HLI: z.m[5] = kZBOnes; break;
     case SET_6_HLI: z.m[6] = kZBOnes; break;
     case SET_7_HLI: z.m[7] = kZBOnes; break;
-    default: break;
+    default: zb_acc_step(z, op); break;
+  }
+}
+
+// The A, F, B, C state of a compact sweep.  A compact program (a pair's
+// instructions renamed by compact_map) names no register but A, F, B and C
+// and neither SP nor the memory byte, so nothing else needs to be held.
+struct ZB4 {
+  uint32_t a[8], f[8], b[8], c[8];
+};
+#define ZB4_R(M, base) M((base) + 0, a) M((base) + 1, b) M((base) + 2, c)
+#define ZB4_S(M, base) M((base) + 0, b) M((base) + 1, c) M((base) + 6, a)
+
+// The step on ZB4: the cases of zb_step for every instruction that names no
+// register but A, F, B and C (the only ones a compact program holds); any
+// other opcode leaves the state unchanged and must not occur.
+Z80_HD void zb4_step(ZB4& z, uint32_t op, uint32_t imm) {
+  uint32_t t8[8];
+  switch (op) {
+    ZB4_S(ZB_LDA, LD_A_B)
+    ZB4_R(ZB_LDB, LD_B_A)
+    ZB4_R(ZB_LDC, LD_C_A)
+    ZB4_R(ZB_LDN, LD_A_N)
+    ZB4_S(ZB_ADD, ADD_A_B)
+    case ADD_A_N: zb_set8(t8, imm & 0xFFu); zb_add(z, t8, 0u); break;
+    ZB4_S(ZB_ADC, ADC_A_B)
+    case ADC_A_N: zb_set8(t8, imm & 0xFFu); zb_add(z, t8, z.f[0]); break;
+    ZB4_S(ZB_SUB, SUB_B)
+    case SUB_N: zb_set8(t8, imm & 0xFFu); zb_sub(z, t8, 0u); break;
+    ZB4_S(ZB_SBC, SBC_A_B)
+    case SBC_A_N: zb_set8(t8, imm & 0xFFu); zb_sub(z, t8, z.f[0]); break;
+    ZB4_S(ZB_AND, AND_B)
+    case AND_N: zb_set8(t8, imm & 0xFFu); zb_and(z, t8); break;
+    ZB4_S(ZB_XOR, XOR_B)
+    case XOR_N: zb_set8(t8, imm & 0xFFu); zb_xor(z, t8); break;
+    ZB4_S(ZB_OR, OR_B)
+    case OR_N: zb_set8(t8, imm & 0xFFu); zb_or(z, t8); break;
+    ZB4_S(ZB_CP, CP_B)
+    case CP_N: zb_set8(t8, imm & 0xFFu); zb_cp(z, t8); break;
+    ZB4_R(ZB_INC, INC_A)
+    ZB4_R(ZB_DEC, DEC_A)
+    ZB4_R(ZB_RLC, RLC_A)
+    ZB4_R(ZB_RRC, RRC_A)
+    ZB4_R(ZB_RL, RL_A)
+    ZB4_R(ZB_RR, RR_A)
+    ZB4_R(ZB_SLA, SLA_A)
+    ZB4_R(ZB_SRA, SRA_A)
+    ZB4_R(ZB_SRL, SRL_A)
+    ZB4_R(ZB_SLL, SLL_A)
+    ZB4_R(ZB_BIT, BIT_0_A) ZB4_R(ZB_BIT, BIT_1_A) ZB4_R(ZB_BIT, BIT_2_A) ZB4_R(ZB_BIT, BIT_3_A)
+    ZB4_R(ZB_BIT, BIT_4_A) ZB4_R(ZB_BIT, BIT_5_A) ZB4_R(ZB_BIT, BIT_6_A) ZB4_R(ZB_BIT, BIT_7_A)
+    ZB4_R(ZB_RES, RES_0_A) ZB4_R(ZB_RES, RES_1_A) ZB4_R(ZB_RES, RES_2_A) ZB4_R(ZB_RES, RES_3_A)
+    ZB4_R(ZB_RES, RES_4_A) ZB4_R(ZB_RES, RES_5_A) ZB4_R(ZB_RES, RES_6_A) ZB4_R(ZB_RES, RES_7_A)
+    ZB4_R(ZB_SET, SET_0_A) ZB4_R(ZB_SET, SET_1_A) ZB4_R(ZB_SET, SET_2_A) ZB4_R(ZB_SET, SET_3_A)
+    ZB4_R(ZB_SET, SET_4_A) ZB4_R(ZB_SET, SET_5_A) ZB4_R(ZB_SET, SET_6_A) ZB4_R(ZB_SET, SET_7_A)
+    case INC_BC: zb_inc16(z.b, z.c, false); break;
+    case DEC_BC: zb_inc16(z.b, z.c, true); break;
+    case LD_BC_NN: zb_set8(z.b, (imm >> 8) & 0xFFu); zb_set8(z.c, imm & 0xFFu); break;
+    default: zb_acc_step(z, op); break;
   }
 }
 

@@ -732,7 +732,7 @@ __device__ __forceinline__ bool bits_unit(unsigned long long u, unsigned long lo
 }
 
 // One unit of a compact sweep: the layout of bits_unit (lane l: block 4u +
-// l/8, A = 32(l % 8) .. +31) on the compact state (A, F, B, C; ZBc).  The
+// l/8, A = 32(l % 8) .. +31) on the compact state (A, F, B, C; ZB4).  The
 // pair's programs arrive renamed onto B and C; o0 / o1 are the original
 // registers (0..5 = B..L) that B and C stand for, or -1 where none does.
 // Only A, F (under keepF) and those registers (under keepR) can differ.
@@ -758,7 +758,7 @@ __device__ __forceinline__ bool cbits_unit(unsigned long long u, unsigned long l
     }
   };
   const uint32_t vb = regval(o0), vc = regval(o1);
-  ZBc z;
+  ZB4 z;
   auto init = [&]() {
     z.a[0] = 0xAAAAAAAAu;
     z.a[1] = 0xCCCCCCCCu;
@@ -771,9 +771,6 @@ __device__ __forceinline__ bool cbits_unit(unsigned long long u, unsigned long l
     zb_set8(z.f, x.f);
     zb_set8(z.b, vb);
     zb_set8(z.c, vc);
-    zb_set8(z.x, 0u);
-#pragma unroll
-    for (int i = 0; i < 16; i++) z.sp[i] = 0u;
   };
   init();
 #pragma unroll 1
@@ -790,7 +787,7 @@ __device__ __forceinline__ bool cbits_unit(unsigned long long u, unsigned long l
     }
     const int src = st < cl ? tl + st : st - cl;
     const uint32_t w = __shfl_sync(kFull, pw, src);
-    zb_step(z, w & 0xFFFFu, w >> 16);
+    zb4_step(z, w & 0xFFFFu, w >> 16);
   }
   const bool cmp_b = o0 >= 0 && ((keepR >> o0) & 1u), cmp_c = o1 >= 0 && ((keepR >> o1) & 1u);
   uint32_t d = 0;
@@ -944,14 +941,14 @@ __device__ __noinline__ bool xindep_unit(unsigned long long first, unsigned long
 // One kernel per pair class: CLS 0 runs the bit-sliced pairs (outputs
 // depend on A), CLS 1 the A-independent ones (K states per lane per
 // dispatch), CLS 2 the A-independent ones bit-sliced, CLS 3 the A-dependent
-// ones whose registers fit the compact state (two blocks per SM); each class
+// ones whose registers fit the compact state (three blocks per SM); each class
 // draws chunks from its own numbering and dispenser.  Kept apart so that
 // neither path's registers weigh on the other.
 // dev_total / dev_np (device-driven rounds): the class's chunk total and the
 // round's pair count are read from the device instead of total / npairs.
 // chunks_per_warp: chunks a warp takes before its block retires.
 template <int K, int CLS>
-__global__ void __launch_bounds__(kBlock, CLS == 3 ? 2 : 1)
+__global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : 1)
     k_exhaustive(DevTargets T, DevPool P, RoundBuf R, uint32_t npairs, unsigned long long total,
                  const unsigned long long* __restrict__ dev_total, const uint32_t* __restrict__ dev_np,
                  int chunks_per_warp) {
