@@ -11,8 +11,10 @@
 // gives the full state's A, F, B and C for every opcode that names no
 // register but B and C.  (4) The device's tables
 // (compact_tables) accept, rename and place registers as compact_map does.
-// (5) The compact kernel's sweep unit, restated with its plane layout and its
-// dead-flag and dead-register compares, gives the oracle's verdicts.  Built
+// (5), (6) The compact kernel's sweep units (A-dependent pairs, and
+// A-independent pairs at A = 0 and 1 with 32 blocks per state word),
+// restated with their plane layouts and their dead-flag and dead-register
+// compares, give the oracle's verdicts.  Built
 // and run by tests/test_tables.py.
 #include <cstdio>
 #include <random>
@@ -357,6 +359,102 @@ int main() {
     }
     if (cp < 200 || ceq < 30) {
       std::printf("too few compact A-dependent pairs (%d) or equivalences (%d)\n", cp, ceq);
+      return 1;
+    }
+  }
+  // (6) the compact kernel's A-independent unit restated (cxbits_unit in
+  // z80b_kernels.cu): per aligned group of 32 blocks one state word (block j
+  // in bit j), the moving field -- the last swept register, renamed onto B
+  // or C, or the carry -- as counting planes plus the group's high bits,
+  // every other field the group's decoded value; A at 0 and then 1; lanes
+  // past the sweep's end masked out; against the oracle with dead registers
+  {
+    const CompactTables& T = compact_tables();
+    int cp = 0, ceq = 0;
+    for (int trial = 0; trial < 4000000 && cp < 400; trial++) {
+      const int tn = 1 + int(rng() % 2);
+      int cn = 1 + int(rng() % 2);
+      orc::Instruction ti[2], ci[2];
+      uint32_t tw[2], cw[2];
+      for (int i = 0; i < tn; i++) ti[i] = I[rng() % I.size()];
+      for (int i = 0; i < cn; i++) ci[i] = I[rng() % I.size()];
+      if (rng() % 3 == 0) {
+        ci[0] = ti[tn - 1];
+        cn = 1;
+      }
+      for (int i = 0; i < tn; i++) tw[i] = uint32_t(ti[i].op) | uint32_t(ti[i].imm) << 16;
+      for (int i = 0; i < cn; i++) cw[i] = uint32_t(ci[i].op) | uint32_t(ci[i].imm) << 16;
+      if (!(seq_aflow(tw, tn) && seq_aflow(cw, cn))) continue;  // A-independent pairs only
+      uint8_t fp = 0;
+      for (int i = 0; i < tn; i++) fp |= T.opregs[insn_op(tw[i])];
+      for (int i = 0; i < cn; i++) fp |= T.opregs[insn_op(cw[i])];
+      const int id = (fp & 0xC0) ? 0 : T.id_of_set[fp & 0x3F];
+      bool ok = id != 0;
+      for (int i = 0; i < tn && ok; i++) ok = T.ren[id - 1][insn_op(tw[i])] >= 0;
+      for (int i = 0; i < cn && ok; i++) ok = T.ren[id - 1][insn_op(cw[i])] >= 0;
+      if (!ok) continue;
+      const Shape s = shape_of(uint16_t(seq_reads(tw, tn) | seq_reads(cw, cn)));
+      if (s.spw || s.reduced) {
+        std::printf("a compact pair with a reduced or SP sweep\n");
+        return 1;
+      }
+      cp++;
+      uint32_t tr[2], cr[2];
+      for (int i = 0; i < tn; i++) tr[i] = uint32_t(uint16_t(T.ren[id - 1][insn_op(tw[i])])) | (tw[i] & 0xFFFF0000u);
+      for (int i = 0; i < cn; i++) cr[i] = uint32_t(uint16_t(T.ren[id - 1][insn_op(cw[i])])) | (cw[i] & 0xFFFF0000u);
+      const int o0 = T.orig[id - 1][0], o1 = T.orig[id - 1][1];
+      int rlast = -1;
+      for (int r = 0; r < 7; r++)
+        if (s.slot[r] == s.nx - 1) rlast = r;
+      if (s.nx > 0 && rlast != o0 && rlast != o1) {
+        std::printf("the last swept register is neither renamed register\n");
+        return 1;
+      }
+      const uint8_t dead = uint8_t(rng() & 0xFF), dregs = uint8_t(rng() & 0x3F);
+      const uint32_t keepF = uint8_t(~dead), keepR = ~uint32_t(dregs) & 0x3Fu;
+      const bool cmp_b = o0 >= 0 && ((keepR >> o0) & 1u), cmp_c = o1 >= 0 && ((keepR >> o1) & 1u);
+      bool bad = false;
+      for (uint64_t g0 = 0; g0 < s.nblocks && !bad; g0 += 32) {
+        const uint32_t valid = s.nblocks - g0 >= 32 ? 0xFFFFFFFFu : ((1u << uint32_t(s.nblocks - g0)) - 1u);
+        const Z80S x = decode(g0, s);
+        const uint32_t regs[6] = {x.b, x.c, x.d, x.e, x.h, x.l};
+        const uint32_t vb = o0 >= 0 ? regs[o0] : 0u, vc = o1 >= 0 ? regs[o1] : 0u;
+        const uint32_t v = rlast == o0 ? vb : vc;
+        uint32_t vp[8] = {0xAAAAAAAAu, 0xCCCCCCCCu, 0xF0F0F0F0u, 0xFF00FF00u, 0xFFFF0000u, 0, 0, 0};
+        for (int i = 5; i < 8; i++) vp[i] = ((v >> i) & 1u) ? kZBOnes : 0u;
+        for (uint32_t abit = 0; abit < 2 && !bad; abit++) {
+          ZB4 z;
+          zb_set8(z.a, abit);
+          zb_set8(z.f, x.f);
+          zb_set8(z.b, vb);
+          zb_set8(z.c, vc);
+          if (s.nx == 0) z.f[0] = 0xAAAAAAAAu;
+          else if (rlast == o0) zb_copy8(z.b, vp);
+          else zb_copy8(z.c, vp);
+          ZB4 zc = z, zt = z;
+          for (int i = 0; i < cn; i++) zb4_step(zc, insn_op(cr[i]), insn_imm(cr[i]));
+          for (int i = 0; i < tn; i++) zb4_step(zt, insn_op(tr[i]), insn_imm(tr[i]));
+          uint32_t d = 0;
+          for (int i = 0; i < 8; i++) {
+            d |= zc.a[i] ^ zt.a[i];
+            if ((keepF >> i) & 1u) d |= zc.f[i] ^ zt.f[i];
+            if (cmp_b) d |= zc.b[i] ^ zt.b[i];
+            if (cmp_c) d |= zc.c[i] ^ zt.c[i];
+          }
+          bad = (d & valid) != 0;
+        }
+      }
+      const bool want = orc::ExhaustiveCheckMaskedRegs(ti, tn, ci, cn, dead, dregs);
+      if (want == bad) {
+        std::printf("compact A-independent unit verdict differs: target %08x %08x (%d) candidate %08x %08x (%d) "
+                    "dead %02x regs %02x\n",
+                    tw[0], tn > 1 ? tw[1] : 0, tn, cw[0], cn > 1 ? cw[1] : 0, cn, dead, dregs);
+        return 1;
+      }
+      ceq += want ? 1 : 0;
+    }
+    if (cp < 200 || ceq < 30) {
+      std::printf("too few compact A-independent pairs (%d) or equivalences (%d)\n", cp, ceq);
       return 1;
     }
   }

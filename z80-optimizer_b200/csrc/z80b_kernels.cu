@@ -488,7 +488,9 @@ __device__ __forceinline__ void put_pair(const RoundBuf& R, uint32_t p, const De
   pr.keepF = kind ? uint8_t(~target_dead(T, t)) : uint8_t(0xFFu);
   pr.keepR = kind ? uint8_t((~target_dead_regs(T, t) & 0x3Fu) | 0x80u) : uint8_t(0x3Fu);
   if (pair_xindep(T, t, P, c)) pr.keepR |= uint8_t(kXIndep);
-  pr.cmap = (R.compact && !(pr.keepR & kXIndep)) ? pair_cmap(T, t, P, c) : uint8_t(0);
+  // compact class: A-dependent pairs, and A-independent ones when those are
+  // swept bit-sliced (units of kXBitsBlocks)
+  pr.cmap = (R.compact && (!(pr.keepR & kXIndep) || R.xunit == kXBitsBlocks)) ? pair_cmap(T, t, P, c) : uint8_t(0);
   R.pairs[p] = pr;
   R.pair_src[p] = src;
   set_chunks(R, p, pr);
@@ -907,6 +909,88 @@ __device__ __forceinline__ bool xbits_unit(unsigned long long u, unsigned long l
   return bad;
 }
 
+// One unit of a compact A-independent sweep: xbits_unit's layout (lane l:
+// the 32 A-blocks u*1024 + 32l .. +31 as one state word, at A = 0 then
+// A = 1) on the A/F/B/C state with renamed programs.  A compact pair reads
+// neither SP nor more than two registers, so its sweep is a full one over
+// at most two fields, and the field the low 5 block bits move is the last
+// swept register, now B (o0) or C (o1), or with no swept register the carry.
+__device__ __forceinline__ bool cxbits_unit(unsigned long long u, unsigned long long nblocks, int nx, int fw,
+                                            const int (&slot)[7], int rlast, uint32_t pw, int tl, int cl,
+                                            uint32_t keepF, uint32_t keepR, int o0, int o1, uint32_t* sm) {
+  const unsigned lane = lane_id();
+  const unsigned long long g0 = u * kXBitsBlocks + (unsigned long long)lane * 32ull;
+  const uint32_t valid = g0 >= nblocks ? 0u
+                         : (nblocks - g0 >= 32ull ? 0xFFFFFFFFu : ((1u << uint32_t(nblocks - g0)) - 1u));
+  Z80S x;
+  decode_block<false>(g0 < nblocks ? g0 : 0ull, false, false, nx, fw, slot, x);
+  auto regval = [&](int r) -> uint32_t {
+    switch (r) {
+      case 0: return x.b;
+      case 1: return x.c;
+      case 2: return x.d;
+      case 3: return x.e;
+      case 4: return x.h;
+      case 5: return x.l;
+      default: return 0u;
+    }
+  };
+  const uint32_t vb = regval(o0), vc = regval(o1);
+  // the moving field's planes: state j has j in its low 5 bits, the group's
+  // value above them
+  const uint32_t v = rlast == o0 ? vb : vc;
+  uint32_t vp[8];
+  vp[0] = 0xAAAAAAAAu;
+  vp[1] = 0xCCCCCCCCu;
+  vp[2] = 0xF0F0F0F0u;
+  vp[3] = 0xFF00FF00u;
+  vp[4] = 0xFFFF0000u;
+#pragma unroll
+  for (int i = 5; i < 8; i++) vp[i] = ((v >> i) & 1u) ? kZBOnes : 0u;
+  ZB4 z;
+  bool bad = false;
+#pragma unroll 1
+  for (uint32_t abit = 0; abit < 2u; abit++) {
+    auto init = [&]() {
+      zb_set8(z.a, abit);
+      zb_set8(z.f, x.f);
+      zb_set8(z.b, vb);
+      zb_set8(z.c, vc);
+      if (nx == 0) z.f[0] = 0xAAAAAAAAu;
+      else if (rlast == o0) zb_copy8(z.b, vp);
+      else zb_copy8(z.c, vp);
+    };
+    init();
+#pragma unroll 1
+    for (int st = 0; st < tl + cl; st++) {
+      if (st == cl) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+          sm[(0 + i) * 32] = z.a[i];
+          sm[(8 + i) * 32] = z.f[i];
+          sm[(16 + i) * 32] = z.b[i];
+          sm[(24 + i) * 32] = z.c[i];
+        }
+        init();
+      }
+      const int src = st < cl ? tl + st : st - cl;
+      const uint32_t w = __shfl_sync(kFull, pw, src);
+      zb4_step(z, w & 0xFFFFu, w >> 16);
+    }
+    const bool cmp_b = o0 >= 0 && ((keepR >> o0) & 1u), cmp_c = o1 >= 0 && ((keepR >> o1) & 1u);
+    uint32_t d = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      d |= z.a[i] ^ sm[(0 + i) * 32];
+      if ((keepF >> i) & 1u) d |= z.f[i] ^ sm[(8 + i) * 32];
+      if (cmp_b) d |= z.b[i] ^ sm[(16 + i) * 32];
+      if (cmp_c) d |= z.c[i] ^ sm[(24 + i) * 32];
+    }
+    bad = bad || (d & valid) != 0u;
+  }
+  return bad;
+}
+
 // One unit (128 A-blocks at A = 0, 1) of an A-independent sweep, for the
 // A-independent sweep kernel; kept out of line (that kernel compiles without
 // register spills at every K this way).
@@ -1023,18 +1107,37 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : 1)
       const int o0 = g_corig[e][0], o1 = g_corig[e][1];
       extern __shared__ uint32_t zsm[];
       uint32_t* sm = zsm + (threadIdx.x >> 5) * (kCompactWords * 32) + lane;
-      for (unsigned long long u = u0; u < u1; u++) {
-        const unsigned long long first = u * kBitsBlocks;
-        const unsigned long long nb = (pr.nblocks - first < kBitsBlocks) ? pr.nblocks - first : kBitsBlocks;
-        bad = cbits_unit(u, pr.nblocks, spw, reduced, nx, fw, slot, pw, int(tl), int(cl), pr.keepF, pr.keepR, o0, o1,
-                         sm) ||
-              bad;
-        my_states += 256ull * nb;
-        my_eval += 256ull * nb;
-        if (__any_sync(kFull, bad)) break;
-        if ((u & 15ull) == 15ull &&
-            __shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0))
-          break;
+      if (pr.keepR & kXIndep) {
+        // A-independent: units of 1,024 A-blocks, each at A = 0 and 1
+        int rlast = -1;
+#pragma unroll
+        for (int r = 0; r < 7; r++)
+          if (slot[r] == nx - 1) rlast = r;
+        for (unsigned long long u = u0; u < u1; u++) {
+          const unsigned long long first = u * kXBitsBlocks;
+          const unsigned long long nb = (pr.nblocks - first < kXBitsBlocks) ? pr.nblocks - first : kXBitsBlocks;
+          bad = cxbits_unit(u, pr.nblocks, nx, fw, slot, rlast, pw, int(tl), int(cl), pr.keepF, pr.keepR, o0, o1,
+                            sm) ||
+                bad;
+          my_states += 256ull * nb;
+          my_eval += 2ull * nb;
+          if (__any_sync(kFull, bad)) break;
+          if (__shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0)) break;
+        }
+      } else {
+        for (unsigned long long u = u0; u < u1; u++) {
+          const unsigned long long first = u * kBitsBlocks;
+          const unsigned long long nb = (pr.nblocks - first < kBitsBlocks) ? pr.nblocks - first : kBitsBlocks;
+          bad = cbits_unit(u, pr.nblocks, spw, reduced, nx, fw, slot, pw, int(tl), int(cl), pr.keepF, pr.keepR, o0,
+                           o1, sm) ||
+                bad;
+          my_states += 256ull * nb;
+          my_eval += 256ull * nb;
+          if (__any_sync(kFull, bad)) break;
+          if ((u & 15ull) == 15ull &&
+              __shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0))
+            break;
+        }
       }
     } else if constexpr (!XI) {
       // Unit = 4 A-blocks, bit-sliced (256 states of each block in 8 lanes).
