@@ -98,16 +98,16 @@ def test_a_independent_sweep_kernels_keep_parity(ctx, O, xbits):
     assert st2.checked_ref == checked
 
 
-@pytest.mark.skipif(os.environ.get("Z80B_TEST_COMPACT") != "1",
-                    reason="the compact sweep kernel is off by default until it has run on a GPU "
-                           "(set Z80B_TEST_COMPACT=1)")
-def test_compact_sweep_keeps_parity(ctx, O):
-    """Z80B_OPT_COMPACT_SWEEP = 1: the C3 sample's rules and 'checked'
-    counter, and a C2 sample against the oracle, are unchanged."""
+@pytest.mark.parametrize("compact", [0, 1])
+def test_compact_sweep_keeps_parity(ctx, O, compact):
+    """Z80B_OPT_COMPACT_SWEEP off and on: the C3 sample's rules and 'checked'
+    counter, and a C2 sample against the oracle, are unchanged (on: pairs
+    naming at most two of B..L, A-dependent and A-independent, run on the
+    A/F/B/C-state kernel)."""
     import workloads
     fx = fixture()
     old = ctx.get_option(z80b.OPT_COMPACT_SWEEP)
-    ctx.set_option(z80b.OPT_COMPACT_SWEEP, 1)
+    ctx.set_option(z80b.OPT_COMPACT_SWEEP, compact)
     try:
         rules, st = run(ctx, fx)
         targets = workloads.to_lists(workloads.c2_subset(3000, seed=12))

@@ -32,7 +32,7 @@ OPT_LANE_STATES, OPT_CHUNK_BLOCKS = 1, 2
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--targets", type=int, default=30000)
+    ap.add_argument("--targets", type=int, default=30000, help="C2 targets (0 = all 9,818,041)")
     ap.add_argument("--seed", type=int, default=3)
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--lane-states", type=int, default=4)
@@ -74,7 +74,8 @@ def main():
                   f"{st.rounds} rounds, {st.launches} launches, device {st.device_ms:.2f} ms", flush=True)
         ctx.close()
         return 0
-    arr = np.ascontiguousarray(workloads.c2_subset(a.targets, seed=a.seed))
+    arr = np.ascontiguousarray(workloads.c2_subset(a.targets, seed=a.seed) if a.targets
+                               else workloads.c2_targets())
     ctx = z80b.Context(0)
     ctx.set_option(OPT_LANE_STATES, a.lane_states)
     ctx.set_option(OPT_CHUNK_BLOCKS, a.chunk_blocks)

@@ -133,7 +133,13 @@ def run(rate, seconds, seed, workers=4, max_batch=512, verify=True, memory_budge
     done.set()
     th.join(timeout=600)
     t_end = time.perf_counter() - t0
-    stats = srv.stats().as_dict()
+    # a batch's answers leave before its worker has released the batch's
+    # frontier; wait for the books to settle before reading them
+    for _ in range(1000):
+        stats = srv.stats().as_dict()
+        if stats["inflight_bytes"] == 0 and stats["pending"] == 0:
+            break
+        time.sleep(0.01)
     srv.stop()
     lat = np.array([answers[k].latency_ms for k in range(n) if k in answers])
     served = np.array([answers[k].latency_ms for k in range(n) if k in answers and answers[k].batch_size > 0])
