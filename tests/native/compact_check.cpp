@@ -322,9 +322,19 @@ int main() {
       const uint32_t keepF = uint8_t(~dead), keepR = ~uint32_t(dregs) & 0x3Fu;
       const bool cmp_b = o0 >= 0 && ((keepR >> o0) & 1u), cmp_c = o1 >= 0 && ((keepR >> o1) & 1u);
       bool bad = false;
+      const CDec dec = cdec_make(s.nx, s.slot, o0, o1);
       for (uint64_t b = 0; b < s.nblocks && !bad; b++) {
         const Z80S x = decode(b, s);
         const uint32_t regs[6] = {x.b, x.c, x.d, x.e, x.h, x.l};
+        {
+          // the kernel's shift-and-mask decoding of B, C and the carry
+          uint32_t vb, vc, carry;
+          cdec_vals(dec, b, vb, vc, carry);
+          if (vb != (o0 >= 0 ? regs[o0] : 0u) || vc != (o1 >= 0 ? regs[o1] : 0u) || carry != x.f) {
+            std::printf("compact block decoding differs at block %llu\n", (unsigned long long)b);
+            return 1;
+          }
+        }
         for (uint32_t a0 = 0; a0 < 256 && !bad; a0 += 32) {
           ZB4 z;
           z.a[0] = 0xAAAAAAAAu;
@@ -414,11 +424,20 @@ int main() {
       const uint32_t keepF = uint8_t(~dead), keepR = ~uint32_t(dregs) & 0x3Fu;
       const bool cmp_b = o0 >= 0 && ((keepR >> o0) & 1u), cmp_c = o1 >= 0 && ((keepR >> o1) & 1u);
       bool bad = false;
+      const CDec dec = cdec_make(s.nx, s.slot, o0, o1);
       for (uint64_t g0 = 0; g0 < s.nblocks && !bad; g0 += 32) {
         const uint32_t valid = s.nblocks - g0 >= 32 ? 0xFFFFFFFFu : ((1u << uint32_t(s.nblocks - g0)) - 1u);
         const Z80S x = decode(g0, s);
         const uint32_t regs[6] = {x.b, x.c, x.d, x.e, x.h, x.l};
         const uint32_t vb = o0 >= 0 ? regs[o0] : 0u, vc = o1 >= 0 ? regs[o1] : 0u;
+        {
+          uint32_t db, dc, dcarry;
+          cdec_vals(dec, g0, db, dc, dcarry);
+          if (db != vb || dc != vc || dcarry != x.f) {
+            std::printf("compact group decoding differs at block %llu\n", (unsigned long long)g0);
+            return 1;
+          }
+        }
         const uint32_t v = rlast == o0 ? vb : vc;
         uint32_t vp[8] = {0xAAAAAAAAu, 0xCCCCCCCCu, 0xF0F0F0F0u, 0xFF00FF00u, 0xFFFF0000u, 0, 0, 0};
         for (int i = 5; i < 8; i++) vp[i] = ((v >> i) & 1u) ? kZBOnes : 0u;

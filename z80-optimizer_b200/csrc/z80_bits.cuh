@@ -620,6 +620,36 @@ Z80_HD void zb4_step(ZB4& z, uint32_t op, uint32_t imm) {
   }
 }
 
+// Block decoding for compact pairs.  A compact pair reads at most two
+// registers and neither SP nor the memory byte, so its sweep is a full one:
+// block index = carry above nx 8-bit fields, the last swept register in the
+// lowest byte.  The initial values of the renamed B and C (the registers o0
+// and o1 stand for) and the carry are then shifts and masks of the block
+// index, set up once per pair: slot[r] is register r's field (-1: not
+// swept; a register that is named but not read starts at 0).
+struct CDec {
+  uint32_t shb, mb, shc, mc, shf;
+};
+Z80_HD CDec cdec_make(int nx, const int (&slot)[7], int o0, int o1) {
+  CDec d{0u, 0u, 0u, 0u, uint32_t(8 * nx)};
+  if (o0 >= 0 && slot[o0] >= 0) {
+    d.shb = uint32_t(8 * (nx - 1 - slot[o0]));
+    d.mb = 0xFFu;
+  }
+  if (o1 >= 0 && slot[o1] >= 0) {
+    d.shc = uint32_t(8 * (nx - 1 - slot[o1]));
+    d.mc = 0xFFu;
+  }
+  return d;
+}
+// B, C and the carry of block ab.
+Z80_HD void cdec_vals(const CDec& d, unsigned long long ab, uint32_t& vb, uint32_t& vc, uint32_t& carry) {
+  const uint32_t lo = uint32_t(ab);
+  vb = (lo >> d.shb) & d.mb;
+  vc = (lo >> d.shc) & d.mc;
+  carry = (lo >> d.shf) & 1u;
+}
+
 // Planes <-> scalar states (host tests; the sweep builds planes directly).
 template <class ZT>
 Z80_HD void zb_from(ZT& z, const Z80S (&s)[32]) {

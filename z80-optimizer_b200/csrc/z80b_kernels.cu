@@ -739,27 +739,15 @@ __device__ __forceinline__ bool bits_unit(unsigned long long u, unsigned long lo
 // registers (0..5 = B..L) that B and C stand for, or -1 where none does.
 // Only A, F (under keepF) and those registers (under keepR) can differ.
 constexpr int kCompactWords = 32;  // planes saved per lane: A, F, B, C
-__device__ __forceinline__ bool cbits_unit(unsigned long long u, unsigned long long nblocks, bool spw, bool reduced,
-                                           int nx, int fw, const int (&slot)[7], uint32_t pw, int tl, int cl,
-                                           uint32_t keepF, uint32_t keepR, int o0, int o1, uint32_t* sm) {
+__device__ __forceinline__ bool cbits_unit(unsigned long long u, unsigned long long nblocks, const CDec& dec,
+                                           uint32_t pw, int tl, int cl, uint32_t keepF, uint32_t keepR, int o0, int o1,
+                                           uint32_t* sm) {
   const unsigned lane = lane_id();
   const unsigned long long blk = u * kBitsBlocks + (lane >> 3);
   const bool valid = blk < nblocks;
-  Z80S x;
-  decode_block<false>(valid ? blk : u * kBitsBlocks, spw, reduced, nx, fw, slot, x);
+  uint32_t vb, vc, carry;
+  cdec_vals(dec, valid ? blk : u * kBitsBlocks, vb, vc, carry);
   const uint32_t a0 = (lane & 7u) * 32u;
-  auto regval = [&](int r) -> uint32_t {
-    switch (r) {
-      case 0: return x.b;
-      case 1: return x.c;
-      case 2: return x.d;
-      case 3: return x.e;
-      case 4: return x.h;
-      case 5: return x.l;
-      default: return 0u;
-    }
-  };
-  const uint32_t vb = regval(o0), vc = regval(o1);
   ZB4 z;
   auto init = [&]() {
     z.a[0] = 0xAAAAAAAAu;
@@ -770,7 +758,7 @@ __device__ __forceinline__ bool cbits_unit(unsigned long long u, unsigned long l
     z.a[5] = (a0 & 32u) ? kZBOnes : 0u;
     z.a[6] = (a0 & 64u) ? kZBOnes : 0u;
     z.a[7] = (a0 & 128u) ? kZBOnes : 0u;
-    zb_set8(z.f, x.f);
+    zb_set8(z.f, carry);
     zb_set8(z.b, vb);
     zb_set8(z.c, vc);
   };
@@ -915,27 +903,15 @@ __device__ __forceinline__ bool xbits_unit(unsigned long long u, unsigned long l
 // neither SP nor more than two registers, so its sweep is a full one over
 // at most two fields, and the field the low 5 block bits move is the last
 // swept register, now B (o0) or C (o1), or with no swept register the carry.
-__device__ __forceinline__ bool cxbits_unit(unsigned long long u, unsigned long long nblocks, int nx, int fw,
-                                            const int (&slot)[7], int rlast, uint32_t pw, int tl, int cl,
-                                            uint32_t keepF, uint32_t keepR, int o0, int o1, uint32_t* sm) {
+__device__ __forceinline__ bool cxbits_unit(unsigned long long u, unsigned long long nblocks, int nx, const CDec& dec,
+                                            int rlast, uint32_t pw, int tl, int cl, uint32_t keepF, uint32_t keepR,
+                                            int o0, int o1, uint32_t* sm) {
   const unsigned lane = lane_id();
   const unsigned long long g0 = u * kXBitsBlocks + (unsigned long long)lane * 32ull;
   const uint32_t valid = g0 >= nblocks ? 0u
                          : (nblocks - g0 >= 32ull ? 0xFFFFFFFFu : ((1u << uint32_t(nblocks - g0)) - 1u));
-  Z80S x;
-  decode_block<false>(g0 < nblocks ? g0 : 0ull, false, false, nx, fw, slot, x);
-  auto regval = [&](int r) -> uint32_t {
-    switch (r) {
-      case 0: return x.b;
-      case 1: return x.c;
-      case 2: return x.d;
-      case 3: return x.e;
-      case 4: return x.h;
-      case 5: return x.l;
-      default: return 0u;
-    }
-  };
-  const uint32_t vb = regval(o0), vc = regval(o1);
+  uint32_t vb, vc, carry;
+  cdec_vals(dec, g0 < nblocks ? g0 : 0ull, vb, vc, carry);
   // the moving field's planes: state j has j in its low 5 bits, the group's
   // value above them
   const uint32_t v = rlast == o0 ? vb : vc;
@@ -953,7 +929,7 @@ __device__ __forceinline__ bool cxbits_unit(unsigned long long u, unsigned long 
   for (uint32_t abit = 0; abit < 2u; abit++) {
     auto init = [&]() {
       zb_set8(z.a, abit);
-      zb_set8(z.f, x.f);
+      zb_set8(z.f, carry);
       zb_set8(z.b, vb);
       zb_set8(z.c, vc);
       if (nx == 0) z.f[0] = 0xAAAAAAAAu;
@@ -1107,6 +1083,7 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : 1)
       const int o0 = g_corig[e][0], o1 = g_corig[e][1];
       extern __shared__ uint32_t zsm[];
       uint32_t* sm = zsm + (threadIdx.x >> 5) * (kCompactWords * 32) + lane;
+      const CDec dec = cdec_make(nx, slot, o0, o1);
       if (pr.keepR & kXIndep) {
         // A-independent: units of 1,024 A-blocks, each at A = 0 and 1
         int rlast = -1;
@@ -1116,8 +1093,7 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : 1)
         for (unsigned long long u = u0; u < u1; u++) {
           const unsigned long long first = u * kXBitsBlocks;
           const unsigned long long nb = (pr.nblocks - first < kXBitsBlocks) ? pr.nblocks - first : kXBitsBlocks;
-          bad = cxbits_unit(u, pr.nblocks, nx, fw, slot, rlast, pw, int(tl), int(cl), pr.keepF, pr.keepR, o0, o1,
-                            sm) ||
+          bad = cxbits_unit(u, pr.nblocks, nx, dec, rlast, pw, int(tl), int(cl), pr.keepF, pr.keepR, o0, o1, sm) ||
                 bad;
           my_states += 256ull * nb;
           my_eval += 2ull * nb;
@@ -1128,9 +1104,7 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : 1)
         for (unsigned long long u = u0; u < u1; u++) {
           const unsigned long long first = u * kBitsBlocks;
           const unsigned long long nb = (pr.nblocks - first < kBitsBlocks) ? pr.nblocks - first : kBitsBlocks;
-          bad = cbits_unit(u, pr.nblocks, spw, reduced, nx, fw, slot, pw, int(tl), int(cl), pr.keepF, pr.keepR, o0,
-                           o1, sm) ||
-                bad;
+          bad = cbits_unit(u, pr.nblocks, dec, pw, int(tl), int(cl), pr.keepF, pr.keepR, o0, o1, sm) || bad;
           my_states += 256ull * nb;
           my_eval += 256ull * nb;
           if (__any_sync(kFull, bad)) break;
