@@ -69,6 +69,34 @@ Z80S decode(uint64_t ab, const Shape& s) {
   return Z80S{0, uint32_t(rest & 1), rv[0], rv[1], rv[2], rv[3], rv[4], rv[5], sp, rv[6]};
 }
 
+// The kernels' shift-and-mask block decoder (bdec_make / bdec_state in
+// z80_bits.cuh) against the decoder above, for every combination of swept
+// registers and SP; returns false on a difference.
+bool check_bdec() {
+  std::mt19937_64 rng(99);
+  int n = 0;
+  for (uint32_t m = 0; m < 256; m++) {
+    uint16_t reads = uint16_t(kRegA);
+    const uint32_t bits[8] = {kRegB, kRegC, kRegD, kRegE, kRegH, kRegL, kRegM, kRegSP};
+    for (int i = 0; i < 8; i++)
+      if ((m >> i) & 1u) reads |= uint16_t(bits[i]);
+    const Shape s = shape_of(reads);
+    const BDec d = bdec_make(s.spw, s.reduced, s.nx, s.fw, s.slot);
+    for (int t = 0; t < 600; t++) {
+      const uint64_t ab = t < 64 ? (t < 32 ? uint64_t(t) : s.nblocks - 1 - uint64_t(t - 32) % s.nblocks)
+                                 : rng() % s.nblocks;
+      const Z80S a = decode(ab, s), b = bdec_state(d, ab, rep_values(), rep_sp());
+      if (a.a != b.a || a.f != b.f || a.b != b.b || a.c != b.c || a.d != b.d || a.e != b.e || a.h != b.h ||
+          a.l != b.l || a.sp != b.sp || a.m != b.m) {
+        std::printf("block decoder differs: reads %03x block %llu\n", reads, (unsigned long long)ab);
+        return false;
+      }
+      n++;
+    }
+  }
+  return n > 0;
+}
+
 uint32_t* reg_planes(ZB& z, int r) {
   switch (r) {
     case 0: return z.b;
@@ -148,6 +176,7 @@ uint32_t diff_mask(const ZB& x, const ZB& y, uint32_t keepF) {
 
 int main() {
   orc::Init();
+  if (!check_bdec()) return 1;
   std::mt19937_64 rng(2027);
   // 1. layout: every read mask over B..L, M, SP (A and F do not shape the
   // sweep), sampled groups of each shape

@@ -620,6 +620,59 @@ Z80_HD void zb4_step(ZB4& z, uint32_t op, uint32_t imm) {
   }
 }
 
+// Block decoding of an ExhaustiveCheck sweep (pkg/search/verifier.go:
+// 428-612), set up once per pair.  Block index fields, fastest first: SP (4
+// bits, reduced sweeps that read SP), the swept registers from the last to
+// the first (8 bits each in a full sweep, 5 bits indexing the representative
+// values in a reduced one), carry.  Packed into two words so that it costs
+// the sweep kernels two registers: register r's field position (6 bits, r =
+// B, C, D, E, H, L, M; five in lo, two in hi), then in hi the swept
+// registers (bit r), the SP field, the reduced sweep and the carry's
+// position.  Unswept registers start at 0.
+struct BDec {
+  uint32_t lo, hi;
+};
+Z80_HD BDec bdec_make(bool spw, bool reduced, int nx, int fw, const int (&slot)[7]) {
+  const int base = spw ? 4 : 0;
+  uint32_t sh[7] = {0, 0, 0, 0, 0, 0, 0}, on = 0;
+  for (int r = 0; r < 7; r++) {
+    if (slot[r] < 0) continue;
+    sh[r] = uint32_t(base + (nx - 1 - slot[r]) * fw);
+    on |= 1u << r;
+  }
+  BDec d;
+  d.lo = sh[0] | sh[1] << 6 | sh[2] << 12 | sh[3] << 18 | sh[4] << 24;
+  d.hi = sh[5] | sh[6] << 6 | on << 12 | (spw ? 1u : 0u) << 19 | (reduced ? 1u : 0u) << 20 |
+         uint32_t(base + nx * fw) << 21;
+  return d;
+}
+// The initial state of block ab (A = 0); rep / repsp: the 32 representative
+// register values and the 16 SP values.
+Z80_HD Z80S bdec_state(const BDec& d, unsigned long long ab, const uint8_t* rep, const uint16_t* repsp) {
+  const bool reduced = (d.hi >> 20) & 1u;
+  uint32_t v[7];
+  for (int r = 0; r < 7; r++) {
+    v[r] = 0u;
+    if ((d.hi >> (12 + r)) & 1u) {
+      const uint32_t sh = (r < 5 ? d.lo >> (6 * r) : d.hi >> (6 * (r - 5))) & 63u;
+      const uint32_t x = uint32_t(ab >> sh) & (reduced ? 31u : 255u);
+      v[r] = reduced ? uint32_t(rep[x]) : x;
+    }
+  }
+  Z80S s;
+  s.a = 0;
+  s.f = uint32_t(ab >> (d.hi >> 21)) & 1u;
+  s.b = v[0];
+  s.c = v[1];
+  s.d = v[2];
+  s.e = v[3];
+  s.h = v[4];
+  s.l = v[5];
+  s.m = v[6];
+  s.sp = ((d.hi >> 19) & 1u) ? uint32_t(repsp[uint32_t(ab) & 15u]) : 0u;
+  return s;
+}
+
 // Block decoding for compact pairs.  A compact pair reads at most two
 // registers and neither SP nor the memory byte, so its sweep is a full one:
 // block index = carry above nx 8-bit fields, the last swept register in the

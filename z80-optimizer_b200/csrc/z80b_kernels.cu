@@ -566,11 +566,13 @@ __global__ void k_pairs_from_survivors(DevTargets T, DevPool P, QCOut q, const u
 // K = states per lane per dispatch ("vectors per lane").  One warp
 // iteration covers 32*K values of A; an A-block (256 states) takes 8/K
 // iterations.
-// Initial register values of A-block ab (everything but A and F's carry):
-// block index fields fastest first: SP (reduced sweeps), the swept registers
-// from the last to the first, carry.  UNIFORM selects the __constant__
-// tables (the index is the same in every lane) or their global copies
-// (lane-dependent index).
+// Initial register values of A-block ab (everything but A and F's carry),
+// decoded field by field from the sweep shape: the same values as
+// bdec_state, in a form that keeps the bit-sliced A-independent unit within
+// its registers.  Block index fields fastest first: SP (reduced sweeps), the
+// swept registers from the last to the first, carry.  UNIFORM selects the
+// __constant__ tables (the index is the same in every lane) or their global
+// copies (lane-dependent index).
 template <bool UNIFORM>
 __device__ __forceinline__ void decode_block(unsigned long long ab, bool spw, bool reduced, int nx, int fw,
                                              const int (&slot)[7], Z80S& init) {
@@ -709,14 +711,12 @@ __device__ __forceinline__ uint32_t zb_diff(const ZB& z, const uint32_t* s, uint
 // One unit (4 A-blocks) of an A-dependent sweep, bit-sliced: lane l takes
 // block unit*4 + l/8 and A = (l%8)*32 .. +31; the candidate's outputs wait in
 // shared memory while the target runs.  One dispatch site for both programs.
-__device__ __forceinline__ bool bits_unit(unsigned long long u, unsigned long long nblocks, bool spw, bool reduced,
-                                          int nx, int fw, const int (&slot)[7], uint32_t pw, int tl, int cl,
-                                          uint32_t keepF, uint32_t keepR, uint32_t* sm) {
+__device__ __forceinline__ bool bits_unit(unsigned long long u, unsigned long long nblocks, const BDec& bd,
+                                          uint32_t pw, int tl, int cl, uint32_t keepF, uint32_t keepR, uint32_t* sm) {
   const unsigned lane = lane_id();
   const unsigned long long blk = u * kBitsBlocks + (lane >> 3);
   const bool valid = blk < nblocks;
-  Z80S x;
-  decode_block<false>(valid ? blk : u * kBitsBlocks, spw, reduced, nx, fw, slot, x);
+  const Z80S x = bdec_state(bd, valid ? blk : u * kBitsBlocks, g_rep, g_repsp);
   const uint32_t a0 = (lane & 7u) * 32u;
   ZB z;
 #pragma unroll 1
@@ -971,13 +971,9 @@ __device__ __forceinline__ bool cxbits_unit(unsigned long long u, unsigned long 
 // A-independent sweep kernel; kept out of line (that kernel compiles without
 // register spills at every K this way).
 template <int K>
-__device__ __noinline__ bool xindep_unit(unsigned long long first, unsigned long long nb, bool spw, bool reduced,
-                                         int nx, int fw, const int* slotp, uint32_t pw, int tl, int cl,
-                                         uint32_t keep0, uint32_t keep1) {
+__device__ __noinline__ bool xindep_unit(unsigned long long first, unsigned long long nb, const BDec bd, uint32_t pw,
+                                         int tl, int cl, uint32_t keep0, uint32_t keep1) {
   const unsigned lane = lane_id();
-  int slot[7];
-#pragma unroll
-  for (int r = 0; r < 7; r++) slot[r] = slotp[r];
   bool bad = false;
 #pragma unroll 1
   for (uint32_t i = 0; i < 8u / K; i++) {
@@ -987,8 +983,7 @@ __device__ __noinline__ bool xindep_unit(unsigned long long first, unsigned long
     for (int q = 0; q < K; q++) {
       const uint32_t sl = (i * K + q) * 32u + lane;
       valid[q] = (sl >> 1) < nb;
-      Z80S x;
-      decode_block<false>(valid[q] ? first + (sl >> 1) : first, spw, reduced, nx, fw, slot, x);
+      Z80S x = bdec_state(bd, valid[q] ? first + (sl >> 1) : first, g_rep, g_repsp);
       x.a = sl & 1u;
       z_pack(x, W[q]);
     }
@@ -1069,6 +1064,7 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : 1)
 #pragma unroll
       for (int r = 0; r < 7; r++) slot[r] = (ext & bits[r]) ? k2++ : -1;
     }
+    const BDec bd = bdec_make(spw, reduced, nx, fw, slot);
     // compared bytes of the packed words (A F B C / D E H L / SP M)
     const uint32_t keep0 = 0xFFu | (uint32_t(pr.keepF) << 8) | ((pr.keepR & 1u) ? 0xFF0000u : 0u) |
                            ((pr.keepR & 2u) ? 0xFF000000u : 0u);
@@ -1124,8 +1120,7 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : 1)
       for (unsigned long long u = u0; u < u1; u++) {
         const unsigned long long first = u * kBitsBlocks;
         const unsigned long long nb = (pr.nblocks - first < kBitsBlocks) ? pr.nblocks - first : kBitsBlocks;
-        bad = bits_unit(u, pr.nblocks, spw, reduced, nx, fw, slot, pw, int(tl), int(cl), pr.keepF, pr.keepR, sm) ||
-              bad;
+        bad = bits_unit(u, pr.nblocks, bd, pw, int(tl), int(cl), pr.keepF, pr.keepR, sm) || bad;
         my_states += 256ull * nb;
         my_eval += 256ull * nb;
         if (__any_sync(kFull, bad)) break;
@@ -1159,7 +1154,7 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : 1)
       for (unsigned long long u = u0; u < u1; u++) {
         const unsigned long long first = u * kUnitBlocks;
         const unsigned long long nb = (pr.nblocks - first < kUnitBlocks) ? pr.nblocks - first : kUnitBlocks;
-        bad = xindep_unit<K>(first, nb, spw, reduced, nx, fw, slot, pw, int(tl), int(cl), keep0, keep1) || bad;
+        bad = xindep_unit<K>(first, nb, bd, pw, int(tl), int(cl), keep0, keep1) || bad;
         my_states += 256ull * nb;
         my_eval += 2ull * nb;
         if (__any_sync(kFull, bad)) break;
