@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cstdlib>
 #include <cstdarg>
@@ -445,6 +446,23 @@ int ensure_qc_index(z80b_ctx* ctx, PoolBufs& P, uint32_t w2mask) {
   return Z80B_OK;
 }
 
+// Runs fn(lo, hi) over [0, n) split into contiguous parts on up to 16 host
+// threads (in the calling thread alone below 2^16 items).
+template <class F>
+void host_parallel(size_t n, F fn) {
+  constexpr size_t kMinPart = size_t(1) << 16;
+  size_t parts = std::min<size_t>(16, std::max(1u, std::thread::hardware_concurrency()));
+  parts = std::min(parts, n / kMinPart);
+  if (parts <= 1) {
+    fn(size_t(0), n);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (size_t k = 1; k < parts; k++) th.emplace_back(fn, n * k / parts, n * (k + 1) / parts);
+  fn(size_t(0), n / parts);
+  for (auto& t : th) t.join();
+}
+
 int validate_job(z80b_ctx* ctx, const z80b_job* job) {
   if (!job) return fail(ctx, Z80B_EINVAL, "job is null");
   if (job->n_targets && !job->targets) return fail(ctx, Z80B_EINVAL, "targets is null");
@@ -459,14 +477,31 @@ int validate_job(z80b_ctx* ctx, const z80b_job* job) {
   if ((job->flags & Z80B_JOB_NO_EXHAUSTIVE) && job->mode != Z80B_MODE_ALL)
     return fail(ctx, Z80B_EINVAL, "Z80B_JOB_NO_EXHAUSTIVE needs Z80B_MODE_ALL");
   if (job->global_dead_flags > 0xFF) return fail(ctx, Z80B_EINVAL, "dead flags > 0xFF");
-  for (uint32_t i = 0; i < job->n_targets; i++) {
-    uint32_t l = job->target_lens ? job->target_lens[i] : job->target_len;
+  // the first bad target (the reported one is the lowest index, as a
+  // serial scan would find); the scan runs on several host threads
+  std::atomic<uint64_t> first_bad{~0ull};
+  host_parallel(job->n_targets, [&](size_t lo, size_t hi) {
+    for (size_t i = lo; i < hi; i++) {
+      const uint32_t l = job->target_lens ? job->target_lens[i] : job->target_len;
+      const bool ok = l >= 1 && l <= uint32_t(kMaxSeq) && l <= job->target_stride &&
+                      valid_seq(job->targets + i * job->target_stride, int(l)) &&
+                      !(job->dead_regs && (job->dead_regs[i] & ~0x3Fu));
+      if (!ok) {
+        uint64_t cur = first_bad.load();
+        while (i < cur && !first_bad.compare_exchange_weak(cur, i)) {
+        }
+        return;
+      }
+    }
+  });
+  if (first_bad.load() != ~0ull) {
+    const uint32_t i = uint32_t(first_bad.load());
+    const uint32_t l = job->target_lens ? job->target_lens[i] : job->target_len;
     if (l < 1 || l > uint32_t(kMaxSeq) || l > job->target_stride)
       return fail(ctx, Z80B_EINVAL, "target %u: length %u outside 1..%d", i, l, kMaxSeq);
     if (!valid_seq(job->targets + (size_t)i * job->target_stride, int(l)))
       return fail(ctx, Z80B_EINVAL, "target %u: opcode > 454", i);
-    if (job->dead_regs && (job->dead_regs[i] & ~0x3Fu))
-      return fail(ctx, Z80B_EINVAL, "target %u: dead_regs uses bits above B..L", i);
+    return fail(ctx, Z80B_EINVAL, "target %u: dead_regs uses bits above B..L", i);
   }
   return Z80B_OK;
 }
@@ -985,25 +1020,27 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
 void to_rules(z80b_ctx* ctx, const std::vector<DevRule>& dr, const uint32_t* targets, const uint8_t* tlens,
               uint32_t tlen, uint32_t stride, uint32_t mode, uint32_t tindex_offset, z80b_rule* out) {
   const PoolBufs& P = (mode == Z80B_MODE_ALL) ? (ctx->loaded.loaded ? ctx->loaded : ctx->firstop) : ctx->pool8;
-  for (size_t i = 0; i < dr.size(); i++) {
-    const DevRule& r = dr[i];
-    z80b_rule& o = out[i];
-    std::memset(&o, 0, sizeof o);
-    const uint32_t* t = targets + (size_t)r.target * stride;
-    int tl = tlens ? tlens[r.target] : int(tlen);
-    const PoolBufs& PC = (r.clen == 2) ? ctx->pairpool->pool : P;
-    const uint32_t* c = PC.host_insn.data() + (size_t)r.cand * PC.len;
-    int cl = int(PC.len);
-    o.src_len = tl;
-    o.rep_len = cl;
-    for (int k = 0; k < tl; k++) o.src[k] = t[k];
-    for (int k = 0; k < cl; k++) o.rep[k] = c[k];
-    o.bytes_saved = seq_bytes(t, tl) - seq_bytes(c, cl);
-    o.cycles_saved = seq_tstates(t, tl) - seq_tstates(c, cl);
-    o.dead_flags = (r.kind == 0) ? 0 : int(r.diff & 0xFFu);
-    o.dead_regs = (r.kind == 0) ? 0 : int(r.diff >> 8);
-    o.target_index = int(r.target + tindex_offset);
-  }
+  host_parallel(dr.size(), [&](size_t lo, size_t hi) {
+    for (size_t i = lo; i < hi; i++) {
+      const DevRule& r = dr[i];
+      z80b_rule& o = out[i];
+      std::memset(&o, 0, sizeof o);
+      const uint32_t* t = targets + (size_t)r.target * stride;
+      int tl = tlens ? tlens[r.target] : int(tlen);
+      const PoolBufs& PC = (r.clen == 2) ? ctx->pairpool->pool : P;
+      const uint32_t* c = PC.host_insn.data() + (size_t)r.cand * PC.len;
+      int cl = int(PC.len);
+      o.src_len = tl;
+      o.rep_len = cl;
+      for (int k = 0; k < tl; k++) o.src[k] = t[k];
+      for (int k = 0; k < cl; k++) o.rep[k] = c[k];
+      o.bytes_saved = seq_bytes(t, tl) - seq_bytes(c, cl);
+      o.cycles_saved = seq_tstates(t, tl) - seq_tstates(c, cl);
+      o.dead_flags = (r.kind == 0) ? 0 : int(r.diff & 0xFFu);
+      o.dead_regs = (r.kind == 0) ? 0 : int(r.diff >> 8);
+      o.target_index = int(r.target + tindex_offset);
+    }
+  });
 }
 
 int Reporter::update(z80b_ctx* ctx, uint32_t n, const Lanes& L, const Lanes& L2, uint32_t max_cand, bool phase2,
