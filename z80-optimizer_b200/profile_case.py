@@ -87,7 +87,8 @@ def main():
         t0 = time.perf_counter()
         rules, st = ctx.run_job(job)
         print(f"step {i}: {len(rules)} rules, {st.checks} checks, {st.exhaustive_pairs} exhaustive pairs, "
-              f"{st.exhaustive_states:.4e} states, {st.launches} launches, device {st.device_ms:.2f} ms "
+              f"{st.exhaustive_states:.4e} states ({st.exhaustive_evaluated:.4e} evaluated), {st.rounds} rounds, "
+              f"{st.launches} launches, device {st.device_ms:.2f} ms "
               f"(qc {st.qc_ms:.2f}, exhaustive {st.exh_ms:.2f}), wall {1e3 * (time.perf_counter() - t0):.1f} ms",
               flush=True)
     ctx.close()
