@@ -129,7 +129,9 @@ def test_compact_sweep_keeps_parity(ctx, O, compact):
 def test_device_rounds_equal_host_rounds(ctx, case):
     """The first-found rounds driven on the device (one CUDA graph, a WHILE
     node over build / scan / sweep / resolve) and driven from the host give
-    the same rules, counters, rounds and swept pairs."""
+    the same rules, counters, rounds and swept pairs.  (The count of swept
+    states is not compared: how far other warps get into a pair's sweep
+    before they see it rejected is a matter of timing in either mode.)"""
     import workloads
     saved = ctx.get_option(z80b.OPT_GRAPH_ROUNDS)
     try:
@@ -140,8 +142,7 @@ def test_device_rounds_equal_host_rounds(ctx, case):
                 rules, st = run(ctx, fixture())
             else:
                 rules, st = ctx.search(workloads.to_lists(workloads.c2_subset(6000, seed=4)), dead_flags=0xFF)
-            res.append((dev_keys(rules), st.checked_ref, st.checks, st.rounds, st.exhaustive_pairs,
-                        st.exhaustive_states))
+            res.append((dev_keys(rules), st.checked_ref, st.checks, st.rounds, st.exhaustive_pairs))
         assert res[0] == res[1]
         assert res[0][3] > 1  # several rounds
     finally:
