@@ -217,7 +217,7 @@ int z80b_exhaustive_noalloc(int device, const uint32_t* tgt, const uint8_t* tlen
 #define Z80B_OPT_STREAM_PRIORITY 3  /* the context's stream: -1 high, 0 default, 1 low priority */
 #define Z80B_OPT_QC_INDEX 4         /* QuickCheck through the pool's bucket index: 1 (default) or 0 (scan every candidate) */
 #define Z80B_OPT_XINDEP_BITS 5      /* A-independent sweeps bit-sliced (1, default) or one state per lane slot (0) */
-#define Z80B_OPT_COMPACT_SWEEP 6    /* A-dependent pairs naming at most two of B..L on the compact-state kernel (1) or not (0, default) */
+#define Z80B_OPT_COMPACT_SWEEP 6    /* pairs naming at most two of B..L on the A/F/B/C-state kernel (1, default) or not (0) */
 #define Z80B_OPT_GRAPH_ROUNDS 7     /* first-found ExhaustiveCheck rounds driven on the device by one CUDA graph (1, default;
                                        not for z80b_search_cb, whose callbacks follow the rounds) or from the host (0) */
 int z80b_set_option(z80b_ctx* ctx, int option, int value);

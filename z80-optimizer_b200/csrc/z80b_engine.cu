@@ -175,7 +175,7 @@ struct z80b_ctx {
   int priority = 0;           // Z80B_OPT_STREAM_PRIORITY
   int qc_index = 1;           // Z80B_OPT_QC_INDEX
   int xbits = 1;              // Z80B_OPT_XINDEP_BITS
-  int compact = 0;            // Z80B_OPT_COMPACT_SWEEP
+  int compact = 1;            // Z80B_OPT_COMPACT_SWEEP
   uint32_t sweep_kernels = 0; // kSweep* bits of the sweep kernels launched since the last reset
   int graph_rounds = 1;       // Z80B_OPT_GRAPH_ROUNDS
   DBuf roundctl;              // RoundCtl of the device-driven rounds
