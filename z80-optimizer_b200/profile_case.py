@@ -42,8 +42,11 @@ def main():
                     help="QuickCheck through the pool's bucket index (1) or over every candidate (0)")
     ap.add_argument("--xindep-bits", type=int, default=1, choices=[0, 1],
                     help="A-independent sweeps bit-sliced (1) or one state per lane slot (0)")
-    ap.add_argument("--compact", type=int, default=0, choices=[0, 1],
+    ap.add_argument("--compact", type=int, default=1, choices=[0, 1],
                     help="A-dependent pairs naming at most two of B..L on the compact-state sweep kernel")
+    ap.add_argument("--graph-rounds", type=int, default=1, choices=[0, 1],
+                    help="first-found rounds driven on the device by one CUDA graph (1) or from the host (0; "
+                         "ncu profiles no kernel inside a graph with conditional nodes)")
     ap.add_argument("--case", default="c2", choices=["c2", "c3", "mulopt"])
     ap.add_argument("--pool", type=int, default=2, help="mulopt pool (Z80B_MULPOOL_*)")
     ap.add_argument("--max-len", type=int, default=9, help="mulopt: longest sequence")
@@ -64,6 +67,7 @@ def main():
         ctx.set_option(z80b.OPT_QC_INDEX, a.qc_index)
         ctx.set_option(z80b.OPT_XINDEP_BITS, a.xindep_bits)
         ctx.set_option(z80b.OPT_COMPACT_SWEEP, a.compact)
+        ctx.set_option(z80b.OPT_GRAPH_ROUNDS, a.graph_rounds)
         arr, lens, dead, dregs = workloads.c3_targets(a.targets, seed=1)
         targets = [list(map(int, arr[i, :lens[i]])) for i in range(a.targets)]
         job, keep = ctx.make_job(targets, per_target_dead=list(map(int, dead)), dead_regs=list(map(int, dregs)),
@@ -82,6 +86,7 @@ def main():
     ctx.set_option(z80b.OPT_QC_INDEX, a.qc_index)
     ctx.set_option(z80b.OPT_XINDEP_BITS, a.xindep_bits)
     ctx.set_option(z80b.OPT_COMPACT_SWEEP, a.compact)
+    ctx.set_option(z80b.OPT_GRAPH_ROUNDS, a.graph_rounds)
     job, keep = ctx.make_job(workloads.to_lists(arr), dead_flags=z80b.parse_dead_flags(a.dead_flags))
     for i in range(a.steps):
         t0 = time.perf_counter()
