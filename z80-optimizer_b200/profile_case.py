@@ -75,7 +75,9 @@ def main():
         for i in range(a.steps):
             rules, st = ctx.run_job(job)
             print(f"step {i}: {len(rules)} rules, {st.checks} checks, {st.exhaustive_pairs} exhaustive pairs, "
-                  f"{st.rounds} rounds, {st.launches} launches, device {st.device_ms:.2f} ms", flush=True)
+                  f"{st.exhaustive_states:.4e} states ({st.exhaustive_evaluated:.4e} evaluated), "
+                  f"{st.rounds} rounds, {st.launches} launches, device {st.device_ms:.2f} ms "
+                  f"(qc {st.qc_ms:.2f}, exhaustive {st.exh_ms:.2f})", flush=True)
         ctx.close()
         return 0
     arr = np.ascontiguousarray(workloads.c2_subset(a.targets, seed=a.seed) if a.targets
