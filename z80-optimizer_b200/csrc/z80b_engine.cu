@@ -157,7 +157,7 @@ struct z80b_ctx {
   Staged staged;
   // pipeline scratch
   DBuf cnt_f, cnt_m, cnt_all, base, meta, surv, sdiff, checks;
-  DBuf next, win, windiff, spec, spec2, wlen;
+  DBuf next, win, windiff, spec, spec2, wlen, wend, cdone;
   DBuf pairs, pair_src, nchunks, cbase, nchunks_x, cbase_x, nchunks_c, cbase_c, rejected, npairs, counter, states;
   DBuf rcnt, rbase, rules, checked, surv_target, midpass, flag;
   DBuf cub_tmp;
@@ -797,6 +797,8 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
     }
     CK(ctx->rejected.ensure(4 * cap));
     CK(ctx->wlen.ensure(cap));
+    CK(ctx->wend.ensure(4 * cap));
+    CK(ctx->cdone.ensure(4 * cap));
     CK(ctx->spec.ensure(2ull * n));
     CK(cudaMemsetAsync(ctx->spec.p, 0, 2ull * n, s));
     CK(cudaMemsetAsync(ctx->next.p, 0, 8ull * n, s));
@@ -810,6 +812,8 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
     R.cbase_x = ctx->cbase_x.as<unsigned long long>();
     R.rejected = ctx->rejected.as<uint32_t>();
     R.wlen = ctx->wlen.as<uint8_t>();
+    R.wend = ctx->wend.as<uint32_t>();
+    R.cdone = ctx->cdone.as<uint32_t>();
     R.cap = uint32_t(cap);
     R.npairs = ctx->npairs.as<uint32_t>();
     R.counter = ctx->counter.as<unsigned long long>();

@@ -478,7 +478,7 @@ __device__ __forceinline__ uint32_t alloc_pairs(uint32_t* counter, uint32_t w) {
 // Writes one pair of a round.
 __device__ __forceinline__ void put_pair(const RoundBuf& R, uint32_t p, const DevTargets& T, const DevPool& P,
                                          const QCOut& q, uint32_t t, uint32_t kind, uint32_t c, uint32_t src,
-                                         uint8_t wlen) {
+                                         uint8_t wlen, uint32_t wend) {
   PairRec pr;
   const uint32_t reads = q.meta[t].reads | P.reads[c];
   pr.target = t;
@@ -496,6 +496,32 @@ __device__ __forceinline__ void put_pair(const RoundBuf& R, uint32_t p, const De
   set_chunks(R, p, pr);
   R.rejected[p] = 0;
   R.wlen[p] = wlen;
+  if (R.wend) {
+    R.wend[p] = wend;
+    R.cdone[p] = 0;
+  }
+}
+
+// Lane 0, after a warp's chunk of pair p ran to its end without a mismatch:
+// counts the chunk; the warp that counts the last one of a pair that still
+// stands (its whole sweep passed) cancels the pairs after it in its survivor
+// window (rejected 0 -> 2): the first passing pair of a window wins, so
+// their sweeps cannot change the result.  A chunk with a mismatch rejects
+// the pair and is not counted, so a rejected pair never reaches its count.
+// nch = the pair's chunks.
+__device__ __forceinline__ void chunk_passed(uint32_t* rejected, const uint32_t* wend, uint32_t* cdone, uint32_t p,
+                                          uint32_t nch) {
+  __threadfence();
+  const uint32_t before = atomicAdd(&cdone[p], 1u);
+  if (before + 1u != nch) return;
+  __threadfence();
+  if (atomicAdd(&rejected[p], 0u) != 0u) return;
+  // windows hold at most 64 pairs; an unrolled, guarded run keeps a loop
+  // out of the sweep kernels' loop nest (which made them spill)
+  const uint32_t e = wend[p];
+#pragma unroll
+  for (uint32_t i = 1; i < 64; i++)
+    if (p + i < e) atomicCAS(&rejected[p + i], 0u, 2u);
 }
 
 // One round of the length-1 pass: each unresolved (target, kind) lane puts
@@ -524,7 +550,8 @@ __global__ void k_round_build(DevTargets T, DevPool P, QCOut q, Lanes L, RoundBu
     const uint32_t p0 = alloc_pairs(R.npairs, w);
     const uint32_t fit = p0 >= R.cap ? 0u : min(w, R.cap - p0);
     for (uint32_t j = 0; j < fit; j++)
-      put_pair(R, p0 + j, T, P, q, t, kind, q.surv[sbase + j], sbase + j, j == 0 ? uint8_t(fit) : uint8_t(0));
+      put_pair(R, p0 + j, T, P, q, t, kind, q.surv[sbase + j], sbase + j, j == 0 ? uint8_t(fit) : uint8_t(0),
+               p0 + fit);
   }
 }
 
@@ -1072,6 +1099,7 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : 1)
                            ((pr.keepR & 16u) ? 0xFF0000u : 0u) | ((pr.keepR & 32u) ? 0xFF000000u : 0u);
 
     bool bad = false;
+    bool stopped = false;  // left the loop on the pair's flag (rejected or cancelled elsewhere)
     if constexpr (CLS == 3) {
       // the compact state, the programs renamed onto B and C
       const uint32_t e = pr.cmap - 1u;
@@ -1094,7 +1122,10 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : 1)
           my_states += 256ull * nb;
           my_eval += 2ull * nb;
           if (__any_sync(kFull, bad)) break;
-          if (__shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0)) break;
+          if (__shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0)) {
+          stopped = true;
+          break;
+        }
         }
       } else {
         for (unsigned long long u = u0; u < u1; u++) {
@@ -1106,7 +1137,10 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : 1)
           if (__any_sync(kFull, bad)) break;
           if ((u & 15ull) == 15ull &&
               __shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0))
-            break;
+            {
+              stopped = true;
+              break;
+            }
         }
       }
     } else if constexpr (!XI) {
@@ -1126,7 +1160,10 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : 1)
         if (__any_sync(kFull, bad)) break;
         if ((u & 15ull) == 15ull &&
             __shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0))
-          break;
+          {
+            stopped = true;
+            break;
+          }
       }
     } else if constexpr (CLS == 2) {
       // Unit = 1,024 A-blocks, 32 per lane, each at A = 0 and A = 1.
@@ -1145,7 +1182,10 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : 1)
         my_states += 256ull * nb;
         my_eval += 2ull * nb;
         if (__any_sync(kFull, bad)) break;
-        if (__shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0)) break;
+        if (__shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0)) {
+          stopped = true;
+          break;
+        }
       }
     } else {
       // Unit = 128 A-blocks, each evaluated at A = 0 and A = 1: state slot s
@@ -1160,10 +1200,19 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : 1)
         if (__any_sync(kFull, bad)) break;
         if ((u & 3ull) == 3ull &&
             __shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0))
-          break;
+          {
+            stopped = true;
+            break;
+          }
       }
     }
-    if (__any_sync(kFull, bad) && lane == 0) atomicExch(&R.rejected[p], 1u);
+    const bool any_bad = __any_sync(kFull, bad);
+    if (lane == 0) {
+      if (any_bad) atomicExch(&R.rejected[p], 1u);
+      else if (!stopped && R.wend)
+        chunk_passed(R.rejected, R.wend, R.cdone, p,
+                     uint32_t((p + 1 < npairs ? cbase[p + 1] : total) - cbase[p]));
+    }
   }
   if (lane == 0 && my_states) {
     atomicAdd(R.states, my_states);
@@ -1621,7 +1670,7 @@ __global__ void k_pair_round_build(DevTargets T, DevPool P, QCOut q1, Lanes L2, 
   const uint32_t fit = p0 >= R.cap ? 0u : min(w, R.cap - p0);
   for (uint32_t j = 0; j < fit; j++)
     put_pair(R, p0 + j, T, P, q1, idx >> 1, idx & 1u, ps.surv[sbase + j], sbase + j,
-             j == 0 ? uint8_t(fit) : uint8_t(0));
+             j == 0 ? uint8_t(fit) : uint8_t(0), p0 + fit);
 }
 
 

@@ -74,6 +74,13 @@ struct RoundBuf {
                                    // their own class and kernel
   uint32_t* rejected;              // per pair
   uint8_t* wlen;                   // per pair: survivors in the window it heads (0: not a head)
+  // First-found windows (null for independent pairs): per pair the end
+  // (exclusive) of its survivor window, and the chunks of its sweep that
+  // finished without a mismatch.  A pair whose every chunk finished so
+  // passed; the pairs after it in its window can no longer win, and their
+  // sweeps are cancelled (rejected = 2).
+  uint32_t* wend;
+  uint32_t* cdone;
   uint32_t cap;                    // pair slots of the buffers
   uint32_t* npairs;                // device counter
   unsigned long long* counter;     // chunk dispensers: [0] bit-sliced, [1] A-independent, [2] compact class
