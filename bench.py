@@ -292,7 +292,8 @@ def c3_leg(ctx, z80b, workloads, args):
     # tune the sweep kernel for this workload on its first 2,000 targets
     # (longer sequences than C2's, so another setting may win); the C2
     # setting is restored after the leg
-    tuned = [z80b.OPT_EXH_LANE_STATES, z80b.OPT_EXH_CHUNK_BLOCKS, z80b.OPT_XINDEP_BITS, z80b.OPT_COMPACT_SWEEP]
+    tuned = [z80b.OPT_EXH_LANE_STATES, z80b.OPT_EXH_CHUNK_BLOCKS, z80b.OPT_XINDEP_BITS, z80b.OPT_COMPACT_SWEEP,
+             z80b.OPT_WIDE_SWEEP]
     saved = [ctx.get_option(o) for o in tuned]
     tj, tkeep = job_for(0, min(2000, n), z80b.PATH_BATCHED)
     tr = ctx.autotune(tj)
@@ -513,38 +514,57 @@ def main():
     h2d = int(mine.nbytes)
     d2h = int(nr.value) * 12 + 64
 
-    # ---- roofline of the dominant kernel (ExhaustiveCheck sweep)
+    # ---- roofline of the dominant kernels (the ExhaustiveCheck sweep classes)
+    # Integer issue-bound work (no contraction, nothing per state from
+    # DRAM): peak = SMs x 4 warp-instruction issue slots per clock x the max
+    # SM clock.  The unit is one evaluated sweep state; its cost in warp
+    # instructions is fixed by an ncu capture of every sweep launch of one
+    # step of a C2 sample (roofline.json "sweep_capture": the capture's
+    # smsp__inst_executed.sum over its evaluated states), and this run's
+    # sweep time turns it into an issue rate, so frac reads as the issue-slot
+    # utilisation of the whole sweep phase at this run's speed (gaps between
+    # rounds and tails of launches included).
     rl = json.load(open(os.path.join(PKG, "roofline.json")))
+    cap = rl["sweep_capture"]
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except Exception:
         pass
     sm_mhz = peaks.get("sm_max_mhz", 1965.0)
+    exh_s = exh_ms / args.steps / 1e3
+    evaluated_step = evaluated / args.steps
+    issue_peak = rl["sms"] * rl["issue_slots_per_sm_per_clock"] * sm_mhz * 1e6
+    issued = evaluated_step * cap["warp_instructions_per_evaluated_state"]
+    achieved = issued / exh_s if exh_s else 0.0
+    # the scalar cost model (INT32 lane-ops a one-state-per-lane step of the
+    # reference would need per evaluated state): an algorithmic work rate,
+    # above 1 of the lane peak because the bit-sliced kernels step 32
+    # states per lane instruction
     per_state = 3 * rl["ops_per_emulated_insn"] + rl["ops_per_state"]  # 2-insn target + 1-insn candidate
-    # states the sweep kernel actually ran (A-independent pairs run 2 of
-    # every 256 values of A), so the fraction measures the kernel, not the
-    # states it skips
-    achieved = evaluated / args.steps * per_state / (exh_ms / args.steps / 1e3) / 1e12 if exh_ms else 0.0
-    peak = rl["sms"] * rl["int32_lanes_per_sm"] * sm_mhz * 1e6 / 1e12
-    # DRAM bytes per sweep round (its bit-sliced and A-independent kernels):
-    # the measured bytes per ExhaustiveCheck pair of an ncu capture
-    # (profiles/exhaustive_c2_traffic.txt) times this run's pairs per round;
-    # the kernels read per-pair records and sequences only
-    traffic = None
-    tf = os.path.join(ROOT, "profiles", "exhaustive_c2_traffic.txt")
-    if os.path.exists(tf) and stats_last is not None and stats_last.rounds:
-        for line in open(tf):
-            if line.startswith("dram_bytes_per_pair:"):
-                traffic = float(line.split(":")[1]) * stats_last.exhaustive_pairs / stats_last.rounds
-    roofline = {"bound": "issue", "kernel": "k_exhaustive (bit-sliced and A-independent pair kernels of a round)",
-                "achieved": achieved, "peak": peak,
-                "unit": "Tops/s (INT32 lane-ops)", "frac": achieved / peak if peak else None,
-                "traffic": traffic,
-                "peak_source": f"{rl['sms']} SMs x {rl['int32_lanes_per_sm']} INT32 lanes x "
-                               f"sm_max_mhz {sm_mhz} of MEASURED_PEAKS.json",
-                "algorithmic_ops_per_state": per_state,
-                "exhaustive_ms_per_step": exh_ms / args.steps, "qc_ms_per_step": qc_ms / args.steps}
+    scalar_rate = evaluated_step * per_state / exh_s if exh_s else 0.0
+    scalar_peak = rl["sms"] * rl["int32_lanes_per_sm"] * sm_mhz * 1e6
+    rounds = max(1, stats_last.rounds) if stats_last is not None else 1
+    pairs_step = stats_last.exhaustive_pairs if stats_last is not None else 0
+    roofline = {"bound": "issue", "kernel": "k_exhaustive (the sweep classes of a round)",
+                "achieved": achieved / 1e12, "peak": issue_peak / 1e12,
+                "unit": "T warp-instructions/s (issue slots)",
+                "frac": achieved / issue_peak if issue_peak else None,
+                # DRAM bytes of one round's sweep launches: the capture's
+                # bytes per swept pair (pair records, programs, chunk
+                # prefixes; nothing per state) x this run's pairs per round
+                "traffic": cap["dram_bytes_per_pair"] * pairs_step / rounds,
+                "traffic_unit": "DRAM bytes per sweep round (its sweep launches)",
+                "peak_source": f"{rl['sms']} SMs x {rl['issue_slots_per_sm_per_clock']} issue slots x "
+                               f"{sm_mhz:.0f} MHz ({'MEASURED_PEAKS.json' if 'sm_max_mhz' in peaks else 'nominal max SM clock'})",
+                "work_unit": f"evaluated sweep state, {cap['warp_instructions_per_evaluated_state']:.4g} warp "
+                             f"instructions each ({cap['source']})",
+                "ncu_issue_active_pct": cap["issue_active_pct"],
+                "scalar_equivalent": {"achieved": scalar_rate / 1e12, "peak": scalar_peak / 1e12,
+                                      "unit": "T INT32 lane-ops/s", "frac": scalar_rate / scalar_peak,
+                                      "ops_per_state": per_state},
+                "exhaustive_ms_per_step": exh_ms / args.steps, "qc_ms_per_step": qc_ms / args.steps,
+                "evaluated_states_per_step": evaluated_step}
 
     # ---- plain (one target per launch) vs batched on the same sample
     plain = None

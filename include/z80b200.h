@@ -220,6 +220,8 @@ int z80b_exhaustive_noalloc(int device, const uint32_t* tgt, const uint8_t* tlen
 #define Z80B_OPT_COMPACT_SWEEP 6    /* pairs naming at most two of B..L on the A/F/B/C-state kernel (1, default) or not (0) */
 #define Z80B_OPT_GRAPH_ROUNDS 7     /* first-found ExhaustiveCheck rounds driven on the device by one CUDA graph (1, default;
                                        not for z80b_search_cb, whose callbacks follow the rounds) or from the host (0) */
+#define Z80B_OPT_WIDE_SWEEP 8       /* other pairs naming at most four of B..L and not SP on the A/F/B/C/H/L/M-state
+                                       kernel (1, default) or not (0) */
 int z80b_set_option(z80b_ctx* ctx, int option, int value);
 int z80b_get_option(const z80b_ctx* ctx, int option, int* value);
 
@@ -227,7 +229,7 @@ typedef struct z80b_tune_trial {
   int xindep_bits;            /* Z80B_OPT_XINDEP_BITS of the trial */
   int lane_states;            /* Z80B_OPT_EXH_LANE_STATES (scalar A-independent kernel); 0 when bit-sliced */
   int chunk_blocks;           /* Z80B_OPT_EXH_CHUNK_BLOCKS: sweep units per work chunk */
-  int compact;                /* Z80B_OPT_COMPACT_SWEEP */
+  int compact;                /* Z80B_OPT_COMPACT_SWEEP and Z80B_OPT_WIDE_SWEEP (set together) */
   double ms;                  /* device ms of the pipeline on the sample */
   char kernels[96];           /* the sweep kernels it launched, "k_exhaustive<K,CLS>" joined by '+' */
 } z80b_tune_trial;
@@ -242,7 +244,7 @@ typedef struct z80b_tune_result {
 } z80b_tune_result;
 /* Runs the job (a representative sample) once per sweep configuration --
  * A-independent kernel (bit-sliced, or scalar with 1/2/4/8 states per lane
- * per dispatch) x units per chunk (8, 32, 128, 512) x compact kernel off/on,
+ * per dispatch) x units per chunk (8, 32, 128, 512) x compact kernels off/on,
  * 40 distinct kernel configurations -- keeps the fastest for this context
  * and reports every trial with the kernels it launched.  The rules of the
  * trials are discarded.  No counterpart in the reference (its launch shape

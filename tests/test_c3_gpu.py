@@ -98,22 +98,27 @@ def test_a_independent_sweep_kernels_keep_parity(ctx, O, xbits):
     assert st2.checked_ref == checked
 
 
-@pytest.mark.parametrize("compact", [0, 1])
-def test_compact_sweep_keeps_parity(ctx, O, compact):
-    """Z80B_OPT_COMPACT_SWEEP off and on: the C3 sample's rules and 'checked'
-    counter, and a C2 sample against the oracle, are unchanged (on: pairs
-    naming at most two of B..L, A-dependent and A-independent, run on the
-    A/F/B/C-state kernel)."""
+@pytest.mark.parametrize("compact,wide", [(0, 0), (1, 0), (0, 1), (1, 1)])
+def test_compact_sweep_keeps_parity(ctx, O, compact, wide):
+    """Z80B_OPT_COMPACT_SWEEP and Z80B_OPT_WIDE_SWEEP off and on: the C3
+    sample's rules and 'checked' counter, and a C2 sample against the
+    oracle, are unchanged (compact: pairs naming at most two of B..L,
+    A-dependent and A-independent, on the A/F/B/C-state kernel; wide: the
+    other A-dependent pairs naming at most four of B..L and not SP, on the
+    A/F/B/C/H/L/M-state kernel)."""
     import workloads
     fx = fixture()
-    old = ctx.get_option(z80b.OPT_COMPACT_SWEEP)
+    opts = [z80b.OPT_COMPACT_SWEEP, z80b.OPT_WIDE_SWEEP]
+    old = [ctx.get_option(o) for o in opts]
     ctx.set_option(z80b.OPT_COMPACT_SWEEP, compact)
+    ctx.set_option(z80b.OPT_WIDE_SWEEP, wide)
     try:
         rules, st = run(ctx, fx)
         targets = workloads.to_lists(workloads.c2_subset(3000, seed=12))
         r2, st2 = ctx.search(targets, dead_flags=0xFF)
     finally:
-        ctx.set_option(z80b.OPT_COMPACT_SWEEP, old)
+        for o, v in zip(opts, old):
+            ctx.set_option(o, v)
     got = [tuple([k[0], tuple(k[1]), tuple(k[2])] + list(k[3:])) for k in dev_keys(rules)]
     want = [tuple([r[0], tuple(r[1]), tuple(r[2])] + list(r[3:])) for r in fx["rules"]]
     assert got == want

@@ -366,12 +366,14 @@ def test_tuning_options_keep_parity(ctx, lane_states, chunk):
 def test_autotune_picks_a_valid_setting(ctx):
     targets, want = c2_fixture_slice(50000, 52000, 0xFF)
     job, keep = ctx.make_job(targets)
-    opts = [z80b.OPT_EXH_LANE_STATES, z80b.OPT_EXH_CHUNK_BLOCKS, z80b.OPT_XINDEP_BITS, z80b.OPT_COMPACT_SWEEP]
+    opts = [z80b.OPT_EXH_LANE_STATES, z80b.OPT_EXH_CHUNK_BLOCKS, z80b.OPT_XINDEP_BITS, z80b.OPT_COMPACT_SWEEP,
+            z80b.OPT_WIDE_SWEEP]
     saved = [ctx.get_option(o) for o in opts]
     try:
         r = ctx.autotune(job)
         assert r.lane_states in (1, 2, 4, 8) and r.chunk_blocks in (8, 32, 128, 512)
-        assert [ctx.get_option(o) for o in opts] == [r.lane_states, r.chunk_blocks, r.xindep_bits, r.compact]
+        assert [ctx.get_option(o) for o in opts] == [r.lane_states, r.chunk_blocks, r.xindep_bits, r.compact,
+                                                      r.compact]
         trials = r.trial_list()
         assert len(trials) == 40 and all(t["ms"] > 0 for t in trials)
         # every cell is a distinct kernel configuration, and names what it ran
@@ -385,7 +387,7 @@ def test_autotune_picks_a_valid_setting(ctx):
                 assert "k_exhaustive<1,2>" not in t["kernels"], t
                 assert all(k not in t["kernels"] for k in scalar if k != f"k_exhaustive<{t['lane_states']},1>"), t
             if t["compact"] == 0:
-                assert "k_exhaustive<1,3>" not in t["kernels"], t
+                assert "k_exhaustive<1,3>" not in t["kernels"] and "k_exhaustive<1,4>" not in t["kernels"], t
         assert any("k_exhaustive<1,3>" in t["kernels"] for t in trials if t["compact"])
         # the chosen setting keeps parity
         rules, st = ctx.search(targets, dead_flags=0xFF)

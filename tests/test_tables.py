@@ -140,3 +140,21 @@ def test_compact_state_mapping_against_oracle(tmp_path):
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.startswith("OK")
+
+
+def test_wide_state_against_oracle(tmp_path):
+    """The wide compact state (A, F, B, C, H, L, M): its step equals the full
+    bit-sliced step on every opcode it holds, the device tables rename as
+    wide_map does, and the wide sweep unit with its block decoding gives the
+    oracle's ExhaustiveCheck verdict (dead flags and registers) for pairs
+    the A/F/B/C state does not take, memory and reduced sweeps included."""
+    import subprocess
+    exe = tmp_path / "wide_check"
+    srcs = [os.path.join(ROOT, "tests", "native", "wide_check.cpp"),
+            os.path.join(ROOT, "z80-optimizer_b200", "csrc", "z80_tables.cpp"),
+            os.path.join(ROOT, "oracle", "z80_oracle_isa_cpu.cpp"),
+            os.path.join(ROOT, "oracle", "z80_oracle_search.cpp")]
+    subprocess.run(["g++", "-O2", "-std=c++17", "-o", str(exe)] + srcs + ["-lpthread"], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.startswith("OK")

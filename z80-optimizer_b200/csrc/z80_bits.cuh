@@ -282,56 +282,51 @@ Z80_HD void zb_incsp(uint32_t (&sp)[16], bool dec) {
     c = (dec ? ~t : t) & c;
   }
 }
-// HL + v (+ carry) / HL - v - carry over 16 planes; kind 0 ADD, 1 ADC, 2 SBC.
+// HL + v (+ carry) / HL - v - carry over 16 planes, in place; kind 0 ADD,
+// 1 ADC, 2 SBC.  v is given as its low and high byte planes (vlo, vhi),
+// which may be HL's own: bit i of both operands is read before bit i of HL
+// is written.
 template <class ZT>
-Z80_HD void zb_hl16(ZT& z, const uint32_t (&v)[16], int kind) {
-  uint32_t x[16], y[16], r[16];
-  ZB_UNROLL for (int i = 0; i < 8; i++) {
-    x[i] = z.l[i];
-    x[i + 8] = z.h[i];
-  }
-  ZB_UNROLL for (int i = 0; i < 16; i++) y[i] = kind == 2 ? ~v[i] : v[i];
-  uint32_t c = kind == 0 ? 0u : (kind == 1 ? z.f[0] : ~z.f[0]), c12 = 0;
+Z80_HD void zb_hl16(ZT& z, const uint32_t* vlo, const uint32_t* vhi, int kind) {
+  uint32_t c = kind == 0 ? 0u : (kind == 1 ? z.f[0] : ~z.f[0]), c12 = 0, nz = 0, x15 = 0, v15 = 0;
   ZB_UNROLL for (int i = 0; i < 16; i++) {
+    uint32_t& xr = i < 8 ? z.l[i] : z.h[i - 8];
+    const uint32_t vi = i < 8 ? vlo[i] : vhi[i - 8];
+    const uint32_t x = xr, y = kind == 2 ? ~vi : vi;
     if (i == 12) c12 = c;
-    r[i] = x[i] ^ y[i] ^ c;
-    c = zb_maj(x[i], y[i], c);
+    if (i == 15) {
+      x15 = x;
+      v15 = vi;
+    }
+    const uint32_t r = x ^ y ^ c;
+    c = zb_maj(x, y, c);
+    xr = r;
+    nz |= r;
   }
-  ZB_UNROLL for (int i = 0; i < 8; i++) {
-    z.l[i] = r[i];
-    z.h[i] = r[i + 8];
-  }
+  const uint32_t r15 = z.h[7];
   if (kind == 0) {
     z.f[0] = c;
     z.f[1] = 0;
-    z.f[3] = r[11];
+    z.f[3] = z.h[3];
     z.f[4] = c12;
-    z.f[5] = r[13];
+    z.f[5] = z.h[5];
     return;
   }
-  uint32_t nz = 0;
-  ZB_UNROLL for (int i = 0; i < 16; i++) nz |= r[i];
   if (kind == 1) {
     z.f[0] = c;
     z.f[1] = 0;
-    z.f[2] = (x[15] ^ r[15]) & (v[15] ^ r[15]);
+    z.f[2] = (x15 ^ r15) & (v15 ^ r15);
     z.f[4] = c12;
   } else {
     z.f[0] = ~c;
     z.f[1] = kZBOnes;
-    z.f[2] = (x[15] ^ v[15]) & (x[15] ^ r[15]);
+    z.f[2] = (x15 ^ v15) & (x15 ^ r15);
     z.f[4] = ~c12;
   }
-  z.f[3] = r[11];
-  z.f[5] = r[13];
+  z.f[3] = z.h[3];
+  z.f[5] = z.h[5];
   z.f[6] = ~nz;
-  z.f[7] = r[15];
-}
-Z80_HD void zb_pair(uint32_t (&v)[16], const uint32_t (&hi)[8], const uint32_t (&lo)[8]) {
-  ZB_UNROLL for (int i = 0; i < 8; i++) {
-    v[i] = lo[i];
-    v[i + 8] = hi[i];
-  }
+  z.f[7] = r15;
 }
 
 // Register families in the enum's orders (as z80_exec.cuh's Z80B_R7 / Z80B_S7).
@@ -422,7 +417,6 @@ Z80_HD bool zb_acc_step(ZT& z, uint32_t op) {
 template <class ZT>
 Z80_HD void zb_step(ZT& z, uint32_t op, uint32_t imm) {
   uint32_t t8[8];
-  uint32_t t16[16];
   switch (op) {
     ZB_S7(ZB_LDA, LD_A_B)
     ZB_R7(ZB_LDB, LD_B_A)
@@ -472,10 +466,10 @@ Z80_HD void zb_step(ZT& z, uint32_t op, uint32_t imm) {
     case DEC_DE: zb_inc16(z.d, z.e, true); break;
     case DEC_HL: zb_inc16(z.h, z.l, true); break;
     case DEC_SP: zb_incsp(z.sp, true); break;
-    case ADD_HL_BC: zb_pair(t16, z.b, z.c); zb_hl16(z, t16, 0); break;
-    case ADD_HL_DE: zb_pair(t16, z.d, z.e); zb_hl16(z, t16, 0); break;
-    case ADD_HL_HL: zb_pair(t16, z.h, z.l); zb_hl16(z, t16, 0); break;
-    case ADD_HL_SP: for (int i = 0; i < 16; i++) t16[i] = z.sp[i]; zb_hl16(z, t16, 0); break;
+    case ADD_HL_BC: zb_hl16(z, z.c, z.b, 0); break;
+    case ADD_HL_DE: zb_hl16(z, z.e, z.d, 0); break;
+    case ADD_HL_HL: zb_hl16(z, z.l, z.h, 0); break;
+    case ADD_HL_SP: zb_hl16(z, z.sp, z.sp + 8, 0); break;
     case EX_DE_HL:
       for (int i = 0; i < 8; i++) {
         const uint32_t dd = z.d[i], ee = z.e[i];
@@ -490,14 +484,14 @@ Z80_HD void zb_step(ZT& z, uint32_t op, uint32_t imm) {
     case LD_DE_NN: zb_set8(z.d, (imm >> 8) & 0xFFu); zb_set8(z.e, imm & 0xFFu); break;
     case LD_HL_NN: zb_set8(z.h, (imm >> 8) & 0xFFu); zb_set8(z.l, imm & 0xFFu); break;
     case LD_SP_NN: for (int i = 0; i < 16; i++) z.sp[i] = ((imm >> i) & 1u) ? kZBOnes : 0u; break;
-    case ADC_HL_BC: zb_pair(t16, z.b, z.c); zb_hl16(z, t16, 1); break;
-    case ADC_HL_DE: zb_pair(t16, z.d, z.e); zb_hl16(z, t16, 1); break;
-    case ADC_HL_HL: zb_pair(t16, z.h, z.l); zb_hl16(z, t16, 1); break;
-    case ADC_HL_SP: for (int i = 0; i < 16; i++) t16[i] = z.sp[i]; zb_hl16(z, t16, 1); break;
-    case SBC_HL_BC: zb_pair(t16, z.b, z.c); zb_hl16(z, t16, 2); break;
-    case SBC_HL_DE: zb_pair(t16, z.d, z.e); zb_hl16(z, t16, 2); break;
-    case SBC_HL_HL: zb_pair(t16, z.h, z.l); zb_hl16(z, t16, 2); break;
-    case SBC_HL_SP: for (int i = 0; i < 16; i++) t16[i] = z.sp[i]; zb_hl16(z, t16, 2); break;
+    case ADC_HL_BC: zb_hl16(z, z.c, z.b, 1); break;
+    case ADC_HL_DE: zb_hl16(z, z.e, z.d, 1); break;
+    case ADC_HL_HL: zb_hl16(z, z.l, z.h, 1); break;
+    case ADC_HL_SP: zb_hl16(z, z.sp, z.sp + 8, 1); break;
+    case SBC_HL_BC: zb_hl16(z, z.c, z.b, 2); break;
+    case SBC_HL_DE: zb_hl16(z, z.e, z.d, 2); break;
+    case SBC_HL_HL: zb_hl16(z, z.l, z.h, 2); break;
+    case SBC_HL_SP: zb_hl16(z, z.sp, z.sp + 8, 2); break;
     // memory ops on the single byte M (exec.go:883-1028)
     case LD_A_HLI: zb_copy8(z.a, z.m); break;
     case LD_B_HLI: zb_copy8(z.b, z.m); break;
@@ -620,6 +614,130 @@ Z80_HD void zb4_step(ZB4& z, uint32_t op, uint32_t imm) {
   }
 }
 
+// The wide compact state: A, F, the register pairs BC and HL and the memory
+// byte.  A wide program (a pair's instructions renamed by wide_map) names no
+// register but B, C, H and L and never SP; it may use the memory byte.
+struct ZBW {
+  uint32_t a[8], f[8], b[8], c[8], h[8], l[8], m[8];
+};
+#define ZBW_R(M, base) M((base) + 0, a) M((base) + 1, b) M((base) + 2, c) M((base) + 5, h) M((base) + 6, l)
+#define ZBW_S(M, base) M((base) + 0, b) M((base) + 1, c) M((base) + 4, h) M((base) + 5, l) M((base) + 6, a)
+
+// The step on ZBW: the cases of zb_step for every instruction that names no
+// register but A, F, B, C, H, L (and possibly the memory byte) and not SP;
+// any other opcode leaves the state unchanged and must not occur.
+Z80_HD void zbw_step(ZBW& z, uint32_t op, uint32_t imm) {
+  uint32_t t8[8];
+  switch (op) {
+    ZBW_S(ZB_LDA, LD_A_B)
+    ZBW_R(ZB_LDB, LD_B_A)
+    ZBW_R(ZB_LDC, LD_C_A)
+    ZBW_R(ZB_LDH, LD_H_A)
+    ZBW_R(ZB_LDL, LD_L_A)
+    ZBW_R(ZB_LDN, LD_A_N)
+    ZBW_S(ZB_ADD, ADD_A_B)
+    case ADD_A_N: zb_set8(t8, imm & 0xFFu); zb_add(z, t8, 0u); break;
+    ZBW_S(ZB_ADC, ADC_A_B)
+    case ADC_A_N: zb_set8(t8, imm & 0xFFu); zb_add(z, t8, z.f[0]); break;
+    ZBW_S(ZB_SUB, SUB_B)
+    case SUB_N: zb_set8(t8, imm & 0xFFu); zb_sub(z, t8, 0u); break;
+    ZBW_S(ZB_SBC, SBC_A_B)
+    case SBC_A_N: zb_set8(t8, imm & 0xFFu); zb_sub(z, t8, z.f[0]); break;
+    ZBW_S(ZB_AND, AND_B)
+    case AND_N: zb_set8(t8, imm & 0xFFu); zb_and(z, t8); break;
+    ZBW_S(ZB_XOR, XOR_B)
+    case XOR_N: zb_set8(t8, imm & 0xFFu); zb_xor(z, t8); break;
+    ZBW_S(ZB_OR, OR_B)
+    case OR_N: zb_set8(t8, imm & 0xFFu); zb_or(z, t8); break;
+    ZBW_S(ZB_CP, CP_B)
+    case CP_N: zb_set8(t8, imm & 0xFFu); zb_cp(z, t8); break;
+    ZBW_R(ZB_INC, INC_A)
+    ZBW_R(ZB_DEC, DEC_A)
+    ZBW_R(ZB_RLC, RLC_A)
+    ZBW_R(ZB_RRC, RRC_A)
+    ZBW_R(ZB_RL, RL_A)
+    ZBW_R(ZB_RR, RR_A)
+    ZBW_R(ZB_SLA, SLA_A)
+    ZBW_R(ZB_SRA, SRA_A)
+    ZBW_R(ZB_SRL, SRL_A)
+    ZBW_R(ZB_SLL, SLL_A)
+    ZBW_R(ZB_BIT, BIT_0_A) ZBW_R(ZB_BIT, BIT_1_A) ZBW_R(ZB_BIT, BIT_2_A) ZBW_R(ZB_BIT, BIT_3_A)
+    ZBW_R(ZB_BIT, BIT_4_A) ZBW_R(ZB_BIT, BIT_5_A) ZBW_R(ZB_BIT, BIT_6_A) ZBW_R(ZB_BIT, BIT_7_A)
+    ZBW_R(ZB_RES, RES_0_A) ZBW_R(ZB_RES, RES_1_A) ZBW_R(ZB_RES, RES_2_A) ZBW_R(ZB_RES, RES_3_A)
+    ZBW_R(ZB_RES, RES_4_A) ZBW_R(ZB_RES, RES_5_A) ZBW_R(ZB_RES, RES_6_A) ZBW_R(ZB_RES, RES_7_A)
+    ZBW_R(ZB_SET, SET_0_A) ZBW_R(ZB_SET, SET_1_A) ZBW_R(ZB_SET, SET_2_A) ZBW_R(ZB_SET, SET_3_A)
+    ZBW_R(ZB_SET, SET_4_A) ZBW_R(ZB_SET, SET_5_A) ZBW_R(ZB_SET, SET_6_A) ZBW_R(ZB_SET, SET_7_A)
+    case INC_BC: zb_inc16(z.b, z.c, false); break;
+    case INC_HL: zb_inc16(z.h, z.l, false); break;
+    case DEC_BC: zb_inc16(z.b, z.c, true); break;
+    case DEC_HL: zb_inc16(z.h, z.l, true); break;
+    case ADD_HL_BC: zb_hl16(z, z.c, z.b, 0); break;
+    case ADD_HL_HL: zb_hl16(z, z.l, z.h, 0); break;
+    case LD_BC_NN: zb_set8(z.b, (imm >> 8) & 0xFFu); zb_set8(z.c, imm & 0xFFu); break;
+    case LD_HL_NN: zb_set8(z.h, (imm >> 8) & 0xFFu); zb_set8(z.l, imm & 0xFFu); break;
+    case ADC_HL_BC: zb_hl16(z, z.c, z.b, 1); break;
+    case ADC_HL_HL: zb_hl16(z, z.l, z.h, 1); break;
+    case SBC_HL_BC: zb_hl16(z, z.c, z.b, 2); break;
+    case SBC_HL_HL: zb_hl16(z, z.l, z.h, 2); break;
+    case LD_A_HLI: zb_copy8(z.a, z.m); break;
+    case LD_B_HLI: zb_copy8(z.b, z.m); break;
+    case LD_C_HLI: zb_copy8(z.c, z.m); break;
+    case LD_H_HLI: zb_copy8(z.h, z.m); break;
+    case LD_L_HLI: zb_copy8(z.l, z.m); break;
+    case LD_HLI_A: zb_copy8(z.m, z.a); break;
+    case LD_HLI_B: zb_copy8(z.m, z.b); break;
+    case LD_HLI_C: zb_copy8(z.m, z.c); break;
+    case LD_HLI_H: zb_copy8(z.m, z.h); break;
+    case LD_HLI_L: zb_copy8(z.m, z.l); break;
+    case LD_HLI_N: zb_set8(z.m, imm & 0xFFu); break;
+    case LD_A_BCI: case LD_A_DEI: zb_copy8(z.a, z.m); break;
+    case LD_BCI_A: case LD_DEI_A: zb_copy8(z.m, z.a); break;
+    case ADD_A_HLI: zb_copy8(t8, z.m); zb_add(z, t8, 0u); break;
+    case ADC_A_HLI: zb_copy8(t8, z.m); zb_add(z, t8, z.f[0]); break;
+    case SUB_HLI: zb_copy8(t8, z.m); zb_sub(z, t8, 0u); break;
+    case SBC_A_HLI: zb_copy8(t8, z.m); zb_sub(z, t8, z.f[0]); break;
+    case AND_HLI: zb_copy8(t8, z.m); zb_and(z, t8); break;
+    case XOR_HLI: zb_copy8(t8, z.m); zb_xor(z, t8); break;
+    case OR_HLI: zb_copy8(t8, z.m); zb_or(z, t8); break;
+    case CP_HLI: zb_copy8(t8, z.m); zb_cp(z, t8); break;
+    case INC_HLI: zb_inc(z, z.m); break;
+    case DEC_HLI: zb_dec(z, z.m); break;
+    case RLC_HLI: zb_rot(z, z.m, 0); break;
+    case RRC_HLI: zb_rot(z, z.m, 1); break;
+    case RL_HLI: zb_rot(z, z.m, 2); break;
+    case RR_HLI: zb_rot(z, z.m, 3); break;
+    case SLA_HLI: zb_rot(z, z.m, 4); break;
+    case SRA_HLI: zb_rot(z, z.m, 5); break;
+    case SRL_HLI: zb_rot(z, z.m, 6); break;
+    case SLL_HLI: zb_rot(z, z.m, 7); break;
+    case BIT_0_HLI: zb_bit(z, z.m, 0); break;
+    case BIT_1_HLI: zb_bit(z, z.m, 1); break;
+    case BIT_2_HLI: zb_bit(z, z.m, 2); break;
+    case BIT_3_HLI: zb_bit(z, z.m, 3); break;
+    case BIT_4_HLI: zb_bit(z, z.m, 4); break;
+    case BIT_5_HLI: zb_bit(z, z.m, 5); break;
+    case BIT_6_HLI: zb_bit(z, z.m, 6); break;
+    case BIT_7_HLI: zb_bit(z, z.m, 7); break;
+    case RES_0_HLI: z.m[0] = 0u; break;
+    case RES_1_HLI: z.m[1] = 0u; break;
+    case RES_2_HLI: z.m[2] = 0u; break;
+    case RES_3_HLI: z.m[3] = 0u; break;
+    case RES_4_HLI: z.m[4] = 0u; break;
+    case RES_5_HLI: z.m[5] = 0u; break;
+    case RES_6_HLI: z.m[6] = 0u; break;
+    case RES_7_HLI: z.m[7] = 0u; break;
+    case SET_0_HLI: z.m[0] = kZBOnes; break;
+    case SET_1_HLI: z.m[1] = kZBOnes; break;
+    case SET_2_HLI: z.m[2] = kZBOnes; break;
+    case SET_3_HLI: z.m[3] = kZBOnes; break;
+    case SET_4_HLI: z.m[4] = kZBOnes; break;
+    case SET_5_HLI: z.m[5] = kZBOnes; break;
+    case SET_6_HLI: z.m[6] = kZBOnes; break;
+    case SET_7_HLI: z.m[7] = kZBOnes; break;
+    default: zb_acc_step(z, op); break;
+  }
+}
+
 // Block decoding of an ExhaustiveCheck sweep (pkg/search/verifier.go:
 // 428-612), set up once per pair.  Block index fields, fastest first: SP (4
 // bits, reduced sweeps that read SP), the swept registers from the last to
@@ -701,6 +819,43 @@ Z80_HD void cdec_vals(const CDec& d, unsigned long long ab, uint32_t& vb, uint32
   vb = (lo >> d.shb) & d.mb;
   vc = (lo >> d.shc) & d.mc;
   carry = (lo >> d.shf) & 1u;
+}
+
+// Block decoding for wide compact pairs.  A wide pair reads at most four
+// registers and the memory byte, never SP, so its block index (below 2^26)
+// is the carry above at most five fields, 8 bits each in a full sweep and
+// 5 bits indexing the representative values in a reduced one.  The initial
+// values of the five wide fields (B, C, H, L as renamed, then M) are shifts
+// and masks of the index: lo packs the five fields' shifts (6 bits each),
+// hi the fields that are swept (bits 0..4), the reduced flag (bit 5) and the
+// carry's shift (bits 6..11).  o[s]: the original register (0..5) that
+// field s stands for, or -1; slot[r]: register r's sweep field (-1: not
+// swept; a named register that is not read starts at 0).
+struct WDec {
+  uint32_t lo, hi;
+};
+Z80_HD WDec wdec_make(int nx, bool reduced, const int (&slot)[7], const int (&o)[4]) {
+  const int fw = reduced ? 5 : 8;
+  uint32_t lo = 0, on = 0;
+  for (int s = 0; s < 5; s++) {
+    const int r = s < 4 ? o[s] : 6;
+    if (r < 0 || slot[r] < 0) continue;
+    lo |= uint32_t((nx - 1 - slot[r]) * fw) << (6 * s);
+    on |= 1u << s;
+  }
+  return WDec{lo, on | (reduced ? 32u : 0u) | uint32_t(nx * fw) << 6};
+}
+// The five fields and the carry of block ab.
+Z80_HD void wdec_vals(const WDec& d, uint32_t ab, const uint8_t* rep, uint32_t (&v)[5], uint32_t& carry) {
+  const bool reduced = (d.hi >> 5) & 1u;
+#if defined(__CUDA_ARCH__)
+#pragma unroll
+#endif
+  for (int s = 0; s < 5; s++) {
+    const uint32_t x = (ab >> ((d.lo >> (6 * s)) & 63u)) & (reduced ? 31u : 255u);
+    v[s] = ((d.hi >> s) & 1u) ? (reduced ? uint32_t(rep[x]) : x) : 0u;
+  }
+  carry = (ab >> ((d.hi >> 6) & 63u)) & 1u;
 }
 
 // Planes <-> scalar states (host tests; the sweep builds planes directly).

@@ -351,6 +351,96 @@ const CompactTables& compact_tables() {
   return T;
 }
 
+void wide_set_map(uint8_t set, uint8_t (&map)[6]) {
+  // places B, C, H, L (0, 1, 4, 5); pairs BC, DE, HL are groups 0, 1, 2
+  int target[6] = {-1, -1, -1, -1, -1, -1};
+  bool used[6] = {false, false, false, false, false, false};
+  auto full = [&](int g) { return ((set >> (2 * g)) & 3u) == 3u; };
+  // register pairs (both halves named) onto BC or HL, their own first
+  for (int g : {0, 2, 1}) {
+    if (!full(g)) continue;
+    int slot = -1;
+    if (g != 1 && !used[2 * g]) slot = 2 * g;
+    else if (!used[0]) slot = 0;
+    else if (!used[4]) slot = 4;
+    if (slot < 0) continue;  // three pairs: more than four registers
+    target[2 * g] = slot;
+    target[2 * g + 1] = slot + 1;
+    used[slot] = used[slot + 1] = true;
+  }
+  // single registers: their own place if it is B, C, H or L and free, else
+  // the first free of those
+  static const int kPlaces[4] = {0, 1, 4, 5};
+  for (int r = 0; r < 6; r++) {
+    if (!(set & (1u << r)) || target[r] >= 0) continue;
+    if ((r < 2 || r > 3) && !used[r]) {
+      target[r] = r;
+      used[r] = true;
+      continue;
+    }
+    for (int p : kPlaces)
+      if (!used[p]) {
+        target[r] = p;
+        used[p] = true;
+        break;
+      }
+  }
+  // the registers outside the set take the places left, in order
+  for (int r = 0; r < 6; r++)
+    if (target[r] < 0)
+      for (int d = 0; d < 6; d++)
+        if (!used[d]) {
+          target[r] = d;
+          used[d] = true;
+          break;
+        }
+  for (int r = 0; r < 6; r++) map[r] = uint8_t(target[r]);
+}
+
+bool wide_map(const uint32_t* t, int tn, const uint32_t* c, int cn, uint8_t (&map)[6], uint32_t* tw, uint32_t* cw) {
+  uint8_t fp = 0;
+  for (int i = 0; i < tn; i++) fp |= op_regs(insn_op(t[i]));
+  for (int i = 0; i < cn; i++) fp |= op_regs(insn_op(c[i]));
+  if (fp & 0x80) return false;  // SP
+  if (__builtin_popcount(fp & 0x3Fu) > 4) return false;
+  wide_set_map(uint8_t(fp & 0x3Fu), map);
+  for (int i = 0; i < tn; i++) {
+    const int o = op_rename(insn_op(t[i]), map);
+    if (o < 0) return false;
+    tw[i] = insn(uint16_t(o), insn_imm(t[i]));
+  }
+  for (int i = 0; i < cn; i++) {
+    const int o = op_rename(insn_op(c[i]), map);
+    if (o < 0) return false;
+    cw[i] = insn(uint16_t(o), insn_imm(c[i]));
+  }
+  return true;
+}
+
+const WideTables& wide_tables() {
+  static WideTables T;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    std::memset(T.id_of_set, 0, sizeof T.id_of_set);
+    static const int kPlaces[4] = {0, 1, 4, 5};
+    int e = 0;
+    for (uint32_t set = 0; set < 64; set++) {
+      if (__builtin_popcount(set) > 4) continue;
+      T.id_of_set[set] = uint8_t(e + 1);
+      uint8_t map[6];
+      wide_set_map(uint8_t(set), map);
+      for (int op = 0; op < kNumOps; op++) T.ren[e][op] = int16_t(op_rename(uint16_t(op), map));
+      for (int s = 0; s < 4; s++) {
+        T.orig[e][s] = -1;
+        for (int r = 0; r < 6; r++)
+          if ((set & (1u << r)) && map[r] == kPlaces[s]) T.orig[e][s] = int8_t(r);
+      }
+      e++;
+    }
+  });
+  return T;
+}
+
 int op_rename(uint16_t op, const uint8_t (&map)[6]) {
   static const char* kRegs = "BCDEHL";
   static const char* kPairs[3] = {"BC", "DE", "HL"};

@@ -64,6 +64,25 @@ struct CompactTables {
   uint8_t opregs[kNumOps];
 };
 const CompactTables& compact_tables();
+// The wide compact state holds A, F, B, C, H, L and the memory byte.  A pair
+// whose programs name at most four of B..L and not SP is renamed onto B, C,
+// H and L: a register pair used as one (both halves in the set) onto BC or
+// HL, keeping its own place when that is BC or HL; single registers keep
+// their place when it is B, C, H or L and free, else take the first free of
+// them.  False when the pair names more, or a renamed opcode does not exist.
+bool wide_map(const uint32_t* t, int tn, const uint32_t* c, int cn, uint8_t (&map)[6], uint32_t* tw, uint32_t* cw);
+void wide_set_map(uint8_t set, uint8_t (&map)[6]);
+// The wide renaming as tables for the device, one entry per set of at most
+// four registers (57 sets): id_of_set[set] = 1 + entry (0 for larger sets),
+// ren[entry][op] the renamed opcode or -1, orig[entry][s] the original
+// register (0..5) that plays B, C, H, L (s = 0..3), or -1.
+constexpr int kWideSets = 57;
+struct WideTables {
+  int16_t ren[kWideSets][kNumOps];
+  int8_t orig[kWideSets][4];
+  uint8_t id_of_set[64];
+};
+const WideTables& wide_tables();
 const uint8_t* op_encoding(uint16_t op, int* n);
 std::string disassemble(uint32_t insn);   // catalog.go:73-127
 std::string disasm_seq(const uint32_t* seq, int n);  // " : " joined

@@ -158,7 +158,8 @@ struct z80b_ctx {
   // pipeline scratch
   DBuf cnt_f, cnt_m, cnt_all, base, meta, surv, sdiff, checks;
   DBuf next, win, windiff, spec, spec2, wlen, wend, cdone;
-  DBuf pairs, pair_src, nchunks, cbase, nchunks_x, cbase_x, nchunks_c, cbase_c, rejected, npairs, counter, states;
+  DBuf pairs, pair_src, nchunks, cbase, nchunks_x, cbase_x, nchunks_c, cbase_c, nchunks_w, cbase_w, rejected, npairs,
+      counter, states;
   DBuf rcnt, rbase, rules, checked, surv_target, midpass, flag;
   DBuf cub_tmp;
   DBuf hits, nhits, fpq;
@@ -176,6 +177,7 @@ struct z80b_ctx {
   int qc_index = 1;           // Z80B_OPT_QC_INDEX
   int xbits = 1;              // Z80B_OPT_XINDEP_BITS
   int compact = 1;            // Z80B_OPT_COMPACT_SWEEP
+  int wide = 1;               // Z80B_OPT_WIDE_SWEEP
   uint32_t sweep_kernels = 0; // kSweep* bits of the sweep kernels launched since the last reset
   int graph_rounds = 1;       // Z80B_OPT_GRAPH_ROUNDS
   DBuf roundctl;              // RoundCtl of the device-driven rounds
@@ -578,7 +580,8 @@ int sweep_round(z80b_ctx* ctx, const DevTargets& T, const DevPool& P, const Roun
   CKR(scan(ctx, R.nchunks, R.cbase, np));
   CKR(scan(ctx, R.nchunks_x, R.cbase_x, np));
   if (R.compact) CKR(scan(ctx, R.nchunks_c, R.cbase_c, np));
-  unsigned long long last[6] = {0, 0, 0, 0, 0, 0};
+  if (R.wide) CKR(scan(ctx, R.nchunks_w, R.cbase_w, np));
+  unsigned long long last[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   CK(cudaMemcpyAsync(&last[0], R.cbase + (np - 1), 8, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(&last[1], R.nchunks + (np - 1), 8, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(&last[2], R.cbase_x + (np - 1), 8, cudaMemcpyDeviceToHost, s));
@@ -587,12 +590,17 @@ int sweep_round(z80b_ctx* ctx, const DevTargets& T, const DevPool& P, const Roun
     CK(cudaMemcpyAsync(&last[4], R.cbase_c + (np - 1), 8, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(&last[5], R.nchunks_c + (np - 1), 8, cudaMemcpyDeviceToHost, s));
   }
+  if (R.wide) {
+    CK(cudaMemcpyAsync(&last[6], R.cbase_w + (np - 1), 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&last[7], R.nchunks_w + (np - 1), 8, cudaMemcpyDeviceToHost, s));
+  }
   CK(cudaStreamSynchronize(s));
-  CK(cudaMemsetAsync(R.counter, 0, 24, s));
-  trace("sweep: %u pairs, %llu + %llu + %llu chunks", np, last[0] + last[1], last[2] + last[3], last[4] + last[5]);
+  CK(cudaMemsetAsync(R.counter, 0, 32, s));
+  trace("sweep: %u pairs, %llu + %llu + %llu + %llu chunks", np, last[0] + last[1], last[2] + last[3],
+        last[4] + last[5], last[6] + last[7]);
   int ke = kbegin(ctx, 1);
-  const int nl = launch_exhaustive(T, P, R, np, last[0] + last[1], last[2] + last[3], last[4] + last[5], ctx->exh_k,
-                                   s, &ctx->sweep_kernels);
+  const int nl = launch_exhaustive(T, P, R, np, last[0] + last[1], last[2] + last[3], last[4] + last[5],
+                                   last[6] + last[7], ctx->exh_k, s, &ctx->sweep_kernels);
   kend(ctx, ke);
   CKR(check_launch(ctx, "exhaustive"));
   if (nl > 1) ctx->launches += uint32_t(nl - 1);
@@ -671,7 +679,8 @@ int rounds_on_device(z80b_ctx* ctx, RoundGraph& g, const DevTargets& T, const De
     g.key = key;
     trace("round loop captured (%s pass)", ps ? "length-2" : "length-1");
   }
-  const int per_iter = (ps ? 3 : 2) + 1 + (R.compact ? 3 : 2);  // build, scan, [rescan], sweeps, resolve
+  // build, scan, [rescan], sweeps, resolve
+  const int per_iter = (ps ? 3 : 2) + 1 + 2 + (R.compact ? 1 : 0) + (R.wide ? 1 : 0);
   CK(cudaMemsetAsync(ctl, 0, sizeof(RoundCtl), s));
   int ke = kbegin(ctx, 1);
   CK(cudaGraphLaunch(g.exec, s));
@@ -684,7 +693,7 @@ int rounds_on_device(z80b_ctx* ctx, RoundGraph& g, const DevTargets& T, const De
   *rounds += h.rounds;
   *pairs += h.pairs;
   ctx->launches += h.iters * uint32_t(per_iter);
-  uint32_t mask = (R.compact ? kSweepCompact : 0u) | kSweepBits;
+  uint32_t mask = (R.compact ? kSweepCompact : 0u) | (R.wide ? kSweepWide : 0u) | kSweepBits;
   if (R.xunit == kXBitsBlocks) mask |= kSweepXBits;
   else mask |= kSweepScalarK1 << (ctx->exh_k == 1 ? 0 : ctx->exh_k == 2 ? 1 : ctx->exh_k == 8 ? 3 : 2);
   ctx->sweep_kernels |= mask;
@@ -723,7 +732,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
   CK(ctx->checked.ensure(8));
   CK(ctx->states.ensure(16));
   CK(ctx->npairs.ensure(4));
-  CK(ctx->counter.ensure(24));
+  CK(ctx->counter.ensure(32));
   CK(cudaMemsetAsync(ctx->checks.p, 0, 8, s));
   CK(cudaMemsetAsync(ctx->checked.p, 0, 8, s));
   CK(cudaMemsetAsync(ctx->states.p, 0, 16, s));
@@ -795,6 +804,10 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
       CK(ctx->nchunks_c.ensure(8 * cap));
       CK(ctx->cbase_c.ensure(8 * cap));
     }
+    if (ctx->wide) {
+      CK(ctx->nchunks_w.ensure(8 * cap));
+      CK(ctx->cbase_w.ensure(8 * cap));
+    }
     CK(ctx->rejected.ensure(4 * cap));
     CK(ctx->wlen.ensure(cap));
     CK(ctx->wend.ensure(4 * cap));
@@ -823,6 +836,9 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
     R.compact = mode == Z80B_MODE_FIRST && ctx->compact ? 1u : 0u;
     R.nchunks_c = R.compact ? ctx->nchunks_c.as<unsigned long long>() : nullptr;
     R.cbase_c = R.compact ? ctx->cbase_c.as<unsigned long long>() : nullptr;
+    R.wide = mode == Z80B_MODE_FIRST && ctx->wide ? 1u : 0u;
+    R.nchunks_w = R.wide ? ctx->nchunks_w.as<unsigned long long>() : nullptr;
+    R.cbase_w = R.wide ? ctx->cbase_w.as<unsigned long long>() : nullptr;
     // rounds on the device (one graph) unless the caller takes answers
     // round by round (streaming callbacks)
     const bool dev_rounds = ctx->graph_rounds && !opts.rep;
@@ -959,6 +975,9 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
     R.compact = mode == Z80B_MODE_FIRST && ctx->compact ? 1u : 0u;
     R.nchunks_c = R.compact ? ctx->nchunks_c.as<unsigned long long>() : nullptr;
     R.cbase_c = R.compact ? ctx->cbase_c.as<unsigned long long>() : nullptr;
+    R.wide = mode == Z80B_MODE_FIRST && ctx->wide ? 1u : 0u;
+    R.nchunks_w = R.wide ? ctx->nchunks_w.as<unsigned long long>() : nullptr;
+    R.cbase_w = R.wide ? ctx->cbase_w.as<unsigned long long>() : nullptr;
     if (S) {
       launch_surv_targets(q, n, ctx->surv_target.as<uint32_t>(), s);
       CKR(check_launch(ctx, "surv_targets"));
@@ -1465,7 +1484,7 @@ int z80b_verify_pairs(z80b_ctx* ctx, const uint32_t* tgt, const uint8_t* tlens, 
     CK(ctx->cbase.ensure(8ull * n));
     CK(ctx->cbase_x.ensure(8ull * n));
     CK(ctx->rejected.ensure(4ull * n));
-    CK(ctx->counter.ensure(24));
+    CK(ctx->counter.ensure(32));
     CK(ctx->states.ensure(16));
     CK(cudaMemcpyAsync(ctx->pairs.p, pr.data(), sizeof(PairRec) * n, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(ctx->cbase.p, cb.data(), 8ull * n, cudaMemcpyHostToDevice, s));
@@ -1479,7 +1498,7 @@ int z80b_verify_pairs(z80b_ctx* ctx, const uint32_t* tgt, const uint8_t* tlens, 
     R.rejected = ctx->rejected.as<uint32_t>();
     R.counter = ctx->counter.as<unsigned long long>();
     R.states = ctx->states.as<unsigned long long>();
-    const int nl = launch_exhaustive(T, P, R, n, tot, totx, 0, ctx->exh_k, s);
+    const int nl = launch_exhaustive(T, P, R, n, tot, totx, 0, 0, ctx->exh_k, s);
     CKR(check_launch(ctx, "exhaustive"));
     if (nl > 1) ctx->launches += uint32_t(nl - 1);
     std::vector<uint32_t> rej(n);
@@ -1535,6 +1554,10 @@ int z80b_set_option(z80b_ctx* ctx, int option, int value) {
       if (value != 0 && value != 1) return fail(ctx, Z80B_EINVAL, "graph rounds option must be 0 or 1");
       ctx->graph_rounds = value;
       return Z80B_OK;
+    case Z80B_OPT_WIDE_SWEEP:
+      if (value != 0 && value != 1) return fail(ctx, Z80B_EINVAL, "wide sweep option must be 0 or 1");
+      ctx->wide = value;
+      return Z80B_OK;
   }
   return fail(ctx, Z80B_EINVAL, "unknown option %d", option);
 }
@@ -1549,6 +1572,7 @@ int z80b_get_option(const z80b_ctx* ctx, int option, int* value) {
     case Z80B_OPT_XINDEP_BITS: *value = ctx->xbits; return Z80B_OK;
     case Z80B_OPT_COMPACT_SWEEP: *value = ctx->compact; return Z80B_OK;
     case Z80B_OPT_GRAPH_ROUNDS: *value = ctx->graph_rounds; return Z80B_OK;
+    case Z80B_OPT_WIDE_SWEEP: *value = ctx->wide; return Z80B_OK;
   }
   return Z80B_EINVAL;
 }
@@ -1564,6 +1588,7 @@ static void sweep_kernel_names(uint32_t mask, char* out, size_t cap) {
   if (mask & kSweepBits) add("k_exhaustive<1,0>");
   if (mask & kSweepXBits) add("k_exhaustive<1,2>");
   if (mask & kSweepCompact) add("k_exhaustive<1,3>");
+  if (mask & kSweepWide) add("k_exhaustive<1,4>");
   const char* scalar[4] = {"k_exhaustive<1,1>", "k_exhaustive<2,1>", "k_exhaustive<4,1>", "k_exhaustive<8,1>"};
   for (int i = 0; i < 4; i++)
     if (mask & (kSweepScalarK1 << i)) add(scalar[i]);
@@ -1573,8 +1598,9 @@ static void sweep_kernel_names(uint32_t mask, char* out, size_t cap) {
 // Runs the sample job once for every sweep configuration of the grid and
 // keeps the fastest (device time of the whole pipeline): the kernel for
 // A-independent pairs (bit-sliced, or scalar with 1, 2, 4 or 8 states per
-// lane per dispatch), units per work chunk, and whether A-dependent pairs
-// that fit the compact state take the compact kernel.  Every cell of the
+// lane per dispatch), units per work chunk, and whether pairs that fit the
+// compact states take the compact kernels (both the A/F/B/C state and the
+// wide one, or neither).  Every cell of the
 // grid is a distinct kernel configuration; each trial records the sweep
 // kernels it launched.
 int z80b_autotune(z80b_ctx* ctx, const z80b_job* sample, z80b_tune_result* out) {
@@ -1598,6 +1624,7 @@ int z80b_autotune(z80b_ctx* ctx, const z80b_job* sample, z80b_tune_result* out) 
         ctx->exh_k = xv[a][1] ? xv[a][1] : k0;
         ctx->chunk_blocks = cs[b];
         ctx->compact = m;
+        ctx->wide = m;
         z80b_stats st{};
         uint64_t nr = 0;
         CKR(run_pipeline(ctx, T, ctx->staged.opts, &st, &nr));  // warm
@@ -1625,6 +1652,7 @@ int z80b_autotune(z80b_ctx* ctx, const z80b_job* sample, z80b_tune_result* out) 
   ctx->chunk_blocks = bc;
   ctx->xbits = bx;
   ctx->compact = bm;
+  ctx->wide = bm;
   r.lane_states = bk;
   r.chunk_blocks = bc;
   r.xindep_bits = bx;

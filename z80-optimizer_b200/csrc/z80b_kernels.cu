@@ -60,6 +60,11 @@ __device__ int16_t g_cren[kCompactSets][kNumOps];
 __device__ int8_t g_corig[kCompactSets][2];
 __device__ uint8_t g_cid[64];
 __device__ uint8_t g_opregs[kNumOps];
+// wide compact sweep: the same per register set of at most four registers
+// (wide_tables)
+__device__ int16_t g_wren[kWideSets][kNumOps];
+__device__ int8_t g_worig[kWideSets][4];
+__device__ uint8_t g_wid[64];
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 __device__ __forceinline__ unsigned lanemask_lt() {
@@ -165,6 +170,26 @@ __device__ __forceinline__ uint8_t pair_cmap(const DevTargets& T, uint32_t t, co
     if (g_cren[id - 1][cw[i] & 0xFFFFu] < 0) return 0;
   return uint8_t(id);
 }
+// Wide compact sweep: kWideClass | (1 + the register-set entry) when the
+// pair's instructions name at most four of B..L and not SP, and all rename
+// onto B, C, H and L (wide_map); 0 otherwise.
+constexpr uint8_t kWideClass = 0x80u;
+__device__ __forceinline__ uint8_t pair_wmap(const DevTargets& T, uint32_t t, const DevPool& P, uint32_t c) {
+  const uint32_t tl = target_len(T, t), cl = pool_len(P, c);
+  const uint32_t* tw = T.insn + (size_t)t * T.stride;
+  const uint32_t* cw = P.insn + (size_t)c * P.stride;
+  uint32_t fp = 0;
+  for (uint32_t i = 0; i < tl; i++) fp |= g_opregs[tw[i] & 0xFFFFu];
+  for (uint32_t i = 0; i < cl; i++) fp |= g_opregs[cw[i] & 0xFFFFu];
+  if (fp & 0x80u) return 0;
+  const uint32_t id = g_wid[fp & 0x3Fu];
+  if (!id) return 0;
+  for (uint32_t i = 0; i < tl; i++)
+    if (g_wren[id - 1][tw[i] & 0xFFFFu] < 0) return 0;
+  for (uint32_t i = 0; i < cl; i++)
+    if (g_wren[id - 1][cw[i] & 0xFFFFu] < 0) return 0;
+  return uint8_t(kWideClass | id);
+}
 // A-dependent pairs run bit-sliced (z80_bits.cuh): a unit is 4 A-blocks, a
 // lane takes 32 consecutive values of A of one block.
 constexpr unsigned long long kBitsBlocks = 4;
@@ -183,11 +208,12 @@ __device__ __forceinline__ unsigned long long chunks_for(unsigned long long nb, 
 __device__ __forceinline__ void set_chunks(const RoundBuf& R, uint32_t p, const PairRec& pr) {
   const unsigned long long c = chunks_for(pair_units(pr.nblocks, pr.keepR, R.xunit), R.chunk_blocks);
   const bool xind = (pr.keepR & kXIndep) != 0;
-  const bool comp = pr.cmap != 0;  // only set when R.compact
-  R.nchunks[p] = (xind || comp) ? 0ull : c;
-  R.nchunks_x[p] = xind ? c : 0ull;
-  if (comp) R.nchunks_c[p] = c;
-  else if (R.compact) R.nchunks_c[p] = 0ull;
+  const bool wide = (pr.cmap & kWideClass) != 0;  // only set when R.wide
+  const bool comp = pr.cmap != 0 && !wide;        // only set when R.compact
+  R.nchunks[p] = (xind || comp || wide) ? 0ull : c;
+  R.nchunks_x[p] = (xind && !comp && !wide) ? c : 0ull;
+  if (R.compact) R.nchunks_c[p] = comp ? c : 0ull;
+  if (R.wide) R.nchunks_w[p] = wide ? c : 0ull;
 }
 __device__ __forceinline__ unsigned long long chunks_for(unsigned long long nb, uint32_t cb) {
   unsigned long long c = (nb + cb - 1) / cb;
@@ -488,9 +514,14 @@ __device__ __forceinline__ void put_pair(const RoundBuf& R, uint32_t p, const De
   pr.keepF = kind ? uint8_t(~target_dead(T, t)) : uint8_t(0xFFu);
   pr.keepR = kind ? uint8_t((~target_dead_regs(T, t) & 0x3Fu) | 0x80u) : uint8_t(0x3Fu);
   if (pair_xindep(T, t, P, c)) pr.keepR |= uint8_t(kXIndep);
-  // compact class: A-dependent pairs, and A-independent ones when those are
-  // swept bit-sliced (units of kXBitsBlocks)
-  pr.cmap = (R.compact && (!(pr.keepR & kXIndep) || R.xunit == kXBitsBlocks)) ? pair_cmap(T, t, P, c) : uint8_t(0);
+  // compact classes: A-dependent pairs, and A-independent ones when those
+  // are swept bit-sliced (units of kXBitsBlocks); the narrow state first
+  pr.cmap = 0;
+  if (!(pr.keepR & kXIndep) || R.xunit == kXBitsBlocks) {
+    if (R.compact) pr.cmap = pair_cmap(T, t, P, c);
+    // the wide state: A-dependent pairs only
+    if (!pr.cmap && R.wide && !(pr.keepR & kXIndep)) pr.cmap = pair_wmap(T, t, P, c);
+  }
   R.pairs[p] = pr;
   R.pair_src[p] = src;
   set_chunks(R, p, pr);
@@ -994,6 +1025,80 @@ __device__ __forceinline__ bool cxbits_unit(unsigned long long u, unsigned long 
   return bad;
 }
 
+// Wide compact sweeps (A-dependent pairs): the layout of bits_unit on the
+// wide state (A, F, B, C, H, L, M; ZBW) with renamed programs.  Fields 0..3 are
+// B, C, H, L (standing for the registers the pair's set puts there), field
+// 4 is M; cmp bit s: field s is compared (it stands for a register under
+// keepR).  A and M are always compared, F under keepF.
+constexpr int kWideWords = 56;  // planes saved per lane
+__device__ __forceinline__ void zbw_init(ZBW& z, const uint32_t (&v)[5], uint32_t carry) {
+  zb_set8(z.f, carry);
+  zb_set8(z.b, v[0]);
+  zb_set8(z.c, v[1]);
+  zb_set8(z.h, v[2]);
+  zb_set8(z.l, v[3]);
+  zb_set8(z.m, v[4]);
+}
+__device__ __forceinline__ void zbw_save(const ZBW& z, uint32_t* s) {
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    s[(0 + i) * 32] = z.a[i];
+    s[(8 + i) * 32] = z.f[i];
+    s[(16 + i) * 32] = z.b[i];
+    s[(24 + i) * 32] = z.c[i];
+    s[(32 + i) * 32] = z.h[i];
+    s[(40 + i) * 32] = z.l[i];
+    s[(48 + i) * 32] = z.m[i];
+  }
+}
+__device__ __forceinline__ uint32_t zbw_diff(const ZBW& z, const uint32_t* s, uint32_t keepF, uint32_t cmp) {
+  uint32_t d = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    d |= z.a[i] ^ s[(0 + i) * 32];
+    if ((keepF >> i) & 1u) d |= z.f[i] ^ s[(8 + i) * 32];
+    if (cmp & 1u) d |= z.b[i] ^ s[(16 + i) * 32];
+    if (cmp & 2u) d |= z.c[i] ^ s[(24 + i) * 32];
+    if (cmp & 4u) d |= z.h[i] ^ s[(32 + i) * 32];
+    if (cmp & 8u) d |= z.l[i] ^ s[(40 + i) * 32];
+    d |= z.m[i] ^ s[(48 + i) * 32];
+  }
+  return d;
+}
+// A-dependent: lane l takes block 4u + l/8 and A = 32(l % 8) .. +31.
+__device__ __forceinline__ bool wbits_unit(unsigned long long u, unsigned long long nblocks, const WDec& dec,
+                                           uint32_t pw, int tl, int cl, uint32_t keepF, uint32_t cmp, uint32_t* sm) {
+  const unsigned lane = lane_id();
+  const unsigned long long blk = u * kBitsBlocks + (lane >> 3);
+  const bool valid = blk < nblocks;
+  uint32_t v[5], carry;
+  wdec_vals(dec, uint32_t(valid ? blk : u * kBitsBlocks), g_rep, v, carry);
+  const uint32_t a0 = (lane & 7u) * 32u;
+  ZBW z;
+  auto init = [&]() {
+    z.a[0] = 0xAAAAAAAAu;
+    z.a[1] = 0xCCCCCCCCu;
+    z.a[2] = 0xF0F0F0F0u;
+    z.a[3] = 0xFF00FF00u;
+    z.a[4] = 0xFFFF0000u;
+    z.a[5] = (a0 & 32u) ? kZBOnes : 0u;
+    z.a[6] = (a0 & 64u) ? kZBOnes : 0u;
+    z.a[7] = (a0 & 128u) ? kZBOnes : 0u;
+    zbw_init(z, v, carry);
+  };
+  init();
+#pragma unroll 1
+  for (int st = 0; st < tl + cl; st++) {
+    if (st == cl) {
+      zbw_save(z, sm);
+      init();
+    }
+    const int src = st < cl ? tl + st : st - cl;
+    const uint32_t w = __shfl_sync(kFull, pw, src);
+    zbw_step(z, w & 0xFFFFu, w >> 16);
+  }
+  return valid && zbw_diff(z, sm, keepF, cmp) != 0u;
+}
 // One unit (128 A-blocks at A = 0, 1) of an A-independent sweep, for the
 // A-independent sweep kernel; kept out of line (that kernel compiles without
 // register spills at every K this way).
@@ -1022,15 +1127,16 @@ __device__ __noinline__ bool xindep_unit(unsigned long long first, unsigned long
 
 // One kernel per pair class: CLS 0 runs the bit-sliced pairs (outputs
 // depend on A), CLS 1 the A-independent ones (K states per lane per
-// dispatch), CLS 2 the A-independent ones bit-sliced, CLS 3 the A-dependent
-// ones whose registers fit the compact state (three blocks per SM); each class
+// dispatch), CLS 2 the A-independent ones bit-sliced, CLS 3 the pairs whose
+// registers fit the compact state (three blocks per SM), CLS 4 the
+// A-dependent ones that fit the wide compact state (two blocks per SM); each class
 // draws chunks from its own numbering and dispenser.  Kept apart so that
 // neither path's registers weigh on the other.
 // dev_total / dev_np (device-driven rounds): the class's chunk total and the
 // round's pair count are read from the device instead of total / npairs.
 // chunks_per_warp: chunks a warp takes before its block retires.
 template <int K, int CLS>
-__global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : 1)
+__global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : (CLS == 4 ? 2 : 1))
     k_exhaustive(DevTargets T, DevPool P, RoundBuf R, uint32_t npairs, unsigned long long total,
                  const unsigned long long* __restrict__ dev_total, const uint32_t* __restrict__ dev_np,
                  int chunks_per_warp) {
@@ -1040,7 +1146,8 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : 1)
     npairs = *dev_np;
   }
   constexpr bool XI = CLS != 0;
-  const unsigned long long* __restrict__ cbase = CLS == 3 ? R.cbase_c : (XI ? R.cbase_x : R.cbase);
+  const unsigned long long* __restrict__ cbase =
+      CLS == 4 ? R.cbase_w : (CLS == 3 ? R.cbase_c : (XI ? R.cbase_x : R.cbase));
   const unsigned lane = lane_id();
   unsigned long long my_states = 0, my_eval = 0;
   // At most kChunksPerWarp chunks per warp, then the block retires: the grid
@@ -1048,7 +1155,7 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : 1)
   // priority) get SMs as soon as blocks of a long sweep retire.
   for (int taken = 0; taken < chunks_per_warp; taken++) {
     unsigned long long k = 0;
-    if (lane == 0) k = atomicAdd(R.counter + (CLS == 3 ? 2 : (XI ? 1 : 0)), 1ull);
+    if (lane == 0) k = atomicAdd(R.counter + (CLS >= 3 ? CLS - 1 : (XI ? 1 : 0)), 1ull);
     k = __shfl_sync(kFull, k, 0);
     if (k >= total) break;
     // pair p: cbase[p] <= k < cbase[p + 1]
@@ -1100,7 +1207,34 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : 1)
 
     bool bad = false;
     bool stopped = false;  // left the loop on the pair's flag (rejected or cancelled elsewhere)
-    if constexpr (CLS == 3) {
+    if constexpr (CLS == 4) {
+      // the wide compact state, the programs renamed onto B, C, H and L
+      const uint32_t e = (pr.cmap & ~uint32_t(kWideClass)) - 1u;
+      if (lane < tl + cl) pw = (uint32_t(uint16_t(g_wren[e][pw & 0xFFFFu]))) | (pw & 0xFFFF0000u);
+      int o[4];
+      uint32_t cmp = 0;
+#pragma unroll
+      for (int f = 0; f < 4; f++) {
+        o[f] = g_worig[e][f];
+        if (o[f] >= 0 && ((pr.keepR >> o[f]) & 1u)) cmp |= 1u << f;
+      }
+      extern __shared__ uint32_t zsm[];
+      uint32_t* sm = zsm + (threadIdx.x >> 5) * (kWideWords * 32) + lane;
+      const WDec dec = wdec_make(nx, reduced, slot, o);
+      for (unsigned long long u = u0; u < u1; u++) {
+        const unsigned long long first = u * kBitsBlocks;
+        const unsigned long long nb = (pr.nblocks - first < kBitsBlocks) ? pr.nblocks - first : kBitsBlocks;
+        bad = wbits_unit(u, pr.nblocks, dec, pw, int(tl), int(cl), pr.keepF, cmp, sm) || bad;
+        my_states += 256ull * nb;
+        my_eval += 256ull * nb;
+        if (__any_sync(kFull, bad)) break;
+        if ((u & 15ull) == 15ull &&
+            __shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0)) {
+          stopped = true;
+          break;
+        }
+      }
+    } else if constexpr (CLS == 3) {
       // the compact state, the programs renamed onto B and C
       const uint32_t e = pr.cmap - 1u;
       if (lane < tl + cl) pw = (uint32_t(uint16_t(g_cren[e][pw & 0xFFFFu]))) | (pw & 0xFFFF0000u);
@@ -1745,6 +1879,10 @@ void dev_upload_tables(cudaStream_t s) {
     cudaMemcpyToSymbolAsync(g_corig, C.orig, sizeof C.orig, 0, cudaMemcpyHostToDevice, s);
     cudaMemcpyToSymbolAsync(g_cid, C.id_of_set, sizeof C.id_of_set, 0, cudaMemcpyHostToDevice, s);
     cudaMemcpyToSymbolAsync(g_opregs, C.opregs, sizeof C.opregs, 0, cudaMemcpyHostToDevice, s);
+    const WideTables& W = wide_tables();
+    cudaMemcpyToSymbolAsync(g_wren, W.ren, sizeof W.ren, 0, cudaMemcpyHostToDevice, s);
+    cudaMemcpyToSymbolAsync(g_worig, W.orig, sizeof W.orig, 0, cudaMemcpyHostToDevice, s);
+    cudaMemcpyToSymbolAsync(g_wid, W.id_of_set, sizeof W.id_of_set, 0, cudaMemcpyHostToDevice, s);
   }
 }
 
@@ -1827,20 +1965,23 @@ void launch_pairs_from_survivors(const DevTargets& T, const DevPool& P, const QC
   if (!nsurv) return;
   k_pairs_from_survivors<<<grid_for(nsurv, 256), 256, 0, s>>>(T, P, q, midpass, nsurv, surv_target, R);
 }
+// Shared memory of a sweep kernel (bit-sliced classes): the candidate's
+// output planes, one column of words per lane.
+constexpr int exhaustive_smem(int cls) {
+  return cls == 1 ? 0 : kBlock * (cls == 3 ? kCompactWords : (cls == 4 ? kWideWords : kBitsWords)) * 4;
+}
 // Resident blocks per SM of a sweep kernel on the current device (its
 // shared-memory limit raised first), cached per device.
 template <int K, int CLS>
 int exhaustive_blocks_per_sm() {
-  constexpr int smem = CLS == 1 ? 0 : kBlock * (CLS == 3 ? kCompactWords : kBitsWords) * 4;
+  constexpr int smem = exhaustive_smem(CLS);
   static std::atomic<int> occ[kMaxCachedDevices];
   return blocks_per_sm(occ, k_exhaustive<K, CLS>, kBlock, smem, smem);
 }
 template <int K, int CLS>
 void launch_exhaustive_k(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
                          unsigned long long total, cudaStream_t s) {
-  // shared memory (bit-sliced kernels): the candidate's output planes,
-  // kBitsWords words per lane
-  constexpr int smem = CLS == 1 ? 0 : kBlock * (CLS == 3 ? kCompactWords : kBitsWords) * 4;
+  constexpr int smem = exhaustive_smem(CLS);
   const int per_sm = exhaustive_blocks_per_sm<K, CLS>();
   // resident blocks, or more when the chunks exceed kChunksPerWarp per warp
   const unsigned long long wpb = kBlock / 32;
@@ -1859,18 +2000,23 @@ void launch_exhaustive_k(const DevTargets& T, const DevPool& P, const RoundBuf& 
 template <int K, int CLS>
 void launch_exhaustive_dev_k(const DevTargets& T, const DevPool& P, const RoundBuf& R, const unsigned long long* total,
                              const uint32_t* np, cudaStream_t s) {
-  constexpr int smem = CLS == 1 ? 0 : kBlock * (CLS == 3 ? kCompactWords : kBitsWords) * 4;
+  constexpr int smem = exhaustive_smem(CLS);
   const int per_sm = exhaustive_blocks_per_sm<K, CLS>();
   const unsigned grid = unsigned(dev_num_sms() * per_sm);
   k_exhaustive<K, CLS><<<grid, kBlock, smem, s>>>(T, P, R, 0u, 0ull, total, np, 0x7FFFFFFF);
 }
 
 int launch_exhaustive(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
-                      unsigned long long total_b, unsigned long long total_x, unsigned long long total_c, int k,
-                      cudaStream_t s, uint32_t* kernels) {
+                      unsigned long long total_b, unsigned long long total_x, unsigned long long total_c,
+                      unsigned long long total_w, int k, cudaStream_t s, uint32_t* kernels) {
   if (!npairs) return 0;
   int n = 0;
   uint32_t mask = 0;
+  if (total_w) {
+    launch_exhaustive_k<1, 4>(T, P, R, npairs, total_w, s);
+    mask |= kSweepWide;
+    n++;
+  }
   if (total_c) {
     launch_exhaustive_k<1, 3>(T, P, R, npairs, total_c, s);
     mask |= kSweepCompact;
@@ -1930,21 +2076,21 @@ __global__ void __launch_bounds__(kScanThreads) k_round_scan(RoundBuf R, RoundCt
       ctl->rounds += 1;
       ctl->pairs += np;
     }
-    R.counter[0] = R.counter[1] = R.counter[2] = 0;
+    R.counter[0] = R.counter[1] = R.counter[2] = R.counter[3] = 0;
     if (np == 0 || over) {
-      ctl->totals[0] = ctl->totals[1] = ctl->totals[2] = 0;
+      ctl->totals[0] = ctl->totals[1] = ctl->totals[2] = ctl->totals[3] = 0;
       if (!refill || *refill == 0) cudaGraphSetConditional(loop, 0);
     }
   }
   if (np == 0 || over) return;
   const uint32_t per = (np + kScanThreads - 1) / kScanThreads;
   const uint32_t lo = min(tid * per, np), hi = min(lo + per, np);
-  for (int c = 0; c < 3; c++) {
-    const unsigned long long* in = c == 0 ? R.nchunks : (c == 1 ? R.nchunks_x : R.nchunks_c);
-    unsigned long long* out = c == 0 ? R.cbase : (c == 1 ? R.cbase_x : R.cbase_c);
-    if (c == 2 && !R.compact) {
-      if (tid == 0) ctl->totals[2] = 0;
-      break;
+  for (int c = 0; c < 4; c++) {
+    const unsigned long long* in = c == 0 ? R.nchunks : (c == 1 ? R.nchunks_x : (c == 2 ? R.nchunks_c : R.nchunks_w));
+    unsigned long long* out = c == 0 ? R.cbase : (c == 1 ? R.cbase_x : (c == 2 ? R.cbase_c : R.cbase_w));
+    if ((c == 2 && !R.compact) || (c == 3 && !R.wide)) {  // the same for every thread
+      if (tid == 0) ctl->totals[c] = 0;
+      continue;
     }
     unsigned long long sum = 0;
     for (uint32_t i = lo; i < hi; i++) sum += in[i];
@@ -1978,6 +2124,7 @@ void warm_exhaustive_k() {
 }
 void warm_exhaustive_dev(const RoundBuf& R, int k) {
   (void)dev_num_sms();
+  if (R.wide) warm_exhaustive_k<1, 4>();
   if (R.compact) warm_exhaustive_k<1, 3>();
   warm_exhaustive_k<1, 0>();
   if (R.xunit == kXBitsBlocks) warm_exhaustive_k<1, 2>();
@@ -1990,6 +2137,10 @@ void warm_exhaustive_dev(const RoundBuf& R, int k) {
 int launch_exhaustive_dev(const DevTargets& T, const DevPool& P, const RoundBuf& R, const RoundCtl* ctl, int k,
                           cudaStream_t s) {
   int n = 0;
+  if (R.wide) {
+    launch_exhaustive_dev_k<1, 4>(T, P, R, &ctl->totals[3], &ctl->np, s);
+    n++;
+  }
   if (R.compact) {
     launch_exhaustive_dev_k<1, 3>(T, P, R, &ctl->totals[2], &ctl->np, s);
     n++;

@@ -44,6 +44,8 @@ def main():
                     help="A-independent sweeps bit-sliced (1) or one state per lane slot (0)")
     ap.add_argument("--compact", type=int, default=1, choices=[0, 1],
                     help="A-dependent pairs naming at most two of B..L on the compact-state sweep kernel")
+    ap.add_argument("--wide", type=int, default=1, choices=[0, 1],
+                    help="other A-dependent pairs naming at most four of B..L on the wide compact-state kernel")
     ap.add_argument("--graph-rounds", type=int, default=1, choices=[0, 1],
                     help="first-found rounds driven on the device by one CUDA graph (1) or from the host (0; "
                          "ncu profiles no kernel inside a graph with conditional nodes)")
@@ -67,6 +69,7 @@ def main():
         ctx.set_option(z80b.OPT_QC_INDEX, a.qc_index)
         ctx.set_option(z80b.OPT_XINDEP_BITS, a.xindep_bits)
         ctx.set_option(z80b.OPT_COMPACT_SWEEP, a.compact)
+        ctx.set_option(z80b.OPT_WIDE_SWEEP, a.wide)
         ctx.set_option(z80b.OPT_GRAPH_ROUNDS, a.graph_rounds)
         arr, lens, dead, dregs = workloads.c3_targets(a.targets, seed=1)
         targets = [list(map(int, arr[i, :lens[i]])) for i in range(a.targets)]
@@ -88,6 +91,7 @@ def main():
     ctx.set_option(z80b.OPT_QC_INDEX, a.qc_index)
     ctx.set_option(z80b.OPT_XINDEP_BITS, a.xindep_bits)
     ctx.set_option(z80b.OPT_COMPACT_SWEEP, a.compact)
+    ctx.set_option(z80b.OPT_WIDE_SWEEP, a.wide)
     ctx.set_option(z80b.OPT_GRAPH_ROUNDS, a.graph_rounds)
     job, keep = ctx.make_job(workloads.to_lists(arr), dead_flags=z80b.parse_dead_flags(a.dead_flags))
     for i in range(a.steps):

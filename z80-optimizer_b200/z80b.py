@@ -106,6 +106,7 @@ RULE_CB = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void
 OPT_EXH_LANE_STATES, OPT_EXH_CHUNK_BLOCKS, OPT_STREAM_PRIORITY, OPT_QC_INDEX, OPT_XINDEP_BITS = 1, 2, 3, 4, 5
 OPT_COMPACT_SWEEP = 6
 OPT_GRAPH_ROUNDS = 7
+OPT_WIDE_SWEEP = 8
 JOB_NO_EXHAUSTIVE = 1
 ANSWER_TRUNCATED = 1
 
