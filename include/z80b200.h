@@ -220,8 +220,9 @@ int z80b_exhaustive_noalloc(int device, const uint32_t* tgt, const uint8_t* tlen
 #define Z80B_OPT_COMPACT_SWEEP 6    /* pairs naming at most two of B..L on the A/F/B/C-state kernel (1, default) or not (0) */
 #define Z80B_OPT_GRAPH_ROUNDS 7     /* first-found ExhaustiveCheck rounds driven on the device by one CUDA graph (1, default;
                                        not for z80b_search_cb, whose callbacks follow the rounds) or from the host (0) */
-#define Z80B_OPT_WIDE_SWEEP 8       /* other pairs naming at most four of B..L and not SP on the A/F/B/C/H/L/M-state
-                                       kernel (1, default) or not (0) */
+#define Z80B_OPT_WIDE_SWEEP 8       /* other A-dependent pairs naming at most four of B..L and not SP on the
+                                       A/F/B/C/H/L/M-state kernel, and the rest that name neither SP nor the memory
+                                       byte on the A/F/B..L-state kernel (1, default), or neither (0) */
 int z80b_set_option(z80b_ctx* ctx, int option, int value);
 int z80b_get_option(const z80b_ctx* ctx, int option, int* value);
 

@@ -8,7 +8,10 @@
 // unit (wbits_unit in z80b_kernels.cu), restated with its block decoding
 // (WDec), plane layout and dead-flag and dead-register compares, gives the
 // oracle's ExhaustiveCheck verdict with dead registers for A-dependent pairs
-// that the compact state does not take.  Built and run by
+// that the compact state does not take.  (5), (6) The register state (ZB6:
+// A, F, B..L): zb6_step against the full step, and the register-state unit
+// (rbits_unit) restated against the oracle for pairs naming neither SP nor
+// the memory byte that no compact state takes.  Built and run by
 // tests/test_tables.py.
 #include <cstdio>
 #include <random>
@@ -319,6 +322,150 @@ int main() {
     }
     std::printf("OK wide: %d opcodes, %d pairs (%d equivalent, %d with memory, %d reduced sweeps)\n", wide_ops, wp,
                 weq, mem, many);
+  }
+  // (5) the register state (ZB6: A, F, B..L): zb6_step gives the full step's
+  // planes for every opcode naming neither SP nor the memory byte
+  int reg_ops = 0;
+  for (uint32_t op = 0; op < uint32_t(kNumOps); op++) {
+    if (op_regs(uint16_t(op)) & 0xC0u) continue;
+    reg_ops++;
+    for (int rep = 0; rep < 32; rep++) {
+      Z80S st[32];
+      for (int j = 0; j < 32; j++) {
+        const uint64_t r = rng();
+        st[j] = Z80S{uint32_t(r & 0xFF), uint32_t((r >> 8) & 0xFF), uint32_t((r >> 16) & 0xFF),
+                     uint32_t((r >> 24) & 0xFF), uint32_t((r >> 32) & 0xFF), uint32_t((r >> 40) & 0xFF),
+                     uint32_t((r >> 48) & 0xFF), uint32_t((r >> 56) & 0xFF), 0, 0};
+      }
+      const uint32_t imm = uint32_t(rng() & 0xFFFF);
+      ZB full;
+      zb_from(full, st);
+      ZB6 z6;
+      for (int i = 0; i < 8; i++) {
+        z6.a[i] = full.a[i];
+        z6.f[i] = full.f[i];
+        z6.b[i] = full.b[i];
+        z6.c[i] = full.c[i];
+        z6.d[i] = full.d[i];
+        z6.e[i] = full.e[i];
+        z6.h[i] = full.h[i];
+        z6.l[i] = full.l[i];
+      }
+      zb_step(full, op, imm);
+      zb6_step(z6, op, imm);
+      for (int i = 0; i < 8; i++)
+        if (z6.a[i] != full.a[i] || z6.f[i] != full.f[i] || z6.b[i] != full.b[i] || z6.c[i] != full.c[i] ||
+            z6.d[i] != full.d[i] || z6.e[i] != full.e[i] || z6.h[i] != full.h[i] || z6.l[i] != full.l[i]) {
+          std::printf("register-state step differs on op %u (%s)\n", op, op_mnemonic(uint16_t(op)));
+          return 1;
+        }
+    }
+  }
+  // (6) the register-state unit (rbits_unit in z80b_kernels.cu) restated:
+  // per block and 32 values of A, the planes of the decoded state, A always
+  // compared, F under the dead flags, B..L under the dead registers; against
+  // the oracle with dead registers, for A-dependent pairs naming neither SP
+  // nor the memory byte that no compact state takes
+  {
+    int rp = 0, req = 0, five = 0;
+    for (int trial = 0; trial < 40000000 && rp < 400; trial++) {
+      int tn = 1 + int(rng() % 3);
+      int cn = 1 + int(rng() % 2);
+      orc::Instruction ti[3], ci[2];
+      uint32_t tw[3], cw[2];
+      for (int i = 0; i < tn; i++) ti[i] = I[rng() % I.size()];
+      for (int i = 0; i < cn; i++) ci[i] = I[rng() % I.size()];
+      const uint64_t how = rng() % 4;
+      uint8_t dropped_regs = 0;  // registers the dropped instruction names: made dead below
+      if (how == 3) {
+        // the candidate with one more instruction put in that writes no A:
+        // equivalent when what it writes is dead and nothing after reads it
+        orc::Instruction j;
+        do j = I[rng() % I.size()];
+        while (orc::OpWrites(j.op) & orc::regA);
+        cn = 1 + int(rng() % 2);
+        tn = cn + 1;
+        const int at = (rng() & 1) ? tn - 1 : int(rng() % tn);  // last: nothing after it reads what it writes
+        for (int k = 0, m = 0; k < tn; k++) ti[k] = k == at ? j : ci[m++];
+        dropped_regs = uint8_t(op_regs(j.op) & 0x3Fu);
+      } else if (how == 1) {
+        ci[0] = ti[rng() % tn];
+        if (cn == 2) ci[1] = ti[rng() % tn];
+      } else if (how == 2 && tn >= 2) {
+        const int drop = int(rng() % tn);
+        dropped_regs = uint8_t(op_regs(ti[drop].op) & 0x3Fu);
+        cn = 0;
+        for (int i = 0; i < tn; i++)
+          if (i != drop) ci[cn++] = ti[i];
+      }
+      for (int i = 0; i < tn; i++) tw[i] = uint32_t(ti[i].op) | uint32_t(ti[i].imm) << 16;
+      for (int i = 0; i < cn; i++) cw[i] = uint32_t(ci[i].op) | uint32_t(ci[i].imm) << 16;
+      if (seq_aflow(tw, tn) && seq_aflow(cw, cn)) continue;
+      if (compact_id(tw, tn, cw, cn) || wide_id(tw, tn, cw, cn)) continue;
+      uint8_t fp = 0;
+      for (int i = 0; i < tn; i++) fp |= op_regs(insn_op(tw[i]));
+      for (int i = 0; i < cn; i++) fp |= op_regs(insn_op(cw[i]));
+      if (fp & 0xC0u) continue;
+      const uint16_t reads = uint16_t(seq_reads(tw, tn) | seq_reads(cw, cn));
+      const Shape s = shape_of(reads);
+      if (s.nblocks > 65536) continue;
+      rp++;
+      five += __builtin_popcount(fp & 0x3Fu) >= 5 ? 1 : 0;
+      const bool drop_dead = dropped_regs && (how == 3 || (rng() & 1));
+      const uint8_t dead = drop_dead ? uint8_t(0xFF) : uint8_t(rng() & 0xFF);
+      const uint8_t dregs = drop_dead ? uint8_t(dropped_regs | (rng() & 0x3F))
+                                      : uint8_t(rng() % 4 == 0 ? 0 : rng() & 0x3F);
+      const uint32_t keepF = uint8_t(~dead), keepR = ~uint32_t(dregs) & 0x3Fu;
+      bool bad = false;
+      for (uint64_t b = 0; b < s.nblocks && !bad; b++) {
+        const Z80S x = decode(b, s);
+        for (uint32_t a0 = 0; a0 < 256 && !bad; a0 += 32) {
+          ZB6 z;
+          z.a[0] = 0xAAAAAAAAu;
+          z.a[1] = 0xCCCCCCCCu;
+          z.a[2] = 0xF0F0F0F0u;
+          z.a[3] = 0xFF00FF00u;
+          z.a[4] = 0xFFFF0000u;
+          for (int i = 5; i < 8; i++) z.a[i] = ((a0 >> i) & 1u) ? kZBOnes : 0u;
+          zb_set8(z.f, x.f);
+          zb_set8(z.b, x.b);
+          zb_set8(z.c, x.c);
+          zb_set8(z.d, x.d);
+          zb_set8(z.e, x.e);
+          zb_set8(z.h, x.h);
+          zb_set8(z.l, x.l);
+          ZB6 zc = z, zt = z;
+          for (int i = 0; i < cn; i++) zb6_step(zc, insn_op(cw[i]), insn_imm(cw[i]));
+          for (int i = 0; i < tn; i++) zb6_step(zt, insn_op(tw[i]), insn_imm(tw[i]));
+          uint32_t d = 0;
+          for (int i = 0; i < 8; i++) {
+            d |= zc.a[i] ^ zt.a[i];
+            if ((keepF >> i) & 1u) d |= zc.f[i] ^ zt.f[i];
+            if (keepR & 1u) d |= zc.b[i] ^ zt.b[i];
+            if (keepR & 2u) d |= zc.c[i] ^ zt.c[i];
+            if (keepR & 4u) d |= zc.d[i] ^ zt.d[i];
+            if (keepR & 8u) d |= zc.e[i] ^ zt.e[i];
+            if (keepR & 16u) d |= zc.h[i] ^ zt.h[i];
+            if (keepR & 32u) d |= zc.l[i] ^ zt.l[i];
+          }
+          bad = d != 0;
+        }
+      }
+      const bool want = orc::ExhaustiveCheckMaskedRegs(ti, tn, ci, cn, dead, dregs);
+      if (want == bad) {
+        std::printf("register-state unit verdict differs: target %08x %08x %08x (%d) candidate %08x %08x (%d)\n",
+                    tw[0], tn > 1 ? tw[1] : 0, tn > 2 ? tw[2] : 0, tn, cw[0], cn > 1 ? cw[1] : 0, cn);
+        return 1;
+      }
+      req += want ? 1 : 0;
+    }
+    if (reg_ops < 380 || rp < 300 || req < 2 || five < 20) {
+      std::printf("too few register-state opcodes (%d), pairs (%d), equivalences (%d) or five-register pairs (%d)\n",
+                  reg_ops, rp, req, five);
+      return 1;
+    }
+    std::printf("register state: %d opcodes, %d pairs (%d equivalent, %d naming five or six registers)\n", reg_ops, rp,
+                req, five);
   }
   return 0;
 }

@@ -413,84 +413,90 @@ Z80_HD bool zb_acc_step(ZT& z, uint32_t op) {
   return true;
 }
 
+// The cases of the step for every instruction that names no register but
+// A, F, B..L (neither SP nor the memory byte), shared by zb_step and zb6_step.
+#define ZB_REG_CASES \
+    ZB_S7(ZB_LDA, LD_A_B) \
+    ZB_R7(ZB_LDB, LD_B_A) \
+    ZB_R7(ZB_LDC, LD_C_A) \
+    ZB_R7(ZB_LDD, LD_D_A) \
+    ZB_R7(ZB_LDE, LD_E_A) \
+    ZB_R7(ZB_LDH, LD_H_A) \
+    ZB_R7(ZB_LDL, LD_L_A) \
+    ZB_R7(ZB_LDN, LD_A_N) \
+    ZB_S7(ZB_ADD, ADD_A_B) \
+    case ADD_A_N: zb_set8(t8, imm & 0xFFu); zb_add(z, t8, 0u); break; \
+    ZB_S7(ZB_ADC, ADC_A_B) \
+    case ADC_A_N: zb_set8(t8, imm & 0xFFu); zb_add(z, t8, z.f[0]); break; \
+    ZB_S7(ZB_SUB, SUB_B) \
+    case SUB_N: zb_set8(t8, imm & 0xFFu); zb_sub(z, t8, 0u); break; \
+    ZB_S7(ZB_SBC, SBC_A_B) \
+    case SBC_A_N: zb_set8(t8, imm & 0xFFu); zb_sub(z, t8, z.f[0]); break; \
+    ZB_S7(ZB_AND, AND_B) \
+    case AND_N: zb_set8(t8, imm & 0xFFu); zb_and(z, t8); break; \
+    ZB_S7(ZB_XOR, XOR_B) \
+    case XOR_N: zb_set8(t8, imm & 0xFFu); zb_xor(z, t8); break; \
+    ZB_S7(ZB_OR, OR_B) \
+    case OR_N: zb_set8(t8, imm & 0xFFu); zb_or(z, t8); break; \
+    ZB_S7(ZB_CP, CP_B) \
+    case CP_N: zb_set8(t8, imm & 0xFFu); zb_cp(z, t8); break; \
+    ZB_R7(ZB_INC, INC_A) \
+    ZB_R7(ZB_DEC, DEC_A) \
+    ZB_R7(ZB_RLC, RLC_A) \
+    ZB_R7(ZB_RRC, RRC_A) \
+    ZB_R7(ZB_RL, RL_A) \
+    ZB_R7(ZB_RR, RR_A) \
+    ZB_R7(ZB_SLA, SLA_A) \
+    ZB_R7(ZB_SRA, SRA_A) \
+    ZB_R7(ZB_SRL, SRL_A) \
+    ZB_R7(ZB_SLL, SLL_A) \
+    ZB_R7(ZB_BIT, BIT_0_A) ZB_R7(ZB_BIT, BIT_1_A) ZB_R7(ZB_BIT, BIT_2_A) ZB_R7(ZB_BIT, BIT_3_A) \
+    ZB_R7(ZB_BIT, BIT_4_A) ZB_R7(ZB_BIT, BIT_5_A) ZB_R7(ZB_BIT, BIT_6_A) ZB_R7(ZB_BIT, BIT_7_A) \
+    ZB_R7(ZB_RES, RES_0_A) ZB_R7(ZB_RES, RES_1_A) ZB_R7(ZB_RES, RES_2_A) ZB_R7(ZB_RES, RES_3_A) \
+    ZB_R7(ZB_RES, RES_4_A) ZB_R7(ZB_RES, RES_5_A) ZB_R7(ZB_RES, RES_6_A) ZB_R7(ZB_RES, RES_7_A) \
+    ZB_R7(ZB_SET, SET_0_A) ZB_R7(ZB_SET, SET_1_A) ZB_R7(ZB_SET, SET_2_A) ZB_R7(ZB_SET, SET_3_A) \
+    ZB_R7(ZB_SET, SET_4_A) ZB_R7(ZB_SET, SET_5_A) ZB_R7(ZB_SET, SET_6_A) ZB_R7(ZB_SET, SET_7_A) \
+    case INC_BC: zb_inc16(z.b, z.c, false); break; \
+    case INC_DE: zb_inc16(z.d, z.e, false); break; \
+    case INC_HL: zb_inc16(z.h, z.l, false); break; \
+    case DEC_BC: zb_inc16(z.b, z.c, true); break; \
+    case DEC_DE: zb_inc16(z.d, z.e, true); break; \
+    case DEC_HL: zb_inc16(z.h, z.l, true); break; \
+    case ADD_HL_BC: zb_hl16(z, z.c, z.b, 0); break; \
+    case ADD_HL_DE: zb_hl16(z, z.e, z.d, 0); break; \
+    case ADD_HL_HL: zb_hl16(z, z.l, z.h, 0); break; \
+    case EX_DE_HL: \
+      for (int i = 0; i < 8; i++) { \
+        const uint32_t dd = z.d[i], ee = z.e[i]; \
+        z.d[i] = z.h[i]; \
+        z.e[i] = z.l[i]; \
+        z.h[i] = dd; \
+        z.l[i] = ee; \
+      } \
+      break; \
+    case LD_BC_NN: zb_set8(z.b, (imm >> 8) & 0xFFu); zb_set8(z.c, imm & 0xFFu); break; \
+    case LD_DE_NN: zb_set8(z.d, (imm >> 8) & 0xFFu); zb_set8(z.e, imm & 0xFFu); break; \
+    case LD_HL_NN: zb_set8(z.h, (imm >> 8) & 0xFFu); zb_set8(z.l, imm & 0xFFu); break; \
+    case ADC_HL_BC: zb_hl16(z, z.c, z.b, 1); break; \
+    case ADC_HL_DE: zb_hl16(z, z.e, z.d, 1); break; \
+    case ADC_HL_HL: zb_hl16(z, z.l, z.h, 1); break; \
+    case SBC_HL_BC: zb_hl16(z, z.c, z.b, 2); break; \
+    case SBC_HL_DE: zb_hl16(z, z.e, z.d, 2); break; \
+    case SBC_HL_HL: zb_hl16(z, z.l, z.h, 2); break; \
+  /* end of ZB_REG_CASES */
+
 // One instruction on the 32 states of z (op and imm are the same for all).
 template <class ZT>
 Z80_HD void zb_step(ZT& z, uint32_t op, uint32_t imm) {
   uint32_t t8[8];
   switch (op) {
-    ZB_S7(ZB_LDA, LD_A_B)
-    ZB_R7(ZB_LDB, LD_B_A)
-    ZB_R7(ZB_LDC, LD_C_A)
-    ZB_R7(ZB_LDD, LD_D_A)
-    ZB_R7(ZB_LDE, LD_E_A)
-    ZB_R7(ZB_LDH, LD_H_A)
-    ZB_R7(ZB_LDL, LD_L_A)
-    ZB_R7(ZB_LDN, LD_A_N)
-    ZB_S7(ZB_ADD, ADD_A_B)
-    case ADD_A_N: zb_set8(t8, imm & 0xFFu); zb_add(z, t8, 0u); break;
-    ZB_S7(ZB_ADC, ADC_A_B)
-    case ADC_A_N: zb_set8(t8, imm & 0xFFu); zb_add(z, t8, z.f[0]); break;
-    ZB_S7(ZB_SUB, SUB_B)
-    case SUB_N: zb_set8(t8, imm & 0xFFu); zb_sub(z, t8, 0u); break;
-    ZB_S7(ZB_SBC, SBC_A_B)
-    case SBC_A_N: zb_set8(t8, imm & 0xFFu); zb_sub(z, t8, z.f[0]); break;
-    ZB_S7(ZB_AND, AND_B)
-    case AND_N: zb_set8(t8, imm & 0xFFu); zb_and(z, t8); break;
-    ZB_S7(ZB_XOR, XOR_B)
-    case XOR_N: zb_set8(t8, imm & 0xFFu); zb_xor(z, t8); break;
-    ZB_S7(ZB_OR, OR_B)
-    case OR_N: zb_set8(t8, imm & 0xFFu); zb_or(z, t8); break;
-    ZB_S7(ZB_CP, CP_B)
-    case CP_N: zb_set8(t8, imm & 0xFFu); zb_cp(z, t8); break;
-    ZB_R7(ZB_INC, INC_A)
-    ZB_R7(ZB_DEC, DEC_A)
-    ZB_R7(ZB_RLC, RLC_A)
-    ZB_R7(ZB_RRC, RRC_A)
-    ZB_R7(ZB_RL, RL_A)
-    ZB_R7(ZB_RR, RR_A)
-    ZB_R7(ZB_SLA, SLA_A)
-    ZB_R7(ZB_SRA, SRA_A)
-    ZB_R7(ZB_SRL, SRL_A)
-    ZB_R7(ZB_SLL, SLL_A)
-    ZB_R7(ZB_BIT, BIT_0_A) ZB_R7(ZB_BIT, BIT_1_A) ZB_R7(ZB_BIT, BIT_2_A) ZB_R7(ZB_BIT, BIT_3_A)
-    ZB_R7(ZB_BIT, BIT_4_A) ZB_R7(ZB_BIT, BIT_5_A) ZB_R7(ZB_BIT, BIT_6_A) ZB_R7(ZB_BIT, BIT_7_A)
-    ZB_R7(ZB_RES, RES_0_A) ZB_R7(ZB_RES, RES_1_A) ZB_R7(ZB_RES, RES_2_A) ZB_R7(ZB_RES, RES_3_A)
-    ZB_R7(ZB_RES, RES_4_A) ZB_R7(ZB_RES, RES_5_A) ZB_R7(ZB_RES, RES_6_A) ZB_R7(ZB_RES, RES_7_A)
-    ZB_R7(ZB_SET, SET_0_A) ZB_R7(ZB_SET, SET_1_A) ZB_R7(ZB_SET, SET_2_A) ZB_R7(ZB_SET, SET_3_A)
-    ZB_R7(ZB_SET, SET_4_A) ZB_R7(ZB_SET, SET_5_A) ZB_R7(ZB_SET, SET_6_A) ZB_R7(ZB_SET, SET_7_A)
-    case INC_BC: zb_inc16(z.b, z.c, false); break;
-    case INC_DE: zb_inc16(z.d, z.e, false); break;
-    case INC_HL: zb_inc16(z.h, z.l, false); break;
+    ZB_REG_CASES
     case INC_SP: zb_incsp(z.sp, false); break;
-    case DEC_BC: zb_inc16(z.b, z.c, true); break;
-    case DEC_DE: zb_inc16(z.d, z.e, true); break;
-    case DEC_HL: zb_inc16(z.h, z.l, true); break;
     case DEC_SP: zb_incsp(z.sp, true); break;
-    case ADD_HL_BC: zb_hl16(z, z.c, z.b, 0); break;
-    case ADD_HL_DE: zb_hl16(z, z.e, z.d, 0); break;
-    case ADD_HL_HL: zb_hl16(z, z.l, z.h, 0); break;
     case ADD_HL_SP: zb_hl16(z, z.sp, z.sp + 8, 0); break;
-    case EX_DE_HL:
-      for (int i = 0; i < 8; i++) {
-        const uint32_t dd = z.d[i], ee = z.e[i];
-        z.d[i] = z.h[i];
-        z.e[i] = z.l[i];
-        z.h[i] = dd;
-        z.l[i] = ee;
-      }
-      break;
     case LD_SP_HL: for (int i = 0; i < 8; i++) { z.sp[i] = z.l[i]; z.sp[i + 8] = z.h[i]; } break;
-    case LD_BC_NN: zb_set8(z.b, (imm >> 8) & 0xFFu); zb_set8(z.c, imm & 0xFFu); break;
-    case LD_DE_NN: zb_set8(z.d, (imm >> 8) & 0xFFu); zb_set8(z.e, imm & 0xFFu); break;
-    case LD_HL_NN: zb_set8(z.h, (imm >> 8) & 0xFFu); zb_set8(z.l, imm & 0xFFu); break;
     case LD_SP_NN: for (int i = 0; i < 16; i++) z.sp[i] = ((imm >> i) & 1u) ? kZBOnes : 0u; break;
-    case ADC_HL_BC: zb_hl16(z, z.c, z.b, 1); break;
-    case ADC_HL_DE: zb_hl16(z, z.e, z.d, 1); break;
-    case ADC_HL_HL: zb_hl16(z, z.l, z.h, 1); break;
     case ADC_HL_SP: zb_hl16(z, z.sp, z.sp + 8, 1); break;
-    case SBC_HL_BC: zb_hl16(z, z.c, z.b, 2); break;
-    case SBC_HL_DE: zb_hl16(z, z.e, z.d, 2); break;
-    case SBC_HL_HL: zb_hl16(z, z.l, z.h, 2); break;
     case SBC_HL_SP: zb_hl16(z, z.sp, z.sp + 8, 2); break;
     // memory ops on the single byte M (exec.go:883-1028)
     case LD_A_HLI: zb_copy8(z.a, z.m); break;
@@ -610,6 +616,22 @@ Z80_HD void zb4_step(ZB4& z, uint32_t op, uint32_t imm) {
     case INC_BC: zb_inc16(z.b, z.c, false); break;
     case DEC_BC: zb_inc16(z.b, z.c, true); break;
     case LD_BC_NN: zb_set8(z.b, (imm >> 8) & 0xFFu); zb_set8(z.c, imm & 0xFFu); break;
+    default: zb_acc_step(z, op); break;
+  }
+}
+
+// The register state: A, F and B..L, for pairs whose programs name neither
+// SP nor the memory byte (no renaming: all six registers are held).
+struct ZB6 {
+  uint32_t a[8], f[8], b[8], c[8], d[8], e[8], h[8], l[8];
+};
+// The step on ZB6: the cases of zb_step for every instruction that names
+// neither SP nor the memory byte; any other opcode leaves the state
+// unchanged and must not occur.
+Z80_HD void zb6_step(ZB6& z, uint32_t op, uint32_t imm) {
+  uint32_t t8[8];
+  switch (op) {
+    ZB_REG_CASES
     default: zb_acc_step(z, op); break;
   }
 }

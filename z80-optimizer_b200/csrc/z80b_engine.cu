@@ -158,8 +158,8 @@ struct z80b_ctx {
   // pipeline scratch
   DBuf cnt_f, cnt_m, cnt_all, base, meta, surv, sdiff, checks;
   DBuf next, win, windiff, spec, spec2, wlen, wend, cdone;
-  DBuf pairs, pair_src, nchunks, cbase, nchunks_x, cbase_x, nchunks_c, cbase_c, nchunks_w, cbase_w, rejected, npairs,
-      counter, states;
+  DBuf pairs, pair_src, nchunks, cbase, nchunks_x, cbase_x, nchunks_c, cbase_c, nchunks_w, cbase_w, nchunks_r,
+      cbase_r, rejected, npairs, counter, states;
   DBuf rcnt, rbase, rules, checked, surv_target, midpass, flag;
   DBuf cub_tmp;
   DBuf hits, nhits, fpq;
@@ -580,8 +580,11 @@ int sweep_round(z80b_ctx* ctx, const DevTargets& T, const DevPool& P, const Roun
   CKR(scan(ctx, R.nchunks, R.cbase, np));
   CKR(scan(ctx, R.nchunks_x, R.cbase_x, np));
   if (R.compact) CKR(scan(ctx, R.nchunks_c, R.cbase_c, np));
-  if (R.wide) CKR(scan(ctx, R.nchunks_w, R.cbase_w, np));
-  unsigned long long last[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (R.wide) {
+    CKR(scan(ctx, R.nchunks_w, R.cbase_w, np));
+    CKR(scan(ctx, R.nchunks_r, R.cbase_r, np));
+  }
+  unsigned long long last[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   CK(cudaMemcpyAsync(&last[0], R.cbase + (np - 1), 8, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(&last[1], R.nchunks + (np - 1), 8, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(&last[2], R.cbase_x + (np - 1), 8, cudaMemcpyDeviceToHost, s));
@@ -593,14 +596,16 @@ int sweep_round(z80b_ctx* ctx, const DevTargets& T, const DevPool& P, const Roun
   if (R.wide) {
     CK(cudaMemcpyAsync(&last[6], R.cbase_w + (np - 1), 8, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(&last[7], R.nchunks_w + (np - 1), 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&last[8], R.cbase_r + (np - 1), 8, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&last[9], R.nchunks_r + (np - 1), 8, cudaMemcpyDeviceToHost, s));
   }
   CK(cudaStreamSynchronize(s));
-  CK(cudaMemsetAsync(R.counter, 0, 32, s));
-  trace("sweep: %u pairs, %llu + %llu + %llu + %llu chunks", np, last[0] + last[1], last[2] + last[3],
-        last[4] + last[5], last[6] + last[7]);
+  CK(cudaMemsetAsync(R.counter, 0, 40, s));
+  trace("sweep: %u pairs, %llu + %llu + %llu + %llu + %llu chunks", np, last[0] + last[1], last[2] + last[3],
+        last[4] + last[5], last[6] + last[7], last[8] + last[9]);
   int ke = kbegin(ctx, 1);
   const int nl = launch_exhaustive(T, P, R, np, last[0] + last[1], last[2] + last[3], last[4] + last[5],
-                                   last[6] + last[7], ctx->exh_k, s, &ctx->sweep_kernels);
+                                   last[6] + last[7], last[8] + last[9], ctx->exh_k, s, &ctx->sweep_kernels);
   kend(ctx, ke);
   CKR(check_launch(ctx, "exhaustive"));
   if (nl > 1) ctx->launches += uint32_t(nl - 1);
@@ -680,7 +685,7 @@ int rounds_on_device(z80b_ctx* ctx, RoundGraph& g, const DevTargets& T, const De
     trace("round loop captured (%s pass)", ps ? "length-2" : "length-1");
   }
   // build, scan, [rescan], sweeps, resolve
-  const int per_iter = (ps ? 3 : 2) + 1 + 2 + (R.compact ? 1 : 0) + (R.wide ? 1 : 0);
+  const int per_iter = (ps ? 3 : 2) + 1 + 2 + (R.compact ? 1 : 0) + (R.wide ? 2 : 0);
   CK(cudaMemsetAsync(ctl, 0, sizeof(RoundCtl), s));
   int ke = kbegin(ctx, 1);
   CK(cudaGraphLaunch(g.exec, s));
@@ -693,7 +698,7 @@ int rounds_on_device(z80b_ctx* ctx, RoundGraph& g, const DevTargets& T, const De
   *rounds += h.rounds;
   *pairs += h.pairs;
   ctx->launches += h.iters * uint32_t(per_iter);
-  uint32_t mask = (R.compact ? kSweepCompact : 0u) | (R.wide ? kSweepWide : 0u) | kSweepBits;
+  uint32_t mask = (R.compact ? kSweepCompact : 0u) | (R.wide ? kSweepWide | kSweepRegs : 0u) | kSweepBits;
   if (R.xunit == kXBitsBlocks) mask |= kSweepXBits;
   else mask |= kSweepScalarK1 << (ctx->exh_k == 1 ? 0 : ctx->exh_k == 2 ? 1 : ctx->exh_k == 8 ? 3 : 2);
   ctx->sweep_kernels |= mask;
@@ -732,7 +737,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
   CK(ctx->checked.ensure(8));
   CK(ctx->states.ensure(16));
   CK(ctx->npairs.ensure(4));
-  CK(ctx->counter.ensure(32));
+  CK(ctx->counter.ensure(40));
   CK(cudaMemsetAsync(ctx->checks.p, 0, 8, s));
   CK(cudaMemsetAsync(ctx->checked.p, 0, 8, s));
   CK(cudaMemsetAsync(ctx->states.p, 0, 16, s));
@@ -807,6 +812,8 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
     if (ctx->wide) {
       CK(ctx->nchunks_w.ensure(8 * cap));
       CK(ctx->cbase_w.ensure(8 * cap));
+      CK(ctx->nchunks_r.ensure(8 * cap));
+      CK(ctx->cbase_r.ensure(8 * cap));
     }
     CK(ctx->rejected.ensure(4 * cap));
     CK(ctx->wlen.ensure(cap));
@@ -839,6 +846,8 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
     R.wide = mode == Z80B_MODE_FIRST && ctx->wide ? 1u : 0u;
     R.nchunks_w = R.wide ? ctx->nchunks_w.as<unsigned long long>() : nullptr;
     R.cbase_w = R.wide ? ctx->cbase_w.as<unsigned long long>() : nullptr;
+    R.nchunks_r = R.wide ? ctx->nchunks_r.as<unsigned long long>() : nullptr;
+    R.cbase_r = R.wide ? ctx->cbase_r.as<unsigned long long>() : nullptr;
     // rounds on the device (one graph) unless the caller takes answers
     // round by round (streaming callbacks)
     const bool dev_rounds = ctx->graph_rounds && !opts.rep;
@@ -978,6 +987,8 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
     R.wide = mode == Z80B_MODE_FIRST && ctx->wide ? 1u : 0u;
     R.nchunks_w = R.wide ? ctx->nchunks_w.as<unsigned long long>() : nullptr;
     R.cbase_w = R.wide ? ctx->cbase_w.as<unsigned long long>() : nullptr;
+    R.nchunks_r = R.wide ? ctx->nchunks_r.as<unsigned long long>() : nullptr;
+    R.cbase_r = R.wide ? ctx->cbase_r.as<unsigned long long>() : nullptr;
     if (S) {
       launch_surv_targets(q, n, ctx->surv_target.as<uint32_t>(), s);
       CKR(check_launch(ctx, "surv_targets"));
@@ -1484,7 +1495,7 @@ int z80b_verify_pairs(z80b_ctx* ctx, const uint32_t* tgt, const uint8_t* tlens, 
     CK(ctx->cbase.ensure(8ull * n));
     CK(ctx->cbase_x.ensure(8ull * n));
     CK(ctx->rejected.ensure(4ull * n));
-    CK(ctx->counter.ensure(32));
+    CK(ctx->counter.ensure(40));
     CK(ctx->states.ensure(16));
     CK(cudaMemcpyAsync(ctx->pairs.p, pr.data(), sizeof(PairRec) * n, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(ctx->cbase.p, cb.data(), 8ull * n, cudaMemcpyHostToDevice, s));
@@ -1498,7 +1509,7 @@ int z80b_verify_pairs(z80b_ctx* ctx, const uint32_t* tgt, const uint8_t* tlens, 
     R.rejected = ctx->rejected.as<uint32_t>();
     R.counter = ctx->counter.as<unsigned long long>();
     R.states = ctx->states.as<unsigned long long>();
-    const int nl = launch_exhaustive(T, P, R, n, tot, totx, 0, 0, ctx->exh_k, s);
+    const int nl = launch_exhaustive(T, P, R, n, tot, totx, 0, 0, 0, ctx->exh_k, s);
     CKR(check_launch(ctx, "exhaustive"));
     if (nl > 1) ctx->launches += uint32_t(nl - 1);
     std::vector<uint32_t> rej(n);
@@ -1589,6 +1600,7 @@ static void sweep_kernel_names(uint32_t mask, char* out, size_t cap) {
   if (mask & kSweepXBits) add("k_exhaustive<1,2>");
   if (mask & kSweepCompact) add("k_exhaustive<1,3>");
   if (mask & kSweepWide) add("k_exhaustive<1,4>");
+  if (mask & kSweepRegs) add("k_exhaustive<1,5>");
   const char* scalar[4] = {"k_exhaustive<1,1>", "k_exhaustive<2,1>", "k_exhaustive<4,1>", "k_exhaustive<8,1>"};
   for (int i = 0; i < 4; i++)
     if (mask & (kSweepScalarK1 << i)) add(scalar[i]);

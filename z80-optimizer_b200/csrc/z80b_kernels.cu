@@ -174,6 +174,16 @@ __device__ __forceinline__ uint8_t pair_cmap(const DevTargets& T, uint32_t t, co
 // pair's instructions name at most four of B..L and not SP, and all rename
 // onto B, C, H and L (wide_map); 0 otherwise.
 constexpr uint8_t kWideClass = 0x80u;
+// Register-state sweep: the pair's instructions name neither SP nor the
+// memory byte.
+constexpr uint8_t kRegClass = 0x40u;
+__device__ __forceinline__ bool pair_regstate(const DevTargets& T, uint32_t t, const DevPool& P, uint32_t c) {
+  const uint32_t tl = target_len(T, t), cl = pool_len(P, c);
+  uint32_t fp = 0;
+  for (uint32_t i = 0; i < tl; i++) fp |= g_opregs[T.insn[(size_t)t * T.stride + i] & 0xFFFFu];
+  for (uint32_t i = 0; i < cl; i++) fp |= g_opregs[P.insn[(size_t)c * P.stride + i] & 0xFFFFu];
+  return (fp & 0xC0u) == 0u;
+}
 __device__ __forceinline__ uint8_t pair_wmap(const DevTargets& T, uint32_t t, const DevPool& P, uint32_t c) {
   const uint32_t tl = target_len(T, t), cl = pool_len(P, c);
   const uint32_t* tw = T.insn + (size_t)t * T.stride;
@@ -208,12 +218,17 @@ __device__ __forceinline__ unsigned long long chunks_for(unsigned long long nb, 
 __device__ __forceinline__ void set_chunks(const RoundBuf& R, uint32_t p, const PairRec& pr) {
   const unsigned long long c = chunks_for(pair_units(pr.nblocks, pr.keepR, R.xunit), R.chunk_blocks);
   const bool xind = (pr.keepR & kXIndep) != 0;
-  const bool wide = (pr.cmap & kWideClass) != 0;  // only set when R.wide
-  const bool comp = pr.cmap != 0 && !wide;        // only set when R.compact
-  R.nchunks[p] = (xind || comp || wide) ? 0ull : c;
-  R.nchunks_x[p] = (xind && !comp && !wide) ? c : 0ull;
+  const bool wide = (pr.cmap & kWideClass) != 0;     // only set when R.wide
+  const bool regs = pr.cmap == kRegClass;            // only set when R.wide
+  const bool comp = pr.cmap != 0 && !wide && !regs;  // only set when R.compact
+  const bool other = comp || wide || regs;
+  R.nchunks[p] = (xind || other) ? 0ull : c;
+  R.nchunks_x[p] = (xind && !other) ? c : 0ull;
   if (R.compact) R.nchunks_c[p] = comp ? c : 0ull;
-  if (R.wide) R.nchunks_w[p] = wide ? c : 0ull;
+  if (R.wide) {
+    R.nchunks_w[p] = wide ? c : 0ull;
+    R.nchunks_r[p] = regs ? c : 0ull;
+  }
 }
 __device__ __forceinline__ unsigned long long chunks_for(unsigned long long nb, uint32_t cb) {
   unsigned long long c = (nb + cb - 1) / cb;
@@ -521,6 +536,8 @@ __device__ __forceinline__ void put_pair(const RoundBuf& R, uint32_t p, const De
     if (R.compact) pr.cmap = pair_cmap(T, t, P, c);
     // the wide state: A-dependent pairs only
     if (!pr.cmap && R.wide && !(pr.keepR & kXIndep)) pr.cmap = pair_wmap(T, t, P, c);
+    // the register state: the rest that name neither SP nor the memory byte
+    if (!pr.cmap && R.wide && pair_regstate(T, t, P, c)) pr.cmap = kRegClass;
   }
   R.pairs[p] = pr;
   R.pair_src[p] = src;
@@ -1099,6 +1116,152 @@ __device__ __forceinline__ bool wbits_unit(unsigned long long u, unsigned long l
   }
   return valid && zbw_diff(z, sm, keepF, cmp) != 0u;
 }
+// Register-state sweeps (pairs naming neither SP nor the memory byte that
+// no compact state takes): the layouts of bits_unit (A-dependent pairs) and
+// xbits_unit (A-independent ones) on ZB6 (A, F, B..L), no renaming.
+constexpr int kRegWords = 64;  // planes saved per lane
+__device__ __forceinline__ void zb6_init(ZB6& z, const Z80S& x) {
+  zb_set8(z.f, x.f);
+  zb_set8(z.b, x.b);
+  zb_set8(z.c, x.c);
+  zb_set8(z.d, x.d);
+  zb_set8(z.e, x.e);
+  zb_set8(z.h, x.h);
+  zb_set8(z.l, x.l);
+}
+__device__ __forceinline__ void zb6_save(const ZB6& z, uint32_t* s) {
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    s[(0 + i) * 32] = z.a[i];
+    s[(8 + i) * 32] = z.f[i];
+    s[(16 + i) * 32] = z.b[i];
+    s[(24 + i) * 32] = z.c[i];
+    s[(32 + i) * 32] = z.d[i];
+    s[(40 + i) * 32] = z.e[i];
+    s[(48 + i) * 32] = z.h[i];
+    s[(56 + i) * 32] = z.l[i];
+  }
+}
+__device__ __forceinline__ uint32_t zb6_diff(const ZB6& z, const uint32_t* s, uint32_t keepF, uint32_t keepR) {
+  uint32_t d = 0;
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    d |= z.a[i] ^ s[(0 + i) * 32];
+    if ((keepF >> i) & 1u) d |= z.f[i] ^ s[(8 + i) * 32];
+    if (keepR & 1u) d |= z.b[i] ^ s[(16 + i) * 32];
+    if (keepR & 2u) d |= z.c[i] ^ s[(24 + i) * 32];
+    if (keepR & 4u) d |= z.d[i] ^ s[(32 + i) * 32];
+    if (keepR & 8u) d |= z.e[i] ^ s[(40 + i) * 32];
+    if (keepR & 16u) d |= z.h[i] ^ s[(48 + i) * 32];
+    if (keepR & 32u) d |= z.l[i] ^ s[(56 + i) * 32];
+  }
+  return d;
+}
+// A-dependent: lane l takes block 4u + l/8 and A = 32(l % 8) .. +31.
+__device__ __forceinline__ bool rbits_unit(unsigned long long u, unsigned long long nblocks, const BDec& bd,
+                                           uint32_t pw, int tl, int cl, uint32_t keepF, uint32_t keepR, uint32_t* sm) {
+  const unsigned lane = lane_id();
+  const unsigned long long blk = u * kBitsBlocks + (lane >> 3);
+  const bool valid = blk < nblocks;
+  const Z80S x = bdec_state(bd, valid ? blk : u * kBitsBlocks, g_rep, g_repsp);
+  const uint32_t a0 = (lane & 7u) * 32u;
+  ZB6 z;
+  auto init = [&]() {
+    z.a[0] = 0xAAAAAAAAu;
+    z.a[1] = 0xCCCCCCCCu;
+    z.a[2] = 0xF0F0F0F0u;
+    z.a[3] = 0xFF00FF00u;
+    z.a[4] = 0xFFFF0000u;
+    z.a[5] = (a0 & 32u) ? kZBOnes : 0u;
+    z.a[6] = (a0 & 64u) ? kZBOnes : 0u;
+    z.a[7] = (a0 & 128u) ? kZBOnes : 0u;
+    zb6_init(z, x);
+  };
+  init();
+#pragma unroll 1
+  for (int st = 0; st < tl + cl; st++) {
+    if (st == cl) {
+      zb6_save(z, sm);
+      init();
+    }
+    const int src = st < cl ? tl + st : st - cl;
+    const uint32_t w = __shfl_sync(kFull, pw, src);
+    zb6_step(z, w & 0xFFFFu, w >> 16);
+  }
+  return valid && zb6_diff(z, sm, keepF, keepR) != 0u;
+}
+// A-independent: lane l takes the 32 A-blocks u*1024 + 32l .. +31 as one
+// state word, at A = 0 and then A = 1; the low 5 bits of the block index
+// move the last swept register rlast (its low 5 bits in a full sweep, its
+// 32 representative values in a reduced one) or, with none, the carry.
+__device__ __forceinline__ void zb6_set_reg(ZB6& z, int r, const uint32_t (&pl)[8]) {
+  switch (r) {
+    case 0: zb_copy8(z.b, pl); break;
+    case 1: zb_copy8(z.c, pl); break;
+    case 2: zb_copy8(z.d, pl); break;
+    case 3: zb_copy8(z.e, pl); break;
+    case 4: zb_copy8(z.h, pl); break;
+    case 5: zb_copy8(z.l, pl); break;
+    default: break;
+  }
+}
+__device__ __forceinline__ bool rxbits_unit(unsigned long long u, unsigned long long nblocks, bool reduced, int nx,
+                                            int rlast, const BDec& bd, uint32_t pw, int tl, int cl, uint32_t keepF,
+                                            uint32_t keepR, uint32_t* sm) {
+  const unsigned lane = lane_id();
+  const unsigned long long g0 = u * kXBitsBlocks + (unsigned long long)lane * 32ull;
+  const uint32_t valid = g0 >= nblocks ? 0u
+                         : (nblocks - g0 >= 32ull ? 0xFFFFFFFFu : ((1u << uint32_t(nblocks - g0)) - 1u));
+  const Z80S x = bdec_state(bd, g0 < nblocks ? g0 : 0ull, g_rep, g_repsp);
+  uint32_t vp[8];
+  if (reduced) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) vp[i] = __ballot_sync(kFull, (g_rep[lane] >> i) & 1u);
+  } else {
+    uint32_t v = 0u;
+    switch (rlast) {
+      case 0: v = x.b; break;
+      case 1: v = x.c; break;
+      case 2: v = x.d; break;
+      case 3: v = x.e; break;
+      case 4: v = x.h; break;
+      case 5: v = x.l; break;
+      default: break;
+    }
+    vp[0] = 0xAAAAAAAAu;
+    vp[1] = 0xCCCCCCCCu;
+    vp[2] = 0xF0F0F0F0u;
+    vp[3] = 0xFF00FF00u;
+    vp[4] = 0xFFFF0000u;
+#pragma unroll
+    for (int i = 5; i < 8; i++) vp[i] = ((v >> i) & 1u) ? kZBOnes : 0u;
+  }
+  ZB6 z;
+  bool bad = false;
+#pragma unroll 1
+  for (uint32_t abit = 0; abit < 2u; abit++) {
+    auto init = [&]() {
+      zb_set8(z.a, abit);
+      zb6_init(z, x);
+      if (nx >= 1) zb6_set_reg(z, rlast, vp);
+      else z.f[0] = 0xAAAAAAAAu;
+    };
+    init();
+#pragma unroll 1
+    for (int st = 0; st < tl + cl; st++) {
+      if (st == cl) {
+        zb6_save(z, sm);
+        init();
+      }
+      const int src = st < cl ? tl + st : st - cl;
+      const uint32_t w = __shfl_sync(kFull, pw, src);
+      zb6_step(z, w & 0xFFFFu, w >> 16);
+    }
+    bad = bad || (zb6_diff(z, sm, keepF, keepR) & valid) != 0u;
+  }
+  return bad;
+}
+
 // One unit (128 A-blocks at A = 0, 1) of an A-independent sweep, for the
 // A-independent sweep kernel; kept out of line (that kernel compiles without
 // register spills at every K this way).
@@ -1129,14 +1292,18 @@ __device__ __noinline__ bool xindep_unit(unsigned long long first, unsigned long
 // depend on A), CLS 1 the A-independent ones (K states per lane per
 // dispatch), CLS 2 the A-independent ones bit-sliced, CLS 3 the pairs whose
 // registers fit the compact state (three blocks per SM), CLS 4 the
-// A-dependent ones that fit the wide compact state (two blocks per SM); each class
+// A-dependent ones that fit the wide compact state (two blocks per SM), CLS
+// 5 the rest that name neither SP nor the memory byte, on A, F and B..L; each class
 // draws chunks from its own numbering and dispenser.  Kept apart so that
 // neither path's registers weigh on the other.
 // dev_total / dev_np (device-driven rounds): the class's chunk total and the
 // round's pair count are read from the device instead of total / npairs.
 // chunks_per_warp: chunks a warp takes before its block retires.
+#ifndef Z80B_REG_BLOCKS
+#define Z80B_REG_BLOCKS 2
+#endif
 template <int K, int CLS>
-__global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : (CLS == 4 ? 2 : 1))
+__global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : (CLS == 4 ? 2 : (CLS == 5 ? Z80B_REG_BLOCKS : 1)))
     k_exhaustive(DevTargets T, DevPool P, RoundBuf R, uint32_t npairs, unsigned long long total,
                  const unsigned long long* __restrict__ dev_total, const uint32_t* __restrict__ dev_np,
                  int chunks_per_warp) {
@@ -1147,7 +1314,7 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : (CLS == 4 ? 2 : 1))
   }
   constexpr bool XI = CLS != 0;
   const unsigned long long* __restrict__ cbase =
-      CLS == 4 ? R.cbase_w : (CLS == 3 ? R.cbase_c : (XI ? R.cbase_x : R.cbase));
+      CLS == 5 ? R.cbase_r : (CLS == 4 ? R.cbase_w : (CLS == 3 ? R.cbase_c : (XI ? R.cbase_x : R.cbase)));
   const unsigned lane = lane_id();
   unsigned long long my_states = 0, my_eval = 0;
   // At most kChunksPerWarp chunks per warp, then the block retires: the grid
@@ -1207,7 +1374,44 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : (CLS == 4 ? 2 : 1))
 
     bool bad = false;
     bool stopped = false;  // left the loop on the pair's flag (rejected or cancelled elsewhere)
-    if constexpr (CLS == 4) {
+    if constexpr (CLS == 5) {
+      // the register state (A, F, B..L), programs as they are
+      extern __shared__ uint32_t zsm[];
+      uint32_t* sm = zsm + (threadIdx.x >> 5) * (kRegWords * 32) + lane;
+      if (pr.keepR & kXIndep) {
+        int rlast = -1;  // the register of the last swept field (the fastest)
+#pragma unroll
+        for (int r = 0; r < 6; r++)
+          if (slot[r] == nx - 1) rlast = r;
+        for (unsigned long long u = u0; u < u1; u++) {
+          const unsigned long long first = u * kXBitsBlocks;
+          const unsigned long long nb = (pr.nblocks - first < kXBitsBlocks) ? pr.nblocks - first : kXBitsBlocks;
+          bad = rxbits_unit(u, pr.nblocks, reduced, nx, rlast, bd, pw, int(tl), int(cl), pr.keepF, pr.keepR, sm) ||
+                bad;
+          my_states += 256ull * nb;
+          my_eval += 2ull * nb;
+          if (__any_sync(kFull, bad)) break;
+          if (__shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0)) {
+            stopped = true;
+            break;
+          }
+        }
+      } else {
+        for (unsigned long long u = u0; u < u1; u++) {
+          const unsigned long long first = u * kBitsBlocks;
+          const unsigned long long nb = (pr.nblocks - first < kBitsBlocks) ? pr.nblocks - first : kBitsBlocks;
+          bad = rbits_unit(u, pr.nblocks, bd, pw, int(tl), int(cl), pr.keepF, pr.keepR, sm) || bad;
+          my_states += 256ull * nb;
+          my_eval += 256ull * nb;
+          if (__any_sync(kFull, bad)) break;
+          if ((u & 15ull) == 15ull &&
+              __shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0)) {
+            stopped = true;
+            break;
+          }
+        }
+      }
+    } else if constexpr (CLS == 4) {
       // the wide compact state, the programs renamed onto B, C, H and L
       const uint32_t e = (pr.cmap & ~uint32_t(kWideClass)) - 1u;
       if (lane < tl + cl) pw = (uint32_t(uint16_t(g_wren[e][pw & 0xFFFFu]))) | (pw & 0xFFFF0000u);
@@ -1968,7 +2172,8 @@ void launch_pairs_from_survivors(const DevTargets& T, const DevPool& P, const QC
 // Shared memory of a sweep kernel (bit-sliced classes): the candidate's
 // output planes, one column of words per lane.
 constexpr int exhaustive_smem(int cls) {
-  return cls == 1 ? 0 : kBlock * (cls == 3 ? kCompactWords : (cls == 4 ? kWideWords : kBitsWords)) * 4;
+  return cls == 1 ? 0
+                  : kBlock * (cls == 3 ? kCompactWords : (cls == 4 ? kWideWords : (cls == 5 ? kRegWords : kBitsWords))) * 4;
 }
 // Resident blocks per SM of a sweep kernel on the current device (its
 // shared-memory limit raised first), cached per device.
@@ -2008,10 +2213,16 @@ void launch_exhaustive_dev_k(const DevTargets& T, const DevPool& P, const RoundB
 
 int launch_exhaustive(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
                       unsigned long long total_b, unsigned long long total_x, unsigned long long total_c,
-                      unsigned long long total_w, int k, cudaStream_t s, uint32_t* kernels) {
+                      unsigned long long total_w, unsigned long long total_r, int k, cudaStream_t s,
+                      uint32_t* kernels) {
   if (!npairs) return 0;
   int n = 0;
   uint32_t mask = 0;
+  if (total_r) {
+    launch_exhaustive_k<1, 5>(T, P, R, npairs, total_r, s);
+    mask |= kSweepRegs;
+    n++;
+  }
   if (total_w) {
     launch_exhaustive_k<1, 4>(T, P, R, npairs, total_w, s);
     mask |= kSweepWide;
@@ -2076,19 +2287,21 @@ __global__ void __launch_bounds__(kScanThreads) k_round_scan(RoundBuf R, RoundCt
       ctl->rounds += 1;
       ctl->pairs += np;
     }
-    R.counter[0] = R.counter[1] = R.counter[2] = R.counter[3] = 0;
+    R.counter[0] = R.counter[1] = R.counter[2] = R.counter[3] = R.counter[4] = 0;
     if (np == 0 || over) {
-      ctl->totals[0] = ctl->totals[1] = ctl->totals[2] = ctl->totals[3] = 0;
+      ctl->totals[0] = ctl->totals[1] = ctl->totals[2] = ctl->totals[3] = ctl->totals[4] = 0;
       if (!refill || *refill == 0) cudaGraphSetConditional(loop, 0);
     }
   }
   if (np == 0 || over) return;
   const uint32_t per = (np + kScanThreads - 1) / kScanThreads;
   const uint32_t lo = min(tid * per, np), hi = min(lo + per, np);
-  for (int c = 0; c < 4; c++) {
-    const unsigned long long* in = c == 0 ? R.nchunks : (c == 1 ? R.nchunks_x : (c == 2 ? R.nchunks_c : R.nchunks_w));
-    unsigned long long* out = c == 0 ? R.cbase : (c == 1 ? R.cbase_x : (c == 2 ? R.cbase_c : R.cbase_w));
-    if ((c == 2 && !R.compact) || (c == 3 && !R.wide)) {  // the same for every thread
+  for (int c = 0; c < 5; c++) {
+    const unsigned long long* in =
+        c == 0 ? R.nchunks : (c == 1 ? R.nchunks_x : (c == 2 ? R.nchunks_c : (c == 3 ? R.nchunks_w : R.nchunks_r)));
+    unsigned long long* out =
+        c == 0 ? R.cbase : (c == 1 ? R.cbase_x : (c == 2 ? R.cbase_c : (c == 3 ? R.cbase_w : R.cbase_r)));
+    if ((c == 2 && !R.compact) || (c >= 3 && !R.wide)) {  // the same for every thread
       if (tid == 0) ctl->totals[c] = 0;
       continue;
     }
@@ -2124,7 +2337,10 @@ void warm_exhaustive_k() {
 }
 void warm_exhaustive_dev(const RoundBuf& R, int k) {
   (void)dev_num_sms();
-  if (R.wide) warm_exhaustive_k<1, 4>();
+  if (R.wide) {
+    warm_exhaustive_k<1, 4>();
+    warm_exhaustive_k<1, 5>();
+  }
   if (R.compact) warm_exhaustive_k<1, 3>();
   warm_exhaustive_k<1, 0>();
   if (R.xunit == kXBitsBlocks) warm_exhaustive_k<1, 2>();
@@ -2138,8 +2354,9 @@ int launch_exhaustive_dev(const DevTargets& T, const DevPool& P, const RoundBuf&
                           cudaStream_t s) {
   int n = 0;
   if (R.wide) {
+    launch_exhaustive_dev_k<1, 5>(T, P, R, &ctl->totals[4], &ctl->np, s);
     launch_exhaustive_dev_k<1, 4>(T, P, R, &ctl->totals[3], &ctl->np, s);
-    n++;
+    n += 2;
   }
   if (R.compact) {
     launch_exhaustive_dev_k<1, 3>(T, P, R, &ctl->totals[2], &ctl->np, s);

@@ -74,8 +74,12 @@ struct RoundBuf {
                                    // their own class and kernel
   unsigned long long* nchunks_w;   // per pair, wide compact class (with wide set; else unused)
   unsigned long long* cbase_w;     // exclusive prefix of nchunks_w
+  unsigned long long* nchunks_r;   // per pair, register-state class (with wide set; else unused)
+  unsigned long long* cbase_r;     // exclusive prefix of nchunks_r
   uint32_t wide;                   // pairs whose registers fit the wide compact state (and not
-                                   // the compact one) get their own class and kernel
+                                   // the compact one) get their own class and kernel, and so do
+                                   // the rest that name neither SP nor the memory byte
+                                   // (register-state class)
   uint32_t* rejected;              // per pair
   uint8_t* wlen;                   // per pair: survivors in the window it heads (0: not a head)
   // First-found windows (null for independent pairs): per pair the end
@@ -88,7 +92,7 @@ struct RoundBuf {
   uint32_t cap;                    // pair slots of the buffers
   uint32_t* npairs;                // device counter
   unsigned long long* counter;     // chunk dispensers: [0] bit-sliced, [1] A-independent, [2] compact,
-                                   // [3] wide compact class
+                                   // [3] wide compact, [4] register-state class
   unsigned long long* states;      // [2]: states of the reference's sweeps covered, states evaluated
   uint32_t chunk_blocks;           // A-blocks per work chunk
   uint32_t xunit;                  // A-blocks per unit of an A-independent sweep: kXBitsBlocks
@@ -145,20 +149,22 @@ void launch_pairs_from_survivors(const DevTargets& T, const DevPool& P, const QC
 // kSweep* bits.
 constexpr uint32_t kSweepBits = 1u, kSweepXBits = 2u, kSweepCompact = 4u;
 constexpr uint32_t kSweepScalarK1 = 8u;  // scalar A-independent kernel, K = 1, 2, 4, 8: bits 3..6
-constexpr uint32_t kSweepWide = 128u;
+constexpr uint32_t kSweepWide = 128u, kSweepRegs = 256u;
 int launch_exhaustive(const DevTargets& T, const DevPool& P, const RoundBuf& R, uint32_t npairs,
                       unsigned long long total_b, unsigned long long total_x, unsigned long long total_c,
-                      unsigned long long total_w, int k, cudaStream_t s, uint32_t* kernels = nullptr);
+                      unsigned long long total_w, unsigned long long total_r, int k, cudaStream_t s,
+                      uint32_t* kernels = nullptr);
 void launch_round_resolve(const RoundBuf& R, uint32_t npairs, const QCOut& q, const Lanes& L, uint32_t max_spec,
                           cudaStream_t s);
 
 // ---- device-driven rounds (one CUDA graph, a WHILE node over the round body)
 // The round's pair count and chunk totals stay on the device: k_round_scan
 // takes the count the build left in R.npairs, scans the chunk counts of the
-// four classes, clears the dispensers and ends the loop (sets the graph's
+// five classes, clears the dispensers and ends the loop (sets the graph's
 // condition to 0) when the round is empty and no lane waits for a rescan.
 struct RoundCtl {
-  unsigned long long totals[4];  // chunks of the current round: bit-sliced, A-independent, compact, wide
+  unsigned long long totals[5];  // chunks of the current round: bit-sliced, A-independent, compact, wide,
+                                 // register state
   unsigned long long pairs;      // pairs swept, all rounds
   uint32_t rounds;               // rounds with pairs
   uint32_t iters;                // loop iterations (rounds, rescans, the last empty one)

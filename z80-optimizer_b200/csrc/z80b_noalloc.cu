@@ -114,7 +114,7 @@ int run_on_device(int device, uint32_t n, const uint8_t* tlens, const uint8_t* c
   R.counter = reinterpret_cast<unsigned long long*>(base + kOffCounter);
   R.states = reinterpret_cast<unsigned long long*>(base + kOffStates);
   R.chunk_blocks = 32;
-  launch_exhaustive(T, P, R, n, total, total_x, 0, 0, 4, s);
+  launch_exhaustive(T, P, R, n, total, total_x, 0, 0, 0, 4, s);
   if (cudaGetLastError() != cudaSuccess) return Z80B_ECUDA;
   if (cudaMemcpyAsync(h_rej, base + kOffRej, 4ull * n, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
       cudaStreamSynchronize(s) != cudaSuccess)
