@@ -265,8 +265,8 @@ def c3_leg(ctx, z80b, workloads, args):
     """Batched uneven workload: seeded C3 targets (60% length 2, 40% length
     3, per-target dead-register and dead-flag masks), candidates up to 2
     instructions, first-found semantics.  The sweep configuration is tuned
-    on the first 2,000 targets, the first 20,000 build the length-2 pair pool
-    and its bucket indexes, then one timed search covers every target
+    on the first 20,000 targets (whose first search also builds the length-2
+    pair pool and its bucket indexes), then one timed search covers every target
     (device time of the pipeline).  Beside it, the first 1,000 targets
     through the one-target-per-launch path and the batched path."""
     import torch
@@ -289,16 +289,15 @@ def c3_leg(ctx, z80b, workloads, args):
         j.path = path
         return j, (a, ln, d, r)
 
-    # tune the sweep kernel for this workload on its first 2,000 targets
-    # (longer sequences than C2's, so another setting may win); the C2
+    # tune the sweep kernel for this workload on its first 20,000 targets
+    # (longer sequences than C2's, so another setting may win; the first
+    # trial also builds the pair pool and its bucket indexes); the C2
     # setting is restored after the leg
     tuned = [z80b.OPT_EXH_LANE_STATES, z80b.OPT_EXH_CHUNK_BLOCKS, z80b.OPT_XINDEP_BITS, z80b.OPT_COMPACT_SWEEP,
              z80b.OPT_WIDE_SWEEP]
     saved = [ctx.get_option(o) for o in tuned]
-    tj, tkeep = job_for(0, min(2000, n), z80b.PATH_BATCHED)
+    tj, tkeep = job_for(0, min(20000, n), z80b.PATH_BATCHED)
     tr = ctx.autotune(tj)
-    wj, wkeep = job_for(0, min(20000, n), z80b.PATH_BATCHED)
-    ctx.run_job(wj)  # builds the pair pool and its bucket indexes once
     job, keep = job_for(0, n, z80b.PATH_BATCHED)
     torch.cuda.synchronize()
     t1 = time.perf_counter()
@@ -312,8 +311,8 @@ def c3_leg(ctx, z80b, workloads, args):
            "qc_survivors": st.qc_survivors, "exhaustive_pairs": st.exhaustive_pairs,
            "exhaustive_states": st.exhaustive_states, "rounds": st.rounds, "launches": st.launches,
            "exhaustive_ms": st.exh_ms, "checks": st.checks, "wall_s": wall,
-           "steps": 1, "timing": "one search over every target after a warm-up search of the first 20,000",
-           "autotune": tune_record(tr, "first 2,000 targets of the leg")}
+           "steps": 1, "timing": "one search over every target after the tuning searches of the first 20,000",
+           "autotune": tune_record(tr, "first 20,000 targets of the leg")}
     if args.plain_sample:
         m = min(1000, n)
         pj, keep2 = job_for(0, m, z80b.PATH_PLAIN)
@@ -427,9 +426,10 @@ def main():
     progress(f"rank {rank}: {len(mine)} targets staged")
 
     # ---- autotune (sweep kernel configuration) on a 200k-target sample
-    tune_arr = np.ascontiguousarray(workloads.c2_subset(200000, seed=11))
-    tr = ctx.autotune(make_job(z80b, tune_arr, dead))
-    tuning = tune_record(tr, "200,000 C2 targets (seed 11)")
+    # tuned on the workload itself: small samples favour small chunks (few
+    # chunks to balance), which lose at the full size
+    tr = ctx.autotune(make_job(z80b, mine, dead))
+    tuning = tune_record(tr, f"the workload itself ({len(mine):,} targets)")
     progress(f"autotune: {tuning['chosen']}")
 
     # ---- value: targets resident in HBM
