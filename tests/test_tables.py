@@ -158,3 +158,21 @@ def test_wide_state_against_oracle(tmp_path):
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
     assert r.stdout.startswith("OK")
+
+
+def test_dependency_sets_against_oracle(tmp_path):
+    """The dependency sets derived from the bit-sliced step hold under the
+    oracle's Exec (an output never changes with an input outside its set),
+    and sweeps that leave out the swept registers no compared output depends
+    on give the oracle's ExhaustiveCheck verdicts with dead flags and
+    registers."""
+    import subprocess
+    exe = tmp_path / "deps_check"
+    srcs = [os.path.join(ROOT, "tests", "native", "deps_check.cpp"),
+            os.path.join(ROOT, "z80-optimizer_b200", "csrc", "z80_tables.cpp"),
+            os.path.join(ROOT, "oracle", "z80_oracle_isa_cpu.cpp"),
+            os.path.join(ROOT, "oracle", "z80_oracle_search.cpp")]
+    subprocess.run(["g++", "-O2", "-std=c++17", "-o", str(exe)] + srcs + ["-lpthread"], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert r.stdout.startswith("OK")

@@ -239,6 +239,89 @@ const uint8_t* op_aclass() {
   return cls;
 }
 
+}  // namespace z80b
+
+// The bit-sliced step on planes that carry dependency sets: a plane word is
+// the mask of input fields it was computed from; every logic operation
+// unites its operands' sets and a constant has none.
+namespace z80b_dep {
+using namespace z80b;
+struct ZW {
+  uint32_t m = 0;
+  ZW() = default;
+  ZW(uint32_t) {}  // a constant depends on nothing
+};
+inline ZW dep_join(ZW a, ZW b) {
+  ZW r;
+  r.m = a.m | b.m;
+  return r;
+}
+inline ZW operator~(ZW a) { return a; }
+inline ZW operator&(ZW a, ZW b) { return dep_join(a, b); }
+inline ZW operator|(ZW a, ZW b) { return dep_join(a, b); }
+inline ZW operator^(ZW a, ZW b) { return dep_join(a, b); }
+inline ZW& operator&=(ZW& a, ZW b) { return a = dep_join(a, b); }
+inline ZW& operator|=(ZW& a, ZW b) { return a = dep_join(a, b); }
+inline ZW& operator^=(ZW& a, ZW b) { return a = dep_join(a, b); }
+#include "z80_bits_core.cuh"
+}  // namespace z80b_dep
+
+namespace z80b {
+
+const uint32_t (*op_deps())[kDepFields] {
+  static uint32_t T[kNumOps][kDepFields];
+  static std::once_flag once;
+  std::call_once(once, [] {
+    for (int op = 0; op < kNumOps; op++) {
+      z80b_dep::ZB z;
+      for (int i = 0; i < 8; i++) {
+        z.a[i].m = kRegA;
+        z.f[i].m = 1u << (kDepF0 + i);
+        z.b[i].m = kRegB;
+        z.c[i].m = kRegC;
+        z.d[i].m = kRegD;
+        z.e[i].m = kRegE;
+        z.h[i].m = kRegH;
+        z.l[i].m = kRegL;
+        z.m[i].m = kRegM;
+      }
+      for (int i = 0; i < 16; i++) z.sp[i].m = kRegSP;
+      z80b_dep::zb_step(z, uint32_t(op), 0u);
+      auto join8 = [](const z80b_dep::ZW (&r)[8]) {
+        uint32_t m = 0;
+        for (int i = 0; i < 8; i++) m |= r[i].m;
+        return m;
+      };
+      uint32_t* d = T[op];
+      for (int g = 0; g < kDepFields; g++) d[g] = 0;
+      d[0] = join8(z.a);
+      d[2] = join8(z.b);
+      d[3] = join8(z.c);
+      d[4] = join8(z.d);
+      d[5] = join8(z.e);
+      d[6] = join8(z.h);
+      d[7] = join8(z.l);
+      uint32_t sp = 0;
+      for (int i = 0; i < 16; i++) sp |= z.sp[i].m;
+      d[8] = sp;
+      d[9] = join8(z.m);
+      for (int k = 0; k < 8; k++) d[kDepF0 + k] = z.f[k].m;
+    }
+  });
+  return T;
+}
+
+uint32_t seq_relevant(const uint32_t* s, int n, uint32_t out) {
+  const uint32_t (*D)[kDepFields] = op_deps();
+  for (int i = n - 1; i >= 0; i--) {
+    const uint32_t* d = D[insn_op(s[i])];
+    uint32_t in = 0;
+    for (uint32_t o = out; o; o &= o - 1) in |= d[__builtin_ctz(o)];
+    out = in;
+  }
+  return out;
+}
+
 uint32_t seq_aflow(const uint32_t* s, int n) {
   const uint8_t* c = op_aclass();
   bool a_is_x = true;

@@ -26,6 +26,21 @@ const uint8_t* op_aclass();               // kNumOps entries
 // Folds the classes over a sequence: 0 when some output depends on the input
 // A; else 1 (A is overwritten) or 3 (A passes through to the output).
 uint32_t seq_aflow(const uint32_t* s, int n);
+// Which input fields each output field of an instruction depends on.  A
+// field is a bit of a mask laid out like the register read masks: A bit 0,
+// B..L bits 2..7, SP bit 8, the memory byte bit 9, and the flag bits F0..F7
+// one by one at bits 16..23 (kDepF0 + k).  deps[op][g] is the mask of input
+// fields that output field g can depend on, g a bit position of that layout
+// (entries of unused positions are 0); an output the instruction leaves
+// alone depends on itself.  Derived by running the bit-sliced step
+// (z80_bits_core.cuh) on planes that carry, instead of bits, the set of
+// input fields they were computed from: a sound over-approximation (every
+// real dependency is in the set).
+constexpr int kDepF0 = 16, kDepFields = 24;
+const uint32_t (*op_deps())[kDepFields];  // kNumOps rows
+// Input fields that the outputs in `out` (a mask of the layout above) of
+// the sequence s can depend on.
+uint32_t seq_relevant(const uint32_t* s, int n, uint32_t out);
 const char* op_mnemonic(uint16_t op);     // "ADD A, n" style with placeholders
 // The instruction that does op's work with the 8-bit registers renamed:
 // register r (0..5 = B, C, D, E, H, L) plays the part of map[r] (map is a

@@ -57,6 +57,11 @@ struct PairRec {
   uint8_t keepF;       // ~deadFlags
   uint8_t keepR;       // bits 0..5: register compared (B,C,D,E,H,L); bit 7: masked pass
   uint8_t cmap;        // compact sweep: 1 + the register-set entry of its tables; 0: full state
+  // Swept registers left out because no compared output of either program
+  // depends on them (reads holds the ones swept): bit 7 the reference's
+  // sweep of this pair is a reduced one (32 values per register), bits 0..5
+  // log2 of the reference states each evaluated state stands for.
+  uint8_t sweepf;
 };
 
 __device__ __forceinline__ uint32_t target_len(const DevTargets& T, uint32_t t) {

@@ -62,6 +62,8 @@ __device__ uint8_t g_cid[64];
 __device__ uint8_t g_opregs[kNumOps];
 // wide compact sweep: the same per register set of at most four registers
 // (wide_tables)
+// input fields each output field of an opcode depends on (op_deps)
+__device__ uint32_t g_dep[kNumOps][kDepFields];
 __device__ int16_t g_wren[kWideSets][kNumOps];
 __device__ int8_t g_worig[kWideSets][4];
 __device__ uint8_t g_wid[64];
@@ -117,14 +119,27 @@ __device__ __forceinline__ uint32_t reg_diff(uint32_t d0, uint32_t d1) {
 }
 
 // Number of A-blocks of the ExhaustiveCheck sweep for a read mask
-// (verifier.go:159-171,428-476).
-__device__ __forceinline__ unsigned long long sweep_blocks(uint32_t reads) {
+// (verifier.go:159-171,428-476); reduced: the reference's sweep of the pair
+// is a reduced one although these reads alone would not make it so (swept
+// registers left out, see put_pair).
+__device__ __forceinline__ unsigned long long sweep_blocks(uint32_t reads, bool reduced = false) {
   uint32_t ext = reads & (kRegB | kRegC | kRegD | kRegE | kRegH | kRegL | kRegM);
   int n = __popc(ext);
   bool sp = (reads & kRegSP) != 0;
-  if (n == 0 && !sp) return 2ull;
-  if (n <= 2 && !sp) return 2ull << (8 * n);
+  if (n == 0 && !sp && !reduced) return 2ull;
+  if (n <= 2 && !sp && !reduced) return 2ull << (8 * n);
   return (2ull << (5 * n)) * (sp ? 16ull : 1ull);
+}
+// Input fields (op_deps layout) that the outputs in `out` of a program can
+// depend on: the dependency sets of its instructions, walked backwards.
+__device__ __forceinline__ uint32_t dev_seq_relevant(const uint32_t* w, uint32_t n, uint32_t out) {
+  for (int i = int(n) - 1; i >= 0; i--) {
+    const uint32_t* d = g_dep[w[i] & 0xFFFFu];
+    uint32_t in = 0;
+    for (uint32_t o = out; o; o &= o - 1) in |= d[__ffs(o) - 1];
+    out = in;
+  }
+  return out;
 }
 // A-independent sweeps.  When no output of either sequence depends on the
 // input A except A itself passing through (AClass folds of both sequences),
@@ -524,11 +539,37 @@ __device__ __forceinline__ void put_pair(const RoundBuf& R, uint32_t p, const De
   const uint32_t reads = q.meta[t].reads | P.reads[c];
   pr.target = t;
   pr.cand = c;
-  pr.reads = uint16_t(reads);
-  pr.nblocks = sweep_blocks(reads);
   pr.keepF = kind ? uint8_t(~target_dead(T, t)) : uint8_t(0xFFu);
   pr.keepR = kind ? uint8_t((~target_dead_regs(T, t) & 0x3Fu) | 0x80u) : uint8_t(0x3Fu);
   if (pair_xindep(T, t, P, c)) pr.keepR |= uint8_t(kXIndep);
+  // A swept register that no compared output of either program depends on
+  // (dead registers and flags make this common in masked passes: SET 6, B
+  // with B dead) cannot change the verdict, so one value of it stands for
+  // all the reference sweeps: it is left out of the sweep, whose other
+  // registers keep the reference's values (a reduced sweep stays reduced).
+  // The same holds for the carry, the most significant field of the block
+  // index: when no compared output depends on it, the first half of the
+  // blocks (carry 0) decides.
+  uint32_t swept = reads;
+  pr.sweepf = 0;
+  const uint32_t ext = reads & (kRegB | kRegC | kRegD | kRegE | kRegH | kRegL | kRegM);
+  const uint32_t cmp = kRegA | kRegSP | kRegM | ((uint32_t(pr.keepR) & 0x3Fu) << 2) |
+                       (uint32_t(pr.keepF) << kDepF0);
+  const uint32_t rel = dev_seq_relevant(T.insn + (size_t)t * T.stride, target_len(T, t), cmp) |
+                       dev_seq_relevant(P.insn + (size_t)c * P.stride, pool_len(P, c), cmp);
+  const uint32_t drop = ext & ~rel;
+  const bool carry_out = (rel & (1u << kDepF0)) == 0;
+  if (drop) {
+    const bool red = (reads & kRegSP) != 0 || __popc(ext) > 2;
+    swept = reads & ~drop;
+    pr.sweepf = uint8_t((red ? 0x80u : 0u) | uint32_t(__popc(drop)) * (red ? 5u : 8u));
+  }
+  pr.reads = uint16_t(swept);
+  pr.nblocks = sweep_blocks(swept, (pr.sweepf & 0x80u) != 0);
+  if (carry_out) {
+    pr.nblocks >>= 1;
+    pr.sweepf += 1;
+  }
   // compact classes: A-dependent pairs, and A-independent ones when those
   // are swept bit-sliced (units of kXBitsBlocks); the narrow state first
   pr.cmap = 0;
@@ -622,6 +663,7 @@ __global__ void k_pairs_from_survivors(DevTargets T, DevPool P, QCOut q, const u
     pr.keepR = uint8_t(~target_dead_regs(T, t) & 0x3Fu);
     if (pair_xindep(T, t, P, c)) pr.keepR |= uint8_t(kXIndep);
     pr.cmap = 0;
+    pr.sweepf = 0;
     have = true;
   }
   unsigned b = __ballot_sync(kFull, have);
@@ -1356,7 +1398,8 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : (CLS == 4 ? 2 : (CLS ==
     const uint32_t ext = pr.reads & (kRegB | kRegC | kRegD | kRegE | kRegH | kRegL | kRegM);
     const int nx = __popc(ext);
     const bool spw = (pr.reads & kRegSP) != 0;
-    const bool reduced = spw || nx > 2;
+    const bool reduced = spw || nx > 2 || (pr.sweepf & 0x80u) != 0;
+    const uint32_t xs = pr.sweepf & 0x3Fu;  // reference states per evaluated state, log2
     const int fw = reduced ? 5 : 8;  // bits per swept register in the block index
     int slot[7];
     {
@@ -1388,7 +1431,7 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : (CLS == 4 ? 2 : (CLS ==
           const unsigned long long nb = (pr.nblocks - first < kXBitsBlocks) ? pr.nblocks - first : kXBitsBlocks;
           bad = rxbits_unit(u, pr.nblocks, reduced, nx, rlast, bd, pw, int(tl), int(cl), pr.keepF, pr.keepR, sm) ||
                 bad;
-          my_states += 256ull * nb;
+          my_states += (256ull * nb) << xs;
           my_eval += 2ull * nb;
           if (__any_sync(kFull, bad)) break;
           if (__shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0)) {
@@ -1401,7 +1444,7 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : (CLS == 4 ? 2 : (CLS ==
           const unsigned long long first = u * kBitsBlocks;
           const unsigned long long nb = (pr.nblocks - first < kBitsBlocks) ? pr.nblocks - first : kBitsBlocks;
           bad = rbits_unit(u, pr.nblocks, bd, pw, int(tl), int(cl), pr.keepF, pr.keepR, sm) || bad;
-          my_states += 256ull * nb;
+          my_states += (256ull * nb) << xs;
           my_eval += 256ull * nb;
           if (__any_sync(kFull, bad)) break;
           if ((u & 15ull) == 15ull &&
@@ -1429,7 +1472,7 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : (CLS == 4 ? 2 : (CLS ==
         const unsigned long long first = u * kBitsBlocks;
         const unsigned long long nb = (pr.nblocks - first < kBitsBlocks) ? pr.nblocks - first : kBitsBlocks;
         bad = wbits_unit(u, pr.nblocks, dec, pw, int(tl), int(cl), pr.keepF, cmp, sm) || bad;
-        my_states += 256ull * nb;
+        my_states += (256ull * nb) << xs;
         my_eval += 256ull * nb;
         if (__any_sync(kFull, bad)) break;
         if ((u & 15ull) == 15ull &&
@@ -1457,7 +1500,7 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : (CLS == 4 ? 2 : (CLS ==
           const unsigned long long nb = (pr.nblocks - first < kXBitsBlocks) ? pr.nblocks - first : kXBitsBlocks;
           bad = cxbits_unit(u, pr.nblocks, nx, dec, rlast, pw, int(tl), int(cl), pr.keepF, pr.keepR, o0, o1, sm) ||
                 bad;
-          my_states += 256ull * nb;
+          my_states += (256ull * nb) << xs;
           my_eval += 2ull * nb;
           if (__any_sync(kFull, bad)) break;
           if (__shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0)) {
@@ -1470,7 +1513,7 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : (CLS == 4 ? 2 : (CLS ==
           const unsigned long long first = u * kBitsBlocks;
           const unsigned long long nb = (pr.nblocks - first < kBitsBlocks) ? pr.nblocks - first : kBitsBlocks;
           bad = cbits_unit(u, pr.nblocks, dec, pw, int(tl), int(cl), pr.keepF, pr.keepR, o0, o1, sm) || bad;
-          my_states += 256ull * nb;
+          my_states += (256ull * nb) << xs;
           my_eval += 256ull * nb;
           if (__any_sync(kFull, bad)) break;
           if ((u & 15ull) == 15ull &&
@@ -1493,7 +1536,7 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : (CLS == 4 ? 2 : (CLS ==
         const unsigned long long first = u * kBitsBlocks;
         const unsigned long long nb = (pr.nblocks - first < kBitsBlocks) ? pr.nblocks - first : kBitsBlocks;
         bad = bits_unit(u, pr.nblocks, bd, pw, int(tl), int(cl), pr.keepF, pr.keepR, sm) || bad;
-        my_states += 256ull * nb;
+        my_states += (256ull * nb) << xs;
         my_eval += 256ull * nb;
         if (__any_sync(kFull, bad)) break;
         if ((u & 15ull) == 15ull &&
@@ -1517,7 +1560,7 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : (CLS == 4 ? 2 : (CLS ==
         bad = xbits_unit(u, pr.nblocks, spw, reduced, nx, fw, slot, rlast, pw, int(tl), int(cl), pr.keepF,
                          pr.keepR, sm) ||
               bad;
-        my_states += 256ull * nb;
+        my_states += (256ull * nb) << xs;
         my_eval += 2ull * nb;
         if (__any_sync(kFull, bad)) break;
         if (__shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0)) {
@@ -1533,7 +1576,7 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : (CLS == 4 ? 2 : (CLS ==
         const unsigned long long first = u * kUnitBlocks;
         const unsigned long long nb = (pr.nblocks - first < kUnitBlocks) ? pr.nblocks - first : kUnitBlocks;
         bad = xindep_unit<K>(first, nb, bd, pw, int(tl), int(cl), keep0, keep1) || bad;
-        my_states += 256ull * nb;
+        my_states += (256ull * nb) << xs;
         my_eval += 2ull * nb;
         if (__any_sync(kFull, bad)) break;
         if ((u & 3ull) == 3ull &&
@@ -2078,6 +2121,7 @@ void dev_upload_tables(cudaStream_t s) {
   cudaMemcpyToSymbolAsync(g_repsp, rep_sp(), 32, 0, cudaMemcpyHostToDevice, s);
   cudaMemcpyToSymbolAsync(g_aclass, op_aclass(), kNumOps, 0, cudaMemcpyHostToDevice, s);
   {
+    cudaMemcpyToSymbolAsync(g_dep, op_deps(), sizeof(uint32_t) * kNumOps * kDepFields, 0, cudaMemcpyHostToDevice, s);
     const CompactTables& C = compact_tables();
     cudaMemcpyToSymbolAsync(g_cren, C.ren, sizeof C.ren, 0, cudaMemcpyHostToDevice, s);
     cudaMemcpyToSymbolAsync(g_corig, C.orig, sizeof C.orig, 0, cudaMemcpyHostToDevice, s);
