@@ -570,6 +570,10 @@ __device__ __forceinline__ void put_pair(const RoundBuf& R, uint32_t p, const De
     pr.nblocks >>= 1;
     pr.sweepf += 1;
   }
+  // A on which no compared output depends (a comparison whose flags are
+  // dead, say) is as good as independent: the A-independent sweeps, two
+  // values of A, decide the pair
+  if ((rel & kRegA) == 0) pr.keepR |= uint8_t(kXIndep);
   // compact classes: A-dependent pairs, and A-independent ones when those
   // are swept bit-sliced (units of kXBitsBlocks); the narrow state first
   pr.cmap = 0;
