@@ -24,6 +24,7 @@
 #include <cstring>
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -98,6 +99,10 @@ struct PairShared {
   DBuf idx[64];
   bool ok[64] = {};
   DBuf ptrs, eligible_dev, keys_tmp, sort_tmp;
+  // the indexes restricted to unpruned pairs of at most 2 / 3 bytes
+  uint32_t n_le[2] = {0, 0};
+  DBuf idx_le[2][64];
+  DBuf ptrs_le[2], sel_tmp, sel_count;
 };
 
 std::mutex g_pairs_mu;
@@ -362,15 +367,31 @@ int ensure_pairpool(z80b_ctx* ctx) {
       by_size[std::min<uint32_t>(size[q], 16)]++;
     }
   S.valid = valid;
+  S.n_le[0] = uint32_t(by_size[0] + by_size[1] + by_size[2]);
+  S.n_le[1] = uint32_t(S.n_le[0] + by_size[3]);
   S.eligible.assign(16, 0);
   for (int b = 1; b < 16; b++) S.eligible[size_t(b)] = S.eligible[size_t(b - 1)] + by_size[size_t(b - 1)];
   CK(S.eligible_dev.ensure(16 * sizeof(unsigned long long)));
   CK(cudaMemcpy(S.eligible_dev.p, S.eligible.data(), 16 * sizeof(unsigned long long), cudaMemcpyHostToDevice));
   CK(S.ptrs.ensure(64 * sizeof(void*)));
   CK(cudaMemset(S.ptrs.p, 0, 64 * sizeof(void*)));
-  trace("pair pool ready: %u unpruned", valid);
+  for (int k = 0; k < 2; k++) {
+    CK(S.ptrs_le[k].ensure(64 * sizeof(void*)));
+    CK(cudaMemset(S.ptrs_le[k].p, 0, 64 * sizeof(void*)));
+  }
+  trace("pair pool ready: %u unpruned (%u of at most 2 bytes, %u of at most 3)", valid, S.n_le[0], S.n_le[1]);
   return Z80B_OK;
 }
+
+// Selects index entries of unpruned pairs of at most max_size bytes (pruned
+// pairs' keys are all ones).
+struct ShortPair {
+  const uint8_t* size;
+  uint8_t max_size;
+  __device__ bool operator()(const unsigned long long& key) const {
+    return key != ~0ull && size[uint32_t(key)] <= max_size;
+  }
+};
 
 // Bucket index of the pair pool for one dead-register mask: the pairs'
 // (hash of the masked vector-0 output, pair index) keys, sorted.
@@ -393,6 +414,28 @@ int ensure_pair_index(z80b_ctx* ctx, uint32_t m) {
   ctx->launches += 2;
   void* ptr = S.idx[m].p;
   CK(cudaMemcpyAsync(S.ptrs.as<void*>() + m, &ptr, sizeof ptr, cudaMemcpyHostToDevice, ctx->stream));
+  // the short-pair indexes: the entries of pairs of at most 2 / 3 bytes, in
+  // the full index's order (a stable selection)
+  CK(S.sel_count.ensure(sizeof(int)));
+  for (int k = 0; k < 2; k++) {
+    CK(S.idx_le[k][m].ensure(8ull * std::max<uint32_t>(S.n_le[k], 1)));
+    const ShortPair pred{P.size, uint8_t(2 + k)};
+    size_t stmp = 0;
+    CK(cub::DeviceSelect::If(nullptr, stmp, S.idx[m].as<unsigned long long>(), S.idx_le[k][m].as<unsigned long long>(),
+                             S.sel_count.as<int>(), int(n), pred, ctx->stream));
+    CK(S.sel_tmp.ensure(stmp));
+    CK(cub::DeviceSelect::If(S.sel_tmp.p, stmp, S.idx[m].as<unsigned long long>(),
+                             S.idx_le[k][m].as<unsigned long long>(), S.sel_count.as<int>(), int(n), pred,
+                             ctx->stream));
+    ctx->launches += 1;
+    int got = 0;
+    CK(cudaMemcpyAsync(&got, S.sel_count.p, sizeof got, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (uint32_t(got) != S.n_le[k])
+      return fail(ctx, Z80B_ECUDA, "short-pair index holds %d entries, expected %u", got, S.n_le[k]);
+    void* q = S.idx_le[k][m].p;
+    CK(cudaMemcpyAsync(S.ptrs_le[k].as<void*>() + m, &q, sizeof q, cudaMemcpyHostToDevice, ctx->stream));
+  }
   CK(cudaStreamSynchronize(ctx->stream));
   S.ok[m] = true;
   trace("pair index for dead-register mask %02X built", m);
@@ -896,6 +939,10 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
       PairScan ps{};
       ps.idx = reinterpret_cast<const unsigned long long* const*>(PS.ptrs.p);
       ps.n_valid = PS.valid;
+      ps.idx_le2 = reinterpret_cast<const unsigned long long* const*>(PS.ptrs_le[0].p);
+      ps.idx_le3 = reinterpret_cast<const unsigned long long* const*>(PS.ptrs_le[1].p);
+      ps.n_le2 = PS.n_le[0];
+      ps.n_le3 = PS.n_le[1];
       ps.cnt = ctx->cnt2.as<uint32_t>();
       ps.resume = ctx->resume2.as<uint32_t>();
       ps.surv = ctx->surv2.as<uint32_t>();

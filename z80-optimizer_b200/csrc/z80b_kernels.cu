@@ -1956,12 +1956,14 @@ __global__ void __launch_bounds__(kBlock) k_pair_scan(DevTargets T, DevPool P, Q
       if (!need[kind]) continue;
       const uint32_t idx = 2 * t + kind;
       const uint32_t m = kind ? dregs : 0u;
-      const unsigned long long* ix = ps.idx[m];
+      // the index holding only pairs that can be shorter than the target
+      const unsigned long long* ix = tb == 3 ? ps.idx_le2[m] : (tb == 4 ? ps.idx_le3[m] : ps.idx[m]);
+      const uint32_t nv = tb == 3 ? ps.n_le2 : (tb == 4 ? ps.n_le3 : ps.n_valid);
       const uint32_t h = bucket_hash(tw[0][0] & key_keep0(m), tw[0][1] & key_keep1(m), tw[0][2]);
       uint32_t lo = 0, hi = 0;
       if (lane == 0) {
-        lo = lower_bound_u64(ix, ps.n_valid, (unsigned long long)h << 32);
-        hi = (h == 0xFFFFFFFFu) ? ps.n_valid : lower_bound_u64(ix, ps.n_valid, (unsigned long long)(h + 1u) << 32);
+        lo = lower_bound_u64(ix, nv, (unsigned long long)h << 32);
+        hi = (h == 0xFFFFFFFFu) ? nv : lower_bound_u64(ix, nv, (unsigned long long)(h + 1u) << 32);
       }
       lo = __shfl_sync(kFull, lo, 0);
       hi = __shfl_sync(kFull, hi, 0);

@@ -104,6 +104,12 @@ constexpr uint32_t kSlots2 = 32;  // survivors held per (target, kind) lane
 struct PairScan {
   const unsigned long long* const* idx;  // [64] sorted bucket keys per dead-register mask
   uint32_t n_valid;                      // entries of each index (the unpruned pairs)
+  // The same indexes over the unpruned pairs of at most 2 and at most 3
+  // bytes ([64] each, in the same order): a target of 3 or 4 bytes can only
+  // take those, and its bucket in the full index is nearly all longer pairs.
+  const unsigned long long* const* idx_le2;
+  const unsigned long long* const* idx_le3;
+  uint32_t n_le2, n_le3;
   uint32_t* cnt;                         // [2n] survivors in the lane's slots
   uint32_t* resume;                      // [2n] bucket offset to rescan from; kNone: exhausted
   uint32_t* surv;                        // [2n * kSlots2] pair-pool indices
