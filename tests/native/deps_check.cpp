@@ -8,8 +8,10 @@
 // a dead register, a sweep that drops the swept registers no compared output
 // depends on (the others keeping the reference's values: a reduced sweep
 // stays reduced), keeps only carry 0 when no compared output depends on the
-// carry, and only A = 0, 1 when none depends on A, gives the oracle's
-// ExhaustiveCheck verdict.  Built and run
+// carry, and only A = 0, 1 when no compared output but A depends on A and
+// each program keeps A or computes it from other inputs (pair_a_free), gives
+// the oracle's ExhaustiveCheck verdict.  (1b) The instructions said to keep
+// A leave it unchanged under the oracle's Exec.  Built and run
 // by tests/test_tables.py.
 #include <cstdio>
 #include <random>
@@ -126,6 +128,26 @@ int main() {
       }
     }
   }
+  // (1b) instructions said to keep A leave it exactly as it was
+  int keepers = 0;
+  for (int op = 0; op < orc::OpCodeCount; op++) {
+    if (!op_keeps_a()[op]) continue;
+    keepers++;
+    for (int k = 0; k < 256; k++) {
+      const uint64_t r = rng(), r2 = rng();
+      orc::State st{uint8_t(k), uint8_t(r >> 8), uint8_t(r >> 16), uint8_t(r >> 24), uint8_t(r >> 32),
+                    uint8_t(r >> 40), uint8_t(r >> 48), uint8_t(r >> 56), uint16_t(r2), uint8_t(r2 >> 16)};
+      orc::Exec(st, uint16_t(op), uint16_t(rng()));
+      if (st.A != uint8_t(k)) {
+        std::printf("op %d (%s) is said to keep A but changes it\n", op, op_mnemonic(uint16_t(op)));
+        return 1;
+      }
+    }
+  }
+  if (keepers < 200) {
+    std::printf("too few instructions keep A (%d)\n", keepers);
+    return 1;
+  }
   // (2) sweeps without the irrelevant registers give the oracle's verdicts
   const auto& I = orc::Instructions8();
   int pairs = 0, equal = 0, dropped = 0, carries = 0, carry_only = 0, a_free = 0;
@@ -157,8 +179,9 @@ int main() {
     const uint32_t rel = seq_relevant(tw, tn, cmp) | seq_relevant(cw, cn, cmp);
     const uint32_t drop = ext & ~rel;
     const bool carry_out = (rel & (1u << kDepF0)) == 0;
-    if (!drop && !carry_out && (rel & kRegA)) continue;
-    if (pairs >= 400 && (rel & kRegA)) continue;  // past 400: A-free pairs only
+    const bool a_out = pair_a_free(tw, tn, cw, cn, cmp);
+    if (!drop && !carry_out && !a_out) continue;
+    if (pairs >= 400 && !a_out) continue;  // past 400: A-free pairs only
     if (sweep_for(reads).states > (1ull << 23)) continue;
     const int n_ext = __builtin_popcount(ext);
     const bool ref_reduced = (reads & kRegSP) != 0 || n_ext > 2;
@@ -167,16 +190,16 @@ int main() {
     if (s.nblocks > 4096) continue;
     if (!drop && carry_only >= 150) continue;
     pairs++;
-    a_free += (rel & kRegA) ? 0 : 1;
+    a_free += a_out ? 1 : 0;
     carry_only += drop ? 0 : 1;
     carries += carry_out ? 1 : 0;
     dropped += __builtin_popcount(drop);
     bool bad = false;
     for (uint64_t b = 0; b < s.nblocks && !bad; b++) {
       const Z80S x = decode(b, s);
-      // A that no compared output depends on: A = 0 and 1 decide, as in the
-      // A-independent sweeps the pair is then given to
-      const bool a_out = (rel & kRegA) == 0;
+      // a pair whose compared outputs other than A do not depend on A, and
+      // whose programs keep A or compute it from other inputs: A = 0 and 1
+      // decide, as in the A-independent sweeps the pair is then given to
       for (uint32_t a0 = 0; a0 < (a_out ? 32u : 256u) && !bad; a0 += 32) {
         Z80S st[32];
         for (int j = 0; j < 32; j++) {

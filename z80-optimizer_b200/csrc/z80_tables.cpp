@@ -248,6 +248,7 @@ namespace z80b_dep {
 using namespace z80b;
 struct ZW {
   uint32_t m = 0;
+  int id = -1;  // the input plane this word still is, moved only by copies; -1 once computed
   ZW() = default;
   ZW(uint32_t) {}  // a constant depends on nothing
 };
@@ -256,7 +257,10 @@ inline ZW dep_join(ZW a, ZW b) {
   r.m = a.m | b.m;
   return r;
 }
-inline ZW operator~(ZW a) { return a; }
+inline ZW operator~(ZW a) {
+  a.id = -1;
+  return a;
+}
 inline ZW operator&(ZW a, ZW b) { return dep_join(a, b); }
 inline ZW operator|(ZW a, ZW b) { return dep_join(a, b); }
 inline ZW operator^(ZW a, ZW b) { return dep_join(a, b); }
@@ -268,6 +272,10 @@ inline ZW& operator^=(ZW& a, ZW b) { return a = dep_join(a, b); }
 
 namespace z80b {
 
+namespace {
+uint8_t g_keeps_a[kNumOps];
+}
+
 const uint32_t (*op_deps())[kDepFields] {
   static uint32_t T[kNumOps][kDepFields];
   static std::once_flag once;
@@ -276,6 +284,7 @@ const uint32_t (*op_deps())[kDepFields] {
       z80b_dep::ZB z;
       for (int i = 0; i < 8; i++) {
         z.a[i].m = kRegA;
+        z.a[i].id = i;
         z.f[i].m = 1u << (kDepF0 + i);
         z.b[i].m = kRegB;
         z.c[i].m = kRegC;
@@ -306,9 +315,32 @@ const uint32_t (*op_deps())[kDepFields] {
       d[8] = sp;
       d[9] = join8(z.m);
       for (int k = 0; k < 8; k++) d[kDepF0 + k] = z.f[k].m;
+      bool keeps = true;
+      for (int i = 0; i < 8; i++) keeps = keeps && z.a[i].id == i;
+      g_keeps_a[op] = keeps ? 1 : 0;
     }
   });
   return T;
+}
+
+const uint8_t* op_keeps_a() {
+  (void)op_deps();
+  return g_keeps_a;
+}
+
+bool seq_keeps_a(const uint32_t* s, int n) {
+  const uint8_t* k = op_keeps_a();
+  for (int i = 0; i < n; i++)
+    if (!k[insn_op(s[i])]) return false;
+  return true;
+}
+
+bool pair_a_free(const uint32_t* t, int tn, const uint32_t* c, int cn, uint32_t cmp) {
+  const uint32_t rest = seq_relevant(t, tn, cmp & ~uint32_t(kRegA)) | seq_relevant(c, cn, cmp & ~uint32_t(kRegA));
+  if (rest & kRegA) return false;
+  const bool t_ok = !(seq_relevant(t, tn, kRegA) & kRegA) || seq_keeps_a(t, tn);
+  const bool c_ok = !(seq_relevant(c, cn, kRegA) & kRegA) || seq_keeps_a(c, cn);
+  return t_ok && c_ok;
 }
 
 uint32_t seq_relevant(const uint32_t* s, int n, uint32_t out) {

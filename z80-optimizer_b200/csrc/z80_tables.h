@@ -41,6 +41,18 @@ const uint32_t (*op_deps())[kDepFields];  // kNumOps rows
 // Input fields that the outputs in `out` (a mask of the layout above) of
 // the sequence s can depend on.
 uint32_t seq_relevant(const uint32_t* s, int n, uint32_t out);
+// Instructions that leave A exactly as it was (from the same run: every A
+// plane is still the input plane, moved by nothing but copies); kNumOps
+// entries, 1 = keeps A.
+const uint8_t* op_keeps_a();
+bool seq_keeps_a(const uint32_t* s, int n);
+// Two values of A decide the pair's ExhaustiveCheck when no compared output
+// but A depends on the input A (cmp: the compared outputs, layout above) and
+// each program either keeps A or computes its A from other inputs: every
+// other output is then the same for all values of A, and A_out is A_in or a
+// constant in each program (the argument of the A-independent sweeps, now
+// under the dead flags and registers).
+bool pair_a_free(const uint32_t* t, int tn, const uint32_t* c, int cn, uint32_t cmp);
 const char* op_mnemonic(uint16_t op);     // "ADD A, n" style with placeholders
 // The instruction that does op's work with the 8-bit registers renamed:
 // register r (0..5 = B, C, D, E, H, L) plays the part of map[r] (map is a

@@ -62,8 +62,10 @@ __device__ uint8_t g_cid[64];
 __device__ uint8_t g_opregs[kNumOps];
 // wide compact sweep: the same per register set of at most four registers
 // (wide_tables)
-// input fields each output field of an opcode depends on (op_deps)
+// input fields each output field of an opcode depends on (op_deps), and
+// whether it leaves A exactly as it was (op_keeps_a)
 __device__ uint32_t g_dep[kNumOps][kDepFields];
+__device__ uint8_t g_keepa[kNumOps];
 __device__ int16_t g_wren[kWideSets][kNumOps];
 __device__ int8_t g_worig[kWideSets][4];
 __device__ uint8_t g_wid[64];
@@ -140,6 +142,11 @@ __device__ __forceinline__ uint32_t dev_seq_relevant(const uint32_t* w, uint32_t
     out = in;
   }
   return out;
+}
+__device__ __forceinline__ bool dev_seq_keeps_a(const uint32_t* w, uint32_t n) {
+  for (uint32_t i = 0; i < n; i++)
+    if (!g_keepa[w[i] & 0xFFFFu]) return false;
+  return true;
 }
 // A-independent sweeps.  When no output of either sequence depends on the
 // input A except A itself passing through (AClass folds of both sequences),
@@ -555,8 +562,13 @@ __device__ __forceinline__ void put_pair(const RoundBuf& R, uint32_t p, const De
   const uint32_t ext = reads & (kRegB | kRegC | kRegD | kRegE | kRegH | kRegL | kRegM);
   const uint32_t cmp = kRegA | kRegSP | kRegM | ((uint32_t(pr.keepR) & 0x3Fu) << 2) |
                        (uint32_t(pr.keepF) << kDepF0);
-  const uint32_t rel = dev_seq_relevant(T.insn + (size_t)t * T.stride, target_len(T, t), cmp) |
-                       dev_seq_relevant(P.insn + (size_t)c * P.stride, pool_len(P, c), cmp);
+  const uint32_t* tw = T.insn + (size_t)t * T.stride;
+  const uint32_t* cw = P.insn + (size_t)c * P.stride;
+  const uint32_t tl = target_len(T, t), cl = pool_len(P, c);
+  // what the compared outputs other than A, and A itself, depend on
+  const uint32_t rest = dev_seq_relevant(tw, tl, cmp & ~uint32_t(kRegA)) | dev_seq_relevant(cw, cl, cmp & ~uint32_t(kRegA));
+  const uint32_t at = dev_seq_relevant(tw, tl, kRegA), ac = dev_seq_relevant(cw, cl, kRegA);
+  const uint32_t rel = rest | at | ac;
   const uint32_t drop = ext & ~rel;
   const bool carry_out = (rel & (1u << kDepF0)) == 0;
   if (drop) {
@@ -570,10 +582,13 @@ __device__ __forceinline__ void put_pair(const RoundBuf& R, uint32_t p, const De
     pr.nblocks >>= 1;
     pr.sweepf += 1;
   }
-  // A on which no compared output depends (a comparison whose flags are
-  // dead, say) is as good as independent: the A-independent sweeps, two
-  // values of A, decide the pair
-  if ((rel & kRegA) == 0) pr.keepR |= uint8_t(kXIndep);
+  // Two values of A decide the pair when no compared output but A depends
+  // on the input A (a comparison whose flags are dead or overwritten, A
+  // copied into a dead register) and each program keeps A or computes its A
+  // from other inputs: the argument of the A-independent sweeps under the
+  // pair's masks.
+  if (!(rest & kRegA) && (!(at & kRegA) || dev_seq_keeps_a(tw, tl)) && (!(ac & kRegA) || dev_seq_keeps_a(cw, cl)))
+    pr.keepR |= uint8_t(kXIndep);
   // compact classes: A-dependent pairs, and A-independent ones when those
   // are swept bit-sliced (units of kXBitsBlocks); the narrow state first
   pr.cmap = 0;
@@ -2128,6 +2143,7 @@ void dev_upload_tables(cudaStream_t s) {
   cudaMemcpyToSymbolAsync(g_aclass, op_aclass(), kNumOps, 0, cudaMemcpyHostToDevice, s);
   {
     cudaMemcpyToSymbolAsync(g_dep, op_deps(), sizeof(uint32_t) * kNumOps * kDepFields, 0, cudaMemcpyHostToDevice, s);
+    cudaMemcpyToSymbolAsync(g_keepa, op_keeps_a(), kNumOps, 0, cudaMemcpyHostToDevice, s);
     const CompactTables& C = compact_tables();
     cudaMemcpyToSymbolAsync(g_cren, C.ren, sizeof C.ren, 0, cudaMemcpyHostToDevice, s);
     cudaMemcpyToSymbolAsync(g_corig, C.orig, sizeof C.orig, 0, cudaMemcpyHostToDevice, s);
