@@ -6,7 +6,8 @@
 // leaves every output field whose set does not hold it unchanged.  (2) For
 // random pairs, many with dead flags and registers and an inserted write of
 // a dead register, a sweep that drops the swept registers no compared output
-// depends on (the others keeping the reference's values: a reduced sweep
+// depends on, or that both programs keep exactly and no other compared
+// output depends on (the others keeping the reference's values: a reduced sweep
 // stays reduced), keeps only carry 0 when no compared output depends on the
 // carry, and only A = 0, 1 when no compared output but A depends on A and
 // each program keeps A or computes it from other inputs (pair_a_free), gives
@@ -128,9 +129,28 @@ int main() {
       }
     }
   }
-  // (1b) instructions said to keep A leave it exactly as it was
+  // (1b) instructions said to keep A (or any register, or the memory byte)
+  // leave it exactly as it was
   int keepers = 0;
   for (int op = 0; op < orc::OpCodeCount; op++) {
+    const uint16_t kept = op_keeps()[op];
+    if (bool(kept & kRegA) != bool(op_keeps_a()[op])) {
+      std::printf("op %d (%s): the two keeps-A tables disagree\n", op, op_mnemonic(uint16_t(op)));
+      return 1;
+    }
+    for (int k = 0; k < 64; k++) {
+      const uint64_t r = rng(), r2 = rng();
+      orc::State st{uint8_t(r), uint8_t(r >> 8), uint8_t(r >> 16), uint8_t(r >> 24), uint8_t(r >> 32),
+                    uint8_t(r >> 40), uint8_t(r >> 48), uint8_t(r >> 56), uint16_t(r2), uint8_t(r2 >> 16)};
+      const orc::State in = st;
+      orc::Exec(st, uint16_t(op), uint16_t(rng()));
+      const int fields[7] = {2, 3, 4, 5, 6, 7, 9};
+      for (int g : fields)
+        if ((kept & (1u << g)) && get_field(st, g) != get_field(in, g)) {
+          std::printf("op %d (%s) is said to keep field %d but changes it\n", op, op_mnemonic(uint16_t(op)), g);
+          return 1;
+        }
+    }
     if (!op_keeps_a()[op]) continue;
     keepers++;
     for (int k = 0; k < 256; k++) {
@@ -177,7 +197,7 @@ int main() {
     const uint32_t ext = reads & (kRegB | kRegC | kRegD | kRegE | kRegH | kRegL | kRegM);
     const uint32_t cmp = kRegA | kRegSP | kRegM | (keepR << 2) | (keepF << kDepF0);
     const uint32_t rel = seq_relevant(tw, tn, cmp) | seq_relevant(cw, cn, cmp);
-    const uint32_t drop = ext & ~rel;
+    const uint32_t drop = (ext & ~rel) | pair_kept_out(tw, tn, cw, cn, cmp, ext);
     const bool carry_out = (rel & (1u << kDepF0)) == 0;
     const bool a_out = pair_a_free(tw, tn, cw, cn, cmp);
     if (!drop && !carry_out && !a_out) continue;

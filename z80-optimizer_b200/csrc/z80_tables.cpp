@@ -274,6 +274,7 @@ namespace z80b {
 
 namespace {
 uint8_t g_keeps_a[kNumOps];
+uint16_t g_keeps[kNumOps];
 }
 
 const uint32_t (*op_deps())[kDepFields] {
@@ -285,6 +286,13 @@ const uint32_t (*op_deps())[kDepFields] {
       for (int i = 0; i < 8; i++) {
         z.a[i].m = kRegA;
         z.a[i].id = i;
+        z.b[i].id = 8 + i;
+        z.c[i].id = 16 + i;
+        z.d[i].id = 24 + i;
+        z.e[i].id = 32 + i;
+        z.h[i].id = 40 + i;
+        z.l[i].id = 48 + i;
+        z.m[i].id = 56 + i;
         z.f[i].m = 1u << (kDepF0 + i);
         z.b[i].m = kRegB;
         z.c[i].m = kRegC;
@@ -315,9 +323,20 @@ const uint32_t (*op_deps())[kDepFields] {
       d[8] = sp;
       d[9] = join8(z.m);
       for (int k = 0; k < 8; k++) d[kDepF0 + k] = z.f[k].m;
-      bool keeps = true;
-      for (int i = 0; i < 8; i++) keeps = keeps && z.a[i].id == i;
-      g_keeps_a[op] = keeps ? 1 : 0;
+      bool ka = true, kb = true, kc = true, kd = true, ke = true, kh = true, kl = true, km = true;
+      for (int i = 0; i < 8; i++) {
+        ka = ka && z.a[i].id == i;
+        kb = kb && z.b[i].id == 8 + i;
+        kc = kc && z.c[i].id == 16 + i;
+        kd = kd && z.d[i].id == 24 + i;
+        ke = ke && z.e[i].id == 32 + i;
+        kh = kh && z.h[i].id == 40 + i;
+        kl = kl && z.l[i].id == 48 + i;
+        km = km && z.m[i].id == 56 + i;
+      }
+      g_keeps_a[op] = ka ? 1 : 0;
+      g_keeps[op] = uint16_t((ka ? kRegA : 0) | (kb ? kRegB : 0) | (kc ? kRegC : 0) | (kd ? kRegD : 0) |
+                             (ke ? kRegE : 0) | (kh ? kRegH : 0) | (kl ? kRegL : 0) | (km ? kRegM : 0));
     }
   });
   return T;
@@ -326,6 +345,27 @@ const uint32_t (*op_deps())[kDepFields] {
 const uint8_t* op_keeps_a() {
   (void)op_deps();
   return g_keeps_a;
+}
+
+const uint16_t* op_keeps() {
+  (void)op_deps();
+  return g_keeps;
+}
+
+uint32_t seq_keeps(const uint32_t* s, int n) {
+  uint32_t k = 0xFFFFu;
+  for (int i = 0; i < n; i++) k &= op_keeps()[insn_op(s[i])];
+  return k;
+}
+
+uint32_t pair_kept_out(const uint32_t* t, int tn, const uint32_t* c, int cn, uint32_t cmp, uint32_t swept) {
+  const uint32_t both = seq_keeps(t, tn) & seq_keeps(c, cn) & swept & ~uint32_t(kRegA);
+  uint32_t out = 0;
+  for (uint32_t b = both; b; b &= b - 1) {
+    const uint32_t r = b & (0u - b);
+    if (!((seq_relevant(t, tn, cmp & ~r) | seq_relevant(c, cn, cmp & ~r)) & r)) out |= r;
+  }
+  return out;
 }
 
 bool seq_keeps_a(const uint32_t* s, int n) {

@@ -53,6 +53,15 @@ bool seq_keeps_a(const uint32_t* s, int n);
 // constant in each program (the argument of the A-independent sweeps, now
 // under the dead flags and registers).
 bool pair_a_free(const uint32_t* t, int tn, const uint32_t* c, int cn, uint32_t cmp);
+// The same for every register and the memory byte (read-mask bits): kNumOps
+// entries of the fields the instruction leaves exactly as they were, and
+// their AND over a sequence.
+const uint16_t* op_keeps();
+uint32_t seq_keeps(const uint32_t* s, int n);
+// Swept registers (`swept`, B..L and M bits) that both programs keep
+// exactly and that no other compared output depends on: their compared
+// outputs are equal whatever their value, so one value decides.
+uint32_t pair_kept_out(const uint32_t* t, int tn, const uint32_t* c, int cn, uint32_t cmp, uint32_t swept);
 const char* op_mnemonic(uint16_t op);     // "ADD A, n" style with placeholders
 // The instruction that does op's work with the 8-bit registers renamed:
 // register r (0..5 = B, C, D, E, H, L) plays the part of map[r] (map is a

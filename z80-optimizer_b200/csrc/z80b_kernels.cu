@@ -66,6 +66,7 @@ __device__ uint8_t g_opregs[kNumOps];
 // whether it leaves A exactly as it was (op_keeps_a)
 __device__ uint32_t g_dep[kNumOps][kDepFields];
 __device__ uint8_t g_keepa[kNumOps];
+__device__ uint16_t g_keeps[kNumOps];  // fields (read-mask bits) an opcode leaves exactly as they were
 __device__ int16_t g_wren[kWideSets][kNumOps];
 __device__ int8_t g_worig[kWideSets][4];
 __device__ uint8_t g_wid[64];
@@ -142,6 +143,11 @@ __device__ __forceinline__ uint32_t dev_seq_relevant(const uint32_t* w, uint32_t
     out = in;
   }
   return out;
+}
+__device__ __forceinline__ uint32_t dev_seq_keeps(const uint32_t* w, uint32_t n) {
+  uint32_t k = 0xFFFFu;
+  for (uint32_t i = 0; i < n; i++) k &= g_keeps[w[i] & 0xFFFFu];
+  return k;
 }
 __device__ __forceinline__ bool dev_seq_keeps_a(const uint32_t* w, uint32_t n) {
   for (uint32_t i = 0; i < n; i++)
@@ -569,7 +575,14 @@ __device__ __forceinline__ void put_pair(const RoundBuf& R, uint32_t p, const De
   const uint32_t rest = dev_seq_relevant(tw, tl, cmp & ~uint32_t(kRegA)) | dev_seq_relevant(cw, cl, cmp & ~uint32_t(kRegA));
   const uint32_t at = dev_seq_relevant(tw, tl, kRegA), ac = dev_seq_relevant(cw, cl, kRegA);
   const uint32_t rel = rest | at | ac;
-  const uint32_t drop = ext & ~rel;
+  uint32_t drop = ext & ~rel;
+  // a swept register both programs keep exactly, on which no other compared
+  // output depends, compares equal whatever its value: one value decides
+  const uint32_t both = dev_seq_keeps(tw, tl) & dev_seq_keeps(cw, cl) & ext & ~drop;
+  for (uint32_t b = both; b; b &= b - 1) {
+    const uint32_t r = b & (0u - b);
+    if (!((dev_seq_relevant(tw, tl, cmp & ~r) | dev_seq_relevant(cw, cl, cmp & ~r)) & r)) drop |= r;
+  }
   const bool carry_out = (rel & (1u << kDepF0)) == 0;
   if (drop) {
     const bool red = (reads & kRegSP) != 0 || __popc(ext) > 2;
@@ -2144,6 +2157,7 @@ void dev_upload_tables(cudaStream_t s) {
   {
     cudaMemcpyToSymbolAsync(g_dep, op_deps(), sizeof(uint32_t) * kNumOps * kDepFields, 0, cudaMemcpyHostToDevice, s);
     cudaMemcpyToSymbolAsync(g_keepa, op_keeps_a(), kNumOps, 0, cudaMemcpyHostToDevice, s);
+    cudaMemcpyToSymbolAsync(g_keeps, op_keeps(), sizeof(uint16_t) * kNumOps, 0, cudaMemcpyHostToDevice, s);
     const CompactTables& C = compact_tables();
     cudaMemcpyToSymbolAsync(g_cren, C.ren, sizeof C.ren, 0, cudaMemcpyHostToDevice, s);
     cudaMemcpyToSymbolAsync(g_corig, C.orig, sizeof C.orig, 0, cudaMemcpyHostToDevice, s);
