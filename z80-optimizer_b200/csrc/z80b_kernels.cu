@@ -1903,28 +1903,91 @@ __global__ void k_qc_top(const unsigned long long* __restrict__ keys, uint32_t n
 // word 2 (the flags are compared per candidate, under the dead flags), which
 // is every candidate that can pass.  Entries of a bucket are in pool order,
 // so survivors come out in enumeration order as in the full scan.
+// Four targets per warp, eight lanes each: lane 8g + v runs target t0 + g on
+// vector v, so one pass of the dispatch loop, the output shuffles and the
+// bucket loop serve four targets (the buckets hold a candidate or two; a
+// warp per target left three quarters of its lanes idle).  Lanes of a group
+// that has no target (past the end) take part in the warp's collectives
+// with nothing to do.
+__device__ __forceinline__ void qc_target4(const DevTargets& T, uint32_t t, bool valid, QCTarget& g) {
+  const unsigned lane = lane_id();
+  const unsigned sub = lane & 7u;
+  const uint32_t tl = valid ? target_len(T, t) : 0u;
+  const uint32_t pw = sub < tl ? T.insn[(size_t)t * T.stride + sub] : 0u;
+  uint32_t sz = 0, ts = 0, rd = 0;
+  if (sub < tl) {
+    const OpInfo oi = g_ops[pw & 0xFFFFu];
+    sz = oi.size;
+    ts = oi.tstates;
+    rd = oi.reads;
+  }
+#pragma unroll
+  for (int off = 2; off >= 1; off >>= 1) {
+    sz += __shfl_down_sync(kFull, sz, off, 8);
+    ts += __shfl_down_sync(kFull, ts, off, 8);
+    rd |= __shfl_down_sync(kFull, rd, off, 8);
+  }
+  g.tl = tl;
+  g.tb = __shfl_sync(kFull, sz, 0, 8);
+  g.tts = __shfl_sync(kFull, ts, 0, 8);
+  g.trd = __shfl_sync(kFull, rd, 0, 8);
+  Z80S s = vec_state(int(sub));
+  const uint32_t steps = __reduce_max_sync(kFull, tl);
+#pragma unroll 1
+  for (uint32_t i = 0; i < steps; i++) {
+    const uint32_t w = __shfl_sync(kFull, pw, int(i), 8);
+    if (i < tl) z_step(s, w & 0xFFFFu, w >> 16);
+  }
+  uint32_t w[3];
+  z_pack(s, w);
+#pragma unroll
+  for (int v = 0; v < 8; v++) {
+    g.tw[v][0] = __shfl_sync(kFull, w[0], v, 8);
+    g.tw[v][1] = __shfl_sync(kFull, w[1], v, 8);
+    g.tw[v][2] = __shfl_sync(kFull, w[2], v, 8);
+  }
+  const uint32_t dead = valid ? target_dead(T, t) & 0xFFu : 0u;
+  const uint32_t dregs = valid ? target_dead_regs(T, t) & 0x3Fu : 0u;
+  g.keep0 = 0xFFu | ((~dead & 0xFFu) << 8) | ((dregs & 1u) ? 0u : 0xFF0000u) | ((dregs & 2u) ? 0u : 0xFF000000u);
+  g.keep1 = ((dregs & 4u) ? 0u : 0xFFu) | ((dregs & 8u) ? 0u : 0xFF00u) | ((dregs & 16u) ? 0u : 0xFF0000u) |
+            ((dregs & 32u) ? 0u : 0xFF000000u);
+}
+
 template <bool COLLECT>
 __global__ void __launch_bounds__(kBlock) k_qc_bucket(DevTargets T, DevPool P, QCConfig cfg, QCIndex ix, QCOut o) {
   const unsigned lane = lane_id();
+  const unsigned sub = lane & 7u, gshift = lane & ~7u;
+  const unsigned group_lt = lanemask_lt() & (0xFFu << gshift);
   const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const uint32_t nw = gridDim.x * (blockDim.x >> 5);
   unsigned long long my_checks = 0;
-  for (uint32_t t = gw; t < T.n; t += nw) {
+  for (uint32_t t0 = gw * 4u; t0 < T.n; t0 += nw * 4u) {
+    const uint32_t t = t0 + (lane >> 3);
+    const bool valid = t < T.n;
     uint32_t nf_total = 0, obase = 0;
+    bool work = valid;
     if (COLLECT) {
-      nf_total = o.cnt_f[t];
-      if (nf_total + o.cnt_m[t] == 0) continue;
-      obase = o.base[t];
+      if (valid) {
+        nf_total = o.cnt_f[t];
+        work = nf_total + o.cnt_m[t] != 0;
+        obase = o.base[t];
+      }
+      if (!__any_sync(kFull, work)) continue;
     }
     QCTarget g;
-    qc_target(T, t, g);
-    const uint32_t m = target_dead_regs(T, t) & 0x3Fu;
+    qc_target4(T, t, valid, g);
+    const uint32_t m = valid ? target_dead_regs(T, t) & 0x3Fu : 0u;
     const uint32_t h = bucket_hash(g.tw[0][0] & key_keep0(m), g.tw[0][1] & key_keep1(m), g.tw[0][2] & cfg.w2mask);
-    const uint32_t* top = ix.top + m * (kQCTop + 1) + (h >> (32 - kQCTopBits));
-    const uint32_t r0 = top[0], r1 = top[1];
+    uint32_t r0 = 0, r1 = 0;
+    if (work) {
+      const uint32_t* top = ix.top + m * (kQCTop + 1) + (h >> (32 - kQCTopBits));
+      r0 = top[0];
+      r1 = top[1];
+    }
+    const uint32_t iters = (__reduce_max_sync(kFull, r1 - r0) + 7u) / 8u;
     uint32_t nf = 0, nm = 0, lf = 0, lm = 0;
-    for (uint32_t base = r0; base < r1; base += 32) {
-      const uint32_t i = base + lane;
+    for (uint32_t k = 0; k < iters; k++) {
+      const uint32_t i = r0 + 8u * k + sub;
       bool fp = false, mp = false;
       uint32_t diff = 0, c = 0;
       if (i < r1) {
@@ -1933,18 +1996,42 @@ __global__ void __launch_bounds__(kBlock) k_qc_bucket(DevTargets T, DevPool P, Q
         if (uint32_t(key >> 16) == h && P.size[c] < g.tb)
           qc_candidate(P, P.qc[c], c, g, cfg.w2mask, cfg.all_hits != 0, fp, mp, diff);
       }
-      qc_emit<COLLECT>(o, fp, mp, c, diff, obase, nf_total, nf, nm, lf, lm);
+      if constexpr (!COLLECT) {
+        lf += fp ? 1u : 0u;
+        lm += mp ? 1u : 0u;
+      } else {
+        // this group's survivors of the step, in enumeration order
+        const unsigned bf = __ballot_sync(kFull, fp), bm = __ballot_sync(kFull, mp);
+        if (fp) {
+          const uint32_t idx = obase + nf + __popc(bf & group_lt);
+          o.surv[idx] = c;
+          o.sdiff[idx] = uint16_t(diff);
+        }
+        if (mp) {
+          const uint32_t idx = obase + nf_total + nm + __popc(bm & group_lt);
+          o.surv[idx] = c;
+          o.sdiff[idx] = uint16_t(diff);
+        }
+        nf += __popc((bf >> gshift) & 0xFFu);
+        nm += __popc((bm >> gshift) & 0xFFu);
+      }
     }
     if constexpr (!COLLECT) {
-      nf = __reduce_add_sync(kFull, lf);
-      nm = __reduce_add_sync(kFull, lm);
-      if (lane == 0) {
+#pragma unroll
+      for (int off = 4; off >= 1; off >>= 1) {
+        lf += __shfl_xor_sync(kFull, lf, off);
+        lm += __shfl_xor_sync(kFull, lm, off);
+      }
+      if (sub == 0 && valid) {
         my_checks += ix.elig_lt[g.tb < 255u ? g.tb : 255u];
-        qc_count_out(o, t, g, nf, nm);
+        qc_count_out(o, t, g, lf, lm);
       }
     }
   }
-  if (!COLLECT && lane == 0 && my_checks) atomicAdd(o.checks, my_checks);
+  if constexpr (!COLLECT) {
+    for (int off = 16; off; off >>= 1) my_checks += __shfl_down_sync(kFull, my_checks, off);
+    if (lane == 0 && my_checks) atomicAdd(o.checks, my_checks);
+  }
 }
 
 // Warp per target: (re)fills the slots of each lane whose slots are used up
@@ -2232,7 +2319,7 @@ void launch_qc_bucket(const DevTargets& T, const DevPool& P, const QCConfig& cfg
   static std::atomic<int> occ[2][kMaxCachedDevices];
   const int per_sm = collect ? blocks_per_sm(occ[1], k_qc_bucket<true>, kBlock, 0, 0)
                              : blocks_per_sm(occ[0], k_qc_bucket<false>, kBlock, 0, 0);
-  unsigned need = grid_for(T.n, kBlock / 32);
+  unsigned need = grid_for((T.n + 3u) / 4u, kBlock / 32);  // four targets per warp
   unsigned grid = unsigned(dev_num_sms() * per_sm);
   if (grid > need) grid = need;
   if (collect) k_qc_bucket<true><<<grid, kBlock, 0, s>>>(T, P, cfg, ix, o);
