@@ -64,6 +64,29 @@ struct DBuf {
   }
 };
 
+// Pinned host memory (device-to-host copies run as DMA at full speed).
+struct HBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~HBuf() {
+    if (p) cudaFreeHost(p);
+  }
+  cudaError_t ensure(size_t b) {
+    if (b <= bytes && p) return cudaSuccess;
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    bytes = 0;
+    size_t want = std::max<size_t>(b, 4096);
+    cudaError_t e = cudaHostAlloc(&p, want, cudaHostAllocDefault);
+    if (e == cudaSuccess) bytes = want;
+    return e;
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
 struct PoolBufs {
   DBuf insn, qc, mid, size, prune, reads, lens;
   // QuickCheck bucket index (pools of at most kQCIndexMax candidates)
@@ -166,6 +189,7 @@ struct z80b_ctx {
   DBuf pairs, pair_src, nchunks, cbase, nchunks_x, cbase_x, nchunks_c, cbase_c, nchunks_w, cbase_w, nchunks_r,
       cbase_r, rejected, npairs, counter, states;
   DBuf rcnt, rbase, rules, checked, surv_target, midpass, flag;
+  HBuf h_rules;               // pinned staging of the device rules read back
   DBuf cub_tmp;
   DBuf hits, nhits, fpq;
   DBuf v_tgt, v_cand, v_tl, v_cl, v_dead, v_out, v_fd, v_in, v_outs;
@@ -522,6 +546,13 @@ int validate_job(z80b_ctx* ctx, const z80b_job* job) {
   if ((job->flags & Z80B_JOB_NO_EXHAUSTIVE) && job->mode != Z80B_MODE_ALL)
     return fail(ctx, Z80B_EINVAL, "Z80B_JOB_NO_EXHAUSTIVE needs Z80B_MODE_ALL");
   if (job->global_dead_flags > 0xFF) return fail(ctx, Z80B_EINVAL, "dead flags > 0xFF");
+  return Z80B_OK;
+}
+
+// The targets themselves (lengths, opcodes, dead-register masks).  Runs after
+// validate_job, while the targets' upload is in flight; nothing reads the
+// device copy before this returns Z80B_OK.
+int validate_targets(z80b_ctx* ctx, const z80b_job* job) {
   // the first bad target (the reported one is the lowest index, as a
   // serial scan would find); the scan runs on several host threads
   std::atomic<uint64_t> first_bad{~0ull};
@@ -594,7 +625,7 @@ struct Timer {
   }
 };
 
-void to_rules(z80b_ctx* ctx, const std::vector<DevRule>& dr, const uint32_t* targets, const uint8_t* tlens,
+void to_rules(z80b_ctx* ctx, const DevRule* dr, size_t ndr, const uint32_t* targets, const uint8_t* tlens,
               uint32_t tlen, uint32_t stride, uint32_t mode, uint32_t tindex_offset, z80b_rule* out);
 
 // Hands each target's rules to a callback as soon as both of its
@@ -727,15 +758,15 @@ int rounds_on_device(z80b_ctx* ctx, RoundGraph& g, const DevTargets& T, const De
     g.key = key;
     trace("round loop captured (%s pass)", ps ? "length-2" : "length-1");
   }
-  // build, scan, [rescan], sweeps, resolve
-  const int per_iter = (ps ? 3 : 2) + 1 + 2 + (R.compact ? 1 : 0) + (R.wide ? 2 : 0);
+  // build, scan (3), [rescan], sweeps, resolve
+  const int per_iter = (ps ? 5 : 4) + 1 + 2 + (R.compact ? 1 : 0) + (R.wide ? 2 : 0);
   CK(cudaMemsetAsync(ctl, 0, sizeof(RoundCtl), s));
   int ke = kbegin(ctx, 1);
   CK(cudaGraphLaunch(g.exec, s));
   kend(ctx, ke);
   CKR(check_launch(ctx, "round loop"));
   RoundCtl h{};
-  CK(cudaMemcpyAsync(&h, ctl, sizeof h, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&h, ctl, offsetof(RoundCtl, bsum), cudaMemcpyDeviceToHost, s));  // the counters
   CK(cudaStreamSynchronize(s));
   if (h.overrun) return fail(ctx, Z80B_ETIMEOUT, "device round loop did not end within %u iterations", kMaxRoundIters);
   *rounds += h.rounds;
@@ -1098,14 +1129,13 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
 }
 
 // Converts device rules to z80b_rule records.
-void to_rules(z80b_ctx* ctx, const std::vector<DevRule>& dr, const uint32_t* targets, const uint8_t* tlens,
+void to_rules(z80b_ctx* ctx, const DevRule* dr, size_t ndr, const uint32_t* targets, const uint8_t* tlens,
               uint32_t tlen, uint32_t stride, uint32_t mode, uint32_t tindex_offset, z80b_rule* out) {
   const PoolBufs& P = (mode == Z80B_MODE_ALL) ? (ctx->loaded.loaded ? ctx->loaded : ctx->firstop) : ctx->pool8;
-  host_parallel(dr.size(), [&](size_t lo, size_t hi) {
+  host_parallel(ndr, [&](size_t lo, size_t hi) {
     for (size_t i = lo; i < hi; i++) {
       const DevRule& r = dr[i];
       z80b_rule& o = out[i];
-      std::memset(&o, 0, sizeof o);
       const uint32_t* t = targets + (size_t)r.target * stride;
       int tl = tlens ? tlens[r.target] : int(tlen);
       const PoolBufs& PC = (r.clen == 2) ? ctx->pairpool->pool : P;
@@ -1113,8 +1143,11 @@ void to_rules(z80b_ctx* ctx, const std::vector<DevRule>& dr, const uint32_t* tar
       int cl = int(PC.len);
       o.src_len = tl;
       o.rep_len = cl;
-      for (int k = 0; k < tl; k++) o.src[k] = t[k];
-      for (int k = 0; k < cl; k++) o.rep[k] = c[k];
+      // every field is written (no memset first): the record is 64 bytes
+      // and a search returns hundreds of thousands of them
+      for (int k = 0; k < 4; k++) o.src[k] = k < tl ? t[k] : 0u;
+      for (int k = 0; k < 4; k++) o.rep[k] = k < cl ? c[k] : 0u;
+      o.reserved = 0;
       o.bytes_saved = seq_bytes(t, tl) - seq_bytes(c, cl);
       o.cycles_saved = seq_tstates(t, tl) - seq_tstates(c, cl);
       o.dead_flags = (r.kind == 0) ? 0 : int(r.diff & 0xFFu);
@@ -1181,7 +1214,7 @@ int Reporter::update(z80b_ctx* ctx, uint32_t n, const Lanes& L, const Lanes& L2,
     if (!final_all) continue;
     done[t] = 1;
     out.resize(dr.size());
-    if (!dr.empty()) to_rules(ctx, dr, targets, tlens, tlen, stride, Z80B_MODE_FIRST, 0, out.data());
+    if (!dr.empty()) to_rules(ctx, dr.data(), dr.size(), targets, tlens, tlen, stride, Z80B_MODE_FIRST, 0, out.data());
     cb(user, t, out.data(), uint32_t(out.size()));
   }
   return Z80B_OK;
@@ -1241,6 +1274,18 @@ int upload_targets(z80b_ctx* ctx, Staged& S, const z80b_job* job, DevTargets* T,
   return Z80B_OK;
 }
 
+// Reads the first nr device rules into the context's pinned staging buffer
+// (*out points there until the next call).
+int rules_to_host(z80b_ctx* ctx, uint64_t nr, const DevRule** out) {
+  *out = nullptr;
+  if (!nr) return Z80B_OK;
+  CK(ctx->h_rules.ensure(sizeof(DevRule) * nr));
+  CK(cudaMemcpyAsync(ctx->h_rules.p, ctx->rules.p, sizeof(DevRule) * nr, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  *out = ctx->h_rules.as<DevRule>();
+  return Z80B_OK;
+}
+
 DevTargets staged_targets(Staged& S) {
   DevTargets T{};
   T.insn = S.d_targets.as<uint32_t>();
@@ -1281,7 +1326,7 @@ int run_staged(z80b_ctx* ctx, z80b_stats* st, uint64_t* nr, std::vector<z80b_rul
       if (host_rules) {
         size_t off = host_rules->size();
         host_rules->resize(off + k);
-        to_rules(ctx, dr, host_targets + (size_t)i * T.stride, S.lens.empty() ? nullptr : &S.lens[i],
+        to_rules(ctx, dr.data(), dr.size(), host_targets + (size_t)i * T.stride, S.lens.empty() ? nullptr : &S.lens[i],
                  job.target_len, T.stride, job.mode, i, host_rules->data() + off);
       }
     }
@@ -1665,6 +1710,7 @@ static void sweep_kernel_names(uint32_t mask, char* out, size_t cap) {
 int z80b_autotune(z80b_ctx* ctx, const z80b_job* sample, z80b_tune_result* out) {
   if (!ctx) return Z80B_EINVAL;
   CKR(validate_job(ctx, sample));
+  CKR(validate_targets(ctx, sample));
   if (sample->path != Z80B_PATH_BATCHED) return fail(ctx, Z80B_EINVAL, "autotune runs the batched path");
   cudaSetDevice(ctx->device);
   DevTargets T;
@@ -1727,8 +1773,10 @@ int z80b_stage_job(z80b_ctx* ctx, const z80b_job* job) {
   cudaSetDevice(ctx->device);
   DevTargets T;
   CKR(upload_targets(ctx, ctx->staged, job, &T, true));
+  const int v = validate_targets(ctx, job);  // while the copy runs
   CK(cudaStreamSynchronize(ctx->stream));
-  return Z80B_OK;
+  if (v != Z80B_OK) ctx->staged.valid = false;
+  return v;
 }
 
 int z80b_run_staged(z80b_ctx* ctx, uint64_t* n_rules, z80b_stats* stats) {
@@ -1753,13 +1801,10 @@ int z80b_fetch_rules(z80b_ctx* ctx, z80b_rule* out, uint64_t cap, uint64_t* n_ru
   if (nr > cap) return fail(ctx, Z80B_ECAPACITY, "%llu rules, capacity %llu", (unsigned long long)nr,
                             (unsigned long long)cap);
   if (nr && !out) return fail(ctx, Z80B_EINVAL, "null output");
-  std::vector<DevRule> dr(nr);
-  if (nr) {
-    CK(cudaMemcpyAsync(dr.data(), ctx->rules.p, sizeof(DevRule) * nr, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-  }
+  const DevRule* dr = nullptr;
+  CKR(rules_to_host(ctx, nr, &dr));
   const Staged& S = ctx->staged;
-  to_rules(ctx, dr, S.targets.data(), S.lens.empty() ? nullptr : S.lens.data(), S.job.target_len,
+  to_rules(ctx, dr, nr, S.targets.data(), S.lens.empty() ? nullptr : S.lens.data(), S.job.target_len,
            S.job.target_stride, S.job.mode, 0, out);
   return Z80B_OK;
 }
@@ -1775,6 +1820,15 @@ static int search_impl(z80b_ctx* ctx, const z80b_job* job, z80b_rule* out, uint6
   DevTargets T;
   CKR(upload_targets(ctx, ctx->staged, job, &T, false));
   ctx->staged.valid = false;  // this job's targets are not kept for z80b_fetch_rules
+  {
+    // the host scan of the targets runs while their copy is in flight; on
+    // an error the copy ends before the caller gets its buffers back
+    const int v = validate_targets(ctx, job);
+    if (v != Z80B_OK) {
+      cudaStreamSynchronize(ctx->stream);
+      return v;
+    }
+  }
   uint64_t nr = 0;
   if (job->path == Z80B_PATH_PLAIN) {
     std::vector<z80b_rule> hr;
@@ -1801,12 +1855,9 @@ static int search_impl(z80b_ctx* ctx, const z80b_job* job, z80b_rule* out, uint6
   if (nr > cap)
     return fail(ctx, Z80B_ECAPACITY, "%llu rules, capacity %llu", (unsigned long long)nr, (unsigned long long)cap);
   if (nr && !out) return fail(ctx, Z80B_EINVAL, "null output");
-  std::vector<DevRule> dr(nr);
-  if (nr) {
-    CK(cudaMemcpyAsync(dr.data(), ctx->rules.p, sizeof(DevRule) * nr, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-  }
-  to_rules(ctx, dr, job->targets, job->target_lens, job->target_len, job->target_stride, job->mode, 0, out);
+  const DevRule* dr = nullptr;
+  CKR(rules_to_host(ctx, nr, &dr));
+  to_rules(ctx, dr, nr, job->targets, job->target_lens, job->target_len, job->target_stride, job->mode, 0, out);
   return Z80B_OK;
 }
 

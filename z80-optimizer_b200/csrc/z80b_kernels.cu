@@ -2428,74 +2428,136 @@ void launch_round_resolve(const RoundBuf& R, uint32_t npairs, const QCOut& q, co
   k_round_resolve<<<grid_for(npairs, 256), 256, 0, s>>>(R, npairs, q, L, max_spec, nullptr);
 }
 
-// One block: the round's pair count, the exclusive prefix of each class's
-// chunk counts over the round's pairs (each thread sums a contiguous run,
-// the block scans the 1,024 run sums, each thread writes its run), the
-// classes' totals, cleared dispensers, and the loop condition.
-constexpr int kScanThreads = 1024;
-__global__ void __launch_bounds__(kScanThreads) k_round_scan(RoundBuf R, RoundCtl* __restrict__ ctl,
-                                                             const uint32_t* __restrict__ refill,
-                                                             cudaGraphConditionalHandle loop) {
-  __shared__ unsigned long long part[kScanThreads];
-  const uint32_t tid = threadIdx.x;
+// The round's chunk prefixes on the device, in three launches: every block
+// of k_round_scan_sum sums its contiguous segment of each class's chunk
+// counts (coalesced tiles), k_round_scan_write rescans its segment from the
+// sum of the blocks before it, and k_round_scan_ctl takes the totals, clears
+// the dispensers, keeps the loop's counters and sets its condition.  The
+// first two only read RoundCtl; the third alone writes it.
+constexpr int kRScanThreads = 256;
+static_assert(kRScanThreads == kRScanBlocks, "one block sum per thread in the offset reduction");
+
+__device__ __forceinline__ bool rscan_on(const RoundBuf& R, int c) { return !((c == 2 && !R.compact) || (c >= 3 && !R.wide)); }
+__device__ __forceinline__ const unsigned long long* rscan_in(const RoundBuf& R, int c) {
+  return c == 0 ? R.nchunks : (c == 1 ? R.nchunks_x : (c == 2 ? R.nchunks_c : (c == 3 ? R.nchunks_w : R.nchunks_r)));
+}
+__device__ __forceinline__ unsigned long long* rscan_out(const RoundBuf& R, int c) {
+  return c == 0 ? R.cbase : (c == 1 ? R.cbase_x : (c == 2 ? R.cbase_c : (c == 3 ? R.cbase_w : R.cbase_r)));
+}
+// The pairs to scan: the build's count, or 0 once the loop is past its bound.
+__device__ __forceinline__ uint32_t rscan_np(const RoundBuf& R, const RoundCtl* ctl) {
+  const uint32_t np = min(*R.npairs, R.cap);
+  return ctl->iters + 1 >= kMaxRoundIters ? 0u : np;
+}
+// Block-wide sum, the result in every thread (red: kRScanThreads / 32 slots).
+__device__ __forceinline__ unsigned long long rscan_block_sum(unsigned long long v, unsigned long long* red) {
+#pragma unroll
+  for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  __syncthreads();  // red is free (an earlier call has been read)
+  if (lane_id() == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  unsigned long long t = 0;
+#pragma unroll
+  for (int w = 0; w < kRScanThreads / 32; w++) t += red[w];
+  return t;
+}
+
+__global__ void __launch_bounds__(kRScanThreads) k_round_scan_sum(RoundBuf R, RoundCtl* __restrict__ ctl) {
+  __shared__ unsigned long long red[kRScanThreads / 32];
+  const uint32_t np = rscan_np(R, ctl);
+  if (np == 0) return;
+  const uint32_t per = (np + kRScanBlocks - 1) / kRScanBlocks;
+  const uint32_t lo = uint32_t(min((unsigned long long)blockIdx.x * per, (unsigned long long)np));
+  const uint32_t hi = lo + min(per, np - lo);
+  for (int c = 0; c < 5; c++) {
+    if (!rscan_on(R, c)) continue;  // the same for every block
+    const unsigned long long* __restrict__ in = rscan_in(R, c);
+    unsigned long long v = 0;
+    for (uint32_t i = lo + threadIdx.x; i < hi; i += kRScanThreads) v += in[i];
+    v = rscan_block_sum(v, red);
+    if (threadIdx.x == 0) ctl->bsum[c][blockIdx.x] = v;  // 0 for an empty segment
+  }
+}
+
+__global__ void __launch_bounds__(kRScanThreads) k_round_scan_write(RoundBuf R, const RoundCtl* __restrict__ ctl) {
+  __shared__ unsigned long long red[kRScanThreads / 32];
+  const uint32_t np = rscan_np(R, ctl);
+  if (np == 0) return;
+  const uint32_t per = (np + kRScanBlocks - 1) / kRScanBlocks;
+  const uint32_t lo = uint32_t(min((unsigned long long)blockIdx.x * per, (unsigned long long)np));
+  const uint32_t hi = lo + min(per, np - lo);
+  const unsigned lane = lane_id(), warp = threadIdx.x >> 5;
+  for (int c = 0; c < 5; c++) {
+    if (!rscan_on(R, c)) continue;
+    const unsigned long long* __restrict__ in = rscan_in(R, c);
+    unsigned long long* __restrict__ out = rscan_out(R, c);
+    // chunks of the blocks before this one
+    unsigned long long run = rscan_block_sum(threadIdx.x < blockIdx.x ? ctl->bsum[c][threadIdx.x] : 0ull, red);
+    for (uint32_t base = lo; base < hi; base += kRScanThreads) {
+      const uint32_t i = base + threadIdx.x;
+      const unsigned long long v = i < hi ? in[i] : 0ull;
+      // inclusive warp scan, then the warps' totals
+      unsigned long long x = v;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(kFull, x, o);
+        if (lane >= unsigned(o)) x += y;
+      }
+      __syncthreads();  // red is free
+      if (lane == 31) red[warp] = x;
+      __syncthreads();
+      unsigned long long before = 0, tile = 0;
+#pragma unroll
+      for (int w = 0; w < kRScanThreads / 32; w++) {
+        before += unsigned(w) < warp ? red[w] : 0ull;
+        tile += red[w];
+      }
+      if (i < hi) out[i] = run + before + x - v;
+      run += tile;
+    }
+  }
+}
+
+__global__ void k_round_scan_ctl(RoundBuf R, RoundCtl* __restrict__ ctl, const uint32_t* __restrict__ refill,
+                                 cudaGraphConditionalHandle loop) {
+  const unsigned lane = lane_id();
   const uint32_t np = min(*R.npairs, R.cap);
   const bool over = ctl->iters + 1 >= kMaxRoundIters;
-  __syncthreads();  // every thread has read ctl before thread 0 updates it
-  if (tid == 0) {
-    ctl->iters += 1;
-    if (over) {
-      // the loop has run far past any legitimate number of rounds: end it,
-      // sweep nothing more, and let the host report the error
-      ctl->overrun = 1;
-      cudaGraphSetConditional(loop, 0);
-    }
-    ctl->np = over ? 0u : np;
-    if (np && !over) {
-      ctl->rounds += 1;
-      ctl->pairs += np;
-    }
-    R.counter[0] = R.counter[1] = R.counter[2] = R.counter[3] = R.counter[4] = 0;
-    if (np == 0 || over) {
-      ctl->totals[0] = ctl->totals[1] = ctl->totals[2] = ctl->totals[3] = ctl->totals[4] = 0;
-      if (!refill || *refill == 0) cudaGraphSetConditional(loop, 0);
-    }
-  }
-  if (np == 0 || over) return;
-  const uint32_t per = (np + kScanThreads - 1) / kScanThreads;
-  const uint32_t lo = min(tid * per, np), hi = min(lo + per, np);
+  const bool empty = np == 0 || over;
+  unsigned long long tot[5];
+#pragma unroll
   for (int c = 0; c < 5; c++) {
-    const unsigned long long* in =
-        c == 0 ? R.nchunks : (c == 1 ? R.nchunks_x : (c == 2 ? R.nchunks_c : (c == 3 ? R.nchunks_w : R.nchunks_r)));
-    unsigned long long* out =
-        c == 0 ? R.cbase : (c == 1 ? R.cbase_x : (c == 2 ? R.cbase_c : (c == 3 ? R.cbase_w : R.cbase_r)));
-    if ((c == 2 && !R.compact) || (c >= 3 && !R.wide)) {  // the same for every thread
-      if (tid == 0) ctl->totals[c] = 0;
-      continue;
-    }
-    unsigned long long sum = 0;
-    for (uint32_t i = lo; i < hi; i++) sum += in[i];
-    part[tid] = sum;
-    __syncthreads();
-    // inclusive Hillis-Steele scan of the run sums
-    for (uint32_t d = 1; d < kScanThreads; d <<= 1) {
-      const unsigned long long v = tid >= d ? part[tid - d] : 0ull;
-      __syncthreads();
-      part[tid] += v;
-      __syncthreads();
-    }
-    unsigned long long run = part[tid] - sum;
-    for (uint32_t i = lo; i < hi; i++) {
-      out[i] = run;
-      run += in[i];
-    }
-    if (tid == kScanThreads - 1) ctl->totals[c] = part[tid];
-    __syncthreads();
+    unsigned long long v = 0;
+    if (!empty && rscan_on(R, c))
+      for (int b = lane; b < kRScanBlocks; b += 32) v += ctl->bsum[c][b];
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    tot[c] = v;
   }
+  if (lane != 0) return;
+  ctl->iters += 1;
+  if (over) {
+    // the loop has run far past any legitimate number of rounds: end it,
+    // sweep nothing more, and let the host report the error
+    ctl->overrun = 1;
+    cudaGraphSetConditional(loop, 0);
+  }
+  ctl->np = over ? 0u : np;
+  if (!empty) {
+    ctl->rounds += 1;
+    ctl->pairs += np;
+  }
+  R.counter[0] = R.counter[1] = R.counter[2] = R.counter[3] = R.counter[4] = 0;
+#pragma unroll
+  for (int c = 0; c < 5; c++) ctl->totals[c] = tot[c];
+  if (empty && (!refill || *refill == 0)) cudaGraphSetConditional(loop, 0);
 }
 
 void launch_round_scan(const RoundBuf& R, RoundCtl* ctl, const uint32_t* refill, cudaGraphConditionalHandle loop,
                        cudaStream_t s) {
-  k_round_scan<<<1, kScanThreads, 0, s>>>(R, ctl, refill, loop);
+  k_round_scan_sum<<<kRScanBlocks, kRScanThreads, 0, s>>>(R, ctl);
+  k_round_scan_write<<<kRScanBlocks, kRScanThreads, 0, s>>>(R, ctl);
+  k_round_scan_ctl<<<1, 32, 0, s>>>(R, ctl, refill, loop);
 }
 
 template <int K, int CLS>

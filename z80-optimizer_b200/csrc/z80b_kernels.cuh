@@ -164,10 +164,13 @@ void launch_round_resolve(const RoundBuf& R, uint32_t npairs, const QCOut& q, co
                           cudaStream_t s);
 
 // ---- device-driven rounds (one CUDA graph, a WHILE node over the round body)
-// The round's pair count and chunk totals stay on the device: k_round_scan
-// takes the count the build left in R.npairs, scans the chunk counts of the
-// five classes, clears the dispensers and ends the loop (sets the graph's
-// condition to 0) when the round is empty and no lane waits for a rescan.
+// The round's pair count and chunk totals stay on the device: the round
+// scan (three launches) takes the count the build left in R.npairs, scans
+// the chunk counts of the five classes (per-block segment sums in bsum, then
+// each segment from its blocks' offset), clears the dispensers and ends the
+// loop (sets the graph's condition to 0) when the round is empty and no lane
+// waits for a rescan.
+constexpr int kRScanBlocks = 256;
 struct RoundCtl {
   unsigned long long totals[5];  // chunks of the current round: bit-sliced, A-independent, compact, wide,
                                  // register state
@@ -176,6 +179,7 @@ struct RoundCtl {
   uint32_t iters;                // loop iterations (rounds, rescans, the last empty one)
   uint32_t np;                   // pairs of the current round
   uint32_t overrun;              // set when the loop stopped at kMaxRoundIters (an error)
+  unsigned long long bsum[5][kRScanBlocks];  // the current round's chunks per class and scan block
 };
 // Bound on the iterations of one device-driven loop: a loop that has not
 // ended by then stops and reports an error instead of running on.
