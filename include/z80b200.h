@@ -223,6 +223,8 @@ int z80b_exhaustive_noalloc(int device, const uint32_t* tgt, const uint8_t* tlen
 #define Z80B_OPT_WIDE_SWEEP 8       /* other A-dependent pairs naming at most four of B..L and not SP on the
                                        A/F/B/C/H/L/M-state kernel, and the rest that name neither SP nor the memory
                                        byte on the A/F/B..L-state kernel (1, default), or neither (0) */
+#define Z80B_OPT_CONCURRENT_SWEEPS 9 /* device-driven rounds: the sweep classes' kernels on parallel branches of the
+                                       round graph (1, default) or one after another (0) */
 int z80b_set_option(z80b_ctx* ctx, int option, int value);
 int z80b_get_option(const z80b_ctx* ctx, int option, int* value);
 

@@ -133,22 +133,26 @@ def test_compact_sweep_keeps_parity(ctx, O, compact, wide):
 @pytest.mark.parametrize("case", ["c3", "c2"])
 def test_device_rounds_equal_host_rounds(ctx, case):
     """The first-found rounds driven on the device (one CUDA graph, a WHILE
-    node over build / scan / sweep / resolve) and driven from the host give
-    the same rules, counters, rounds and swept pairs.  (The count of swept
-    states is not compared: how far other warps get into a pair's sweep
-    before they see it rejected is a matter of timing in either mode.)"""
+    node over build / scan / sweep / resolve), with the sweep classes on
+    parallel branches of the graph or one after another, and driven from the
+    host give the same rules, counters, rounds and swept pairs.  (The count
+    of swept states is not compared: how far other warps get into a pair's
+    sweep before they see it rejected is a matter of timing in every mode.)"""
     import workloads
-    saved = ctx.get_option(z80b.OPT_GRAPH_ROUNDS)
+    opts = [z80b.OPT_GRAPH_ROUNDS, z80b.OPT_CONCURRENT_SWEEPS]
+    saved = [ctx.get_option(o) for o in opts]
     try:
         res = []
-        for g in (1, 0):
+        for g, conc in ((1, 1), (1, 0), (0, 1)):
             ctx.set_option(z80b.OPT_GRAPH_ROUNDS, g)
+            ctx.set_option(z80b.OPT_CONCURRENT_SWEEPS, conc)
             if case == "c3":
                 rules, st = run(ctx, fixture())
             else:
                 rules, st = ctx.search(workloads.to_lists(workloads.c2_subset(6000, seed=4)), dead_flags=0xFF)
             res.append((dev_keys(rules), st.checked_ref, st.checks, st.rounds, st.exhaustive_pairs))
-        assert res[0] == res[1]
+        assert res[0] == res[1] == res[2]
         assert res[0][3] > 1  # several rounds
     finally:
-        ctx.set_option(z80b.OPT_GRAPH_ROUNDS, saved)
+        for o, v in zip(opts, saved):
+            ctx.set_option(o, v)

@@ -31,6 +31,9 @@
 #include <string>
 #include <thread>
 #include <vector>
+#if defined(__SSE2__)
+#include <emmintrin.h>
+#endif
 
 #include "../../include/z80b200.h"
 #include "z80_tables.h"
@@ -209,6 +212,11 @@ struct z80b_ctx {
   int wide = 1;               // Z80B_OPT_WIDE_SWEEP
   uint32_t sweep_kernels = 0; // kSweep* bits of the sweep kernels launched since the last reset
   int graph_rounds = 1;       // Z80B_OPT_GRAPH_ROUNDS
+  int concurrent_sweeps = 1;  // Z80B_OPT_CONCURRENT_SWEEPS
+  // capture-time streams and events of the device rounds' parallel sweep
+  // branches (created with the first graph that uses them)
+  cudaStream_t side[4] = {};
+  cudaEvent_t fork_ev = nullptr, join_ev[4] = {};
   DBuf roundctl;              // RoundCtl of the device-driven rounds
   RoundGraph rg1, rg2;        // instantiated round loops: length-1 and length-2 candidate passes
 };
@@ -516,10 +524,10 @@ int ensure_qc_index(z80b_ctx* ctx, PoolBufs& P, uint32_t w2mask) {
 }
 
 // Runs fn(lo, hi) over [0, n) split into contiguous parts on up to 16 host
-// threads (in the calling thread alone below 2^16 items).
+// threads (in the calling thread alone below 2^15 items).
 template <class F>
 void host_parallel(size_t n, F fn) {
-  constexpr size_t kMinPart = size_t(1) << 16;
+  constexpr size_t kMinPart = size_t(1) << 14;
   size_t parts = std::min<size_t>(16, std::max(1u, std::thread::hardware_concurrency()));
   parts = std::min(parts, n / kMinPart);
   if (parts <= 1) {
@@ -720,9 +728,17 @@ int rounds_on_device(z80b_ctx* ctx, RoundGraph& g, const DevTargets& T, const De
     key_put(key, *ps);
     key_put(key, *qres);
   }
+  key_put(key, ctx->concurrent_sweeps);
   if (!g.exec || g.key != key) {
     g.reset();
     warm_exhaustive_dev(R, ctx->exh_k);
+    if (ctx->concurrent_sweeps && !ctx->side[0]) {
+      CK(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming));
+      for (int i = 0; i < 4; i++) {
+        CK(cudaStreamCreateWithFlags(&ctx->side[i], cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&ctx->join_ev[i], cudaEventDisableTiming));
+      }
+    }
     CK(cudaGraphCreate(&g.graph, 0));
     cudaGraphConditionalHandle loop;
     CK(cudaGraphConditionalHandleCreate(&loop, g.graph, 1, cudaGraphCondAssignDefault));
@@ -745,7 +761,23 @@ int rounds_on_device(z80b_ctx* ctx, RoundGraph& g, const DevTargets& T, const De
       launch_round_build(T, P, q, L, R, s);
       launch_round_scan(R, ctl, nullptr, loop, s);
     }
-    launch_exhaustive_dev(T, P, R, ctl, ctx->exh_k, s);
+    {
+      // the classes' sweeps on parallel branches of the body graph
+      cudaStream_t ss[5] = {s, s, s, s, s};
+      if (ctx->concurrent_sweeps) {
+        cudaEventRecord(ctx->fork_ev, s);
+        for (int i = 0; i < 4; i++) {
+          cudaStreamWaitEvent(ctx->side[i], ctx->fork_ev, 0);
+          ss[i + 1] = ctx->side[i];
+        }
+      }
+      launch_exhaustive_dev(T, P, R, ctl, ctx->exh_k, ss);
+      if (ctx->concurrent_sweeps)
+        for (int i = 0; i < 4; i++) {
+          cudaEventRecord(ctx->join_ev[i], ctx->side[i]);
+          cudaStreamWaitEvent(s, ctx->join_ev[i], 0);
+        }
+    }
     launch_round_resolve_dev(R, ctl, ps ? *qres : q, L, max_spec, s);
     cudaGraph_t captured = nullptr;
     const cudaError_t ce = cudaStreamEndCapture(s, &captured);
@@ -1132,10 +1164,14 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
 void to_rules(z80b_ctx* ctx, const DevRule* dr, size_t ndr, const uint32_t* targets, const uint8_t* tlens,
               uint32_t tlen, uint32_t stride, uint32_t mode, uint32_t tindex_offset, z80b_rule* out) {
   const PoolBufs& P = (mode == Z80B_MODE_ALL) ? (ctx->loaded.loaded ? ctx->loaded : ctx->firstop) : ctx->pool8;
+  // Records go out with streaming stores when the output is 16-byte
+  // aligned: the 64-byte records (tens of MB for a large search) are written
+  // once and not read here, so no cache line is fetched before its write.
+  const bool stream = (reinterpret_cast<uintptr_t>(out) & 15u) == 0;
   host_parallel(ndr, [&](size_t lo, size_t hi) {
     for (size_t i = lo; i < hi; i++) {
       const DevRule& r = dr[i];
-      z80b_rule& o = out[i];
+      z80b_rule o;
       const uint32_t* t = targets + (size_t)r.target * stride;
       int tl = tlens ? tlens[r.target] : int(tlen);
       const PoolBufs& PC = (r.clen == 2) ? ctx->pairpool->pool : P;
@@ -1153,7 +1189,20 @@ void to_rules(z80b_ctx* ctx, const DevRule* dr, size_t ndr, const uint32_t* targ
       o.dead_flags = (r.kind == 0) ? 0 : int(r.diff & 0xFFu);
       o.dead_regs = (r.kind == 0) ? 0 : int(r.diff >> 8);
       o.target_index = int(r.target + tindex_offset);
+#if defined(__SSE2__)
+      if (stream) {
+        static_assert(sizeof(z80b_rule) % 16 == 0, "whole 16-byte stores");
+        const __m128i* src = reinterpret_cast<const __m128i*>(&o);
+        __m128i* dst = reinterpret_cast<__m128i*>(out + i);
+        for (size_t k = 0; k < sizeof(z80b_rule) / 16; k++) _mm_stream_si128(dst + k, _mm_loadu_si128(src + k));
+        continue;
+      }
+#endif
+      out[i] = o;
     }
+#if defined(__SSE2__)
+    if (stream) _mm_sfence();
+#endif
   });
 }
 
@@ -1399,6 +1448,11 @@ void z80b_destroy(z80b_ctx* ctx) {
   for (auto& e : ctx->ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : ctx->kev) cudaEventDestroy(e);
+  if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+  for (int i = 0; i < 4; i++) {
+    if (ctx->join_ev[i]) cudaEventDestroy(ctx->join_ev[i]);
+    if (ctx->side[i]) cudaStreamDestroy(ctx->side[i]);
+  }
   cudaStream_t s = ctx->stream;
   delete ctx;
   if (s) cudaStreamDestroy(s);
@@ -1661,6 +1715,10 @@ int z80b_set_option(z80b_ctx* ctx, int option, int value) {
       if (value != 0 && value != 1) return fail(ctx, Z80B_EINVAL, "wide sweep option must be 0 or 1");
       ctx->wide = value;
       return Z80B_OK;
+    case Z80B_OPT_CONCURRENT_SWEEPS:
+      if (value != 0 && value != 1) return fail(ctx, Z80B_EINVAL, "concurrent sweeps option must be 0 or 1");
+      ctx->concurrent_sweeps = value;
+      return Z80B_OK;
   }
   return fail(ctx, Z80B_EINVAL, "unknown option %d", option);
 }
@@ -1676,6 +1734,7 @@ int z80b_get_option(const z80b_ctx* ctx, int option, int* value) {
     case Z80B_OPT_COMPACT_SWEEP: *value = ctx->compact; return Z80B_OK;
     case Z80B_OPT_GRAPH_ROUNDS: *value = ctx->graph_rounds; return Z80B_OK;
     case Z80B_OPT_WIDE_SWEEP: *value = ctx->wide; return Z80B_OK;
+    case Z80B_OPT_CONCURRENT_SWEEPS: *value = ctx->concurrent_sweeps; return Z80B_OK;
   }
   return Z80B_EINVAL;
 }

@@ -2580,26 +2580,27 @@ void warm_exhaustive_dev(const RoundBuf& R, int k) {
 }
 
 int launch_exhaustive_dev(const DevTargets& T, const DevPool& P, const RoundBuf& R, const RoundCtl* ctl, int k,
-                          cudaStream_t s) {
+                          const cudaStream_t* ss) {
   int n = 0;
   if (R.wide) {
-    launch_exhaustive_dev_k<1, 5>(T, P, R, &ctl->totals[4], &ctl->np, s);
-    launch_exhaustive_dev_k<1, 4>(T, P, R, &ctl->totals[3], &ctl->np, s);
+    launch_exhaustive_dev_k<1, 5>(T, P, R, &ctl->totals[4], &ctl->np, ss[0]);
+    launch_exhaustive_dev_k<1, 4>(T, P, R, &ctl->totals[3], &ctl->np, ss[1]);
     n += 2;
   }
   if (R.compact) {
-    launch_exhaustive_dev_k<1, 3>(T, P, R, &ctl->totals[2], &ctl->np, s);
+    launch_exhaustive_dev_k<1, 3>(T, P, R, &ctl->totals[2], &ctl->np, ss[2]);
     n++;
   }
-  launch_exhaustive_dev_k<1, 0>(T, P, R, &ctl->totals[0], &ctl->np, s);
+  launch_exhaustive_dev_k<1, 0>(T, P, R, &ctl->totals[0], &ctl->np, ss[3]);
+  const cudaStream_t sx = ss[4];
   if (R.xunit == kXBitsBlocks) {
-    launch_exhaustive_dev_k<1, 2>(T, P, R, &ctl->totals[1], &ctl->np, s);
+    launch_exhaustive_dev_k<1, 2>(T, P, R, &ctl->totals[1], &ctl->np, sx);
   } else {
     switch (k) {
-      case 1: launch_exhaustive_dev_k<1, 1>(T, P, R, &ctl->totals[1], &ctl->np, s); break;
-      case 2: launch_exhaustive_dev_k<2, 1>(T, P, R, &ctl->totals[1], &ctl->np, s); break;
-      case 8: launch_exhaustive_dev_k<8, 1>(T, P, R, &ctl->totals[1], &ctl->np, s); break;
-      default: launch_exhaustive_dev_k<4, 1>(T, P, R, &ctl->totals[1], &ctl->np, s); break;
+      case 1: launch_exhaustive_dev_k<1, 1>(T, P, R, &ctl->totals[1], &ctl->np, sx); break;
+      case 2: launch_exhaustive_dev_k<2, 1>(T, P, R, &ctl->totals[1], &ctl->np, sx); break;
+      case 8: launch_exhaustive_dev_k<8, 1>(T, P, R, &ctl->totals[1], &ctl->np, sx); break;
+      default: launch_exhaustive_dev_k<4, 1>(T, P, R, &ctl->totals[1], &ctl->np, sx); break;
     }
   }
   return n + 2;

@@ -186,10 +186,14 @@ struct RoundCtl {
 constexpr uint32_t kMaxRoundIters = 1u << 20;
 void launch_round_scan(const RoundBuf& R, RoundCtl* ctl, const uint32_t* refill, cudaGraphConditionalHandle loop,
                        cudaStream_t s);
-// The sweep kernels of the configured classes on a persistent grid, the
+// The sweep kernels of the configured classes on persistent grids, the
 // chunk totals and pair count read from ctl; returns the launches per round.
+// ss[0..4]: the streams of the register-state, wide, compact, bit-sliced
+// and A-independent classes (the classes share no chunk, pair or
+// dispenser, so their launches may run side by side: one class's blocks
+// take the SMs that another's finished blocks leave).
 int launch_exhaustive_dev(const DevTargets& T, const DevPool& P, const RoundBuf& R, const RoundCtl* ctl, int k,
-                          cudaStream_t s);
+                          const cudaStream_t* ss);
 // Sets up (outside any stream capture) the launch facts of the kernels
 // launch_exhaustive_dev will launch for R and k.
 void warm_exhaustive_dev(const RoundBuf& R, int k);

@@ -49,6 +49,8 @@ def main():
     ap.add_argument("--graph-rounds", type=int, default=1, choices=[0, 1],
                     help="first-found rounds driven on the device by one CUDA graph (1) or from the host (0; "
                          "ncu profiles no kernel inside a graph with conditional nodes)")
+    ap.add_argument("--concurrent", type=int, default=1, choices=[0, 1],
+                    help="device-driven rounds: sweep classes on parallel graph branches (1) or in sequence (0)")
     ap.add_argument("--case", default="c2", choices=["c2", "c3", "mulopt"])
     ap.add_argument("--pool", type=int, default=2, help="mulopt pool (Z80B_MULPOOL_*)")
     ap.add_argument("--max-len", type=int, default=9, help="mulopt: longest sequence")
@@ -71,6 +73,7 @@ def main():
         ctx.set_option(z80b.OPT_COMPACT_SWEEP, a.compact)
         ctx.set_option(z80b.OPT_WIDE_SWEEP, a.wide)
         ctx.set_option(z80b.OPT_GRAPH_ROUNDS, a.graph_rounds)
+        ctx.set_option(z80b.OPT_CONCURRENT_SWEEPS, a.concurrent)
         arr, lens, dead, dregs = workloads.c3_targets(a.targets, seed=1)
         targets = [list(map(int, arr[i, :lens[i]])) for i in range(a.targets)]
         job, keep = ctx.make_job(targets, per_target_dead=list(map(int, dead)), dead_regs=list(map(int, dregs)),
@@ -93,6 +96,7 @@ def main():
     ctx.set_option(z80b.OPT_COMPACT_SWEEP, a.compact)
     ctx.set_option(z80b.OPT_WIDE_SWEEP, a.wide)
     ctx.set_option(z80b.OPT_GRAPH_ROUNDS, a.graph_rounds)
+    ctx.set_option(z80b.OPT_CONCURRENT_SWEEPS, a.concurrent)
     job, keep = ctx.make_job(workloads.to_lists(arr), dead_flags=z80b.parse_dead_flags(a.dead_flags))
     for i in range(a.steps):
         t0 = time.perf_counter()

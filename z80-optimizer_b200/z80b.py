@@ -107,6 +107,7 @@ OPT_EXH_LANE_STATES, OPT_EXH_CHUNK_BLOCKS, OPT_STREAM_PRIORITY, OPT_QC_INDEX, OP
 OPT_COMPACT_SWEEP = 6
 OPT_GRAPH_ROUNDS = 7
 OPT_WIDE_SWEEP = 8
+OPT_CONCURRENT_SWEEPS = 9
 JOB_NO_EXHAUSTIVE = 1
 ANSWER_TRUNCATED = 1
 
