@@ -225,6 +225,9 @@ int z80b_exhaustive_noalloc(int device, const uint32_t* tgt, const uint8_t* tlen
                                        byte on the A/F/B..L-state kernel (1, default), or neither (0) */
 #define Z80B_OPT_CONCURRENT_SWEEPS 9 /* device-driven rounds: the sweep classes' kernels on parallel branches of the
                                        round graph (1, default) or one after another (0) */
+#define Z80B_OPT_QC_SINGLE_PASS 10  /* bucket-index QuickCheck: the count pass keeps the survivors of targets with at
+                                       most 8 and the collect pass runs for the others alone (1, default), or the
+                                       collect pass runs for every target (0) */
 int z80b_set_option(z80b_ctx* ctx, int option, int value);
 int z80b_get_option(const z80b_ctx* ctx, int option, int* value);
 

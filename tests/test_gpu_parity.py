@@ -294,10 +294,11 @@ def test_staged_equals_search(ctx):
 
 @pytest.mark.parametrize("all_hits", [False, True])
 def test_qc_index_equals_full_scan(ctx, O, all_hits):
-    """QuickCheck through the pool's bucket index gives the rules, survivor
-    counts and QuickCheck unit counts of the scan over every candidate, under
-    per-target dead flags and dead registers (and, in all-hits mode, the
-    80-byte fingerprint compare over a loaded pool)."""
+    """QuickCheck through the pool's bucket index, in one pass (the count
+    pass keeps the survivors of targets with few) and in two, gives the
+    rules, survivor counts and QuickCheck unit counts of the scan over every
+    candidate, under per-target dead flags and dead registers (and, in
+    all-hits mode, the 80-byte fingerprint compare over a loaded pool)."""
     targets = workloads.to_lists(workloads.c2_subset(4000, seed=21))
     g = workloads.splitmix64(5)
     dead = [next(g) & 0xFF for _ in targets]
@@ -308,13 +309,15 @@ def test_qc_index_equals_full_scan(ctx, O, all_hits):
         kw = dict(dead_flags=0xFF, mode=z80b.MODE_ALL)
     out = []
     try:
-        for on in (0, 1):
+        for on, single in ((0, 1), (1, 0), (1, 1)):
             ctx.set_option(z80b.OPT_QC_INDEX, on)
+            ctx.set_option(z80b.OPT_QC_SINGLE_PASS, single)
             rules, st = ctx.search(targets, **kw)
             out.append((rule_keys(rules), st.checks, st.checked_ref, st.qc_survivors, st.exhaustive_pairs))
     finally:
         ctx.set_option(z80b.OPT_QC_INDEX, 1)
-    assert out[0] == out[1]
+        ctx.set_option(z80b.OPT_QC_SINGLE_PASS, 1)
+    assert out[0] == out[1] == out[2]
     assert len(out[1][0]) > 100
     if not all_hits:
         exp, checked = O.search_ext(targets, 1, dead=dead, dregs=dregs)

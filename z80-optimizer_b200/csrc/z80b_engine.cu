@@ -188,6 +188,7 @@ struct z80b_ctx {
   Staged staged;
   // pipeline scratch
   DBuf cnt_f, cnt_m, cnt_all, base, meta, surv, sdiff, checks;
+  DBuf qc_tmp, qc_over;       // single-pass QuickCheck: kept survivors, targets with more
   DBuf next, win, windiff, spec, spec2, wlen, wend, cdone;
   DBuf pairs, pair_src, nchunks, cbase, nchunks_x, cbase_x, nchunks_c, cbase_c, nchunks_w, cbase_w, nchunks_r,
       cbase_r, rejected, npairs, counter, states;
@@ -213,6 +214,7 @@ struct z80b_ctx {
   uint32_t sweep_kernels = 0; // kSweep* bits of the sweep kernels launched since the last reset
   int graph_rounds = 1;       // Z80B_OPT_GRAPH_ROUNDS
   int concurrent_sweeps = 1;  // Z80B_OPT_CONCURRENT_SWEEPS
+  int qc_single = 1;          // Z80B_OPT_QC_SINGLE_PASS
   // capture-time streams and events of the device rounds' parallel sweep
   // branches (created with the first graph that uses them)
   cudaStream_t side[4] = {};
@@ -870,8 +872,19 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
   q.cnt_all = ctx->cnt_all.as<uint32_t>();
   q.meta = ctx->meta.as<TargetMeta>();
   q.checks = ctx->checks.as<unsigned long long>();
-  if (use_ix) launch_qc_bucket(T, P, cfg, qix, q, false, s);
-  else launch_qc_scan(T, P, cfg, q, false, s);
+  if (use_ix && ctx->qc_single) {
+    // single pass: the count pass keeps the survivors of targets with few
+    CK(ctx->qc_tmp.ensure(4ull * kQCSlots * n));
+    CK(ctx->qc_over.ensure(4));
+    CK(cudaMemsetAsync(ctx->qc_over.p, 0, 4, s));
+    q.tmp = ctx->qc_tmp.as<uint32_t>();
+    q.over = ctx->qc_over.as<uint32_t>();
+    launch_qc_bucket(T, P, cfg, qix, q, false, s);
+  } else if (use_ix) {
+    launch_qc_bucket(T, P, cfg, qix, q, false, s);
+  } else {
+    launch_qc_scan(T, P, cfg, q, false, s);
+  }
   kend(ctx, kq);
   CKR(check_launch(ctx, "qc_count"));
   CKR(scan(ctx, ctx->cnt_all.as<uint32_t>(), ctx->base.as<uint32_t>(), n));
@@ -879,6 +892,7 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
   CK(cudaMemcpyAsync(&last[0], ctx->base.as<uint32_t>() + (n - 1), 4, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(&last[1], ctx->cnt_f.as<uint32_t>() + (n - 1), 4, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(&last[2], ctx->cnt_m.as<uint32_t>() + (n - 1), 4, cudaMemcpyDeviceToHost, s));
+  if (q.over) CK(cudaMemcpyAsync(&last[3], q.over, 4, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   const uint64_t nsurv = uint64_t(last[0]) + last[1] + last[2];
   trace("qc count done: %llu survivors", (unsigned long long)nsurv);
@@ -888,7 +902,15 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
   q.base = ctx->base.as<uint32_t>();
   q.surv = ctx->surv.as<uint32_t>();
   q.sdiff = ctx->sdiff.as<uint16_t>();
-  if (nsurv) {
+  if (nsurv && q.tmp) {
+    int kc = kbegin(ctx, 0);
+    launch_qc_compact(q, n, s);
+    kend(ctx, kc);
+    CKR(check_launch(ctx, "qc_compact"));
+  }
+  if (nsurv && (!q.tmp || last[3])) {
+    // every target (two passes), or those with more survivors than the
+    // count pass kept
     int kc = kbegin(ctx, 0);
     if (use_ix) launch_qc_bucket(T, P, cfg, qix, q, true, s);
     else launch_qc_scan(T, P, cfg, q, true, s);
@@ -1719,6 +1741,10 @@ int z80b_set_option(z80b_ctx* ctx, int option, int value) {
       if (value != 0 && value != 1) return fail(ctx, Z80B_EINVAL, "concurrent sweeps option must be 0 or 1");
       ctx->concurrent_sweeps = value;
       return Z80B_OK;
+    case Z80B_OPT_QC_SINGLE_PASS:
+      if (value != 0 && value != 1) return fail(ctx, Z80B_EINVAL, "QuickCheck single-pass option must be 0 or 1");
+      ctx->qc_single = value;
+      return Z80B_OK;
   }
   return fail(ctx, Z80B_EINVAL, "unknown option %d", option);
 }
@@ -1735,6 +1761,7 @@ int z80b_get_option(const z80b_ctx* ctx, int option, int* value) {
     case Z80B_OPT_GRAPH_ROUNDS: *value = ctx->graph_rounds; return Z80B_OK;
     case Z80B_OPT_WIDE_SWEEP: *value = ctx->wide; return Z80B_OK;
     case Z80B_OPT_CONCURRENT_SWEEPS: *value = ctx->concurrent_sweeps; return Z80B_OK;
+    case Z80B_OPT_QC_SINGLE_PASS: *value = ctx->qc_single; return Z80B_OK;
   }
   return Z80B_EINVAL;
 }
@@ -2063,6 +2090,7 @@ uint64_t target_frontier_bytes(const uint32_t* seq, int len, int max_cand, bool 
   const uint64_t passes = masked ? 2 : 1;
   uint64_t b = 4ull * 4 + 4 + 3;                          // target words, length, dead flags and registers
   b += 4ull * 4 + sizeof(TargetMeta);                      // cnt_f, cnt_m, cnt_all, base, meta
+  b += 4ull * kQCSlots;                                    // survivors the count pass keeps
   b += passes * uint64_t(elig_lt[size_t(tb)]) * (4 + 2);   // survivor indices and flag differences
   b += 8 + 8 + 4 + 2;                                      // next, win, windiff, spec
   b += 128ull * (sizeof(PairRec) + 4 + 8 * 6 + 4 + 1);     // pair slots of the windows (cap 128 per target)

@@ -1376,6 +1376,26 @@ __device__ __noinline__ bool xindep_unit(unsigned long long first, unsigned long
 #ifndef Z80B_REG_BLOCKS
 #define Z80B_REG_BLOCKS 2
 #endif
+// The pair whose chunk range holds chunk k: the last p with cbase[p] <= k
+// (cbase ascending from cbase[0] = 0; pairs without chunks in the class
+// repeat their successor's base).  Warp-wide, k the same in every lane: each
+// step the 32 lanes probe 32 evenly spaced pairs of the range left and a
+// ballot keeps the span after the last probe that is <= k, so a round of n
+// pairs takes ceil(log32 n) dependent loads instead of log2 n.
+__device__ __forceinline__ uint32_t chunk_pair(const unsigned long long* __restrict__ cbase, uint32_t npairs,
+                                               unsigned long long k, unsigned lane) {
+  uint32_t lo = 0, n = npairs;  // the answer lies in [lo, lo + n); cbase[lo] <= k
+  while (n > 1) {
+    const uint32_t step = (n + 31u) / 32u;
+    const uint32_t off = lane * step;
+    const bool le = off < n && cbase[lo + off] <= k;
+    const unsigned b = __ballot_sync(kFull, le);  // a prefix of the lanes, lane 0 always
+    const uint32_t last = 31u - uint32_t(__clz(b));
+    lo += last * step;
+    n = min(step, n - last * step);
+  }
+  return lo;
+}
 template <int K, int CLS>
 __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : (CLS == 4 ? 2 : (CLS == 5 ? Z80B_REG_BLOCKS : 1)))
     k_exhaustive(DevTargets T, DevPool P, RoundBuf R, uint32_t npairs, unsigned long long total,
@@ -1400,13 +1420,7 @@ __global__ void __launch_bounds__(kBlock, CLS == 3 ? 3 : (CLS == 4 ? 2 : (CLS ==
     k = __shfl_sync(kFull, k, 0);
     if (k >= total) break;
     // pair p: cbase[p] <= k < cbase[p + 1]
-    uint32_t lo = 0, hi = npairs - 1;
-    while (lo < hi) {
-      uint32_t mid = (lo + hi + 1) >> 1;
-      if (cbase[mid] <= k) lo = mid;
-      else hi = mid - 1;
-    }
-    const uint32_t p = lo;
+    const uint32_t p = chunk_pair(cbase, npairs, k, lane);
     // lane 0 reads the flag and the warp acts on one value, so the
     // shuffles below always see all 32 lanes
     if (__shfl_sync(kFull, lane == 0 ? *reinterpret_cast<volatile uint32_t*>(&R.rejected[p]) : 0u, 0))
@@ -1953,8 +1967,10 @@ __device__ __forceinline__ void qc_target4(const DevTargets& T, uint32_t t, bool
             ((dregs & 32u) ? 0u : 0xFF000000u);
 }
 
-template <bool COLLECT>
-__global__ void __launch_bounds__(kBlock) k_qc_bucket(DevTargets T, DevPool P, QCConfig cfg, QCIndex ix, QCOut o) {
+// COLLECT: the collect pass; else the count pass, which with KEEP also keeps
+// the survivors of targets with at most kQCSlots (single pass).
+template <bool COLLECT, bool KEEP>
+__global__ void __launch_bounds__(kBlock, 4) k_qc_bucket(DevTargets T, DevPool P, QCConfig cfg, QCIndex ix, QCOut o) {
   const unsigned lane = lane_id();
   const unsigned sub = lane & 7u, gshift = lane & ~7u;
   const unsigned group_lt = lanemask_lt() & (0xFFu << gshift);
@@ -1969,7 +1985,10 @@ __global__ void __launch_bounds__(kBlock) k_qc_bucket(DevTargets T, DevPool P, Q
     if (COLLECT) {
       if (valid) {
         nf_total = o.cnt_f[t];
-        work = nf_total + o.cnt_m[t] != 0;
+        const uint32_t tot = nf_total + o.cnt_m[t];
+        // single pass: the count pass kept the survivors of targets with at
+        // most kQCSlots of them
+        work = o.tmp ? tot > kQCSlots : tot != 0;
         obase = o.base[t];
       }
       if (!__any_sync(kFull, work)) continue;
@@ -1986,6 +2005,8 @@ __global__ void __launch_bounds__(kBlock) k_qc_bucket(DevTargets T, DevPool P, Q
     }
     const uint32_t iters = (__reduce_max_sync(kFull, r1 - r0) + 7u) / 8u;
     uint32_t nf = 0, nm = 0, lf = 0, lm = 0;
+    uint32_t nk = 0;  // this group's survivors so far (count pass, single pass)
+    uint32_t* const keep = KEEP ? o.tmp + (size_t)t * kQCSlots : nullptr;
     for (uint32_t k = 0; k < iters; k++) {
       const uint32_t i = r0 + 8u * k + sub;
       bool fp = false, mp = false;
@@ -1999,6 +2020,15 @@ __global__ void __launch_bounds__(kBlock) k_qc_bucket(DevTargets T, DevPool P, Q
       if constexpr (!COLLECT) {
         lf += fp ? 1u : 0u;
         lm += mp ? 1u : 0u;
+        if constexpr (KEEP) {
+          const bool sv = fp || mp;
+          const unsigned bs = __ballot_sync(kFull, sv);
+          if (bs) {  // most steps find nothing
+            const uint32_t rank = nk + __popc(bs & group_lt);
+            if (sv && rank < kQCSlots) keep[rank] = c | (diff << 16) | (mp ? 0x80000000u : 0u);
+            nk += __popc((bs >> gshift) & 0xFFu);
+          }
+        }
       } else {
         // this group's survivors of the step, in enumeration order
         const unsigned bf = __ballot_sync(kFull, fp), bm = __ballot_sync(kFull, mp);
@@ -2025,12 +2055,31 @@ __global__ void __launch_bounds__(kBlock) k_qc_bucket(DevTargets T, DevPool P, Q
       if (sub == 0 && valid) {
         my_checks += ix.elig_lt[g.tb < 255u ? g.tb : 255u];
         qc_count_out(o, t, g, lf, lm);
+        if (KEEP && lf + lm > kQCSlots) atomicAdd(o.over, 1u);
       }
     }
   }
   if constexpr (!COLLECT) {
     for (int off = 16; off; off >>= 1) my_checks += __shfl_down_sync(kFull, my_checks, off);
     if (lane == 0 && my_checks) atomicAdd(o.checks, my_checks);
+  }
+}
+
+// Thread per target: the survivors the single-pass count kept go to
+// base[t] + (full ones in order, then masked ones in order), as the collect
+// pass would have placed them.
+__global__ void __launch_bounds__(256) k_qc_compact(QCOut o, uint32_t n) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const uint32_t nf = o.cnt_f[t], tot = nf + o.cnt_m[t];
+  if (tot == 0 || tot > kQCSlots) return;
+  const uint32_t* __restrict__ kept = o.tmp + (size_t)t * kQCSlots;
+  uint32_t jf = o.base[t], jm = jf + nf;
+  for (uint32_t j = 0; j < tot; j++) {
+    const uint32_t e = kept[j];
+    const uint32_t idx = (e >> 31) ? jm++ : jf++;
+    o.surv[idx] = e & 0xFFFFu;
+    o.sdiff[idx] = uint16_t((e >> 16) & 0x7FFFu);
   }
 }
 
@@ -2313,17 +2362,25 @@ void launch_qc_top(const unsigned long long* keys, uint32_t nv, uint32_t* top, c
   const uint32_t n = 64u * (kQCTop + 1);
   k_qc_top<<<grid_for(n, 256), 256, 0, s>>>(keys, nv, top);
 }
+void launch_qc_compact(const QCOut& q, uint32_t n, cudaStream_t s) {
+  if (!n) return;
+  k_qc_compact<<<grid_for(n, 256), 256, 0, s>>>(q, n);
+}
+
 void launch_qc_bucket(const DevTargets& T, const DevPool& P, const QCConfig& cfg, const QCIndex& ix,
                       const QCOut& o, bool collect, cudaStream_t s) {
   if (!T.n) return;
-  static std::atomic<int> occ[2][kMaxCachedDevices];
-  const int per_sm = collect ? blocks_per_sm(occ[1], k_qc_bucket<true>, kBlock, 0, 0)
-                             : blocks_per_sm(occ[0], k_qc_bucket<false>, kBlock, 0, 0);
+  static std::atomic<int> occ[3][kMaxCachedDevices];
+  const bool keep = !collect && o.tmp;
+  const int per_sm = collect ? blocks_per_sm(occ[1], k_qc_bucket<true, false>, kBlock, 0, 0)
+                             : (keep ? blocks_per_sm(occ[2], k_qc_bucket<false, true>, kBlock, 0, 0)
+                                     : blocks_per_sm(occ[0], k_qc_bucket<false, false>, kBlock, 0, 0));
   unsigned need = grid_for((T.n + 3u) / 4u, kBlock / 32);  // four targets per warp
   unsigned grid = unsigned(dev_num_sms() * per_sm);
   if (grid > need) grid = need;
-  if (collect) k_qc_bucket<true><<<grid, kBlock, 0, s>>>(T, P, cfg, ix, o);
-  else k_qc_bucket<false><<<grid, kBlock, 0, s>>>(T, P, cfg, ix, o);
+  if (collect) k_qc_bucket<true, false><<<grid, kBlock, 0, s>>>(T, P, cfg, ix, o);
+  else if (keep) k_qc_bucket<false, true><<<grid, kBlock, 0, s>>>(T, P, cfg, ix, o);
+  else k_qc_bucket<false, false><<<grid, kBlock, 0, s>>>(T, P, cfg, ix, o);
 }
 void launch_round_build(const DevTargets& T, const DevPool& P, const QCOut& q, const Lanes& L,
                         const RoundBuf& R, cudaStream_t s) {

@@ -18,7 +18,16 @@ struct QCOut {
   uint16_t* sdiff;   // FlagDiff (low byte) | differing registers << 8
   TargetMeta* meta;  // [n]
   unsigned long long* checks;  // eligible pairs evaluated (count pass)
+  // Single-pass QuickCheck (bucket index only; null: count and collect
+  // passes): the count pass also keeps the survivors of each target that has
+  // at most kQCSlots of them, in enumeration order, as candidate | diff << 16
+  // | masked << 31 in tmp[t * kQCSlots ...], and counts the targets with more
+  // in *over; k_qc_compact moves the kept ones to their places and the
+  // collect pass runs for the others alone.
+  uint32_t* tmp;
+  uint32_t* over;
 };
+constexpr uint32_t kQCSlots = 8;
 
 struct QCConfig {
   uint32_t w2mask;   // 0xFFFFFFFF: compare SP and M; 0x0000FFFF: fingerprint (SP only)
@@ -127,6 +136,10 @@ struct DevRule {
   uint8_t clen;    // candidate length: 1 (pool index) or 2 (pair-pool index)
 };
 
+// Moves the survivors the count pass kept (targets with 1..kQCSlots) to
+// their places after base[t]: the full ones first, then the masked ones,
+// each in enumeration order.
+void launch_qc_compact(const QCOut& q, uint32_t n, cudaStream_t s);
 void dev_upload_tables(cudaStream_t s);
 int dev_num_sms();
 

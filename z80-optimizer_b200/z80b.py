@@ -108,6 +108,7 @@ OPT_COMPACT_SWEEP = 6
 OPT_GRAPH_ROUNDS = 7
 OPT_WIDE_SWEEP = 8
 OPT_CONCURRENT_SWEEPS = 9
+OPT_QC_SINGLE_PASS = 10
 JOB_NO_EXHAUSTIVE = 1
 ANSWER_TRUNCATED = 1
 
