@@ -112,7 +112,15 @@ struct PipeOpts {
   uint64_t dreg_masks = 1;      // bit m: dead-register mask m occurs in a masked pass (bit 0 always)
   bool no_exhaustive = false;   // all-hits mode: MidCheck survivors are the rules (Z80B_JOB_NO_EXHAUSTIVE)
   Reporter* rep = nullptr;      // per-target answers as they become final (first-found mode)
+  // Targets uploaded in chunks on the copy stream (z80b_search on large
+  // jobs): chunk k holds targets [up_hi[k-1], up_hi[k]) and is complete at
+  // the context's up_ev[k]; the QuickCheck count runs chunk by chunk behind
+  // the copies.  0: the targets are on the device before the pipeline starts.
+  int up_chunks = 0;
+  const uint32_t* up_hi = nullptr;
 };
+constexpr int kUpChunks = 4;
+constexpr uint32_t kUpChunkMin = 1u << 16;  // targets; smaller jobs upload in one copy
 
 // The 4,531^2 pair pool, its QuickCheck outputs and its bucket indexes (one
 // per dead-register mask, built on first use).  Read-only once built, so all
@@ -151,6 +159,8 @@ struct Staged {
   z80b_job job{};
   bool valid = false;
   DBuf d_targets, d_lens, d_dead, d_dregs;
+  int up_chunks = 0;            // the last upload's chunks (PipeOpts::up_chunks)
+  uint32_t up_hi[kUpChunks] = {};
 };
 
 }  // namespace
@@ -219,6 +229,10 @@ struct z80b_ctx {
   // branches (created with the first graph that uses them)
   cudaStream_t side[4] = {};
   cudaEvent_t fork_ev = nullptr, join_ev[4] = {};
+  // chunked target uploads: the copy stream, one event per chunk and one
+  // that orders the copies after the context stream's earlier work
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t up_ev[kUpChunks + 1] = {};
   DBuf roundctl;              // RoundCtl of the device-driven rounds
   RoundGraph rg1, rg2;        // instantiated round loops: length-1 and length-2 candidate passes
 };
@@ -862,10 +876,6 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
     }
   }
   trace("pipeline: %u targets, mode %u, pool %u", n, mode, P.n);
-  Timer tall{ctx, 0, 1};
-  ctx->kev_used = 0;
-  tall.start();
-  int kq = kbegin(ctx, 0);
   QCOut q{};
   q.cnt_f = ctx->cnt_f.as<uint32_t>();
   q.cnt_m = ctx->cnt_m.as<uint32_t>();
@@ -879,14 +889,45 @@ int run_pipeline(z80b_ctx* ctx, const DevTargets& T, const PipeOpts& opts, z80b_
     CK(cudaMemsetAsync(ctx->qc_over.p, 0, 4, s));
     q.tmp = ctx->qc_tmp.as<uint32_t>();
     q.over = ctx->qc_over.as<uint32_t>();
-    launch_qc_bucket(T, P, cfg, qix, q, false, s);
-  } else if (use_ix) {
-    launch_qc_bucket(T, P, cfg, qix, q, false, s);
+  }
+  // the count over targets [lo, hi) (every per-target array offset by lo)
+  auto qc_count = [&](uint32_t lo, uint32_t hi) {
+    DevTargets Tc = T;
+    QCOut qc = q;
+    if (lo) {
+      Tc.insn += (size_t)lo * T.stride;
+      if (Tc.len) Tc.len += lo;
+      if (Tc.dead) Tc.dead += lo;
+      if (Tc.dead_regs) Tc.dead_regs += lo;
+      qc.cnt_f += lo;
+      qc.cnt_m += lo;
+      qc.cnt_all += lo;
+      qc.meta += lo;
+      if (qc.tmp) qc.tmp += (size_t)lo * kQCSlots;
+    }
+    Tc.n = hi - lo;
+    if (use_ix) launch_qc_bucket(Tc, P, cfg, qix, qc, false, s);
+    else launch_qc_scan(Tc, P, cfg, qc, false, s);
+    return check_launch(ctx, "qc_count");
+  };
+  // chunked upload: the first chunk is on the device before the clock starts
+  if (opts.up_chunks) CK(cudaStreamWaitEvent(s, ctx->up_ev[0], 0));
+  Timer tall{ctx, 0, 1};
+  ctx->kev_used = 0;
+  tall.start();
+  int kq = kbegin(ctx, 0);
+  if (opts.up_chunks) {
+    uint32_t lo = 0;
+    for (int k = 0; k < opts.up_chunks; k++) {
+      const uint32_t hi = opts.up_hi[k];
+      if (k) CK(cudaStreamWaitEvent(s, ctx->up_ev[k], 0));
+      if (hi > lo) CKR(qc_count(lo, hi));
+      lo = hi;
+    }
   } else {
-    launch_qc_scan(T, P, cfg, q, false, s);
+    CKR(qc_count(0, n));
   }
   kend(ctx, kq);
-  CKR(check_launch(ctx, "qc_count"));
   CKR(scan(ctx, ctx->cnt_all.as<uint32_t>(), ctx->base.as<uint32_t>(), n));
   uint32_t last[4] = {0, 0, 0, 0};
   CK(cudaMemcpyAsync(&last[0], ctx->base.as<uint32_t>() + (n - 1), 4, cudaMemcpyDeviceToHost, s));
@@ -1319,7 +1360,29 @@ int upload_targets(z80b_ctx* ctx, Staged& S, const z80b_job* job, DevTargets* T,
     }
   cudaStream_t s = ctx->stream;
   CK(S.d_targets.ensure(4ull * std::max<size_t>(words, 1)));
-  if (n) CK(cudaMemcpyAsync(S.d_targets.p, job->targets, 4ull * words, cudaMemcpyHostToDevice, s));
+  S.up_chunks = 0;
+  if (!keep_host && n >= kUpChunkMin) {
+    // in chunks on the copy stream, so that the QuickCheck count of the
+    // first chunks runs while the rest are copied
+    if (!ctx->copy_stream) {
+      CK(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+      for (auto& e : ctx->up_ev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    CK(cudaEventRecord(ctx->up_ev[kUpChunks], s));  // after the stream's earlier use of the buffers
+    CK(cudaStreamWaitEvent(ctx->copy_stream, ctx->up_ev[kUpChunks], 0));
+    const size_t stride = job->target_stride;
+    for (int k = 0; k < kUpChunks; k++) {
+      const size_t lo = (size_t)n * k / kUpChunks, hi = (size_t)n * (k + 1) / kUpChunks;
+      if (hi > lo)
+        CK(cudaMemcpyAsync(S.d_targets.as<uint32_t>() + lo * stride, job->targets + lo * stride,
+                           4ull * (hi - lo) * stride, cudaMemcpyHostToDevice, ctx->copy_stream));
+      CK(cudaEventRecord(ctx->up_ev[k], ctx->copy_stream));
+      S.up_hi[k] = uint32_t(hi);
+    }
+    S.up_chunks = kUpChunks;
+  } else if (n) {
+    CK(cudaMemcpyAsync(S.d_targets.p, job->targets, 4ull * words, cudaMemcpyHostToDevice, s));
+  }
   *T = DevTargets{};
   T->insn = S.d_targets.as<uint32_t>();
   T->n = n;
@@ -1471,6 +1534,10 @@ void z80b_destroy(z80b_ctx* ctx) {
     if (e) cudaEventDestroy(e);
   for (auto& e : ctx->kev) cudaEventDestroy(e);
   if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+  if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+  for (auto& e : ctx->up_ev)
+    if (e) cudaEventDestroy(e);
+  if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   for (int i = 0; i < 4; i++) {
     if (ctx->join_ev[i]) cudaEventDestroy(ctx->join_ev[i]);
     if (ctx->side[i]) cudaStreamDestroy(ctx->side[i]);
@@ -1912,12 +1979,15 @@ static int search_impl(z80b_ctx* ctx, const z80b_job* job, z80b_rule* out, uint6
     const int v = validate_targets(ctx, job);
     if (v != Z80B_OK) {
       cudaStreamSynchronize(ctx->stream);
+      if (ctx->staged.up_chunks) cudaStreamSynchronize(ctx->copy_stream);
       return v;
     }
   }
   uint64_t nr = 0;
   if (job->path == Z80B_PATH_PLAIN) {
     std::vector<z80b_rule> hr;
+    // the chunks are copied in order: the last one's event covers them all
+    if (ctx->staged.up_chunks) CK(cudaStreamWaitEvent(ctx->stream, ctx->up_ev[kUpChunks - 1], 0));
     CKR(run_staged(ctx, stats, &nr, &hr, job->targets));
     *n_rules = nr;
     if (stats) stats->launches = ctx->launches;
@@ -1927,6 +1997,8 @@ static int search_impl(z80b_ctx* ctx, const z80b_job* job, z80b_rule* out, uint6
                     : Z80B_OK;
   }
   PipeOpts opts = ctx->staged.opts;
+  opts.up_chunks = ctx->staged.up_chunks;
+  opts.up_hi = ctx->staged.up_hi;
   if (rep && job->mode == Z80B_MODE_FIRST) {
     rep->targets = job->targets;
     rep->tlens = job->target_lens;
@@ -1935,7 +2007,12 @@ static int search_impl(z80b_ctx* ctx, const z80b_job* job, z80b_rule* out, uint6
     rep->done.assign(job->n_targets, 0);
     opts.rep = rep;
   }
-  CKR(run_pipeline(ctx, T, opts, stats, &nr));
+  {
+    const int r = run_pipeline(ctx, T, opts, stats, &nr);
+    // copies still reading the caller's targets end before it gets them back
+    if (opts.up_chunks) cudaStreamSynchronize(ctx->copy_stream);
+    CKR(r);
+  }
   if (stats) stats->launches = ctx->launches;
   *n_rules = nr;
   if (nr > cap)
