@@ -49,3 +49,12 @@ def test_init_without_device_fails_loudly():
     with pytest.raises(z80b.Z80BError) as e:
         z80b.Context(0)
     assert e.value.status == z80b.ENODEV
+
+
+def test_option_numbers_match_header():
+    """The Python binding's option constants are the header's Z80B_OPT_*."""
+    text = open(os.path.join(ROOT, "include", "z80b200.h")).read()
+    defs = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define Z80B_(OPT_\w+)\s+(\d+)", text)}
+    assert len(defs) >= 10
+    for name, value in defs.items():
+        assert getattr(z80b, name) == value, name
