@@ -159,7 +159,10 @@ int z80b_verify_pairs(z80b_ctx* ctx, const uint32_t* tgt, const uint8_t* tlens,
 /* Runs the job and writes its rules (grouped by target index; within a
  * target the full-equivalence rule precedes the masked one, and all-hits
  * rules follow candidate order).  Writes up to cap rules and the total to
- * *n_rules (Z80B_ECAPACITY if it did not fit).  stats may be NULL. */
+ * *n_rules (Z80B_ECAPACITY if it did not fit).  stats may be NULL.  The
+ * job's arrays are read during the call only (targets in page-locked memory
+ * are copied by DMA, in chunks for large jobs, while the host checks them);
+ * the call returns after its GPU work has finished. */
 int z80b_search(z80b_ctx* ctx, const z80b_job* job, z80b_rule* out, uint64_t cap,
                 uint64_t* n_rules, z80b_stats* stats);
 
