@@ -1986,8 +1986,9 @@ static int search_impl(z80b_ctx* ctx, const z80b_job* job, z80b_rule* out, uint6
   uint64_t nr = 0;
   if (job->path == Z80B_PATH_PLAIN) {
     std::vector<z80b_rule> hr;
-    // the chunks are copied in order: the last one's event covers them all
-    if (ctx->staged.up_chunks) CK(cudaStreamWaitEvent(ctx->stream, ctx->up_ev[kUpChunks - 1], 0));
+    // one target per launch: the whole upload first (nothing of the copy
+    // is left in flight whatever run_staged returns)
+    if (ctx->staged.up_chunks) CK(cudaStreamSynchronize(ctx->copy_stream));
     CKR(run_staged(ctx, stats, &nr, &hr, job->targets));
     *n_rules = nr;
     if (stats) stats->launches = ctx->launches;
